@@ -1,0 +1,241 @@
+/*
+ * ripples_b200.h -- C ABI of the B200-native IMM hot path.
+ *
+ * The reference (pnnl/ripples) exposes this path as header-only C++ templates:
+ *   ripples::IMM                      include/ripples/imm.h:671,768
+ *   ripples::GenerateRRRSets          include/ripples/generate_rrr_sets.h:186,217
+ *   StreamingRRRGenerator::generate   include/ripples/streaming_rrr_generator.h:1026
+ *   ripples::FindMostInfluentialSet   include/ripples/find_most_influential.h:85,176
+ * and its CUDA side through GPU<R>::device_malloc/h2d/d2h
+ * (include/ripples/gpu/gpu_runtime_trait.h:64-320).  This header is the plain
+ * C boundary those templates call instead: plain pointers and sizes, no C++ or
+ * torch types.
+ *
+ * Conventions
+ *   - Every entry point returns an int status: RIP_OK (0) or a negative
+ *     RIP_ERR_* code.  A human-readable message for the last failure on a
+ *     context is returned by rip_last_error().  Nothing aborts the process.
+ *     (The reference prints CUDA errors and continues, src/gpu/cuda_utils.cu:53-59,
+ *     or calls exit(-1), include/ripples/graph.h:866-935.)
+ *   - Host arrays passed in are read during the call and never retained.
+ *   - Vertex ids are uint32 in [0, n); in-edge lists follow the reference's
+ *     backward CSR (GraphBwd, include/ripples/graph.h:107-130): the in-neighbours
+ *     of v are src[index[v] .. index[v+1]).
+ *   - One context = one CUDA device + one stream.  A context is not re-entrant;
+ *     use one context per host thread (the reference is single-threaded at this
+ *     boundary too, include/ripples/imm.h:768).
+ */
+#ifndef RIPPLES_B200_H
+#define RIPPLES_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+#define RIP_OK 0
+#define RIP_ERR_INVALID (-1)   /* bad argument (null pointer, id out of range) */
+#define RIP_ERR_CUDA (-2)      /* a CUDA runtime call failed                    */
+#define RIP_ERR_NOMEM (-3)     /* device or host allocation failed / budget     */
+#define RIP_ERR_STATE (-4)     /* call not valid in the object's current state  */
+#define RIP_ERR_LIMIT (-5)     /* input beyond a documented size limit          */
+#define RIP_ERR_DEVICE (-6)    /* a kernel reported an internal error flag      */
+
+/* ---- enums ---------------------------------------------------------------- */
+/* Diffusion models: independent_cascade_tag / linear_threshold_tag
+ * (include/ripples/diffusion_simulation.h). */
+#define RIP_MODEL_IC 0
+#define RIP_MODEL_LT 1
+
+/* Seed-selection tie-break.  REF_HEAP reproduces the reference CPU lazy
+ * max-heap order (include/ripples/streaming_find_most_influential.h:410-418,
+ * 546-572); LOWEST_ID reproduces the reference GPU selection, which takes
+ * thrust::max_element (src/gpu/find_most_influential.cc:65-72). */
+#define RIP_TIE_REF_HEAP 0
+#define RIP_TIE_LOWEST_ID 1
+
+/* IC sampler variants (LT always uses the walk kernel). */
+#define RIP_SAMPLER_AUTO 0   /* fused multi-colour BFS                        */
+#define RIP_SAMPLER_PLAIN 1  /* one set per warp                              */
+#define RIP_SAMPLER_FUSED 2  /* fused multi-colour reverse BFS                */
+
+/* Synthetic edge-weight models (for graph construction helpers). */
+#define RIP_WEIGHTS_UNIFORM 0       /* U(lo, hi) per edge                       */
+#define RIP_WEIGHTS_LT_NORMALIZED 1 /* U(0,1) then normalised per destination   */
+#define RIP_WEIGHTS_WC 2            /* weighted cascade: 1 / in-degree(dst)     */
+
+typedef struct rip_ctx rip_ctx;
+typedef struct rip_graph rip_graph;
+typedef struct rip_pool rip_pool;
+
+/* ---- context -------------------------------------------------------------- */
+/* Replaces the per-GPU runtime set-up of the streaming engine
+ * (include/ripples/streaming_rrr_generator.h:866-872, gpu_runtime_trait.h:64-160).
+ * hbm_budget: bytes this context may allocate on the device (0 = 90% of free). */
+int rip_ctx_create(int device, size_t hbm_budget, rip_ctx **out);
+int rip_ctx_destroy(rip_ctx *ctx);
+const char *rip_last_error(const rip_ctx *ctx);
+int rip_sync(rip_ctx *ctx);
+/* Device bytes currently held by the context (graphs, pools, scratch). */
+int rip_ctx_memory(rip_ctx *ctx, size_t *used, size_t *budget);
+/* Library version string, e.g. "ripples_b200 0.1.0 sm_100a". */
+const char *rip_version(void);
+
+/* ---- graph ---------------------------------------------------------------- */
+/* Uploads a backward CSR (GraphBwd) and packs it for the kernels: weights are
+ * converted once to uint32 thresholds (IC: floor(w*2^32); LT: cumulative
+ * in-weight in CSR order).  Replaces make_gpu_context / gpu_graph upload
+ * (include/ripples/gpu/gpu_graph.h:47-96, src/gpu/gpu_graph.cc:48-84).
+ * Limits: n < 2^32 - 1, m < 2^32. */
+int rip_graph_upload(rip_ctx *ctx, const uint64_t *index, const uint32_t *src,
+                     const float *weights, uint32_t n, uint64_t m, int model,
+                     rip_graph **out);
+int rip_graph_destroy(rip_graph *g);
+int rip_graph_info(const rip_graph *g, uint32_t *n, uint64_t *m, int *model);
+/* Copies the packed per-edge thresholds (m values) back to the host. */
+int rip_graph_thresholds(rip_graph *g, uint32_t *thr);
+
+/* ---- RRR pool --------------------------------------------------------------- */
+/* A device-resident, growable flat pool of RRR sets, addressed by set id
+ * 0, 1, 2, ...  Replaces RRRsets = std::vector<std::vector<uint32_t>>
+ * (include/ripples/rrr_sets.h:84-105). */
+int rip_pool_create(rip_ctx *ctx, rip_graph *g, rip_pool **out);
+int rip_pool_destroy(rip_pool *p);
+/* Drops every set (keeps the allocation). */
+int rip_pool_clear(rip_pool *p);
+int rip_pool_info(const rip_pool *p, uint64_t *num_sets, uint64_t *num_elements);
+
+/* Appends `count` sets with ids num_sets .. num_sets+count-1 sampled under the
+ * graph's model with the given seed.  Set contents depend only on
+ * (graph, seed, set id), never on batching, sampler variant or stream order.
+ * Replaces GenerateRRRSets(G, gen, begin, end, record, model_tag, ex_tag)
+ * (include/ripples/generate_rrr_sets.h:186-224), whose sets were pre-inserted
+ * by the caller (include/ripples/imm.h:199-200). */
+int rip_sample(rip_pool *p, uint64_t seed, uint64_t count, int sampler);
+
+/* Copies sets [first, first+count) to host buffers: offsets has count+1
+ * entries (offsets[0] = 0), vertices has offsets[count] entries.  Each set is
+ * sorted ascending, as AddRRRSet leaves it (include/ripples/add_rrrset.h:156).
+ * Call with vertices == NULL to learn the sizes (offsets still written). */
+int rip_pool_export(rip_pool *p, uint64_t first, uint64_t count,
+                    uint64_t *offsets, uint32_t *vertices);
+/* Appends `count` host sets (CSR: offsets[count+1], vertices).  Lets tests feed
+ * the reference's own sets to the device selection. */
+int rip_pool_import(rip_pool *p, const uint64_t *offsets,
+                    const uint32_t *vertices, uint64_t count);
+
+/* Device counters of the sampling kernels since the pool was created/cleared:
+ * stats[0] = vertex expansions (a vertex's in-edge list read once, whatever
+ * number of sets it served), stats[1] = in-edges read, stats[2] = sets
+ * written, stats[3] = pool elements written, stats[4] = per-set expansions
+ * (sum over sets of vertices expanded), stats[5] = per-set in-edges
+ * (sum over sets of in-edges of the expanded vertices). */
+int rip_pool_stats(rip_pool *p, uint64_t stats[8]);
+
+/* Kernel time (CUDA events on the context stream) spent in the sampler
+ * launches and in rip_select since the pool was created/cleared. */
+int rip_pool_timing(rip_pool *p, double *sample_kernel_ms, uint64_t *launches,
+                    double *select_ms);
+
+/* Fused-sampler knobs (what the autotuner sets): colour width 64/128/256,
+ * CTA slots (0 = size from the budget), frontier-log entries per slot
+ * (0 = default).  No reference counterpart: the reference fixes the colour
+ * width per run (--gpu-batch-size, include/ripples/imm_configuration.h:67). */
+int rip_pool_configure(rip_pool *p, uint32_t colors, uint32_t slots,
+                       uint32_t log_capacity);
+
+/* ---- seed selection ------------------------------------------------------- */
+/* Greedy max coverage over sets [0, num_sets) of the pool.  Writes up to k
+ * seeds (internal ids) and their marginal coverage, *num_seeds and
+ * f = covered / num_sets.  Stops early when every set is covered.  Sets are
+ * not reordered.  Replaces FindMostInfluentialSet (omp_parallel_tag,
+ * include/ripples/find_most_influential.h:176-196 ->
+ * streaming_find_most_influential.h:607-643). */
+int rip_select(rip_pool *p, uint64_t num_sets, uint32_t k, int tiebreak,
+               uint32_t *seeds, uint64_t *gains, uint32_t *num_seeds,
+               double *f);
+
+/* Coverage counts (n values) as the last rip_select left them: after the
+ * update that followed its last-but-one seed.  For checking the update step
+ * (the reference's known-answer test, test/cuda_find_most_influential.cc:84-167). */
+int rip_select_counts(rip_pool *p, uint32_t *counts);
+
+/* Vertex occurrence counts over sets [0, num_sets) (n values), the first
+ * step of selection (CountOccurrencies, include/ripples/counting.h:65-97). */
+int rip_count(rip_pool *p, uint64_t num_sets, uint32_t *counts);
+
+/* ---- IMM driver ----------------------------------------------------------- */
+/* Fields mirror IMMExecutionRecord (include/ripples/imm_execution_record.h:55-92)
+ * and the JSON keys of the imm tool (tools/imm.cc:104-134).  Times in ms. */
+#define RIP_MAX_ROUNDS 64
+typedef struct rip_imm_record {
+  uint64_t theta;
+  uint32_t num_rounds;
+  uint64_t theta_prime_deltas[RIP_MAX_ROUNDS];
+  double round_generate_ms[RIP_MAX_ROUNDS];
+  double round_select_ms[RIP_MAX_ROUNDS];
+  double theta_estimation_ms;
+  double generate_ms;
+  double select_ms;
+  double total_ms;
+  double f;
+  uint64_t total_sets;
+  uint64_t pool_elements;
+  uint64_t rrr_set_bytes;
+} rip_imm_record;
+
+/* Runs IMM (martingale theta estimation, final sampling, final selection over
+ * sets [0, theta)) on the device.  l is the reference's `l` argument (the imm
+ * tool passes 1; the driver applies l *= 1 + 1/log2(n) as imm.h:815 does).
+ * Replaces ripples::IMM (include/ripples/imm.h:768-860). */
+int rip_imm(rip_ctx *ctx, rip_graph *g, uint32_t k, double epsilon, double l,
+            uint64_t seed, int tiebreak, int sampler, uint32_t *seeds,
+            uint32_t *num_seeds, rip_imm_record *record);
+
+/* IMM on an existing pool: reuses the sets it holds (extending it when theta
+ * needs more), as Sampling does when RR is non-empty (include/ripples/imm.h:173-177). */
+int rip_imm_pool(rip_pool *p, uint32_t k, double epsilon, double l,
+                 uint64_t seed, int tiebreak, int sampler, uint32_t *seeds,
+                 uint32_t *num_seeds, rip_imm_record *record);
+
+/* ---- theta math (host) ------------------------------------------------------ */
+/* Exactly include/ripples/imm.h:77-128 and utility.h:84-87, including the
+ * ssize_t / size_t truncations. */
+int64_t rip_theta_prime(int64_t x, double epsilon_prime, double l, uint64_t k,
+                        uint64_t n);
+int64_t rip_inv_theta_prime(int64_t rr_size, double epsilon_prime, double l,
+                            uint64_t k, uint64_t n);
+uint64_t rip_theta(double epsilon, double l, uint64_t k, double lower_bound,
+                   uint64_t n);
+double rip_log_binomial(uint64_t n, uint64_t k);
+
+/* ---- graph construction helpers (host) ------------------------------------- */
+/* R-MAT (Chakrabarti, Zhan, Faloutsos, SDM'04) edge sampling with quadrant
+ * probabilities a, b, c (d = 1-a-b-c), `num_edges` draws on 2^scale vertices,
+ * self-loops and duplicate edges removed; returns the backward CSR in buffers
+ * allocated by the library (free with rip_free).  Deterministic in seed. */
+int rip_rmat_csr(uint32_t scale, uint64_t num_edges, double a, double b,
+                 double c, uint64_t seed, uint64_t **index, uint32_t **src,
+                 uint64_t *m);
+/* Erdos-Renyi G(n, M): M directed edge draws, self-loops and duplicates
+ * removed, backward CSR as above. */
+int rip_er_csr(uint32_t n, uint64_t num_edges, uint64_t seed, uint64_t **index,
+               uint32_t **src, uint64_t *m);
+/* Fills w[m] for a backward CSR under one of RIP_WEIGHTS_*. */
+int rip_make_weights(int kind, uint32_t n, const uint64_t *index, uint64_t m,
+                     uint64_t seed, double lo, double hi, float *w);
+/* Writes the reference binary graph format (include/ripples/graph.h:700-771)
+ * for the backward CSR (backward != 0) or its transpose (backward == 0). */
+int rip_write_binary(const char *path, uint32_t n, uint64_t m,
+                     const uint64_t *index, const uint32_t *src,
+                     const float *w, int backward);
+void rip_free(void *ptr);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RIPPLES_B200_H */

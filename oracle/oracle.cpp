@@ -1,0 +1,487 @@
+// oracle.cpp -- TEST INFRASTRUCTURE ONLY.
+//
+// CPU restatement of the pnnl/ripples IMM hot path, used exclusively as the
+// checker by tests/, __graft_entry__.smoke() and the cpu_baseline leg of
+// bench.py.  Nothing in the product (ripples_b200/) links, loads or calls this
+// file.  It is single-threaded scalar C++ on purpose: simple enough to read
+// against the reference line by line.
+//
+// What it restates (reference paths are relative to the ripples project):
+//   * Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as
+//     easy as 1, 2, 3", SC'11): the counter-based generator that keys every
+//     random draw of the sampler on (seed, set id, edge id / vertex id).
+//   * IC RRR-set sampling: reverse BFS over live in-edges,
+//     include/ripples/add_rrrset.h:128-135 (edge live with probability w),
+//     output sorted ascending as in add_rrrset.h:156.
+//   * LT RRR-set sampling: one threshold per visited vertex, in-edges walked in
+//     CSR order until the cumulative weight reaches the threshold, stop on a
+//     revisit, include/ripples/add_rrrset.h:136-150.
+//   * Roots uniform in [0, n), include/ripples/generate_rrr_sets.h:192-195.
+//   * Greedy max coverage with the lazy max-heap and its tie-break:
+//     include/ripples/streaming_find_most_influential.h:410-418 (CompareHeap),
+//     :546-572 (getNextSeed), :607-643 (find_most_influential_set);
+//     sequential twin include/ripples/find_most_influential.h:85-174.
+//     The heap IS libstdc++'s std::priority_queue, exactly as in the reference,
+//     so equal-count ties resolve identically.
+//   * The lowest-id argmax tie-break of the reference's GPU seed selection,
+//     src/gpu/find_most_influential.cc:65-72 (thrust::max_element).
+//   * IMM theta math and the martingale loop: include/ripples/imm.h:77-128
+//     (ThetaPrime, InvThetaPrime, Theta), :145-260 (Sampling), :768-860 (IMM),
+//     include/ripples/utility.h:84-87 (logBinomial).
+//
+// Sampler specification (shared with the CUDA kernels, restated here
+// independently):
+//   key                 = (seed & 0xffffffff, seed >> 32)
+//   root(s)             = mulhi64(u64(P(s_lo, 0, 0, ROOT<<24 | s_hi)), n)
+//   coin(s, e)          = P(g_lo, g_hi, s_lo, IC<<24 | s_hi)[e & 3], g = e >> 2
+//   lt_threshold(s, v)  = P(v, 0, s_lo, LT<<24 | s_hi)[0]
+//   IC edge e live for set s  <=>  coin(s, e) < thr[e]
+//   thr[e] = clamp(floor(w_e * 2^32), 0, 2^32-1)
+//   LT: first in-edge j of v (CSR order) with threshold < cum[j],
+//       cum[j] = clamp(floor((sum_{i<=j} w_i in double) * 2^32), 0, 2^32-1)
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
+#include <queue>
+#include <utility>
+#include <vector>
+#include <sys/types.h>
+
+namespace {
+
+enum : uint32_t { DOM_ROOT = 1, DOM_IC = 2, DOM_LT = 3 };
+
+void philox4x32_10(const uint32_t ctr_in[4], const uint32_t key_in[2],
+                   uint32_t out[4]) {
+  const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
+  const uint32_t W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+  uint32_t c0 = ctr_in[0], c1 = ctr_in[1], c2 = ctr_in[2], c3 = ctr_in[3];
+  uint32_t k0 = key_in[0], k1 = key_in[1];
+  for (int r = 0; r < 10; ++r) {
+    if (r > 0) {
+      k0 += W0;
+      k1 += W1;
+    }
+    uint64_t p0 = (uint64_t)M0 * c0;
+    uint64_t p1 = (uint64_t)M1 * c2;
+    uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+    uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+    uint32_t n0 = hi1 ^ c1 ^ k0;
+    uint32_t n2 = hi0 ^ c3 ^ k1;
+    c0 = n0;
+    c1 = lo1;
+    c2 = n2;
+    c3 = lo0;
+  }
+  out[0] = c0;
+  out[1] = c1;
+  out[2] = c2;
+  out[3] = c3;
+}
+
+inline void make_key(uint64_t seed, uint32_t key[2]) {
+  key[0] = (uint32_t)seed;
+  key[1] = (uint32_t)(seed >> 32);
+}
+
+uint32_t root_of(uint64_t seed, uint64_t s, uint32_t n) {
+  uint32_t key[2], ctr[4], out[4];
+  make_key(seed, key);
+  ctr[0] = (uint32_t)s;
+  ctr[1] = 0;
+  ctr[2] = 0;
+  ctr[3] = (DOM_ROOT << 24) | (uint32_t)((s >> 32) & 0xFFFFFFu);
+  philox4x32_10(ctr, key, out);
+  uint64_t u = (uint64_t)out[0] | ((uint64_t)out[1] << 32);
+  return (uint32_t)(((unsigned __int128)u * n) >> 64);
+}
+
+uint32_t ic_coin(uint64_t seed, uint64_t s, uint64_t e) {
+  uint32_t key[2], ctr[4], out[4];
+  make_key(seed, key);
+  uint64_t g = e >> 2;
+  ctr[0] = (uint32_t)g;
+  ctr[1] = (uint32_t)(g >> 32);
+  ctr[2] = (uint32_t)s;
+  ctr[3] = (DOM_IC << 24) | (uint32_t)((s >> 32) & 0xFFFFFFu);
+  philox4x32_10(ctr, key, out);
+  return out[e & 3];
+}
+
+uint32_t lt_threshold(uint64_t seed, uint64_t s, uint32_t v) {
+  uint32_t key[2], ctr[4], out[4];
+  make_key(seed, key);
+  ctr[0] = v;
+  ctr[1] = 0;
+  ctr[2] = (uint32_t)s;
+  ctr[3] = (DOM_LT << 24) | (uint32_t)((s >> 32) & 0xFFFFFFu);
+  philox4x32_10(ctr, key, out);
+  return out[0];
+}
+
+uint32_t prob_to_u32(double x) {
+  double y = x * 4294967296.0;
+  if (!(y > 0.0)) return 0u;
+  if (y >= 4294967295.0) return 0xFFFFFFFFu;
+  return (uint32_t)std::floor(y);
+}
+
+// ---- theta math: include/ripples/imm.h:77-128, utility.h:84-87 -------------
+double logBinomial(size_t n, size_t k) {
+  return lgamma(n + 1) - lgamma(n - k + 1) - lgamma(k + 1);
+}
+
+ssize_t ThetaPrime(ssize_t x, double epsilonPrime, double l, size_t k,
+                   size_t num_nodes) {
+  k = std::min(k, num_nodes / 2);
+  return (2 + 2. / 3. * epsilonPrime) *
+         (l * std::log(num_nodes) + logBinomial(num_nodes, k) +
+          std::log(std::log2(num_nodes))) *
+         std::pow(2.0, x) / (epsilonPrime * epsilonPrime);
+}
+
+ssize_t InvThetaPrime(ssize_t rrsize, double epsilonPrime, double l, size_t k,
+                      size_t num_nodes) {
+  k = std::min(k, num_nodes / 2);
+  return std::log2(rrsize * epsilonPrime * epsilonPrime /
+                   ((2 + 2. / 3. * epsilonPrime) *
+                    (l * std::log(num_nodes) + logBinomial(num_nodes, k) +
+                     std::log(std::log2(num_nodes)))));
+}
+
+size_t Theta(double epsilon, double l, size_t k, double LB, size_t num_nodes) {
+  if (LB == 0) return 0;
+  k = std::min(k, num_nodes / 2);
+  double term1 = 0.6321205588285577;  // 1 - 1/e
+  double alpha = sqrt(l * std::log(num_nodes) + std::log(2));
+  double beta = sqrt(term1 * (logBinomial(num_nodes, k) +
+                              l * std::log(num_nodes) + std::log(2)));
+  double lamdaStar = 2 * num_nodes * (term1 * alpha + beta) *
+                     (term1 * alpha + beta) * pow(epsilon, -2);
+  return lamdaStar / LB;
+}
+
+// ---- sampling ------------------------------------------------------------
+struct Graph {
+  uint32_t n;
+  const uint64_t *index;
+  const uint32_t *src;
+  const uint32_t *thr;  // IC thresholds or LT cumulative thresholds
+};
+
+struct SampleStats {
+  uint64_t edges_scanned = 0;   // in-edges read (IC: all of each member)
+  uint64_t expansions = 0;      // vertices expanded
+};
+
+// One IC set: reverse BFS from root(s) over live edges.
+void sample_ic_one(const Graph &G, uint64_t seed, uint64_t s,
+                   std::vector<uint32_t> &stamp, uint32_t tag,
+                   std::vector<uint32_t> &out, SampleStats &st) {
+  out.clear();
+  uint32_t r = root_of(seed, s, G.n);
+  out.push_back(r);
+  stamp[r] = tag;
+  for (size_t head = 0; head < out.size(); ++head) {
+    uint32_t v = out[head];
+    st.expansions++;
+    for (uint64_t e = G.index[v]; e < G.index[v + 1]; ++e) {
+      st.edges_scanned++;
+      uint32_t u = G.src[e];
+      if (stamp[u] == tag) continue;  // coins are pure: skipping is exact
+      if (ic_coin(seed, s, e) < G.thr[e]) {
+        stamp[u] = tag;
+        out.push_back(u);
+      }
+    }
+  }
+  std::sort(out.begin(), out.end());
+}
+
+// One LT set: single-predecessor walk from root(s).
+void sample_lt_one(const Graph &G, uint64_t seed, uint64_t s,
+                   std::vector<uint32_t> &stamp, uint32_t tag,
+                   std::vector<uint32_t> &out, SampleStats &st) {
+  out.clear();
+  uint32_t cur = root_of(seed, s, G.n);
+  out.push_back(cur);
+  stamp[cur] = tag;
+  for (;;) {
+    st.expansions++;
+    uint32_t t = lt_threshold(seed, s, cur);
+    uint64_t sel = UINT64_MAX;
+    for (uint64_t e = G.index[cur]; e < G.index[cur + 1]; ++e) {
+      st.edges_scanned++;
+      if (t < G.thr[e]) {
+        sel = e;
+        break;
+      }
+    }
+    if (sel == UINT64_MAX) break;
+    uint32_t u = G.src[sel];
+    if (stamp[u] == tag) break;
+    stamp[u] = tag;
+    out.push_back(u);
+    cur = u;
+  }
+  std::sort(out.begin(), out.end());
+}
+
+// ---- selection: include/ripples/streaming_find_most_influential.h ----------
+struct CompareHeap {
+  bool operator()(const std::pair<uint32_t, size_t> &a,
+                  const std::pair<uint32_t, size_t> &b) const {
+    return a.second < b.second;
+  }
+};
+
+struct SelectResult {
+  std::vector<uint32_t> seeds;
+  std::vector<uint64_t> gains;
+  uint64_t uncovered = 0;
+  double f = 0.0;
+};
+
+// tiebreak 0: the reference CPU lazy heap; 1: lowest vertex id wins.
+SelectResult select_sets(uint32_t n, uint64_t nsets, const uint64_t *off,
+                         const uint32_t *vtx, uint32_t k, int tiebreak) {
+  SelectResult R;
+  std::vector<uint32_t> count(n, 0);
+  uint64_t P = off[nsets] - off[0];
+  const uint32_t *base = vtx;
+  for (uint64_t i = 0; i < P; ++i) count[base[i]]++;
+  // inverted index: vertex -> sets containing it
+  std::vector<uint64_t> inv_off(n + 1, 0);
+  for (uint32_t v = 0; v < n; ++v) inv_off[v + 1] = inv_off[v] + count[v];
+  std::vector<uint64_t> inv(P);
+  {
+    std::vector<uint64_t> cur(inv_off.begin(), inv_off.end() - 1);
+    for (uint64_t s = 0; s < nsets; ++s)
+      for (uint64_t i = off[s]; i < off[s + 1]; ++i)
+        inv[cur[vtx[i - off[0]]]++] = s;
+  }
+  std::vector<uint8_t> covered(nsets, 0);
+  auto cover = [&](uint32_t v) {
+    for (uint64_t j = inv_off[v]; j < inv_off[v + 1]; ++j) {
+      uint64_t s = inv[j];
+      if (covered[s]) continue;
+      covered[s] = 1;
+      for (uint64_t i = off[s]; i < off[s + 1]; ++i) count[vtx[i - off[0]]] -= 1;
+    }
+  };
+
+  uint64_t uncovered = nsets;
+  if (tiebreak == 0) {
+    std::vector<std::pair<uint32_t, size_t>> storage(n);
+    for (uint32_t v = 0; v < n; ++v) storage[v] = {v, count[v]};
+    std::priority_queue<std::pair<uint32_t, size_t>,
+                        std::vector<std::pair<uint32_t, size_t>>, CompareHeap>
+        queue(CompareHeap{}, std::move(storage));
+    while (R.seeds.size() < k && uncovered != 0) {
+      std::pair<uint32_t, size_t> element;
+      for (;;) {
+        element = queue.top();
+        queue.pop();
+        if (element.second > count[element.first]) {
+          element.second = count[element.first];
+          queue.push(element);
+          continue;
+        }
+        break;
+      }
+      uncovered -= element.second;
+      R.seeds.push_back(element.first);
+      R.gains.push_back(element.second);
+      if (R.seeds.size() == k) break;
+      cover(element.first);
+    }
+  } else {
+    while (R.seeds.size() < k && uncovered != 0) {
+      uint32_t best = 0;
+      for (uint32_t v = 1; v < n; ++v)
+        if (count[v] > count[best]) best = v;
+      uncovered -= count[best];
+      R.seeds.push_back(best);
+      R.gains.push_back(count[best]);
+      if (R.seeds.size() == k) break;
+      cover(best);
+    }
+  }
+  R.uncovered = uncovered;
+  R.f = nsets ? double(nsets - uncovered) / nsets : 0.0;
+  return R;
+}
+
+struct Pool {
+  std::vector<uint64_t> off{0};
+  std::vector<uint32_t> vtx;
+};
+
+void sample_range(const Graph &G, int model, uint64_t seed, uint64_t first,
+                  uint64_t count, Pool &pool, SampleStats &st) {
+  std::vector<uint32_t> stamp(G.n, 0);
+  std::vector<uint32_t> one;
+  uint32_t tag = 0;
+  for (uint64_t s = first; s < first + count; ++s) {
+    if (++tag == 0) {
+      std::fill(stamp.begin(), stamp.end(), 0);
+      tag = 1;
+    }
+    if (model == 0)
+      sample_ic_one(G, seed, s, stamp, tag, one, st);
+    else
+      sample_lt_one(G, seed, s, stamp, tag, one, st);
+    pool.vtx.insert(pool.vtx.end(), one.begin(), one.end());
+    pool.off.push_back(pool.vtx.size());
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+void orc_philox4x32_10(const uint32_t *ctr, const uint32_t *key,
+                       uint32_t *out) {
+  philox4x32_10(ctr, key, out);
+}
+
+uint32_t orc_root(uint64_t seed, uint64_t s, uint32_t n) {
+  return root_of(seed, s, n);
+}
+
+uint32_t orc_ic_coin(uint64_t seed, uint64_t s, uint64_t e) {
+  return ic_coin(seed, s, e);
+}
+
+uint32_t orc_lt_threshold(uint64_t seed, uint64_t s, uint32_t v) {
+  return lt_threshold(seed, s, v);
+}
+
+void orc_pack_ic(const float *w, uint64_t m, uint32_t *thr) {
+  for (uint64_t e = 0; e < m; ++e) thr[e] = prob_to_u32((double)w[e]);
+}
+
+void orc_pack_lt(const uint64_t *index, uint32_t n, const float *w,
+                 uint32_t *cum) {
+  for (uint32_t v = 0; v < n; ++v) {
+    double acc = 0.0;
+    for (uint64_t e = index[v]; e < index[v + 1]; ++e) {
+      acc += (double)w[e];
+      cum[e] = prob_to_u32(acc);
+    }
+  }
+}
+
+// Samples sets [first, first+count).  Returns an opaque pool handle; the
+// caller reads it with orc_pool_* and releases it with orc_pool_free.
+void *orc_sample(int model, uint32_t n, const uint64_t *index,
+                 const uint32_t *src, const uint32_t *thr, uint64_t seed,
+                 uint64_t first, uint64_t count, uint64_t *stats /*2*/) {
+  Graph G{n, index, src, thr};
+  Pool *p = new Pool();
+  SampleStats st;
+  sample_range(G, model, seed, first, count, *p, st);
+  if (stats) {
+    stats[0] = st.expansions;
+    stats[1] = st.edges_scanned;
+  }
+  return p;
+}
+
+uint64_t orc_pool_elements(void *h) { return ((Pool *)h)->vtx.size(); }
+uint64_t orc_pool_sets(void *h) { return ((Pool *)h)->off.size() - 1; }
+void orc_pool_copy(void *h, uint64_t *off, uint32_t *vtx) {
+  Pool *p = (Pool *)h;
+  std::memcpy(off, p->off.data(), p->off.size() * sizeof(uint64_t));
+  if (!p->vtx.empty())
+    std::memcpy(vtx, p->vtx.data(), p->vtx.size() * sizeof(uint32_t));
+}
+void orc_pool_free(void *h) { delete (Pool *)h; }
+
+// Greedy max coverage over nsets sets given as CSR (off[0..nsets], vtx).
+// Writes up to k seeds and their marginal gains; returns the number of seeds.
+uint32_t orc_select(uint32_t n, uint64_t nsets, const uint64_t *off,
+                    const uint32_t *vtx, uint32_t k, int tiebreak,
+                    uint32_t *seeds, uint64_t *gains, double *f,
+                    uint64_t *uncovered) {
+  SelectResult R = select_sets(n, nsets, off, vtx, k, tiebreak);
+  for (size_t i = 0; i < R.seeds.size(); ++i) {
+    seeds[i] = R.seeds[i];
+    gains[i] = R.gains[i];
+  }
+  *f = R.f;
+  *uncovered = R.uncovered;
+  return (uint32_t)R.seeds.size();
+}
+
+int64_t orc_theta_prime(int64_t x, double eps_prime, double l, uint64_t k,
+                        uint64_t n) {
+  return ThetaPrime(x, eps_prime, l, k, n);
+}
+int64_t orc_inv_theta_prime(int64_t rrsize, double eps_prime, double l,
+                            uint64_t k, uint64_t n) {
+  return InvThetaPrime(rrsize, eps_prime, l, k, n);
+}
+uint64_t orc_theta(double eps, double l, uint64_t k, double LB, uint64_t n) {
+  return Theta(eps, l, k, LB, n);
+}
+double orc_log_binomial(uint64_t n, uint64_t k) { return logBinomial(n, k); }
+
+// Full IMM (omp_parallel_tag flavour of include/ripples/imm.h:768-860) over
+// the restated sampler.  Set ids are assigned 0, 1, 2, ... in generation
+// order and the final selection runs over sets [0, theta).
+// Outputs: seeds (k slots), *nseeds, *theta, deltas (up to 64 slots, one per
+// martingale round), *nrounds, *f_final, *total_sets.
+int orc_imm(int model, uint32_t n, const uint64_t *index, const uint32_t *src,
+            const uint32_t *thr, uint32_t k, double epsilon, uint64_t seed,
+            int tiebreak, uint32_t *seeds, uint32_t *nseeds, uint64_t *theta,
+            uint64_t *deltas, uint32_t *nrounds, double *f_final,
+            uint64_t *total_sets) {
+  Graph G{n, index, src, thr};
+  Pool pool;
+  SampleStats st;
+  double l = 1.0;
+  l = l * (1 + 1 / std::log2(n));
+  double epsilonPrime = 1.4142135623730951 * epsilon;
+  double LB = 0;
+  ssize_t x = 1;
+  uint32_t rounds = 0;
+  for (; x < std::log2(n); ++x) {
+    ssize_t thetaPrime = ThetaPrime(x, epsilonPrime, l, k, n);
+    size_t have = pool.off.size() - 1;
+    double f = 0;
+    if ((size_t)thetaPrime <= have) {
+      if (rounds < 64) deltas[rounds] = 0;
+    } else {
+      size_t delta = thetaPrime - have;
+      if (rounds < 64) deltas[rounds] = delta;
+      sample_range(G, model, seed, have, delta, pool, st);
+    }
+    ++rounds;
+    size_t now = pool.off.size() - 1;
+    SelectResult S =
+        select_sets(n, now, pool.off.data(), pool.vtx.data(), k, tiebreak);
+    f = S.f;
+    if (f >= std::pow(2, -x)) {
+      LB = (n * f) / (1 + epsilonPrime);
+      break;
+    }
+  }
+  size_t th = Theta(epsilon, l, k, LB, n);
+  size_t have = pool.off.size() - 1;
+  if (th > have) sample_range(G, model, seed, have, th - have, pool, st);
+  SelectResult S = select_sets(n, th, pool.off.data(), pool.vtx.data(), k,
+                               tiebreak);
+  for (size_t i = 0; i < S.seeds.size(); ++i) seeds[i] = S.seeds[i];
+  *nseeds = (uint32_t)S.seeds.size();
+  *theta = th;
+  *nrounds = rounds;
+  *f_final = S.f;
+  *total_sets = pool.off.size() - 1;
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,218 @@
+"""Python access to the CPU oracle -- TEST INFRASTRUCTURE ONLY.
+
+Loads ``oracle/liboracle.so`` (built from oracle/oracle.cpp by
+oracle/Makefile) and, when present, ``oracle/_ref/libref_harness.so`` (the
+reference's own selection / theta math / samplers compiled from its sources by
+oracle/ref.mk).  Only tests/, ``__graft_entry__.smoke()`` and the cpu_baseline
+leg of bench.py use this module; the product never does.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from typing import Optional, Tuple
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libref_harness.so")
+
+P = ctypes.c_void_p
+U32, U64, I32, I64, DBL = ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int, ctypes.c_int64, ctypes.c_double
+
+
+def _ptr(a):
+    return None if a is None else ctypes.c_void_p(a.ctypes.data)
+
+
+def build() -> None:
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def _load_oracle() -> ctypes.CDLL:
+    if not os.path.exists(ORACLE_SO):
+        build()
+    L = ctypes.CDLL(ORACLE_SO)
+    sig = {
+        "orc_philox4x32_10": (None, [P, P, P]),
+        "orc_root": (U32, [U64, U64, U32]),
+        "orc_ic_coin": (U32, [U64, U64, U64]),
+        "orc_lt_threshold": (U32, [U64, U64, U32]),
+        "orc_pack_ic": (None, [P, U64, P]),
+        "orc_pack_lt": (None, [P, U32, P, P]),
+        "orc_sample": (P, [I32, U32, P, P, P, U64, U64, U64, P]),
+        "orc_pool_elements": (U64, [P]),
+        "orc_pool_sets": (U64, [P]),
+        "orc_pool_copy": (None, [P, P, P]),
+        "orc_pool_free": (None, [P]),
+        "orc_select": (U32, [U32, U64, P, P, U32, I32, P, P, ctypes.POINTER(DBL),
+                             ctypes.POINTER(U64)]),
+        "orc_theta_prime": (I64, [I64, DBL, DBL, U64, U64]),
+        "orc_inv_theta_prime": (I64, [I64, DBL, DBL, U64, U64]),
+        "orc_theta": (U64, [DBL, DBL, U64, DBL, U64]),
+        "orc_log_binomial": (DBL, [U64, U64]),
+        "orc_imm": (I32, [I32, U32, P, P, P, U32, DBL, U64, I32, P, ctypes.POINTER(U32),
+                          ctypes.POINTER(U64), P, ctypes.POINTER(U32), ctypes.POINTER(DBL),
+                          ctypes.POINTER(U64)]),
+    }
+    for k, (r, a) in sig.items():
+        f = getattr(L, k)
+        f.restype, f.argtypes = r, a
+    return L
+
+
+L = _load_oracle()
+
+
+def philox(ctr, key):
+    c = (ctypes.c_uint32 * 4)(*ctr)
+    k = (ctypes.c_uint32 * 2)(*key)
+    o = (ctypes.c_uint32 * 4)()
+    L.orc_philox4x32_10(c, k, o)
+    return list(o)
+
+
+def root(seed: int, s: int, n: int) -> int:
+    return int(L.orc_root(seed, s, n))
+
+
+def pack(model: str, index: np.ndarray, weights: np.ndarray) -> np.ndarray:
+    m = len(weights)
+    thr = np.zeros(max(m, 1), dtype=np.uint32)
+    w = np.ascontiguousarray(weights, dtype=np.float32)
+    if model == "IC":
+        L.orc_pack_ic(_ptr(w), m, _ptr(thr))
+    else:
+        idx = np.ascontiguousarray(index, dtype=np.uint64)
+        L.orc_pack_lt(_ptr(idx), len(idx) - 1, _ptr(w), _ptr(thr))
+    return thr[:m]
+
+
+def sample(model: str, n: int, index: np.ndarray, src: np.ndarray, thr: np.ndarray,
+           seed: int, first: int, count: int) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """Sets [first, first+count) as CSR (offsets, vertices), each sorted, plus
+    stats [expansions, in-edges read]."""
+    idx = np.ascontiguousarray(index, dtype=np.uint64)
+    s = np.ascontiguousarray(src, dtype=np.uint32)
+    t = np.ascontiguousarray(thr, dtype=np.uint32)
+    if s.size == 0:
+        s = np.zeros(1, np.uint32)
+        t = np.zeros(1, np.uint32)
+    st = np.zeros(2, dtype=np.uint64)
+    h = L.orc_sample(0 if model == "IC" else 1, n, _ptr(idx), _ptr(s), _ptr(t), seed, first,
+                     count, _ptr(st))
+    ns, ne = L.orc_pool_sets(h), L.orc_pool_elements(h)
+    off = np.zeros(ns + 1, dtype=np.uint64)
+    vtx = np.zeros(max(ne, 1), dtype=np.uint32)
+    L.orc_pool_copy(h, _ptr(off), _ptr(vtx))
+    L.orc_pool_free(h)
+    return off, vtx[:ne], st
+
+
+def select(n: int, offsets: np.ndarray, vertices: np.ndarray, k: int, tiebreak: int = 0):
+    """Greedy max coverage; returns (f, seeds, gains, uncovered).
+    tiebreak 0 = reference CPU lazy heap, 1 = lowest id."""
+    off = np.ascontiguousarray(offsets, dtype=np.uint64)
+    vtx = np.ascontiguousarray(vertices, dtype=np.uint32)
+    if vtx.size == 0:
+        vtx = np.zeros(1, np.uint32)
+    seeds = np.zeros(max(k, 1), dtype=np.uint32)
+    gains = np.zeros(max(k, 1), dtype=np.uint64)
+    f, unc = ctypes.c_double(), ctypes.c_uint64()
+    ns = L.orc_select(n, len(off) - 1, _ptr(off), _ptr(vtx), k, tiebreak, _ptr(seeds),
+                      _ptr(gains), ctypes.byref(f), ctypes.byref(unc))
+    return f.value, seeds[:ns].copy(), gains[:ns].copy(), unc.value
+
+
+def imm(model: str, n: int, index, src, thr, k: int, epsilon: float, seed: int = 0,
+        tiebreak: int = 0) -> dict:
+    idx = np.ascontiguousarray(index, dtype=np.uint64)
+    s = np.ascontiguousarray(src, dtype=np.uint32)
+    t = np.ascontiguousarray(thr, dtype=np.uint32)
+    seeds = np.zeros(max(k, 1), dtype=np.uint32)
+    deltas = np.zeros(64, dtype=np.uint64)
+    ns, th, nr, ff, tot = ctypes.c_uint32(), ctypes.c_uint64(), ctypes.c_uint32(), \
+        ctypes.c_double(), ctypes.c_uint64()
+    L.orc_imm(0 if model == "IC" else 1, n, _ptr(idx), _ptr(s), _ptr(t), k, epsilon, seed,
+              tiebreak, _ptr(seeds), ctypes.byref(ns), ctypes.byref(th), _ptr(deltas),
+              ctypes.byref(nr), ctypes.byref(ff), ctypes.byref(tot))
+    return {"seeds": seeds[:ns.value].tolist(), "theta": th.value,
+            "deltas": deltas[:min(nr.value, 64)].tolist(), "f": ff.value,
+            "total_sets": tot.value}
+
+
+def theta_prime(x, eps_prime, l, k, n):
+    return int(L.orc_theta_prime(x, eps_prime, l, k, n))
+
+
+def inv_theta_prime(r, eps_prime, l, k, n):
+    return int(L.orc_inv_theta_prime(r, eps_prime, l, k, n))
+
+
+def theta(eps, l, k, lb, n):
+    return int(L.orc_theta(eps, l, k, lb, n))
+
+
+def log_binomial(n, k):
+    return float(L.orc_log_binomial(n, k))
+
+
+# ---- the reference itself (compiled from its sources), when available -------
+_REF: Optional[ctypes.CDLL] = None
+
+
+def reference() -> Optional[ctypes.CDLL]:
+    """The reference harness, or None when oracle/_ref was not built."""
+    global _REF
+    if _REF is None and os.path.exists(REF_SO):
+        R = ctypes.CDLL(REF_SO)
+        sig = {
+            "ref_select": (U32, [U32, U64, P, P, U32, I32, I32, P, ctypes.POINTER(DBL)]),
+            "ref_theta_prime": (I64, [I64, DBL, DBL, U64, U64]),
+            "ref_inv_theta_prime": (I64, [I64, DBL, DBL, U64, U64]),
+            "ref_theta": (U64, [DBL, DBL, U64, DBL, U64]),
+            "ref_log_binomial": (DBL, [U64, U64]),
+            "ref_graph_load": (P, [ctypes.c_char_p]),
+            "ref_graph_free": (None, [P]),
+            "ref_graph_nodes": (U64, [P]),
+            "ref_graph_edges": (U64, [P]),
+            "ref_sample": (P, [P, I32, U64, U64, ctypes.POINTER(U64)]),
+            "ref_pool_copy": (None, [P, P, P]),
+            "ref_pool_free": (None, [P]),
+            "ref_simulate": (DBL, [ctypes.c_char_p, I32, P, U32, U64, U64]),
+        }
+        for k, (r, a) in sig.items():
+            f = getattr(R, k)
+            f.restype, f.argtypes = r, a
+        _REF = R
+    return _REF
+
+
+def ref_select(n: int, offsets, vertices, k: int, omp: bool = True, threads: int = 4):
+    R = reference()
+    off = np.ascontiguousarray(offsets, dtype=np.uint64)
+    vtx = np.ascontiguousarray(vertices, dtype=np.uint32)
+    if vtx.size == 0:
+        vtx = np.zeros(1, np.uint32)
+    seeds = np.zeros(max(k, 1) + 1, dtype=np.uint32)
+    f = ctypes.c_double()
+    ns = R.ref_select(n, len(off) - 1, _ptr(off), _ptr(vtx), k, 1 if omp else 0, threads,
+                      _ptr(seeds), ctypes.byref(f))
+    return f.value, seeds[:ns].copy()
+
+
+def ref_sample(bin_path: str, model: str, count: int, seed: int = 0):
+    R = reference()
+    g = R.ref_graph_load(bin_path.encode())
+    try:
+        ne = ctypes.c_uint64()
+        h = R.ref_sample(g, 0 if model == "IC" else 1, count, seed, ctypes.byref(ne))
+        off = np.zeros(count + 1, dtype=np.uint64)
+        vtx = np.zeros(max(ne.value, 1), dtype=np.uint32)
+        R.ref_pool_copy(h, _ptr(off), _ptr(vtx))
+        R.ref_pool_free(h)
+        return off, vtx[: ne.value]
+    finally:
+        R.ref_graph_free(g)

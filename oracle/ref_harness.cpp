@@ -1,0 +1,182 @@
+// ref_harness.cpp -- TEST INFRASTRUCTURE ONLY.
+//
+// Compiled against the unmodified ripples headers (include/ripples/*.h) by
+// oracle/ref.mk into oracle/_ref/libref_harness.so.  It exposes the
+// reference's own seed selection, theta math and sequential samplers through a
+// C ABI so tests can pin the oracle (oracle/oracle.cpp) against the reference
+// itself:
+//   ref_select      -> ripples::FindMostInfluentialSet, omp_parallel_tag
+//                      (include/ripples/find_most_influential.h:176-196) or
+//                      sequential_tag (:85-174)
+//   ref_theta_*     -> include/ripples/imm.h:77-128
+//   ref_sample      -> ripples::AddRRRSet (include/ripples/add_rrrset.h:105-157)
+//                      driven like GenerateRRRSets, sequential_tag
+//                      (include/ripples/generate_rrr_sets.h:186-198), with the
+//                      project's trng interface shim as the random stream.
+//   ref_simulate    -> ripples::simulate (include/ripples/diffusion_simulation.h)
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "ripples/find_most_influential.h"
+#include "ripples/generate_rrr_sets.h"
+#include "ripples/graph.h"
+#include "ripples/imm.h"
+#include "ripples/imm_interface.h"
+#include "ripples/diffusion_simulation.h"
+#include "spdlog/sinks/stdout_color_sinks.h"
+
+namespace {
+
+struct MiniGraph {
+  using vertex_type = uint32_t;
+  size_t n;
+  size_t num_nodes() const { return n; }
+};
+
+struct MiniCFG {
+  size_t k;
+  size_t seed_select_max_workers;
+  size_t seed_select_max_gpu_workers;
+};
+
+using RRRsets = std::vector<std::vector<uint32_t>>;
+
+RRRsets make_sets(uint64_t nsets, const uint64_t *off, const uint32_t *vtx) {
+  RRRsets RR(nsets);
+  for (uint64_t s = 0; s < nsets; ++s)
+    RR[s].assign(vtx + off[s], vtx + off[s + 1]);
+  return RR;
+}
+
+void ensure_console() {
+  if (!spdlog::get("console")) spdlog::stdout_color_st("console");
+  spdlog::set_level(spdlog::level::warn);
+}
+
+}  // namespace
+
+extern "C" {
+
+// Returns the number of seeds written.  omp != 0 selects omp_parallel_tag.
+uint32_t ref_select(uint32_t n, uint64_t nsets, const uint64_t *off,
+                    const uint32_t *vtx, uint32_t k, int omp, int threads,
+                    uint32_t *seeds, double *f) {
+  ensure_console();
+  MiniGraph G{n};
+  MiniCFG CFG{k, (size_t)(threads > 0 ? threads : 1), 0};
+  RRRsets RR = make_sets(nsets, off, vtx);
+  ripples::FindMostInfluentialSetRecord record;
+  std::pair<double, std::vector<uint32_t>> S;
+  if (omp) {
+    if (threads > 0) omp_set_num_threads(threads);
+    S = ripples::FindMostInfluentialSet(G, CFG, RR.begin(), RR.end(), record,
+                                        false, ripples::omp_parallel_tag{});
+  } else {
+    S = ripples::FindMostInfluentialSet(G, CFG, RR.begin(), RR.end(), record,
+                                        false, ripples::sequential_tag{});
+  }
+  for (size_t i = 0; i < S.second.size(); ++i) seeds[i] = S.second[i];
+  *f = S.first;
+  return (uint32_t)S.second.size();
+}
+
+int64_t ref_theta_prime(int64_t x, double eps_prime, double l, uint64_t k,
+                        uint64_t n) {
+  return ripples::ThetaPrime(x, eps_prime, l, k, n, ripples::sequential_tag{});
+}
+
+int64_t ref_inv_theta_prime(int64_t rrsize, double eps_prime, double l,
+                            uint64_t k, uint64_t n) {
+  return ripples::InvThetaPrime(rrsize, eps_prime, l, k, n,
+                                ripples::sequential_tag{});
+}
+
+uint64_t ref_theta(double eps, double l, uint64_t k, double LB, uint64_t n) {
+  return ripples::Theta(eps, l, k, LB, n);
+}
+
+double ref_log_binomial(uint64_t n, uint64_t k) {
+  return ripples::logBinomial(n, k);
+}
+
+// Loads a reference-format binary graph (backward direction) from `path`.
+static ripples::GraphBwd *load(const char *path) {
+  auto *G = new ripples::GraphBwd();
+  G->load_binary(path);
+  return G;
+}
+
+void *ref_graph_load(const char *path) {
+  ensure_console();
+  return load(path);
+}
+void ref_graph_free(void *g) { delete (ripples::GraphBwd *)g; }
+uint64_t ref_graph_nodes(void *g) { return ((ripples::GraphBwd *)g)->num_nodes(); }
+uint64_t ref_graph_edges(void *g) { return ((ripples::GraphBwd *)g)->num_edges(); }
+
+// Samples `count` sets with the reference sequential sampler; model 0 = IC,
+// 1 = LT.  Writes the total element count to *nelem and returns a handle to
+// read with ref_pool_copy / release with ref_pool_free.
+void *ref_sample(void *g, int model, uint64_t count, uint64_t seed,
+                 uint64_t *nelem) {
+  auto &G = *(ripples::GraphBwd *)g;
+  std::vector<trng::lcg64> gen(1);
+  gen[0].seed(seed);
+  gen[0].split(2, 1);
+  auto *RR = new ripples::RRRsets<ripples::GraphBwd>(count);
+  ripples::IMMExecutionRecord rec;
+  if (model == 0)
+    ripples::GenerateRRRSets(G, gen, RR->begin(), RR->end(), rec,
+                             ripples::independent_cascade_tag{},
+                             ripples::sequential_tag{});
+  else
+    ripples::GenerateRRRSets(G, gen, RR->begin(), RR->end(), rec,
+                             ripples::linear_threshold_tag{},
+                             ripples::sequential_tag{});
+  uint64_t tot = 0;
+  for (auto &s : *RR) tot += s.size();
+  *nelem = tot;
+  return RR;
+}
+
+void ref_pool_copy(void *h, uint64_t *off, uint32_t *vtx) {
+  auto &RR = *(ripples::RRRsets<ripples::GraphBwd> *)h;
+  off[0] = 0;
+  for (size_t s = 0; s < RR.size(); ++s) {
+    std::memcpy(vtx + off[s], RR[s].data(), RR[s].size() * sizeof(uint32_t));
+    off[s + 1] = off[s] + RR[s].size();
+  }
+}
+void ref_pool_free(void *h) {
+  delete (ripples::RRRsets<ripples::GraphBwd> *)h;
+}
+
+// Monte Carlo spread of `seeds` (internal ids) on a FORWARD-direction graph
+// loaded from `fwd_path`, with the reference simulator: returns the mean
+// number of activated vertices over `replicas` runs.
+double ref_simulate(const char *fwd_path, int model, const uint32_t *seeds,
+                    uint32_t nseeds, uint64_t replicas, uint64_t seed) {
+  ensure_console();
+  ripples::GraphFwd G;
+  G.load_binary(fwd_path);
+  std::vector<uint32_t> S(seeds, seeds + nseeds);
+  trng::lcg64 gen;
+  gen.seed(seed);
+  gen.split(2, 1);
+  double acc = 0.0;
+  for (uint64_t r = 0; r < replicas; ++r) {
+    std::pair<size_t, size_t> res;
+    if (model == 0)
+      res = ripples::simulate(G, S.begin(), S.end(), gen,
+                              ripples::independent_cascade_tag{});
+    else
+      res = ripples::simulate(G, S.begin(), S.end(), gen,
+                              ripples::linear_threshold_tag{});
+    acc += (double)res.first;
+  }
+  return acc / (double)replicas;
+}
+
+}  // extern "C"

@@ -1,0 +1,1194 @@
+// api.cu -- host runtime behind include/ripples_b200.h.
+//
+// Owns device memory (with a per-context byte budget), the CUDA stream, the
+// growable RRR pool, the sampler launch/retry loop, seed selection (device
+// counts + the reference's lazy max-heap on the host) and the IMM driver
+// (include/ripples/imm.h:145-260, 768-860).
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <queue>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include <sys/types.h>
+
+#include "launch.h"
+#include "ripples_b200.h"
+
+using namespace rip;
+
+namespace {
+
+using clk = std::chrono::high_resolution_clock;
+double ms_since(clk::time_point t0) {
+  return std::chrono::duration<double, std::milli>(clk::now() - t0).count();
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// context, memory
+// ---------------------------------------------------------------------------
+struct DevMem {
+  void *p = nullptr;
+  size_t bytes = 0;
+};
+
+struct rip_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int num_sms = 148;
+  size_t budget = 0;
+  size_t used = 0;
+  std::string err;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+static int set_err(rip_ctx *c, int code, const char *fmt, ...) {
+  if (c) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    c->err = buf;
+  }
+  return code;
+}
+
+#define CK(c, call)                                                          \
+  do {                                                                       \
+    cudaError_t e_ = (call);                                                 \
+    if (e_ != cudaSuccess)                                                   \
+      return set_err((c), RIP_ERR_CUDA, "%s failed: %s (%s:%d)", #call,      \
+                     cudaGetErrorString(e_), __FILE__, __LINE__);            \
+  } while (0)
+
+#define TRY(expr)              \
+  do {                         \
+    int r_ = (expr);           \
+    if (r_ != RIP_OK) return r_; \
+  } while (0)
+
+static int dalloc(rip_ctx *c, DevMem &m, size_t bytes) {
+  if (m.p && m.bytes >= bytes) return RIP_OK;
+  bytes = std::max<size_t>(bytes, 256);
+  if (c->used - m.bytes + bytes > c->budget)
+    return set_err(c, RIP_ERR_NOMEM,
+                   "device budget exceeded: need %zu more bytes (used %zu of %zu)",
+                   bytes, c->used, c->budget);
+  void *p = nullptr;
+  cudaError_t e = cudaMalloc(&p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(c, RIP_ERR_NOMEM, "cudaMalloc(%zu) failed: %s", bytes,
+                   cudaGetErrorString(e));
+  }
+  if (m.p) {
+    cudaFree(m.p);
+    c->used -= m.bytes;
+  }
+  m.p = p;
+  m.bytes = bytes;
+  c->used += bytes;
+  return RIP_OK;
+}
+
+// Grows m to `bytes`, preserving the first `keep` bytes.
+static int dgrow(rip_ctx *c, DevMem &m, size_t bytes, size_t keep) {
+  if (m.p && m.bytes >= bytes) return RIP_OK;
+  DevMem n;
+  TRY(dalloc(c, n, bytes));
+  if (m.p && keep) {
+    CK(c, cudaMemcpyAsync(n.p, m.p, std::min(keep, m.bytes),
+                          cudaMemcpyDeviceToDevice, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+  }
+  if (m.p) {
+    cudaFree(m.p);
+    c->used -= m.bytes;
+  }
+  m = n;
+  return RIP_OK;
+}
+
+static void dfree(rip_ctx *c, DevMem &m) {
+  if (m.p) {
+    cudaFree(m.p);
+    c->used -= m.bytes;
+  }
+  m = DevMem{};
+}
+
+template <typename T>
+static T *ptr(DevMem &m) {
+  return reinterpret_cast<T *>(m.p);
+}
+
+struct PinnedMem {
+  void *p = nullptr;
+  size_t bytes = 0;
+  int ensure(rip_ctx *c, size_t b) {
+    if (p && bytes >= b) return RIP_OK;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    bytes = 0;
+    if (cudaMallocHost(&p, b) != cudaSuccess) {
+      cudaGetLastError();
+      return set_err(c, RIP_ERR_NOMEM, "cudaMallocHost(%zu) failed", b);
+    }
+    bytes = b;
+    return RIP_OK;
+  }
+  ~PinnedMem() {
+    if (p) cudaFreeHost(p);
+  }
+};
+
+extern "C" {
+
+const char *rip_version(void) { return "ripples_b200 0.1.0 sm_100a"; }
+
+int rip_ctx_create(int device, size_t hbm_budget, rip_ctx **out) {
+  if (!out) return RIP_ERR_INVALID;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return RIP_ERR_CUDA;
+  }
+  if (device < 0 || device >= ndev) return RIP_ERR_INVALID;
+  if (cudaSetDevice(device) != cudaSuccess) return RIP_ERR_CUDA;
+  rip_ctx *c = new rip_ctx();
+  c->device = device;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) {
+    delete c;
+    return RIP_ERR_CUDA;
+  }
+  c->num_sms = prop.multiProcessorCount;
+  if (prop.major < 10) {
+    delete c;
+    return RIP_ERR_CUDA;  // built for sm_100a only
+  }
+  size_t fr = 0, tot = 0;
+  cudaMemGetInfo(&fr, &tot);
+  c->budget = hbm_budget ? hbm_budget : (size_t)(0.9 * (double)fr);
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&c->ev0) != cudaSuccess ||
+      cudaEventCreate(&c->ev1) != cudaSuccess) {
+    delete c;
+    return RIP_ERR_CUDA;
+  }
+  *out = c;
+  return RIP_OK;
+}
+
+int rip_ctx_destroy(rip_ctx *c) {
+  if (!c) return RIP_ERR_INVALID;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return RIP_OK;
+}
+
+const char *rip_last_error(const rip_ctx *c) {
+  return c ? c->err.c_str() : "null context";
+}
+
+int rip_sync(rip_ctx *c) {
+  if (!c) return RIP_ERR_INVALID;
+  CK(c, cudaStreamSynchronize(c->stream));
+  return RIP_OK;
+}
+
+int rip_ctx_memory(rip_ctx *c, size_t *used, size_t *budget) {
+  if (!c) return RIP_ERR_INVALID;
+  if (used) *used = c->used;
+  if (budget) *budget = c->budget;
+  return RIP_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// graph
+// ---------------------------------------------------------------------------
+struct rip_graph {
+  rip_ctx *ctx;
+  uint32_t n;
+  uint64_t m;
+  int model;
+  DevMem off, edges;
+  DevGraph view() {
+    return DevGraph{n, m, ptr<uint32_t>(off), ptr<uint2>(edges)};
+  }
+};
+
+extern "C" int rip_graph_upload(rip_ctx *c, const uint64_t *index,
+                                const uint32_t *src, const float *w, uint32_t n,
+                                uint64_t m, int model, rip_graph **out) {
+  if (!c || !out || !index || n == 0 || (m && (!src || !w)))
+    return set_err(c, RIP_ERR_INVALID, "rip_graph_upload: bad arguments");
+  if (model != RIP_MODEL_IC && model != RIP_MODEL_LT)
+    return set_err(c, RIP_ERR_INVALID, "rip_graph_upload: unknown model %d", model);
+  if (n >= 0xFFFFFFFFu || m >= 0xFFFFFFFCull)
+    return set_err(c, RIP_ERR_LIMIT, "graph too large: n=%u m=%llu", n,
+                   (unsigned long long)m);
+  if (index[0] != 0 || index[n] != m)
+    return set_err(c, RIP_ERR_INVALID, "index[0] must be 0 and index[n] == m");
+  long bad = 0;
+#pragma omp parallel for reduction(+ : bad) schedule(static)
+  for (long long v = 0; v < (long long)n; ++v)
+    bad += index[v + 1] < index[v];
+#pragma omp parallel for reduction(+ : bad) schedule(static)
+  for (long long e = 0; e < (long long)m; ++e) bad += src[e] >= n;
+  if (bad)
+    return set_err(c, RIP_ERR_INVALID,
+                   "CSR not monotone or source id out of range (%ld bad)", bad);
+  *out = nullptr;
+  CK(c, cudaSetDevice(c->device));
+  rip_graph *g = new rip_graph();
+  g->ctx = c;
+  g->n = n;
+  g->m = m;
+  g->model = model;
+  const uint64_t m_pad = ((m + 3) & ~3ull) + 4;
+  DevMem d_index, d_src, d_w;
+  int rc = RIP_OK;
+  do {
+    if ((rc = dalloc(c, g->off, sizeof(uint32_t) * ((size_t)n + 1)))) break;
+    if ((rc = dalloc(c, g->edges, sizeof(uint2) * m_pad))) break;
+    if ((rc = dalloc(c, d_index, sizeof(uint64_t) * ((size_t)n + 1)))) break;
+    if ((rc = dalloc(c, d_src, sizeof(uint32_t) * std::max<uint64_t>(m, 1)))) break;
+    if ((rc = dalloc(c, d_w, sizeof(float) * std::max<uint64_t>(m, 1)))) break;
+    cudaError_t e = cudaMemcpyAsync(d_index.p, index, sizeof(uint64_t) * ((size_t)n + 1),
+                                    cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess && m)
+      e = cudaMemcpyAsync(d_src.p, src, sizeof(uint32_t) * m,
+                          cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess && m)
+      e = cudaMemcpyAsync(d_w.p, w, sizeof(float) * m, cudaMemcpyHostToDevice,
+                          c->stream);
+    if (e != cudaSuccess) {
+      rc = set_err(c, RIP_ERR_CUDA, "graph upload copy failed: %s",
+                   cudaGetErrorString(e));
+      break;
+    }
+    if (model == RIP_MODEL_IC)
+      launch_pack_ic(ptr<uint64_t>(d_index), ptr<float>(d_w), n, m,
+                     ptr<uint32_t>(g->off), ptr<uint2>(g->edges),
+                     ptr<uint32_t>(d_src), c->stream);
+    else
+      launch_pack_lt(ptr<uint64_t>(d_index), ptr<float>(d_w), n, m,
+                     ptr<uint32_t>(g->off), ptr<uint2>(g->edges),
+                     ptr<uint32_t>(d_src), c->stream);
+    e = cudaStreamSynchronize(c->stream);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess)
+      rc = set_err(c, RIP_ERR_CUDA, "graph pack failed: %s", cudaGetErrorString(e));
+  } while (0);
+  dfree(c, d_index);
+  dfree(c, d_src);
+  dfree(c, d_w);
+  if (rc != RIP_OK) {
+    dfree(c, g->off);
+    dfree(c, g->edges);
+    delete g;
+    return rc;
+  }
+  *out = g;
+  return RIP_OK;
+}
+
+extern "C" int rip_graph_destroy(rip_graph *g) {
+  if (!g) return RIP_ERR_INVALID;
+  cudaSetDevice(g->ctx->device);
+  cudaStreamSynchronize(g->ctx->stream);
+  dfree(g->ctx, g->off);
+  dfree(g->ctx, g->edges);
+  delete g;
+  return RIP_OK;
+}
+
+extern "C" int rip_graph_info(const rip_graph *g, uint32_t *n, uint64_t *m,
+                              int *model) {
+  if (!g) return RIP_ERR_INVALID;
+  if (n) *n = g->n;
+  if (m) *m = g->m;
+  if (model) *model = g->model;
+  return RIP_OK;
+}
+
+extern "C" int rip_graph_thresholds(rip_graph *g, uint32_t *thr) {
+  if (!g || (!thr && g->m)) return RIP_ERR_INVALID;
+  rip_ctx *c = g->ctx;
+  std::vector<uint2> rec(g->m);
+  if (g->m) {
+    CK(c, cudaMemcpyAsync(rec.data(), g->edges.p, sizeof(uint2) * g->m,
+                          cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+  }
+  for (uint64_t e = 0; e < g->m; ++e) thr[e] = rec[e].y;
+  return RIP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// pool
+// ---------------------------------------------------------------------------
+struct PoolMeta {  // device-side bookkeeping block (one D2H reads it all)
+  unsigned long long cursor;
+  unsigned long long first_bad;
+  unsigned long long stats[8];
+  unsigned int fail_count;
+  unsigned int next;
+  unsigned int dirty_n;
+  unsigned int fused_dirty;
+  unsigned long long best;
+  unsigned long long covered_sets;
+};
+
+struct rip_pool {
+  rip_ctx *ctx;
+  rip_graph *g;
+  DevMem vtx, set_off, set_len, meta;
+  uint64_t cap = 0, set_cap = 0;
+  uint64_t num_sets = 0, num_elems = 0;
+  // sampler scratch (one buffer partitioned into per-warp bitmap + queue)
+  DevMem scratch, ids_a, ids_b;
+  uint64_t bm_words = 0;
+  uint32_t qcap = 0;
+  uint32_t warps = 0;
+  // fused sampler scratch (per slot: colour masks, pending masks, level
+  // flags, frontier log); all-zero between batches
+  DevMem f_vis, f_pend, f_flag, f_log, f_order;
+  uint32_t f_slots = 0, f_cw = 0, f_lcap = 0;
+  uint32_t colors = 64;      // fused colour width (64/128/256)
+  uint32_t fused_slots = 0;  // 0 = size from the budget
+  uint32_t lcap_pref = 0;    // 0 = default frontier-log capacity
+  // selection state
+  DevMem count, inv_off, inv_cur, inv, covered, dirty_bits, dirty_list, pairs,
+      scan_sums;
+  PinnedMem h_pairs, h_count;
+  std::vector<uint32_t> last_counts;
+  bool have_last_counts = false;
+  // timing of sampler kernels (CUDA events on the context stream)
+  double kernel_ms = 0.0;
+  uint64_t kernel_launches = 0;
+  double select_kernel_ms = 0.0;
+
+  PoolMeta *dmeta() { return ptr<PoolMeta>(meta); }
+  DevPool view() {
+    return DevPool{ptr<uint32_t>(vtx), &dmeta()->cursor, cap,
+                   ptr<uint64_t>(set_off), ptr<uint32_t>(set_len)};
+  }
+};
+
+static int read_meta(rip_pool *p, PoolMeta &m) {
+  rip_ctx *c = p->ctx;
+  CK(c, cudaMemcpyAsync(&m, p->meta.p, sizeof(PoolMeta), cudaMemcpyDeviceToHost,
+                        c->stream));
+  CK(c, cudaStreamSynchronize(c->stream));
+  return RIP_OK;
+}
+
+extern "C" int rip_pool_create(rip_ctx *c, rip_graph *g, rip_pool **out) {
+  if (!c || !g || !out || g->ctx != c) return set_err(c, RIP_ERR_INVALID, "rip_pool_create: bad arguments");
+  CK(c, cudaSetDevice(c->device));
+  rip_pool *p = new rip_pool();
+  p->ctx = c;
+  p->g = g;
+  int rc = dalloc(c, p->meta, sizeof(PoolMeta));
+  if (rc) {
+    delete p;
+    return rc;
+  }
+  cudaMemsetAsync(p->meta.p, 0, sizeof(PoolMeta), c->stream);
+  *out = p;
+  return RIP_OK;
+}
+
+extern "C" int rip_pool_destroy(rip_pool *p) {
+  if (!p) return RIP_ERR_INVALID;
+  rip_ctx *c = p->ctx;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  DevMem *all[] = {&p->vtx,     &p->set_off,   &p->set_len,  &p->meta,
+                   &p->scratch, &p->ids_a,     &p->ids_b,    &p->f_vis,
+                   &p->f_pend,  &p->f_flag,    &p->f_log,    &p->f_order,
+                   &p->count,   &p->inv_off,   &p->inv_cur,  &p->inv,
+                   &p->covered, &p->dirty_bits, &p->dirty_list, &p->pairs,
+                   &p->scan_sums};
+  for (DevMem *m : all) dfree(c, *m);
+  delete p;
+  return RIP_OK;
+}
+
+extern "C" int rip_pool_clear(rip_pool *p) {
+  if (!p) return RIP_ERR_INVALID;
+  rip_ctx *c = p->ctx;
+  CK(c, cudaMemsetAsync(p->meta.p, 0, sizeof(PoolMeta), c->stream));
+  CK(c, cudaStreamSynchronize(c->stream));
+  p->num_sets = p->num_elems = 0;
+  p->kernel_ms = p->select_kernel_ms = 0.0;
+  p->kernel_launches = 0;
+  p->have_last_counts = false;
+  return RIP_OK;
+}
+
+extern "C" int rip_pool_info(const rip_pool *p, uint64_t *num_sets,
+                             uint64_t *num_elements) {
+  if (!p) return RIP_ERR_INVALID;
+  if (num_sets) *num_sets = p->num_sets;
+  if (num_elements) *num_elements = p->num_elems;
+  return RIP_OK;
+}
+
+extern "C" int rip_pool_stats(rip_pool *p, uint64_t stats[8]) {
+  if (!p || !stats) return RIP_ERR_INVALID;
+  PoolMeta m;
+  TRY(read_meta(p, m));
+  for (int i = 0; i < 8; ++i) stats[i] = m.stats[i];
+  return RIP_OK;
+}
+
+// Kernel-time accounting of the sampler launches (CUDA events on the stream).
+extern "C" int rip_pool_timing(rip_pool *p, double *sample_kernel_ms,
+                               uint64_t *launches, double *select_kernel_ms) {
+  if (!p) return RIP_ERR_INVALID;
+  if (sample_kernel_ms) *sample_kernel_ms = p->kernel_ms;
+  if (launches) *launches = p->kernel_launches;
+  if (select_kernel_ms) *select_kernel_ms = p->select_kernel_ms;
+  return RIP_OK;
+}
+
+static int ensure_sets(rip_pool *p, uint64_t need) {
+  rip_ctx *c = p->ctx;
+  if (need <= p->set_cap) return RIP_OK;
+  uint64_t nc = std::max<uint64_t>(need, std::max<uint64_t>(p->set_cap * 2, 4096));
+  TRY(dgrow(c, p->set_off, nc * sizeof(uint64_t), p->num_sets * sizeof(uint64_t)));
+  TRY(dgrow(c, p->set_len, nc * sizeof(uint32_t), p->num_sets * sizeof(uint32_t)));
+  p->set_cap = nc;
+  return RIP_OK;
+}
+
+static int ensure_elems(rip_pool *p, uint64_t need) {
+  rip_ctx *c = p->ctx;
+  if (need <= p->cap) return RIP_OK;
+  uint64_t nc = std::max<uint64_t>(need, std::max<uint64_t>(p->cap + p->cap / 2, 1 << 16));
+  TRY(dgrow(c, p->vtx, nc * sizeof(uint32_t), p->num_elems * sizeof(uint32_t)));
+  p->cap = nc;
+  return RIP_OK;
+}
+
+// Partitions the sampler scratch into `warps` x (bitmap + queue of qcap).
+static int ensure_scratch(rip_pool *p, uint32_t warps, uint32_t qcap) {
+  rip_ctx *c = p->ctx;
+  const uint64_t bm_words = (((uint64_t)p->g->n + 31) / 32 + 7) & ~7ull;
+  const uint64_t per = bm_words * 4 + (uint64_t)qcap * 4;
+  const uint64_t bytes = per * warps;
+  if (p->scratch.p && p->bm_words == bm_words && p->qcap == qcap &&
+      p->warps == warps)
+    return RIP_OK;
+  TRY(dalloc(c, p->scratch, bytes));
+  // bitmaps must start all-zero; queue contents are don't-care
+  CK(c, cudaMemsetAsync(p->scratch.p, 0, bytes, c->stream));
+  p->bm_words = bm_words;
+  p->qcap = qcap;
+  p->warps = warps;
+  return RIP_OK;
+}
+
+static uint32_t default_warps(rip_pool *p, uint32_t qcap) {
+  rip_ctx *c = p->ctx;
+  const uint64_t bm_bytes = ((((uint64_t)p->g->n + 31) / 32 + 7) & ~7ull) * 4;
+  const uint64_t per = bm_bytes + (uint64_t)qcap * 4;
+  uint64_t want = (uint64_t)c->num_sms * 32;  // 32 resident warps per SM
+  size_t avail = c->budget > c->used ? c->budget - c->used : 0;
+  uint64_t fit = (avail / 4) / per;  // scratch gets at most a quarter
+  uint64_t w = std::min<uint64_t>(want, std::max<uint64_t>(fit, 8));
+  return (uint32_t)std::max<uint64_t>(8, w & ~7ull);
+}
+
+static int sample_fused(rip_pool *p, uint64_t seed, uint64_t first, uint32_t count);
+
+static int sample_warp_per_set(rip_pool *p, uint64_t seed, uint64_t first,
+                               uint32_t count, const std::vector<uint32_t> *only) {
+  rip_ctx *c = p->ctx;
+  rip_graph *g = p->g;
+  uint32_t qcap = std::min<uint32_t>(g->n, 1u << 14);
+  if (p->qcap > qcap && p->scratch.p) qcap = p->qcap;
+  uint32_t warps = p->warps && p->qcap == qcap ? p->warps : default_warps(p, qcap);
+  TRY(ensure_scratch(p, warps, qcap));
+  TRY(dalloc(c, p->ids_a, sizeof(uint32_t) * (size_t)count));
+  TRY(dalloc(c, p->ids_b, sizeof(uint32_t) * (size_t)count));
+  PoolMeta *dm = p->dmeta();
+  const uint32_t *ids = nullptr;
+  uint32_t todo = count;
+  bool use_a = true;
+  if (only) {  // run just these indices (relative to first)
+    todo = (uint32_t)only->size();
+    if (todo == 0) return RIP_OK;
+    CK(c, cudaMemcpyAsync(p->ids_b.p, only->data(), sizeof(uint32_t) * todo,
+                          cudaMemcpyHostToDevice, c->stream));
+    ids = ptr<uint32_t>(p->ids_b);
+  }
+  for (int attempt = 0; attempt < 64; ++attempt) {
+    CK(c, cudaMemsetAsync(&dm->fail_count, 0, sizeof(unsigned int), c->stream));
+    CK(c, cudaMemsetAsync(&dm->next, 0, sizeof(unsigned int), c->stream));
+    CK(c, cudaMemsetAsync(&dm->first_bad, 0xFF, sizeof(unsigned long long), c->stream));
+    SampleLaunch L;
+    L.G = g->view();
+    L.P = p->view();
+    L.key = make_key(seed);
+    L.first = first;
+    L.count = todo;
+    L.ids = ids;
+    L.next = &dm->next;
+    L.bitmaps = ptr<uint32_t>(p->scratch);
+    L.bm_words = p->bm_words;
+    L.queues = ptr<uint32_t>(p->scratch) + (size_t)p->bm_words * p->warps;
+    L.qcap = p->qcap;
+    L.F = FailList{ptr<uint32_t>(use_a ? p->ids_a : p->ids_b), &dm->fail_count,
+                   &dm->first_bad};
+    L.st = Stats{dm->stats};
+    L.threads = 256;
+    const uint32_t active = std::min<uint32_t>(p->warps, todo);
+    L.blocks = (int)std::max<uint32_t>(1, (active + 7) / 8);
+    CK(c, cudaEventRecord(c->ev0, c->stream));
+    if (g->model == RIP_MODEL_IC)
+      launch_ic_plain(L, c->stream);
+    else
+      launch_lt_walk(L, c->stream);
+    CK(c, cudaGetLastError());
+    CK(c, cudaEventRecord(c->ev1, c->stream));
+    PoolMeta m;
+    TRY(read_meta(p, m));
+    float kms = 0.f;
+    cudaEventElapsedTime(&kms, c->ev0, c->ev1);
+    p->kernel_ms += kms;
+    p->kernel_launches++;
+    if (m.fail_count == 0) {
+      p->num_elems = m.cursor;
+      return RIP_OK;
+    }
+    // Some sets did not fit.  Roll the bump pointer back to the end of the
+    // last stored set, grow what overflowed, and re-run only the failures.
+    unsigned long long cur = std::min<unsigned long long>(m.cursor, m.first_bad);
+    CK(c, cudaMemcpyAsync(&dm->cursor, &cur, sizeof(cur), cudaMemcpyHostToDevice,
+                          c->stream));
+    p->num_elems = cur;
+    if (m.first_bad != ~0ull) {
+      double mean = m.stats[2] ? (double)m.stats[3] / (double)m.stats[2] : 16.0;
+      uint64_t need = cur + (uint64_t)(mean * 2.0 * m.fail_count) + 4096;
+      TRY(ensure_elems(p, std::max<uint64_t>(need, p->cap * 2)));
+    }
+    if (p->qcap < g->n) {
+      // queue overflow is the other failure cause: widen the queues (fewer
+      // warps) so the worst case, a set holding every vertex, fits eventually
+      uint32_t nq = (uint32_t)std::min<uint64_t>(g->n, (uint64_t)p->qcap * 4);
+      uint32_t nw = std::max<uint32_t>(8, std::min(default_warps(p, nq), p->warps));
+      TRY(ensure_scratch(p, nw, nq));
+    }
+    ids = ptr<uint32_t>(use_a ? p->ids_a : p->ids_b);
+    use_a = !use_a;
+    todo = m.fail_count;
+  }
+  return set_err(c, RIP_ERR_DEVICE, "sampler did not converge after retries");
+}
+
+// ---------------------------------------------------------------------------
+// fused multi-colour sampler (IC)
+// ---------------------------------------------------------------------------
+static int ensure_fused_scratch(rip_pool *p, uint32_t slots, uint32_t cw,
+                                uint32_t lcap) {
+  rip_ctx *c = p->ctx;
+  const size_t n = p->g->n;
+  if (p->f_vis.p && p->f_slots == slots && p->f_cw == cw && p->f_lcap == lcap)
+    return RIP_OK;
+  const size_t mask_bytes = (size_t)slots * n * cw * sizeof(uint64_t);
+  TRY(dalloc(c, p->f_vis, mask_bytes));
+  TRY(dalloc(c, p->f_pend, mask_bytes));
+  TRY(dalloc(c, p->f_flag, (size_t)slots * n * sizeof(uint32_t)));
+  TRY(dalloc(c, p->f_log, (size_t)slots * lcap * sizeof(uint32_t)));
+  CK(c, cudaMemsetAsync(p->f_vis.p, 0, mask_bytes, c->stream));
+  CK(c, cudaMemsetAsync(p->f_pend.p, 0, mask_bytes, c->stream));
+  CK(c, cudaMemsetAsync(p->f_flag.p, 0, (size_t)slots * n * sizeof(uint32_t), c->stream));
+  p->f_slots = slots;
+  p->f_cw = cw;
+  p->f_lcap = lcap;
+  return RIP_OK;
+}
+
+static int clear_fused_scratch(rip_pool *p) {
+  rip_ctx *c = p->ctx;
+  const size_t n = p->g->n;
+  const size_t mask_bytes = (size_t)p->f_slots * n * p->f_cw * sizeof(uint64_t);
+  CK(c, cudaMemsetAsync(p->f_vis.p, 0, mask_bytes, c->stream));
+  CK(c, cudaMemsetAsync(p->f_pend.p, 0, mask_bytes, c->stream));
+  CK(c, cudaMemsetAsync(p->f_flag.p, 0, (size_t)p->f_slots * n * sizeof(uint32_t), c->stream));
+  return RIP_OK;
+}
+
+static int sample_fused(rip_pool *p, uint64_t seed, uint64_t first,
+                        uint32_t count) {
+  rip_ctx *c = p->ctx;
+  rip_graph *g = p->g;
+  const uint32_t colors = p->colors;
+  const uint32_t cw = colors / 64;
+  uint32_t lcap = p->lcap_pref ? p->lcap_pref
+                 : p->f_lcap  ? p->f_lcap
+                              : (uint32_t)std::min<uint64_t>(
+                                    std::max<uint64_t>((uint64_t)g->n * 2, 4096), 1u << 20);
+  // slots: one per resident CTA, limited by what the masks cost
+  const size_t per_slot = (size_t)g->n * (cw * 16 + 4) + (size_t)lcap * 4;
+  size_t avail = c->budget > c->used ? c->budget - c->used : 0;
+  avail += p->f_vis.bytes + p->f_pend.bytes + p->f_flag.bytes + p->f_log.bytes;
+  uint64_t fit = (avail / 2) / std::max<size_t>(per_slot, 1);
+  uint64_t want = p->fused_slots ? p->fused_slots
+                                 : (uint64_t)c->num_sms * fused_ctas_per_sm(colors);
+  uint32_t slots = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(want, fit));
+  if (p->f_vis.p && p->f_cw == cw && p->f_lcap == lcap && p->f_slots >= 1 &&
+      p->f_slots <= slots)
+    slots = p->f_slots;  // reuse the existing partition
+  TRY(ensure_fused_scratch(p, slots, cw, lcap));
+  TRY(dalloc(c, p->ids_a, sizeof(uint32_t) * ((size_t)count / 64 + 2)));
+  PoolMeta *dm = p->dmeta();
+  std::vector<uint32_t> order;  // empty: identity over [0, count)
+  uint32_t todo = count;
+  for (int attempt = 0; attempt < 4 && todo; ++attempt) {
+    const uint32_t nb = (todo + colors - 1) / colors;
+    if (!order.empty()) {
+      TRY(dalloc(c, p->f_order, sizeof(uint32_t) * order.size()));
+      CK(c, cudaMemcpyAsync(p->f_order.p, order.data(), sizeof(uint32_t) * order.size(),
+                            cudaMemcpyHostToDevice, c->stream));
+    }
+    CK(c, cudaMemsetAsync(&dm->fail_count, 0, sizeof(unsigned int), c->stream));
+    CK(c, cudaMemsetAsync(&dm->next, 0, sizeof(unsigned int), c->stream));
+    CK(c, cudaMemsetAsync(&dm->fused_dirty, 0, sizeof(unsigned int), c->stream));
+    CK(c, cudaMemsetAsync(&dm->first_bad, 0xFF, sizeof(unsigned long long), c->stream));
+    FusedLaunch L;
+    L.G = g->view();
+    L.P = p->view();
+    L.key = make_key(seed);
+    L.first = first;
+    L.count = todo;
+    L.order = order.empty() ? nullptr : ptr<uint32_t>(p->f_order);
+    L.num_batches = nb;
+    L.colors = colors;
+    L.next = &dm->next;
+    L.vis = ptr<uint64_t>(p->f_vis);
+    L.pend = ptr<uint64_t>(p->f_pend);
+    L.pflag = ptr<uint32_t>(p->f_flag);
+    L.log = ptr<uint32_t>(p->f_log);
+    L.lcap = p->f_lcap;
+    L.dirty = &dm->fused_dirty;
+    L.F = FailList{ptr<uint32_t>(p->ids_a), &dm->fail_count, &dm->first_bad};
+    L.st = Stats{dm->stats};
+    L.blocks = (int)std::min<uint32_t>(p->f_slots, nb);
+    CK(c, cudaEventRecord(c->ev0, c->stream));
+    launch_ic_fused(L, c->stream);
+    CK(c, cudaGetLastError());
+    CK(c, cudaEventRecord(c->ev1, c->stream));
+    PoolMeta m;
+    TRY(read_meta(p, m));
+    float kms = 0.f;
+    cudaEventElapsedTime(&kms, c->ev0, c->ev1);
+    p->kernel_ms += kms;
+    p->kernel_launches++;
+    const uint32_t claimed = std::min<uint32_t>(m.next, nb);
+    if (m.fail_count == 0 && claimed == nb) {
+      p->num_elems = m.cursor;
+      return RIP_OK;
+    }
+    unsigned long long cur = std::min<unsigned long long>(m.cursor, m.first_bad);
+    CK(c, cudaMemcpyAsync(&dm->cursor, &cur, sizeof(cur), cudaMemcpyHostToDevice,
+                          c->stream));
+    p->num_elems = cur;
+    std::vector<uint32_t> failed(m.fail_count);
+    if (m.fail_count)
+      CK(c, cudaMemcpyAsync(failed.data(), p->ids_a.p, sizeof(uint32_t) * m.fail_count,
+                            cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    for (uint32_t b = claimed; b < nb; ++b) failed.push_back(b);
+    std::vector<uint32_t> next_order;
+    for (uint32_t b : failed)
+      for (uint32_t i = b * colors; i < std::min<uint32_t>((b + 1) * colors, todo); ++i)
+        next_order.push_back(order.empty() ? i : order[i]);
+    order.swap(next_order);
+    todo = (uint32_t)order.size();
+    if (m.first_bad != ~0ull) {
+      double mean = m.stats[2] ? (double)m.stats[3] / (double)m.stats[2] : 16.0;
+      TRY(ensure_elems(p, std::max<uint64_t>(cur + (uint64_t)(mean * 2.0 * todo) + 4096,
+                                             p->cap * 2)));
+    }
+    if (m.fused_dirty) {
+      // a frontier log overflowed: clear the masks and give the logs more room
+      TRY(clear_fused_scratch(p));
+      const uint32_t nl = (uint32_t)std::min<uint64_t>((uint64_t)p->f_lcap * 4,
+                                                       (uint64_t)g->n * colors);
+      const uint32_t ns = std::max<uint32_t>(1, p->f_slots / 2);
+      TRY(ensure_fused_scratch(p, ns, cw, nl));
+    }
+  }
+  if (todo == 0) return RIP_OK;
+  // Whatever still failed runs set by set (same sets, bit for bit).
+  return sample_warp_per_set(p, seed, first, todo, &order);
+}
+
+// Fused-sampler configuration (the autotuner's knobs): colour width 64, 128
+// or 256, number of CTA slots (0 = size from the budget) and frontier-log
+// capacity per slot (0 = default).  Takes effect at the next rip_sample.
+extern "C" int rip_pool_configure(rip_pool *p, uint32_t colors, uint32_t slots,
+                                  uint32_t log_capacity) {
+  if (!p) return RIP_ERR_INVALID;
+  if (colors != 64 && colors != 128 && colors != 256)
+    return set_err(p->ctx, RIP_ERR_INVALID, "colors must be 64, 128 or 256");
+  p->colors = colors;
+  p->fused_slots = slots;
+  p->lcap_pref = log_capacity;
+  return RIP_OK;
+}
+
+extern "C" int rip_sample(rip_pool *p, uint64_t seed, uint64_t count,
+                          int sampler) {
+  if (!p) return RIP_ERR_INVALID;
+  rip_ctx *c = p->ctx;
+  if (count == 0) return RIP_OK;
+  if (count >= (1ull << 31))
+    return set_err(c, RIP_ERR_LIMIT, "rip_sample: at most 2^31-1 sets per call");
+  if (p->num_sets + count >= (1ull << 56))
+    return set_err(c, RIP_ERR_LIMIT, "rip_sample: set ids are limited to 2^56");
+  CK(c, cudaSetDevice(c->device));
+  const uint64_t first = p->num_sets;
+  TRY(ensure_sets(p, first + count));
+  PoolMeta m;
+  TRY(read_meta(p, m));
+  double mean = m.stats[2] ? (double)m.stats[3] / (double)m.stats[2] : 8.0;
+  TRY(ensure_elems(p, p->num_elems + (uint64_t)(mean * 1.25 * count) + 1024));
+  int rc;
+  if (p->g->model == RIP_MODEL_IC && sampler != RIP_SAMPLER_PLAIN)
+    rc = sample_fused(p, seed, first, (uint32_t)count);
+  else
+    rc = sample_warp_per_set(p, seed, first, (uint32_t)count, nullptr);
+  if (rc != RIP_OK) return rc;
+  p->num_sets += count;
+  p->have_last_counts = false;
+  return RIP_OK;
+}
+
+extern "C" int rip_pool_export(rip_pool *p, uint64_t first, uint64_t count,
+                               uint64_t *offsets, uint32_t *vertices) {
+  if (!p || !offsets) return RIP_ERR_INVALID;
+  rip_ctx *c = p->ctx;
+  if (first + count > p->num_sets)
+    return set_err(c, RIP_ERR_INVALID, "export range beyond the pool (%llu sets)",
+                   (unsigned long long)p->num_sets);
+  std::vector<uint32_t> lens(count);
+  if (count) {
+    CK(c, cudaMemcpyAsync(lens.data(), ptr<uint32_t>(p->set_len) + first,
+                          sizeof(uint32_t) * count, cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+  }
+  offsets[0] = 0;
+  for (uint64_t i = 0; i < count; ++i) offsets[i + 1] = offsets[i] + lens[i];
+  if (!vertices || offsets[count] == 0) return RIP_OK;
+  DevMem d_csr, d_out;
+  int rc = RIP_OK;
+  do {
+    if ((rc = dalloc(c, d_csr, sizeof(uint64_t) * (count + 1)))) break;
+    if ((rc = dalloc(c, d_out, sizeof(uint32_t) * offsets[count]))) break;
+    cudaMemcpyAsync(d_csr.p, offsets, sizeof(uint64_t) * (count + 1),
+                    cudaMemcpyHostToDevice, c->stream);
+    launch_gather_sets(p->view(), first, count, ptr<uint64_t>(d_csr),
+                       ptr<uint32_t>(d_out), c->stream);
+    cudaMemcpyAsync(vertices, d_out.p, sizeof(uint32_t) * offsets[count],
+                    cudaMemcpyDeviceToHost, c->stream);
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess) rc = set_err(c, RIP_ERR_CUDA, "export failed: %s", cudaGetErrorString(e));
+  } while (0);
+  dfree(c, d_csr);
+  dfree(c, d_out);
+  if (rc) return rc;
+#pragma omp parallel for schedule(dynamic, 256)
+  for (long long i = 0; i < (long long)count; ++i)
+    std::sort(vertices + offsets[i], vertices + offsets[i + 1]);
+  return RIP_OK;
+}
+
+extern "C" int rip_pool_import(rip_pool *p, const uint64_t *offsets,
+                               const uint32_t *vertices, uint64_t count) {
+  if (!p || !offsets || (offsets[count] && !vertices)) return RIP_ERR_INVALID;
+  rip_ctx *c = p->ctx;
+  if (offsets[0] != 0)
+    return set_err(c, RIP_ERR_INVALID, "rip_pool_import: offsets[0] must be 0");
+  const uint64_t P = offsets[count];
+  for (uint64_t i = 0; i < count; ++i) {
+    if (offsets[i + 1] < offsets[i])
+      return set_err(c, RIP_ERR_INVALID, "rip_pool_import: offsets not monotone");
+    if (offsets[i + 1] - offsets[i] > p->g->n)
+      return set_err(c, RIP_ERR_INVALID, "rip_pool_import: set larger than n");
+  }
+  for (uint64_t i = 0; i < P; ++i)
+    if (vertices[i] >= p->g->n)
+      return set_err(c, RIP_ERR_INVALID, "rip_pool_import: vertex %u out of range",
+                     vertices[i]);
+  CK(c, cudaSetDevice(c->device));
+  TRY(ensure_sets(p, p->num_sets + count));
+  TRY(ensure_elems(p, p->num_elems + P));
+  std::vector<uint64_t> so(count);
+  std::vector<uint32_t> sl(count);
+  for (uint64_t i = 0; i < count; ++i) {
+    so[i] = p->num_elems + offsets[i];
+    sl[i] = (uint32_t)(offsets[i + 1] - offsets[i]);
+  }
+  if (P)
+    CK(c, cudaMemcpyAsync(ptr<uint32_t>(p->vtx) + p->num_elems, vertices,
+                          sizeof(uint32_t) * P, cudaMemcpyHostToDevice, c->stream));
+  if (count) {
+    CK(c, cudaMemcpyAsync(ptr<uint64_t>(p->set_off) + p->num_sets, so.data(),
+                          sizeof(uint64_t) * count, cudaMemcpyHostToDevice, c->stream));
+    CK(c, cudaMemcpyAsync(ptr<uint32_t>(p->set_len) + p->num_sets, sl.data(),
+                          sizeof(uint32_t) * count, cudaMemcpyHostToDevice, c->stream));
+  }
+  unsigned long long cur = p->num_elems + P;
+  CK(c, cudaMemcpyAsync(&p->dmeta()->cursor, &cur, sizeof(cur),
+                        cudaMemcpyHostToDevice, c->stream));
+  CK(c, cudaStreamSynchronize(c->stream));
+  p->num_elems += P;
+  p->num_sets += count;
+  p->have_last_counts = false;
+  return RIP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// selection
+// ---------------------------------------------------------------------------
+namespace {
+struct CompareHeap {  // include/ripples/streaming_find_most_influential.h:410-418
+  bool operator()(const std::pair<uint32_t, size_t> &a,
+                  const std::pair<uint32_t, size_t> &b) const {
+    return a.second < b.second;
+  }
+};
+}  // namespace
+
+static int count_sets(rip_pool *p, uint64_t S) {
+  rip_ctx *c = p->ctx;
+  const uint32_t n = p->g->n;
+  TRY(dalloc(c, p->count, sizeof(uint32_t) * (size_t)n));
+  CK(c, cudaMemsetAsync(p->count.p, 0, sizeof(uint32_t) * (size_t)n, c->stream));
+  launch_count(p->view(), S, ptr<uint32_t>(p->count), c->num_sms * 8, c->stream);
+  CK(c, cudaGetLastError());
+  return RIP_OK;
+}
+
+extern "C" int rip_count(rip_pool *p, uint64_t num_sets, uint32_t *counts) {
+  if (!p || !counts || num_sets > p->num_sets) return RIP_ERR_INVALID;
+  rip_ctx *c = p->ctx;
+  CK(c, cudaSetDevice(c->device));
+  TRY(count_sets(p, num_sets));
+  CK(c, cudaMemcpyAsync(counts, p->count.p, sizeof(uint32_t) * p->g->n,
+                        cudaMemcpyDeviceToHost, c->stream));
+  CK(c, cudaStreamSynchronize(c->stream));
+  return RIP_OK;
+}
+
+// Counts left by the last rip_select (after its last update step).
+extern "C" int rip_select_counts(rip_pool *p, uint32_t *counts) {
+  if (!p || !counts) return RIP_ERR_INVALID;
+  if (!p->have_last_counts)
+    return set_err(p->ctx, RIP_ERR_STATE, "no selection has run on this pool");
+  std::memcpy(counts, p->last_counts.data(), sizeof(uint32_t) * p->g->n);
+  return RIP_OK;
+}
+
+extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
+                          uint32_t *seeds, uint64_t *gains, uint32_t *num_seeds,
+                          double *f) {
+  if (!p || (k && !seeds) || !num_seeds) return RIP_ERR_INVALID;
+  rip_ctx *c = p->ctx;
+  if (S > p->num_sets)
+    return set_err(c, RIP_ERR_INVALID, "rip_select: %llu sets requested, pool has %llu",
+                   (unsigned long long)S, (unsigned long long)p->num_sets);
+  if (tiebreak != RIP_TIE_REF_HEAP && tiebreak != RIP_TIE_LOWEST_ID)
+    return set_err(c, RIP_ERR_INVALID, "rip_select: unknown tie-break %d", tiebreak);
+  if (S >= (1ull << 32))
+    return set_err(c, RIP_ERR_LIMIT, "rip_select: at most 2^32-1 sets");
+  CK(c, cudaSetDevice(c->device));
+  const uint32_t n = p->g->n;
+  *num_seeds = 0;
+  if (f) *f = 0.0;
+  CK(c, cudaEventRecord(c->ev0, c->stream));
+  // 1. histogram, 2. vertex -> sets index
+  TRY(count_sets(p, S));
+  TRY(dalloc(c, p->inv_off, sizeof(uint64_t) * ((size_t)n + 1)));
+  TRY(dalloc(c, p->inv_cur, sizeof(uint64_t) * ((size_t)n + 1)));
+  TRY(dalloc(c, p->scan_sums, sizeof(uint64_t) * scan_block_sums_needed(n)));
+  launch_exclusive_scan(ptr<uint32_t>(p->count), ptr<uint64_t>(p->inv_off), n,
+                        ptr<uint64_t>(p->scan_sums), c->stream);
+  uint64_t P = 0;
+  CK(c, cudaMemcpyAsync(&P, ptr<uint64_t>(p->inv_off) + n, sizeof(uint64_t),
+                        cudaMemcpyDeviceToHost, c->stream));
+  CK(c, cudaMemcpyAsync(p->inv_cur.p, p->inv_off.p, sizeof(uint64_t) * ((size_t)n + 1),
+                        cudaMemcpyDeviceToDevice, c->stream));
+  CK(c, cudaStreamSynchronize(c->stream));
+  TRY(dalloc(c, p->inv, sizeof(uint32_t) * std::max<uint64_t>(P, 1)));
+  launch_build_inverted(p->view(), S, ptr<uint64_t>(p->inv_cur), ptr<uint32_t>(p->inv),
+                        c->num_sms * 8, c->stream);
+  CK(c, cudaGetLastError());
+  TRY(dalloc(c, p->covered, std::max<uint64_t>(S, 1)));
+  CK(c, cudaMemsetAsync(p->covered.p, 0, std::max<uint64_t>(S, 1), c->stream));
+  const size_t dwords = ((size_t)n + 31) / 32;
+  TRY(dalloc(c, p->dirty_bits, sizeof(uint32_t) * dwords));
+  CK(c, cudaMemsetAsync(p->dirty_bits.p, 0, sizeof(uint32_t) * dwords, c->stream));
+  TRY(dalloc(c, p->dirty_list, sizeof(uint32_t) * (size_t)n));
+  TRY(dalloc(c, p->pairs, sizeof(uint2) * (size_t)n));
+  PoolMeta *dm = p->dmeta();
+  CK(c, cudaMemsetAsync(&dm->dirty_n, 0, sizeof(unsigned int), c->stream));
+  CK(c, cudaMemsetAsync(&dm->covered_sets, 0, sizeof(unsigned long long), c->stream));
+
+  CoverLaunch C;
+  C.P = p->view();
+  C.inv_off = ptr<uint64_t>(p->inv_off);
+  C.inv = ptr<uint32_t>(p->inv);
+  C.covered = ptr<uint8_t>(p->covered);
+  C.count = ptr<uint32_t>(p->count);
+  C.dirty_bits = ptr<uint32_t>(p->dirty_bits);
+  C.dirty_list = ptr<uint32_t>(p->dirty_list);
+  C.dirty_n = &dm->dirty_n;
+  C.covered_sets = &dm->covered_sets;
+  C.blocks = c->num_sms * 4;
+
+  std::vector<uint32_t> &hcount = p->last_counts;
+  hcount.resize(n);
+  TRY(p->h_pairs.ensure(c, sizeof(uint2) * (size_t)n));
+  TRY(p->h_count.ensure(c, sizeof(uint32_t) * (size_t)n));
+
+  uint64_t uncovered = S;
+  std::vector<uint32_t> out_seeds;
+  std::vector<uint64_t> out_gains;
+
+  // Applies the dirty (vertex, count) list of the last cover step to hcount.
+  auto sync_dirty = [&]() -> int {
+    unsigned int dn = 0;
+    CK(c, cudaMemcpyAsync(&dn, &dm->dirty_n, sizeof(dn), cudaMemcpyDeviceToHost,
+                          c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    if (dn == 0) return RIP_OK;
+    launch_gather_dirty(ptr<uint32_t>(p->dirty_list), &dm->dirty_n, n,
+                        ptr<uint32_t>(p->count), ptr<uint32_t>(p->dirty_bits),
+                        ptr<uint2>(p->pairs), c->num_sms * 4, c->stream);
+    CK(c, cudaMemcpyAsync(p->h_pairs.p, p->pairs.p, sizeof(uint2) * dn,
+                          cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaMemsetAsync(&dm->dirty_n, 0, sizeof(unsigned int), c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    const uint2 *hp = reinterpret_cast<const uint2 *>(p->h_pairs.p);
+    for (unsigned int i = 0; i < dn; ++i) hcount[hp[i].x] = hp[i].y;
+    return RIP_OK;
+  };
+
+  if (tiebreak == RIP_TIE_REF_HEAP) {
+    CK(c, cudaMemcpyAsync(p->h_count.p, p->count.p, sizeof(uint32_t) * (size_t)n,
+                          cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    std::memcpy(hcount.data(), p->h_count.p, sizeof(uint32_t) * (size_t)n);
+    // InitHeapStorage + std::priority_queue(cmp, std::move(storage)), exactly
+    // as the reference builds its heap (streaming_find_most_influential.h:541-544)
+    std::vector<std::pair<uint32_t, size_t>> storage(n);
+    for (uint32_t v = 0; v < n; ++v) storage[v] = {v, hcount[v]};
+    std::priority_queue<std::pair<uint32_t, size_t>,
+                        std::vector<std::pair<uint32_t, size_t>>, CompareHeap>
+        queue(CompareHeap{}, std::move(storage));
+    while (out_seeds.size() < k && uncovered != 0) {
+      std::pair<uint32_t, size_t> element;
+      for (;;) {  // getNextSeed, streaming_find_most_influential.h:560-571
+        if (queue.empty())
+          return set_err(c, RIP_ERR_STATE, "selection heap exhausted");
+        element = queue.top();
+        queue.pop();
+        if (element.second > hcount[element.first]) {
+          element.second = hcount[element.first];
+          queue.push(element);
+          continue;
+        }
+        break;
+      }
+      uncovered -= element.second;
+      out_seeds.push_back(element.first);
+      out_gains.push_back(element.second);
+      if (out_seeds.size() == k) break;
+      C.vertex = element.first;
+      launch_cover(C, c->stream);
+      CK(c, cudaGetLastError());
+      TRY(sync_dirty());
+    }
+  } else {
+    while (out_seeds.size() < k && uncovered != 0) {
+      CK(c, cudaMemsetAsync(&dm->best, 0, sizeof(unsigned long long), c->stream));
+      launch_argmax(ptr<uint32_t>(p->count), n, &dm->best, c->num_sms * 4, c->stream);
+      unsigned long long best = 0;
+      CK(c, cudaMemcpyAsync(&best, &dm->best, sizeof(best), cudaMemcpyDeviceToHost,
+                            c->stream));
+      CK(c, cudaStreamSynchronize(c->stream));
+      const uint32_t v = ~(uint32_t)(best & 0xFFFFFFFFull);
+      const uint64_t cnt = best >> 32;
+      uncovered -= cnt;
+      out_seeds.push_back(v);
+      out_gains.push_back(cnt);
+      if (out_seeds.size() == k) break;
+      C.vertex = v;
+      launch_cover(C, c->stream);
+      CK(c, cudaGetLastError());
+      CK(c, cudaMemsetAsync(&dm->dirty_n, 0, sizeof(unsigned int), c->stream));
+      // the lowest-id path keeps no host mirror; dirty bits are reset below
+    }
+    CK(c, cudaMemcpyAsync(p->h_count.p, p->count.p, sizeof(uint32_t) * (size_t)n,
+                          cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    std::memcpy(hcount.data(), p->h_count.p, sizeof(uint32_t) * (size_t)n);
+  }
+  CK(c, cudaEventRecord(c->ev1, c->stream));
+  CK(c, cudaStreamSynchronize(c->stream));
+  float sms = 0.f;
+  cudaEventElapsedTime(&sms, c->ev0, c->ev1);
+  p->select_kernel_ms += sms;
+  p->have_last_counts = true;
+  for (size_t i = 0; i < out_seeds.size(); ++i) {
+    seeds[i] = out_seeds[i];
+    if (gains) gains[i] = out_gains[i];
+  }
+  *num_seeds = (uint32_t)out_seeds.size();
+  if (f) *f = S ? double(S - uncovered) / (double)S : 0.0;
+  return RIP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// theta math: include/ripples/imm.h:77-128, utility.h:84-87
+// ---------------------------------------------------------------------------
+extern "C" double rip_log_binomial(uint64_t n, uint64_t k) {
+  return lgamma(n + 1) - lgamma(n - k + 1) - lgamma(k + 1);
+}
+
+extern "C" int64_t rip_theta_prime(int64_t x, double epsilonPrime, double l,
+                                   uint64_t k, uint64_t num_nodes) {
+  k = std::min<uint64_t>(k, num_nodes / 2);
+  return (ssize_t)((2 + 2. / 3. * epsilonPrime) *
+                   (l * std::log(num_nodes) + rip_log_binomial(num_nodes, k) +
+                    std::log(std::log2(num_nodes))) *
+                   std::pow(2.0, x) / (epsilonPrime * epsilonPrime));
+}
+
+extern "C" int64_t rip_inv_theta_prime(int64_t rrsize, double epsilonPrime,
+                                       double l, uint64_t k, uint64_t num_nodes) {
+  k = std::min<uint64_t>(k, num_nodes / 2);
+  return (ssize_t)std::log2(rrsize * epsilonPrime * epsilonPrime /
+                            ((2 + 2. / 3. * epsilonPrime) *
+                             (l * std::log(num_nodes) +
+                              rip_log_binomial(num_nodes, k) +
+                              std::log(std::log2(num_nodes)))));
+}
+
+extern "C" uint64_t rip_theta(double epsilon, double l, uint64_t k, double LB,
+                              uint64_t num_nodes) {
+  if (LB == 0) return 0;
+  k = std::min<uint64_t>(k, num_nodes / 2);
+  double term1 = 0.6321205588285577;  // 1 - 1/e
+  double alpha = sqrt(l * std::log(num_nodes) + std::log(2));
+  double beta = sqrt(term1 * (rip_log_binomial(num_nodes, k) +
+                              l * std::log(num_nodes) + std::log(2)));
+  double lamdaStar = 2 * num_nodes * (term1 * alpha + beta) *
+                     (term1 * alpha + beta) * pow(epsilon, -2);
+  return (size_t)(lamdaStar / LB);
+}
+
+// ---------------------------------------------------------------------------
+// IMM driver: include/ripples/imm.h:145-260 (Sampling, omp) + :768-860 (IMM)
+// ---------------------------------------------------------------------------
+extern "C" int rip_imm_pool(rip_pool *p, uint32_t k, double epsilon, double l,
+                            uint64_t seed, int tiebreak, int sampler,
+                            uint32_t *seeds, uint32_t *num_seeds,
+                            rip_imm_record *rec) {
+  if (!p || !num_seeds || (k && !seeds) || !(epsilon > 0)) return RIP_ERR_INVALID;
+  rip_ctx *c = p->ctx;
+  rip_imm_record R;
+  std::memset(&R, 0, sizeof(R));
+  const auto t_total = clk::now();
+  const uint64_t n = p->g->n;
+  l = l * (1 + 1 / std::log2(n));
+  const double epsilonPrime = 1.4142135623730951 * epsilon;
+  double LB = 0;
+  std::vector<uint32_t> tmp_seeds(std::max<uint32_t>(k, 1));
+  const auto t_est = clk::now();
+  int64_t x = 1;
+  if (p->num_sets != 0)
+    x = rip_inv_theta_prime((int64_t)(p->num_sets / 2), epsilonPrime, l, k, n);
+  for (; x < std::log2(n); ++x) {
+    int64_t thetaPrime = rip_theta_prime(x, epsilonPrime, l, k, n);
+    double f = 0;
+    auto t0 = clk::now();
+    uint64_t delta = 0;
+    if ((uint64_t)std::max<int64_t>(thetaPrime, 0) > p->num_sets) {
+      delta = (uint64_t)thetaPrime - p->num_sets;
+      TRY(rip_sample(p, seed, delta, sampler));
+      TRY(rip_sync(c));
+    }
+    double gen_ms = ms_since(t0);
+    t0 = clk::now();
+    uint32_t ns = 0;
+    TRY(rip_select(p, p->num_sets, k, tiebreak, tmp_seeds.data(), nullptr, &ns, &f));
+    double sel_ms = ms_since(t0);
+    if (R.num_rounds < RIP_MAX_ROUNDS) {
+      R.theta_prime_deltas[R.num_rounds] = delta;
+      R.round_generate_ms[R.num_rounds] = gen_ms;
+      R.round_select_ms[R.num_rounds] = sel_ms;
+    }
+    R.num_rounds++;
+    if (f >= std::pow(2, -x)) {
+      LB = (n * f) / (1 + epsilonPrime);
+      break;
+    }
+  }
+  const uint64_t theta = rip_theta(epsilon, l, k, LB, n);
+  R.theta_estimation_ms = ms_since(t_est);
+  R.theta = theta;
+  auto t0 = clk::now();
+  if (theta > p->num_sets) {
+    TRY(rip_sample(p, seed, theta - p->num_sets, sampler));
+    TRY(rip_sync(c));
+  }
+  R.generate_ms = ms_since(t0);
+  t0 = clk::now();
+  double f = 0;
+  TRY(rip_select(p, std::min<uint64_t>(theta, p->num_sets), k, tiebreak, seeds,
+                 nullptr, num_seeds, &f));
+  R.select_ms = ms_since(t0);
+  R.f = f;
+  R.total_sets = p->num_sets;
+  R.pool_elements = p->num_elems;
+  R.rrr_set_bytes = p->num_elems * sizeof(uint32_t);
+  R.total_ms = ms_since(t_total);
+  if (rec) *rec = R;
+  return RIP_OK;
+}
+
+extern "C" int rip_imm(rip_ctx *c, rip_graph *g, uint32_t k, double epsilon,
+                       double l, uint64_t seed, int tiebreak, int sampler,
+                       uint32_t *seeds, uint32_t *num_seeds,
+                       rip_imm_record *record) {
+  rip_pool *p = nullptr;
+  TRY(rip_pool_create(c, g, &p));
+  int rc = rip_imm_pool(p, k, epsilon, l, seed, tiebreak, sampler, seeds,
+                        num_seeds, record);
+  rip_pool_destroy(p);
+  return rc;
+}

@@ -1,0 +1,92 @@
+// device.cuh -- device data views and warp-level helpers shared by the kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "philox.cuh"
+
+namespace rip {
+
+constexpr uint32_t FULL = 0xFFFFFFFFu;
+
+// Backward CSR packed for the sampler.  edges[e] = {source vertex, threshold}:
+//   IC: threshold = floor(p_e * 2^32)  (edge live iff coin < threshold)
+//   LT: threshold = floor(cumulative in-weight up to e * 2^32)
+// off has n+1 entries; edges is padded with {0, 0} records to a multiple of 4
+// and 32-byte aligned so a 4-edge group is one aligned 32-byte read.
+struct DevGraph {
+  uint32_t n;
+  uint64_t m;
+  const uint32_t *off;
+  const uint2 *edges;
+};
+
+// Flat RRR pool: set s occupies vtx[set_off[s] .. set_off[s] + set_len[s]).
+struct DevPool {
+  uint32_t *vtx;
+  unsigned long long *cursor;  // next free element (atomic bump pointer)
+  uint64_t cap;                // element capacity
+  uint64_t *set_off;
+  uint32_t *set_len;
+};
+
+// Failure list for sets that did not fit their scratch or the pool; the host
+// re-runs them with larger buffers (results do not depend on the retry).
+struct FailList {
+  uint32_t *ids;          // indices relative to the launch's first set
+  unsigned int *count;
+  unsigned long long *first_bad_base;  // lowest pool offset of a failed reservation
+};
+
+// Counters for roofline accounting (see rip_pool_stats in ripples_b200.h).
+struct Stats {
+  unsigned long long *v;  // [8]
+};
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+__device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x) {
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    uint32_t y = __shfl_up_sync(FULL, x, d);
+    if (lane_id() >= (uint32_t)d) x += y;
+  }
+  return x;
+}
+
+__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long x) {
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) x += __shfl_xor_sync(FULL, x, d);
+  return x;
+}
+
+// Given an inclusive warp scan `incl` (held per lane) of per-lane item
+// counts, returns the lane whose range holds item j (0 <= j < total):
+// the smallest lane i with incl[i] > j.  Five shuffle steps.
+__device__ __forceinline__ uint32_t warp_find_owner(uint32_t incl, uint32_t j) {
+  uint32_t lo = 0;
+#pragma unroll
+  for (int step = 16; step > 0; step >>= 1) {
+    uint32_t probe = __shfl_sync(FULL, incl, lo + step - 1);
+    if (probe <= j) lo += step;
+  }
+  return lo;
+}
+
+// Number of 4-edge groups covering [beg, end).
+__device__ __forceinline__ uint32_t group_count(uint32_t beg, uint32_t end) {
+  return end > beg ? ((end - 1) >> 2) - (beg >> 2) + 1 : 0;
+}
+
+// Loads the 4 edge records of group g (32-byte aligned).
+__device__ __forceinline__ void load_group(const uint2 *edges, uint32_t g,
+                                           uint2 rec[4]) {
+  const uint4 *p = reinterpret_cast<const uint4 *>(edges + ((size_t)g << 2));
+  uint4 a = __ldg(p), b = __ldg(p + 1);
+  rec[0] = make_uint2(a.x, a.y);
+  rec[1] = make_uint2(a.z, a.w);
+  rec[2] = make_uint2(b.x, b.y);
+  rec[3] = make_uint2(b.z, b.w);
+}
+
+}  // namespace rip

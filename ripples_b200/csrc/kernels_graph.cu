@@ -1,0 +1,80 @@
+// kernels_graph.cu -- packs a backward CSR into the sampler's layout.
+//
+// The reference keeps index u64[n+1], edges u32[m], weights f32[m] as three
+// arrays (include/ripples/graph.h:364-1086; device copy in
+// src/gpu/gpu_graph.cc:48-84) and compares a fresh uniform01 draw with the
+// float weight on every coin flip.  Here the weight is converted once into an
+// integer threshold and interleaved with the source id, so one aligned 8-byte
+// record serves an edge and the coin test is an integer compare:
+//   IC : thr = clamp(floor(w * 2^32), 0, 2^32-1)   live iff coin < thr
+//   LT : thr = clamp(floor((sum of in-weights up to this edge, in double,
+//                           CSR order) * 2^32), 0, 2^32-1)
+// Offsets shrink to u32 (m < 2^32 is required).
+#include "device.cuh"
+#include "launch.h"
+
+namespace rip {
+
+namespace {
+
+__device__ __forceinline__ uint32_t prob_u32(double p) {
+  const double y = p * 4294967296.0;
+  if (!(y > 0.0)) return 0u;
+  if (y >= 4294967295.0) return 0xFFFFFFFFu;
+  return (uint32_t)floor(y);
+}
+
+__global__ void pack_off_kernel(const uint64_t *index, uint32_t n,
+                                uint32_t *off) {
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v <= n;
+       v += (uint64_t)gridDim.x * blockDim.x)
+    off[v] = (uint32_t)index[v];
+}
+
+__global__ void pack_ic_kernel(const uint32_t *src, const float *w, uint64_t m,
+                               uint64_t m_pad, uint2 *edges) {
+  for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < m_pad;
+       e += (uint64_t)gridDim.x * blockDim.x)
+    edges[e] = e < m ? make_uint2(src[e], prob_u32((double)w[e]))
+                     : make_uint2(0u, 0u);
+}
+
+// One thread per vertex sums the in-weights serially, in double, in CSR order:
+// the same left-to-right sum the host-side restatement computes, so the
+// cumulative thresholds are bit-identical.  (A parallel scan would reassociate
+// the additions.)
+__global__ void pack_lt_kernel(const uint64_t *index, const uint32_t *src,
+                               const float *w, uint32_t n, uint64_t m,
+                               uint64_t m_pad, uint2 *edges) {
+  const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t v = tid; v < n; v += stride) {
+    double acc = 0.0;
+    for (uint64_t e = index[v]; e < index[v + 1]; ++e) {
+      acc += (double)w[e];
+      edges[e] = make_uint2(src[e], prob_u32(acc));
+    }
+  }
+  for (uint64_t e = m + tid; e < m_pad; e += stride) edges[e] = make_uint2(0u, 0u);
+}
+
+}  // namespace
+
+static uint64_t pad4(uint64_t m) { return (m + 3) & ~uint64_t(3); }
+
+void launch_pack_ic(const uint64_t *index, const float *w, uint32_t n,
+                    uint64_t m, uint32_t *off, uint2 *edges, const uint32_t *src,
+                    cudaStream_t stream) {
+  pack_off_kernel<<<1184, 256, 0, stream>>>(index, n, off);
+  pack_ic_kernel<<<2368, 256, 0, stream>>>(src, w, m, pad4(m) + 4, edges);
+}
+
+void launch_pack_lt(const uint64_t *index, const float *w, uint32_t n,
+                    uint64_t m, uint32_t *off, uint2 *edges, const uint32_t *src,
+                    cudaStream_t stream) {
+  pack_off_kernel<<<1184, 256, 0, stream>>>(index, n, off);
+  pack_lt_kernel<<<1184, 128, 0, stream>>>(index, src, w, n, m, pad4(m) + 4,
+                                           edges);
+}
+
+}  // namespace rip

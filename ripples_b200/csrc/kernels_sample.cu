@@ -1,0 +1,280 @@
+// kernels_sample.cu -- RRR-set sampling kernels for sm_100a.
+//
+// ic_plain_kernel   one IC set per warp: reverse BFS over live in-edges
+//                   (semantics of include/ripples/add_rrrset.h:128-135, with
+//                   the per-edge coin keyed on (set, edge) instead of drawn
+//                   from a sequential trng stream).
+// lt_walk_kernel    one LT set per warp: single-predecessor walk
+//                   (include/ripples/add_rrrset.h:136-150) with no length cap
+//                   and no host fallback (the reference GPU walk stops at 8
+//                   vertices and redoes longer walks on the CPU,
+//                   include/ripples/gpu/lt_kernel.h:59-130,
+//                   streaming_rrr_generator.h:492-520).
+//
+// Both are persistent: each warp pulls set indices from an atomic counter
+// until the range is exhausted.  A warp owns an n-bit visited bitmap and a
+// queue (the set's members in discovery order) in global scratch; at the end
+// of a set it reserves room in the pool with one atomicAdd, copies the queue
+// out and clears exactly the bitmap words it touched.  A set that outgrows
+// the queue, or does not fit in the pool, is recorded in the failure list and
+// the host re-runs it with larger buffers -- the result does not change,
+// because every draw is a pure function of (seed, set id, edge / vertex id).
+#include "device.cuh"
+#include "launch.h"
+
+namespace rip {
+
+namespace {
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+struct WarpCtx {
+  uint32_t *bm;  // visited bitmap, ceil(n/32) words
+  uint32_t *q;   // queue, qcap entries
+  uint32_t qcap;
+};
+
+// Writes the finished set to the pool (or records a failure) and clears the
+// warp's bitmap.  Returns true when the set was stored.
+__device__ bool finish_set(const WarpCtx &W, uint32_t qlen, bool overflow,
+                           uint64_t s, uint32_t rel, const DevPool &P,
+                           const FailList &F) {
+  const uint32_t lane = lane_id();
+  bool stored = false;
+  if (!overflow) {
+    unsigned long long b = 0;
+    if (lane == 0) b = atomicAdd(P.cursor, (unsigned long long)qlen);
+    b = __shfl_sync(FULL, b, 0);
+    if (b + qlen <= P.cap) {
+      for (uint32_t i = lane; i < qlen; i += 32) P.vtx[b + i] = W.q[i];
+      if (lane == 0) {
+        P.set_off[s] = b;
+        P.set_len[s] = qlen;
+      }
+      stored = true;
+    } else if (lane == 0) {
+      atomicMin(F.first_bad_base, b);
+    }
+  }
+  for (uint32_t i = lane; i < qlen; i += 32) W.bm[W.q[i] >> 5] = 0u;
+  if (!stored && lane == 0) F.ids[atomicAdd(F.count, 1u)] = rel;
+  __syncwarp();
+  return stored;
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(256)
+ic_plain_kernel(DevGraph G, DevPool P, Key key, uint64_t first, uint32_t count,
+                const uint32_t *ids, unsigned int *next, uint32_t *bitmaps,
+                uint64_t bm_words, uint32_t *queues, uint32_t qcap,
+                FailList F, Stats st) {
+  const uint32_t lane = lane_id();
+  const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  WarpCtx W{bitmaps + w * bm_words, queues + w * (uint64_t)qcap, qcap};
+  unsigned long long n_exp = 0, n_edges = 0, n_sets = 0, n_elems = 0;
+
+  for (;;) {
+    uint32_t idx = 0;
+    if (lane == 0) idx = atomicAdd(next, 1u);
+    idx = __shfl_sync(FULL, idx, 0);
+    if (idx >= count) break;
+    const uint32_t rel = ids ? ids[idx] : idx;
+    const uint64_t s = first + rel;
+    const uint32_t root = root_of(key, s, G.n);
+    if (lane == 0) {
+      W.q[0] = root;
+      atomicOr(&W.bm[root >> 5], 1u << (root & 31));
+    }
+    __syncwarp();
+    uint32_t qlen = 1, head = 0;
+    bool overflow = false;
+
+    while (head < qlen && !overflow) {
+      const uint32_t take = min(32u, qlen - head);
+      uint32_t beg = 0, end = 0, ng = 0;
+      if (lane < take) {
+        const uint32_t v = W.q[head + lane];
+        beg = __ldg(G.off + v);
+        end = __ldg(G.off + v + 1);
+        ng = group_count(beg, end);
+        n_edges += end - beg;
+      }
+      n_exp += (lane == 0) ? take : 0;
+      const uint32_t incl = warp_incl_scan(ng);
+      const uint32_t total = __shfl_sync(FULL, incl, 31);
+      for (uint32_t base = 0; base < total && !overflow; base += 32) {
+        const uint32_t j = base + lane;
+        const bool valid = j < total;
+        const uint32_t owner = warp_find_owner(incl, valid ? j : total - 1);
+        const uint32_t ob = __shfl_sync(FULL, beg, owner);
+        const uint32_t oe = __shfl_sync(FULL, end, owner);
+        const uint32_t oexcl = __shfl_sync(FULL, incl, owner) -
+                               __shfl_sync(FULL, ng, owner);
+        uint32_t nu[4];
+        bool isnew[4];
+        if (valid) {
+          const uint32_t g = (ob >> 2) + (j - oexcl);
+          uint2 rec[4];
+          load_group(G.edges, g, rec);
+          const u32x4 c = ic_coins(key, g, s);
+#pragma unroll
+          for (int t = 0; t < 4; ++t) {
+            const uint32_t e = (g << 2) + t;
+            const bool live = e >= ob && e < oe && lane_of(c, t) < rec[t].y;
+            isnew[t] = false;
+            nu[t] = rec[t].x;
+            if (live) {
+              const uint32_t bit = 1u << (nu[t] & 31);
+              const uint32_t old = atomicOr(&W.bm[nu[t] >> 5], bit);
+              isnew[t] = !(old & bit);
+            }
+          }
+        } else {
+#pragma unroll
+          for (int t = 0; t < 4; ++t) {
+            isnew[t] = false;
+            nu[t] = 0;
+          }
+        }
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          const uint32_t bal = __ballot_sync(FULL, isnew[t]);
+          if (bal == 0) continue;
+          const uint32_t cnt = __popc(bal);
+          if (overflow || qlen + cnt > W.qcap) {
+            // Abandon the set: clear the bits of vertices that will never
+            // reach the queue (queued ones are cleared by finish_set).
+            if (isnew[t]) W.bm[nu[t] >> 5] = 0u;
+            overflow = true;
+            continue;
+          }
+          if (isnew[t]) W.q[qlen + __popc(bal & lanemask_lt())] = nu[t];
+          qlen += cnt;
+        }
+        __syncwarp();
+      }
+      head += take;
+    }
+    if (finish_set(W, qlen, overflow, s, rel, P, F)) {
+      n_sets += (lane == 0);
+      n_elems += (lane == 0) ? qlen : 0;
+    }
+  }
+  n_exp = warp_sum_u64(n_exp);
+  n_edges = warp_sum_u64(n_edges);
+  n_sets = warp_sum_u64(n_sets);
+  n_elems = warp_sum_u64(n_elems);
+  if (lane == 0) {
+    atomicAdd(st.v + 0, n_exp);
+    atomicAdd(st.v + 1, n_edges);
+    atomicAdd(st.v + 2, n_sets);
+    atomicAdd(st.v + 3, n_elems);
+    atomicAdd(st.v + 4, n_exp);
+    atomicAdd(st.v + 5, n_edges);
+  }
+}
+
+__global__ void __launch_bounds__(256)
+lt_walk_kernel(DevGraph G, DevPool P, Key key, uint64_t first, uint32_t count,
+               const uint32_t *ids, unsigned int *next, uint32_t *bitmaps,
+               uint64_t bm_words, uint32_t *queues, uint32_t qcap, FailList F,
+               Stats st) {
+  const uint32_t lane = lane_id();
+  const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  WarpCtx W{bitmaps + w * bm_words, queues + w * (uint64_t)qcap, qcap};
+  unsigned long long n_exp = 0, n_edges = 0, n_sets = 0, n_elems = 0;
+
+  for (;;) {
+    uint32_t idx = 0;
+    if (lane == 0) idx = atomicAdd(next, 1u);
+    idx = __shfl_sync(FULL, idx, 0);
+    if (idx >= count) break;
+    const uint32_t rel = ids ? ids[idx] : idx;
+    const uint64_t s = first + rel;
+    uint32_t cur = root_of(key, s, G.n);
+    if (lane == 0) {
+      W.q[0] = cur;
+      atomicOr(&W.bm[cur >> 5], 1u << (cur & 31));
+    }
+    __syncwarp();
+    uint32_t qlen = 1;
+    bool overflow = false;
+    for (;;) {
+      n_exp += (lane == 0);
+      const uint32_t t = lt_threshold(key, s, cur);
+      uint32_t lo = __ldg(G.off + cur), hi = __ldg(G.off + cur + 1);
+      if (hi == lo) break;
+      n_edges += (lane == 0);
+      if (__ldg(&G.edges[hi - 1].y) <= t) break;  // total in-weight < threshold
+      // 32-ary search for the first edge whose cumulative threshold exceeds t.
+      while (hi - lo > 32) {
+        const uint32_t stride = (hi - lo + 31) / 32;
+        const uint32_t p = min(lo + (lane + 1) * stride - 1, hi - 1);
+        const bool pred = t < __ldg(&G.edges[p].y);
+        const uint32_t bal = __ballot_sync(FULL, pred);
+        n_edges += (lane == 0) ? 32 : 0;
+        const uint32_t L = __ffs(bal) - 1;
+        const uint32_t nlo = lo + L * stride;
+        hi = min(hi, lo + (L + 1) * stride);
+        lo = nlo;
+      }
+      const uint32_t e = lo + lane;
+      const bool pred = e < hi && t < __ldg(&G.edges[e].y);
+      const uint32_t bal = __ballot_sync(FULL, pred);
+      n_edges += (lane == 0) ? (hi - lo) : 0;
+      const uint32_t jsel = lo + __ffs(bal) - 1;
+      const uint32_t u = __ldg(&G.edges[jsel].x);
+      uint32_t seen = 0;
+      if (lane == 0) {
+        const uint32_t bit = 1u << (u & 31);
+        seen = atomicOr(&W.bm[u >> 5], bit) & bit;
+      }
+      seen = __shfl_sync(FULL, seen, 0);
+      if (seen) break;
+      if (qlen + 1 > W.qcap) {
+        if (lane == 0) W.bm[u >> 5] = 0u;
+        overflow = true;
+        break;
+      }
+      if (lane == 0) W.q[qlen] = u;
+      ++qlen;
+      cur = u;
+    }
+    __syncwarp();
+    if (finish_set(W, qlen, overflow, s, rel, P, F)) {
+      n_sets += (lane == 0);
+      n_elems += (lane == 0) ? qlen : 0;
+    }
+  }
+  n_exp = warp_sum_u64(n_exp);
+  n_edges = warp_sum_u64(n_edges);
+  n_sets = warp_sum_u64(n_sets);
+  n_elems = warp_sum_u64(n_elems);
+  if (lane == 0) {
+    atomicAdd(st.v + 0, n_exp);
+    atomicAdd(st.v + 1, n_edges);
+    atomicAdd(st.v + 2, n_sets);
+    atomicAdd(st.v + 3, n_elems);
+    atomicAdd(st.v + 4, n_exp);
+    atomicAdd(st.v + 5, n_edges);
+  }
+}
+
+void launch_ic_plain(const SampleLaunch &L, cudaStream_t stream) {
+  ic_plain_kernel<<<L.blocks, L.threads, 0, stream>>>(
+      L.G, L.P, L.key, L.first, L.count, L.ids, L.next, L.bitmaps, L.bm_words,
+      L.queues, L.qcap, L.F, L.st);
+}
+
+void launch_lt_walk(const SampleLaunch &L, cudaStream_t stream) {
+  lt_walk_kernel<<<L.blocks, L.threads, 0, stream>>>(
+      L.G, L.P, L.key, L.first, L.count, L.ids, L.next, L.bitmaps, L.bm_words,
+      L.queues, L.qcap, L.F, L.st);
+}
+
+}  // namespace rip

@@ -1,0 +1,313 @@
+// kernels_select.cu -- greedy max-coverage building blocks for sm_100a.
+//
+// count_kernel      vertex-occurrence histogram over sets [0, S)
+//                   (CountOccurrencies, include/ripples/counting.h:65-97;
+//                   reference GPU kernel_count, src/gpu/find_most_influential.cc:56-63)
+//                   with warp-aggregated atomics: __match_any_sync groups
+//                   lanes holding the same vertex and one leader adds the
+//                   group size.
+// inverted_kernel   vertex -> sets index (a CSR transpose of the pool), built
+//                   once per selection so each pick touches only the sets that
+//                   contain the seed, instead of re-scanning the pool
+//                   (update_mask_kernel + count_uncovered_kernel,
+//                   src/gpu/find_most_influential.cc:74-98).
+// cover_kernel      after a pick: marks the seed's still-uncovered sets
+//                   covered and decrements the counts of their members
+//                   (UpdateCounters, include/ripples/counting.h:141-151),
+//                   recording each vertex whose count changed once in a dirty
+//                   list so the host heap can mirror the counts exactly.
+// argmax_kernel     max count, lowest vertex id on ties (thrust::max_element,
+//                   src/gpu/find_most_influential.cc:65-72).
+//
+// All per-set loops use the same warp-level load balancing: a warp takes 32
+// sets, scans their lengths and walks the concatenated elements 32 at a time,
+// each lane finding its set with a 5-step shuffle search.
+#include "device.cuh"
+#include "launch.h"
+
+namespace rip {
+
+namespace {
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+constexpr uint32_t NONE = 0xFFFFFFFFu;
+
+// Iterates the elements of 32 sets per warp.  `set_of(i)` returns the set
+// index for lane i of the current 32-set window (or a value >= limit for
+// none); `fn(set, vertex, valid)` is called by ALL lanes (valid says whether
+// the lane holds an element) so it may use warp collectives.
+template <typename SetOf, typename Fn>
+__device__ __forceinline__ void for_each_element(const DevPool &P,
+                                                 uint64_t window_base,
+                                                 uint64_t limit, SetOf set_of,
+                                                 Fn fn) {
+  const uint32_t lane = lane_id();
+  const uint64_t sidx = window_base + lane;
+  uint64_t s = 0;
+  uint32_t len = 0;
+  uint64_t off = 0;
+  if (sidx < limit) {
+    s = set_of(sidx);
+    if (s != ~0ull) {
+      len = P.set_len[s];
+      off = P.set_off[s];
+    }
+  }
+  const uint32_t incl = warp_incl_scan(len);
+  const uint32_t total = __shfl_sync(FULL, incl, 31);
+  for (uint32_t base = 0; base < total; base += 32) {
+    const uint32_t j = base + lane;
+    const bool valid = j < total;
+    const uint32_t owner = warp_find_owner(incl, valid ? j : total - 1);
+    const uint64_t ooff = __shfl_sync(FULL, off, owner);
+    const uint32_t oexcl =
+        __shfl_sync(FULL, incl, owner) - __shfl_sync(FULL, len, owner);
+    const uint64_t os = __shfl_sync(FULL, s, owner);
+    const uint32_t v = valid ? P.vtx[ooff + (j - oexcl)] : NONE;
+    fn(os, v, valid);
+  }
+}
+
+__global__ void __launch_bounds__(256)
+count_kernel(DevPool P, uint64_t S, uint32_t *count) {
+  const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t wb = gw * 32; wb < S; wb += nw * 32) {
+    for_each_element(
+        P, wb, S, [](uint64_t i) { return i; },
+        [&](uint64_t, uint32_t v, bool valid) {
+          const uint32_t peers = __match_any_sync(FULL, v);
+          if (valid && (__ffs(peers) - 1) == (int)lane_id())
+            atomicAdd(count + v, (uint32_t)__popc(peers));
+        });
+  }
+}
+
+__global__ void __launch_bounds__(256)
+inverted_kernel(DevPool P, uint64_t S, uint64_t *cursor, uint32_t *inv) {
+  const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t wb = gw * 32; wb < S; wb += nw * 32) {
+    for_each_element(
+        P, wb, S, [](uint64_t i) { return i; },
+        [&](uint64_t s, uint32_t v, bool valid) {
+          const uint32_t peers = __match_any_sync(FULL, v);
+          const uint32_t leader = __ffs(peers) - 1;
+          unsigned long long b = 0;
+          if (valid && leader == lane_id())
+            b = atomicAdd((unsigned long long *)cursor + v,
+                          (unsigned long long)__popc(peers));
+          b = __shfl_sync(FULL, b, leader);
+          if (valid) inv[b + __popc(peers & lanemask_lt())] = (uint32_t)s;
+        });
+  }
+}
+
+__global__ void __launch_bounds__(256) cover_kernel(CoverLaunch C) {
+  const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const uint64_t lo = C.inv_off[C.vertex], hi = C.inv_off[C.vertex + 1];
+  const uint64_t cnt = hi - lo;
+  unsigned long long newly = 0;
+  for (uint64_t wb = gw * 32; wb < cnt; wb += nw * 32) {
+    for_each_element(
+        C.P, wb, cnt,
+        [&](uint64_t i) -> uint64_t {
+          const uint32_t s = C.inv[lo + i];
+          if (C.covered[s]) return ~0ull;  // already covered by an earlier seed
+          C.covered[s] = 1;                // s holds the vertex once: no race
+          ++newly;
+          return s;
+        },
+        [&](uint64_t, uint32_t u, bool valid) {
+          const uint32_t peers = __match_any_sync(FULL, u);
+          const bool leader = valid && (__ffs(peers) - 1) == (int)lane_id();
+          bool fresh = false;
+          if (leader) {
+            atomicSub(C.count + u, (uint32_t)__popc(peers));
+            const uint32_t bit = 1u << (u & 31);
+            fresh = !(atomicOr(C.dirty_bits + (u >> 5), bit) & bit);
+          }
+          const uint32_t bal = __ballot_sync(FULL, fresh);
+          if (bal) {
+            unsigned int b = 0;
+            if (lane_id() == (uint32_t)(__ffs(bal) - 1))
+              b = atomicAdd(C.dirty_n, (unsigned int)__popc(bal));
+            b = __shfl_sync(FULL, b, __ffs(bal) - 1);
+            if (fresh) C.dirty_list[b + __popc(bal & lanemask_lt())] = u;
+          }
+        });
+  }
+  newly = warp_sum_u64(newly);
+  if (lane_id() == 0 && newly) atomicAdd(C.covered_sets, newly);
+}
+
+__global__ void gather_dirty_kernel(const uint32_t *list, const unsigned int *n,
+                                    uint32_t max_n, const uint32_t *count,
+                                    uint32_t *bits, uint2 *pairs) {
+  const uint32_t total = min(*n, max_n);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += gridDim.x * blockDim.x) {
+    const uint32_t u = list[i];
+    pairs[i] = make_uint2(u, count[u]);
+    bits[u >> 5] = 0u;  // every set bit of this word is in the list too
+  }
+}
+
+__global__ void argmax_kernel(const uint32_t *count, uint32_t n,
+                              unsigned long long *best) {
+  unsigned long long key = 0;
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n;
+       v += gridDim.x * blockDim.x) {
+    const unsigned long long k =
+        ((unsigned long long)count[v] << 32) | (unsigned long long)(~v);
+    key = k > key ? k : key;
+  }
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) {
+    const unsigned long long o = __shfl_xor_sync(FULL, key, d);
+    key = o > key ? o : key;
+  }
+  if (lane_id() == 0 && key) atomicMax(best, key);
+}
+
+// ---- exclusive scan of u32 counts into u64 offsets (n+1 outputs) ----------
+constexpr int SCAN_THREADS = 1024;
+constexpr int SCAN_ITEMS = 4;
+constexpr uint32_t SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+
+__device__ unsigned long long block_excl_scan(unsigned long long x,
+                                              unsigned long long *warp_tot,
+                                              unsigned long long *total) {
+  const uint32_t lane = lane_id(), wid = threadIdx.x >> 5;
+  unsigned long long incl = x;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const unsigned long long y = __shfl_up_sync(FULL, incl, d);
+    if (lane >= (uint32_t)d) incl += y;
+  }
+  if (lane == 31) warp_tot[wid] = incl;
+  __syncthreads();
+  if (wid == 0) {
+    unsigned long long t = lane < (blockDim.x >> 5) ? warp_tot[lane] : 0;
+    unsigned long long ti = t;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const unsigned long long y = __shfl_up_sync(FULL, ti, d);
+      if (lane >= (uint32_t)d) ti += y;
+    }
+    warp_tot[lane] = ti - t;
+    if (lane == 31) *total = ti;
+  }
+  __syncthreads();
+  const unsigned long long r = warp_tot[wid] + incl - x;
+  __syncthreads();
+  return r;
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS)
+scan_tiles_kernel(const uint32_t *in, uint32_t n, uint64_t *tile_sums) {
+  __shared__ unsigned long long wt[32];
+  __shared__ unsigned long long tot;
+  const uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
+  unsigned long long s = 0;
+#pragma unroll
+  for (int i = 0; i < SCAN_ITEMS; ++i)
+    if (base + i < n) s += in[base + i];
+  block_excl_scan(s, wt, &tot);
+  if (threadIdx.x == 0) tile_sums[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS)
+scan_sums_kernel(uint64_t *tile_sums, uint32_t tiles) {
+  __shared__ unsigned long long wt[32];
+  __shared__ unsigned long long tot;
+  unsigned long long carry = 0;
+  for (uint32_t b = 0; b < tiles; b += SCAN_THREADS) {
+    const uint32_t i = b + threadIdx.x;
+    const unsigned long long x = i < tiles ? tile_sums[i] : 0;
+    const unsigned long long ex = block_excl_scan(x, wt, &tot);
+    if (i < tiles) tile_sums[i] = carry + ex;
+    carry += tot;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) tile_sums[tiles] = carry;
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS)
+scan_apply_kernel(const uint32_t *in, uint32_t n, const uint64_t *tile_sums,
+                  uint64_t *out) {
+  __shared__ unsigned long long wt[32];
+  __shared__ unsigned long long tot;
+  const uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
+  uint32_t v[SCAN_ITEMS];
+  unsigned long long s = 0;
+#pragma unroll
+  for (int i = 0; i < SCAN_ITEMS; ++i) {
+    v[i] = base + i < n ? in[base + i] : 0u;
+    s += v[i];
+  }
+  unsigned long long ex = block_excl_scan(s, wt, &tot) + tile_sums[blockIdx.x];
+#pragma unroll
+  for (int i = 0; i < SCAN_ITEMS; ++i) {
+    if (base + i < n) out[base + i] = ex;
+    ex += v[i];
+  }
+  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) {
+    const uint32_t tiles = gridDim.x;
+    out[n] = tile_sums[tiles];
+  }
+}
+
+}  // namespace
+
+void launch_count(const DevPool &P, uint64_t num_sets, uint32_t *count,
+                  int blocks, cudaStream_t stream) {
+  count_kernel<<<blocks, 256, 0, stream>>>(P, num_sets, count);
+}
+
+size_t scan_block_sums_needed(uint32_t n) {
+  return (size_t)((uint64_t)n + SCAN_TILE - 1) / SCAN_TILE + 1;
+}
+
+void launch_exclusive_scan(const uint32_t *in, uint64_t *out, uint32_t n,
+                           uint64_t *block_sums, cudaStream_t stream) {
+  const uint32_t tiles = (uint32_t)((n + (uint64_t)SCAN_TILE - 1) / SCAN_TILE);
+  if (tiles == 0) {
+    cudaMemsetAsync(out, 0, sizeof(uint64_t), stream);
+    return;
+  }
+  scan_tiles_kernel<<<tiles, SCAN_THREADS, 0, stream>>>(in, n, block_sums);
+  scan_sums_kernel<<<1, SCAN_THREADS, 0, stream>>>(block_sums, tiles);
+  scan_apply_kernel<<<tiles, SCAN_THREADS, 0, stream>>>(in, n, block_sums, out);
+}
+
+void launch_build_inverted(const DevPool &P, uint64_t num_sets,
+                           uint64_t *cursor, uint32_t *inv, int blocks,
+                           cudaStream_t stream) {
+  inverted_kernel<<<blocks, 256, 0, stream>>>(P, num_sets, cursor, inv);
+}
+
+void launch_cover(const CoverLaunch &C, cudaStream_t stream) {
+  cover_kernel<<<C.blocks, 256, 0, stream>>>(C);
+}
+
+void launch_gather_dirty(const uint32_t *dirty_list, const unsigned int *dirty_n,
+                         uint32_t max_n, const uint32_t *count,
+                         uint32_t *dirty_bits, uint2 *pairs, int blocks,
+                         cudaStream_t stream) {
+  gather_dirty_kernel<<<blocks, 256, 0, stream>>>(dirty_list, dirty_n, max_n,
+                                                  count, dirty_bits, pairs);
+}
+
+void launch_argmax(const uint32_t *count, uint32_t n, unsigned long long *best,
+                   int blocks, cudaStream_t stream) {
+  argmax_kernel<<<blocks, 256, 0, stream>>>(count, n, best);
+}
+
+}  // namespace rip

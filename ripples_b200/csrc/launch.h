@@ -1,0 +1,97 @@
+// launch.h -- host-side launchers of the device kernels (one per .cu file).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "device.cuh"
+
+namespace rip {
+
+struct SampleLaunch {
+  DevGraph G;
+  DevPool P;
+  Key key;
+  uint64_t first;       // set id of the launch's first set (== pool set index)
+  uint32_t count;       // number of set indices to process
+  const uint32_t *ids;  // optional list of indices relative to `first`
+  unsigned int *next;   // work counter (zeroed by the host)
+  uint32_t *bitmaps;
+  uint64_t bm_words;
+  uint32_t *queues;
+  uint32_t qcap;
+  FailList F;
+  Stats st;
+  int blocks, threads;
+};
+
+void launch_ic_plain(const SampleLaunch &L, cudaStream_t stream);
+void launch_lt_walk(const SampleLaunch &L, cudaStream_t stream);
+
+// Fused multi-colour IC BFS: one CTA (slot) per batch of `colors` sets.
+struct FusedLaunch {
+  DevGraph G;
+  DevPool P;
+  Key key;
+  uint64_t first;
+  uint32_t count;        // number of sets
+  const uint32_t *order; // set indices relative to `first`, batch-major (or null)
+  uint32_t num_batches;
+  uint32_t colors;       // 64, 128 or 256
+  unsigned int *next;    // batch counter
+  uint64_t *vis;         // per slot: n * (colors/64) words, all-zero between batches
+  uint64_t *pend;        // per slot: n * (colors/64) words, all-zero between batches
+  uint32_t *pflag;       // per slot: n level flags, all-zero between batches
+  uint32_t *log;         // per slot: lcap frontier-log entries
+  uint32_t lcap;
+  unsigned int *dirty;   // slots abandoned with scratch left dirty
+  FailList F;            // failed batch indices
+  Stats st;
+  int blocks;            // slots
+};
+void launch_ic_fused(const FusedLaunch &L, cudaStream_t stream);
+// Resident fused CTAs per SM for a colour width (occupancy API).
+int fused_ctas_per_sm(uint32_t colors);
+
+// Graph packing.
+void launch_pack_ic(const uint64_t *index, const float *w, uint32_t n,
+                    uint64_t m, uint32_t *off, uint2 *edges, const uint32_t *src,
+                    cudaStream_t stream);
+void launch_pack_lt(const uint64_t *index, const float *w, uint32_t n,
+                    uint64_t m, uint32_t *off, uint2 *edges, const uint32_t *src,
+                    cudaStream_t stream);
+
+// Selection.
+void launch_count(const DevPool &P, uint64_t num_sets, uint32_t *count,
+                  int blocks, cudaStream_t stream);
+void launch_exclusive_scan(const uint32_t *in, uint64_t *out, uint32_t n,
+                           uint64_t *block_sums, cudaStream_t stream);
+size_t scan_block_sums_needed(uint32_t n);
+void launch_build_inverted(const DevPool &P, uint64_t num_sets,
+                           uint64_t *cursor, uint32_t *inv, int blocks,
+                           cudaStream_t stream);
+struct CoverLaunch {
+  DevPool P;
+  const uint64_t *inv_off;
+  const uint32_t *inv;
+  uint32_t vertex;
+  uint8_t *covered;
+  uint32_t *count;
+  uint32_t *dirty_bits;   // n bits
+  uint32_t *dirty_list;   // n entries
+  unsigned int *dirty_n;
+  unsigned long long *covered_sets;  // running total of newly covered sets
+  int blocks;
+};
+void launch_cover(const CoverLaunch &C, cudaStream_t stream);
+void launch_gather_dirty(const uint32_t *dirty_list, const unsigned int *dirty_n,
+                         uint32_t max_n, const uint32_t *count,
+                         uint32_t *dirty_bits, uint2 *pairs, int blocks,
+                         cudaStream_t stream);
+void launch_argmax(const uint32_t *count, uint32_t n, unsigned long long *best,
+                   int blocks, cudaStream_t stream);
+
+// Copies sets [first, first+count) into out[csr[i] ..] in set-id order.
+void launch_gather_sets(const DevPool &P, uint64_t first, uint64_t count,
+                        const uint64_t *csr, uint32_t *out, cudaStream_t s);
+
+}  // namespace rip

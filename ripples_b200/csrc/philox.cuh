@@ -1,0 +1,113 @@
+// philox.cuh -- counter-based random draws of the sampler (host + device).
+//
+// Philox4x32-10 as published by Salmon, Moraes, Dror and Shaw, "Parallel
+// random numbers: as easy as 1, 2, 3" (SC'11): 10 rounds of two 32x32->64
+// multiplies (constants 0xD2511F53, 0xCD9E8D57) with a Weyl key schedule
+// (0x9E3779B9, 0xBB67AE85).
+//
+// Every random decision of the sampler is a pure function of
+// (seed, set id, edge id / vertex id), which is what lets the fused
+// multi-colour BFS, the one-set-per-warp BFS and the CPU oracle produce
+// bit-identical RRR sets whatever order they visit edges in.
+//   key                = (seed_lo, seed_hi)
+//   root(s)            = mulhi64(P(s_lo, 0, 0, ROOT<<24 | s_hi)[0..1], n)
+//   coin(s, e)         = P(g_lo, g_hi, s_lo, IC<<24 | s_hi)[e & 3],  g = e >> 2
+//   lt_threshold(s, v) = P(v, 0, s_lo, LT<<24 | s_hi)[0]
+// (s_hi = bits 32..55 of the set id; set ids are limited to 2^56.)
+#pragma once
+#include <stdint.h>
+
+#ifdef __CUDACC__
+#define RIP_HD __host__ __device__ __forceinline__
+#else
+#define RIP_HD inline
+#endif
+
+namespace rip {
+
+enum : uint32_t { DOM_ROOT = 1, DOM_IC = 2, DOM_LT = 3 };
+
+RIP_HD void mulhilo32(uint32_t a, uint32_t b, uint32_t &hi, uint32_t &lo) {
+#if defined(__CUDA_ARCH__)
+  hi = __umulhi(a, b);
+  lo = a * b;
+#else
+  uint64_t p = (uint64_t)a * (uint64_t)b;
+  hi = (uint32_t)(p >> 32);
+  lo = (uint32_t)p;
+#endif
+}
+
+struct u32x4 {
+  uint32_t x, y, z, w;
+};
+
+RIP_HD u32x4 philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
+                    uint32_t k0, uint32_t k1) {
+#if defined(__CUDA_ARCH__)
+#pragma unroll
+#endif
+  for (int r = 0; r < 10; ++r) {
+    if (r > 0) {
+      k0 += 0x9E3779B9u;
+      k1 += 0xBB67AE85u;
+    }
+    uint32_t hi0, lo0, hi1, lo1;
+    mulhilo32(0xD2511F53u, c0, hi0, lo0);
+    mulhilo32(0xCD9E8D57u, c2, hi1, lo1);
+    uint32_t n0 = hi1 ^ c1 ^ k0;
+    uint32_t n2 = hi0 ^ c3 ^ k1;
+    c0 = n0;
+    c1 = lo1;
+    c2 = n2;
+    c3 = lo0;
+  }
+  return u32x4{c0, c1, c2, c3};
+}
+
+RIP_HD void philox4x32_10(const uint32_t ctr[4], const uint32_t key[2],
+                          uint32_t out[4]) {
+  u32x4 r = philox(ctr[0], ctr[1], ctr[2], ctr[3], key[0], key[1]);
+  out[0] = r.x;
+  out[1] = r.y;
+  out[2] = r.z;
+  out[3] = r.w;
+}
+
+struct Key {
+  uint32_t k0, k1;
+};
+
+RIP_HD Key make_key(uint64_t seed) {
+  return Key{(uint32_t)seed, (uint32_t)(seed >> 32)};
+}
+
+RIP_HD uint32_t set_hi(uint64_t s, uint32_t dom) {
+  return (dom << 24) | (uint32_t)((s >> 32) & 0xFFFFFFu);
+}
+
+RIP_HD uint32_t root_of(Key k, uint64_t s, uint32_t n) {
+  u32x4 r = philox((uint32_t)s, 0u, 0u, set_hi(s, DOM_ROOT), k.k0, k.k1);
+  uint64_t u = (uint64_t)r.x | ((uint64_t)r.y << 32);
+#if defined(__CUDA_ARCH__)
+  return (uint32_t)__umul64hi(u, (uint64_t)n);
+#else
+  return (uint32_t)(((unsigned __int128)u * n) >> 64);
+#endif
+}
+
+// Coins for the 4 edges 4g .. 4g+3 of set s.
+RIP_HD u32x4 ic_coins(Key k, uint64_t g, uint64_t s) {
+  return philox((uint32_t)g, (uint32_t)(g >> 32), (uint32_t)s,
+                set_hi(s, DOM_IC), k.k0, k.k1);
+}
+
+RIP_HD uint32_t lt_threshold(Key k, uint64_t s, uint32_t v) {
+  return philox(v, 0u, (uint32_t)s, set_hi(s, DOM_LT), k.k0, k.k1).x;
+}
+
+RIP_HD uint32_t lane_of(const u32x4 &r, uint32_t i) {
+  return i == 0 ? r.x : i == 1 ? r.y : i == 2 ? r.z : r.w;
+}
+
+}  // namespace rip

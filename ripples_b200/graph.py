@@ -1,0 +1,279 @@
+"""Graphs on the host and on the device.
+
+:class:`HostGraph` holds a backward CSR exactly as the reference's ``GraphBwd``
+(include/ripples/graph.h:364-1086): ``index`` u64[n+1], ``src`` u32[m] (the
+in-neighbours of v are ``src[index[v]:index[v+1]]``), ``weights`` f32[m].
+Synthetic graphs (R-MAT, Erdos-Renyi) and weight models are produced by the
+native library's host code, deterministically in their seeds.
+:class:`Context`, :class:`DeviceGraph` and :class:`Pool` wrap the C ABI
+objects ``rip_ctx``, ``rip_graph`` and ``rip_pool``.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from typing import Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, lib
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else ctypes.c_void_p(a.ctypes.data)
+
+
+@dataclass
+class HostGraph:
+    n: int
+    index: np.ndarray  # uint64[n+1]
+    src: np.ndarray  # uint32[m]
+    weights: Optional[np.ndarray] = None  # float32[m]
+
+    @property
+    def m(self) -> int:
+        return int(self.src.shape[0])
+
+    def in_degree(self) -> np.ndarray:
+        return np.diff(self.index).astype(np.uint64)
+
+    # ---- construction -------------------------------------------------
+    @staticmethod
+    def _from_native(n: int, pidx, psrc, m: int) -> "HostGraph":
+        idx = np.ctypeslib.as_array(ctypes.cast(pidx, ctypes.POINTER(ctypes.c_uint64)),
+                                    shape=(n + 1,)).copy()
+        if m:
+            src = np.ctypeslib.as_array(ctypes.cast(psrc, ctypes.POINTER(ctypes.c_uint32)),
+                                        shape=(m,)).copy()
+        else:
+            src = np.zeros(0, dtype=np.uint32)
+        lib.rip_free(pidx)
+        lib.rip_free(psrc)
+        return HostGraph(n, idx, src)
+
+    @classmethod
+    def rmat(cls, scale: int, num_edges: int, a: float = 0.57, b: float = 0.19,
+             c: float = 0.19, seed: int = 0) -> "HostGraph":
+        """Directed R-MAT graph on 2^scale vertices from ``num_edges`` draws
+        (self-loops and duplicates removed)."""
+        pidx, psrc, m = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_uint64()
+        check(lib.rip_rmat_csr(scale, num_edges, a, b, c, seed, ctypes.byref(pidx),
+                               ctypes.byref(psrc), ctypes.byref(m)), "rip_rmat_csr")
+        return cls._from_native(1 << scale, pidx, psrc, m.value)
+
+    @classmethod
+    def erdos_renyi(cls, n: int, num_edges: int, seed: int = 0) -> "HostGraph":
+        pidx, psrc, m = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_uint64()
+        check(lib.rip_er_csr(n, num_edges, seed, ctypes.byref(pidx), ctypes.byref(psrc),
+                             ctypes.byref(m)), "rip_er_csr")
+        return cls._from_native(n, pidx, psrc, m.value)
+
+    @classmethod
+    def from_edges(cls, n: int, src: Sequence[int], dst: Sequence[int],
+                   weights: Optional[Sequence[float]] = None) -> "HostGraph":
+        """Backward CSR from a directed edge list (src -> dst); in-edges of
+        each vertex ordered by source id.  Duplicates are kept."""
+        s = np.asarray(src, dtype=np.uint64)
+        d = np.asarray(dst, dtype=np.uint64)
+        order = np.lexsort((s, d))
+        s, d = s[order], d[order]
+        idx = np.zeros(n + 1, dtype=np.uint64)
+        np.add.at(idx, d.astype(np.int64) + 1, 1)
+        idx = np.cumsum(idx).astype(np.uint64)
+        w = None
+        if weights is not None:
+            w = np.asarray(weights, dtype=np.float32)[order]
+        return cls(n, idx, s.astype(np.uint32), w)
+
+    def with_weights(self, kind: int, seed: int = 1, lo: float = 0.0,
+                     hi: float = 1.0) -> "HostGraph":
+        w = np.empty(self.m, dtype=np.float32)
+        check(lib.rip_make_weights(kind, self.n, _ptr(self.index), self.m, seed, lo, hi,
+                                   _ptr(w)), "rip_make_weights")
+        return HostGraph(self.n, self.index, self.src, w)
+
+    def write_binary(self, path: str, backward: bool = True) -> None:
+        """Writes the reference binary format (include/ripples/graph.h:700-771)."""
+        assert self.weights is not None
+        check(lib.rip_write_binary(path.encode(), self.n, self.m, _ptr(self.index),
+                                   _ptr(self.src), _ptr(self.weights), 1 if backward else 0),
+              "rip_write_binary")
+
+    def transpose_edges(self) -> Tuple[np.ndarray, np.ndarray]:
+        """(src, dst) arrays of the directed edges, in backward-CSR order."""
+        dst = np.repeat(np.arange(self.n, dtype=np.uint32), np.diff(self.index).astype(np.int64))
+        return self.src.copy(), dst
+
+
+class Context:
+    """One CUDA device + stream (``rip_ctx``)."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 0):
+        h = ctypes.c_void_p()
+        check(lib.rip_ctx_create(device, hbm_budget, ctypes.byref(h)), "rip_ctx_create")
+        self.h = h
+
+    def close(self) -> None:
+        if self.h:
+            lib.rip_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def sync(self) -> None:
+        check(lib.rip_sync(self.h), "rip_sync", self.h)
+
+    def memory(self) -> Tuple[int, int]:
+        used, budget = ctypes.c_size_t(), ctypes.c_size_t()
+        check(lib.rip_ctx_memory(self.h, ctypes.byref(used), ctypes.byref(budget)),
+              "rip_ctx_memory", self.h)
+        return used.value, budget.value
+
+
+MODELS = {"IC": _lib.MODEL_IC, "LT": _lib.MODEL_LT}
+
+
+class DeviceGraph:
+    """A packed backward CSR resident in HBM (``rip_graph``)."""
+
+    def __init__(self, ctx: Context, g: HostGraph, model: str):
+        assert g.weights is not None, "weights required"
+        self.ctx, self.model, self.n, self.m = ctx, model, g.n, g.m
+        h = ctypes.c_void_p()
+        idx = np.ascontiguousarray(g.index, dtype=np.uint64)
+        src = np.ascontiguousarray(g.src, dtype=np.uint32)
+        w = np.ascontiguousarray(g.weights, dtype=np.float32)
+        check(lib.rip_graph_upload(ctx.h, _ptr(idx), _ptr(src), _ptr(w), g.n, g.m,
+                                   MODELS[model], ctypes.byref(h)), "rip_graph_upload", ctx.h)
+        self.h = h
+
+    def thresholds(self) -> np.ndarray:
+        out = np.empty(self.m, dtype=np.uint32)
+        check(lib.rip_graph_thresholds(self.h, _ptr(out)), "rip_graph_thresholds", self.ctx.h)
+        return out
+
+    def close(self) -> None:
+        if self.h:
+            lib.rip_graph_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Pool:
+    """Device-resident flat RRR pool (``rip_pool``)."""
+
+    def __init__(self, graph: DeviceGraph):
+        self.graph, self.ctx = graph, graph.ctx
+        h = ctypes.c_void_p()
+        check(lib.rip_pool_create(self.ctx.h, graph.h, ctypes.byref(h)), "rip_pool_create",
+              self.ctx.h)
+        self.h = h
+
+    def close(self) -> None:
+        if self.h:
+            lib.rip_pool_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _chk(self, rc, where):
+        check(rc, where, self.ctx.h)
+
+    def configure(self, colors: int = 64, slots: int = 0, log_capacity: int = 0) -> None:
+        self._chk(lib.rip_pool_configure(self.h, colors, slots, log_capacity),
+                  "rip_pool_configure")
+
+    def clear(self) -> None:
+        self._chk(lib.rip_pool_clear(self.h), "rip_pool_clear")
+
+    @property
+    def num_sets(self) -> int:
+        s, e = ctypes.c_uint64(), ctypes.c_uint64()
+        self._chk(lib.rip_pool_info(self.h, ctypes.byref(s), ctypes.byref(e)), "rip_pool_info")
+        return s.value
+
+    @property
+    def num_elements(self) -> int:
+        s, e = ctypes.c_uint64(), ctypes.c_uint64()
+        self._chk(lib.rip_pool_info(self.h, ctypes.byref(s), ctypes.byref(e)), "rip_pool_info")
+        return e.value
+
+    def sample(self, count: int, seed: int = 0, sampler: int = _lib.SAMPLER_AUTO) -> None:
+        self._chk(lib.rip_sample(self.h, seed, count, sampler), "rip_sample")
+
+    def export(self, first: int = 0, count: Optional[int] = None) -> Tuple[np.ndarray, np.ndarray]:
+        if count is None:
+            count = self.num_sets - first
+        off = np.zeros(count + 1, dtype=np.uint64)
+        self._chk(lib.rip_pool_export(self.h, first, count, _ptr(off), None), "rip_pool_export")
+        vtx = np.zeros(max(int(off[-1]), 1), dtype=np.uint32)
+        self._chk(lib.rip_pool_export(self.h, first, count, _ptr(off), _ptr(vtx)),
+                  "rip_pool_export")
+        return off, vtx[: int(off[-1])]
+
+    def import_sets(self, offsets: np.ndarray, vertices: np.ndarray) -> None:
+        off = np.ascontiguousarray(offsets, dtype=np.uint64)
+        vtx = np.ascontiguousarray(vertices, dtype=np.uint32)
+        if vtx.size == 0:
+            vtx = np.zeros(1, dtype=np.uint32)
+        self._chk(lib.rip_pool_import(self.h, _ptr(off), _ptr(vtx), len(off) - 1),
+                  "rip_pool_import")
+
+    def stats(self) -> np.ndarray:
+        st = np.zeros(8, dtype=np.uint64)
+        self._chk(lib.rip_pool_stats(self.h, _ptr(st)), "rip_pool_stats")
+        return st
+
+    def timing(self) -> Tuple[float, int, float]:
+        ms, n, sms = ctypes.c_double(), ctypes.c_uint64(), ctypes.c_double()
+        self._chk(lib.rip_pool_timing(self.h, ctypes.byref(ms), ctypes.byref(n),
+                                      ctypes.byref(sms)), "rip_pool_timing")
+        return ms.value, n.value, sms.value
+
+    def count(self, num_sets: Optional[int] = None) -> np.ndarray:
+        if num_sets is None:
+            num_sets = self.num_sets
+        out = np.zeros(self.graph.n, dtype=np.uint32)
+        self._chk(lib.rip_count(self.h, num_sets, _ptr(out)), "rip_count")
+        return out
+
+    def select(self, k: int, num_sets: Optional[int] = None,
+               tiebreak: int = _lib.TIE_REF_HEAP):
+        """Greedy max coverage; returns (f, seeds, gains)."""
+        if num_sets is None:
+            num_sets = self.num_sets
+        seeds = np.zeros(max(k, 1), dtype=np.uint32)
+        gains = np.zeros(max(k, 1), dtype=np.uint64)
+        ns, f = ctypes.c_uint32(), ctypes.c_double()
+        self._chk(lib.rip_select(self.h, num_sets, k, tiebreak, _ptr(seeds), _ptr(gains),
+                                 ctypes.byref(ns), ctypes.byref(f)), "rip_select")
+        return f.value, seeds[: ns.value].copy(), gains[: ns.value].copy()
+
+    def select_counts(self) -> np.ndarray:
+        out = np.zeros(self.graph.n, dtype=np.uint32)
+        self._chk(lib.rip_select_counts(self.h, _ptr(out)), "rip_select_counts")
+        return out
+
+    def imm(self, k: int, epsilon: float, l: float = 1.0, seed: int = 0,
+            tiebreak: int = _lib.TIE_REF_HEAP, sampler: int = _lib.SAMPLER_AUTO):
+        seeds = np.zeros(max(k, 1), dtype=np.uint32)
+        ns = ctypes.c_uint32()
+        rec = _lib.ImmRecord()
+        self._chk(lib.rip_imm_pool(self.h, k, epsilon, l, seed, tiebreak, sampler,
+                                   _ptr(seeds), ctypes.byref(ns), ctypes.byref(rec)),
+                  "rip_imm_pool")
+        return seeds[: ns.value].copy(), rec

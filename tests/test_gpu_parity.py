@@ -1,0 +1,266 @@
+"""Parity of the CUDA path with the oracle and with the reference's golden
+outputs.  Integer work must be bit-exact: sampled sets (vs the CPU
+restatement), seed sequences, gains, coverage and theta (vs the reference's
+FindMostInfluentialSet / IMM math)."""
+import numpy as np
+import pytest
+
+import ripples_b200 as rb
+from conftest import csr_of, karate
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+SAMPLERS = [(rb.SAMPLER_PLAIN, 64), (rb.SAMPLER_FUSED, 64), (rb.SAMPLER_FUSED, 128),
+            (rb.SAMPLER_FUSED, 256)]
+
+
+def ic_graph(scale=12, deg=8, hi=0.3, seed=1):
+    return rb.HostGraph.rmat(scale, deg << scale, seed=seed).with_weights(
+        rb.WEIGHTS_UNIFORM, seed=seed + 100, lo=0.0, hi=hi)
+
+
+def lt_graph(scale=12, deg=8, seed=2):
+    return rb.HostGraph.rmat(scale, deg << scale, seed=seed).with_weights(
+        rb.WEIGHTS_LT_NORMALIZED, seed=seed + 100)
+
+
+def oracle_sets(g, model, seed, first, count):
+    thr = O.pack(model, g.index, g.weights)
+    return O.sample(model, g.n, g.index, g.src, thr, seed, first, count)
+
+
+def device_pool(ctx, g, model, colors=64):
+    dg = rb.DeviceGraph(ctx, g, model)
+    p = rb.Pool(dg)
+    p.configure(colors=colors)
+    return dg, p
+
+
+def assert_same_sets(off_a, vtx_a, off_b, vtx_b):
+    assert np.array_equal(off_a, off_b)
+    assert np.array_equal(vtx_a, vtx_b)
+
+
+def test_thresholds_match_oracle(ctx):
+    for model, g in [("IC", ic_graph(10)), ("LT", lt_graph(10))]:
+        dg = rb.DeviceGraph(ctx, g, model)
+        assert np.array_equal(dg.thresholds(), O.pack(model, g.index, g.weights))
+        dg.close()
+
+
+@pytest.mark.parametrize("sampler,colors", SAMPLERS)
+def test_ic_sets_bit_exact(ctx, sampler, colors):
+    g = ic_graph()
+    dg, p = device_pool(ctx, g, "IC", colors)
+    p.sample(3000, seed=7, sampler=sampler)
+    off, vtx = p.export()
+    ooff, ovtx, ost = oracle_sets(g, "IC", 7, 0, 3000)
+    assert_same_sets(off, vtx, ooff, ovtx)
+    st = p.stats()
+    assert st[2] == 3000 and st[3] == len(vtx)
+    assert st[4] == ost[0]  # per-set expansions = sum of set sizes
+    assert st[5] == ost[1]  # per-set in-edges read
+    if sampler == rb.SAMPLER_PLAIN:
+        assert st[0] == st[4] and st[1] == st[5]
+    else:
+        assert st[0] <= st[4] and st[1] <= st[5]  # fusion never reads more
+
+
+def test_karate_ic_bit_exact(ctx):
+    g = karate(weight=0.5)
+    for sampler, colors in SAMPLERS:
+        dg, p = device_pool(ctx, g, "IC", colors)
+        p.sample(2000, seed=1, sampler=sampler)
+        off, vtx = p.export()
+        ooff, ovtx, _ = oracle_sets(g, "IC", 1, 0, 2000)
+        assert_same_sets(off, vtx, ooff, ovtx)
+
+
+def test_lt_sets_bit_exact(ctx):
+    g = lt_graph()
+    dg, p = device_pool(ctx, g, "LT")
+    p.sample(4000, seed=3)
+    off, vtx = p.export()
+    ooff, ovtx, ost = oracle_sets(g, "LT", 3, 0, 4000)
+    assert_same_sets(off, vtx, ooff, ovtx)
+    assert p.stats()[4] == ost[0]
+
+
+def test_lt_long_walks_retry(ctx):
+    """A chain 0 <- 1 <- ... <- n-1 with weight 1: walks from high roots run
+    past the default per-warp queue, forcing the widen-and-retry path."""
+    n = 40000
+    g = rb.HostGraph.from_edges(n, np.arange(1, n), np.arange(0, n - 1),
+                                np.ones(n - 1, np.float32))
+    dg, p = device_pool(ctx, g, "LT")
+    p.sample(64, seed=5)
+    off, vtx = p.export()
+    ooff, ovtx, _ = oracle_sets(g, "LT", 5, 0, 64)
+    assert_same_sets(off, vtx, ooff, ovtx)
+    assert np.diff(off).max() > 16384
+
+
+def test_ic_giant_sets_retry(ctx):
+    """p = 1 on a strongly connected graph: every set is the whole graph, far
+    above the first pool-size estimate and the default queue."""
+    n = 30000
+    src = np.concatenate([np.arange(n), np.arange(n)])
+    dst = np.concatenate([(np.arange(n) + 1) % n, (np.arange(n) + 7) % n])
+    g = rb.HostGraph.from_edges(n, src, dst, np.ones(2 * n, np.float32))
+    for sampler, colors in [(rb.SAMPLER_PLAIN, 64), (rb.SAMPLER_FUSED, 64)]:
+        dg, p = device_pool(ctx, g, "IC", colors)
+        p.sample(70, seed=2, sampler=sampler)
+        off, vtx = p.export()
+        assert np.all(np.diff(off) == n)
+        ooff, ovtx, _ = oracle_sets(g, "IC", 2, 0, 70)
+        assert_same_sets(off, vtx, ooff, ovtx)
+
+
+def test_fused_log_overflow_falls_back(ctx):
+    g = ic_graph(11, hi=0.5)
+    dg, p = device_pool(ctx, g, "IC", 64)
+    p.configure(colors=64, slots=4, log_capacity=8)
+    p.sample(500, seed=9, sampler=rb.SAMPLER_FUSED)
+    off, vtx = p.export()
+    ooff, ovtx, _ = oracle_sets(g, "IC", 9, 0, 500)
+    assert_same_sets(off, vtx, ooff, ovtx)
+
+
+def test_sets_depend_only_on_set_id(ctx):
+    g = ic_graph(11)
+    dg, p1 = device_pool(ctx, g, "IC")
+    p1.sample(1000, seed=4)
+    p2 = rb.Pool(dg)
+    p2.sample(300, seed=4, sampler=rb.SAMPLER_PLAIN)
+    p2.sample(700, seed=4, sampler=rb.SAMPLER_FUSED)
+    a = p1.export()
+    b = p2.export()
+    assert_same_sets(*a, *b)
+    # a different seed gives different sets
+    p3 = rb.Pool(dg)
+    p3.sample(1000, seed=5)
+    assert not np.array_equal(p3.export()[1][:1000], a[1][:1000])
+
+
+def empty_graph(ctx, n):
+    g = rb.HostGraph(n, np.zeros(n + 1, np.uint64), np.zeros(0, np.uint32),
+                     np.zeros(0, np.float32))
+    return rb.DeviceGraph(ctx, g, "IC")
+
+
+def test_selection_matches_reference_golden(ctx, golden_selection):
+    for i, c in enumerate(golden_selection):
+        dg = empty_graph(ctx, c["n"])
+        p = rb.Pool(dg)
+        p.import_sets(c["off"], c["vtx"])
+        f, seeds, gains = p.select(c["k"], tiebreak=rb.TIE_REF_HEAP)
+        assert seeds.tolist() == c["seeds"].tolist(), f"case {i}"
+        assert f == c["f"], f"case {i}"
+        of, oseeds, ogains, _ = O.select(c["n"], c["off"], c["vtx"], c["k"], 0)
+        assert gains.tolist() == ogains.tolist()
+        p.close()
+        dg.close()
+
+
+def test_counting_known_answers_on_device(ctx, golden_kat):
+    kat = golden_kat
+    off, vtx = csr_of(kat["sets"])
+    dg = empty_graph(ctx, kat["n"])
+    p = rb.Pool(dg)
+    p.import_sets(off, vtx)
+    assert p.count().tolist() == kat["counts"]
+    f, seeds, gains = p.select(2, tiebreak=rb.TIE_LOWEST_ID)
+    assert seeds.tolist() == [2, 1]
+    # counts after covering seed 2 (the last update before k was reached)
+    assert p.select_counts().tolist() == kat["after_seed_2"]
+    f, seeds, gains = p.select(3, tiebreak=rb.TIE_LOWEST_ID)
+    assert seeds.tolist()[:2] == [2, 1]
+    assert p.select_counts().tolist() == kat["after_seed_1"]
+    # heap tie-break on the same sets agrees with the oracle (= reference)
+    f, seeds, gains = p.select(3, tiebreak=rb.TIE_REF_HEAP)
+    of, oseeds, ogains, _ = O.select(kat["n"], off, vtx, 3, 0)
+    assert seeds.tolist() == oseeds.tolist() and gains.tolist() == ogains.tolist()
+
+
+@pytest.mark.parametrize("tiebreak", [rb.TIE_REF_HEAP, rb.TIE_LOWEST_ID])
+def test_selection_on_sampled_pool(ctx, tiebreak):
+    g = ic_graph(12, hi=0.2)
+    dg, p = device_pool(ctx, g, "IC")
+    p.sample(20000, seed=11)
+    off, vtx = p.export()
+    for k, S in [(50, 20000), (20, 7000), (1, 20000)]:
+        f, seeds, gains = p.select(k, num_sets=S, tiebreak=tiebreak)
+        of, oseeds, ogains, _ = O.select(g.n, off[: S + 1], vtx[: int(off[S])], k, tiebreak)
+        assert seeds.tolist() == oseeds.tolist()
+        assert gains.tolist() == ogains.tolist()
+        assert f == of
+
+
+def test_selection_stops_when_all_covered(ctx):
+    dg = empty_graph(ctx, 10)
+    p = rb.Pool(dg)
+    off, vtx = csr_of([[1, 2], [2, 3], [3], [9]])
+    p.import_sets(off, vtx)
+    f, seeds, gains = p.select(8)
+    assert f == 1.0 and len(seeds) == 2 and gains.sum() == 4
+    f, seeds, gains = p.select(0)
+    assert len(seeds) == 0 and f == 0.0
+
+
+@pytest.mark.parametrize("sampler", [rb.SAMPLER_PLAIN, rb.SAMPLER_FUSED])
+def test_imm_ic_matches_oracle(ctx, sampler):
+    # the 2^14-vertex IC configuration: R-MAT 2^14 / 2^18 draws, p ~ U(0, 0.1)
+    g = rb.HostGraph.rmat(14, 1 << 18, seed=0).with_weights(rb.WEIGHTS_UNIFORM, seed=1,
+                                                             lo=0.0, hi=0.1)
+    gen = rb.B200RRRGenerator(g, "IC", seed=0, ctx=ctx, sampler=sampler)
+    CFG = rb.IMMConfiguration(k=20, epsilon=0.5, diffusionModel="IC")
+    rec = rb.IMMExecutionRecord()
+    seeds = rb.IMM(g, CFG, 1.0, gen, rec)
+    thr = O.pack("IC", g.index, g.weights)
+    o = O.imm("IC", g.n, g.index, g.src, thr, 20, 0.5, seed=0)
+    assert seeds == o["seeds"]
+    assert rec.Theta == o["theta"]
+    assert rec.ThetaPrimeDeltas == o["deltas"]
+    assert rec.TotalSets == o["total_sets"]
+
+
+def test_imm_lt_matches_oracle(ctx):
+    g = lt_graph(13, 8, seed=9)
+    gen = rb.B200RRRGenerator(g, "LT", seed=3, ctx=ctx)
+    CFG = rb.IMMConfiguration(k=10, epsilon=0.5, diffusionModel="LT")
+    rec = rb.IMMExecutionRecord()
+    seeds = rb.IMM(g, CFG, 1.0, gen, rec)
+    thr = O.pack("LT", g.index, g.weights)
+    o = O.imm("LT", g.n, g.index, g.src, thr, 10, 0.5, seed=3)
+    assert seeds == o["seeds"] and rec.Theta == o["theta"]
+    assert rec.ThetaPrimeDeltas == o["deltas"]
+
+
+def test_find_most_influential_set_host_lists(ctx, golden_selection):
+    c = golden_selection[-1]
+    sets = [c["vtx"][c["off"][i]:c["off"][i + 1]] for i in range(len(c["off"]) - 1)]
+    G = rb.HostGraph(c["n"], np.zeros(c["n"] + 1, np.uint64), np.zeros(0, np.uint32),
+                     np.zeros(0, np.float32))
+    CFG = rb.IMMConfiguration(k=c["k"])
+    f, seeds = rb.FindMostInfluentialSet(G, CFG, sets, ctx=ctx)
+    assert seeds == c["seeds"].tolist() and f == c["f"]
+
+
+def test_errors_are_reported(ctx):
+    g = ic_graph(8)
+    dg, p = device_pool(ctx, g, "IC")
+    p.sample(10)
+    with pytest.raises(rb.RipError):
+        p.select(5, num_sets=11)
+    with pytest.raises(rb.RipError):
+        p.configure(colors=96)
+    bad = rb.HostGraph(g.n, g.index, g.src.copy(), g.weights)
+    bad.src[0] = g.n + 5
+    with pytest.raises(rb.RipError):
+        rb.DeviceGraph(ctx, bad, "IC")
+    dg2 = empty_graph(ctx, 4)
+    p2 = rb.Pool(dg2)
+    off, vtx = csr_of([[1, 7]])
+    with pytest.raises(rb.RipError):
+        p2.import_sets(off, vtx)

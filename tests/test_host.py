@@ -1,0 +1,137 @@
+"""Host-side product logic (no GPU): the C ABI library loads and exports every
+declared symbol; theta math equals the reference's; graph construction helpers
+are deterministic and write the reference's binary format."""
+import ctypes
+import os
+import re
+import struct
+
+import numpy as np
+import pytest
+
+import ripples_b200 as rb
+from ripples_b200 import _lib
+from conftest import ROOT
+
+
+def header_symbols():
+    txt = open(os.path.join(ROOT, "include", "ripples_b200.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(rip_[a-z0-9_]+)\s*\(", txt)))
+
+
+def test_library_exports_every_declared_symbol():
+    so = ctypes.CDLL(_lib.LIB_PATH)
+    syms = header_symbols()
+    assert len(syms) >= 30
+    missing = [s for s in syms if not hasattr(so, s)]
+    assert not missing, missing
+    # and the Python binding declares a signature for each of them
+    assert set(syms) <= set(_lib.SIGNATURES), set(syms) - set(_lib.SIGNATURES)
+
+
+def test_library_is_sm100a_only():
+    assert "sm_100a" in rb.library_version()
+
+
+def test_theta_math_matches_reference(golden_theta):
+    for r in golden_theta:
+        if r["kind"] == "theta_prime":
+            assert rb.theta_prime(r["x"], r["eps_prime"], r["l"], r["k"], r["n"]) == r["value"]
+        elif r["kind"] == "inv_theta_prime":
+            assert rb.inv_theta_prime(r["x"], r["eps_prime"], r["l"], r["k"], r["n"]) == r["value"]
+        elif r["kind"] == "theta":
+            assert rb.theta(r["eps"], r["l"], r["k"], r["lb"], r["n"]) == r["value"]
+        else:
+            assert rb.log_binomial(r["n"], r["k"]) == r["value"]
+
+
+def test_rmat_deterministic_and_clean():
+    a = rb.HostGraph.rmat(12, 1 << 16, seed=5)
+    b = rb.HostGraph.rmat(12, 1 << 16, seed=5)
+    c = rb.HostGraph.rmat(12, 1 << 16, seed=6)
+    assert np.array_equal(a.index, b.index) and np.array_equal(a.src, b.src)
+    assert not np.array_equal(a.src, c.src)
+    assert a.n == 4096 and a.index[0] == 0 and a.index[-1] == a.m
+    assert 0 < a.m <= 1 << 16
+    dst = np.repeat(np.arange(a.n), np.diff(a.index).astype(np.int64))
+    assert np.all(a.src != dst)  # no self loops
+    key = dst.astype(np.uint64) << np.uint64(32) | a.src.astype(np.uint64)
+    assert np.all(np.diff(key.astype(np.int64)) > 0)  # sorted by (dst, src), no duplicates
+    # R-MAT skew: vertex 0 (all-"a" quadrant) is the heaviest source
+    out_deg = np.bincount(a.src, minlength=a.n)
+    assert out_deg.argmax() == 0
+
+
+def test_erdos_renyi():
+    g = rb.HostGraph.erdos_renyi(1000, 20000, seed=1)
+    assert g.n == 1000 and 19000 < g.m <= 20000
+    deg = np.diff(g.index)
+    assert deg.max() < 60  # no skew
+
+
+def test_weight_models():
+    g = rb.HostGraph.rmat(10, 1 << 14, seed=2)
+    u = g.with_weights(rb.WEIGHTS_UNIFORM, seed=1, lo=0.0, hi=0.1).weights
+    assert u.min() >= 0 and u.max() < 0.1 and abs(u.mean() - 0.05) < 0.005
+    lt = g.with_weights(rb.WEIGHTS_LT_NORMALIZED, seed=1).weights
+    sums = np.add.reduceat(lt.astype(np.float64), g.index[:-1].astype(np.int64)[np.diff(g.index) > 0])
+    assert np.allclose(sums, 1.0, atol=1e-5)
+    wc = g.with_weights(rb.WEIGHTS_WC).weights
+    deg = np.diff(g.index).astype(np.int64)
+    assert np.allclose(wc, np.repeat(1.0 / np.maximum(deg, 1), deg).astype(np.float32))
+
+
+def test_binary_format_layout(tmp_path):
+    g = rb.HostGraph.rmat(8, 2000, seed=3).with_weights(rb.WEIGHTS_UNIFORM, seed=1, lo=0, hi=1)
+    p = str(tmp_path / "g.bin")
+    g.write_binary(p, backward=True)
+    raw = open(p, "rb").read()
+    hdr = struct.unpack("<5Q", raw[:40])
+    assert hdr == (0xC0FFEE, 0xA1CCAC0F, 32, g.n, g.m)
+    off = 40
+    rmap = np.frombuffer(raw, np.uint32, g.n, off); off += 4 * g.n
+    idx = np.frombuffer(raw, np.uint64, g.n + 1, off); off += 8 * (g.n + 1)
+    src = np.frombuffer(raw, np.uint32, g.m, off); off += 4 * g.m
+    w = np.frombuffer(raw, np.float32, g.m, off); off += 4 * g.m
+    assert off == len(raw)
+    assert np.array_equal(rmap, np.arange(g.n)) and np.array_equal(idx, g.index)
+    assert np.array_equal(src, g.src) and np.array_equal(w, g.weights)
+    pf = str(tmp_path / "f.bin")
+    g.write_binary(pf, backward=False)
+    hdr = struct.unpack("<5Q", open(pf, "rb").read()[:40])
+    assert hdr[1] == 0xF0CACC1A
+
+
+def test_binary_loads_in_reference(tmp_path):
+    from oracle import oracle as O
+    R = O.reference()
+    if R is None:
+        pytest.skip("oracle/_ref not built")
+    g = rb.HostGraph.rmat(9, 4000, seed=4).with_weights(rb.WEIGHTS_UNIFORM, seed=1, lo=0, hi=1)
+    p = str(tmp_path / "g.bin")
+    g.write_binary(p)
+    h = R.ref_graph_load(p.encode())
+    assert R.ref_graph_nodes(h) == g.n and R.ref_graph_edges(h) == g.m
+    R.ref_graph_free(h)
+
+
+def test_context_fails_loudly_without_gpu():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(rb.RipError):
+        rb.Context(0)
+
+
+def test_json_log_keys():
+    CFG = rb.IMMConfiguration(k=5, epsilon=0.5, diffusionModel="IC")
+    rec = rb.IMMExecutionRecord(Theta=10, ThetaPrimeDeltas=[3])
+    e = rec.experiment(CFG, [1, 2])
+    for key in ["Algorithm", "Input", "Output", "DiffusionModel", "Epsilon", "K", "L",
+                "NumThreads", "NumWalkWorkers", "NumCPUTeams", "NumGPUWalkWorkers",
+                "PauseThreshold", "Total", "ThetaPrimeDeltas", "ThetaEstimation",
+                "ThetaEstimationGenerateRRR", "ThetaEstimationMostInfluential", "Theta",
+                "Counting", "Pivoting", "Microbenchmarking", "CPUBatchSize", "GPUBatchSize",
+                "RRRSetSizeBytes", "GenerateRRRSets", "FindMostInfluentialSet", "Seeds"]:
+        assert key in e
