@@ -1,0 +1,397 @@
+"""Benchmark: RRR sets/s of full IMM runs on one or more B200s.
+
+Default workload (N=1): plain IMM under the LT model on a directed R-MAT graph
+with 2^20 vertices and 16*2^20 edge draws (a,b,c,d = .57,.19,.19,.05, seed 0,
+self-loops and duplicates removed), in-weights U(0,1) normalised per
+destination, k=50, epsilon=0.3.  Other workloads: --workload ic14 (R-MAT 2^14,
+2^18 draws, IC p ~ U(0,0.1), k=20, eps=0.5).
+
+One step = one complete IMM (martingale theta estimation + final sampling +
+final greedy selection) from an empty RRR pool, with a fresh sampler seed each
+step, the graph already resident in HBM.  value = RRR sets generated per
+second, summed over ranks, over the max-over-ranks device time of the K timed
+steps.  e2e = the same metric through the public API with the graph uploaded
+from pinned host memory and the seeds read back every step.
+
+Multi-GPU: the path does not shard across GPUs in this build ("replicas
+only"): each rank runs its own independent IMM query (its own seeds), and
+`value` aggregates the ranks' sets -- weak scaling, no collective on the data
+path.
+
+--impl reference runs the reference's own CPU imm (built from its sources into
+oracle/_ref/ by oracle/ref.mk) on the same graph, written in the reference's
+binary format, on rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "lt20": dict(name="imm_lt_rmat20_deg16_k50_eps0.3", scale=20, draws=16 << 20, model="LT",
+                 k=50, eps=0.3, weights="lt_normalized"),
+    "ic14": dict(name="imm_ic_rmat14_2^18_k20_eps0.5", scale=14, draws=1 << 18, model="IC",
+                 k=20, eps=0.5, weights="uniform_0_0.1"),
+}
+METRIC = "RRR sets/s (full IMM)"
+
+
+def build_graph(w):
+    import ripples_b200 as rb
+    g = rb.HostGraph.rmat(w["scale"], w["draws"], 0.57, 0.19, 0.19, seed=0)
+    if w["weights"] == "lt_normalized":
+        return g.with_weights(rb.WEIGHTS_LT_NORMALIZED, seed=1)
+    if w["weights"] == "wc":
+        return g.with_weights(rb.WEIGHTS_WC)
+    return g.with_weights(rb.WEIGHTS_UNIFORM, seed=1, lo=0.0, hi=0.1)
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            d = json.load(fh)
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device, self.rows, self.proc = device, [], None
+
+    def start(self):
+        if not shutil.which("nvidia-smi"):
+            return
+        self.proc = subprocess.Popen(
+            ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+             "--format=csv,noheader,nounits", "-lms", "200"],
+            stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        self.t = threading.Thread(target=self._read, daemon=True)
+        self.t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4)
+                          if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        backend = "nccl"
+        dist.init_process_group(backend, timeout=timedelta(seconds=300))
+    return world, rank, local
+
+
+def allreduce_max(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def allreduce_sum(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def run_reference_imm(bin_path, w, threads, parallel, timeout_s):
+    """One run of the reference imm tool; returns (sets, total_ms, record)."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "imm")
+    out = tempfile.mktemp(suffix=".json")
+    cmd = [exe, "-i", bin_path, "--reload-binary", "-d", w["model"], "-k", str(w["k"]),
+           "-e", str(w["eps"]), "-o", out]
+    if parallel:
+        cmd.append("-p")
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+    subprocess.run(cmd, env=env, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL,
+                   timeout=timeout_s, check=True)
+    with open(out) as fh:
+        rec = json.load(fh)[0]
+    os.unlink(out)
+    sets = max(int(rec["Theta"]), int(sum(rec["ThetaPrimeDeltas"])))
+    return sets, float(rec["Total"]), rec
+
+
+def reference_arm(args, w, world, rank):
+    if rank != 0:
+        return 0
+    exe = os.path.join(ROOT, "oracle", "_ref", "imm")
+    if not os.path.exists(exe):
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref/imm not built (make -f oracle/ref.mk needs the "
+                          "reference sources)"}))
+        return 0
+    g = build_graph(w)
+    tmp = tempfile.mkdtemp()
+    path = os.path.join(tmp, "graph.bin")
+    g.write_binary(path, backward=True)
+    cores = os.cpu_count() or 1
+    # The reference's LT sampler is only correct on its sequential path: the
+    # parallel CPU workers run IC coin flips whatever the model
+    # (include/ripples/batched_add_rrrset.h:231-245).  IC runs use all cores.
+    parallel = w["model"] == "IC"
+    threads = cores if parallel else 1
+    for _ in range(args.warmup):
+        run_reference_imm(path, w, threads, parallel, 600)
+    tot_sets, tot_ms = 0, 0.0
+    for _ in range(args.steps):
+        s, ms, rec = run_reference_imm(path, w, threads, parallel, 600)
+        tot_sets += s
+        tot_ms += ms
+    value = tot_sets / (tot_ms / 1e3)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "sets/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic R-MAT (seed 0), written in the reference binary format",
+            "config": {"workload": w["name"], "model": w["model"], "k": w["k"],
+                       "epsilon": w["eps"], "n": g.n, "m": g.m,
+                       "reference_path": "imm -p" if parallel else "imm (sequential)"},
+            "cpu_baseline": {"value": value, "unit": "sets/s", "cores": threads,
+                             "kind": "reference",
+                             "sample": f"{args.steps} full IMM runs of the workload"},
+            "e2e": {"value": value, "unit": "sets/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    shutil.rmtree(tmp, ignore_errors=True)
+    return 0
+
+
+def cpu_baseline(w, g, budget_s=30.0):
+    """The reference's own CPU imm on this box's host cores (one IMM run)."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "imm")
+    if not os.path.exists(exe):
+        return None
+    tmp = tempfile.mkdtemp()
+    path = os.path.join(tmp, "graph.bin")
+    g.write_binary(path, backward=True)
+    parallel = w["model"] == "IC"
+    threads = (os.cpu_count() or 1) if parallel else 1
+    try:
+        s, ms, rec = run_reference_imm(path, w, threads, parallel, max(60, budget_s * 4))
+    except (subprocess.TimeoutExpired, subprocess.CalledProcessError) as e:
+        return {"value": None, "unit": "sets/s", "cores": threads, "kind": "reference",
+                "sample": f"failed: {type(e).__name__}"}
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    return {"value": s / (ms / 1e3), "unit": "sets/s", "cores": threads, "kind": "reference",
+            "sample": f"one full IMM run ({s} sets, {ms:.0f} ms) with the reference's "
+                      f"{'parallel' if parallel else 'sequential'} imm built from its sources"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="lt20", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    w = WORKLOADS[args.workload]
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        rc = reference_arm(args, w, world, rank)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return rc
+
+    import numpy as np
+    import torch
+    import ripples_b200 as rb
+    import ctypes
+
+    torch.cuda.set_device(local)
+    g = build_graph(w)
+    ctx = rb.Context(local)
+    sp = ctypes.c_void_p()
+    rb._lib.check(rb._lib.lib.rip_ctx_stream(ctx.h, ctypes.byref(sp)), "rip_ctx_stream")
+    stream = torch.cuda.ExternalStream(sp.value, device=torch.device("cuda", local))
+    dg = rb.DeviceGraph(ctx, g, w["model"])
+    pool = rb.Pool(dg)
+    seed_base = 1000003 * (rank + 1)
+
+    def one_step(step):
+        pool.clear()
+        seeds, rec = pool.imm(w["k"], w["eps"], 1.0, seed=seed_base + step)
+        return rec
+
+    for i in range(args.warmup):
+        one_step(-1 - i)
+    # ---- timed region (device events on the library's stream) --------------
+    pool.clear()
+    st0 = pool.stats()
+    launches0 = rb._lib.lib.rip_kernel_launches()
+    clocks = ClockSampler(local)
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    total_sets, kern_ms, kern_n, st_tot = 0, 0.0, 0, np.zeros(8, np.uint64)
+    thetas = []
+    for step in range(args.steps):
+        pool.clear()
+        seeds, rec = pool.imm(w["k"], w["eps"], 1.0, seed=seed_base + step)
+        total_sets += rec.total_sets
+        thetas.append(int(rec.theta))
+        km, kn, _ = pool.timing()
+        kern_ms += km
+        kern_n += kn
+        st_tot += pool.stats()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    launches = int(rb._lib.lib.rip_kernel_launches() - launches0)
+    elapsed_ms = ev0.elapsed_time(ev1)
+    t_max = allreduce_max(elapsed_ms, world)
+    sets_all = allreduce_sum(total_sets, world)
+    value = sets_all / (t_max / 1e3)
+
+    # ---- e2e through the public API: host graph -> device -> seeds ---------
+    pin_idx = torch.from_numpy(g.index).pin_memory()
+    pin_src = torch.from_numpy(g.src).pin_memory()
+    pin_w = torch.from_numpy(g.weights).pin_memory()
+    h2d = pin_idx.numel() * 8 + pin_src.numel() * 4 + pin_w.numel() * 4
+    d2h = 4 * w["k"]
+
+    def e2e_step(step):
+        gen_g = rb.HostGraph(g.n, pin_idx.numpy(), pin_src.numpy(), pin_w.numpy())
+        gen = rb.B200RRRGenerator(gen_g, w["model"], seed=seed_base + 7919 + step, ctx=ctx)
+        CFG = rb.IMMConfiguration(k=w["k"], epsilon=w["eps"], diffusionModel=w["model"])
+        rec = rb.IMMExecutionRecord()
+        seeds = rb.IMM(gen_g, CFG, 1.0, gen, rec)
+        n_sets = rec.TotalSets
+        gen.pool.close()
+        gen.graph.close()
+        return n_sets, seeds
+
+    e2e_steps = max(1, min(args.steps, 3))
+    e2e_step(-1)
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e2e_sets = 0
+    for step in range(e2e_steps):
+        s, _ = e2e_step(step)
+        e2e_sets += s
+    torch.cuda.synchronize()
+    e2e_ms = (time.perf_counter() - t0) * 1e3
+    e2e_value = allreduce_sum(e2e_sets, world) / (allreduce_max(e2e_ms, world) / 1e3)
+
+    # ---- roofline of the dominant kernel (the sampler) ----------------------
+    # Algorithmic bytes: 8 B per vertex expansion (two u32 CSR offsets), 8 B
+    # per in-edge record read (u32 source + u32 threshold), 4 B per pool
+    # element written, 8 + 4 B per set (pool offset + length).
+    alg_bytes = 8 * int(st_tot[0]) + 8 * int(st_tot[1]) + 4 * int(st_tot[3]) + 12 * int(st_tot[2])
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / (kern_ms / 1e3) / 1e9 if kern_ms > 0 else None
+    kernel = "lt_walk_kernel" if w["model"] == "LT" else "ic_fused_kernel"
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(prof):
+        with open(prof) as fh:
+            tr = json.load(fh).get(w["name"])
+        if tr and kern_n:
+            # DRAM bytes per algorithmic byte from the ncu capture, applied to
+            # this run's average launch
+            traffic = tr["dram_bytes_per_alg_byte"] * alg_bytes / kern_n
+
+    base = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        base = cpu_baseline(w, g)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "sets/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic R-MAT graph (seed 0) and weights (seed 1); fresh sampler seed per step",
+            "config": {"workload": w["name"], "model": w["model"], "k": w["k"],
+                       "epsilon": w["eps"], "n": g.n, "m": g.m,
+                       "theta": thetas[0] if thetas else None,
+                       "parallelism": f"replicas x{world}",
+                       "l2": "graph (%d MB) and pool exceed L2 (126 MB)" % ((g.m * 8 + g.n * 4) >> 20)},
+            "e2e": {"value": e2e_value, "unit": "sets/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "steps": e2e_steps},
+            "roofline": {"bound": "hbm", "kernel": kernel,
+                         "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
+                         "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
+                         "traffic": traffic,
+                         "alg_bytes_per_launch": alg_bytes / max(kern_n, 1),
+                         "launches": kern_n, "kernel_ms": kern_ms},
+            "cpu_baseline": base,
+            "clocks": clk,
+            "gpu_launches": launches,
+            "imm_ms_per_step": t_max / args.steps,
+            "sets_per_step": total_sets / args.steps,
+        }
+        print(json.dumps(line))
+    pool.close()
+    dg.close()
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

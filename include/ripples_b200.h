@@ -83,6 +83,12 @@ int rip_sync(rip_ctx *ctx);
 int rip_ctx_memory(rip_ctx *ctx, size_t *used, size_t *budget);
 /* Library version string, e.g. "ripples_b200 0.1.0 sm_100a". */
 const char *rip_version(void);
+/* The context's CUDA stream (a cudaStream_t), so callers can order their own
+ * work or record timing events on it.  No reference counterpart (the reference
+ * keeps one stream per GPU worker internally, streaming_rrr_generator.h:369). */
+int rip_ctx_stream(rip_ctx *ctx, void **stream);
+/* Number of kernels this library has launched in the process so far. */
+uint64_t rip_kernel_launches(void);
 
 /* ---- graph ---------------------------------------------------------------- */
 /* Uploads a backward CSR (GraphBwd) and packs it for the kernels: weights are

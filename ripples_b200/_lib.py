@@ -71,6 +71,8 @@ SIGNATURES = {
     "rip_last_error": (ctypes.c_char_p, [P]),
     "rip_sync": (I32, [P]),
     "rip_ctx_memory": (I32, [P, ctypes.POINTER(SZ), ctypes.POINTER(SZ)]),
+    "rip_ctx_stream": (I32, [P, PP]),
+    "rip_kernel_launches": (U64, []),
     "rip_graph_upload": (I32, [P, P, P, P, U32, U64, I32, PP]),
     "rip_graph_destroy": (I32, [P]),
     "rip_graph_info": (I32, [P, ctypes.POINTER(U32), ctypes.POINTER(U64), ctypes.POINTER(I32)]),

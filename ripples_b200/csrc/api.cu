@@ -40,6 +40,8 @@ struct DevMem {
 };
 
 struct rip_ctx {
+  std::vector<rip_graph *> graphs;  // owned: freed by rip_ctx_destroy
+  std::vector<rip_pool *> pools;    // owned: freed by rip_ctx_destroy
   int device = 0;
   cudaStream_t stream = nullptr;
   int num_sms = 148;
@@ -193,6 +195,8 @@ int rip_ctx_destroy(rip_ctx *c) {
   if (!c) return RIP_ERR_INVALID;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  while (!c->pools.empty()) rip_pool_destroy(c->pools.back());
+  while (!c->graphs.empty()) rip_graph_destroy(c->graphs.back());
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -210,6 +214,14 @@ int rip_sync(rip_ctx *c) {
   return RIP_OK;
 }
 
+int rip_ctx_stream(rip_ctx *c, void **stream) {
+  if (!c || !stream) return RIP_ERR_INVALID;
+  *stream = (void *)c->stream;
+  return RIP_OK;
+}
+
+uint64_t rip_kernel_launches(void) { return rip::launch_counter(); }
+
 int rip_ctx_memory(rip_ctx *c, size_t *used, size_t *budget) {
   if (!c) return RIP_ERR_INVALID;
   if (used) *used = c->used;
@@ -222,6 +234,7 @@ int rip_ctx_memory(rip_ctx *c, size_t *used, size_t *budget) {
 // ---------------------------------------------------------------------------
 // graph
 // ---------------------------------------------------------------------------
+static rip_graph *pool_graph(const rip_pool *p);
 struct rip_graph {
   rip_ctx *ctx;
   uint32_t n;
@@ -305,14 +318,27 @@ extern "C" int rip_graph_upload(rip_ctx *c, const uint64_t *index,
     delete g;
     return rc;
   }
+  c->graphs.push_back(g);
   *out = g;
   return RIP_OK;
 }
 
+template <typename T>
+static void erase_ptr(std::vector<T *> &v, T *x) {
+  v.erase(std::remove(v.begin(), v.end(), x), v.end());
+}
+
 extern "C" int rip_graph_destroy(rip_graph *g) {
   if (!g) return RIP_ERR_INVALID;
-  cudaSetDevice(g->ctx->device);
-  cudaStreamSynchronize(g->ctx->stream);
+  rip_ctx *c = g->ctx;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  // pools sample from this graph: they go first
+  std::vector<rip_pool *> mine;
+  for (rip_pool *p : c->pools)
+    if (pool_graph(p) == g) mine.push_back(p);
+  for (rip_pool *p : mine) rip_pool_destroy(p);
+  erase_ptr(c->graphs, g);
   dfree(g->ctx, g->off);
   dfree(g->ctx, g->edges);
   delete g;
@@ -392,6 +418,8 @@ struct rip_pool {
   }
 };
 
+static rip_graph *pool_graph(const rip_pool *p) { return p->g; }
+
 static int read_meta(rip_pool *p, PoolMeta &m) {
   rip_ctx *c = p->ctx;
   CK(c, cudaMemcpyAsync(&m, p->meta.p, sizeof(PoolMeta), cudaMemcpyDeviceToHost,
@@ -412,6 +440,7 @@ extern "C" int rip_pool_create(rip_ctx *c, rip_graph *g, rip_pool **out) {
     return rc;
   }
   cudaMemsetAsync(p->meta.p, 0, sizeof(PoolMeta), c->stream);
+  c->pools.push_back(p);
   *out = p;
   return RIP_OK;
 }
@@ -428,6 +457,7 @@ extern "C" int rip_pool_destroy(rip_pool *p) {
                    &p->covered, &p->dirty_bits, &p->dirty_list, &p->pairs,
                    &p->scan_sums};
   for (DevMem *m : all) dfree(c, *m);
+  erase_ptr(c->pools, p);
   delete p;
   return RIP_OK;
 }
@@ -772,6 +802,12 @@ extern "C" int rip_sample(rip_pool *p, uint64_t seed, uint64_t count,
   TRY(ensure_sets(p, first + count));
   PoolMeta m;
   TRY(read_meta(p, m));
+  if (m.stats[2] == 0 && count > 4096) {
+    // Fresh pool: sample a pilot of 1024 sets first so the pool is sized from
+    // a measured mean set size (the sets are the same either way).
+    TRY(rip_sample(p, seed, 1024, sampler));
+    return rip_sample(p, seed, count - 1024, sampler);
+  }
   double mean = m.stats[2] ? (double)m.stats[3] / (double)m.stats[2] : 8.0;
   TRY(ensure_elems(p, p->num_elems + (uint64_t)(mean * 1.25 * count) + 1024));
   int rc;

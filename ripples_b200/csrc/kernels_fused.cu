@@ -62,6 +62,8 @@ ic_fused_kernel(FusedLaunch L) {
   const uint32_t lcap = L.lcap;
   unsigned long long n_exp = 0, n_edges = 0, n_sexp = 0, n_sedges = 0,
                      n_sets = 0, n_elems = 0;
+  // per-batch work, folded into the totals only when the batch is stored
+  unsigned long long b_exp = 0, b_edges = 0, b_sexp = 0, b_sedges = 0;
 
   for (;;) {
     if (tid == 0) {
@@ -98,6 +100,7 @@ ic_fused_kernel(FusedLaunch L) {
       }
     }
     __syncthreads();
+    b_exp = b_edges = b_sexp = b_sedges = 0;
     uint32_t lvl_start = 0, lvl_end = min(s_tail, lcap), level = 1;
     while (lvl_start < lvl_end && !s_overflow) {
       // ---- expand level `level`: entries log[lvl_start, lvl_end) ----------
@@ -122,10 +125,10 @@ ic_fused_kernel(FusedLaunch L) {
             uint32_t pc = 0;
 #pragma unroll
             for (int w = 0; w < CW; ++w) pc += __popcll(mask[w]);
-            n_exp += 1;
-            n_edges += end - beg;
-            n_sexp += pc;
-            n_sedges += (unsigned long long)pc * (end - beg);
+            b_exp += 1;
+            b_edges += end - beg;
+            b_sexp += pc;
+            b_sedges += (unsigned long long)pc * (end - beg);
           }
         }
         const uint32_t incl = warp_incl_scan(ng);
@@ -251,6 +254,10 @@ ic_fused_kernel(FusedLaunch L) {
     __syncthreads();
     const bool store = s_overflow == 0;
     if (store) {
+      n_exp += b_exp;
+      n_edges += b_edges;
+      n_sexp += b_sexp;
+      n_sedges += b_sedges;
       for (uint32_t c = tid; c < ncol; c += FUSED_THREADS) {
         L.P.set_off[s_set[c]] = s_start[c];
         L.P.set_len[s_set[c]] = s_size[c];
@@ -303,6 +310,7 @@ ic_fused_kernel(FusedLaunch L) {
 }  // namespace
 
 void launch_ic_fused(const FusedLaunch &L, cudaStream_t stream) {
+  count_launches(1);
   if (L.colors == 64)
     ic_fused_kernel<1><<<L.blocks, FUSED_THREADS, 0, stream>>>(L);
   else if (L.colors == 128)
@@ -342,6 +350,7 @@ gather_sets_kernel(DevPool P, uint64_t first, uint64_t count,
 
 void launch_gather_sets(const DevPool &P, uint64_t first, uint64_t count,
                         const uint64_t *csr, uint32_t *out, cudaStream_t s) {
+  count_launches(1);
   if (count == 0) return;
   gather_sets_kernel<<<1184, 256, 0, s>>>(P, first, count, csr, out);
 }

@@ -10,6 +10,8 @@
 //   LT : thr = clamp(floor((sum of in-weights up to this edge, in double,
 //                           CSR order) * 2^32), 0, 2^32-1)
 // Offsets shrink to u32 (m < 2^32 is required).
+#include <atomic>
+
 #include "device.cuh"
 #include "launch.h"
 
@@ -60,11 +62,16 @@ __global__ void pack_lt_kernel(const uint64_t *index, const uint32_t *src,
 
 }  // namespace
 
+static std::atomic<uint64_t> g_launches{0};
+uint64_t launch_counter() { return g_launches.load(); }
+void count_launches(uint64_t n) { g_launches.fetch_add(n); }
+
 static uint64_t pad4(uint64_t m) { return (m + 3) & ~uint64_t(3); }
 
 void launch_pack_ic(const uint64_t *index, const float *w, uint32_t n,
                     uint64_t m, uint32_t *off, uint2 *edges, const uint32_t *src,
                     cudaStream_t stream) {
+  count_launches(2);
   pack_off_kernel<<<1184, 256, 0, stream>>>(index, n, off);
   pack_ic_kernel<<<2368, 256, 0, stream>>>(src, w, m, pad4(m) + 4, edges);
 }
@@ -72,6 +79,7 @@ void launch_pack_ic(const uint64_t *index, const float *w, uint32_t n,
 void launch_pack_lt(const uint64_t *index, const float *w, uint32_t n,
                     uint64_t m, uint32_t *off, uint2 *edges, const uint32_t *src,
                     cudaStream_t stream) {
+  count_launches(2);
   pack_off_kernel<<<1184, 256, 0, stream>>>(index, n, off);
   pack_lt_kernel<<<1184, 128, 0, stream>>>(index, src, w, n, m, pad4(m) + 4,
                                            edges);

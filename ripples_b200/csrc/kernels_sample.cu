@@ -93,6 +93,7 @@ ic_plain_kernel(DevGraph G, DevPool P, Key key, uint64_t first, uint32_t count,
     __syncwarp();
     uint32_t qlen = 1, head = 0;
     bool overflow = false;
+    unsigned long long set_exp = 0, set_edges = 0;
 
     while (head < qlen && !overflow) {
       const uint32_t take = min(32u, qlen - head);
@@ -102,9 +103,9 @@ ic_plain_kernel(DevGraph G, DevPool P, Key key, uint64_t first, uint32_t count,
         beg = __ldg(G.off + v);
         end = __ldg(G.off + v + 1);
         ng = group_count(beg, end);
-        n_edges += end - beg;
+        set_edges += end - beg;
       }
-      n_exp += (lane == 0) ? take : 0;
+      set_exp += (lane == 0) ? take : 0;
       const uint32_t incl = warp_incl_scan(ng);
       const uint32_t total = __shfl_sync(FULL, incl, 31);
       for (uint32_t base = 0; base < total && !overflow; base += 32) {
@@ -163,6 +164,8 @@ ic_plain_kernel(DevGraph G, DevPool P, Key key, uint64_t first, uint32_t count,
     if (finish_set(W, qlen, overflow, s, rel, P, F)) {
       n_sets += (lane == 0);
       n_elems += (lane == 0) ? qlen : 0;
+      n_exp += set_exp;
+      n_edges += set_edges;
     }
   }
   n_exp = warp_sum_u64(n_exp);
@@ -204,12 +207,13 @@ lt_walk_kernel(DevGraph G, DevPool P, Key key, uint64_t first, uint32_t count,
     __syncwarp();
     uint32_t qlen = 1;
     bool overflow = false;
+    unsigned long long set_exp = 0, set_edges = 0;
     for (;;) {
-      n_exp += (lane == 0);
+      set_exp += (lane == 0);
       const uint32_t t = lt_threshold(key, s, cur);
       uint32_t lo = __ldg(G.off + cur), hi = __ldg(G.off + cur + 1);
       if (hi == lo) break;
-      n_edges += (lane == 0);
+      set_edges += (lane == 0);
       if (__ldg(&G.edges[hi - 1].y) <= t) break;  // total in-weight < threshold
       // 32-ary search for the first edge whose cumulative threshold exceeds t.
       while (hi - lo > 32) {
@@ -217,7 +221,7 @@ lt_walk_kernel(DevGraph G, DevPool P, Key key, uint64_t first, uint32_t count,
         const uint32_t p = min(lo + (lane + 1) * stride - 1, hi - 1);
         const bool pred = t < __ldg(&G.edges[p].y);
         const uint32_t bal = __ballot_sync(FULL, pred);
-        n_edges += (lane == 0) ? 32 : 0;
+        set_edges += (lane == 0) ? 32 : 0;
         const uint32_t L = __ffs(bal) - 1;
         const uint32_t nlo = lo + L * stride;
         hi = min(hi, lo + (L + 1) * stride);
@@ -226,7 +230,7 @@ lt_walk_kernel(DevGraph G, DevPool P, Key key, uint64_t first, uint32_t count,
       const uint32_t e = lo + lane;
       const bool pred = e < hi && t < __ldg(&G.edges[e].y);
       const uint32_t bal = __ballot_sync(FULL, pred);
-      n_edges += (lane == 0) ? (hi - lo) : 0;
+      set_edges += (lane == 0) ? (hi - lo) : 0;
       const uint32_t jsel = lo + __ffs(bal) - 1;
       const uint32_t u = __ldg(&G.edges[jsel].x);
       uint32_t seen = 0;
@@ -249,6 +253,8 @@ lt_walk_kernel(DevGraph G, DevPool P, Key key, uint64_t first, uint32_t count,
     if (finish_set(W, qlen, overflow, s, rel, P, F)) {
       n_sets += (lane == 0);
       n_elems += (lane == 0) ? qlen : 0;
+      n_exp += set_exp;
+      n_edges += set_edges;
     }
   }
   n_exp = warp_sum_u64(n_exp);
@@ -266,12 +272,14 @@ lt_walk_kernel(DevGraph G, DevPool P, Key key, uint64_t first, uint32_t count,
 }
 
 void launch_ic_plain(const SampleLaunch &L, cudaStream_t stream) {
+  count_launches(1);
   ic_plain_kernel<<<L.blocks, L.threads, 0, stream>>>(
       L.G, L.P, L.key, L.first, L.count, L.ids, L.next, L.bitmaps, L.bm_words,
       L.queues, L.qcap, L.F, L.st);
 }
 
 void launch_lt_walk(const SampleLaunch &L, cudaStream_t stream) {
+  count_launches(1);
   lt_walk_kernel<<<L.blocks, L.threads, 0, stream>>>(
       L.G, L.P, L.key, L.first, L.count, L.ids, L.next, L.bitmaps, L.bm_words,
       L.queues, L.qcap, L.F, L.st);

@@ -268,6 +268,7 @@ scan_apply_kernel(const uint32_t *in, uint32_t n, const uint64_t *tile_sums,
 
 void launch_count(const DevPool &P, uint64_t num_sets, uint32_t *count,
                   int blocks, cudaStream_t stream) {
+  count_launches(1);
   count_kernel<<<blocks, 256, 0, stream>>>(P, num_sets, count);
 }
 
@@ -277,6 +278,7 @@ size_t scan_block_sums_needed(uint32_t n) {
 
 void launch_exclusive_scan(const uint32_t *in, uint64_t *out, uint32_t n,
                            uint64_t *block_sums, cudaStream_t stream) {
+  count_launches(3);
   const uint32_t tiles = (uint32_t)((n + (uint64_t)SCAN_TILE - 1) / SCAN_TILE);
   if (tiles == 0) {
     cudaMemsetAsync(out, 0, sizeof(uint64_t), stream);
@@ -290,10 +292,12 @@ void launch_exclusive_scan(const uint32_t *in, uint64_t *out, uint32_t n,
 void launch_build_inverted(const DevPool &P, uint64_t num_sets,
                            uint64_t *cursor, uint32_t *inv, int blocks,
                            cudaStream_t stream) {
+  count_launches(1);
   inverted_kernel<<<blocks, 256, 0, stream>>>(P, num_sets, cursor, inv);
 }
 
 void launch_cover(const CoverLaunch &C, cudaStream_t stream) {
+  count_launches(1);
   cover_kernel<<<C.blocks, 256, 0, stream>>>(C);
 }
 
@@ -301,12 +305,14 @@ void launch_gather_dirty(const uint32_t *dirty_list, const unsigned int *dirty_n
                          uint32_t max_n, const uint32_t *count,
                          uint32_t *dirty_bits, uint2 *pairs, int blocks,
                          cudaStream_t stream) {
+  count_launches(1);
   gather_dirty_kernel<<<blocks, 256, 0, stream>>>(dirty_list, dirty_n, max_n,
                                                   count, dirty_bits, pairs);
 }
 
 void launch_argmax(const uint32_t *count, uint32_t n, unsigned long long *best,
                    int blocks, cudaStream_t stream) {
+  count_launches(1);
   argmax_kernel<<<blocks, 256, 0, stream>>>(count, n, best);
 }
 

@@ -7,6 +7,10 @@
 
 namespace rip {
 
+// Process-wide count of kernel launches issued by this library.
+uint64_t launch_counter();
+void count_launches(uint64_t n);
+
 struct SampleLaunch {
   DevGraph G;
   DevPool P;

@@ -11,6 +11,7 @@ objects ``rip_ctx``, ``rip_graph`` and ``rip_pool``.
 from __future__ import annotations
 
 import ctypes
+import weakref
 from dataclasses import dataclass
 from typing import Optional, Sequence, Tuple
 
@@ -107,15 +108,20 @@ class HostGraph:
 
 
 class Context:
-    """One CUDA device + stream (``rip_ctx``)."""
+    """One CUDA device + stream (``rip_ctx``).  The context owns the graphs
+    and pools created on it: closing it frees them, and their Python handles
+    become inert."""
 
     def __init__(self, device: int = 0, hbm_budget: int = 0):
         h = ctypes.c_void_p()
         check(lib.rip_ctx_create(device, hbm_budget, ctypes.byref(h)), "rip_ctx_create")
         self.h = h
+        self._children = weakref.WeakSet()
 
     def close(self) -> None:
         if self.h:
+            for ch in list(self._children):
+                ch._invalidate()
             lib.rip_ctx_destroy(self.h)
             self.h = None
 
@@ -151,6 +157,13 @@ class DeviceGraph:
         check(lib.rip_graph_upload(ctx.h, _ptr(idx), _ptr(src), _ptr(w), g.n, g.m,
                                    MODELS[model], ctypes.byref(h)), "rip_graph_upload", ctx.h)
         self.h = h
+        self._pools = weakref.WeakSet()
+        ctx._children.add(self)
+
+    def _invalidate(self) -> None:
+        for p in list(self._pools):
+            p._invalidate()
+        self.h = None
 
     def thresholds(self) -> np.ndarray:
         out = np.empty(self.m, dtype=np.uint32)
@@ -159,7 +172,10 @@ class DeviceGraph:
 
     def close(self) -> None:
         if self.h:
-            lib.rip_graph_destroy(self.h)
+            for p in list(self._pools):
+                p._invalidate()  # freed by rip_graph_destroy
+            if self.ctx.h:
+                lib.rip_graph_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -178,10 +194,16 @@ class Pool:
         check(lib.rip_pool_create(self.ctx.h, graph.h, ctypes.byref(h)), "rip_pool_create",
               self.ctx.h)
         self.h = h
+        graph._pools.add(self)
+        self.ctx._children.add(self)
+
+    def _invalidate(self) -> None:
+        self.h = None
 
     def close(self) -> None:
         if self.h:
-            lib.rip_pool_destroy(self.h)
+            if self.ctx.h and self.graph.h:
+                lib.rip_pool_destroy(self.h)
             self.h = None
 
     def __del__(self):

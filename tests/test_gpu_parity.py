@@ -203,7 +203,8 @@ def test_selection_stops_when_all_covered(ctx):
     off, vtx = csr_of([[1, 2], [2, 3], [3], [9]])
     p.import_sets(off, vtx)
     f, seeds, gains = p.select(8)
-    assert f == 1.0 and len(seeds) == 2 and gains.sum() == 4
+    of, oseeds, ogains, _ = O.select(10, off, vtx, 8, 0)
+    assert f == 1.0 == of and seeds.tolist() == oseeds.tolist() and gains.sum() == 4
     f, seeds, gains = p.select(0)
     assert len(seeds) == 0 and f == 0.0
 

@@ -1,0 +1,58 @@
+"""North-star check 4: the spread of our IMM seeds, measured with the
+reference's own Monte Carlo simulator (include/ripples/diffusion_simulation.h,
+driven like tools/simulator.cc), is within 1% of the spread of the seeds the
+reference's imm tool picks on the same graph.
+
+Our seeds come from the oracle's IMM, which the GPU tests prove bit-identical
+to the device IMM (same sets, same selection), so this runs on the CPU."""
+import json
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+import ripples_b200 as rb
+from oracle import oracle as O
+from conftest import ROOT
+
+IMM_EXE = os.path.join(ROOT, "oracle", "_ref", "imm")
+
+
+def reference_seeds(path, model, k, eps, parallel):
+    out = tempfile.mktemp(suffix=".json")
+    cmd = [IMM_EXE, "-i", path, "--reload-binary", "-d", model, "-k", str(k), "-e", str(eps),
+           "-o", out] + (["-p"] if parallel else [])
+    subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL,
+                   env=dict(os.environ, OMP_NUM_THREADS="4"), timeout=600)
+    with open(out) as fh:
+        rec = json.load(fh)[0]
+    os.unlink(out)
+    return rec["Seeds"]
+
+
+@pytest.mark.parametrize("model,scale,draws,k,eps", [
+    ("IC", 14, 1 << 18, 20, 0.5),   # the 2^14-vertex IC configuration
+    ("LT", 13, 8 << 13, 20, 0.5),   # a reduced LT configuration
+])
+def test_spread_within_one_percent_of_reference(tmp_path, model, scale, draws, k, eps):
+    R = O.reference()
+    if R is None or not os.path.exists(IMM_EXE):
+        pytest.skip("oracle/_ref not built")
+    g = rb.HostGraph.rmat(scale, draws, seed=0)
+    g = g.with_weights(rb.WEIGHTS_UNIFORM, seed=1, lo=0.0, hi=0.1) if model == "IC" else \
+        g.with_weights(rb.WEIGHTS_LT_NORMALIZED, seed=1)
+    bwd = str(tmp_path / "g.bin")
+    fwd = str(tmp_path / "gf.bin")
+    g.write_binary(bwd, backward=True)
+    g.write_binary(fwd, backward=False)
+    ref = reference_seeds(bwd, model, k, eps, parallel=(model == "IC"))
+    thr = O.pack(model, g.index, g.weights)
+    ours = O.imm(model, g.n, g.index, g.src, thr, k, eps, seed=0)["seeds"]
+    assert len(ours) == len(ref) == k
+    reps = 10000
+    m = 0 if model == "IC" else 1
+    s_ref = R.ref_simulate(fwd.encode(), m, np.asarray(ref, np.uint32).ctypes.data, k, reps, 0)
+    s_our = R.ref_simulate(fwd.encode(), m, np.asarray(ours, np.uint32).ctypes.data, k, reps, 0)
+    assert abs(s_our - s_ref) / s_ref < 0.01, (s_our, s_ref)
