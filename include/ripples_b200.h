@@ -169,6 +169,11 @@ int rip_select(rip_pool *p, uint64_t num_sets, uint32_t k, int tiebreak,
  * (the reference's known-answer test, test/cuda_find_most_influential.cc:84-167). */
 int rip_select_counts(rip_pool *p, uint32_t *counts);
 
+/* Diagnostic: builds a heap of n random (vertex, count) entries, counts in
+ * [0, max_count), with the library's level-parallel heap construction and with
+ * std::make_heap; returns 1 when the two are identical element for element. */
+int rip_selftest_heap(uint64_t n, uint32_t max_count, uint64_t seed);
+
 /* Vertex occurrence counts over sets [0, num_sets) (n values), the first
  * step of selection (CountOccurrencies, include/ripples/counting.h:65-97). */
 int rip_count(rip_pool *p, uint64_t num_sets, uint32_t *counts);

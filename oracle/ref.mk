@@ -16,7 +16,7 @@ DEFS     := -DNDEBUG -DSORTING=1 -DREORDERING=1 -DRIPPLES_ENABLE_FLOAT_WEIGHTS=1
 INC      := -I$(REF)/include -Ioracle/shims -I$(SPDLOG) -I$(NLOHMANN)
 FLAGS    := -O3 -fopenmp -std=c++17 -w $(DEFS) $(INC)
 
-all: $(OUT)/imm $(OUT)/simulator $(OUT)/libref_harness.so
+all: $(OUT)/imm $(OUT)/simulator $(OUT)/libref_harness.so $(OUT)/adapter_imm
 
 $(OUT):
 	mkdir -p $(OUT)
@@ -26,6 +26,12 @@ $(OUT)/imm: $(REF)/tools/imm.cc | $(OUT)
 
 $(OUT)/simulator: $(REF)/tools/simulator.cc | $(OUT)
 	$(REFCXX) $(FLAGS) $< -o $@
+
+# Integration check of the drop-in adapter (include/ripples_b200/imm_adapter.hpp)
+# compiled against the reference headers and linked to the in-tree library.
+LIBDIR   := $(abspath ripples_b200/_lib)
+$(OUT)/adapter_imm: tests/integration/adapter_imm.cc include/ripples_b200/imm_adapter.hpp include/ripples_b200.h $(LIBDIR)/libripples_b200.so | $(OUT)
+	$(REFCXX) $(FLAGS) -Iinclude $< -o $@ -L$(LIBDIR) -lripples_b200 -Wl,-rpath,'$$ORIGIN/../../ripples_b200/_lib'
 
 $(OUT)/libref_harness.so: oracle/ref_harness.cpp | $(OUT)
 	$(REFCXX) $(FLAGS) -fPIC -shared $< -o $@

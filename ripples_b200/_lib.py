@@ -89,6 +89,7 @@ SIGNATURES = {
     "rip_pool_configure": (I32, [P, U32, U32, U32]),
     "rip_select": (I32, [P, U64, U32, I32, P, P, ctypes.POINTER(U32), ctypes.POINTER(DBL)]),
     "rip_select_counts": (I32, [P, P]),
+    "rip_selftest_heap": (I32, [U64, U32, U64]),
     "rip_count": (I32, [P, U64, P]),
     "rip_imm": (I32, [P, P, U32, DBL, DBL, U64, I32, I32, P, ctypes.POINTER(U32),
                       ctypes.POINTER(ImmRecord)]),
@@ -110,7 +111,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     if not os.path.exists(path):
         raise ImportError(
             f"native library not found at {path}; build it with "
-            "`python -m ripples_b200.build` (the package has no non-CUDA fallback)")
+            "`python ripples_b200/build.py` (the package has no non-CUDA fallback)")
     lib = ctypes.CDLL(path)
     for name, (res, args) in SIGNATURES.items():
         fn = getattr(lib, name)

@@ -4,7 +4,8 @@ Compiles ripples_b200/csrc/*.cu and *.cpp with nvcc for
 ``-gencode arch=compute_100a,code=sm_100a`` and links
 ``ripples_b200/_lib/libripples_b200.so`` plus the drop-in ``imm`` tool.
 Objects are rebuilt when a source or any header under csrc/ or include/ is
-newer.  Run ``python -m ripples_b200.build`` or call :func:`build`.
+newer.  Run ``python ripples_b200/build.py`` (not ``-m``: importing the
+package loads the library this script builds) or call :func:`build`.
 """
 from __future__ import annotations
 

@@ -134,15 +134,23 @@ static T *ptr(DevMem &m) {
 
 struct PinnedMem {
   void *p = nullptr;
+  void *dev = nullptr;  // device alias when mapped
   size_t bytes = 0;
-  int ensure(rip_ctx *c, size_t b) {
+  int ensure(rip_ctx *c, size_t b, bool mapped = false) {
     if (p && bytes >= b) return RIP_OK;
     if (p) cudaFreeHost(p);
-    p = nullptr;
+    p = dev = nullptr;
     bytes = 0;
-    if (cudaMallocHost(&p, b) != cudaSuccess) {
+    if (cudaHostAlloc(&p, b, mapped ? cudaHostAllocMapped : cudaHostAllocDefault) !=
+        cudaSuccess) {
       cudaGetLastError();
-      return set_err(c, RIP_ERR_NOMEM, "cudaMallocHost(%zu) failed", b);
+      return set_err(c, RIP_ERR_NOMEM, "cudaHostAlloc(%zu) failed", b);
+    }
+    if (mapped && cudaHostGetDevicePointer(&dev, p, 0) != cudaSuccess) {
+      cudaGetLastError();
+      cudaFreeHost(p);
+      p = nullptr;
+      return set_err(c, RIP_ERR_CUDA, "cudaHostGetDevicePointer failed");
     }
     bytes = b;
     return RIP_OK;
@@ -916,7 +924,57 @@ struct CompareHeap {  // include/ripples/streaming_find_most_influential.h:410-4
     return a.second < b.second;
   }
 };
+using HeapItem = std::pair<uint32_t, size_t>;
+using RefQueue = std::priority_queue<HeapItem, std::vector<HeapItem>, CompareHeap>;
+
+// std::priority_queue that adopts an already-heapified container instead of
+// running make_heap again (its container and comparator are protected
+// members).  pop/push are libstdc++'s own pop_heap/push_heap, as in the
+// reference.
+struct AdoptedQueue : RefQueue {
+  explicit AdoptedQueue(std::vector<HeapItem> &&heap) { this->c = std::move(heap); }
+};
+
+// Bit-identical to std::make_heap(v.begin(), v.end(), CompareHeap{}), built
+// level by level in parallel.  libstdc++'s make_heap runs __adjust_heap on
+// every parent from (len-2)/2 down to 0; each call only touches the subtree
+// under its parent, and all parents at one depth have disjoint subtrees and
+// larger indices than every parent above them, so processing the depths from
+// the deepest up -- each depth in any order -- performs the same operations on
+// the same data.
+void parallel_make_heap(std::vector<HeapItem> &v) {
+  const std::ptrdiff_t len = (std::ptrdiff_t)v.size();
+  if (len < 2) return;
+  const std::ptrdiff_t last_parent = (len - 2) / 2;
+  int dmax = 0;
+  while ((((std::ptrdiff_t)2) << dmax) - 1 <= last_parent) ++dmax;
+  for (int d = dmax; d >= 0; --d) {
+    const std::ptrdiff_t lo = (((std::ptrdiff_t)1) << d) - 1;
+    const std::ptrdiff_t hi = std::min(last_parent, (((std::ptrdiff_t)2) << d) - 2);
+#pragma omp parallel for schedule(static) if (hi - lo > 8192)
+    for (std::ptrdiff_t p = hi; p >= lo; --p) {
+      HeapItem val = std::move(v[p]);
+      std::__adjust_heap(v.begin(), p, len, std::move(val),
+                         __gnu_cxx::__ops::_Iter_comp_iter<CompareHeap>(CompareHeap{}));
+    }
+  }
+}
 }  // namespace
+
+// Diagnostic: checks parallel_make_heap against std::make_heap on n random
+// counts drawn from [0, max_count) (many ties); returns 1 when identical.
+extern "C" int rip_selftest_heap(uint64_t n, uint32_t max_count, uint64_t seed) {
+  std::vector<HeapItem> a(n), b;
+  uint64_t x = seed * 6364136223846793005ull + 1442695040888963407ull;
+  for (uint64_t i = 0; i < n; ++i) {
+    x = x * 6364136223846793005ull + 1442695040888963407ull;
+    a[i] = {(uint32_t)i, (size_t)((x >> 33) % (max_count ? max_count : 1))};
+  }
+  b = a;
+  std::make_heap(b.begin(), b.end(), CompareHeap{});
+  parallel_make_heap(a);
+  return a == b ? 1 : 0;
+}
 
 static int count_sets(rip_pool *p, uint64_t S) {
   rip_ctx *c = p->ctx;
@@ -988,7 +1046,6 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
   TRY(dalloc(c, p->dirty_bits, sizeof(uint32_t) * dwords));
   CK(c, cudaMemsetAsync(p->dirty_bits.p, 0, sizeof(uint32_t) * dwords, c->stream));
   TRY(dalloc(c, p->dirty_list, sizeof(uint32_t) * (size_t)n));
-  TRY(dalloc(c, p->pairs, sizeof(uint2) * (size_t)n));
   PoolMeta *dm = p->dmeta();
   CK(c, cudaMemsetAsync(&dm->dirty_n, 0, sizeof(unsigned int), c->stream));
   CK(c, cudaMemsetAsync(&dm->covered_sets, 0, sizeof(unsigned long long), c->stream));
@@ -1007,7 +1064,8 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
 
   std::vector<uint32_t> &hcount = p->last_counts;
   hcount.resize(n);
-  TRY(p->h_pairs.ensure(c, sizeof(uint2) * (size_t)n));
+  // mapped: [count u32, pad][n pairs]; the gather kernel writes it directly
+  TRY(p->h_pairs.ensure(c, 16 + sizeof(uint2) * (size_t)n, true));
   TRY(p->h_count.ensure(c, sizeof(uint32_t) * (size_t)n));
 
   uint64_t uncovered = S;
@@ -1015,20 +1073,19 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
   std::vector<uint64_t> out_gains;
 
   // Applies the dirty (vertex, count) list of the last cover step to hcount.
+  // After a cover step: the dirty (vertex, count) pairs go straight to mapped
+  // host memory; one synchronisation, then the host mirror is patched.
   auto sync_dirty = [&]() -> int {
-    unsigned int dn = 0;
-    CK(c, cudaMemcpyAsync(&dn, &dm->dirty_n, sizeof(dn), cudaMemcpyDeviceToHost,
-                          c->stream));
-    CK(c, cudaStreamSynchronize(c->stream));
-    if (dn == 0) return RIP_OK;
+    unsigned char *hb = static_cast<unsigned char *>(p->h_pairs.p);
+    unsigned char *db = static_cast<unsigned char *>(p->h_pairs.dev);
     launch_gather_dirty(ptr<uint32_t>(p->dirty_list), &dm->dirty_n, n,
                         ptr<uint32_t>(p->count), ptr<uint32_t>(p->dirty_bits),
-                        ptr<uint2>(p->pairs), c->num_sms * 4, c->stream);
-    CK(c, cudaMemcpyAsync(p->h_pairs.p, p->pairs.p, sizeof(uint2) * dn,
-                          cudaMemcpyDeviceToHost, c->stream));
+                        reinterpret_cast<uint2 *>(db + 16),
+                        reinterpret_cast<unsigned int *>(db), c->num_sms * 4, c->stream);
     CK(c, cudaMemsetAsync(&dm->dirty_n, 0, sizeof(unsigned int), c->stream));
     CK(c, cudaStreamSynchronize(c->stream));
-    const uint2 *hp = reinterpret_cast<const uint2 *>(p->h_pairs.p);
+    const unsigned int dn = *reinterpret_cast<volatile unsigned int *>(hb);
+    const uint2 *hp = reinterpret_cast<const uint2 *>(hb + 16);
     for (unsigned int i = 0; i < dn; ++i) hcount[hp[i].x] = hp[i].y;
     return RIP_OK;
   };
@@ -1038,13 +1095,14 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
                           cudaMemcpyDeviceToHost, c->stream));
     CK(c, cudaStreamSynchronize(c->stream));
     std::memcpy(hcount.data(), p->h_count.p, sizeof(uint32_t) * (size_t)n);
-    // InitHeapStorage + std::priority_queue(cmp, std::move(storage)), exactly
-    // as the reference builds its heap (streaming_find_most_influential.h:541-544)
-    std::vector<std::pair<uint32_t, size_t>> storage(n);
-    for (uint32_t v = 0; v < n; ++v) storage[v] = {v, hcount[v]};
-    std::priority_queue<std::pair<uint32_t, size_t>,
-                        std::vector<std::pair<uint32_t, size_t>>, CompareHeap>
-        queue(CompareHeap{}, std::move(storage));
+    // InitHeapStorage + std::priority_queue(cmp, std::move(storage)), as the
+    // reference builds its heap (streaming_find_most_influential.h:541-544;
+    // counting.h:196-206): the same heap, built level-parallel
+    std::vector<HeapItem> storage(n);
+#pragma omp parallel for schedule(static)
+    for (long long v = 0; v < (long long)n; ++v) storage[v] = {(uint32_t)v, hcount[v]};
+    parallel_make_heap(storage);
+    AdoptedQueue queue(std::move(storage));
     while (out_seeds.size() < k && uncovered != 0) {
       std::pair<uint32_t, size_t> element;
       for (;;) {  // getNextSeed, streaming_find_most_influential.h:560-571

@@ -147,10 +147,15 @@ __global__ void __launch_bounds__(256) cover_kernel(CoverLaunch C) {
   if (lane_id() == 0 && newly) atomicAdd(C.covered_sets, newly);
 }
 
+// Writes the (vertex, count) pairs of the dirty list, and their number, to
+// `pairs` / `total_out` -- mapped pinned host memory, so the host reads them
+// after one stream synchronisation.
 __global__ void gather_dirty_kernel(const uint32_t *list, const unsigned int *n,
                                     uint32_t max_n, const uint32_t *count,
-                                    uint32_t *bits, uint2 *pairs) {
+                                    uint32_t *bits, uint2 *pairs,
+                                    unsigned int *total_out) {
   const uint32_t total = min(*n, max_n);
+  if (blockIdx.x == 0 && threadIdx.x == 0) *total_out = total;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total;
        i += gridDim.x * blockDim.x) {
     const uint32_t u = list[i];
@@ -303,11 +308,11 @@ void launch_cover(const CoverLaunch &C, cudaStream_t stream) {
 
 void launch_gather_dirty(const uint32_t *dirty_list, const unsigned int *dirty_n,
                          uint32_t max_n, const uint32_t *count,
-                         uint32_t *dirty_bits, uint2 *pairs, int blocks,
-                         cudaStream_t stream) {
+                         uint32_t *dirty_bits, uint2 *pairs, unsigned int *total_out,
+                         int blocks, cudaStream_t stream) {
   count_launches(1);
   gather_dirty_kernel<<<blocks, 256, 0, stream>>>(dirty_list, dirty_n, max_n,
-                                                  count, dirty_bits, pairs);
+                                                  count, dirty_bits, pairs, total_out);
 }
 
 void launch_argmax(const uint32_t *count, uint32_t n, unsigned long long *best,

@@ -89,8 +89,8 @@ struct CoverLaunch {
 void launch_cover(const CoverLaunch &C, cudaStream_t stream);
 void launch_gather_dirty(const uint32_t *dirty_list, const unsigned int *dirty_n,
                          uint32_t max_n, const uint32_t *count,
-                         uint32_t *dirty_bits, uint2 *pairs, int blocks,
-                         cudaStream_t stream);
+                         uint32_t *dirty_bits, uint2 *pairs, unsigned int *total_out,
+                         int blocks, cudaStream_t stream);
 void launch_argmax(const uint32_t *count, uint32_t n, unsigned long long *best,
                    int blocks, cudaStream_t stream);
 

@@ -135,3 +135,12 @@ def test_json_log_keys():
                 "Counting", "Pivoting", "Microbenchmarking", "CPUBatchSize", "GPUBatchSize",
                 "RRRSetSizeBytes", "GenerateRRRSets", "FindMostInfluentialSet", "Seeds"]:
         assert key in e
+
+
+@pytest.mark.parametrize("n,max_count,seed", [(1, 3, 0), (2, 1, 1), (37, 2, 2), (5000, 3, 3),
+                                              (1 << 20, 5, 4), ((1 << 20) + 12345, 1000, 5)])
+def test_parallel_heap_is_libstdcxx_make_heap(n, max_count, seed):
+    """The selection heap is built level-parallel; it must equal
+    std::make_heap element for element (the reference's tie-break depends on
+    the exact heap layout), including with heavy ties."""
+    assert _lib.lib.rip_selftest_heap(n, max_count, seed) == 1
