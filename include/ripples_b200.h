@@ -212,6 +212,45 @@ int rip_imm_pool(rip_pool *p, uint32_t k, double epsilon, double l,
                  uint64_t seed, int tiebreak, int sampler, uint32_t *seeds,
                  uint32_t *num_seeds, rip_imm_record *record);
 
+/* ---- sampling without allocation ------------------------------------------- */
+/* No counterpart in the reference.  A variant of rip_sample's one-set-per-warp
+ * samplers (IC BFS / LT walk) for callers that cannot allocate device memory
+ * when they sample -- e.g. a serving process whose HBM is reserved up front by
+ * its own arena allocator, a latency-critical loop where cudaMalloc/cudaFree
+ * would synchronise the device, or a plugin host that forbids allocations
+ * outside its allocator.  It calls no cudaMalloc/cudaFree: all scratch comes
+ * from one file-scope device array of RIP_STATIC_SCRATCH_BYTES that every GPU
+ * loading the library holds until exit.
+ *   Inputs : the packed graph in caller-owned device memory -- d_off, u32[n+1]
+ *            edge offsets, and d_edges, 8-byte {u32 source, u32 threshold}
+ *            records, padded with zero records to a multiple of 4 plus 4 and
+ *            32-byte aligned (the layout rip_graph_upload builds; thresholds as
+ *            rip_graph_thresholds returns them).
+ *   Outputs: caller-owned device buffers -- set s = first+i (i < count) is
+ *            d_vertices[d_set_offsets[i] .. + d_set_lengths[i]) (members in
+ *            discovery order, not sorted); *num_elements = elements written.
+ *            Sets are bit-identical to rip_sample's for the same seed and ids.
+ *   Limits : count <= RIP_STATIC_MAX_SETS per call; n such that eight warps'
+ *            n-bit bitmaps plus queues fit in the array (about 24 million
+ *            vertices); larger requests return RIP_ERR_LIMIT, as does a
+ *            vertex_capacity too small for the sets (message from
+ *            rip_static_last_error()).
+ *   Rules  : the first call on a device looks up the array's address with
+ *            cudaGetSymbolAddress; make it before any stream capture.  Every
+ *            call shares the array and it keeps the last call's contents (each
+ *            call re-zeroes what must start at zero); calls that overlap on the
+ *            GPU race, so serialise them.  `stream` is a cudaStream_t (NULL =
+ *            legacy default stream); the call returns after it synchronises. */
+#define RIP_STATIC_SCRATCH_BYTES (32u << 20)
+#define RIP_STATIC_MAX_SETS (1u << 20)
+int rip_sample_static(const uint32_t *d_off, const void *d_edges, uint32_t n,
+                      uint64_t m, int model, uint64_t seed, uint64_t first,
+                      uint32_t count, uint32_t *d_vertices, uint64_t vertex_capacity,
+                      uint64_t *d_set_offsets, uint32_t *d_set_lengths,
+                      uint64_t *num_elements, void *stream);
+/* Message for the last rip_sample_static failure on the calling thread. */
+const char *rip_static_last_error(void);
+
 /* ---- theta math (host) ------------------------------------------------------ */
 /* Exactly include/ripples/imm.h:77-128 and utility.h:84-87, including the
  * ssize_t / size_t truncations. */

@@ -95,6 +95,9 @@ SIGNATURES = {
                       ctypes.POINTER(ImmRecord)]),
     "rip_imm_pool": (I32, [P, U32, DBL, DBL, U64, I32, I32, P, ctypes.POINTER(U32),
                            ctypes.POINTER(ImmRecord)]),
+    "rip_sample_static": (I32, [P, P, U32, U64, I32, U64, U64, U32, P, U64, P, P,
+                                ctypes.POINTER(U64), P]),
+    "rip_static_last_error": (ctypes.c_char_p, []),
     "rip_theta_prime": (I64, [I64, DBL, DBL, U64, U64]),
     "rip_inv_theta_prime": (I64, [I64, DBL, DBL, U64, U64]),
     "rip_theta": (U64, [DBL, DBL, U64, DBL, U64]),
