@@ -80,7 +80,7 @@ class ClockSampler:
             return
         self.proc = subprocess.Popen(
             ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-             "--format=csv,noheader,nounits", "-lms", "200"],
+             "--format=csv,noheader,nounits", "-lms", "100"],
             stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         self.t = threading.Thread(target=self._read, daemon=True)
         self.t.start()
@@ -236,7 +236,7 @@ def cpu_baseline(w, g, budget_s=30.0):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="lt20", choices=sorted(WORKLOADS))
@@ -284,12 +284,15 @@ def main():
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     total_sets, kern_ms, kern_n, st_tot = 0, 0.0, 0, np.zeros(8, np.uint64)
-    thetas = []
+    thetas, gen_ms, sel_ms = [], 0.0, 0.0
     for step in range(args.steps):
         pool.clear()
         seeds, rec = pool.imm(w["k"], w["eps"], 1.0, seed=seed_base + step)
         total_sets += rec.total_sets
         thetas.append(int(rec.theta))
+        nr = min(rec.num_rounds, 64)
+        gen_ms += rec.generate_ms + sum(rec.round_generate_ms[i] for i in range(nr))
+        sel_ms += rec.select_ms + sum(rec.round_select_ms[i] for i in range(nr))
         km, kn, _ = pool.timing()
         kern_ms += km
         kern_n += kn
@@ -381,6 +384,8 @@ def main():
             "clocks": clk,
             "gpu_launches": launches,
             "imm_ms_per_step": t_max / args.steps,
+            "host_split_ms_per_step": {"generate": gen_ms / args.steps,
+                                       "select": sel_ms / args.steps},
             "sets_per_step": total_sets / args.steps,
         }
         print(json.dumps(line))

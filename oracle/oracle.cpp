@@ -38,7 +38,9 @@
 //   IC edge e live for set s  <=>  coin(s, e) < thr[e]
 //   thr[e] = clamp(floor(w_e * 2^32), 0, 2^32-1)
 //   LT: first in-edge j of v (CSR order) with threshold < cum[j],
-//       cum[j] = clamp(floor((sum_{i<=j} w_i in double) * 2^32), 0, 2^32-1)
+//       W_i = floor(clamp(w_i, 0, 2) * 2^40)            (exact, 64-bit)
+//       cum[j] = min(min(sum_{i<=j} W_i, 2^41) >> 8, 2^32-1)
+//       (integer sums: any summation order gives the same thresholds)
 
 #include <algorithm>
 #include <cmath>
@@ -366,11 +368,15 @@ void orc_pack_ic(const float *w, uint64_t m, uint32_t *thr) {
 
 void orc_pack_lt(const uint64_t *index, uint32_t n, const float *w,
                  uint32_t *cum) {
+  const uint64_t CAP = 1ull << 41;
   for (uint32_t v = 0; v < n; ++v) {
-    double acc = 0.0;
+    uint64_t acc = 0;
     for (uint64_t e = index[v]; e < index[v + 1]; ++e) {
-      acc += (double)w[e];
-      cum[e] = prob_to_u32(acc);
+      double x = (double)w[e];
+      uint64_t W = !(x > 0.0) ? 0 : x >= 2.0 ? (2ull << 40) : (uint64_t)std::floor(x * 1099511627776.0);
+      acc = acc + W > CAP ? CAP : acc + W;
+      uint64_t c = acc >> 8;
+      cum[e] = c > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)c;
     }
   }
 }

@@ -39,9 +39,17 @@ struct DevMem {
   size_t bytes = 0;
 };
 
+struct PinnedMem;
+
 struct rip_ctx {
   std::vector<rip_graph *> graphs;  // owned: freed by rip_ctx_destroy
   std::vector<rip_pool *> pools;    // owned: freed by rip_ctx_destroy
+  // Device blocks released by graphs/pools, kept for reuse (a graph upload
+  // or a new pool then costs no cudaMalloc); counted in `used`.
+  std::vector<DevMem> cache;
+  size_t cached = 0;
+  PinnedMem *h_pairs = nullptr;  // mapped: dirty (vertex, count) pairs
+  PinnedMem *h_count = nullptr;  // counts at the start of a selection
   int device = 0;
   cudaStream_t stream = nullptr;
   int num_sms = 148;
@@ -77,27 +85,79 @@ static int set_err(rip_ctx *c, int code, const char *fmt, ...) {
     if (r_ != RIP_OK) return r_; \
   } while (0)
 
-static int dalloc(rip_ctx *c, DevMem &m, size_t bytes) {
-  if (m.p && m.bytes >= bytes) return RIP_OK;
-  bytes = std::max<size_t>(bytes, 256);
-  if (c->used - m.bytes + bytes > c->budget)
-    return set_err(c, RIP_ERR_NOMEM,
-                   "device budget exceeded: need %zu more bytes (used %zu of %zu)",
-                   bytes, c->used, c->budget);
-  void *p = nullptr;
-  cudaError_t e = cudaMalloc(&p, bytes);
-  if (e != cudaSuccess) {
-    cudaGetLastError();
-    return set_err(c, RIP_ERR_NOMEM, "cudaMalloc(%zu) failed: %s", bytes,
-                   cudaGetErrorString(e));
+static void cache_release_all(rip_ctx *c) {
+  if (!c->cache.empty()) cudaStreamSynchronize(c->stream);
+  for (DevMem &b : c->cache) {
+    cudaFree(b.p);
+    c->used -= b.bytes;
   }
-  if (m.p) {
+  c->cache.clear();
+  c->cached = 0;
+}
+
+// Returns a block to the context cache (or frees it when the cache is full).
+static void cache_put(rip_ctx *c, DevMem m) {
+  if (!m.p) return;
+  const size_t limit = c->budget / 4;
+  if (m.bytes > limit) {
+    cudaStreamSynchronize(c->stream);
     cudaFree(m.p);
     c->used -= m.bytes;
+    return;
   }
-  m.p = p;
-  m.bytes = bytes;
-  c->used += bytes;
+  while (c->cached + m.bytes > limit && !c->cache.empty()) {
+    cudaStreamSynchronize(c->stream);
+    cudaFree(c->cache.front().p);
+    c->used -= c->cache.front().bytes;
+    c->cached -= c->cache.front().bytes;
+    c->cache.erase(c->cache.begin());
+  }
+  c->cache.push_back(m);
+  c->cached += m.bytes;
+}
+
+// Takes the smallest cached block of at least `bytes` (and at most twice that).
+static bool cache_take(rip_ctx *c, size_t bytes, DevMem &out) {
+  size_t best = c->cache.size();
+  for (size_t i = 0; i < c->cache.size(); ++i) {
+    const size_t b = c->cache[i].bytes;
+    if (b >= bytes && b <= 2 * bytes + (1u << 20) &&
+        (best == c->cache.size() || b < c->cache[best].bytes))
+      best = i;
+  }
+  if (best == c->cache.size()) return false;
+  out = c->cache[best];
+  c->cached -= out.bytes;
+  c->cache.erase(c->cache.begin() + best);
+  return true;
+}
+
+static int dalloc(rip_ctx *c, DevMem &m, size_t bytes) {
+  if (m.p && m.bytes >= bytes) return RIP_OK;
+  bytes = std::max<size_t>((bytes + 255) & ~(size_t)255, 256);
+  DevMem fresh;
+  if (!cache_take(c, bytes, fresh)) {
+    if (c->used + bytes > c->budget) cache_release_all(c);
+    if (c->used + bytes > c->budget)
+      return set_err(c, RIP_ERR_NOMEM,
+                     "device budget exceeded: need %zu more bytes (used %zu of %zu)",
+                     bytes, c->used, c->budget);
+    cudaError_t e = cudaMalloc(&fresh.p, bytes);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      cache_release_all(c);
+      e = cudaMalloc(&fresh.p, bytes);
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        return set_err(c, RIP_ERR_NOMEM, "cudaMalloc(%zu) failed: %s", bytes,
+                       cudaGetErrorString(e));
+      }
+    }
+    fresh.bytes = bytes;
+    c->used += bytes;
+  }
+  cache_put(c, m);
+  m = fresh;
   return RIP_OK;
 }
 
@@ -111,19 +171,13 @@ static int dgrow(rip_ctx *c, DevMem &m, size_t bytes, size_t keep) {
                           cudaMemcpyDeviceToDevice, c->stream));
     CK(c, cudaStreamSynchronize(c->stream));
   }
-  if (m.p) {
-    cudaFree(m.p);
-    c->used -= m.bytes;
-  }
+  cache_put(c, m);
   m = n;
   return RIP_OK;
 }
 
 static void dfree(rip_ctx *c, DevMem &m) {
-  if (m.p) {
-    cudaFree(m.p);
-    c->used -= m.bytes;
-  }
+  cache_put(c, m);
   m = DevMem{};
 }
 
@@ -205,6 +259,9 @@ int rip_ctx_destroy(rip_ctx *c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   while (!c->pools.empty()) rip_pool_destroy(c->pools.back());
   while (!c->graphs.empty()) rip_graph_destroy(c->graphs.back());
+  cache_release_all(c);
+  delete c->h_pairs;
+  delete c->h_count;
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -411,7 +468,6 @@ struct rip_pool {
   // selection state
   DevMem count, inv_off, inv_cur, inv, covered, dirty_bits, dirty_list, pairs,
       scan_sums;
-  PinnedMem h_pairs, h_count;
   std::vector<uint32_t> last_counts;
   bool have_last_counts = false;
   // timing of sampler kernels (CUDA events on the context stream)
@@ -1065,8 +1121,11 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
   std::vector<uint32_t> &hcount = p->last_counts;
   hcount.resize(n);
   // mapped: [count u32, pad][n pairs]; the gather kernel writes it directly
-  TRY(p->h_pairs.ensure(c, 16 + sizeof(uint2) * (size_t)n, true));
-  TRY(p->h_count.ensure(c, sizeof(uint32_t) * (size_t)n));
+  if (!c->h_pairs) c->h_pairs = new PinnedMem();
+  if (!c->h_count) c->h_count = new PinnedMem();
+  TRY(c->h_pairs->ensure(c, 16 + sizeof(uint2) * (size_t)n, true));
+  TRY(c->h_count->ensure(c, sizeof(uint32_t) * (size_t)n));
+  PinnedMem &h_pairs = *c->h_pairs, &h_count = *c->h_count;
 
   uint64_t uncovered = S;
   std::vector<uint32_t> out_seeds;
@@ -1075,13 +1134,33 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
   // Applies the dirty (vertex, count) list of the last cover step to hcount.
   // After a cover step: the dirty (vertex, count) pairs go straight to mapped
   // host memory; one synchronisation, then the host mirror is patched.
-  auto sync_dirty = [&]() -> int {
-    unsigned char *hb = static_cast<unsigned char *>(p->h_pairs.p);
-    unsigned char *db = static_cast<unsigned char *>(p->h_pairs.dev);
+  // Initial counts: the heap's keys, and |sets containing v| (the length of
+  // v's inverted list) for sizing each pick's cover grid.
+  CK(c, cudaMemcpyAsync(h_count.p, p->count.p, sizeof(uint32_t) * (size_t)n,
+                        cudaMemcpyDeviceToHost, c->stream));
+  CK(c, cudaStreamSynchronize(c->stream));
+  const uint32_t *init_count = static_cast<const uint32_t *>(h_count.p);
+  const double mean_len = S ? (double)P / (double)S : 1.0;
+  const int max_blocks = c->num_sms * 4;
+  auto cover = [&](uint32_t v, uint64_t gain) -> int {
+    C.vertex = v;
+    // 8 warps x 32 sets per block per pass
+    C.blocks = (int)std::min<uint64_t>(max_blocks, std::max<uint64_t>(1, (init_count[v] + 255) / 256));
+    launch_cover(C, c->stream);
+    CK(c, cudaGetLastError());
+    return (int)std::min<uint64_t>(max_blocks,
+                                   std::max<uint64_t>(1, (uint64_t)(gain * mean_len) / 2048 + 1));
+  };
+
+  // After a cover step: the dirty (vertex, count) pairs go straight to mapped
+  // host memory; one synchronisation, then the host mirror is patched.
+  auto sync_dirty = [&](int gather_blocks) -> int {
+    unsigned char *hb = static_cast<unsigned char *>(h_pairs.p);
+    unsigned char *db = static_cast<unsigned char *>(h_pairs.dev);
     launch_gather_dirty(ptr<uint32_t>(p->dirty_list), &dm->dirty_n, n,
                         ptr<uint32_t>(p->count), ptr<uint32_t>(p->dirty_bits),
                         reinterpret_cast<uint2 *>(db + 16),
-                        reinterpret_cast<unsigned int *>(db), c->num_sms * 4, c->stream);
+                        reinterpret_cast<unsigned int *>(db), gather_blocks, c->stream);
     CK(c, cudaMemsetAsync(&dm->dirty_n, 0, sizeof(unsigned int), c->stream));
     CK(c, cudaStreamSynchronize(c->stream));
     const unsigned int dn = *reinterpret_cast<volatile unsigned int *>(hb);
@@ -1091,10 +1170,7 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
   };
 
   if (tiebreak == RIP_TIE_REF_HEAP) {
-    CK(c, cudaMemcpyAsync(p->h_count.p, p->count.p, sizeof(uint32_t) * (size_t)n,
-                          cudaMemcpyDeviceToHost, c->stream));
-    CK(c, cudaStreamSynchronize(c->stream));
-    std::memcpy(hcount.data(), p->h_count.p, sizeof(uint32_t) * (size_t)n);
+    std::memcpy(hcount.data(), h_count.p, sizeof(uint32_t) * (size_t)n);
     // InitHeapStorage + std::priority_queue(cmp, std::move(storage)), as the
     // reference builds its heap (streaming_find_most_influential.h:541-544;
     // counting.h:196-206): the same heap, built level-parallel
@@ -1121,10 +1197,7 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
       out_seeds.push_back(element.first);
       out_gains.push_back(element.second);
       if (out_seeds.size() == k) break;
-      C.vertex = element.first;
-      launch_cover(C, c->stream);
-      CK(c, cudaGetLastError());
-      TRY(sync_dirty());
+      TRY(sync_dirty(cover(element.first, element.second)));
     }
   } else {
     while (out_seeds.size() < k && uncovered != 0) {
@@ -1140,16 +1213,14 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
       out_seeds.push_back(v);
       out_gains.push_back(cnt);
       if (out_seeds.size() == k) break;
-      C.vertex = v;
-      launch_cover(C, c->stream);
-      CK(c, cudaGetLastError());
+      cover(v, cnt);
       CK(c, cudaMemsetAsync(&dm->dirty_n, 0, sizeof(unsigned int), c->stream));
       // the lowest-id path keeps no host mirror; dirty bits are reset below
     }
-    CK(c, cudaMemcpyAsync(p->h_count.p, p->count.p, sizeof(uint32_t) * (size_t)n,
+    CK(c, cudaMemcpyAsync(h_count.p, p->count.p, sizeof(uint32_t) * (size_t)n,
                           cudaMemcpyDeviceToHost, c->stream));
     CK(c, cudaStreamSynchronize(c->stream));
-    std::memcpy(hcount.data(), p->h_count.p, sizeof(uint32_t) * (size_t)n);
+    std::memcpy(hcount.data(), h_count.p, sizeof(uint32_t) * (size_t)n);
   }
   CK(c, cudaEventRecord(c->ev1, c->stream));
   CK(c, cudaStreamSynchronize(c->stream));

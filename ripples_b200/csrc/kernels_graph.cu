@@ -7,8 +7,10 @@
 // integer threshold and interleaved with the source id, so one aligned 8-byte
 // record serves an edge and the coin test is an integer compare:
 //   IC : thr = clamp(floor(w * 2^32), 0, 2^32-1)   live iff coin < thr
-//   LT : thr = clamp(floor((sum of in-weights up to this edge, in double,
-//                           CSR order) * 2^32), 0, 2^32-1)
+//   LT : thr = min(min(sum_{i<=e} W_i, 2^41) >> 8, 2^32-1) over the vertex's
+//        in-edges in CSR order, W_i = floor(clamp(w_i, 0, 2) * 2^40): exact
+//        64-bit fixed point, so the prefix sum may run in any order (here a
+//        warp-parallel scan) and still equal a left-to-right sum bit for bit
 // Offsets shrink to u32 (m < 2^32 is required).
 #include <atomic>
 
@@ -41,22 +43,47 @@ __global__ void pack_ic_kernel(const uint32_t *src, const float *w, uint64_t m,
                      : make_uint2(0u, 0u);
 }
 
-// One thread per vertex sums the in-weights serially, in double, in CSR order:
-// the same left-to-right sum the host-side restatement computes, so the
-// cumulative thresholds are bit-identical.  (A parallel scan would reassociate
-// the additions.)
+__device__ __forceinline__ uint64_t lt_fixed(float w) {
+  const double x = (double)w;
+  if (!(x > 0.0)) return 0ull;
+  if (x >= 2.0) return 2ull << 40;
+  return (uint64_t)floor(x * 1099511627776.0);  // exact: w has a 24-bit mantissa
+}
+
+__device__ __forceinline__ uint64_t sat_add(uint64_t a, uint64_t b) {
+  const uint64_t s = a + b;  // a, b <= 2^41: no wrap
+  return s > (1ull << 41) ? (1ull << 41) : s;
+}
+
+// One warp per vertex: coalesced 32-edge chunks, a saturating integer warp
+// scan per chunk, carried across chunks.
 __global__ void pack_lt_kernel(const uint64_t *index, const uint32_t *src,
                                const float *w, uint32_t n, uint64_t m,
                                uint64_t m_pad, uint2 *edges) {
-  const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t v = tid; v < n; v += stride) {
-    double acc = 0.0;
-    for (uint64_t e = index[v]; e < index[v + 1]; ++e) {
-      acc += (double)w[e];
-      edges[e] = make_uint2(src[e], prob_u32(acc));
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t v = gw; v < n; v += nw) {
+    const uint64_t beg = index[v], end = index[v + 1];
+    uint64_t carry = 0;
+    for (uint64_t base = beg; base < end; base += 32) {
+      const uint64_t e = base + lane;
+      uint64_t x = e < end ? lt_fixed(w[e]) : 0ull;
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const uint64_t y = __shfl_up_sync(0xFFFFFFFFu, x, d);
+        if (lane >= (uint32_t)d) x = sat_add(x, y);
+      }
+      x = sat_add(x, carry);
+      if (e < end) {
+        const uint64_t c = x >> 8;
+        edges[e] = make_uint2(src[e], c > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)c);
+      }
+      carry = __shfl_sync(0xFFFFFFFFu, x, 31);
     }
   }
+  const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t e = m + tid; e < m_pad; e += stride) edges[e] = make_uint2(0u, 0u);
 }
 
@@ -81,7 +108,7 @@ void launch_pack_lt(const uint64_t *index, const float *w, uint32_t n,
                     cudaStream_t stream) {
   count_launches(2);
   pack_off_kernel<<<1184, 256, 0, stream>>>(index, n, off);
-  pack_lt_kernel<<<1184, 128, 0, stream>>>(index, src, w, n, m, pad4(m) + 4,
+  pack_lt_kernel<<<2368, 256, 0, stream>>>(index, src, w, n, m, pad4(m) + 4,
                                            edges);
 }
 
