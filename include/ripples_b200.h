@@ -104,6 +104,22 @@ int rip_graph_info(const rip_graph *g, uint32_t *n, uint64_t *m, int *model);
 /* Copies the packed per-edge thresholds (m values) back to the host. */
 int rip_graph_thresholds(rip_graph *g, uint32_t *thr);
 
+/* Copies the graph's backward CSR (index u64[n+1], src u32[m]) to the host. */
+int rip_graph_export(rip_graph *g, uint64_t *index, uint32_t *src);
+
+/* Device-side R-MAT draws for graphs too large to build on the host:
+ * d_keys[j] = (dst << 32) | src of draw first+j, ~0 for a self-loop -- the same
+ * draws as rip_rmat_csr.  d_keys is caller-owned device memory (count u64). */
+int rip_rmat_keys_device(rip_ctx *ctx, uint32_t scale, uint64_t first,
+                         uint64_t count, double a, double b, double c,
+                         uint64_t seed, uint64_t *d_keys);
+/* Builds a packed graph on the device from m sorted, unique (dst << 32 | src)
+ * keys in device memory (no self-loops), with one of the RIP_WEIGHTS_* models
+ * computed on the device exactly as rip_make_weights computes them. */
+int rip_graph_from_keys(rip_ctx *ctx, const uint64_t *d_keys, uint64_t m,
+                        uint32_t n, int weights, uint64_t weight_seed, double lo,
+                        double hi, int model, rip_graph **out);
+
 /* ---- RRR pool --------------------------------------------------------------- */
 /* A device-resident, growable flat pool of RRR sets, addressed by set id
  * 0, 1, 2, ...  Replaces RRRsets = std::vector<std::vector<uint32_t>>
@@ -168,6 +184,12 @@ int rip_select(rip_pool *p, uint64_t num_sets, uint32_t k, int tiebreak,
  * update that followed its last-but-one seed.  For checking the update step
  * (the reference's known-answer test, test/cuda_find_most_influential.cc:84-167). */
 int rip_select_counts(rip_pool *p, uint32_t *counts);
+
+/* Diagnostic breakdown of the rip_select calls on this pool: out[0] ms in
+ * counting/indexing kernels + count download, out[1] ms building the heap,
+ * out[2] ms in the pick loop, out[3] heap pops, out[4] seeds picked,
+ * out[5] dirty (vertex, count) pairs applied, out[6] selections. */
+int rip_select_profile(rip_pool *p, double out[8]);
 
 /* Diagnostic: builds a heap of n random (vertex, count) entries, counts in
  * [0, max_count), with the library's level-parallel heap construction and with

@@ -77,6 +77,9 @@ SIGNATURES = {
     "rip_graph_destroy": (I32, [P]),
     "rip_graph_info": (I32, [P, ctypes.POINTER(U32), ctypes.POINTER(U64), ctypes.POINTER(I32)]),
     "rip_graph_thresholds": (I32, [P, P]),
+    "rip_graph_export": (I32, [P, P, P]),
+    "rip_rmat_keys_device": (I32, [P, U32, U64, U64, DBL, DBL, DBL, U64, P]),
+    "rip_graph_from_keys": (I32, [P, P, U64, U32, I32, U64, DBL, DBL, I32, PP]),
     "rip_pool_create": (I32, [P, P, PP]),
     "rip_pool_destroy": (I32, [P]),
     "rip_pool_clear": (I32, [P]),
@@ -90,6 +93,7 @@ SIGNATURES = {
     "rip_select": (I32, [P, U64, U32, I32, P, P, ctypes.POINTER(U32), ctypes.POINTER(DBL)]),
     "rip_select_counts": (I32, [P, P]),
     "rip_selftest_heap": (I32, [U64, U32, U64]),
+    "rip_select_profile": (I32, [P, P]),
     "rip_count": (I32, [P, U64, P]),
     "rip_imm": (I32, [P, P, U32, DBL, DBL, U64, I32, I32, P, ctypes.POINTER(U32),
                       ctypes.POINTER(ImmRecord)]),

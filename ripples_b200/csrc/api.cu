@@ -393,6 +393,101 @@ static void erase_ptr(std::vector<T *> &v, T *x) {
   v.erase(std::remove(v.begin(), v.end(), x), v.end());
 }
 
+// Packs index/src/weights already in device memory into a new graph.
+static int pack_device_csr(rip_ctx *c, const uint64_t *d_index, const uint32_t *d_src,
+                           const float *d_w, uint32_t n, uint64_t m, int model,
+                           rip_graph **out) {
+  rip_graph *g = new rip_graph();
+  g->ctx = c;
+  g->n = n;
+  g->m = m;
+  g->model = model;
+  const uint64_t m_pad = ((m + 3) & ~3ull) + 4;
+  int rc = dalloc(c, g->off, sizeof(uint32_t) * ((size_t)n + 1));
+  if (!rc) rc = dalloc(c, g->edges, sizeof(uint2) * m_pad);
+  if (!rc) {
+    if (model == RIP_MODEL_IC)
+      launch_pack_ic(d_index, d_w, n, m, ptr<uint32_t>(g->off), ptr<uint2>(g->edges), d_src,
+                     c->stream);
+    else
+      launch_pack_lt(d_index, d_w, n, m, ptr<uint32_t>(g->off), ptr<uint2>(g->edges), d_src,
+                     c->stream);
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess) rc = set_err(c, RIP_ERR_CUDA, "pack failed: %s", cudaGetErrorString(e));
+  }
+  if (rc) {
+    dfree(c, g->off);
+    dfree(c, g->edges);
+    delete g;
+    return rc;
+  }
+  c->graphs.push_back(g);
+  *out = g;
+  return RIP_OK;
+}
+
+extern "C" int rip_rmat_keys_device(rip_ctx *c, uint32_t scale, uint64_t first,
+                                    uint64_t count, double a, double b, double cc,
+                                    uint64_t seed, uint64_t *d_keys) {
+  if (!c || !d_keys || scale == 0 || scale > 31 || a < 0 || b < 0 || cc < 0 ||
+      a + b + cc > 1.0)
+    return set_err(c, RIP_ERR_INVALID, "rip_rmat_keys_device: bad arguments");
+  CK(c, cudaSetDevice(c->device));
+  launch_rmat_keys(scale, first, count, a, b, cc, seed,
+                   reinterpret_cast<unsigned long long *>(d_keys), c->stream);
+  CK(c, cudaGetLastError());
+  CK(c, cudaStreamSynchronize(c->stream));
+  return RIP_OK;
+}
+
+extern "C" int rip_graph_from_keys(rip_ctx *c, const uint64_t *d_keys, uint64_t m,
+                                   uint32_t n, int weights, uint64_t weight_seed, double lo,
+                                   double hi, int model, rip_graph **out) {
+  if (!c || !out || (m && !d_keys) || n == 0)
+    return set_err(c, RIP_ERR_INVALID, "rip_graph_from_keys: bad arguments");
+  if (model != RIP_MODEL_IC && model != RIP_MODEL_LT)
+    return set_err(c, RIP_ERR_INVALID, "rip_graph_from_keys: unknown model %d", model);
+  if (weights != RIP_WEIGHTS_UNIFORM && weights != RIP_WEIGHTS_LT_NORMALIZED &&
+      weights != RIP_WEIGHTS_WC)
+    return set_err(c, RIP_ERR_INVALID, "rip_graph_from_keys: unknown weight model %d", weights);
+  if (n >= 0xFFFFFFFFu || m >= 0xFFFFFFFCull)
+    return set_err(c, RIP_ERR_LIMIT, "graph too large: n=%u m=%llu", n, (unsigned long long)m);
+  CK(c, cudaSetDevice(c->device));
+  DevMem d_index, d_src, d_w;
+  int rc = dalloc(c, d_index, sizeof(uint64_t) * ((size_t)n + 1));
+  if (!rc) rc = dalloc(c, d_src, sizeof(uint32_t) * std::max<uint64_t>(m, 1));
+  if (!rc) rc = dalloc(c, d_w, sizeof(float) * std::max<uint64_t>(m, 1));
+  if (!rc) {
+    launch_csr_from_keys(reinterpret_cast<const unsigned long long *>(d_keys), m, n,
+                         ptr<uint64_t>(d_index), ptr<uint32_t>(d_src), c->stream);
+    launch_weights(weights, ptr<uint64_t>(d_index), n, weight_seed, lo, hi, ptr<float>(d_w),
+                   c->stream);
+    rc = pack_device_csr(c, ptr<uint64_t>(d_index), ptr<uint32_t>(d_src), ptr<float>(d_w), n,
+                         m, model, out);
+  }
+  dfree(c, d_index);
+  dfree(c, d_src);
+  dfree(c, d_w);
+  return rc;
+}
+
+extern "C" int rip_graph_export(rip_graph *g, uint64_t *index, uint32_t *src) {
+  if (!g || !index || (g->m && !src)) return RIP_ERR_INVALID;
+  rip_ctx *c = g->ctx;
+  std::vector<uint32_t> off(g->n + 1);
+  std::vector<uint2> rec(g->m);
+  CK(c, cudaMemcpyAsync(off.data(), g->off.p, sizeof(uint32_t) * (g->n + 1),
+                        cudaMemcpyDeviceToHost, c->stream));
+  if (g->m)
+    CK(c, cudaMemcpyAsync(rec.data(), g->edges.p, sizeof(uint2) * g->m,
+                          cudaMemcpyDeviceToHost, c->stream));
+  CK(c, cudaStreamSynchronize(c->stream));
+  for (uint64_t v = 0; v <= g->n; ++v) index[v] = off[v];
+  for (uint64_t e = 0; e < g->m; ++e) src[e] = rec[e].x;
+  return RIP_OK;
+}
+
 extern "C" int rip_graph_destroy(rip_graph *g) {
   if (!g) return RIP_ERR_INVALID;
   rip_ctx *c = g->ctx;
@@ -470,6 +565,10 @@ struct rip_pool {
       scan_sums;
   std::vector<uint32_t> last_counts;
   bool have_last_counts = false;
+  std::vector<std::pair<uint32_t, size_t>> heap_store;  // reused across selections
+  // selection profile: [0] count+index kernels and counts D2H, [1] heap build,
+  // [2] pick loop, [3] heap pops, [4] picks, [5] dirty pairs, [6] selections
+  double sel_prof[8] = {0};
   // timing of sampler kernels (CUDA events on the context stream)
   double kernel_ms = 0.0;
   uint64_t kernel_launches = 0;
@@ -533,6 +632,7 @@ extern "C" int rip_pool_clear(rip_pool *p) {
   CK(c, cudaStreamSynchronize(c->stream));
   p->num_sets = p->num_elems = 0;
   p->kernel_ms = p->select_kernel_ms = 0.0;
+  for (double &x : p->sel_prof) x = 0.0;
   p->kernel_launches = 0;
   p->have_last_counts = false;
   return RIP_OK;
@@ -841,6 +941,14 @@ static int sample_fused(rip_pool *p, uint64_t seed, uint64_t first,
 // Fused-sampler configuration (the autotuner's knobs): colour width 64, 128
 // or 256, number of CTA slots (0 = size from the budget) and frontier-log
 // capacity per slot (0 = default).  Takes effect at the next rip_sample.
+// Diagnostic breakdown of rip_select since the pool was created (see
+// rip_pool::sel_prof).
+extern "C" int rip_select_profile(rip_pool *p, double out[8]) {
+  if (!p || !out) return RIP_ERR_INVALID;
+  for (int i = 0; i < 8; ++i) out[i] = p->sel_prof[i];
+  return RIP_OK;
+}
+
 extern "C" int rip_pool_configure(rip_pool *p, uint32_t colors, uint32_t slots,
                                   uint32_t log_capacity) {
   if (!p) return RIP_ERR_INVALID;
@@ -989,6 +1097,7 @@ using RefQueue = std::priority_queue<HeapItem, std::vector<HeapItem>, CompareHea
 // reference.
 struct AdoptedQueue : RefQueue {
   explicit AdoptedQueue(std::vector<HeapItem> &&heap) { this->c = std::move(heap); }
+  std::vector<HeapItem> release() { return std::move(this->c); }
 };
 
 // Bit-identical to std::make_heap(v.begin(), v.end(), CompareHeap{}), built
@@ -1079,6 +1188,7 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
   *num_seeds = 0;
   if (f) *f = 0.0;
   CK(c, cudaEventRecord(c->ev0, c->stream));
+  const auto t_sel0 = clk::now();
   // 1. histogram, 2. vertex -> sets index
   TRY(count_sets(p, S));
   TRY(dalloc(c, p->inv_off, sizeof(uint64_t) * ((size_t)n + 1)));
@@ -1140,6 +1250,8 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
                         cudaMemcpyDeviceToHost, c->stream));
   CK(c, cudaStreamSynchronize(c->stream));
   const uint32_t *init_count = static_cast<const uint32_t *>(h_count.p);
+  p->sel_prof[0] += ms_since(t_sel0);
+  p->sel_prof[6] += 1;
   const double mean_len = S ? (double)P / (double)S : 1.0;
   const int max_blocks = c->num_sms * 4;
   auto cover = [&](uint32_t v, uint64_t gain) -> int {
@@ -1166,19 +1278,24 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
     const unsigned int dn = *reinterpret_cast<volatile unsigned int *>(hb);
     const uint2 *hp = reinterpret_cast<const uint2 *>(hb + 16);
     for (unsigned int i = 0; i < dn; ++i) hcount[hp[i].x] = hp[i].y;
+    p->sel_prof[5] += dn;
     return RIP_OK;
   };
 
   if (tiebreak == RIP_TIE_REF_HEAP) {
+    const auto t_h0 = clk::now();
     std::memcpy(hcount.data(), h_count.p, sizeof(uint32_t) * (size_t)n);
     // InitHeapStorage + std::priority_queue(cmp, std::move(storage)), as the
     // reference builds its heap (streaming_find_most_influential.h:541-544;
     // counting.h:196-206): the same heap, built level-parallel
-    std::vector<HeapItem> storage(n);
+    std::vector<HeapItem> storage = std::move(p->heap_store);
+    storage.resize(n);
 #pragma omp parallel for schedule(static)
     for (long long v = 0; v < (long long)n; ++v) storage[v] = {(uint32_t)v, hcount[v]};
     parallel_make_heap(storage);
     AdoptedQueue queue(std::move(storage));
+    p->sel_prof[1] += ms_since(t_h0);
+    const auto t_p0 = clk::now();
     while (out_seeds.size() < k && uncovered != 0) {
       std::pair<uint32_t, size_t> element;
       for (;;) {  // getNextSeed, streaming_find_most_influential.h:560-571
@@ -1186,6 +1303,7 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
           return set_err(c, RIP_ERR_STATE, "selection heap exhausted");
         element = queue.top();
         queue.pop();
+        p->sel_prof[3] += 1;
         if (element.second > hcount[element.first]) {
           element.second = hcount[element.first];
           queue.push(element);
@@ -1199,6 +1317,9 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
       if (out_seeds.size() == k) break;
       TRY(sync_dirty(cover(element.first, element.second)));
     }
+    p->sel_prof[2] += ms_since(t_p0);
+    p->sel_prof[4] += out_seeds.size();
+    p->heap_store = queue.release();
   } else {
     while (out_seeds.size() < k && uncovered != 0) {
       CK(c, cudaMemsetAsync(&dm->best, 0, sizeof(unsigned long long), c->stream));

@@ -182,6 +182,13 @@ ic_plain_kernel(DevGraph G, DevPool P, Key key, uint64_t first, uint32_t count,
   }
 }
 
+// One walk per warp.  Each step needs the chosen in-edge of the current
+// vertex: a 32-ary search over the cumulative thresholds (one probe per lane
+// per round, log32(in-degree) rounds), finishing with one 8-byte load per lane
+// so the lane that holds the pick also holds its source id.  The visited-bit
+// atomic of the picked vertex is issued before that vertex's offsets and
+// threshold are fetched, and its result is only consumed afterwards, so the
+// two round trips overlap.
 __global__ void __launch_bounds__(256)
 lt_walk_kernel(DevGraph G, DevPool P, Key key, uint64_t first, uint32_t count,
                const uint32_t *ids, unsigned int *next, uint32_t *bitmaps,
@@ -208,37 +215,43 @@ lt_walk_kernel(DevGraph G, DevPool P, Key key, uint64_t first, uint32_t count,
     uint32_t qlen = 1;
     bool overflow = false;
     unsigned long long set_exp = 0, set_edges = 0;
+    uint32_t t = lt_threshold(key, s, cur);
+    uint32_t lo = __ldg(G.off + cur), hi = __ldg(G.off + cur + 1);
     for (;;) {
       set_exp += (lane == 0);
-      const uint32_t t = lt_threshold(key, s, cur);
-      uint32_t lo = __ldg(G.off + cur), hi = __ldg(G.off + cur + 1);
       if (hi == lo) break;
-      set_edges += (lane == 0);
-      if (__ldg(&G.edges[hi - 1].y) <= t) break;  // total in-weight < threshold
-      // 32-ary search for the first edge whose cumulative threshold exceeds t.
+      // 32-ary search for the first edge whose cumulative threshold exceeds t
+      bool none = false;
       while (hi - lo > 32) {
         const uint32_t stride = (hi - lo + 31) / 32;
         const uint32_t p = min(lo + (lane + 1) * stride - 1, hi - 1);
         const bool pred = t < __ldg(&G.edges[p].y);
         const uint32_t bal = __ballot_sync(FULL, pred);
         set_edges += (lane == 0) ? 32 : 0;
+        if (bal == 0) {  // even the last edge's cumulative weight is <= t
+          none = true;
+          break;
+        }
         const uint32_t L = __ffs(bal) - 1;
         const uint32_t nlo = lo + L * stride;
         hi = min(hi, lo + (L + 1) * stride);
         lo = nlo;
       }
+      if (none) break;
       const uint32_t e = lo + lane;
-      const bool pred = e < hi && t < __ldg(&G.edges[e].y);
-      const uint32_t bal = __ballot_sync(FULL, pred);
+      uint2 rec = make_uint2(0u, 0u);
+      if (e < hi) rec = __ldg(&G.edges[e]);
+      const uint32_t bal = __ballot_sync(FULL, e < hi && t < rec.y);
       set_edges += (lane == 0) ? (hi - lo) : 0;
-      const uint32_t jsel = lo + __ffs(bal) - 1;
-      const uint32_t u = __ldg(&G.edges[jsel].x);
-      uint32_t seen = 0;
-      if (lane == 0) {
-        const uint32_t bit = 1u << (u & 31);
-        seen = atomicOr(&W.bm[u >> 5], bit) & bit;
-      }
-      seen = __shfl_sync(FULL, seen, 0);
+      if (bal == 0) break;  // no in-edge picked: the walk ends here
+      const uint32_t u = __shfl_sync(FULL, rec.x, __ffs(bal) - 1);
+      uint32_t old = 0;
+      const uint32_t bit = 1u << (u & 31);
+      if (lane == 0) old = atomicOr(&W.bm[u >> 5], bit);
+      // next step's inputs, fetched while the atomic is in flight
+      const uint32_t t2 = lt_threshold(key, s, u);
+      const uint32_t lo2 = __ldg(G.off + u), hi2 = __ldg(G.off + u + 1);
+      const uint32_t seen = __shfl_sync(FULL, old & bit, 0);
       if (seen) break;
       if (qlen + 1 > W.qcap) {
         if (lane == 0) W.bm[u >> 5] = 0u;
@@ -248,6 +261,9 @@ lt_walk_kernel(DevGraph G, DevPool P, Key key, uint64_t first, uint32_t count,
       if (lane == 0) W.q[qlen] = u;
       ++qlen;
       cur = u;
+      t = t2;
+      lo = lo2;
+      hi = hi2;
     }
     __syncwarp();
     if (finish_set(W, qlen, overflow, s, rel, P, F)) {

@@ -56,6 +56,20 @@ void launch_ic_fused(const FusedLaunch &L, cudaStream_t stream);
 // Resident fused CTAs per SM for a colour width (occupancy API).
 int fused_ctas_per_sm(uint32_t colors);
 
+// Synthetic graphs on the device (kernels_graphgen.cu).
+inline uint32_t prob_u32_host(double p) {
+  const double y = p * 4294967296.0;
+  if (!(y > 0.0)) return 0u;
+  if (y >= 4294967295.0) return 0xFFFFFFFFu;
+  return (uint32_t)(uint64_t)y;
+}
+void launch_rmat_keys(uint32_t scale, uint64_t first, uint64_t count, double a, double b,
+                      double c, uint64_t seed, unsigned long long *keys, cudaStream_t stream);
+void launch_csr_from_keys(const unsigned long long *keys, uint64_t m, uint32_t n,
+                          uint64_t *index, uint32_t *src, cudaStream_t stream);
+void launch_weights(int kind, const uint64_t *index, uint32_t n, uint64_t seed, double lo,
+                    double hi, float *w, cudaStream_t stream);
+
 // Graph packing.
 void launch_pack_ic(const uint64_t *index, const float *w, uint32_t n,
                     uint64_t m, uint32_t *off, uint2 *edges, const uint32_t *src,

@@ -165,6 +165,41 @@ class DeviceGraph:
             p._invalidate()
         self.h = None
 
+    @classmethod
+    def rmat_on_device(cls, ctx: Context, scale: int, num_edges: int, model: str,
+                       weights: int, seed: int = 0, weight_seed: int = 1, lo: float = 0.0,
+                       hi: float = 1.0, a: float = 0.57, b: float = 0.19,
+                       c: float = 0.19) -> "DeviceGraph":
+        """The graph HostGraph.rmat(...).with_weights(...) would build, built on
+        the device: R-MAT keys by the library, sort + unique by torch (input
+        plumbing), CSR + weights + packing by the library."""
+        import torch
+        dev = torch.device("cuda", torch.cuda.current_device())
+        keys = torch.empty(num_edges, dtype=torch.int64, device=dev)
+        check(lib.rip_rmat_keys_device(ctx.h, scale, 0, num_edges, a, b, c, seed,
+                                       ctypes.c_void_p(keys.data_ptr())),
+              "rip_rmat_keys_device", ctx.h)
+        keys = torch.unique(keys[keys >= 0])  # drop self-loops (~0), sort, dedup
+        torch.cuda.synchronize(dev)
+        h = ctypes.c_void_p()
+        check(lib.rip_graph_from_keys(ctx.h, ctypes.c_void_p(keys.data_ptr()), keys.numel(),
+                                      1 << scale, weights, weight_seed, lo, hi, MODELS[model],
+                                      ctypes.byref(h)), "rip_graph_from_keys", ctx.h)
+        m = keys.numel()
+        del keys
+        obj = cls.__new__(cls)
+        obj.ctx, obj.model, obj.n, obj.m, obj.h = ctx, model, 1 << scale, m, h
+        obj._pools = weakref.WeakSet()
+        ctx._children.add(obj)
+        return obj
+
+    def export(self) -> Tuple[np.ndarray, np.ndarray]:
+        idx = np.zeros(self.n + 1, dtype=np.uint64)
+        src = np.zeros(max(self.m, 1), dtype=np.uint32)
+        check(lib.rip_graph_export(self.h, _ptr(idx), _ptr(src)), "rip_graph_export",
+              self.ctx.h)
+        return idx, src[: self.m]
+
     def thresholds(self) -> np.ndarray:
         out = np.empty(self.m, dtype=np.uint32)
         check(lib.rip_graph_thresholds(self.h, _ptr(out)), "rip_graph_thresholds", self.ctx.h)
@@ -265,6 +300,12 @@ class Pool:
         self._chk(lib.rip_pool_timing(self.h, ctypes.byref(ms), ctypes.byref(n),
                                       ctypes.byref(sms)), "rip_pool_timing")
         return ms.value, n.value, sms.value
+
+    def select_profile(self) -> dict:
+        out = np.zeros(8, dtype=np.float64)
+        self._chk(lib.rip_select_profile(self.h, _ptr(out)), "rip_select_profile")
+        keys = ["prep_ms", "heap_ms", "picks_ms", "pops", "seeds", "dirty", "selections"]
+        return dict(zip(keys, out.tolist()))
 
     def count(self, num_sets: Optional[int] = None) -> np.ndarray:
         if num_sets is None:

@@ -265,3 +265,17 @@ def test_errors_are_reported(ctx):
     off, vtx = csr_of([[1, 7]])
     with pytest.raises(rb.RipError):
         p2.import_sets(off, vtx)
+
+
+@pytest.mark.parametrize("model,weights,lo,hi", [("IC", rb.WEIGHTS_UNIFORM, 0.0, 0.1),
+                                                 ("IC", rb.WEIGHTS_WC, 0.0, 1.0),
+                                                 ("LT", rb.WEIGHTS_LT_NORMALIZED, 0.0, 1.0)])
+def test_device_graph_construction_matches_host(ctx, model, weights, lo, hi):
+    scale, draws = 12, 16 << 12
+    hg = rb.HostGraph.rmat(scale, draws, seed=3).with_weights(weights, seed=4, lo=lo, hi=hi)
+    dg = rb.DeviceGraph.rmat_on_device(ctx, scale, draws, model, weights, seed=3,
+                                       weight_seed=4, lo=lo, hi=hi)
+    idx, src = dg.export()
+    assert np.array_equal(idx, hg.index) and np.array_equal(src, hg.src)
+    assert np.array_equal(dg.thresholds(), O.pack(model, hg.index, hg.weights))
+    dg.close()
