@@ -285,7 +285,7 @@ def main():
     ev0.record(stream)
     total_sets, kern_ms, kern_n, st_tot = 0, 0.0, 0, np.zeros(8, np.uint64)
     thetas, gen_ms, sel_ms = [], 0.0, 0.0
-    prof = {}
+    sel_prof = {}
     for step in range(args.steps):
         pool.clear()
         seeds, rec = pool.imm(w["k"], w["eps"], 1.0, seed=seed_base + step)
@@ -299,7 +299,7 @@ def main():
         kern_n += kn
         st_tot += pool.stats()
         for kk, vv in pool.select_profile().items():
-            prof[kk] = prof.get(kk, 0.0) + vv
+            sel_prof[kk] = sel_prof.get(kk, 0.0) + vv
     ev1.record(stream)
     torch.cuda.synchronize()
     barrier(world)
@@ -389,7 +389,7 @@ def main():
             "imm_ms_per_step": t_max / args.steps,
             "host_split_ms_per_step": {"generate": gen_ms / args.steps,
                                        "select": sel_ms / args.steps},
-            "select_profile_per_step": {kk: vv / args.steps for kk, vv in prof.items()},
+            "select_profile_per_step": {kk: vv / args.steps for kk, vv in sel_prof.items()},
             "sets_per_step": total_sets / args.steps,
         }
         print(json.dumps(line))
