@@ -39,6 +39,20 @@ struct DevMem {
   size_t bytes = 0;
 };
 
+// The reference's heap holds std::pair<vertex, size_t count> ordered by count
+// alone (CompareHeap, include/ripples/streaming_find_most_influential.h:410-418).
+// The heap algorithms only move elements and compare them with the
+// comparator, so an 8-byte {vertex, u32 count} item with the same comparison
+// yields the same sequence of heaps (counts never exceed the number of sets,
+// < 2^32), at half the memory.
+struct HeapItem {
+  uint32_t first;   // vertex
+  uint32_t second;  // count when pushed
+  bool operator==(const HeapItem &o) const { return first == o.first && second == o.second; }
+};
+struct CompareHeap {
+  bool operator()(const HeapItem &a, const HeapItem &b) const { return a.second < b.second; }
+};
 struct PinnedMem;
 
 struct rip_ctx {
@@ -540,6 +554,8 @@ struct PoolMeta {  // device-side bookkeeping block (one D2H reads it all)
   unsigned int fused_dirty;
   unsigned long long best;
   unsigned long long covered_sets;
+  unsigned int cover_done;
+  unsigned int pad2;
 };
 
 struct rip_pool {
@@ -565,7 +581,7 @@ struct rip_pool {
       scan_sums;
   std::vector<uint32_t> last_counts;
   bool have_last_counts = false;
-  std::vector<std::pair<uint32_t, size_t>> heap_store;  // reused across selections
+  std::vector<HeapItem> heap_store;  // heap storage reused across selections
   // selection profile: [0] count+index kernels and counts D2H, [1] heap build,
   // [2] pick loop, [3] heap pops, [4] picks, [5] dirty pairs, [6] selections
   double sel_prof[8] = {0};
@@ -1082,13 +1098,6 @@ extern "C" int rip_pool_import(rip_pool *p, const uint64_t *offsets,
 // selection
 // ---------------------------------------------------------------------------
 namespace {
-struct CompareHeap {  // include/ripples/streaming_find_most_influential.h:410-418
-  bool operator()(const std::pair<uint32_t, size_t> &a,
-                  const std::pair<uint32_t, size_t> &b) const {
-    return a.second < b.second;
-  }
-};
-using HeapItem = std::pair<uint32_t, size_t>;
 using RefQueue = std::priority_queue<HeapItem, std::vector<HeapItem>, CompareHeap>;
 
 // std::priority_queue that adopts an already-heapified container instead of
@@ -1133,7 +1142,7 @@ extern "C" int rip_selftest_heap(uint64_t n, uint32_t max_count, uint64_t seed) 
   uint64_t x = seed * 6364136223846793005ull + 1442695040888963407ull;
   for (uint64_t i = 0; i < n; ++i) {
     x = x * 6364136223846793005ull + 1442695040888963407ull;
-    a[i] = {(uint32_t)i, (size_t)((x >> 33) % (max_count ? max_count : 1))};
+    a[i] = {(uint32_t)i, (uint32_t)((x >> 33) % (max_count ? max_count : 1))};
   }
   b = a;
   std::make_heap(b.begin(), b.end(), CompareHeap{});
@@ -1226,7 +1235,12 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
   C.dirty_list = ptr<uint32_t>(p->dirty_list);
   C.dirty_n = &dm->dirty_n;
   C.covered_sets = &dm->covered_sets;
+  C.done = nullptr;
+  C.pairs = nullptr;
+  C.total_out = nullptr;
+  C.max_dirty = n;
   C.blocks = c->num_sms * 4;
+  CK(c, cudaMemsetAsync(&dm->cover_done, 0, sizeof(unsigned int), c->stream));
 
   std::vector<uint32_t> &hcount = p->last_counts;
   hcount.resize(n);
@@ -1254,26 +1268,37 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
   p->sel_prof[6] += 1;
   const double mean_len = S ? (double)P / (double)S : 1.0;
   const int max_blocks = c->num_sms * 4;
-  auto cover = [&](uint32_t v, uint64_t gain) -> int {
+  unsigned char *hb = static_cast<unsigned char *>(h_pairs.p);
+  unsigned char *db = static_cast<unsigned char *>(h_pairs.dev);
+  // One pick: mark + decrement; small picks gather their dirty pairs in the
+  // same launch (last-block epilogue), large ones in a wide gather launch.
+  // with_pairs = false (lowest-id mode): only the counters are reset.
+  auto cover = [&](uint32_t v, uint64_t gain, bool with_pairs) -> int {
     C.vertex = v;
     // 8 warps x 32 sets per block per pass
     C.blocks = (int)std::min<uint64_t>(max_blocks, std::max<uint64_t>(1, (init_count[v] + 255) / 256));
+    const uint64_t est_dirty = (uint64_t)(gain * mean_len);
+    const bool fused_gather = !with_pairs || est_dirty <= 16384;
+    C.done = &dm->cover_done;
+    C.pairs = (with_pairs && fused_gather) ? reinterpret_cast<uint2 *>(db + 16) : nullptr;
+    C.total_out = (with_pairs && fused_gather) ? reinterpret_cast<unsigned int *>(db) : nullptr;
+    if (with_pairs && !fused_gather) C.done = nullptr;  // the wide gather resets
     launch_cover(C, c->stream);
     CK(c, cudaGetLastError());
-    return (int)std::min<uint64_t>(max_blocks,
-                                   std::max<uint64_t>(1, (uint64_t)(gain * mean_len) / 2048 + 1));
+    if (with_pairs && !fused_gather) {
+      const int gb = (int)std::min<uint64_t>(max_blocks, est_dirty / 2048 + 1);
+      launch_gather_dirty(ptr<uint32_t>(p->dirty_list), &dm->dirty_n, n,
+                          ptr<uint32_t>(p->count), ptr<uint32_t>(p->dirty_bits),
+                          reinterpret_cast<uint2 *>(db + 16),
+                          reinterpret_cast<unsigned int *>(db), gb, c->stream);
+      CK(c, cudaMemsetAsync(&dm->dirty_n, 0, sizeof(unsigned int), c->stream));
+    }
+    return RIP_OK;
   };
 
-  // After a cover step: the dirty (vertex, count) pairs go straight to mapped
-  // host memory; one synchronisation, then the host mirror is patched.
-  auto sync_dirty = [&](int gather_blocks) -> int {
-    unsigned char *hb = static_cast<unsigned char *>(h_pairs.p);
-    unsigned char *db = static_cast<unsigned char *>(h_pairs.dev);
-    launch_gather_dirty(ptr<uint32_t>(p->dirty_list), &dm->dirty_n, n,
-                        ptr<uint32_t>(p->count), ptr<uint32_t>(p->dirty_bits),
-                        reinterpret_cast<uint2 *>(db + 16),
-                        reinterpret_cast<unsigned int *>(db), gather_blocks, c->stream);
-    CK(c, cudaMemsetAsync(&dm->dirty_n, 0, sizeof(unsigned int), c->stream));
+  // After a pick's launch(es): one synchronisation, then the host mirror is
+  // patched from the mapped pairs.
+  auto sync_dirty = [&]() -> int {
     CK(c, cudaStreamSynchronize(c->stream));
     const unsigned int dn = *reinterpret_cast<volatile unsigned int *>(hb);
     const uint2 *hp = reinterpret_cast<const uint2 *>(hb + 16);
@@ -1297,7 +1322,7 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
     p->sel_prof[1] += ms_since(t_h0);
     const auto t_p0 = clk::now();
     while (out_seeds.size() < k && uncovered != 0) {
-      std::pair<uint32_t, size_t> element;
+      HeapItem element;
       for (;;) {  // getNextSeed, streaming_find_most_influential.h:560-571
         if (queue.empty())
           return set_err(c, RIP_ERR_STATE, "selection heap exhausted");
@@ -1315,7 +1340,8 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
       out_seeds.push_back(element.first);
       out_gains.push_back(element.second);
       if (out_seeds.size() == k) break;
-      TRY(sync_dirty(cover(element.first, element.second)));
+      TRY(cover(element.first, element.second, true));
+      TRY(sync_dirty());
     }
     p->sel_prof[2] += ms_since(t_p0);
     p->sel_prof[4] += out_seeds.size();
@@ -1334,8 +1360,7 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
       out_seeds.push_back(v);
       out_gains.push_back(cnt);
       if (out_seeds.size() == k) break;
-      cover(v, cnt);
-      CK(c, cudaMemsetAsync(&dm->dirty_n, 0, sizeof(unsigned int), c->stream));
+      TRY(cover(v, cnt, false));
       // the lowest-id path keeps no host mirror; dirty bits are reset below
     }
     CK(c, cudaMemcpyAsync(h_count.p, p->count.p, sizeof(uint32_t) * (size_t)n,

@@ -109,6 +109,7 @@ inverted_kernel(DevPool P, uint64_t S, uint64_t *cursor, uint32_t *inv) {
 }
 
 __global__ void __launch_bounds__(256) cover_kernel(CoverLaunch C) {
+  __shared__ bool s_last;
   const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   const uint64_t lo = C.inv_off[C.vertex], hi = C.inv_off[C.vertex + 1];
@@ -145,6 +146,30 @@ __global__ void __launch_bounds__(256) cover_kernel(CoverLaunch C) {
   }
   newly = warp_sum_u64(newly);
   if (lane_id() == 0 && newly) atomicAdd(C.covered_sets, newly);
+  if (!C.done) return;
+  // The last block to finish publishes the pick: it gathers the dirty
+  // (vertex, count) pairs into mapped host memory (when asked to) and resets
+  // the per-pick counters, so a pick costs one launch and one sync.
+  __threadfence();  // each thread's dirty-list stores, before the block signals
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = atomicAdd(C.done, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  const uint32_t total = min(__ldcg(C.dirty_n), C.max_dirty);
+  if (C.pairs) {
+    for (uint32_t i = threadIdx.x; i < total; i += blockDim.x) {
+      const uint32_t u = __ldcg(C.dirty_list + i);
+      C.pairs[i] = make_uint2(u, __ldcg(C.count + u));
+      C.dirty_bits[u >> 5] = 0u;  // every set bit of this word is in the list
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (C.total_out) *C.total_out = C.pairs ? total : 0u;
+    *C.dirty_n = 0u;
+    *C.done = 0u;
+  }
 }
 
 // Writes the (vertex, count) pairs of the dirty list, and their number, to

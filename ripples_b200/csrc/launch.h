@@ -98,6 +98,12 @@ struct CoverLaunch {
   uint32_t *dirty_list;   // n entries
   unsigned int *dirty_n;
   unsigned long long *covered_sets;  // running total of newly covered sets
+  // Last-block epilogue (used when `done` is set): gather the dirty pairs into
+  // `pairs` / `total_out` when `pairs` is set, then zero dirty_n and done.
+  unsigned int *done;
+  uint2 *pairs;
+  unsigned int *total_out;
+  uint32_t max_dirty;
   int blocks;
 };
 void launch_cover(const CoverLaunch &C, cudaStream_t stream);
