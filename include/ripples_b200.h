@@ -169,6 +169,13 @@ int rip_pool_timing(rip_pool *p, double *sample_kernel_ms, uint64_t *launches,
 int rip_pool_configure(rip_pool *p, uint32_t colors, uint32_t slots,
                        uint32_t log_capacity);
 
+/* Edge-work budgets (in-edges read) after which a one-set-per-warp set, or a
+ * fused CTA batch, is handed to the grid-wide BFS that spreads each level's
+ * edge groups over the whole GPU (the heavy tail of IC sampling on skewed
+ * graphs); 0 disables the hand-over.  Defaults 2^18 and 2^23.  Results do not
+ * depend on these values. */
+int rip_pool_work_caps(rip_pool *p, uint64_t plain_cap, uint64_t fused_cap);
+
 /* ---- seed selection ------------------------------------------------------- */
 /* Greedy max coverage over sets [0, num_sets) of the pool.  Writes up to k
  * seeds (internal ids) and their marginal coverage, *num_seeds and

@@ -90,6 +90,7 @@ SIGNATURES = {
     "rip_pool_stats": (I32, [P, P]),
     "rip_pool_timing": (I32, [P, ctypes.POINTER(DBL), ctypes.POINTER(U64), ctypes.POINTER(DBL)]),
     "rip_pool_configure": (I32, [P, U32, U32, U32]),
+    "rip_pool_work_caps": (I32, [P, U64, U64]),
     "rip_select": (I32, [P, U64, U32, I32, P, P, ctypes.POINTER(U32), ctypes.POINTER(DBL)]),
     "rip_select_counts": (I32, [P, P]),
     "rip_selftest_heap": (I32, [U64, U32, U64]),

@@ -573,6 +573,12 @@ struct rip_pool {
   // flags, frontier log); all-zero between batches
   DevMem f_vis, f_pend, f_flag, f_log, f_order;
   uint32_t f_slots = 0, f_cw = 0, f_lcap = 0;
+  // grid-wide BFS slot for sets with very large edge work
+  DevMem w_vis, w_pend, w_flag, w_log, w_ent, w_small, w_scan;
+  uint32_t w_lcap = 0;
+  uint64_t cap_plain = 1ull << 18;  // in-edges per set before a warp hands it over
+  uint64_t cap_fused = 1ull << 23;  // in-edges per fused batch before handing over
+  uint64_t wide_sets = 0;           // sets grown by the wide path (diagnostic)
   uint32_t colors = 64;      // fused colour width (64/128/256)
   uint32_t fused_slots = 0;  // 0 = size from the budget
   uint32_t lcap_pref = 0;    // 0 = default frontier-log capacity
@@ -632,6 +638,8 @@ extern "C" int rip_pool_destroy(rip_pool *p) {
   DevMem *all[] = {&p->vtx,     &p->set_off,   &p->set_len,  &p->meta,
                    &p->scratch, &p->ids_a,     &p->ids_b,    &p->f_vis,
                    &p->f_pend,  &p->f_flag,    &p->f_log,    &p->f_order,
+                   &p->w_vis,   &p->w_pend,    &p->w_flag,   &p->w_log,
+                   &p->w_ent,   &p->w_small,   &p->w_scan,
                    &p->count,   &p->inv_off,   &p->inv_cur,  &p->inv,
                    &p->covered, &p->dirty_bits, &p->dirty_list, &p->pairs,
                    &p->scan_sums};
@@ -729,7 +737,12 @@ static uint32_t default_warps(rip_pool *p, uint32_t qcap) {
 }
 
 static int sample_fused(rip_pool *p, uint64_t seed, uint64_t first, uint32_t count);
+static int sample_wide(rip_pool *p, uint64_t seed, uint64_t first,
+                       const std::vector<uint32_t> &ids);
 
+// One set per warp (IC BFS / LT walk).  IC sets whose edge work exceeds the
+// per-set cap are handed to the grid-wide BFS; sets that outgrow the warp
+// queues or the pool are re-run with larger buffers.
 static int sample_warp_per_set(rip_pool *p, uint64_t seed, uint64_t first,
                                uint32_t count, const std::vector<uint32_t> *only) {
   rip_ctx *c = p->ctx;
@@ -743,7 +756,6 @@ static int sample_warp_per_set(rip_pool *p, uint64_t seed, uint64_t first,
   PoolMeta *dm = p->dmeta();
   const uint32_t *ids = nullptr;
   uint32_t todo = count;
-  bool use_a = true;
   if (only) {  // run just these indices (relative to first)
     todo = (uint32_t)only->size();
     if (todo == 0) return RIP_OK;
@@ -751,6 +763,8 @@ static int sample_warp_per_set(rip_pool *p, uint64_t seed, uint64_t first,
                           cudaMemcpyHostToDevice, c->stream));
     ids = ptr<uint32_t>(p->ids_b);
   }
+  const bool capped = g->model == RIP_MODEL_IC && p->cap_plain != 0;
+  std::vector<uint32_t> big, retry;
   for (int attempt = 0; attempt < 64; ++attempt) {
     CK(c, cudaMemsetAsync(&dm->fail_count, 0, sizeof(unsigned int), c->stream));
     CK(c, cudaMemsetAsync(&dm->next, 0, sizeof(unsigned int), c->stream));
@@ -767,8 +781,8 @@ static int sample_warp_per_set(rip_pool *p, uint64_t seed, uint64_t first,
     L.bm_words = p->bm_words;
     L.queues = ptr<uint32_t>(p->scratch) + (size_t)p->bm_words * p->warps;
     L.qcap = p->qcap;
-    L.F = FailList{ptr<uint32_t>(use_a ? p->ids_a : p->ids_b), &dm->fail_count,
-                   &dm->first_bad};
+    L.work_cap = capped ? p->cap_plain : 0;
+    L.F = FailList{ptr<uint32_t>(p->ids_a), &dm->fail_count, &dm->first_bad};
     L.st = Stats{dm->stats};
     L.threads = 256;
     const uint32_t active = std::min<uint32_t>(p->warps, todo);
@@ -788,31 +802,169 @@ static int sample_warp_per_set(rip_pool *p, uint64_t seed, uint64_t first,
     p->kernel_launches++;
     if (m.fail_count == 0) {
       p->num_elems = m.cursor;
-      return RIP_OK;
+      break;
     }
-    // Some sets did not fit.  Roll the bump pointer back to the end of the
-    // last stored set, grow what overflowed, and re-run only the failures.
+    // Roll the bump pointer back to the end of the last stored set.
     unsigned long long cur = std::min<unsigned long long>(m.cursor, m.first_bad);
-    CK(c, cudaMemcpyAsync(&dm->cursor, &cur, sizeof(cur), cudaMemcpyHostToDevice,
-                          c->stream));
+    CK(c, cudaMemcpyAsync(&dm->cursor, &cur, sizeof(cur), cudaMemcpyHostToDevice, c->stream));
     p->num_elems = cur;
+    std::vector<uint32_t> failed(m.fail_count);
+    CK(c, cudaMemcpyAsync(failed.data(), p->ids_a.p, sizeof(uint32_t) * m.fail_count,
+                          cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    retry.clear();
+    bool queue_overflow = false;
+    for (uint32_t f : failed) {
+      if (f & FAIL_BIG) big.push_back(f & ~FAIL_BIG);
+      else retry.push_back(f);
+    }
+    if (retry.empty()) break;
     if (m.first_bad != ~0ull) {
       double mean = m.stats[2] ? (double)m.stats[3] / (double)m.stats[2] : 16.0;
-      uint64_t need = cur + (uint64_t)(mean * 2.0 * m.fail_count) + 4096;
+      uint64_t need = cur + (uint64_t)(mean * 2.0 * retry.size()) + 4096;
       TRY(ensure_elems(p, std::max<uint64_t>(need, p->cap * 2)));
+    } else {
+      queue_overflow = true;
     }
-    if (p->qcap < g->n) {
-      // queue overflow is the other failure cause: widen the queues (fewer
-      // warps) so the worst case, a set holding every vertex, fits eventually
+    if (queue_overflow && p->qcap < g->n) {
+      // widen the queues (fewer warps) so the worst case, a set holding every
+      // vertex, fits eventually
       uint32_t nq = (uint32_t)std::min<uint64_t>(g->n, (uint64_t)p->qcap * 4);
       uint32_t nw = std::max<uint32_t>(8, std::min(default_warps(p, nq), p->warps));
       TRY(ensure_scratch(p, nw, nq));
     }
-    ids = ptr<uint32_t>(use_a ? p->ids_a : p->ids_b);
-    use_a = !use_a;
-    todo = m.fail_count;
+    CK(c, cudaMemcpyAsync(p->ids_b.p, retry.data(), sizeof(uint32_t) * retry.size(),
+                          cudaMemcpyHostToDevice, c->stream));
+    ids = ptr<uint32_t>(p->ids_b);
+    todo = (uint32_t)retry.size();
+    if (attempt == 63) return set_err(c, RIP_ERR_DEVICE, "sampler did not converge after retries");
   }
-  return set_err(c, RIP_ERR_DEVICE, "sampler did not converge after retries");
+  if (!big.empty()) {
+    std::sort(big.begin(), big.end());
+    TRY(sample_wide(p, seed, first, big));
+  }
+  return RIP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// grid-wide fused BFS for the heavy tail (IC)
+// ---------------------------------------------------------------------------
+static int ensure_wide(rip_pool *p, uint32_t lcap) {
+  rip_ctx *c = p->ctx;
+  const size_t n = p->g->n;
+  if (p->w_vis.p && p->w_lcap >= lcap) return RIP_OK;
+  TRY(dalloc(c, p->w_vis, n * 8));
+  TRY(dalloc(c, p->w_pend, n * 8));
+  TRY(dalloc(c, p->w_flag, n * 4));
+  TRY(dalloc(c, p->w_log, (size_t)lcap * 4));
+  // entries: beg, end, groups (u32) + mask (u64) + prefix (u64, lcap+1)
+  TRY(dalloc(c, p->w_ent, (size_t)lcap * 12 + (size_t)lcap * 8 + ((size_t)lcap + 1) * 8 + 256));
+  TRY(dalloc(c, p->w_small, 4096));
+  TRY(dalloc(c, p->w_scan, sizeof(uint64_t) * scan_block_sums_needed(lcap)));
+  CK(c, cudaMemsetAsync(p->w_vis.p, 0, n * 8, c->stream));
+  CK(c, cudaMemsetAsync(p->w_pend.p, 0, n * 8, c->stream));
+  CK(c, cudaMemsetAsync(p->w_flag.p, 0, n * 4, c->stream));
+  p->w_lcap = lcap;
+  return RIP_OK;
+}
+
+// Grows the sets first+ids[i] with the whole GPU, 64 at a time.
+static int sample_wide(rip_pool *p, uint64_t seed, uint64_t first,
+                       const std::vector<uint32_t> &ids) {
+  if (ids.empty()) return RIP_OK;
+  rip_ctx *c = p->ctx;
+  rip_graph *g = p->g;
+  uint32_t lcap = p->w_lcap ? p->w_lcap
+                            : (uint32_t)std::min<uint64_t>((uint64_t)g->n * 64, 1u << 22);
+  TRY(ensure_wide(p, lcap));
+  PoolMeta *dm = p->dmeta();
+  for (size_t b0 = 0; b0 < ids.size();) {
+    const uint32_t ncol = (uint32_t)std::min<size_t>(64, ids.size() - b0);
+    const size_t lc = p->w_lcap;
+    WideLaunch L;
+    L.G = g->view();
+    L.P = p->view();
+    L.key = make_key(seed);
+    L.F = FailList{nullptr, nullptr, &dm->first_bad};
+    L.ncol = ncol;
+    L.cw = 1;
+    L.vis = ptr<uint64_t>(p->w_vis);
+    L.pend = ptr<uint64_t>(p->w_pend);
+    L.pflag = ptr<uint32_t>(p->w_flag);
+    L.log = ptr<uint32_t>(p->w_log);
+    L.lcap = (uint32_t)lc;
+    unsigned char *ent = static_cast<unsigned char *>(p->w_ent.p);
+    L.ent_beg = reinterpret_cast<uint32_t *>(ent);
+    L.ent_end = reinterpret_cast<uint32_t *>(ent + lc * 4);
+    L.ent_groups = reinterpret_cast<uint32_t *>(ent + lc * 8);
+    L.ent_mask = reinterpret_cast<uint64_t *>(ent + ((lc * 12 + 7) & ~(size_t)7));
+    L.ent_prefix = reinterpret_cast<uint64_t *>(ent + ((lc * 12 + 7) & ~(size_t)7) + lc * 8);
+    unsigned char *sm = static_cast<unsigned char *>(p->w_small.p);
+    // small block: sets[64] u64 | starts[64] u64 | sizes[64] | fill[64] | tail | overflow | stats[4]
+    uint64_t *d_sets = reinterpret_cast<uint64_t *>(sm);
+    L.sets = d_sets;
+    L.starts = reinterpret_cast<unsigned long long *>(sm + 512);
+    L.sizes = reinterpret_cast<uint32_t *>(sm + 1024);
+    L.fill = reinterpret_cast<uint32_t *>(sm + 1280);
+    L.tail = reinterpret_cast<unsigned int *>(sm + 1536);
+    L.overflow = reinterpret_cast<unsigned int *>(sm + 1540);
+    L.batch_stats = reinterpret_cast<unsigned long long *>(sm + 1544);
+    uint64_t hsets[64];
+    for (uint32_t i = 0; i < ncol; ++i) hsets[i] = first + ids[b0 + i];
+    CK(c, cudaMemcpyAsync(d_sets, hsets, 8 * ncol, cudaMemcpyHostToDevice, c->stream));
+    CK(c, cudaMemsetAsync(sm + 1024, 0, 1576 - 1024, c->stream));
+    CK(c, cudaMemsetAsync(&dm->first_bad, 0xFF, sizeof(unsigned long long), c->stream));
+    launch_wide_seed(L, c->stream);
+    unsigned int h[2] = {0, 0};
+    CK(c, cudaMemcpyAsync(h, L.tail, 8, cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    uint32_t lo = 0, hi = std::min<uint32_t>(h[0], (uint32_t)lc), level = 1;
+    while (lo < hi && !h[1]) {
+      launch_wide_prepare(L, lo, hi, c->stream);
+      launch_exclusive_scan(L.ent_groups, L.ent_prefix, hi - lo, ptr<uint64_t>(p->w_scan),
+                            c->stream);
+      launch_wide_expand(L, hi - lo, level, c->num_sms * 8, c->stream);
+      CK(c, cudaGetLastError());
+      CK(c, cudaMemcpyAsync(h, L.tail, 8, cudaMemcpyDeviceToHost, c->stream));
+      CK(c, cudaStreamSynchronize(c->stream));
+      lo = hi;
+      hi = std::min<uint32_t>(h[0], (uint32_t)lc);
+      ++level;
+    }
+    if (h[1]) {
+      // the frontier log overflowed: vertices outside it may hold colours, so
+      // clear the whole slot and retry the batch with a longer log
+      CK(c, cudaMemsetAsync(p->w_vis.p, 0, (size_t)g->n * 8, c->stream));
+      CK(c, cudaMemsetAsync(p->w_pend.p, 0, (size_t)g->n * 8, c->stream));
+      CK(c, cudaMemsetAsync(p->w_flag.p, 0, (size_t)g->n * 4, c->stream));
+      if (lc >= (uint64_t)g->n * 64)
+        return set_err(c, RIP_ERR_DEVICE, "wide BFS log overflow at full size");
+      TRY(ensure_wide(p, (uint32_t)std::min<uint64_t>(lc * 4, (uint64_t)g->n * 64)));
+      continue;
+    }
+    launch_wide_reserve(L, c->stream);
+    CK(c, cudaMemcpyAsync(h, L.tail, 8, cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    const bool store = h[1] == 0;
+    launch_wide_emit(L, std::min<uint32_t>(h[0], (uint32_t)lc), store, c->stream);
+    if (!store) {  // pool full: grow it and redo the batch
+      PoolMeta m;
+      TRY(read_meta(p, m));
+      const unsigned long long cur = std::min<unsigned long long>(m.cursor, m.first_bad);
+      CK(c, cudaMemcpyAsync(&dm->cursor, &cur, sizeof(cur), cudaMemcpyHostToDevice, c->stream));
+      p->num_elems = cur;
+      TRY(ensure_elems(p, std::max<uint64_t>(p->cap * 2, cur + (1u << 20))));
+      continue;
+    }
+    launch_wide_commit(L, Stats{dm->stats}, c->stream);
+    CK(c, cudaGetLastError());
+    p->wide_sets += ncol;
+    b0 += ncol;
+  }
+  PoolMeta m;
+  TRY(read_meta(p, m));
+  p->num_elems = m.cursor;
+  return RIP_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -873,6 +1025,7 @@ static int sample_fused(rip_pool *p, uint64_t seed, uint64_t first,
   TRY(dalloc(c, p->ids_a, sizeof(uint32_t) * ((size_t)count / 64 + 2)));
   PoolMeta *dm = p->dmeta();
   std::vector<uint32_t> order;  // empty: identity over [0, count)
+  std::vector<uint32_t> big;    // sets of batches that outgrew their edge budget
   uint32_t todo = count;
   for (int attempt = 0; attempt < 4 && todo; ++attempt) {
     const uint32_t nb = (todo + colors - 1) / colors;
@@ -901,6 +1054,7 @@ static int sample_fused(rip_pool *p, uint64_t seed, uint64_t first,
     L.log = ptr<uint32_t>(p->f_log);
     L.lcap = p->f_lcap;
     L.dirty = &dm->fused_dirty;
+    L.work_cap = p->cap_fused;
     L.F = FailList{ptr<uint32_t>(p->ids_a), &dm->fail_count, &dm->first_bad};
     L.st = Stats{dm->stats};
     L.blocks = (int)std::min<uint32_t>(p->f_slots, nb);
@@ -917,7 +1071,8 @@ static int sample_fused(rip_pool *p, uint64_t seed, uint64_t first,
     const uint32_t claimed = std::min<uint32_t>(m.next, nb);
     if (m.fail_count == 0 && claimed == nb) {
       p->num_elems = m.cursor;
-      return RIP_OK;
+      todo = 0;
+      break;
     }
     unsigned long long cur = std::min<unsigned long long>(m.cursor, m.first_bad);
     CK(c, cudaMemcpyAsync(&dm->cursor, &cur, sizeof(cur), cudaMemcpyHostToDevice,
@@ -930,9 +1085,11 @@ static int sample_fused(rip_pool *p, uint64_t seed, uint64_t first,
     CK(c, cudaStreamSynchronize(c->stream));
     for (uint32_t b = claimed; b < nb; ++b) failed.push_back(b);
     std::vector<uint32_t> next_order;
-    for (uint32_t b : failed)
+    for (uint32_t fb : failed) {
+      const uint32_t b = fb & ~FAIL_BIG;
       for (uint32_t i = b * colors; i < std::min<uint32_t>((b + 1) * colors, todo); ++i)
-        next_order.push_back(order.empty() ? i : order[i]);
+        ((fb & FAIL_BIG) ? big : next_order).push_back(order.empty() ? i : order[i]);
+    }
     order.swap(next_order);
     todo = (uint32_t)order.size();
     if (m.first_bad != ~0ull) {
@@ -949,9 +1106,14 @@ static int sample_fused(rip_pool *p, uint64_t seed, uint64_t first,
       TRY(ensure_fused_scratch(p, ns, cw, nl));
     }
   }
-  if (todo == 0) return RIP_OK;
-  // Whatever still failed runs set by set (same sets, bit for bit).
-  return sample_warp_per_set(p, seed, first, todo, &order);
+  // Whatever still failed runs set by set (same sets, bit for bit); sets of
+  // batches that outgrew their edge budget are grown by the whole GPU.
+  if (todo) TRY(sample_warp_per_set(p, seed, first, todo, &order));
+  if (!big.empty()) {
+    std::sort(big.begin(), big.end());
+    TRY(sample_wide(p, seed, first, big));
+  }
+  return RIP_OK;
 }
 
 // Fused-sampler configuration (the autotuner's knobs): colour width 64, 128
@@ -962,6 +1124,15 @@ static int sample_fused(rip_pool *p, uint64_t seed, uint64_t first,
 extern "C" int rip_select_profile(rip_pool *p, double out[8]) {
   if (!p || !out) return RIP_ERR_INVALID;
   for (int i = 0; i < 8; ++i) out[i] = p->sel_prof[i];
+  return RIP_OK;
+}
+
+// Edge-work budgets before a warp (plain) or a CTA batch (fused) hands its
+// set(s) to the grid-wide BFS; 0 disables the hand-over.
+extern "C" int rip_pool_work_caps(rip_pool *p, uint64_t plain_cap, uint64_t fused_cap) {
+  if (!p) return RIP_ERR_INVALID;
+  p->cap_plain = plain_cap;
+  p->cap_fused = fused_cap;
   return RIP_OK;
 }
 

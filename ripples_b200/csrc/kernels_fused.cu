@@ -50,7 +50,7 @@ ic_fused_kernel(FusedLaunch L) {
   __shared__ uint32_t s_size[W];
   __shared__ uint32_t s_fill[W];
   __shared__ uint32_t s_batch, s_ncol, s_tail, s_overflow;
-  __shared__ unsigned long long s_base;
+  __shared__ unsigned long long s_base, s_work;
 
   const uint32_t tid = threadIdx.x, lane = lane_id(), wid = tid >> 5;
   const uint32_t slot = blockIdx.x;
@@ -70,6 +70,7 @@ ic_fused_kernel(FusedLaunch L) {
       s_batch = atomicAdd(L.next, 1u);
       s_tail = 0;
       s_overflow = 0;
+      s_work = 0;
     }
     __syncthreads();
     const uint32_t b = s_batch;
@@ -127,6 +128,7 @@ ic_fused_kernel(FusedLaunch L) {
             for (int w = 0; w < CW; ++w) pc += __popcll(mask[w]);
             b_exp += 1;
             b_edges += end - beg;
+            if (L.work_cap) atomicAdd(&s_work, (unsigned long long)(end - beg));
             b_sexp += pc;
             b_sedges += (unsigned long long)pc * (end - beg);
           }
@@ -223,9 +225,11 @@ ic_fused_kernel(FusedLaunch L) {
       lvl_start = lvl_end;
       lvl_end = min(s_tail, lcap);
       ++level;
+      // a batch that outgrows its edge budget goes to the grid-wide BFS
+      if (tid == 0 && L.work_cap && s_work > L.work_cap && !s_overflow) s_overflow = 3;
       __syncthreads();
     }
-    if (s_overflow) {
+    if (s_overflow == 1) {
       // Abandon: the scratch may now hold colours of vertices that never
       // reached the log.  Record the batch, mark the slot dirty and stop.
       if (tid == 0) {
@@ -235,7 +239,7 @@ ic_fused_kernel(FusedLaunch L) {
       break;
     }
     // ---- compaction into the pool ----------------------------------------
-    if (tid == 0) {
+    if (tid == 0 && s_overflow == 0) {
       unsigned long long tot = 0;
       for (uint32_t c = 0; c < ncol; ++c) tot += s_size[c];
       const unsigned long long base = atomicAdd(L.P.cursor, tot);
@@ -264,10 +268,12 @@ ic_fused_kernel(FusedLaunch L) {
       }
     }
     const uint32_t tail = min(s_tail, lcap);
+    const bool aborted = s_overflow == 3;  // frontier left unexpanded: clear pend too
     for (uint32_t i = tid; i < tail; i += FUSED_THREADS) {
       const uint32_t v = log[i];
 #pragma unroll
       for (int w = 0; w < CW; ++w) {
+        if (aborted) pend[(size_t)v * CW + w] = 0ull;
         uint64_t mm = atomicExch((unsigned long long *)&vis[(size_t)v * CW + w], 0ull);
         while (mm && store) {
           const int bi = __ffsll((long long)mm) - 1;
@@ -286,7 +292,7 @@ ic_fused_kernel(FusedLaunch L) {
         n_sets += ncol;
         n_elems += tot;
       } else {
-        L.F.ids[atomicAdd(L.F.count, 1u)] = b;
+        L.F.ids[atomicAdd(L.F.count, 1u)] = aborted ? (b | FAIL_BIG) : b;
       }
     }
     __syncthreads();

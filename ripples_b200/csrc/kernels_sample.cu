@@ -42,7 +42,7 @@ struct WarpCtx {
 // warp's bitmap.  Returns true when the set was stored.
 __device__ bool finish_set(const WarpCtx &W, uint32_t qlen, bool overflow,
                            uint64_t s, uint32_t rel, const DevPool &P,
-                           const FailList &F) {
+                           const FailList &F, bool big = false) {
   const uint32_t lane = lane_id();
   bool stored = false;
   if (!overflow) {
@@ -61,7 +61,7 @@ __device__ bool finish_set(const WarpCtx &W, uint32_t qlen, bool overflow,
     }
   }
   for (uint32_t i = lane; i < qlen; i += 32) W.bm[W.q[i] >> 5] = 0u;
-  if (!stored && lane == 0) F.ids[atomicAdd(F.count, 1u)] = rel;
+  if (!stored && lane == 0) F.ids[atomicAdd(F.count, 1u)] = big ? (rel | FAIL_BIG) : rel;
   __syncwarp();
   return stored;
 }
@@ -72,7 +72,7 @@ __global__ void __launch_bounds__(256)
 ic_plain_kernel(DevGraph G, DevPool P, Key key, uint64_t first, uint32_t count,
                 const uint32_t *ids, unsigned int *next, uint32_t *bitmaps,
                 uint64_t bm_words, uint32_t *queues, uint32_t qcap,
-                FailList F, Stats st) {
+                uint64_t work_cap, FailList F, Stats st) {
   const uint32_t lane = lane_id();
   const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   WarpCtx W{bitmaps + w * bm_words, queues + w * (uint64_t)qcap, qcap};
@@ -92,8 +92,8 @@ ic_plain_kernel(DevGraph G, DevPool P, Key key, uint64_t first, uint32_t count,
     }
     __syncwarp();
     uint32_t qlen = 1, head = 0;
-    bool overflow = false;
-    unsigned long long set_exp = 0, set_edges = 0;
+    bool overflow = false, big = false;
+    unsigned long long set_exp = 0, set_edges = 0, warp_edges = 0;
 
     while (head < qlen && !overflow) {
       const uint32_t take = min(32u, qlen - head);
@@ -108,6 +108,12 @@ ic_plain_kernel(DevGraph G, DevPool P, Key key, uint64_t first, uint32_t count,
       set_exp += (lane == 0) ? take : 0;
       const uint32_t incl = warp_incl_scan(ng);
       const uint32_t total = __shfl_sync(FULL, incl, 31);
+      warp_edges += (unsigned long long)total * 4;
+      if (work_cap && warp_edges > work_cap) {
+        // too much edge work for one warp: leave the set to the grid-wide BFS
+        overflow = big = true;
+        break;
+      }
       for (uint32_t base = 0; base < total && !overflow; base += 32) {
         const uint32_t j = base + lane;
         const bool valid = j < total;
@@ -161,7 +167,7 @@ ic_plain_kernel(DevGraph G, DevPool P, Key key, uint64_t first, uint32_t count,
       }
       head += take;
     }
-    if (finish_set(W, qlen, overflow, s, rel, P, F)) {
+    if (finish_set(W, qlen, overflow, s, rel, P, F, big)) {
       n_sets += (lane == 0);
       n_elems += (lane == 0) ? qlen : 0;
       n_exp += set_exp;
@@ -291,7 +297,7 @@ void launch_ic_plain(const SampleLaunch &L, cudaStream_t stream) {
   count_launches(1);
   ic_plain_kernel<<<L.blocks, L.threads, 0, stream>>>(
       L.G, L.P, L.key, L.first, L.count, L.ids, L.next, L.bitmaps, L.bm_words,
-      L.queues, L.qcap, L.F, L.st);
+      L.queues, L.qcap, L.work_cap, L.F, L.st);
 }
 
 void launch_lt_walk(const SampleLaunch &L, cudaStream_t stream) {

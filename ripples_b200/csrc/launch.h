@@ -11,21 +11,26 @@ namespace rip {
 uint64_t launch_counter();
 void count_launches(uint64_t n);
 
+// Failure ids carry this bit when a set (or fused batch) was abandoned for
+// exceeding its edge-work cap rather than for lack of room.
+constexpr uint32_t FAIL_BIG = 0x80000000u;
+
 struct SampleLaunch {
-  DevGraph G;
-  DevPool P;
-  Key key;
-  uint64_t first;       // set id of the launch's first set (== pool set index)
-  uint32_t count;       // number of set indices to process
-  const uint32_t *ids;  // optional list of indices relative to `first`
-  unsigned int *next;   // work counter (zeroed by the host)
-  uint32_t *bitmaps;
-  uint64_t bm_words;
-  uint32_t *queues;
-  uint32_t qcap;
-  FailList F;
-  Stats st;
-  int blocks, threads;
+  DevGraph G{};
+  DevPool P{};
+  Key key{};
+  uint64_t first = 0;        // set id of the launch's first set (== pool set index)
+  uint32_t count = 0;        // number of set indices to process
+  const uint32_t *ids = nullptr;  // optional list of indices relative to `first`
+  unsigned int *next = nullptr;   // work counter (zeroed by the host)
+  uint32_t *bitmaps = nullptr;
+  uint64_t bm_words = 0;
+  uint32_t *queues = nullptr;
+  uint32_t qcap = 0;
+  uint64_t work_cap = 0;     // IC: abandon a set after this many in-edges (0 = none)
+  FailList F{};
+  Stats st{};
+  int blocks = 0, threads = 0;
 };
 
 void launch_ic_plain(const SampleLaunch &L, cudaStream_t stream);
@@ -48,10 +53,39 @@ struct FusedLaunch {
   uint32_t *log;         // per slot: lcap frontier-log entries
   uint32_t lcap;
   unsigned int *dirty;   // slots abandoned with scratch left dirty
+  uint64_t work_cap = 0; // abandon a batch after this many in-edges (0 = none)
   FailList F;            // failed batch indices
   Stats st;
   int blocks;            // slots
 };
+
+// Grid-wide fused BFS for sets with very large edge work (kernels_wide.cu).
+struct WideLaunch {
+  DevGraph G{};
+  DevPool P{};
+  Key key{};
+  FailList F{};
+  const uint64_t *sets = nullptr;  // ncol set ids
+  uint32_t ncol = 0, cw = 1;
+  uint64_t *vis = nullptr, *pend = nullptr;  // n * cw words each
+  uint32_t *pflag = nullptr;                 // n level flags
+  uint32_t *log = nullptr;                   // lcap frontier-log entries
+  uint32_t lcap = 0;
+  unsigned int *tail = nullptr, *overflow = nullptr;
+  uint32_t *sizes = nullptr, *fill = nullptr;  // per colour
+  unsigned long long *starts = nullptr;         // per colour
+  uint32_t *ent_beg = nullptr, *ent_end = nullptr, *ent_groups = nullptr;  // lcap each
+  uint64_t *ent_mask = nullptr;    // lcap * cw
+  uint64_t *ent_prefix = nullptr;  // lcap + 1
+  unsigned long long *batch_stats = nullptr;  // [4]
+};
+void launch_wide_seed(const WideLaunch &L, cudaStream_t s);
+void launch_wide_prepare(const WideLaunch &L, uint32_t lo, uint32_t hi, cudaStream_t s);
+void launch_wide_expand(const WideLaunch &L, uint32_t nent, uint32_t level, int blocks,
+                        cudaStream_t s);
+void launch_wide_reserve(const WideLaunch &L, cudaStream_t s);
+void launch_wide_emit(const WideLaunch &L, uint32_t tail, bool store, cudaStream_t s);
+void launch_wide_commit(const WideLaunch &L, Stats st, cudaStream_t s);
 void launch_ic_fused(const FusedLaunch &L, cudaStream_t stream);
 // Resident fused CTAs per SM for a colour width (occupancy API).
 int fused_ctas_per_sm(uint32_t colors);

@@ -254,6 +254,9 @@ class Pool:
         self._chk(lib.rip_pool_configure(self.h, colors, slots, log_capacity),
                   "rip_pool_configure")
 
+    def work_caps(self, plain: int, fused: int) -> None:
+        self._chk(lib.rip_pool_work_caps(self.h, plain, fused), "rip_pool_work_caps")
+
     def clear(self) -> None:
         self._chk(lib.rip_pool_clear(self.h), "rip_pool_clear")
 

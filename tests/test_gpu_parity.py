@@ -279,3 +279,19 @@ def test_device_graph_construction_matches_host(ctx, model, weights, lo, hi):
     assert np.array_equal(idx, hg.index) and np.array_equal(src, hg.src)
     assert np.array_equal(dg.thresholds(), O.pack(model, hg.index, hg.weights))
     dg.close()
+
+
+@pytest.mark.parametrize("weights", [rb.WEIGHTS_UNIFORM, rb.WEIGHTS_WC])
+@pytest.mark.parametrize("sampler", [rb.SAMPLER_PLAIN, rb.SAMPLER_FUSED])
+def test_wide_path_bit_exact(ctx, weights, sampler):
+    """Tiny edge-work budgets send most sets to the grid-wide BFS; the sets
+    must not change."""
+    g = rb.HostGraph.rmat(12, 16 << 12, seed=8).with_weights(weights, seed=9, lo=0.0, hi=0.4)
+    dg, p = device_pool(ctx, g, "IC", 64)
+    p.work_caps(64, 256)
+    p.sample(3000, seed=12, sampler=sampler)
+    off, vtx = p.export()
+    ooff, ovtx, ost = oracle_sets(g, "IC", 12, 0, 3000)
+    assert_same_sets(off, vtx, ooff, ovtx)
+    st = p.stats()
+    assert st[2] == 3000 and st[4] == ost[0] and st[5] == ost[1]
