@@ -202,6 +202,8 @@ int rip_select_profile(rip_pool *p, double out[8]);
  * [0, max_count), with the library's level-parallel heap construction and with
  * std::make_heap; returns 1 when the two are identical element for element. */
 int rip_selftest_heap(uint64_t n, uint32_t max_count, uint64_t seed);
+/* Same check for the device heap build that rip_select uses. */
+int rip_selftest_heap_device(rip_ctx *ctx, uint64_t n, uint32_t max_count, uint64_t seed);
 
 /* Vertex occurrence counts over sets [0, num_sets) (n values), the first
  * step of selection (CountOccurrencies, include/ripples/counting.h:65-97). */

@@ -94,6 +94,7 @@ SIGNATURES = {
     "rip_select": (I32, [P, U64, U32, I32, P, P, ctypes.POINTER(U32), ctypes.POINTER(DBL)]),
     "rip_select_counts": (I32, [P, P]),
     "rip_selftest_heap": (I32, [U64, U32, U64]),
+    "rip_selftest_heap_device": (I32, [P, U64, U32, U64]),
     "rip_select_profile": (I32, [P, P]),
     "rip_count": (I32, [P, U64, P]),
     "rip_imm": (I32, [P, P, U32, DBL, DBL, U64, I32, I32, P, ctypes.POINTER(U32),

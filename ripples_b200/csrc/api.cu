@@ -554,8 +554,6 @@ struct PoolMeta {  // device-side bookkeeping block (one D2H reads it all)
   unsigned int fused_dirty;
   unsigned long long best;
   unsigned long long covered_sets;
-  unsigned int cover_done;
-  unsigned int pad2;
 };
 
 struct rip_pool {
@@ -583,11 +581,14 @@ struct rip_pool {
   uint32_t fused_slots = 0;  // 0 = size from the budget
   uint32_t lcap_pref = 0;    // 0 = default frontier-log capacity
   // selection state
-  DevMem count, inv_off, inv_cur, inv, covered, dirty_bits, dirty_list, pairs,
+  DevMem count, inv_off, inv_cur, inv, covered,
       scan_sums;
   std::vector<uint32_t> last_counts;
   bool have_last_counts = false;
   std::vector<HeapItem> heap_store;  // heap storage reused across selections
+  void *heap_registered = nullptr;   // heap_store's buffer while page-locked
+  size_t heap_registered_bytes = 0;
+  DevMem d_heap;                     // heap built on the device
   // selection profile: [0] count+index kernels and counts D2H, [1] heap build,
   // [2] pick loop, [3] heap pops, [4] picks, [5] dirty pairs, [6] selections
   double sel_prof[8] = {0};
@@ -639,11 +640,12 @@ extern "C" int rip_pool_destroy(rip_pool *p) {
                    &p->scratch, &p->ids_a,     &p->ids_b,    &p->f_vis,
                    &p->f_pend,  &p->f_flag,    &p->f_log,    &p->f_order,
                    &p->w_vis,   &p->w_pend,    &p->w_flag,   &p->w_log,
-                   &p->w_ent,   &p->w_small,   &p->w_scan,
+                   &p->w_ent,   &p->w_small,   &p->w_scan,   &p->d_heap,
                    &p->count,   &p->inv_off,   &p->inv_cur,  &p->inv,
-                   &p->covered, &p->dirty_bits, &p->dirty_list, &p->pairs,
+                   &p->covered,
                    &p->scan_sums};
   for (DevMem *m : all) dfree(c, *m);
+  if (p->heap_registered) cudaHostUnregister(p->heap_registered);
   erase_ptr(c->pools, p);
   delete p;
   return RIP_OK;
@@ -1306,6 +1308,37 @@ void parallel_make_heap(std::vector<HeapItem> &v) {
 }
 }  // namespace
 
+// Diagnostic: the device heap build against std::make_heap on n random
+// {vertex, count} items with counts in [0, max_count); 1 when identical.
+extern "C" int rip_selftest_heap_device(rip_ctx *c, uint64_t n, uint32_t max_count,
+                                        uint64_t seed) {
+  if (!c || n == 0 || n >= 0xFFFFFFFFull) return RIP_ERR_INVALID;
+  std::vector<uint32_t> cnt(n);
+  uint64_t x = seed * 6364136223846793005ull + 1442695040888963407ull;
+  for (uint64_t i = 0; i < n; ++i) {
+    x = x * 6364136223846793005ull + 1442695040888963407ull;
+    cnt[i] = (uint32_t)((x >> 33) % (max_count ? max_count : 1));
+  }
+  std::vector<HeapItem> ref(n), got(n);
+  for (uint64_t i = 0; i < n; ++i) ref[i] = {(uint32_t)i, cnt[i]};
+  std::make_heap(ref.begin(), ref.end(), CompareHeap{});
+  DevMem d_cnt, d_heap;
+  int rc = dalloc(c, d_cnt, 4 * n);
+  if (!rc) rc = dalloc(c, d_heap, 8 * n);
+  if (!rc) {
+    cudaMemcpyAsync(d_cnt.p, cnt.data(), 4 * n, cudaMemcpyHostToDevice, c->stream);
+    launch_make_heap(ptr<uint32_t>(d_cnt), (uint32_t)n, ptr<uint2>(d_heap), c->stream);
+    cudaMemcpyAsync(got.data(), d_heap.p, 8 * n, cudaMemcpyDeviceToHost, c->stream);
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess) rc = set_err(c, RIP_ERR_CUDA, "heap selftest: %s", cudaGetErrorString(e));
+  }
+  dfree(c, d_cnt);
+  dfree(c, d_heap);
+  if (rc) return rc;
+  return ref == got ? 1 : 0;
+}
+
 // Diagnostic: checks parallel_make_heap against std::make_heap on n random
 // counts drawn from [0, max_count) (many ties); returns 1 when identical.
 extern "C" int rip_selftest_heap(uint64_t n, uint32_t max_count, uint64_t seed) {
@@ -1388,10 +1421,6 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
   CK(c, cudaGetLastError());
   TRY(dalloc(c, p->covered, std::max<uint64_t>(S, 1)));
   CK(c, cudaMemsetAsync(p->covered.p, 0, std::max<uint64_t>(S, 1), c->stream));
-  const size_t dwords = ((size_t)n + 31) / 32;
-  TRY(dalloc(c, p->dirty_bits, sizeof(uint32_t) * dwords));
-  CK(c, cudaMemsetAsync(p->dirty_bits.p, 0, sizeof(uint32_t) * dwords, c->stream));
-  TRY(dalloc(c, p->dirty_list, sizeof(uint32_t) * (size_t)n));
   PoolMeta *dm = p->dmeta();
   CK(c, cudaMemsetAsync(&dm->dirty_n, 0, sizeof(unsigned int), c->stream));
   CK(c, cudaMemsetAsync(&dm->covered_sets, 0, sizeof(unsigned long long), c->stream));
@@ -1402,23 +1431,20 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
   C.inv = ptr<uint32_t>(p->inv);
   C.covered = ptr<uint8_t>(p->covered);
   C.count = ptr<uint32_t>(p->count);
-  C.dirty_bits = ptr<uint32_t>(p->dirty_bits);
-  C.dirty_list = ptr<uint32_t>(p->dirty_list);
   C.dirty_n = &dm->dirty_n;
   C.covered_sets = &dm->covered_sets;
-  C.done = nullptr;
   C.pairs = nullptr;
-  C.total_out = nullptr;
-  C.max_dirty = n;
+  C.max_dirty = 0;
   C.blocks = c->num_sms * 4;
-  CK(c, cudaMemsetAsync(&dm->cover_done, 0, sizeof(unsigned int), c->stream));
 
   std::vector<uint32_t> &hcount = p->last_counts;
   hcount.resize(n);
   // mapped: [count u32, pad][n pairs]; the gather kernel writes it directly
   if (!c->h_pairs) c->h_pairs = new PinnedMem();
   if (!c->h_count) c->h_count = new PinnedMem();
-  TRY(c->h_pairs->ensure(c, 16 + sizeof(uint2) * (size_t)n, true));
+  // mapped: the cover kernel writes its (vertex, count-after) reports here
+  const uint32_t max_reports = std::max<uint32_t>(n, 1u << 20);
+  TRY(c->h_pairs->ensure(c, 16 + sizeof(uint2) * (size_t)max_reports, true));
   TRY(c->h_count->ensure(c, sizeof(uint32_t) * (size_t)n));
   PinnedMem &h_pairs = *c->h_pairs, &h_count = *c->h_count;
 
@@ -1426,7 +1452,6 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
   std::vector<uint32_t> out_seeds;
   std::vector<uint64_t> out_gains;
 
-  // Applies the dirty (vertex, count) list of the last cover step to hcount.
   // After a cover step: the dirty (vertex, count) pairs go straight to mapped
   // host memory; one synchronisation, then the host mirror is patched.
   // Initial counts: the heap's keys, and |sets containing v| (the length of
@@ -1441,39 +1466,37 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
   const int max_blocks = c->num_sms * 4;
   unsigned char *hb = static_cast<unsigned char *>(h_pairs.p);
   unsigned char *db = static_cast<unsigned char *>(h_pairs.dev);
-  // One pick: mark + decrement; small picks gather their dirty pairs in the
-  // same launch (last-block epilogue), large ones in a wide gather launch.
-  // with_pairs = false (lowest-id mode): only the counters are reset.
-  auto cover = [&](uint32_t v, uint64_t gain, bool with_pairs) -> int {
+  unsigned int *h_dn = reinterpret_cast<unsigned int *>(hb);  // pinned landing for dirty_n
+  // One pick: mark + decrement in one launch; with_pairs also streams the
+  // (vertex, count-after) reports to mapped host memory.
+  auto cover = [&](uint32_t v, bool with_pairs) -> int {
     C.vertex = v;
     // 8 warps x 32 sets per block per pass
     C.blocks = (int)std::min<uint64_t>(max_blocks, std::max<uint64_t>(1, (init_count[v] + 255) / 256));
-    const uint64_t est_dirty = (uint64_t)(gain * mean_len);
-    const bool fused_gather = !with_pairs || est_dirty <= 16384;
-    C.done = &dm->cover_done;
-    C.pairs = (with_pairs && fused_gather) ? reinterpret_cast<uint2 *>(db + 16) : nullptr;
-    C.total_out = (with_pairs && fused_gather) ? reinterpret_cast<unsigned int *>(db) : nullptr;
-    if (with_pairs && !fused_gather) C.done = nullptr;  // the wide gather resets
+    C.pairs = with_pairs ? reinterpret_cast<uint2 *>(db + 16) : nullptr;
+    C.max_dirty = with_pairs ? max_reports : 0;
+    if (with_pairs) CK(c, cudaMemsetAsync(&dm->dirty_n, 0, sizeof(unsigned int), c->stream));
     launch_cover(C, c->stream);
     CK(c, cudaGetLastError());
-    if (with_pairs && !fused_gather) {
-      const int gb = (int)std::min<uint64_t>(max_blocks, est_dirty / 2048 + 1);
-      launch_gather_dirty(ptr<uint32_t>(p->dirty_list), &dm->dirty_n, n,
-                          ptr<uint32_t>(p->count), ptr<uint32_t>(p->dirty_bits),
-                          reinterpret_cast<uint2 *>(db + 16),
-                          reinterpret_cast<unsigned int *>(db), gb, c->stream);
-      CK(c, cudaMemsetAsync(&dm->dirty_n, 0, sizeof(unsigned int), c->stream));
-    }
     return RIP_OK;
   };
 
-  // After a pick's launch(es): one synchronisation, then the host mirror is
-  // patched from the mapped pairs.
+  // After a pick: one synchronisation, then the host mirror takes the minimum
+  // report per vertex (or the whole count array when the reports overflowed).
   auto sync_dirty = [&]() -> int {
+    CK(c, cudaMemcpyAsync(h_dn, &dm->dirty_n, sizeof(unsigned int), cudaMemcpyDeviceToHost,
+                          c->stream));
     CK(c, cudaStreamSynchronize(c->stream));
-    const unsigned int dn = *reinterpret_cast<volatile unsigned int *>(hb);
-    const uint2 *hp = reinterpret_cast<const uint2 *>(hb + 16);
-    for (unsigned int i = 0; i < dn; ++i) hcount[hp[i].x] = hp[i].y;
+    const unsigned int dn = *reinterpret_cast<volatile unsigned int *>(h_dn);
+    if (dn > max_reports) {
+      CK(c, cudaMemcpyAsync(hcount.data(), p->count.p, sizeof(uint32_t) * (size_t)n,
+                            cudaMemcpyDeviceToHost, c->stream));
+      CK(c, cudaStreamSynchronize(c->stream));
+    } else {
+      const uint2 *hp = reinterpret_cast<const uint2 *>(hb + 16);
+      for (unsigned int i = 0; i < dn; ++i)
+        if (hp[i].y < hcount[hp[i].x]) hcount[hp[i].x] = hp[i].y;
+    }
     p->sel_prof[5] += dn;
     return RIP_OK;
   };
@@ -1483,12 +1506,29 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
     std::memcpy(hcount.data(), h_count.p, sizeof(uint32_t) * (size_t)n);
     // InitHeapStorage + std::priority_queue(cmp, std::move(storage)), as the
     // reference builds its heap (streaming_find_most_influential.h:541-544;
-    // counting.h:196-206): the same heap, built level-parallel
+    // counting.h:196-206): the same heap, built level-parallel on the device
+    // and downloaded into page-locked storage the queue adopts as is.
     std::vector<HeapItem> storage = std::move(p->heap_store);
+    if (storage.capacity() < n || !p->heap_registered) {
+      if (p->heap_registered) cudaHostUnregister(p->heap_registered);
+      p->heap_registered = nullptr;
+      storage.reserve(n);
+      storage.resize(n);
+      if (cudaHostRegister(storage.data(), sizeof(HeapItem) * storage.capacity(), 0) ==
+          cudaSuccess) {
+        p->heap_registered = storage.data();
+        p->heap_registered_bytes = sizeof(HeapItem) * storage.capacity();
+      } else {
+        cudaGetLastError();  // pageable copy still works, only slower
+      }
+    }
     storage.resize(n);
-#pragma omp parallel for schedule(static)
-    for (long long v = 0; v < (long long)n; ++v) storage[v] = {(uint32_t)v, hcount[v]};
-    parallel_make_heap(storage);
+    TRY(dalloc(c, p->d_heap, sizeof(uint2) * (size_t)n));
+    launch_make_heap(ptr<uint32_t>(p->count), n, ptr<uint2>(p->d_heap), c->stream);
+    CK(c, cudaGetLastError());
+    CK(c, cudaMemcpyAsync(storage.data(), p->d_heap.p, sizeof(uint2) * (size_t)n,
+                          cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
     AdoptedQueue queue(std::move(storage));
     p->sel_prof[1] += ms_since(t_h0);
     const auto t_p0 = clk::now();
@@ -1511,8 +1551,10 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
       out_seeds.push_back(element.first);
       out_gains.push_back(element.second);
       if (out_seeds.size() == k) break;
-      TRY(cover(element.first, element.second, true));
+      const auto t_g0 = clk::now();
+      TRY(cover(element.first, true));
       TRY(sync_dirty());
+      p->sel_prof[7] += ms_since(t_g0);
     }
     p->sel_prof[2] += ms_since(t_p0);
     p->sel_prof[4] += out_seeds.size();
@@ -1531,7 +1573,7 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
       out_seeds.push_back(v);
       out_gains.push_back(cnt);
       if (out_seeds.size() == k) break;
-      TRY(cover(v, cnt, false));
+      TRY(cover(v, false));
       // the lowest-id path keeps no host mirror; dirty bits are reset below
     }
     CK(c, cudaMemcpyAsync(h_count.p, p->count.p, sizeof(uint32_t) * (size_t)n,

@@ -14,14 +14,18 @@
 // cover_kernel      after a pick: marks the seed's still-uncovered sets
 //                   covered and decrements the counts of their members
 //                   (UpdateCounters, include/ripples/counting.h:141-151),
-//                   recording each vertex whose count changed once in a dirty
-//                   list so the host heap can mirror the counts exactly.
+//                   reporting (vertex, count after) pairs straight to mapped
+//                   host memory so the host heap mirrors the counts exactly.
+// heap kernels      the selection max-heap built on the device, level by
+//                   level, element for element the one std::make_heap builds.
 // argmax_kernel     max count, lowest vertex id on ties (thrust::max_element,
 //                   src/gpu/find_most_influential.cc:65-72).
 //
 // All per-set loops use the same warp-level load balancing: a warp takes 32
 // sets, scans their lengths and walks the concatenated elements 32 at a time,
 // each lane finding its set with a 5-step shuffle search.
+#include <algorithm>
+
 #include "device.cuh"
 #include "launch.h"
 
@@ -109,7 +113,6 @@ inverted_kernel(DevPool P, uint64_t S, uint64_t *cursor, uint32_t *inv) {
 }
 
 __global__ void __launch_bounds__(256) cover_kernel(CoverLaunch C) {
-  __shared__ bool s_last;
   const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   const uint64_t lo = C.inv_off[C.vertex], hi = C.inv_off[C.vertex + 1];
@@ -126,67 +129,31 @@ __global__ void __launch_bounds__(256) cover_kernel(CoverLaunch C) {
           return s;
         },
         [&](uint64_t, uint32_t u, bool valid) {
+          // one leader per distinct vertex in the warp decrements and, when
+          // asked, reports the count it left; counts only fall during a pick,
+          // so the minimum of a vertex's reports is its count after the pick
           const uint32_t peers = __match_any_sync(FULL, u);
           const bool leader = valid && (__ffs(peers) - 1) == (int)lane_id();
-          bool fresh = false;
+          uint32_t after = 0;
           if (leader) {
-            atomicSub(C.count + u, (uint32_t)__popc(peers));
-            const uint32_t bit = 1u << (u & 31);
-            fresh = !(atomicOr(C.dirty_bits + (u >> 5), bit) & bit);
+            const uint32_t k = (uint32_t)__popc(peers);
+            after = atomicSub(C.count + u, k) - k;
           }
-          const uint32_t bal = __ballot_sync(FULL, fresh);
-          if (bal) {
-            unsigned int b = 0;
-            if (lane_id() == (uint32_t)(__ffs(bal) - 1))
-              b = atomicAdd(C.dirty_n, (unsigned int)__popc(bal));
-            b = __shfl_sync(FULL, b, __ffs(bal) - 1);
-            if (fresh) C.dirty_list[b + __popc(bal & lanemask_lt())] = u;
+          if (C.pairs) {
+            const uint32_t bal = __ballot_sync(FULL, leader);
+            if (bal) {
+              unsigned int b = 0;
+              if (lane_id() == (uint32_t)(__ffs(bal) - 1))
+                b = atomicAdd(C.dirty_n, (unsigned int)__popc(bal));
+              b = __shfl_sync(FULL, b, __ffs(bal) - 1);
+              const uint32_t idx = b + __popc(bal & lanemask_lt());
+              if (leader && idx < C.max_dirty) C.pairs[idx] = make_uint2(u, after);
+            }
           }
         });
   }
   newly = warp_sum_u64(newly);
   if (lane_id() == 0 && newly) atomicAdd(C.covered_sets, newly);
-  if (!C.done) return;
-  // The last block to finish publishes the pick: it gathers the dirty
-  // (vertex, count) pairs into mapped host memory (when asked to) and resets
-  // the per-pick counters, so a pick costs one launch and one sync.
-  __threadfence();  // each thread's dirty-list stores, before the block signals
-  __syncthreads();
-  if (threadIdx.x == 0) s_last = atomicAdd(C.done, 1u) == gridDim.x - 1;
-  __syncthreads();
-  if (!s_last) return;
-  __threadfence();
-  const uint32_t total = min(__ldcg(C.dirty_n), C.max_dirty);
-  if (C.pairs) {
-    for (uint32_t i = threadIdx.x; i < total; i += blockDim.x) {
-      const uint32_t u = __ldcg(C.dirty_list + i);
-      C.pairs[i] = make_uint2(u, __ldcg(C.count + u));
-      C.dirty_bits[u >> 5] = 0u;  // every set bit of this word is in the list
-    }
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    if (C.total_out) *C.total_out = C.pairs ? total : 0u;
-    *C.dirty_n = 0u;
-    *C.done = 0u;
-  }
-}
-
-// Writes the (vertex, count) pairs of the dirty list, and their number, to
-// `pairs` / `total_out` -- mapped pinned host memory, so the host reads them
-// after one stream synchronisation.
-__global__ void gather_dirty_kernel(const uint32_t *list, const unsigned int *n,
-                                    uint32_t max_n, const uint32_t *count,
-                                    uint32_t *bits, uint2 *pairs,
-                                    unsigned int *total_out) {
-  const uint32_t total = min(*n, max_n);
-  if (blockIdx.x == 0 && threadIdx.x == 0) *total_out = total;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total;
-       i += gridDim.x * blockDim.x) {
-    const uint32_t u = list[i];
-    pairs[i] = make_uint2(u, count[u]);
-    bits[u >> 5] = 0u;  // every set bit of this word is in the list too
-  }
 }
 
 __global__ void argmax_kernel(const uint32_t *count, uint32_t n,
@@ -294,7 +261,64 @@ scan_apply_kernel(const uint32_t *in, uint32_t n, const uint64_t *tile_sums,
   }
 }
 
+// libstdc++-compatible sift of make_heap: the hole at `hole` sinks to a leaf
+// along the larger child (the right one unless the left is strictly larger),
+// then `value` rises from there while its parent compares less.  Elements are
+// {vertex, count}; only counts are compared.
+__device__ void adjust_heap_dev(uint2 *h, int64_t hole, int64_t len, uint2 value) {
+  const int64_t top = hole;
+  int64_t child = hole;
+  while (child < (len - 1) / 2) {
+    child = 2 * (child + 1);
+    if (h[child].y < h[child - 1].y) child--;
+    h[hole] = h[child];
+    hole = child;
+  }
+  if ((len & 1) == 0 && child == (len - 2) / 2) {
+    child = 2 * (child + 1);
+    h[hole] = h[child - 1];
+    hole = child - 1;
+  }
+  int64_t parent = (hole - 1) / 2;
+  while (hole > top && h[parent].y < value.y) {
+    h[hole] = h[parent];
+    hole = parent;
+    parent = (hole - 1) / 2;
+  }
+  h[hole] = value;
+}
+
+// heap[v] = {v, count[v]}
+__global__ void heap_fill_kernel(const uint32_t *count, uint32_t n, uint2 *heap) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+    heap[v] = make_uint2(v, count[v]);
+}
+
+// make_heap's parents [lo, hi] (one depth) in parallel: disjoint subtrees.
+__global__ void heap_level_kernel(uint2 *heap, int64_t len, int64_t lo, int64_t hi) {
+  for (int64_t p = hi - (int64_t)(blockIdx.x * blockDim.x + threadIdx.x); p >= lo;
+       p -= (int64_t)gridDim.x * blockDim.x)
+    adjust_heap_dev(heap, p, len, heap[p]);
+}
+
 }  // namespace
+
+void launch_make_heap(const uint32_t *count, uint32_t n, uint2 *heap, cudaStream_t stream) {
+  count_launches(1);
+  heap_fill_kernel<<<592, 256, 0, stream>>>(count, n, heap);
+  const int64_t len = n;
+  if (len < 2) return;
+  const int64_t last_parent = (len - 2) / 2;
+  int dmax = 0;
+  while ((((int64_t)2) << dmax) - 1 <= last_parent) ++dmax;
+  for (int d = dmax; d >= 0; --d) {
+    const int64_t lo = (((int64_t)1) << d) - 1;
+    const int64_t hi = std::min<int64_t>(last_parent, (((int64_t)2) << d) - 2);
+    const int blocks = (int)std::min<int64_t>(1184, (hi - lo + 1 + 255) / 256);
+    count_launches(1);
+    heap_level_kernel<<<blocks, 256, 0, stream>>>(heap, len, lo, hi);
+  }
+}
 
 void launch_count(const DevPool &P, uint64_t num_sets, uint32_t *count,
                   int blocks, cudaStream_t stream) {
@@ -329,15 +353,6 @@ void launch_build_inverted(const DevPool &P, uint64_t num_sets,
 void launch_cover(const CoverLaunch &C, cudaStream_t stream) {
   count_launches(1);
   cover_kernel<<<C.blocks, 256, 0, stream>>>(C);
-}
-
-void launch_gather_dirty(const uint32_t *dirty_list, const unsigned int *dirty_n,
-                         uint32_t max_n, const uint32_t *count,
-                         uint32_t *dirty_bits, uint2 *pairs, unsigned int *total_out,
-                         int blocks, cudaStream_t stream) {
-  count_launches(1);
-  gather_dirty_kernel<<<blocks, 256, 0, stream>>>(dirty_list, dirty_n, max_n,
-                                                  count, dirty_bits, pairs, total_out);
 }
 
 void launch_argmax(const uint32_t *count, uint32_t n, unsigned long long *best,

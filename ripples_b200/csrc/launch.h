@@ -128,23 +128,18 @@ struct CoverLaunch {
   uint32_t vertex;
   uint8_t *covered;
   uint32_t *count;
-  uint32_t *dirty_bits;   // n bits
-  uint32_t *dirty_list;   // n entries
   unsigned int *dirty_n;
   unsigned long long *covered_sets;  // running total of newly covered sets
-  // Last-block epilogue (used when `done` is set): gather the dirty pairs into
-  // `pairs` / `total_out` when `pairs` is set, then zero dirty_n and done.
-  unsigned int *done;
+  // When set, every decrement reports (vertex, count after it) here, at
+  // positions counted by dirty_n (entries past max_dirty are dropped).
   uint2 *pairs;
-  unsigned int *total_out;
   uint32_t max_dirty;
   int blocks;
 };
 void launch_cover(const CoverLaunch &C, cudaStream_t stream);
-void launch_gather_dirty(const uint32_t *dirty_list, const unsigned int *dirty_n,
-                         uint32_t max_n, const uint32_t *count,
-                         uint32_t *dirty_bits, uint2 *pairs, unsigned int *total_out,
-                         int blocks, cudaStream_t stream);
+// Builds the selection max-heap of {vertex, count} on the device, element for
+// element the heap std::make_heap builds (level-parallel).
+void launch_make_heap(const uint32_t *count, uint32_t n, uint2 *heap, cudaStream_t stream);
 void launch_argmax(const uint32_t *count, uint32_t n, unsigned long long *best,
                    int blocks, cudaStream_t stream);
 

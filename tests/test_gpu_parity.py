@@ -295,3 +295,11 @@ def test_wide_path_bit_exact(ctx, weights, sampler):
     assert_same_sets(off, vtx, ooff, ovtx)
     st = p.stats()
     assert st[2] == 3000 and st[4] == ost[0] and st[5] == ost[1]
+
+
+@pytest.mark.parametrize("n,max_count,seed", [(1, 3, 0), (2, 1, 1), (37, 2, 2), (5000, 3, 3),
+                                              (1 << 20, 5, 4), ((1 << 20) + 12345, 1000, 5)])
+def test_device_heap_is_libstdcxx_make_heap(ctx, n, max_count, seed):
+    """rip_select builds its max-heap on the device; it must equal
+    std::make_heap element for element (ties included)."""
+    assert rb._lib.lib.rip_selftest_heap_device(ctx.h, n, max_count, seed) == 1
