@@ -170,10 +170,10 @@ int rip_pool_configure(rip_pool *p, uint32_t colors, uint32_t slots,
                        uint32_t log_capacity);
 
 /* Edge-work budgets (in-edges read) after which a one-set-per-warp set, or a
- * fused CTA batch, is handed to the grid-wide BFS that spreads each level's
- * edge groups over the whole GPU (the heavy tail of IC sampling on skewed
- * graphs); 0 disables the hand-over.  Defaults 2^18 and 2^23.  Results do not
- * depend on these values. */
+ * fused CTA batch, is handed to the CTA-per-set sampler, whose 32 warps split
+ * each level's edge groups (the heavy tail of IC sampling on skewed graphs);
+ * 0 disables the hand-over.  Defaults 2^18 and 2^23.  Results do not depend on
+ * these values. */
 int rip_pool_work_caps(rip_pool *p, uint64_t plain_cap, uint64_t fused_cap);
 
 /* ---- seed selection ------------------------------------------------------- */
@@ -195,8 +195,10 @@ int rip_select_counts(rip_pool *p, uint32_t *counts);
 /* Diagnostic breakdown of the rip_select calls on this pool: out[0] ms in
  * counting/indexing kernels + count download, out[1] ms building the heap,
  * out[2] ms in the pick loop, out[3] heap pops, out[4] seeds picked,
- * out[5] dirty (vertex, count) pairs applied, out[6] selections. */
-int rip_select_profile(rip_pool *p, double out[8]);
+ * out[5] (vertex, count) reports applied, out[6] selections, out[7] ms in
+ * cover launches + syncs (includes out[8]), out[8] ms applying reports,
+ * out[9] ms in heap pops. */
+int rip_select_profile(rip_pool *p, double out[12]);
 
 /* Diagnostic: builds a heap of n random (vertex, count) entries, counts in
  * [0, max_count), with the library's level-parallel heap construction and with

@@ -571,12 +571,12 @@ struct rip_pool {
   // flags, frontier log); all-zero between batches
   DevMem f_vis, f_pend, f_flag, f_log, f_order;
   uint32_t f_slots = 0, f_cw = 0, f_lcap = 0;
-  // grid-wide BFS slot for sets with very large edge work
-  DevMem w_vis, w_pend, w_flag, w_log, w_ent, w_small, w_scan;
-  uint32_t w_lcap = 0;
+  // CTA-per-set scratch for sets with very large edge work
+  DevMem b_scratch, b_ids;
+  uint32_t b_slots = 0, b_qcap = 0;
   uint64_t cap_plain = 1ull << 18;  // in-edges per set before a warp hands it over
   uint64_t cap_fused = 1ull << 23;  // in-edges per fused batch before handing over
-  uint64_t wide_sets = 0;           // sets grown by the wide path (diagnostic)
+  uint64_t big_sets = 0;            // sets grown one CTA each (diagnostic)
   uint32_t colors = 64;      // fused colour width (64/128/256)
   uint32_t fused_slots = 0;  // 0 = size from the budget
   uint32_t lcap_pref = 0;    // 0 = default frontier-log capacity
@@ -590,8 +590,9 @@ struct rip_pool {
   size_t heap_registered_bytes = 0;
   DevMem d_heap;                     // heap built on the device
   // selection profile: [0] count+index kernels and counts D2H, [1] heap build,
-  // [2] pick loop, [3] heap pops, [4] picks, [5] dirty pairs, [6] selections
-  double sel_prof[8] = {0};
+  // [2] pick loop, [3] heap pops, [4] picks, [5] count reports, [6] selections,
+  // [7] ms in cover launch + sync, [8] ms applying reports, [9] ms in heap pops
+  double sel_prof[12] = {0};
   // timing of sampler kernels (CUDA events on the context stream)
   double kernel_ms = 0.0;
   uint64_t kernel_launches = 0;
@@ -639,8 +640,7 @@ extern "C" int rip_pool_destroy(rip_pool *p) {
   DevMem *all[] = {&p->vtx,     &p->set_off,   &p->set_len,  &p->meta,
                    &p->scratch, &p->ids_a,     &p->ids_b,    &p->f_vis,
                    &p->f_pend,  &p->f_flag,    &p->f_log,    &p->f_order,
-                   &p->w_vis,   &p->w_pend,    &p->w_flag,   &p->w_log,
-                   &p->w_ent,   &p->w_small,   &p->w_scan,   &p->d_heap,
+                   &p->b_scratch, &p->b_ids,   &p->d_heap,
                    &p->count,   &p->inv_off,   &p->inv_cur,  &p->inv,
                    &p->covered,
                    &p->scan_sums};
@@ -739,11 +739,11 @@ static uint32_t default_warps(rip_pool *p, uint32_t qcap) {
 }
 
 static int sample_fused(rip_pool *p, uint64_t seed, uint64_t first, uint32_t count);
-static int sample_wide(rip_pool *p, uint64_t seed, uint64_t first,
-                       const std::vector<uint32_t> &ids);
+static int sample_big(rip_pool *p, uint64_t seed, uint64_t first,
+                      const std::vector<uint32_t> &ids);
 
 // One set per warp (IC BFS / LT walk).  IC sets whose edge work exceeds the
-// per-set cap are handed to the grid-wide BFS; sets that outgrow the warp
+// per-set cap are handed to the CTA-per-set sampler; sets that outgrow the warp
 // queues or the pool are re-run with larger buffers.
 static int sample_warp_per_set(rip_pool *p, uint64_t seed, uint64_t first,
                                uint32_t count, const std::vector<uint32_t> *only) {
@@ -843,130 +843,99 @@ static int sample_warp_per_set(rip_pool *p, uint64_t seed, uint64_t first,
   }
   if (!big.empty()) {
     std::sort(big.begin(), big.end());
-    TRY(sample_wide(p, seed, first, big));
+    TRY(sample_big(p, seed, first, big));
   }
   return RIP_OK;
 }
 
 // ---------------------------------------------------------------------------
-// grid-wide fused BFS for the heavy tail (IC)
+// heavy-tail IC sets: one CTA per set
 // ---------------------------------------------------------------------------
-static int ensure_wide(rip_pool *p, uint32_t lcap) {
+static int ensure_big_scratch(rip_pool *p, uint32_t slots, uint32_t qcap) {
   rip_ctx *c = p->ctx;
-  const size_t n = p->g->n;
-  if (p->w_vis.p && p->w_lcap >= lcap) return RIP_OK;
-  TRY(dalloc(c, p->w_vis, n * 8));
-  TRY(dalloc(c, p->w_pend, n * 8));
-  TRY(dalloc(c, p->w_flag, n * 4));
-  TRY(dalloc(c, p->w_log, (size_t)lcap * 4));
-  // entries: beg, end, groups (u32) + mask (u64) + prefix (u64, lcap+1)
-  TRY(dalloc(c, p->w_ent, (size_t)lcap * 12 + (size_t)lcap * 8 + ((size_t)lcap + 1) * 8 + 256));
-  TRY(dalloc(c, p->w_small, 4096));
-  TRY(dalloc(c, p->w_scan, sizeof(uint64_t) * scan_block_sums_needed(lcap)));
-  CK(c, cudaMemsetAsync(p->w_vis.p, 0, n * 8, c->stream));
-  CK(c, cudaMemsetAsync(p->w_pend.p, 0, n * 8, c->stream));
-  CK(c, cudaMemsetAsync(p->w_flag.p, 0, n * 4, c->stream));
-  p->w_lcap = lcap;
+  const uint64_t bm_words = (((uint64_t)p->g->n + 31) / 32 + 7) & ~7ull;
+  if (p->b_scratch.p && p->b_slots == slots && p->b_qcap == qcap) return RIP_OK;
+  const size_t bytes = (size_t)slots * (bm_words * 4 + (size_t)qcap * 4);
+  TRY(dalloc(c, p->b_scratch, bytes));
+  CK(c, cudaMemsetAsync(p->b_scratch.p, 0, (size_t)slots * bm_words * 4, c->stream));
+  p->b_slots = slots;
+  p->b_qcap = qcap;
   return RIP_OK;
 }
 
-// Grows the sets first+ids[i] with the whole GPU, 64 at a time.
-static int sample_wide(rip_pool *p, uint64_t seed, uint64_t first,
-                       const std::vector<uint32_t> &ids) {
-  if (ids.empty()) return RIP_OK;
+// Grows the sets first+ids[i], one 1024-thread CTA each.
+static int sample_big(rip_pool *p, uint64_t seed, uint64_t first,
+                      const std::vector<uint32_t> &ids_in) {
+  if (ids_in.empty()) return RIP_OK;
   rip_ctx *c = p->ctx;
   rip_graph *g = p->g;
-  uint32_t lcap = p->w_lcap ? p->w_lcap
-                            : (uint32_t)std::min<uint64_t>((uint64_t)g->n * 64, 1u << 22);
-  TRY(ensure_wide(p, lcap));
+  const uint64_t bm_words = (((uint64_t)g->n + 31) / 32 + 7) & ~7ull;
+  uint32_t qcap = p->b_qcap ? p->b_qcap : std::min<uint32_t>(g->n, 1u << 20);
+  auto slots_for = [&](uint32_t q) {
+    const size_t per = bm_words * 4 + (size_t)q * 4;
+    size_t avail = c->budget > c->used ? c->budget - c->used : 0;
+    avail += p->b_scratch.bytes;
+    return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)c->num_sms,
+                                                               (avail / 4) / per));
+  };
+  TRY(ensure_big_scratch(p, slots_for(qcap), qcap));
+  std::vector<uint32_t> ids = ids_in;
   PoolMeta *dm = p->dmeta();
-  for (size_t b0 = 0; b0 < ids.size();) {
-    const uint32_t ncol = (uint32_t)std::min<size_t>(64, ids.size() - b0);
-    const size_t lc = p->w_lcap;
-    WideLaunch L;
+  for (int attempt = 0; attempt < 32 && !ids.empty(); ++attempt) {
+    TRY(dalloc(c, p->b_ids, sizeof(uint32_t) * ids.size() * 2));
+    CK(c, cudaMemcpyAsync(p->b_ids.p, ids.data(), sizeof(uint32_t) * ids.size(),
+                          cudaMemcpyHostToDevice, c->stream));
+    CK(c, cudaMemsetAsync(&dm->fail_count, 0, sizeof(unsigned int), c->stream));
+    CK(c, cudaMemsetAsync(&dm->next, 0, sizeof(unsigned int), c->stream));
+    CK(c, cudaMemsetAsync(&dm->first_bad, 0xFF, sizeof(unsigned long long), c->stream));
+    BigLaunch L;
     L.G = g->view();
     L.P = p->view();
     L.key = make_key(seed);
-    L.F = FailList{nullptr, nullptr, &dm->first_bad};
-    L.ncol = ncol;
-    L.cw = 1;
-    L.vis = ptr<uint64_t>(p->w_vis);
-    L.pend = ptr<uint64_t>(p->w_pend);
-    L.pflag = ptr<uint32_t>(p->w_flag);
-    L.log = ptr<uint32_t>(p->w_log);
-    L.lcap = (uint32_t)lc;
-    unsigned char *ent = static_cast<unsigned char *>(p->w_ent.p);
-    L.ent_beg = reinterpret_cast<uint32_t *>(ent);
-    L.ent_end = reinterpret_cast<uint32_t *>(ent + lc * 4);
-    L.ent_groups = reinterpret_cast<uint32_t *>(ent + lc * 8);
-    L.ent_mask = reinterpret_cast<uint64_t *>(ent + ((lc * 12 + 7) & ~(size_t)7));
-    L.ent_prefix = reinterpret_cast<uint64_t *>(ent + ((lc * 12 + 7) & ~(size_t)7) + lc * 8);
-    unsigned char *sm = static_cast<unsigned char *>(p->w_small.p);
-    // small block: sets[64] u64 | starts[64] u64 | sizes[64] | fill[64] | tail | overflow | stats[4]
-    uint64_t *d_sets = reinterpret_cast<uint64_t *>(sm);
-    L.sets = d_sets;
-    L.starts = reinterpret_cast<unsigned long long *>(sm + 512);
-    L.sizes = reinterpret_cast<uint32_t *>(sm + 1024);
-    L.fill = reinterpret_cast<uint32_t *>(sm + 1280);
-    L.tail = reinterpret_cast<unsigned int *>(sm + 1536);
-    L.overflow = reinterpret_cast<unsigned int *>(sm + 1540);
-    L.batch_stats = reinterpret_cast<unsigned long long *>(sm + 1544);
-    uint64_t hsets[64];
-    for (uint32_t i = 0; i < ncol; ++i) hsets[i] = first + ids[b0 + i];
-    CK(c, cudaMemcpyAsync(d_sets, hsets, 8 * ncol, cudaMemcpyHostToDevice, c->stream));
-    CK(c, cudaMemsetAsync(sm + 1024, 0, 1576 - 1024, c->stream));
-    CK(c, cudaMemsetAsync(&dm->first_bad, 0xFF, sizeof(unsigned long long), c->stream));
-    launch_wide_seed(L, c->stream);
-    unsigned int h[2] = {0, 0};
-    CK(c, cudaMemcpyAsync(h, L.tail, 8, cudaMemcpyDeviceToHost, c->stream));
-    CK(c, cudaStreamSynchronize(c->stream));
-    uint32_t lo = 0, hi = std::min<uint32_t>(h[0], (uint32_t)lc), level = 1;
-    while (lo < hi && !h[1]) {
-      launch_wide_prepare(L, lo, hi, c->stream);
-      launch_exclusive_scan(L.ent_groups, L.ent_prefix, hi - lo, ptr<uint64_t>(p->w_scan),
-                            c->stream);
-      launch_wide_expand(L, hi - lo, level, c->num_sms * 8, c->stream);
-      CK(c, cudaGetLastError());
-      CK(c, cudaMemcpyAsync(h, L.tail, 8, cudaMemcpyDeviceToHost, c->stream));
-      CK(c, cudaStreamSynchronize(c->stream));
-      lo = hi;
-      hi = std::min<uint32_t>(h[0], (uint32_t)lc);
-      ++level;
-    }
-    if (h[1]) {
-      // the frontier log overflowed: vertices outside it may hold colours, so
-      // clear the whole slot and retry the batch with a longer log
-      CK(c, cudaMemsetAsync(p->w_vis.p, 0, (size_t)g->n * 8, c->stream));
-      CK(c, cudaMemsetAsync(p->w_pend.p, 0, (size_t)g->n * 8, c->stream));
-      CK(c, cudaMemsetAsync(p->w_flag.p, 0, (size_t)g->n * 4, c->stream));
-      if (lc >= (uint64_t)g->n * 64)
-        return set_err(c, RIP_ERR_DEVICE, "wide BFS log overflow at full size");
-      TRY(ensure_wide(p, (uint32_t)std::min<uint64_t>(lc * 4, (uint64_t)g->n * 64)));
-      continue;
-    }
-    launch_wide_reserve(L, c->stream);
-    CK(c, cudaMemcpyAsync(h, L.tail, 8, cudaMemcpyDeviceToHost, c->stream));
-    CK(c, cudaStreamSynchronize(c->stream));
-    const bool store = h[1] == 0;
-    launch_wide_emit(L, std::min<uint32_t>(h[0], (uint32_t)lc), store, c->stream);
-    if (!store) {  // pool full: grow it and redo the batch
-      PoolMeta m;
-      TRY(read_meta(p, m));
-      const unsigned long long cur = std::min<unsigned long long>(m.cursor, m.first_bad);
-      CK(c, cudaMemcpyAsync(&dm->cursor, &cur, sizeof(cur), cudaMemcpyHostToDevice, c->stream));
-      p->num_elems = cur;
-      TRY(ensure_elems(p, std::max<uint64_t>(p->cap * 2, cur + (1u << 20))));
-      continue;
-    }
-    launch_wide_commit(L, Stats{dm->stats}, c->stream);
+    L.first = first;
+    L.count = (uint32_t)ids.size();
+    L.ids = ptr<uint32_t>(p->b_ids);
+    L.next = &dm->next;
+    L.bitmaps = ptr<uint32_t>(p->b_scratch);
+    L.bm_words = bm_words;
+    L.queues = ptr<uint32_t>(p->b_scratch) + (size_t)p->b_slots * bm_words;
+    L.qcap = p->b_qcap;
+    L.F = FailList{ptr<uint32_t>(p->b_ids) + ids.size(), &dm->fail_count, &dm->first_bad};
+    L.st = Stats{dm->stats};
+    L.blocks = (int)std::min<uint32_t>(p->b_slots, (uint32_t)ids.size());
+    CK(c, cudaEventRecord(c->ev0, c->stream));
+    launch_ic_bigset(L, c->stream);
     CK(c, cudaGetLastError());
-    p->wide_sets += ncol;
-    b0 += ncol;
+    CK(c, cudaEventRecord(c->ev1, c->stream));
+    PoolMeta m;
+    TRY(read_meta(p, m));
+    float kms = 0.f;
+    cudaEventElapsedTime(&kms, c->ev0, c->ev1);
+    p->kernel_ms += kms;
+    p->kernel_launches++;
+    p->big_sets += ids.size() - m.fail_count;
+    if (m.fail_count == 0) {
+      p->num_elems = m.cursor;
+      return RIP_OK;
+    }
+    const unsigned long long cur = std::min<unsigned long long>(m.cursor, m.first_bad);
+    CK(c, cudaMemcpyAsync(&dm->cursor, &cur, sizeof(cur), cudaMemcpyHostToDevice, c->stream));
+    p->num_elems = cur;
+    std::vector<uint32_t> failed(m.fail_count);
+    CK(c, cudaMemcpyAsync(failed.data(), ptr<uint32_t>(p->b_ids) + ids.size(),
+                          sizeof(uint32_t) * m.fail_count, cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    if (m.first_bad != ~0ull) {
+      TRY(ensure_elems(p, std::max<uint64_t>(p->cap * 2, cur + (1u << 20))));
+    } else if (p->b_qcap < g->n) {
+      const uint32_t nq = (uint32_t)std::min<uint64_t>(g->n, (uint64_t)p->b_qcap * 4);
+      TRY(ensure_big_scratch(p, std::min(slots_for(nq), p->b_slots), nq));
+    } else {
+      return set_err(c, RIP_ERR_DEVICE, "big-set sampler failed with full-size queues");
+    }
+    ids.swap(failed);
   }
-  PoolMeta m;
-  TRY(read_meta(p, m));
-  p->num_elems = m.cursor;
-  return RIP_OK;
+  return ids.empty() ? RIP_OK : set_err(c, RIP_ERR_DEVICE, "big-set sampler did not converge");
 }
 
 // ---------------------------------------------------------------------------
@@ -1109,11 +1078,11 @@ static int sample_fused(rip_pool *p, uint64_t seed, uint64_t first,
     }
   }
   // Whatever still failed runs set by set (same sets, bit for bit); sets of
-  // batches that outgrew their edge budget are grown by the whole GPU.
+  // batches that outgrew their edge budget are grown one CTA each.
   if (todo) TRY(sample_warp_per_set(p, seed, first, todo, &order));
   if (!big.empty()) {
     std::sort(big.begin(), big.end());
-    TRY(sample_wide(p, seed, first, big));
+    TRY(sample_big(p, seed, first, big));
   }
   return RIP_OK;
 }
@@ -1123,14 +1092,14 @@ static int sample_fused(rip_pool *p, uint64_t seed, uint64_t first,
 // capacity per slot (0 = default).  Takes effect at the next rip_sample.
 // Diagnostic breakdown of rip_select since the pool was created (see
 // rip_pool::sel_prof).
-extern "C" int rip_select_profile(rip_pool *p, double out[8]) {
+extern "C" int rip_select_profile(rip_pool *p, double out[12]) {
   if (!p || !out) return RIP_ERR_INVALID;
-  for (int i = 0; i < 8; ++i) out[i] = p->sel_prof[i];
+  for (int i = 0; i < 12; ++i) out[i] = p->sel_prof[i];
   return RIP_OK;
 }
 
 // Edge-work budgets before a warp (plain) or a CTA batch (fused) hands its
-// set(s) to the grid-wide BFS; 0 disables the hand-over.
+// set(s) to the CTA-per-set sampler; 0 disables the hand-over.
 extern "C" int rip_pool_work_caps(rip_pool *p, uint64_t plain_cap, uint64_t fused_cap) {
   if (!p) return RIP_ERR_INVALID;
   p->cap_plain = plain_cap;
@@ -1487,6 +1456,7 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
     CK(c, cudaMemcpyAsync(h_dn, &dm->dirty_n, sizeof(unsigned int), cudaMemcpyDeviceToHost,
                           c->stream));
     CK(c, cudaStreamSynchronize(c->stream));
+    const auto t_a0 = clk::now();
     const unsigned int dn = *reinterpret_cast<volatile unsigned int *>(h_dn);
     if (dn > max_reports) {
       CK(c, cudaMemcpyAsync(hcount.data(), p->count.p, sizeof(uint32_t) * (size_t)n,
@@ -1498,6 +1468,7 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
         if (hp[i].y < hcount[hp[i].x]) hcount[hp[i].x] = hp[i].y;
     }
     p->sel_prof[5] += dn;
+    p->sel_prof[8] += ms_since(t_a0);
     return RIP_OK;
   };
 
@@ -1534,6 +1505,7 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
     const auto t_p0 = clk::now();
     while (out_seeds.size() < k && uncovered != 0) {
       HeapItem element;
+      const auto t_q0 = clk::now();
       for (;;) {  // getNextSeed, streaming_find_most_influential.h:560-571
         if (queue.empty())
           return set_err(c, RIP_ERR_STATE, "selection heap exhausted");
@@ -1547,6 +1519,7 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
         }
         break;
       }
+      p->sel_prof[9] += ms_since(t_q0);
       uncovered -= element.second;
       out_seeds.push_back(element.first);
       out_gains.push_back(element.second);

@@ -1,0 +1,179 @@
+// kernels_bigset.cu -- IC sets with very large edge work, one CTA each.
+//
+// Under weighted-cascade probabilities on skewed graphs a few RRR sets reach
+// many hubs and read millions of in-edge records each (on an R-MAT graph with
+// 2^20 vertices 1% of the sets carry ~40% of the edge work).  One warp per set
+// (ic_plain_kernel) or one warp per frontier entry (ic_fused_kernel) walks a
+// hub's in-list alone, so those sets set the kernel's length.  Here one
+// 1024-thread CTA grows one such set: level by level, the level's entries are
+// taken 1024 at a time, a block scan turns their 4-edge group counts into
+// offsets, and all 32 warps stride over the concatenated groups (each thread
+// finds its entry by binary search in shared memory) -- a hub's in-list is
+// split over the whole CTA.  Levels are separated by __syncthreads only.
+// Coins are the same (set, edge)-keyed Philox draws as every other sampler.
+#include "device.cuh"
+#include "launch.h"
+
+namespace rip {
+
+namespace {
+
+constexpr int BIG_THREADS = 1024;
+constexpr int BIG_WARPS = BIG_THREADS / 32;
+
+// Exclusive block scan of one u32 per thread; returns the exclusive value and
+// writes the block total to *total.  Uses `warp_tot` (BIG_WARPS entries).
+__device__ uint32_t big_block_scan(uint32_t x, uint32_t *warp_tot, uint32_t *total) {
+  const uint32_t lane = lane_id(), wid = threadIdx.x >> 5;
+  const uint32_t incl = warp_incl_scan(x);
+  if (lane == 31) warp_tot[wid] = incl;
+  __syncthreads();
+  if (wid == 0) {
+    const uint32_t t = lane < BIG_WARPS ? warp_tot[lane] : 0u;
+    const uint32_t ti = warp_incl_scan(t);
+    if (lane < BIG_WARPS) warp_tot[lane] = ti - t;
+    if (lane == 31) *total = ti;
+  }
+  __syncthreads();
+  const uint32_t r = warp_tot[wid] + incl - x;
+  __syncthreads();
+  return r;
+}
+
+__global__ void __launch_bounds__(BIG_THREADS)
+ic_bigset_kernel(BigLaunch L) {
+  __shared__ uint32_t s_off[BIG_THREADS + 1];  // exclusive group offsets of the chunk
+  __shared__ uint32_t s_beg[BIG_THREADS], s_end[BIG_THREADS];
+  __shared__ uint32_t s_warp[BIG_WARPS];
+  __shared__ uint32_t s_idx, s_qlen, s_overflow, s_total;
+  __shared__ unsigned long long s_edges, s_base;
+
+  const uint32_t tid = threadIdx.x;
+  uint32_t *bm = L.bitmaps + (size_t)blockIdx.x * L.bm_words;
+  uint32_t *q = L.queues + (size_t)blockIdx.x * L.qcap;
+  unsigned long long n_exp = 0, n_edges = 0, n_sets = 0, n_elems = 0;
+
+  for (;;) {
+    if (tid == 0) s_idx = atomicAdd(L.next, 1u);
+    __syncthreads();
+    const uint32_t idx = s_idx;
+    if (idx >= L.count) break;
+    const uint32_t rel = L.ids[idx];
+    const uint64_t s = L.first + rel;
+    if (tid == 0) {
+      const uint32_t root = root_of(L.key, s, L.G.n);
+      q[0] = root;
+      atomicOr(&bm[root >> 5], 1u << (root & 31));
+      s_qlen = 1;
+      s_overflow = 0;
+      s_edges = 0;
+    }
+    __syncthreads();
+    uint32_t lo = 0, hi = 1;
+    while (lo < hi && !s_overflow) {
+      for (uint32_t cb = lo; cb < hi; cb += BIG_THREADS) {
+        const uint32_t e = cb + tid;
+        uint32_t beg = 0, end = 0;
+        if (e < hi) {
+          const uint32_t v = q[e];
+          beg = __ldg(L.G.off + v);
+          end = __ldg(L.G.off + v + 1);
+          atomicAdd(&s_edges, (unsigned long long)(end - beg));
+        }
+        s_beg[tid] = beg;
+        s_end[tid] = end;
+        const uint32_t ng = group_count(beg, end);
+        s_off[tid] = big_block_scan(ng, s_warp, &s_total);
+        if (tid == 0) s_off[BIG_THREADS] = s_total;
+        __syncthreads();
+        const uint32_t total = s_off[BIG_THREADS];
+        for (uint32_t j = tid; j < total; j += BIG_THREADS) {
+          // entry a: s_off[a] <= j < s_off[a + 1]
+          uint32_t a = 0, b = BIG_THREADS;
+          while (b - a > 1) {
+            const uint32_t mid = (a + b) >> 1;
+            if (s_off[mid] <= j) a = mid;
+            else b = mid;
+          }
+          const uint32_t ob = s_beg[a], oe = s_end[a];
+          const uint32_t g = (ob >> 2) + (j - s_off[a]);
+          uint2 rec[4];
+          load_group(L.G.edges, g, rec);
+          const u32x4 c = ic_coins(L.key, g, s);
+#pragma unroll
+          for (int t = 0; t < 4; ++t) {
+            const uint32_t ed = (g << 2) + t;
+            if (ed >= ob && ed < oe && lane_of(c, t) < rec[t].y) {
+              const uint32_t u = rec[t].x;
+              const uint32_t bit = 1u << (u & 31);
+              if (!(atomicOr(&bm[u >> 5], bit) & bit)) {
+                const uint32_t pos = atomicAdd(&s_qlen, 1u);
+                if (pos < L.qcap) q[pos] = u;
+                else s_overflow = 1;
+              }
+            }
+          }
+        }
+        __syncthreads();
+      }
+      lo = hi;
+      hi = min(s_qlen, L.qcap);
+      __syncthreads();
+    }
+    const uint32_t qlen = min(s_qlen, L.qcap);
+    bool stored = false;
+    if (!s_overflow) {
+      if (tid == 0) {
+        const unsigned long long b = atomicAdd(L.P.cursor, (unsigned long long)qlen);
+        if (b + qlen <= L.P.cap) {
+          s_base = b;
+          L.P.set_off[s] = b;
+          L.P.set_len[s] = qlen;
+        } else {
+          atomicMin(L.F.first_bad_base, b);
+          s_base = ~0ull;
+        }
+      }
+      __syncthreads();
+      stored = s_base != ~0ull;
+      if (stored)
+        for (uint32_t i = tid; i < qlen; i += BIG_THREADS) L.P.vtx[s_base + i] = q[i];
+    }
+    __syncthreads();
+    // clear the bitmap: every set bit belongs to a queued vertex -- except on
+    // queue overflow, where discovered vertices past the queue also set bits
+    if (s_overflow) {
+      for (uint64_t w = tid; w < L.bm_words; w += BIG_THREADS) bm[w] = 0u;
+    } else {
+      for (uint32_t i = tid; i < qlen; i += BIG_THREADS) bm[q[i] >> 5] = 0u;
+    }
+    if (tid == 0) {
+      if (stored) {
+        n_sets += 1;
+        n_elems += qlen;
+        n_exp += qlen;
+        n_edges += s_edges;
+      } else {
+        L.F.ids[atomicAdd(L.F.count, 1u)] = rel;
+      }
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    atomicAdd(L.st.v + 0, n_exp);
+    atomicAdd(L.st.v + 1, n_edges);
+    atomicAdd(L.st.v + 2, n_sets);
+    atomicAdd(L.st.v + 3, n_elems);
+    atomicAdd(L.st.v + 4, n_exp);
+    atomicAdd(L.st.v + 5, n_edges);
+  }
+}
+
+}  // namespace
+
+void launch_ic_bigset(const BigLaunch &L, cudaStream_t stream) {
+  count_launches(1);
+  ic_bigset_kernel<<<L.blocks, BIG_THREADS, 0, stream>>>(L);
+}
+
+}  // namespace rip

@@ -225,7 +225,7 @@ ic_fused_kernel(FusedLaunch L) {
       lvl_start = lvl_end;
       lvl_end = min(s_tail, lcap);
       ++level;
-      // a batch that outgrows its edge budget goes to the grid-wide BFS
+      // a batch that outgrows its edge budget goes to the CTA-per-set sampler
       if (tid == 0 && L.work_cap && s_work > L.work_cap && !s_overflow) s_overflow = 3;
       __syncthreads();
     }

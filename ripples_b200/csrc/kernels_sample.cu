@@ -110,7 +110,7 @@ ic_plain_kernel(DevGraph G, DevPool P, Key key, uint64_t first, uint32_t count,
       const uint32_t total = __shfl_sync(FULL, incl, 31);
       warp_edges += (unsigned long long)total * 4;
       if (work_cap && warp_edges > work_cap) {
-        // too much edge work for one warp: leave the set to the grid-wide BFS
+        // too much edge work for one warp: leave the set to a whole CTA
         overflow = big = true;
         break;
       }

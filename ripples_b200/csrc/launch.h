@@ -59,33 +59,25 @@ struct FusedLaunch {
   int blocks;            // slots
 };
 
-// Grid-wide fused BFS for sets with very large edge work (kernels_wide.cu).
-struct WideLaunch {
+// IC sets with very large edge work: one 1024-thread CTA per set, the CTA's
+// warps splitting every level's edge groups (kernels_bigset.cu).
+struct BigLaunch {
   DevGraph G{};
   DevPool P{};
   Key key{};
+  uint64_t first = 0;
+  uint32_t count = 0;             // entries of ids
+  const uint32_t *ids = nullptr;  // set indices relative to first
+  unsigned int *next = nullptr;
+  uint32_t *bitmaps = nullptr;    // per CTA slot, bm_words words, all-zero between sets
+  uint64_t bm_words = 0;
+  uint32_t *queues = nullptr;     // per CTA slot, qcap entries
+  uint32_t qcap = 0;
   FailList F{};
-  const uint64_t *sets = nullptr;  // ncol set ids
-  uint32_t ncol = 0, cw = 1;
-  uint64_t *vis = nullptr, *pend = nullptr;  // n * cw words each
-  uint32_t *pflag = nullptr;                 // n level flags
-  uint32_t *log = nullptr;                   // lcap frontier-log entries
-  uint32_t lcap = 0;
-  unsigned int *tail = nullptr, *overflow = nullptr;
-  uint32_t *sizes = nullptr, *fill = nullptr;  // per colour
-  unsigned long long *starts = nullptr;         // per colour
-  uint32_t *ent_beg = nullptr, *ent_end = nullptr, *ent_groups = nullptr;  // lcap each
-  uint64_t *ent_mask = nullptr;    // lcap * cw
-  uint64_t *ent_prefix = nullptr;  // lcap + 1
-  unsigned long long *batch_stats = nullptr;  // [4]
+  Stats st{};
+  int blocks = 0;
 };
-void launch_wide_seed(const WideLaunch &L, cudaStream_t s);
-void launch_wide_prepare(const WideLaunch &L, uint32_t lo, uint32_t hi, cudaStream_t s);
-void launch_wide_expand(const WideLaunch &L, uint32_t nent, uint32_t level, int blocks,
-                        cudaStream_t s);
-void launch_wide_reserve(const WideLaunch &L, cudaStream_t s);
-void launch_wide_emit(const WideLaunch &L, uint32_t tail, bool store, cudaStream_t s);
-void launch_wide_commit(const WideLaunch &L, Stats st, cudaStream_t s);
+void launch_ic_bigset(const BigLaunch &L, cudaStream_t stream);
 void launch_ic_fused(const FusedLaunch &L, cudaStream_t stream);
 // Resident fused CTAs per SM for a colour width (occupancy API).
 int fused_ctas_per_sm(uint32_t colors);

@@ -305,9 +305,10 @@ class Pool:
         return ms.value, n.value, sms.value
 
     def select_profile(self) -> dict:
-        out = np.zeros(8, dtype=np.float64)
+        out = np.zeros(12, dtype=np.float64)
         self._chk(lib.rip_select_profile(self.h, _ptr(out)), "rip_select_profile")
-        keys = ["prep_ms", "heap_ms", "picks_ms", "pops", "seeds", "dirty", "selections"]
+        keys = ["prep_ms", "heap_ms", "picks_ms", "pops", "seeds", "reports", "selections",
+                "cover_sync_ms", "apply_ms", "pop_ms"]
         return dict(zip(keys, out.tolist()))
 
     def count(self, num_sets: Optional[int] = None) -> np.ndarray:

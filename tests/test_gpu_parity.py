@@ -283,9 +283,9 @@ def test_device_graph_construction_matches_host(ctx, model, weights, lo, hi):
 
 @pytest.mark.parametrize("weights", [rb.WEIGHTS_UNIFORM, rb.WEIGHTS_WC])
 @pytest.mark.parametrize("sampler", [rb.SAMPLER_PLAIN, rb.SAMPLER_FUSED])
-def test_wide_path_bit_exact(ctx, weights, sampler):
-    """Tiny edge-work budgets send most sets to the grid-wide BFS; the sets
-    must not change."""
+def test_big_set_path_bit_exact(ctx, weights, sampler):
+    """Tiny edge-work budgets send most sets to the CTA-per-set sampler; the
+    sets must not change."""
     g = rb.HostGraph.rmat(12, 16 << 12, seed=8).with_weights(weights, seed=9, lo=0.0, hi=0.4)
     dg, p = device_pool(ctx, g, "IC", 64)
     p.work_caps(64, 256)
