@@ -62,7 +62,7 @@ struct rip_ctx {
   // or a new pool then costs no cudaMalloc); counted in `used`.
   std::vector<DevMem> cache;
   size_t cached = 0;
-  PinnedMem *h_pairs = nullptr;  // mapped: dirty (vertex, count) pairs
+  PinnedMem *h_pairs = nullptr;  // mapped: per-pick decrement reports
   PinnedMem *h_count = nullptr;  // counts at the start of a selection
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -1402,18 +1402,17 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
   C.count = ptr<uint32_t>(p->count);
   C.dirty_n = &dm->dirty_n;
   C.covered_sets = &dm->covered_sets;
-  C.pairs = nullptr;
-  C.max_dirty = 0;
+  C.reports = nullptr;
+  C.max_reports = 0;
   C.blocks = c->num_sms * 4;
 
   std::vector<uint32_t> &hcount = p->last_counts;
   hcount.resize(n);
-  // mapped: [count u32, pad][n pairs]; the gather kernel writes it directly
   if (!c->h_pairs) c->h_pairs = new PinnedMem();
   if (!c->h_count) c->h_count = new PinnedMem();
-  // mapped: the cover kernel writes its (vertex, count-after) reports here
-  const uint32_t max_reports = std::max<uint32_t>(n, 1u << 20);
-  TRY(c->h_pairs->ensure(c, 16 + sizeof(uint2) * (size_t)max_reports, true));
+  // mapped: the cover kernel writes its decrement reports (vertex ids) here
+  const uint32_t max_reports = std::max<uint32_t>(2 * n, 1u << 21);
+  TRY(c->h_pairs->ensure(c, 16 + sizeof(uint32_t) * (size_t)max_reports, true));
   TRY(c->h_count->ensure(c, sizeof(uint32_t) * (size_t)n));
   PinnedMem &h_pairs = *c->h_pairs, &h_count = *c->h_count;
 
@@ -1421,8 +1420,6 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
   std::vector<uint32_t> out_seeds;
   std::vector<uint64_t> out_gains;
 
-  // After a cover step: the dirty (vertex, count) pairs go straight to mapped
-  // host memory; one synchronisation, then the host mirror is patched.
   // Initial counts: the heap's keys, and |sets containing v| (the length of
   // v's inverted list) for sizing each pick's cover grid.
   CK(c, cudaMemcpyAsync(h_count.p, p->count.p, sizeof(uint32_t) * (size_t)n,
@@ -1437,21 +1434,22 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
   unsigned char *db = static_cast<unsigned char *>(h_pairs.dev);
   unsigned int *h_dn = reinterpret_cast<unsigned int *>(hb);  // pinned landing for dirty_n
   // One pick: mark + decrement in one launch; with_pairs also streams the
-  // (vertex, count-after) reports to mapped host memory.
+  // decremented vertex ids to mapped host memory.
   auto cover = [&](uint32_t v, bool with_pairs) -> int {
     C.vertex = v;
-    // 8 warps x 32 sets per block per pass
-    C.blocks = (int)std::min<uint64_t>(max_blocks, std::max<uint64_t>(1, (init_count[v] + 255) / 256));
-    C.pairs = with_pairs ? reinterpret_cast<uint2 *>(db + 16) : nullptr;
-    C.max_dirty = with_pairs ? max_reports : 0;
+    // one warp per set of v's inverted list, 8 warps per block
+    C.blocks = (int)std::min<uint64_t>(max_blocks * 4, std::max<uint64_t>(1, (init_count[v] + 7) / 8));
+    C.reports = with_pairs ? reinterpret_cast<uint32_t *>(db + 16) : nullptr;
+    C.max_reports = with_pairs ? max_reports : 0;
     if (with_pairs) CK(c, cudaMemsetAsync(&dm->dirty_n, 0, sizeof(unsigned int), c->stream));
     launch_cover(C, c->stream);
     CK(c, cudaGetLastError());
     return RIP_OK;
   };
 
-  // After a pick: one synchronisation, then the host mirror takes the minimum
-  // report per vertex (or the whole count array when the reports overflowed).
+  // After a pick: one synchronisation, then the host mirror applies one
+  // decrement per report (or takes the whole count array when the reports
+  // overflowed their buffer).
   auto sync_dirty = [&]() -> int {
     CK(c, cudaMemcpyAsync(h_dn, &dm->dirty_n, sizeof(unsigned int), cudaMemcpyDeviceToHost,
                           c->stream));
@@ -1463,9 +1461,8 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
                             cudaMemcpyDeviceToHost, c->stream));
       CK(c, cudaStreamSynchronize(c->stream));
     } else {
-      const uint2 *hp = reinterpret_cast<const uint2 *>(hb + 16);
-      for (unsigned int i = 0; i < dn; ++i)
-        if (hp[i].y < hcount[hp[i].x]) hcount[hp[i].x] = hp[i].y;
+      const uint32_t *hr = reinterpret_cast<const uint32_t *>(hb + 16);
+      for (unsigned int i = 0; i < dn; ++i) hcount[hr[i]] -= 1;
     }
     p->sel_prof[5] += dn;
     p->sel_prof[8] += ms_since(t_a0);

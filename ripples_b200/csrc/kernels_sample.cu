@@ -38,11 +38,11 @@ struct WarpCtx {
   uint32_t qcap;
 };
 
-// Writes the finished set to the pool (or records a failure) and clears the
-// warp's bitmap.  Returns true when the set was stored.
-__device__ bool finish_set(const WarpCtx &W, uint32_t qlen, bool overflow,
-                           uint64_t s, uint32_t rel, const DevPool &P,
-                           const FailList &F, bool big = false) {
+// Writes the finished set to the pool (unless it overflowed) and clears the
+// warp's bitmap.  Returns true when the set was stored; on a pool overflow
+// the reservation's offset is recorded in *first_bad.
+__device__ bool store_set(const WarpCtx &W, uint32_t qlen, bool overflow, uint64_t s,
+                          const DevPool &P, unsigned long long *first_bad) {
   const uint32_t lane = lane_id();
   bool stored = false;
   if (!overflow) {
@@ -57,13 +57,185 @@ __device__ bool finish_set(const WarpCtx &W, uint32_t qlen, bool overflow,
       }
       stored = true;
     } else if (lane == 0) {
-      atomicMin(F.first_bad_base, b);
+      atomicMin(first_bad, b);
     }
   }
   for (uint32_t i = lane; i < qlen; i += 32) W.bm[W.q[i] >> 5] = 0u;
-  if (!stored && lane == 0) F.ids[atomicAdd(F.count, 1u)] = big ? (rel | FAIL_BIG) : rel;
   __syncwarp();
   return stored;
+}
+
+__device__ bool finish_set(const WarpCtx &W, uint32_t qlen, bool overflow,
+                           uint64_t s, uint32_t rel, const DevPool &P,
+                           const FailList &F, bool big = false) {
+  const bool stored = store_set(W, qlen, overflow, s, P, F.first_bad_base);
+  if (!stored && lane_id() == 0) F.ids[atomicAdd(F.count, 1u)] = big ? (rel | FAIL_BIG) : rel;
+  __syncwarp();
+  return stored;
+}
+
+struct SetOutcome {
+  uint32_t qlen;
+  bool overflow, big;
+  unsigned long long exp, edges;  // per-set work (valid on lane 0 / summed over lanes)
+};
+
+// One IC set: reverse BFS from root(s) over live in-edges, warp-cooperative,
+// members in discovery order in W.q.  Sets past `work_cap` in-edges (when
+// nonzero) are abandoned with big = true.
+__device__ __forceinline__ SetOutcome ic_plain_set(const DevGraph &G, Key key, uint64_t s,
+                                                   const WarpCtx &W, uint64_t work_cap) {
+  const uint32_t lane = lane_id();
+  const uint32_t root = root_of(key, s, G.n);
+  if (lane == 0) {
+    W.q[0] = root;
+    atomicOr(&W.bm[root >> 5], 1u << (root & 31));
+  }
+  __syncwarp();
+  uint32_t qlen = 1, head = 0;
+  bool overflow = false, big = false;
+  unsigned long long set_exp = 0, set_edges = 0, warp_edges = 0;
+
+  while (head < qlen && !overflow) {
+    const uint32_t take = min(32u, qlen - head);
+    uint32_t beg = 0, end = 0, ng = 0;
+    if (lane < take) {
+      const uint32_t v = W.q[head + lane];
+      beg = __ldg(G.off + v);
+      end = __ldg(G.off + v + 1);
+      ng = group_count(beg, end);
+      set_edges += end - beg;
+    }
+    set_exp += (lane == 0) ? take : 0;
+    const uint32_t incl = warp_incl_scan(ng);
+    const uint32_t total = __shfl_sync(FULL, incl, 31);
+    warp_edges += (unsigned long long)total * 4;
+    if (work_cap && warp_edges > work_cap) {
+      // too much edge work for one warp: leave the set to a whole CTA
+      overflow = big = true;
+      break;
+    }
+    for (uint32_t base = 0; base < total && !overflow; base += 32) {
+      const uint32_t j = base + lane;
+      const bool valid = j < total;
+      const uint32_t owner = warp_find_owner(incl, valid ? j : total - 1);
+      const uint32_t ob = __shfl_sync(FULL, beg, owner);
+      const uint32_t oe = __shfl_sync(FULL, end, owner);
+      const uint32_t oexcl = __shfl_sync(FULL, incl, owner) -
+                             __shfl_sync(FULL, ng, owner);
+      uint32_t nu[4];
+      bool isnew[4];
+      if (valid) {
+        const uint32_t g = (ob >> 2) + (j - oexcl);
+        uint2 rec[4];
+        load_group(G.edges, g, rec);
+        const u32x4 c = ic_coins(key, g, s);
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          const uint32_t e = (g << 2) + t;
+          const bool live = e >= ob && e < oe && lane_of(c, t) < rec[t].y;
+          isnew[t] = false;
+          nu[t] = rec[t].x;
+          if (live) {
+            const uint32_t bit = 1u << (nu[t] & 31);
+            const uint32_t old = atomicOr(&W.bm[nu[t] >> 5], bit);
+            isnew[t] = !(old & bit);
+          }
+        }
+      } else {
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          isnew[t] = false;
+          nu[t] = 0;
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const uint32_t bal = __ballot_sync(FULL, isnew[t]);
+        if (bal == 0) continue;
+        const uint32_t cnt = __popc(bal);
+        if (overflow || qlen + cnt > W.qcap) {
+          // Abandon the set: clear the bits of vertices that will never
+          // reach the queue (queued ones are cleared by store_set).
+          if (isnew[t]) W.bm[nu[t] >> 5] = 0u;
+          overflow = true;
+          continue;
+        }
+        if (isnew[t]) W.q[qlen + __popc(bal & lanemask_lt())] = nu[t];
+        qlen += cnt;
+      }
+      __syncwarp();
+    }
+    head += take;
+  }
+  return SetOutcome{qlen, overflow, big, set_exp, set_edges};
+}
+
+// One LT set: the single-predecessor walk from root(s) (see lt_walk_kernel).
+__device__ __forceinline__ SetOutcome lt_walk_set(const DevGraph &G, Key key, uint64_t s,
+                                                  const WarpCtx &W) {
+  const uint32_t lane = lane_id();
+  uint32_t cur = root_of(key, s, G.n);
+  if (lane == 0) {
+    W.q[0] = cur;
+    atomicOr(&W.bm[cur >> 5], 1u << (cur & 31));
+  }
+  __syncwarp();
+  uint32_t qlen = 1;
+  bool overflow = false;
+  unsigned long long set_exp = 0, set_edges = 0;
+  uint32_t t = lt_threshold(key, s, cur);
+  uint32_t lo = __ldg(G.off + cur), hi = __ldg(G.off + cur + 1);
+  for (;;) {
+    set_exp += (lane == 0);
+    if (hi == lo) break;
+    // 32-ary search for the first edge whose cumulative threshold exceeds t
+    bool none = false;
+    while (hi - lo > 32) {
+      const uint32_t stride = (hi - lo + 31) / 32;
+      const uint32_t p = min(lo + (lane + 1) * stride - 1, hi - 1);
+      const bool pred = t < __ldg(&G.edges[p].y);
+      const uint32_t bal = __ballot_sync(FULL, pred);
+      set_edges += (lane == 0) ? 32 : 0;
+      if (bal == 0) {  // even the last edge's cumulative weight is <= t
+        none = true;
+        break;
+      }
+      const uint32_t L = __ffs(bal) - 1;
+      const uint32_t nlo = lo + L * stride;
+      hi = min(hi, lo + (L + 1) * stride);
+      lo = nlo;
+    }
+    if (none) break;
+    const uint32_t e = lo + lane;
+    uint2 rec = make_uint2(0u, 0u);
+    if (e < hi) rec = __ldg(&G.edges[e]);
+    const uint32_t bal = __ballot_sync(FULL, e < hi && t < rec.y);
+    set_edges += (lane == 0) ? (hi - lo) : 0;
+    if (bal == 0) break;  // no in-edge picked: the walk ends here
+    const uint32_t u = __shfl_sync(FULL, rec.x, __ffs(bal) - 1);
+    uint32_t old = 0;
+    const uint32_t bit = 1u << (u & 31);
+    if (lane == 0) old = atomicOr(&W.bm[u >> 5], bit);
+    // next step's inputs, fetched while the atomic is in flight
+    const uint32_t t2 = lt_threshold(key, s, u);
+    const uint32_t lo2 = __ldg(G.off + u), hi2 = __ldg(G.off + u + 1);
+    const uint32_t seen = __shfl_sync(FULL, old & bit, 0);
+    if (seen) break;
+    if (qlen + 1 > W.qcap) {
+      if (lane == 0) W.bm[u >> 5] = 0u;
+      overflow = true;
+      break;
+    }
+    if (lane == 0) W.q[qlen] = u;
+    ++qlen;
+    cur = u;
+    t = t2;
+    lo = lo2;
+    hi = hi2;
+  }
+  __syncwarp();
+  return SetOutcome{qlen, overflow, false, set_exp, set_edges};
 }
 
 }  // namespace
@@ -85,93 +257,12 @@ ic_plain_kernel(DevGraph G, DevPool P, Key key, uint64_t first, uint32_t count,
     if (idx >= count) break;
     const uint32_t rel = ids ? ids[idx] : idx;
     const uint64_t s = first + rel;
-    const uint32_t root = root_of(key, s, G.n);
-    if (lane == 0) {
-      W.q[0] = root;
-      atomicOr(&W.bm[root >> 5], 1u << (root & 31));
-    }
-    __syncwarp();
-    uint32_t qlen = 1, head = 0;
-    bool overflow = false, big = false;
-    unsigned long long set_exp = 0, set_edges = 0, warp_edges = 0;
-
-    while (head < qlen && !overflow) {
-      const uint32_t take = min(32u, qlen - head);
-      uint32_t beg = 0, end = 0, ng = 0;
-      if (lane < take) {
-        const uint32_t v = W.q[head + lane];
-        beg = __ldg(G.off + v);
-        end = __ldg(G.off + v + 1);
-        ng = group_count(beg, end);
-        set_edges += end - beg;
-      }
-      set_exp += (lane == 0) ? take : 0;
-      const uint32_t incl = warp_incl_scan(ng);
-      const uint32_t total = __shfl_sync(FULL, incl, 31);
-      warp_edges += (unsigned long long)total * 4;
-      if (work_cap && warp_edges > work_cap) {
-        // too much edge work for one warp: leave the set to a whole CTA
-        overflow = big = true;
-        break;
-      }
-      for (uint32_t base = 0; base < total && !overflow; base += 32) {
-        const uint32_t j = base + lane;
-        const bool valid = j < total;
-        const uint32_t owner = warp_find_owner(incl, valid ? j : total - 1);
-        const uint32_t ob = __shfl_sync(FULL, beg, owner);
-        const uint32_t oe = __shfl_sync(FULL, end, owner);
-        const uint32_t oexcl = __shfl_sync(FULL, incl, owner) -
-                               __shfl_sync(FULL, ng, owner);
-        uint32_t nu[4];
-        bool isnew[4];
-        if (valid) {
-          const uint32_t g = (ob >> 2) + (j - oexcl);
-          uint2 rec[4];
-          load_group(G.edges, g, rec);
-          const u32x4 c = ic_coins(key, g, s);
-#pragma unroll
-          for (int t = 0; t < 4; ++t) {
-            const uint32_t e = (g << 2) + t;
-            const bool live = e >= ob && e < oe && lane_of(c, t) < rec[t].y;
-            isnew[t] = false;
-            nu[t] = rec[t].x;
-            if (live) {
-              const uint32_t bit = 1u << (nu[t] & 31);
-              const uint32_t old = atomicOr(&W.bm[nu[t] >> 5], bit);
-              isnew[t] = !(old & bit);
-            }
-          }
-        } else {
-#pragma unroll
-          for (int t = 0; t < 4; ++t) {
-            isnew[t] = false;
-            nu[t] = 0;
-          }
-        }
-#pragma unroll
-        for (int t = 0; t < 4; ++t) {
-          const uint32_t bal = __ballot_sync(FULL, isnew[t]);
-          if (bal == 0) continue;
-          const uint32_t cnt = __popc(bal);
-          if (overflow || qlen + cnt > W.qcap) {
-            // Abandon the set: clear the bits of vertices that will never
-            // reach the queue (queued ones are cleared by finish_set).
-            if (isnew[t]) W.bm[nu[t] >> 5] = 0u;
-            overflow = true;
-            continue;
-          }
-          if (isnew[t]) W.q[qlen + __popc(bal & lanemask_lt())] = nu[t];
-          qlen += cnt;
-        }
-        __syncwarp();
-      }
-      head += take;
-    }
-    if (finish_set(W, qlen, overflow, s, rel, P, F, big)) {
+    const SetOutcome o = ic_plain_set(G, key, s, W, work_cap);
+    if (finish_set(W, o.qlen, o.overflow, s, rel, P, F, o.big)) {
       n_sets += (lane == 0);
-      n_elems += (lane == 0) ? qlen : 0;
-      n_exp += set_exp;
-      n_edges += set_edges;
+      n_elems += (lane == 0) ? o.qlen : 0;
+      n_exp += o.exp;
+      n_edges += o.edges;
     }
   }
   n_exp = warp_sum_u64(n_exp);
@@ -212,71 +303,12 @@ lt_walk_kernel(DevGraph G, DevPool P, Key key, uint64_t first, uint32_t count,
     if (idx >= count) break;
     const uint32_t rel = ids ? ids[idx] : idx;
     const uint64_t s = first + rel;
-    uint32_t cur = root_of(key, s, G.n);
-    if (lane == 0) {
-      W.q[0] = cur;
-      atomicOr(&W.bm[cur >> 5], 1u << (cur & 31));
-    }
-    __syncwarp();
-    uint32_t qlen = 1;
-    bool overflow = false;
-    unsigned long long set_exp = 0, set_edges = 0;
-    uint32_t t = lt_threshold(key, s, cur);
-    uint32_t lo = __ldg(G.off + cur), hi = __ldg(G.off + cur + 1);
-    for (;;) {
-      set_exp += (lane == 0);
-      if (hi == lo) break;
-      // 32-ary search for the first edge whose cumulative threshold exceeds t
-      bool none = false;
-      while (hi - lo > 32) {
-        const uint32_t stride = (hi - lo + 31) / 32;
-        const uint32_t p = min(lo + (lane + 1) * stride - 1, hi - 1);
-        const bool pred = t < __ldg(&G.edges[p].y);
-        const uint32_t bal = __ballot_sync(FULL, pred);
-        set_edges += (lane == 0) ? 32 : 0;
-        if (bal == 0) {  // even the last edge's cumulative weight is <= t
-          none = true;
-          break;
-        }
-        const uint32_t L = __ffs(bal) - 1;
-        const uint32_t nlo = lo + L * stride;
-        hi = min(hi, lo + (L + 1) * stride);
-        lo = nlo;
-      }
-      if (none) break;
-      const uint32_t e = lo + lane;
-      uint2 rec = make_uint2(0u, 0u);
-      if (e < hi) rec = __ldg(&G.edges[e]);
-      const uint32_t bal = __ballot_sync(FULL, e < hi && t < rec.y);
-      set_edges += (lane == 0) ? (hi - lo) : 0;
-      if (bal == 0) break;  // no in-edge picked: the walk ends here
-      const uint32_t u = __shfl_sync(FULL, rec.x, __ffs(bal) - 1);
-      uint32_t old = 0;
-      const uint32_t bit = 1u << (u & 31);
-      if (lane == 0) old = atomicOr(&W.bm[u >> 5], bit);
-      // next step's inputs, fetched while the atomic is in flight
-      const uint32_t t2 = lt_threshold(key, s, u);
-      const uint32_t lo2 = __ldg(G.off + u), hi2 = __ldg(G.off + u + 1);
-      const uint32_t seen = __shfl_sync(FULL, old & bit, 0);
-      if (seen) break;
-      if (qlen + 1 > W.qcap) {
-        if (lane == 0) W.bm[u >> 5] = 0u;
-        overflow = true;
-        break;
-      }
-      if (lane == 0) W.q[qlen] = u;
-      ++qlen;
-      cur = u;
-      t = t2;
-      lo = lo2;
-      hi = hi2;
-    }
-    __syncwarp();
-    if (finish_set(W, qlen, overflow, s, rel, P, F)) {
+    const SetOutcome o = lt_walk_set(G, key, s, W);
+    if (finish_set(W, o.qlen, o.overflow, s, rel, P, F)) {
       n_sets += (lane == 0);
-      n_elems += (lane == 0) ? qlen : 0;
-      n_exp += set_exp;
-      n_edges += set_edges;
+      n_elems += (lane == 0) ? o.qlen : 0;
+      n_exp += o.exp;
+      n_edges += o.edges;
     }
   }
   n_exp = warp_sum_u64(n_exp);

@@ -14,8 +14,8 @@
 // cover_kernel      after a pick: marks the seed's still-uncovered sets
 //                   covered and decrements the counts of their members
 //                   (UpdateCounters, include/ripples/counting.h:141-151),
-//                   reporting (vertex, count after) pairs straight to mapped
-//                   host memory so the host heap mirrors the counts exactly.
+//                   reporting each decremented vertex straight to mapped host
+//                   memory so the host heap mirrors the counts exactly.
 // heap kernels      the selection max-heap built on the device, level by
 //                   level, element for element the one std::make_heap builds.
 // argmax_kernel     max count, lowest vertex id on ties (thrust::max_element,
@@ -112,48 +112,37 @@ inverted_kernel(DevPool P, uint64_t S, uint64_t *cursor, uint32_t *inv) {
   }
 }
 
+// One warp per set of the seed's inverted list.  A set holds each vertex
+// once, so its members are decremented with plain reductions (no result
+// needed, nothing to aggregate); when asked, every decrement is reported as
+// the vertex id into a slot range the warp reserves for the whole set, and
+// the host mirror applies count[u] -= 1 per report.
 __global__ void __launch_bounds__(256) cover_kernel(CoverLaunch C) {
   const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const uint32_t lane = lane_id();
   const uint64_t lo = C.inv_off[C.vertex], hi = C.inv_off[C.vertex + 1];
-  const uint64_t cnt = hi - lo;
   unsigned long long newly = 0;
-  for (uint64_t wb = gw * 32; wb < cnt; wb += nw * 32) {
-    for_each_element(
-        C.P, wb, cnt,
-        [&](uint64_t i) -> uint64_t {
-          const uint32_t s = C.inv[lo + i];
-          if (C.covered[s]) return ~0ull;  // already covered by an earlier seed
-          C.covered[s] = 1;                // s holds the vertex once: no race
-          ++newly;
-          return s;
-        },
-        [&](uint64_t, uint32_t u, bool valid) {
-          // one leader per distinct vertex in the warp decrements and, when
-          // asked, reports the count it left; counts only fall during a pick,
-          // so the minimum of a vertex's reports is its count after the pick
-          const uint32_t peers = __match_any_sync(FULL, u);
-          const bool leader = valid && (__ffs(peers) - 1) == (int)lane_id();
-          uint32_t after = 0;
-          if (leader) {
-            const uint32_t k = (uint32_t)__popc(peers);
-            after = atomicSub(C.count + u, k) - k;
-          }
-          if (C.pairs) {
-            const uint32_t bal = __ballot_sync(FULL, leader);
-            if (bal) {
-              unsigned int b = 0;
-              if (lane_id() == (uint32_t)(__ffs(bal) - 1))
-                b = atomicAdd(C.dirty_n, (unsigned int)__popc(bal));
-              b = __shfl_sync(FULL, b, __ffs(bal) - 1);
-              const uint32_t idx = b + __popc(bal & lanemask_lt());
-              if (leader && idx < C.max_dirty) C.pairs[idx] = make_uint2(u, after);
-            }
-          }
-        });
+  for (uint64_t i = lo + gw; i < hi; i += nw) {
+    const uint32_t s = C.inv[i];
+    if (C.covered[s]) continue;  // covered by an earlier seed (warp-uniform)
+    const uint32_t len = C.P.set_len[s];
+    const uint64_t off = C.P.set_off[s];
+    unsigned int base = 0;
+    if (lane == 0) {
+      C.covered[s] = 1;  // s holds the vertex once: no other warp has s
+      ++newly;
+      if (C.reports) base = atomicAdd(C.dirty_n, len);
+    }
+    base = __shfl_sync(FULL, base, 0);
+    for (uint32_t j = lane; j < len; j += 32) {
+      const uint32_t u = C.P.vtx[off + j];
+      atomicSub(C.count + u, 1u);
+      if (C.reports && base + j < C.max_reports) C.reports[base + j] = u;
+    }
   }
   newly = warp_sum_u64(newly);
-  if (lane_id() == 0 && newly) atomicAdd(C.covered_sets, newly);
+  if (lane == 0 && newly) atomicAdd(C.covered_sets, newly);
 }
 
 __global__ void argmax_kernel(const uint32_t *count, uint32_t n,

@@ -122,10 +122,10 @@ struct CoverLaunch {
   uint32_t *count;
   unsigned int *dirty_n;
   unsigned long long *covered_sets;  // running total of newly covered sets
-  // When set, every decrement reports (vertex, count after it) here, at
-  // positions counted by dirty_n (entries past max_dirty are dropped).
-  uint2 *pairs;
-  uint32_t max_dirty;
+  // When set, every decrement reports its vertex here, at positions counted
+  // by dirty_n (reports past max_reports are dropped; dirty_n still counts).
+  uint32_t *reports;
+  uint32_t max_reports;
   int blocks;
 };
 void launch_cover(const CoverLaunch &C, cudaStream_t stream);
