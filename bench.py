@@ -43,6 +43,15 @@ WORKLOADS = {
                  k=50, eps=0.3, weights="lt_normalized"),
     "ic14": dict(name="imm_ic_rmat14_2^18_k20_eps0.5", scale=14, draws=1 << 18, model="IC",
                  k=20, eps=0.5, weights="uniform_0_0.1"),
+    # 64 IMM instances over 16 graphs (ER + R-MAT, 2^12..2^22 vertices, average
+    # degree 4..64; half IC p ~ U(0,0.05), half LT normalised), k ~ U[10,200],
+    # eps ~ U[0.1,0.5], generator seed 2: batched (one continuous batch, one
+    # sampling launch per round) against one plain IMM at a time
+    "b1": dict(name="batch_64_imm_16_graphs", kind="batch"),
+    # request loop: resident R-MAT graphs 2^18..2^24 (degree 16) with IC
+    # p ~ U(0,0.1) and LT normalised weights, Poisson arrivals at 200 req/s
+    # (seed 3), k log-uniform in [5,500], eps in {0.5,0.3,0.13}, IC/LT 50/50
+    "s1": dict(name="serve_rmat18-24_poisson200", kind="serve"),
 }
 METRIC = "RRR sets/s (full IMM)"
 
@@ -241,9 +250,19 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="lt20", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve-scales", default="18,20,22,24",
+                    help="s1: R-MAT scales of the resident graphs")
+    ap.add_argument("--serve-queries", type=int, default=256)
+    ap.add_argument("--serve-eps", default="0.5,0.3,0.13")
+    ap.add_argument("--serve-max-active", type=int, default=32)
+    ap.add_argument("--baseline-seconds", type=float, default=60.0)
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
     world, rank, local = dist_setup()
+    if w.get("kind") == "batch":
+        return run_batch(args, w, world, rank, local)
+    if w.get("kind") == "serve":
+        return run_serve(args, w, world, rank, local)
     if args.impl == "reference":
         rc = reference_arm(args, w, world, rank)
         if world > 1:
@@ -399,6 +418,220 @@ def main():
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+    return 0
+
+
+def _pct(xs, q):
+    import numpy as np
+    return float(np.percentile(np.asarray(xs, dtype=np.float64), q)) if xs else None
+
+
+def _not_on_rank0(world, rank, args, w):
+    """Batch and serve workloads run on rank 0 only (one GPU each: the path
+    does not shard); the other ranks exit without work."""
+    return rank != 0
+
+
+def run_batch(args, w, world, rank, local):
+    import numpy as np
+    import torch
+    import ripples_b200 as rb
+    if _not_on_rank0(world, rank, args, w):
+        return 0
+    torch.cuda.set_device(local)
+    rng = np.random.default_rng(2)
+    ctx = rb.Context(local)
+    graphs = []
+    for i in range(16):
+        scale = int(rng.integers(12, 23))
+        deg = int(rng.choice([4, 8, 16, 32, 64]))
+        kind = "er" if i % 2 else "rmat"
+        model = "IC" if (i // 2) % 2 == 0 else "LT"
+        wk = rb.WEIGHTS_UNIFORM if model == "IC" else rb.WEIGHTS_LT_NORMALIZED
+        if kind == "rmat":
+            dg = rb.DeviceGraph.rmat_on_device(ctx, scale, deg << scale, model, wk, seed=i,
+                                               weight_seed=100 + i, lo=0.0, hi=0.05)
+        else:
+            hg = rb.HostGraph.erdos_renyi(1 << scale, deg << scale, seed=i)
+            hg = hg.with_weights(wk, seed=100 + i, lo=0.0, hi=0.05)
+            dg = rb.DeviceGraph(ctx, hg, model)
+        graphs.append(dict(dg=dg, scale=scale, deg=deg, kind=kind, model=model))
+    inst = []
+    for j in range(64):
+        gi = int(rng.integers(0, 16))
+        inst.append(dict(g=gi, k=int(rng.integers(10, 201)), eps=float(rng.uniform(0.1, 0.5)),
+                         seed=10_000 + j))
+
+    def batched(tag):
+        qs = [rb.Query(graphs[x["g"]]["dg"], x["k"], x["eps"], seed=x["seed"] + tag)
+              for x in inst]
+        rb.imm_batch(ctx, qs)
+        return qs
+
+    def plain(tag, limit_s=None):
+        out, t0 = [], time.perf_counter()
+        for x in inst:
+            p = rb.Pool(graphs[x["g"]]["dg"])
+            seeds, rec = p.imm(x["k"], x["eps"], seed=x["seed"] + tag,
+                               tiebreak=rb.TIE_LOWEST_ID, sampler=rb.SAMPLER_PLAIN)
+            out.append((seeds, rec.total_sets))
+            p.close()
+            if limit_s and time.perf_counter() - t0 > limit_s:
+                break
+        return out
+
+    for i in range(args.warmup):
+        batched(1_000_000 * (i + 1))
+    launches0 = rb._lib.lib.rip_kernel_launches()
+    clocks = ClockSampler(local)
+    clocks.start()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    sets = 0
+    last = None
+    for s in range(args.steps):
+        last = batched(0 if s == 0 else 7 * s)
+        sets += sum(q.record.total_sets for q in last)
+    torch.cuda.synchronize()
+    t_b = time.perf_counter() - t0
+    clk = clocks.stop()
+    launches = int(rb._lib.lib.rip_kernel_launches() - launches0)
+    # plain one-instance-at-a-time path on the same instances (step 0 seeds)
+    plain(12345, limit_s=5)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    pl = plain(0, limit_s=args.baseline_seconds)
+    torch.cuda.synchronize()
+    t_p = time.perf_counter() - t0
+    first = batched(0)
+    same = all(np.array_equal(a[0], q.seeds) for a, q in zip(pl, first))
+    p_sets = sum(x[1] for x in pl)
+    line = {"metric": "RRR sets/s (64 batched IMM instances)", "value": sets / t_b,
+            "unit": "sets/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * t_b / args.steps, "higher_is_better": True,
+            "scaling": "replicas only", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic ER/R-MAT graphs and weights (generator seed 2)",
+            "config": {"workload": w["name"], "instances": 64,
+                       "graphs": [{k: v for k, v in g.items() if k != "dg"} for g in graphs],
+                       "tiebreak": "lowest id (device picks)"},
+            "plain_one_at_a_time": {"value": p_sets / t_p, "unit": "sets/s",
+                                    "instances": len(pl), "seconds": t_p,
+                                    "imm_per_s": len(pl) / t_p},
+            "batched_imm_per_s": 64 * args.steps / t_b,
+            "speedup_vs_plain": (sets / t_b) / (p_sets / t_p),
+            "same_seeds_as_plain": bool(same),
+            "e2e": {"value": sets / t_b, "unit": "sets/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": int(sum(4 * x["k"] for x in inst)),
+                    "note": "queries and seeds cross the host boundary; graphs resident"},
+            "clocks": clk, "gpu_launches": launches}
+    print(json.dumps(line))
+    ctx.close()
+    return 0
+
+
+def run_serve(args, w, world, rank, local):
+    import numpy as np
+    import torch
+    import ripples_b200 as rb
+    if _not_on_rank0(world, rank, args, w):
+        return 0
+    torch.cuda.set_device(local)
+    ctx = rb.Context(local)
+    scales = [int(x) for x in args.serve_scales.split(",") if x]
+    eps_choices = [float(x) for x in args.serve_eps.split(",") if x]
+    graphs = {}
+    t_build = time.perf_counter()
+    for sc in scales:
+        graphs[(sc, "IC")] = rb.DeviceGraph.rmat_on_device(
+            ctx, sc, 16 << sc, "IC", rb.WEIGHTS_UNIFORM, seed=0, weight_seed=1, lo=0.0, hi=0.1)
+        graphs[(sc, "LT")] = rb.DeviceGraph.rmat_on_device(
+            ctx, sc, 16 << sc, "LT", rb.WEIGHTS_LT_NORMALIZED, seed=0, weight_seed=1)
+    t_build = time.perf_counter() - t_build
+    rng = np.random.default_rng(3)
+    N = args.serve_queries
+    arrivals = np.cumsum(rng.exponential(1.0 / 200.0, size=N))
+    arrivals -= arrivals[0]
+    spec = []
+    for i in range(N):
+        sc = scales[int(rng.integers(0, len(scales)))]
+        model = "IC" if rng.random() < 0.5 else "LT"
+        k = int(round(float(np.exp(rng.uniform(np.log(5), np.log(500))))))
+        eps = eps_choices[int(rng.integers(0, len(eps_choices)))]
+        spec.append(dict(scale=sc, model=model, k=k, eps=eps))
+    used, budget = ctx.memory()
+    fp_budget = min(150 << 30, int(0.8 * budget))
+    srv = rb.Server(ctx, footprint_budget=fp_budget, max_active=args.serve_max_active)
+    qs = [rb.Query(graphs[(s["scale"], s["model"])], s["k"], s["eps"], seed=3) for s in spec]
+    launches0 = rb._lib.lib.rip_kernel_launches()
+    clocks = ClockSampler(local)
+    clocks.start()
+    torch.cuda.synchronize()
+    sub_t = [0.0] * N
+    t0 = time.perf_counter()
+    nxt = 0
+    while True:
+        now = time.perf_counter() - t0
+        while nxt < N and arrivals[nxt] <= now:
+            srv.submit(qs[nxt])
+            sub_t[nxt] = now
+            nxt += 1
+        active, queued = srv.pending()
+        if active == 0 and queued == 0:
+            if nxt >= N:
+                break
+            time.sleep(max(0.0, arrivals[nxt] - (time.perf_counter() - t0)))
+            continue
+        srv.tick()
+    torch.cuda.synchronize()
+    makespan = time.perf_counter() - t0
+    clk = clocks.stop()
+    launches = int(rb._lib.lib.rip_kernel_launches() - launches0)
+    ok = [q for q in qs if q.status == 0]
+    lat = [1e3 * (sub_t[i] - arrivals[i]) + qs[i].latency_ms for i in range(N) if qs[i].status == 0]
+    st = srv.stats()
+    srv.close()
+    # plain path, one query at a time (fresh pool, one set per warp), on the
+    # queries in arrival order until the time budget runs out
+    torch.cuda.synchronize()
+    tb = time.perf_counter()
+    base, same = [], True
+    for i in range(N):
+        s = spec[i]
+        p = rb.Pool(graphs[(s["scale"], s["model"])])
+        t1 = time.perf_counter()
+        seeds, rec = p.imm(s["k"], s["eps"], seed=3, tiebreak=rb.TIE_LOWEST_ID,
+                           sampler=rb.SAMPLER_PLAIN)
+        base.append(1e3 * (time.perf_counter() - t1))
+        p.close()
+        same = same and qs[i].status == 0 and np.array_equal(seeds, qs[i].seeds)
+        if time.perf_counter() - tb > args.baseline_seconds:
+            break
+    t_base = time.perf_counter() - tb
+    base_qps = len(base) / t_base
+    line = {"metric": "IMM queries/s (serving loop)", "value": len(ok) / makespan,
+            "unit": "queries/s", "n_gpus": 1, "steps": N, "warmup": 0,
+            "ms_per_step": 1e3 * makespan / max(N, 1), "higher_is_better": True,
+            "scaling": "replicas only", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic R-MAT graphs (seed 0) and weights (seed 1); query stream seed 3",
+            "config": {"workload": w["name"], "scales": scales, "degree": 16,
+                       "arrival_rate": 200, "queries": N, "eps": eps_choices,
+                       "k": "log-uniform 5..500", "max_active": args.serve_max_active,
+                       "footprint_budget_gb": fp_budget / 2**30},
+            "latency_ms": {"p50": _pct(lat, 50), "p99": _pct(lat, 99), "max": max(lat) if lat else None},
+            "completed": len(ok), "failed": N - len(ok), "makespan_s": makespan,
+            "plain_one_at_a_time": {"value": base_qps, "unit": "queries/s",
+                                    "queries": len(base), "seconds": t_base,
+                                    "service_ms_p50": _pct(base, 50),
+                                    "service_ms_p99": _pct(base, 99)},
+            "speedup_vs_plain": (len(ok) / makespan) / base_qps if base_qps else None,
+            "same_seeds_as_plain": bool(same),
+            "server": st, "graph_build_s": t_build,
+            "e2e": {"value": len(ok) / makespan, "unit": "queries/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": int(np.mean([4 * s["k"] for s in spec])),
+                    "note": "queries and seeds cross the host boundary; graphs resident"},
+            "clocks": clk, "gpu_launches": launches}
+    print(json.dumps(line))
+    ctx.close()
     return 0
 
 

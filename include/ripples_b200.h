@@ -245,6 +245,59 @@ int rip_imm_pool(rip_pool *p, uint32_t k, double epsilon, double l,
                  uint64_t seed, int tiebreak, int sampler, uint32_t *seeds,
                  uint32_t *num_seeds, rip_imm_record *record);
 
+/* ---- batching and serving --------------------------------------------------- */
+/* No counterpart in the reference (its GenerateRRRSets, include/ripples/
+ * generate_rrr_sets.h:60-120, fills one instance's sets per call).  Extends
+ * n_pools pools (all of this context, each listed once) by counts[i] sets of
+ * seeds[i] in ONE persistent launch whose warps pull (pool, set) work items
+ * from a single device counter; sets are identical to rip_sample's. */
+int rip_sample_multi(rip_ctx *ctx, rip_pool *const *pools, const uint64_t *seeds,
+                     const uint64_t *counts, uint32_t n_pools);
+
+/* One IMM query for rip_imm_batch / rip_server_*.  The answer equals a fresh
+ * rip_imm(graph, k, epsilon, l, seed, tiebreak) whatever it is batched with;
+ * queries with equal (graph, seed) share one resident pool. */
+typedef struct rip_imm_query {
+  rip_graph *graph;       /* in: the graph (its model: IC or LT) */
+  uint32_t k;             /* in */
+  double epsilon;         /* in */
+  double l;               /* in: the reference's l (the imm tool passes 1) */
+  uint64_t seed;          /* in: sampler seed */
+  int tiebreak;           /* in: RIP_TIE_LOWEST_ID (picks on the device, in a
+                             CUDA graph) or RIP_TIE_REF_HEAP (host heap) */
+  uint32_t *seeds;        /* in: caller buffer of k entries; out: the seeds */
+  uint32_t num_seeds;     /* out */
+  int status;             /* out: RIP_OK or an error code, once done != 0 */
+  int done;               /* out: set when the query has finished */
+  double f;               /* out: covered fraction of the final selection */
+  double queue_ms;        /* out: submit -> admission */
+  double latency_ms;      /* out: submit -> done */
+  rip_imm_record record;  /* out; pool_elements/rrr_set_bytes describe the
+                             shared pool */
+} rip_imm_query;
+
+/* Runs n queries to completion as one continuous batch. */
+int rip_imm_batch(rip_ctx *ctx, rip_imm_query *queries, uint32_t n);
+
+/* Request loop: queries are submitted at any time and admitted at the next
+ * tick while one of max_active slots is free and the sum of the admitted
+ * queries' estimated footprints (theta x mean set size, selection buffers)
+ * stays within footprint_budget bytes (0 = half the context budget; a query
+ * is always admitted when none is active).  Each tick samples every pool's
+ * shortfall in one launch and runs one martingale round (or the final
+ * selection) of every admitted query, their device picks concurrently on
+ * per-slot streams.  The query struct must stay valid until done != 0. */
+typedef struct rip_server rip_server;
+int rip_server_create(rip_ctx *ctx, size_t footprint_budget, uint32_t max_active,
+                      rip_server **out);
+int rip_server_destroy(rip_server *s);
+int rip_server_submit(rip_server *s, rip_imm_query *q);
+int rip_server_tick(rip_server *s, uint32_t *completed);
+int rip_server_pending(const rip_server *s, uint32_t *active, uint32_t *queued);
+/* [0] ticks, [1] completed, [2] selection-graph launches, [3] resident pools,
+ * [4] admitted footprint bytes, [5] microseconds spent in ticks */
+int rip_server_stats(const rip_server *s, uint64_t out[6]);
+
 /* ---- sampling without allocation ------------------------------------------- */
 /* No counterpart in the reference.  A variant of rip_sample's one-set-per-warp
  * samplers (IC BFS / LT walk) for callers that cannot allocate device memory

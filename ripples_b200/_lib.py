@@ -58,6 +58,25 @@ class ImmRecord(ctypes.Structure):
     ]
 
 
+class ImmQuery(ctypes.Structure):
+    _fields_ = [
+        ("graph", ctypes.c_void_p),
+        ("k", ctypes.c_uint32),
+        ("epsilon", ctypes.c_double),
+        ("l", ctypes.c_double),
+        ("seed", ctypes.c_uint64),
+        ("tiebreak", ctypes.c_int),
+        ("seeds", ctypes.c_void_p),
+        ("num_seeds", ctypes.c_uint32),
+        ("status", ctypes.c_int),
+        ("done", ctypes.c_int),
+        ("f", ctypes.c_double),
+        ("queue_ms", ctypes.c_double),
+        ("latency_ms", ctypes.c_double),
+        ("record", ImmRecord),
+    ]
+
+
 P = ctypes.c_void_p
 U32, U64, I32, I64, DBL, SZ = (ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int,
                                ctypes.c_int64, ctypes.c_double, ctypes.c_size_t)
@@ -101,6 +120,14 @@ SIGNATURES = {
                       ctypes.POINTER(ImmRecord)]),
     "rip_imm_pool": (I32, [P, U32, DBL, DBL, U64, I32, I32, P, ctypes.POINTER(U32),
                            ctypes.POINTER(ImmRecord)]),
+    "rip_sample_multi": (I32, [P, P, P, P, U32]),
+    "rip_imm_batch": (I32, [P, ctypes.POINTER(ImmQuery), U32]),
+    "rip_server_create": (I32, [P, SZ, U32, PP]),
+    "rip_server_destroy": (I32, [P]),
+    "rip_server_submit": (I32, [P, ctypes.POINTER(ImmQuery)]),
+    "rip_server_tick": (I32, [P, ctypes.POINTER(U32)]),
+    "rip_server_pending": (I32, [P, ctypes.POINTER(U32), ctypes.POINTER(U32)]),
+    "rip_server_stats": (I32, [P, P]),
     "rip_sample_static": (I32, [P, P, U32, U64, I32, U64, U64, U32, P, U64, P, P,
                                 ctypes.POINTER(U64), P]),
     "rip_static_last_error": (ctypes.c_char_p, []),

@@ -4,229 +4,7 @@
 // growable RRR pool, the sampler launch/retry loop, seed selection (device
 // counts + the reference's lazy max-heap on the host) and the IMM driver
 // (include/ripples/imm.h:145-260, 768-860).
-#include <algorithm>
-#include <chrono>
-#include <cmath>
-#include <cstdarg>
-#include <cstdio>
-#include <cstring>
-#include <queue>
-#include <string>
-#include <utility>
-#include <vector>
-
-#include <sys/types.h>
-
-#include "launch.h"
-#include "ripples_b200.h"
-
-using namespace rip;
-
-namespace {
-
-using clk = std::chrono::high_resolution_clock;
-double ms_since(clk::time_point t0) {
-  return std::chrono::duration<double, std::milli>(clk::now() - t0).count();
-}
-
-}  // namespace
-
-// ---------------------------------------------------------------------------
-// context, memory
-// ---------------------------------------------------------------------------
-struct DevMem {
-  void *p = nullptr;
-  size_t bytes = 0;
-};
-
-// The reference's heap holds std::pair<vertex, size_t count> ordered by count
-// alone (CompareHeap, include/ripples/streaming_find_most_influential.h:410-418).
-// The heap algorithms only move elements and compare them with the
-// comparator, so an 8-byte {vertex, u32 count} item with the same comparison
-// yields the same sequence of heaps (counts never exceed the number of sets,
-// < 2^32), at half the memory.
-struct HeapItem {
-  uint32_t first;   // vertex
-  uint32_t second;  // count when pushed
-  bool operator==(const HeapItem &o) const { return first == o.first && second == o.second; }
-};
-struct CompareHeap {
-  bool operator()(const HeapItem &a, const HeapItem &b) const { return a.second < b.second; }
-};
-struct PinnedMem;
-
-struct rip_ctx {
-  std::vector<rip_graph *> graphs;  // owned: freed by rip_ctx_destroy
-  std::vector<rip_pool *> pools;    // owned: freed by rip_ctx_destroy
-  // Device blocks released by graphs/pools, kept for reuse (a graph upload
-  // or a new pool then costs no cudaMalloc); counted in `used`.
-  std::vector<DevMem> cache;
-  size_t cached = 0;
-  PinnedMem *h_pairs = nullptr;  // mapped: per-pick decrement reports
-  PinnedMem *h_count = nullptr;  // counts at the start of a selection
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  int num_sms = 148;
-  size_t budget = 0;
-  size_t used = 0;
-  std::string err;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-};
-
-static int set_err(rip_ctx *c, int code, const char *fmt, ...) {
-  if (c) {
-    char buf[512];
-    va_list ap;
-    va_start(ap, fmt);
-    vsnprintf(buf, sizeof(buf), fmt, ap);
-    va_end(ap);
-    c->err = buf;
-  }
-  return code;
-}
-
-#define CK(c, call)                                                          \
-  do {                                                                       \
-    cudaError_t e_ = (call);                                                 \
-    if (e_ != cudaSuccess)                                                   \
-      return set_err((c), RIP_ERR_CUDA, "%s failed: %s (%s:%d)", #call,      \
-                     cudaGetErrorString(e_), __FILE__, __LINE__);            \
-  } while (0)
-
-#define TRY(expr)              \
-  do {                         \
-    int r_ = (expr);           \
-    if (r_ != RIP_OK) return r_; \
-  } while (0)
-
-static void cache_release_all(rip_ctx *c) {
-  if (!c->cache.empty()) cudaStreamSynchronize(c->stream);
-  for (DevMem &b : c->cache) {
-    cudaFree(b.p);
-    c->used -= b.bytes;
-  }
-  c->cache.clear();
-  c->cached = 0;
-}
-
-// Returns a block to the context cache (or frees it when the cache is full).
-static void cache_put(rip_ctx *c, DevMem m) {
-  if (!m.p) return;
-  const size_t limit = c->budget / 4;
-  if (m.bytes > limit) {
-    cudaStreamSynchronize(c->stream);
-    cudaFree(m.p);
-    c->used -= m.bytes;
-    return;
-  }
-  while (c->cached + m.bytes > limit && !c->cache.empty()) {
-    cudaStreamSynchronize(c->stream);
-    cudaFree(c->cache.front().p);
-    c->used -= c->cache.front().bytes;
-    c->cached -= c->cache.front().bytes;
-    c->cache.erase(c->cache.begin());
-  }
-  c->cache.push_back(m);
-  c->cached += m.bytes;
-}
-
-// Takes the smallest cached block of at least `bytes` (and at most twice that).
-static bool cache_take(rip_ctx *c, size_t bytes, DevMem &out) {
-  size_t best = c->cache.size();
-  for (size_t i = 0; i < c->cache.size(); ++i) {
-    const size_t b = c->cache[i].bytes;
-    if (b >= bytes && b <= 2 * bytes + (1u << 20) &&
-        (best == c->cache.size() || b < c->cache[best].bytes))
-      best = i;
-  }
-  if (best == c->cache.size()) return false;
-  out = c->cache[best];
-  c->cached -= out.bytes;
-  c->cache.erase(c->cache.begin() + best);
-  return true;
-}
-
-static int dalloc(rip_ctx *c, DevMem &m, size_t bytes) {
-  if (m.p && m.bytes >= bytes) return RIP_OK;
-  bytes = std::max<size_t>((bytes + 255) & ~(size_t)255, 256);
-  DevMem fresh;
-  if (!cache_take(c, bytes, fresh)) {
-    if (c->used + bytes > c->budget) cache_release_all(c);
-    if (c->used + bytes > c->budget)
-      return set_err(c, RIP_ERR_NOMEM,
-                     "device budget exceeded: need %zu more bytes (used %zu of %zu)",
-                     bytes, c->used, c->budget);
-    cudaError_t e = cudaMalloc(&fresh.p, bytes);
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      cache_release_all(c);
-      e = cudaMalloc(&fresh.p, bytes);
-      if (e != cudaSuccess) {
-        cudaGetLastError();
-        return set_err(c, RIP_ERR_NOMEM, "cudaMalloc(%zu) failed: %s", bytes,
-                       cudaGetErrorString(e));
-      }
-    }
-    fresh.bytes = bytes;
-    c->used += bytes;
-  }
-  cache_put(c, m);
-  m = fresh;
-  return RIP_OK;
-}
-
-// Grows m to `bytes`, preserving the first `keep` bytes.
-static int dgrow(rip_ctx *c, DevMem &m, size_t bytes, size_t keep) {
-  if (m.p && m.bytes >= bytes) return RIP_OK;
-  DevMem n;
-  TRY(dalloc(c, n, bytes));
-  if (m.p && keep) {
-    CK(c, cudaMemcpyAsync(n.p, m.p, std::min(keep, m.bytes),
-                          cudaMemcpyDeviceToDevice, c->stream));
-    CK(c, cudaStreamSynchronize(c->stream));
-  }
-  cache_put(c, m);
-  m = n;
-  return RIP_OK;
-}
-
-static void dfree(rip_ctx *c, DevMem &m) {
-  cache_put(c, m);
-  m = DevMem{};
-}
-
-template <typename T>
-static T *ptr(DevMem &m) {
-  return reinterpret_cast<T *>(m.p);
-}
-
-struct PinnedMem {
-  void *p = nullptr;
-  void *dev = nullptr;  // device alias when mapped
-  size_t bytes = 0;
-  int ensure(rip_ctx *c, size_t b, bool mapped = false) {
-    if (p && bytes >= b) return RIP_OK;
-    if (p) cudaFreeHost(p);
-    p = dev = nullptr;
-    bytes = 0;
-    if (cudaHostAlloc(&p, b, mapped ? cudaHostAllocMapped : cudaHostAllocDefault) !=
-        cudaSuccess) {
-      cudaGetLastError();
-      return set_err(c, RIP_ERR_NOMEM, "cudaHostAlloc(%zu) failed", b);
-    }
-    if (mapped && cudaHostGetDevicePointer(&dev, p, 0) != cudaSuccess) {
-      cudaGetLastError();
-      cudaFreeHost(p);
-      p = nullptr;
-      return set_err(c, RIP_ERR_CUDA, "cudaHostGetDevicePointer failed");
-    }
-    bytes = b;
-    return RIP_OK;
-  }
-  ~PinnedMem() {
-    if (p) cudaFreeHost(p);
-  }
-};
+#include "host.h"
 
 extern "C" {
 
@@ -271,11 +49,16 @@ int rip_ctx_destroy(rip_ctx *c) {
   if (!c) return RIP_ERR_INVALID;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  while (!c->servers.empty()) rip_server_destroy(c->servers.back());
   while (!c->pools.empty()) rip_pool_destroy(c->pools.back());
   while (!c->graphs.empty()) rip_graph_destroy(c->graphs.back());
   cache_release_all(c);
+  dfree(c, c->m_scratch);
+  dfree(c, c->m_table);
+  dfree(c, c->m_fail);
   delete c->h_pairs;
   delete c->h_count;
+  delete c->h_meta;
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -314,16 +97,6 @@ int rip_ctx_memory(rip_ctx *c, size_t *used, size_t *budget) {
 // graph
 // ---------------------------------------------------------------------------
 static rip_graph *pool_graph(const rip_pool *p);
-struct rip_graph {
-  rip_ctx *ctx;
-  uint32_t n;
-  uint64_t m;
-  int model;
-  DevMem off, edges;
-  DevGraph view() {
-    return DevGraph{n, m, ptr<uint32_t>(off), ptr<uint2>(edges)};
-  }
-};
 
 extern "C" int rip_graph_upload(rip_ctx *c, const uint64_t *index,
                                 const uint32_t *src, const float *w, uint32_t n,
@@ -507,6 +280,7 @@ extern "C" int rip_graph_destroy(rip_graph *g) {
   rip_ctx *c = g->ctx;
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
+  server_graph_gone(c, g);
   // pools sample from this graph: they go first
   std::vector<rip_pool *> mine;
   for (rip_pool *p : c->pools)
@@ -544,66 +318,6 @@ extern "C" int rip_graph_thresholds(rip_graph *g, uint32_t *thr) {
 // ---------------------------------------------------------------------------
 // pool
 // ---------------------------------------------------------------------------
-struct PoolMeta {  // device-side bookkeeping block (one D2H reads it all)
-  unsigned long long cursor;
-  unsigned long long first_bad;
-  unsigned long long stats[8];
-  unsigned int fail_count;
-  unsigned int next;
-  unsigned int dirty_n;
-  unsigned int fused_dirty;
-  unsigned long long best;
-  unsigned long long covered_sets;
-};
-
-struct rip_pool {
-  rip_ctx *ctx;
-  rip_graph *g;
-  DevMem vtx, set_off, set_len, meta;
-  uint64_t cap = 0, set_cap = 0;
-  uint64_t num_sets = 0, num_elems = 0;
-  // sampler scratch (one buffer partitioned into per-warp bitmap + queue)
-  DevMem scratch, ids_a, ids_b;
-  uint64_t bm_words = 0;
-  uint32_t qcap = 0;
-  uint32_t warps = 0;
-  // fused sampler scratch (per slot: colour masks, pending masks, level
-  // flags, frontier log); all-zero between batches
-  DevMem f_vis, f_pend, f_flag, f_log, f_order;
-  uint32_t f_slots = 0, f_cw = 0, f_lcap = 0;
-  // CTA-per-set scratch for sets with very large edge work
-  DevMem b_scratch, b_ids;
-  uint32_t b_slots = 0, b_qcap = 0;
-  uint64_t cap_plain = 1ull << 18;  // in-edges per set before a warp hands it over
-  uint64_t cap_fused = 1ull << 23;  // in-edges per fused batch before handing over
-  uint64_t big_sets = 0;            // sets grown one CTA each (diagnostic)
-  uint32_t colors = 64;      // fused colour width (64/128/256)
-  uint32_t fused_slots = 0;  // 0 = size from the budget
-  uint32_t lcap_pref = 0;    // 0 = default frontier-log capacity
-  // selection state
-  DevMem count, inv_off, inv_cur, inv, covered,
-      scan_sums;
-  std::vector<uint32_t> last_counts;
-  bool have_last_counts = false;
-  std::vector<HeapItem> heap_store;  // heap storage reused across selections
-  void *heap_registered = nullptr;   // heap_store's buffer while page-locked
-  size_t heap_registered_bytes = 0;
-  DevMem d_heap;                     // heap built on the device
-  // selection profile: [0] count+index kernels and counts D2H, [1] heap build,
-  // [2] pick loop, [3] heap pops, [4] picks, [5] count reports, [6] selections,
-  // [7] ms in cover launch + sync, [8] ms applying reports, [9] ms in heap pops
-  double sel_prof[12] = {0};
-  // timing of sampler kernels (CUDA events on the context stream)
-  double kernel_ms = 0.0;
-  uint64_t kernel_launches = 0;
-  double select_kernel_ms = 0.0;
-
-  PoolMeta *dmeta() { return ptr<PoolMeta>(meta); }
-  DevPool view() {
-    return DevPool{ptr<uint32_t>(vtx), &dmeta()->cursor, cap,
-                   ptr<uint64_t>(set_off), ptr<uint32_t>(set_len)};
-  }
-};
 
 static rip_graph *pool_graph(const rip_pool *p) { return p->g; }
 
@@ -643,7 +357,8 @@ extern "C" int rip_pool_destroy(rip_pool *p) {
                    &p->b_scratch, &p->b_ids,   &p->d_heap,
                    &p->count,   &p->inv_off,   &p->inv_cur,  &p->inv,
                    &p->covered,
-                   &p->scan_sums};
+                   &p->scan_sums, &p->sv_count, &p->sv_off, &p->sv_cur,
+                   &p->sv_inv,  &p->sv_sums};
   for (DevMem *m : all) dfree(c, *m);
   if (p->heap_registered) cudaHostUnregister(p->heap_registered);
   erase_ptr(c->pools, p);
@@ -661,6 +376,7 @@ extern "C" int rip_pool_clear(rip_pool *p) {
   for (double &x : p->sel_prof) x = 0.0;
   p->kernel_launches = 0;
   p->have_last_counts = false;
+  p->sv_sets = 0;
   return RIP_OK;
 }
 
@@ -1563,6 +1279,196 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
   }
   *num_seeds = (uint32_t)out_seeds.size();
   if (f) *f = S ? double(S - uncovered) / (double)S : 0.0;
+  return RIP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// many pools in one launch
+// ---------------------------------------------------------------------------
+// Sets of every pool come from the same one-set-per-warp bodies as rip_sample
+// (same set ids, same Philox streams), so a pool extended here holds exactly
+// the sets rip_sample would have put there.  Sets that fail in the shared
+// launch (queue or pool overflow, IC edge work over the cap) are finished per
+// pool by the single-pool paths.
+extern "C" int rip_sample_multi(rip_ctx *c, rip_pool *const *pools, const uint64_t *seeds,
+                                const uint64_t *counts, uint32_t n_pools) {
+  if (!c || (n_pools && (!pools || !seeds || !counts))) return RIP_ERR_INVALID;
+  uint64_t total = 0;
+  for (uint32_t i = 0; i < n_pools; ++i) {
+    if (!pools[i] || pools[i]->ctx != c)
+      return set_err(c, RIP_ERR_INVALID, "rip_sample_multi: pool %u is not of this context", i);
+    for (uint32_t j = 0; j < i; ++j)
+      if (pools[j] == pools[i] && counts[i] && counts[j])
+        return set_err(c, RIP_ERR_INVALID, "rip_sample_multi: pool %u listed twice", i);
+    if (counts[i] >= (1ull << 31))
+      return set_err(c, RIP_ERR_LIMIT, "rip_sample_multi: at most 2^31-1 sets per pool");
+    if (pools[i]->num_sets + counts[i] >= (1ull << 56))
+      return set_err(c, RIP_ERR_LIMIT, "rip_sample_multi: set ids are limited to 2^56");
+    total += counts[i];
+  }
+  if (total == 0) return RIP_OK;
+  if (total >= (1ull << 32) - 1)
+    return set_err(c, RIP_ERR_LIMIT, "rip_sample_multi: at most 2^32-2 sets per call");
+  CK(c, cudaSetDevice(c->device));
+  std::vector<uint32_t> act;  // pools with work
+  for (uint32_t i = 0; i < n_pools; ++i)
+    if (counts[i]) act.push_back(i);
+  // per-pool meta (set-size means for the pool sizing), read in one sync
+  if (!c->h_meta) c->h_meta = new PinnedMem();
+  TRY(c->h_meta->ensure(c, sizeof(PoolMeta) * act.size()));
+  PoolMeta *hm = reinterpret_cast<PoolMeta *>(c->h_meta->p);
+  for (size_t a = 0; a < act.size(); ++a)
+    CK(c, cudaMemcpyAsync(hm + a, pools[act[a]]->meta.p, sizeof(PoolMeta),
+                          cudaMemcpyDeviceToHost, c->stream));
+  CK(c, cudaStreamSynchronize(c->stream));
+  {
+    // Fresh pools with large requests first take a pilot of 1024 sets (as
+    // rip_sample does) so they are sized from a measured mean set size.
+    std::vector<rip_pool *> pp;
+    std::vector<uint64_t> ps, pc;
+    for (size_t a = 0; a < act.size(); ++a)
+      if (hm[a].stats[2] == 0 && counts[act[a]] > 4096) {
+        pp.push_back(pools[act[a]]);
+        ps.push_back(seeds[act[a]]);
+        pc.push_back(1024);
+      }
+    if (!pp.empty()) {
+      TRY(rip_sample_multi(c, pp.data(), ps.data(), pc.data(), (uint32_t)pp.size()));
+      std::vector<uint64_t> rest(counts, counts + n_pools);
+      for (uint32_t i = 0; i < n_pools; ++i)
+        for (rip_pool *q : pp)
+          if (pools[i] == q && rest[i]) {
+            rest[i] -= 1024;
+            break;
+          }
+      return rip_sample_multi(c, pools, seeds, rest.data(), n_pools);
+    }
+  }
+  uint64_t max_n = 1;
+  std::vector<uint64_t> firsts(act.size());
+  for (size_t a = 0; a < act.size(); ++a) {
+    rip_pool *p = pools[act[a]];
+    const uint64_t cnt = counts[act[a]];
+    max_n = std::max<uint64_t>(max_n, p->g->n);
+    firsts[a] = p->num_sets;
+    TRY(ensure_sets(p, p->num_sets + cnt));
+    const double mean = hm[a].stats[2] ? (double)hm[a].stats[3] / (double)hm[a].stats[2] : 8.0;
+    TRY(ensure_elems(p, p->num_elems + (uint64_t)(mean * 1.25 * cnt) + 1024));
+  }
+  // shared per-warp scratch, sized for the largest graph of the launch
+  const uint64_t bm_words = ((max_n + 31) / 32 + 7) & ~7ull;
+  const uint32_t qcap = (uint32_t)std::min<uint64_t>(max_n, 1u << 14);
+  if (!c->m_scratch.p || c->m_bm_words < bm_words || c->m_qcap < qcap) {
+    const uint64_t per = bm_words * 4 + (uint64_t)qcap * 4;
+    const size_t avail = c->budget > c->used ? c->budget - c->used : 0;
+    uint64_t w = std::min<uint64_t>((uint64_t)c->num_sms * 32,
+                                    std::max<uint64_t>((avail / 4) / per, 8));
+    w = std::max<uint64_t>(8, w & ~7ull);
+    TRY(dalloc(c, c->m_scratch, per * w));
+    CK(c, cudaMemsetAsync(c->m_scratch.p, 0, per * w, c->stream));
+    c->m_bm_words = bm_words;
+    c->m_qcap = qcap;
+    c->m_warps = (uint32_t)w;
+  }
+  // instance table | prefix | launch counters, one upload
+  const size_t n_act = act.size();
+  const size_t desc_bytes = sizeof(InstanceDesc) * n_act;
+  const size_t pre_off = (desc_bytes + 15) & ~(size_t)15;
+  const size_t ctr_off = (pre_off + sizeof(uint32_t) * (n_act + 1) + 15) & ~(size_t)15;
+  const size_t table_bytes = ctr_off + 16;
+  std::vector<uint8_t> table(table_bytes, 0);
+  InstanceDesc *desc = reinterpret_cast<InstanceDesc *>(table.data());
+  uint32_t *prefix = reinterpret_cast<uint32_t *>(table.data() + pre_off);
+  prefix[0] = 0;
+  for (size_t a = 0; a < n_act; ++a) {
+    rip_pool *p = pools[act[a]];
+    InstanceDesc &D = desc[a];
+    D.G = p->g->view();
+    D.P = p->view();
+    D.key = make_key(seeds[act[a]]);
+    D.first = firsts[a];
+    D.work_cap = p->g->model == RIP_MODEL_IC ? p->cap_plain : 0;
+    D.first_bad = &p->dmeta()->first_bad;
+    D.stats = p->dmeta()->stats;
+    D.model = (uint32_t)p->g->model;
+    prefix[a + 1] = prefix[a] + (uint32_t)counts[act[a]];
+    CK(c, cudaMemsetAsync(&p->dmeta()->first_bad, 0xFF, sizeof(unsigned long long), c->stream));
+  }
+  TRY(dalloc(c, c->m_table, table_bytes));
+  TRY(dalloc(c, c->m_fail, sizeof(uint32_t) * 2 * (size_t)total));
+  CK(c, cudaMemcpyAsync(c->m_table.p, table.data(), table_bytes, cudaMemcpyHostToDevice,
+                        c->stream));
+  uint8_t *dt = ptr<uint8_t>(c->m_table);
+  MultiLaunch L;
+  L.inst = reinterpret_cast<const InstanceDesc *>(dt);
+  L.prefix = reinterpret_cast<const uint32_t *>(dt + pre_off);
+  L.n_inst = (uint32_t)n_act;
+  L.total = (uint32_t)total;
+  L.next = reinterpret_cast<unsigned int *>(dt + ctr_off);
+  L.fail_count = reinterpret_cast<unsigned int *>(dt + ctr_off + 4);
+  L.bitmaps = ptr<uint32_t>(c->m_scratch);
+  L.bm_words = c->m_bm_words;
+  L.queues = ptr<uint32_t>(c->m_scratch) + (size_t)c->m_bm_words * c->m_warps;
+  L.qcap = c->m_qcap;
+  L.fail = ptr<uint32_t>(c->m_fail);
+  L.blocks = (int)std::max<uint64_t>(1, (std::min<uint64_t>(c->m_warps, total) + 7) / 8);
+  CK(c, cudaEventRecord(c->ev0, c->stream));
+  launch_multi_sample(L, c->stream);
+  CK(c, cudaGetLastError());
+  CK(c, cudaEventRecord(c->ev1, c->stream));
+  uint32_t n_fail = 0;
+  CK(c, cudaMemcpyAsync(&n_fail, L.fail_count, sizeof(n_fail), cudaMemcpyDeviceToHost,
+                        c->stream));
+  for (size_t a = 0; a < n_act; ++a)
+    CK(c, cudaMemcpyAsync(hm + a, pools[act[a]]->meta.p, sizeof(PoolMeta),
+                          cudaMemcpyDeviceToHost, c->stream));
+  CK(c, cudaStreamSynchronize(c->stream));
+  float kms = 0.f;
+  cudaEventElapsedTime(&kms, c->ev0, c->ev1);
+  c->multi_kernel_ms += kms;
+  std::vector<uint32_t> fails(2 * (size_t)n_fail);
+  if (n_fail) {
+    CK(c, cudaMemcpyAsync(fails.data(), L.fail, sizeof(uint32_t) * 2 * n_fail,
+                          cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+  }
+  std::vector<std::vector<uint32_t>> retry(n_act), big(n_act);
+  for (uint32_t f = 0; f < n_fail; ++f) {
+    const uint32_t a = fails[2 * f], r = fails[2 * f + 1];
+    if (r & FAIL_BIG) big[a].push_back(r & ~FAIL_BIG);
+    else retry[a].push_back(r);
+  }
+  for (size_t a = 0; a < n_act; ++a) {
+    rip_pool *p = pools[act[a]];
+    const double share = (double)counts[act[a]] / (double)total;
+    p->kernel_ms += kms * share;
+    p->kernel_launches++;
+    // roll the bump pointer back to the end of the last stored set
+    const unsigned long long cur = std::min<unsigned long long>(hm[a].cursor, hm[a].first_bad);
+    if (cur != hm[a].cursor)
+      CK(c, cudaMemcpyAsync(&p->dmeta()->cursor, &cur, sizeof(cur), cudaMemcpyHostToDevice,
+                            c->stream));
+    p->num_elems = cur;
+    if (!retry[a].empty()) {
+      if (hm[a].first_bad != ~0ull) {
+        const double mean =
+            hm[a].stats[2] ? (double)hm[a].stats[3] / (double)hm[a].stats[2] : 16.0;
+        TRY(ensure_elems(p, std::max<uint64_t>(
+                                cur + (uint64_t)(mean * 2.0 * retry[a].size()) + 4096,
+                                p->cap * 2)));
+      }
+      std::sort(retry[a].begin(), retry[a].end());
+      TRY(sample_warp_per_set(p, seeds[act[a]], firsts[a], (uint32_t)counts[act[a]],
+                              &retry[a]));
+    }
+    if (!big[a].empty()) {
+      std::sort(big[a].begin(), big[a].end());
+      TRY(sample_big(p, seeds[act[a]], firsts[a], big[a]));
+    }
+    p->num_sets += counts[act[a]];
+    p->have_last_counts = false;
+  }
+  CK(c, cudaStreamSynchronize(c->stream));
   return RIP_OK;
 }
 

@@ -1,0 +1,313 @@
+// host.h -- host runtime internals shared by the C-ABI translation units:
+// the context (stream, device-memory budget and block cache, pinned
+// buffers), the device graph and the RRR pool objects, error and CUDA-call
+// macros.
+#pragma once
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <queue>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include <sys/types.h>
+
+#include "launch.h"
+#include "ripples_b200.h"
+
+using namespace rip;
+
+using clk = std::chrono::high_resolution_clock;
+inline double ms_since(clk::time_point t0) {
+  return std::chrono::duration<double, std::milli>(clk::now() - t0).count();
+}
+
+// ---------------------------------------------------------------------------
+// context, memory
+// ---------------------------------------------------------------------------
+struct DevMem {
+  void *p = nullptr;
+  size_t bytes = 0;
+};
+
+// The reference's heap holds std::pair<vertex, size_t count> ordered by count
+// alone (CompareHeap, include/ripples/streaming_find_most_influential.h:410-418).
+// The heap algorithms only move elements and compare them with the
+// comparator, so an 8-byte {vertex, u32 count} item with the same comparison
+// yields the same sequence of heaps (counts never exceed the number of sets,
+// < 2^32), at half the memory.
+struct HeapItem {
+  uint32_t first;   // vertex
+  uint32_t second;  // count when pushed
+  bool operator==(const HeapItem &o) const { return first == o.first && second == o.second; }
+};
+struct CompareHeap {
+  bool operator()(const HeapItem &a, const HeapItem &b) const { return a.second < b.second; }
+};
+struct PinnedMem;
+
+struct rip_ctx {
+  std::vector<rip_graph *> graphs;  // owned: freed by rip_ctx_destroy
+  std::vector<rip_pool *> pools;    // owned: freed by rip_ctx_destroy
+  std::vector<rip_server *> servers;  // owned: freed by rip_ctx_destroy
+  // Device blocks released by graphs/pools, kept for reuse (a graph upload
+  // or a new pool then costs no cudaMalloc); counted in `used`.
+  std::vector<DevMem> cache;
+  size_t cached = 0;
+  PinnedMem *h_pairs = nullptr;  // mapped: per-pick decrement reports
+  PinnedMem *h_count = nullptr;  // counts at the start of a selection
+  // multi-instance sampler scratch (per warp: bitmap for the largest graph
+  // of the launch + queue), instance table, failure pairs
+  DevMem m_scratch, m_table, m_fail;
+  uint64_t m_bm_words = 0;
+  uint32_t m_qcap = 0, m_warps = 0;
+  PinnedMem *h_meta = nullptr;  // per-pool meta blocks read back together
+  double multi_kernel_ms = 0.0;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int num_sms = 148;
+  size_t budget = 0;
+  size_t used = 0;
+  std::string err;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+inline int set_err(rip_ctx *c, int code, const char *fmt, ...) {
+  if (c) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    c->err = buf;
+  }
+  return code;
+}
+
+#define CK(c, call)                                                          \
+  do {                                                                       \
+    cudaError_t e_ = (call);                                                 \
+    if (e_ != cudaSuccess)                                                   \
+      return set_err((c), RIP_ERR_CUDA, "%s failed: %s (%s:%d)", #call,      \
+                     cudaGetErrorString(e_), __FILE__, __LINE__);            \
+  } while (0)
+
+#define TRY(expr)              \
+  do {                         \
+    int r_ = (expr);           \
+    if (r_ != RIP_OK) return r_; \
+  } while (0)
+
+inline void cache_release_all(rip_ctx *c) {
+  if (!c->cache.empty()) cudaStreamSynchronize(c->stream);
+  for (DevMem &b : c->cache) {
+    cudaFree(b.p);
+    c->used -= b.bytes;
+  }
+  c->cache.clear();
+  c->cached = 0;
+}
+
+// Returns a block to the context cache (or frees it when the cache is full).
+inline void cache_put(rip_ctx *c, DevMem m) {
+  if (!m.p) return;
+  const size_t limit = c->budget / 4;
+  if (m.bytes > limit) {
+    cudaStreamSynchronize(c->stream);
+    cudaFree(m.p);
+    c->used -= m.bytes;
+    return;
+  }
+  while (c->cached + m.bytes > limit && !c->cache.empty()) {
+    cudaStreamSynchronize(c->stream);
+    cudaFree(c->cache.front().p);
+    c->used -= c->cache.front().bytes;
+    c->cached -= c->cache.front().bytes;
+    c->cache.erase(c->cache.begin());
+  }
+  c->cache.push_back(m);
+  c->cached += m.bytes;
+}
+
+// Takes the smallest cached block of at least `bytes` (and at most twice that).
+inline bool cache_take(rip_ctx *c, size_t bytes, DevMem &out) {
+  size_t best = c->cache.size();
+  for (size_t i = 0; i < c->cache.size(); ++i) {
+    const size_t b = c->cache[i].bytes;
+    if (b >= bytes && b <= 2 * bytes + (1u << 20) &&
+        (best == c->cache.size() || b < c->cache[best].bytes))
+      best = i;
+  }
+  if (best == c->cache.size()) return false;
+  out = c->cache[best];
+  c->cached -= out.bytes;
+  c->cache.erase(c->cache.begin() + best);
+  return true;
+}
+
+inline int dalloc(rip_ctx *c, DevMem &m, size_t bytes) {
+  if (m.p && m.bytes >= bytes) return RIP_OK;
+  bytes = std::max<size_t>((bytes + 255) & ~(size_t)255, 256);
+  DevMem fresh;
+  if (!cache_take(c, bytes, fresh)) {
+    if (c->used + bytes > c->budget) cache_release_all(c);
+    if (c->used + bytes > c->budget)
+      return set_err(c, RIP_ERR_NOMEM,
+                     "device budget exceeded: need %zu more bytes (used %zu of %zu)",
+                     bytes, c->used, c->budget);
+    cudaError_t e = cudaMalloc(&fresh.p, bytes);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      cache_release_all(c);
+      e = cudaMalloc(&fresh.p, bytes);
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        return set_err(c, RIP_ERR_NOMEM, "cudaMalloc(%zu) failed: %s", bytes,
+                       cudaGetErrorString(e));
+      }
+    }
+    fresh.bytes = bytes;
+    c->used += bytes;
+  }
+  cache_put(c, m);
+  m = fresh;
+  return RIP_OK;
+}
+
+// Grows m to `bytes`, preserving the first `keep` bytes.
+inline int dgrow(rip_ctx *c, DevMem &m, size_t bytes, size_t keep) {
+  if (m.p && m.bytes >= bytes) return RIP_OK;
+  DevMem n;
+  TRY(dalloc(c, n, bytes));
+  if (m.p && keep) {
+    CK(c, cudaMemcpyAsync(n.p, m.p, std::min(keep, m.bytes),
+                          cudaMemcpyDeviceToDevice, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+  }
+  cache_put(c, m);
+  m = n;
+  return RIP_OK;
+}
+
+inline void dfree(rip_ctx *c, DevMem &m) {
+  cache_put(c, m);
+  m = DevMem{};
+}
+
+template <typename T>
+inline T *ptr(DevMem &m) {
+  return reinterpret_cast<T *>(m.p);
+}
+
+struct PinnedMem {
+  void *p = nullptr;
+  void *dev = nullptr;  // device alias when mapped
+  size_t bytes = 0;
+  int ensure(rip_ctx *c, size_t b, bool mapped = false) {
+    if (p && bytes >= b) return RIP_OK;
+    if (p) cudaFreeHost(p);
+    p = dev = nullptr;
+    bytes = 0;
+    if (cudaHostAlloc(&p, b, mapped ? cudaHostAllocMapped : cudaHostAllocDefault) !=
+        cudaSuccess) {
+      cudaGetLastError();
+      return set_err(c, RIP_ERR_NOMEM, "cudaHostAlloc(%zu) failed", b);
+    }
+    if (mapped && cudaHostGetDevicePointer(&dev, p, 0) != cudaSuccess) {
+      cudaGetLastError();
+      cudaFreeHost(p);
+      p = nullptr;
+      return set_err(c, RIP_ERR_CUDA, "cudaHostGetDevicePointer failed");
+    }
+    bytes = b;
+    return RIP_OK;
+  }
+  ~PinnedMem() {
+    if (p) cudaFreeHost(p);
+  }
+};
+
+
+struct rip_graph {
+  rip_ctx *ctx;
+  uint32_t n;
+  uint64_t m;
+  int model;
+  DevMem off, edges;
+  DevGraph view() {
+    return DevGraph{n, m, ptr<uint32_t>(off), ptr<uint2>(edges)};
+  }
+};
+
+struct PoolMeta {  // device-side bookkeeping block (one D2H reads it all)
+  unsigned long long cursor;
+  unsigned long long first_bad;
+  unsigned long long stats[8];
+  unsigned int fail_count;
+  unsigned int next;
+  unsigned int dirty_n;
+  unsigned int fused_dirty;
+  unsigned long long best;
+  unsigned long long covered_sets;
+};
+
+struct rip_pool {
+  rip_ctx *ctx;
+  rip_graph *g;
+  DevMem vtx, set_off, set_len, meta;
+  uint64_t cap = 0, set_cap = 0;
+  uint64_t num_sets = 0, num_elems = 0;
+  // sampler scratch (one buffer partitioned into per-warp bitmap + queue)
+  DevMem scratch, ids_a, ids_b;
+  uint64_t bm_words = 0;
+  uint32_t qcap = 0;
+  uint32_t warps = 0;
+  // fused sampler scratch (per slot: colour masks, pending masks, level
+  // flags, frontier log); all-zero between batches
+  DevMem f_vis, f_pend, f_flag, f_log, f_order;
+  uint32_t f_slots = 0, f_cw = 0, f_lcap = 0;
+  // CTA-per-set scratch for sets with very large edge work
+  DevMem b_scratch, b_ids;
+  uint32_t b_slots = 0, b_qcap = 0;
+  uint64_t cap_plain = 1ull << 18;  // in-edges per set before a warp hands it over
+  uint64_t cap_fused = 1ull << 23;  // in-edges per fused batch before handing over
+  uint64_t big_sets = 0;            // sets grown one CTA each (diagnostic)
+  uint32_t colors = 64;      // fused colour width (64/128/256)
+  uint32_t fused_slots = 0;  // 0 = size from the budget
+  uint32_t lcap_pref = 0;    // 0 = default frontier-log capacity
+  // selection state
+  DevMem count, inv_off, inv_cur, inv, covered,
+      scan_sums;
+  // vertex -> sets index over sets [0, sv_sets), shared by the served
+  // queries drawing from this pool (each filters to its own prefix)
+  DevMem sv_count, sv_off, sv_cur, sv_inv, sv_sums;
+  uint64_t sv_sets = 0;
+  std::vector<uint32_t> last_counts;
+  bool have_last_counts = false;
+  std::vector<HeapItem> heap_store;  // heap storage reused across selections
+  void *heap_registered = nullptr;   // heap_store's buffer while page-locked
+  size_t heap_registered_bytes = 0;
+  DevMem d_heap;                     // heap built on the device
+  // selection profile: [0] count+index kernels and counts D2H, [1] heap build,
+  // [2] pick loop, [3] heap pops, [4] picks, [5] count reports, [6] selections,
+  // [7] ms in cover launch + sync, [8] ms applying reports, [9] ms in heap pops
+  double sel_prof[12] = {0};
+  // timing of sampler kernels (CUDA events on the context stream)
+  double kernel_ms = 0.0;
+  uint64_t kernel_launches = 0;
+  double select_kernel_ms = 0.0;
+
+  PoolMeta *dmeta() { return ptr<PoolMeta>(meta); }
+  DevPool view() {
+    return DevPool{ptr<uint32_t>(vtx), &dmeta()->cursor, cap,
+                   ptr<uint64_t>(set_off), ptr<uint32_t>(set_len)};
+  }
+};
+
+// Ends the server queries on graph g and drops the servers' pools on it
+// (called before g is destroyed).
+void server_graph_gone(rip_ctx *c, rip_graph *g);

@@ -92,6 +92,7 @@ __global__ void pack_lt_kernel(const uint64_t *index, const uint32_t *src,
 static std::atomic<uint64_t> g_launches{0};
 uint64_t launch_counter() { return g_launches.load(); }
 void count_launches(uint64_t n) { g_launches.fetch_add(n); }
+void uncount_launches(uint64_t n) { g_launches.fetch_sub(n); }
 
 static uint64_t pad4(uint64_t m) { return (m + 3) & ~uint64_t(3); }
 

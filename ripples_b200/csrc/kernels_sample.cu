@@ -21,6 +21,7 @@
 // because every draw is a pure function of (seed, set id, edge / vertex id).
 #include "device.cuh"
 #include "launch.h"
+#include "ripples_b200.h"
 
 namespace rip {
 
@@ -323,6 +324,71 @@ lt_walk_kernel(DevGraph G, DevPool P, Key key, uint64_t first, uint32_t count,
     atomicAdd(st.v + 4, n_exp);
     atomicAdd(st.v + 5, n_edges);
   }
+}
+
+// Many IMM instances in one persistent launch: warps pull global work indices
+// from one counter; index i belongs to the instance a with
+// prefix[a] <= i < prefix[a+1] and is that instance's set first_a + i -
+// prefix[a], grown with that instance's graph, model and seed into its pool.
+__global__ void __launch_bounds__(256)
+multi_sample_kernel(MultiLaunch L) {
+  const uint32_t lane = lane_id();
+  const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  WarpCtx W{L.bitmaps + w * L.bm_words, L.queues + w * (uint64_t)L.qcap, L.qcap};
+  // counters of the instance the warp is on, flushed when it moves on
+  uint32_t cur = ~0u;
+  unsigned long long n_exp = 0, n_edges = 0, n_sets = 0, n_elems = 0;
+  auto flush = [&]() {
+    const unsigned long long e = warp_sum_u64(n_exp), d = warp_sum_u64(n_edges);
+    if (lane == 0 && cur != ~0u && n_sets) {
+      unsigned long long *st = L.inst[cur].stats;
+      atomicAdd(st + 0, e);
+      atomicAdd(st + 1, d);
+      atomicAdd(st + 2, n_sets);
+      atomicAdd(st + 3, n_elems);
+      atomicAdd(st + 4, e);
+      atomicAdd(st + 5, d);
+    }
+    n_exp = n_edges = n_sets = n_elems = 0;
+  };
+  for (;;) {
+    uint32_t idx = 0;
+    if (lane == 0) idx = atomicAdd(L.next, 1u);
+    idx = __shfl_sync(FULL, idx, 0);
+    if (idx >= L.total) break;
+    uint32_t a = 0, b = L.n_inst;  // prefix[a] <= idx < prefix[b]
+    while (b - a > 1) {
+      const uint32_t mid = (a + b) >> 1;
+      if (L.prefix[mid] <= idx) a = mid;
+      else b = mid;
+    }
+    if (a != cur) {
+      flush();
+      cur = a;
+    }
+    const InstanceDesc &D = L.inst[a];
+    const uint32_t rel = idx - L.prefix[a];
+    const uint64_t s = D.first + rel;
+    const SetOutcome o = D.model == RIP_MODEL_IC ? ic_plain_set(D.G, D.key, s, W, D.work_cap)
+                                                 : lt_walk_set(D.G, D.key, s, W);
+    if (store_set(W, o.qlen, o.overflow, s, D.P, D.first_bad)) {
+      n_sets += 1;
+      n_elems += o.qlen;
+      n_exp += o.exp;
+      n_edges += o.edges;
+    } else if (lane == 0) {
+      const unsigned int f = atomicAdd(L.fail_count, 1u);
+      L.fail[2 * f] = a;
+      L.fail[2 * f + 1] = o.big ? (rel | FAIL_BIG) : rel;
+    }
+    __syncwarp();
+  }
+  flush();
+}
+
+void launch_multi_sample(const MultiLaunch &L, cudaStream_t stream) {
+  count_launches(1);
+  multi_sample_kernel<<<L.blocks, 256, 0, stream>>>(L);
 }
 
 void launch_ic_plain(const SampleLaunch &L, cudaStream_t stream) {

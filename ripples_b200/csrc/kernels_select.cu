@@ -162,6 +162,132 @@ __global__ void argmax_kernel(const uint32_t *count, uint32_t n,
   if (lane_id() == 0 && key) atomicMax(best, key);
 }
 
+// ---- device-only picks (served queries) -----------------------------------
+// Every kernel reads its buffers from a SelDesc in device memory, so one
+// captured CUDA graph serves every round of a query: the host rewrites the
+// descriptor (S, buffers) and replays the graph.  Picks keep the lowest-id
+// tie-break: key(v) = count[v] << 32 | ~v, the maximum key wins.  The count
+// array is split into chunks of SEL_CHUNK vertices with a cached maximum key
+// each; a cover marks the chunks it decrements dirty and the next pick
+// re-reads only those, then reduces the chunk maxima in the last block.
+constexpr uint32_t SEL_CHUNK = 1024;
+
+__device__ __forceinline__ unsigned long long sel_key(uint32_t c, uint32_t v) {
+  return ((unsigned long long)c << 32) | (unsigned long long)(~v);
+}
+__device__ __forceinline__ unsigned long long umax64(unsigned long long a,
+                                                     unsigned long long b) {
+  return a > b ? a : b;
+}
+
+__global__ void __launch_bounds__(256) sel_init_kernel(const SelDesc *__restrict__ dp) {
+  const SelDesc d = *dp;
+  const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t n4 = (uint64_t)d.nchunks * (SEL_CHUNK / 4);
+  uint4 *c4 = reinterpret_cast<uint4 *>(d.count);
+  for (uint64_t i = tid; i < n4; i += stride) c4[i] = make_uint4(0, 0, 0, 0);
+  const uint64_t s16 = (d.S + 15) / 16;
+  uint4 *cv = reinterpret_cast<uint4 *>(d.covered);
+  for (uint64_t i = tid; i < s16; i += stride) cv[i] = make_uint4(0, 0, 0, 0);
+  for (uint64_t i = tid; i < d.nchunks; i += stride) d.dirty[i] = 1;
+  for (uint64_t i = tid; i < d.k; i += stride) d.best[i] = 0ull;
+  if (tid == 0) *d.done_blocks = 0;
+}
+
+__global__ void __launch_bounds__(256) sel_count_kernel(const SelDesc *__restrict__ dp) {
+  const SelDesc d = *dp;
+  const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t wb = gw * 32; wb < d.S; wb += nw * 32) {
+    for_each_element(
+        d.P, wb, d.S, [](uint64_t i) { return i; },
+        [&](uint64_t, uint32_t v, bool valid) {
+          const uint32_t peers = __match_any_sync(FULL, v);
+          if (valid && (__ffs(peers) - 1) == (int)lane_id())
+            atomicAdd(d.count + v, (uint32_t)__popc(peers));
+        });
+  }
+}
+
+// Pick i: refresh the dirty chunk maxima (one warp per chunk), then the last
+// block to finish reduces all chunk maxima into best[i].
+__global__ void __launch_bounds__(256) sel_pick_kernel(const SelDesc *__restrict__ dp,
+                                                       uint32_t i) {
+  __shared__ unsigned long long s_red[8];
+  __shared__ bool s_last;
+  const SelDesc d = *dp;
+  if (i > 0 && (d.best[i - 1] >> 32) == 0) return;  // everything covered
+  const uint32_t lane = lane_id(), wid = threadIdx.x >> 5;
+  const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t c = gw; c < d.nchunks; c += nw) {
+    if (!d.dirty[c]) continue;  // warp-uniform
+    const uint4 *src = reinterpret_cast<const uint4 *>(d.count + c * SEL_CHUNK);
+    unsigned long long key = 0;
+#pragma unroll
+    for (uint32_t j = 0; j < SEL_CHUNK / 128; ++j) {
+      const uint32_t q = j * 32 + lane;
+      const uint4 x = __ldcg(src + q);
+      const uint32_t v = (uint32_t)(c * SEL_CHUNK) + 4 * q;
+      key = umax64(key, umax64(umax64(sel_key(x.x, v), sel_key(x.y, v + 1)),
+                               umax64(sel_key(x.z, v + 2), sel_key(x.w, v + 3))));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) key = umax64(key, __shfl_xor_sync(FULL, key, o));
+    if (lane == 0) {
+      d.cmax[c] = key;
+      d.dirty[c] = 0;
+    }
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = atomicAdd(d.done_blocks, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  unsigned long long key = 0;
+  for (uint64_t c = threadIdx.x; c < d.nchunks; c += blockDim.x)
+    key = umax64(key, __ldcg(d.cmax + c));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) key = umax64(key, __shfl_xor_sync(FULL, key, o));
+  if (lane == 0) s_red[wid] = key;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long b = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) b = umax64(b, s_red[w]);
+    d.best[i] = b;
+    *d.done_blocks = 0;
+  }
+}
+
+// After pick i: one warp per set of the seed's inverted list that lies in
+// [0, S) and is still uncovered; members are decremented and their chunks
+// marked dirty.
+__global__ void __launch_bounds__(256) sel_cover_kernel(const SelDesc *__restrict__ dp,
+                                                        uint32_t i) {
+  const SelDesc d = *dp;
+  const unsigned long long b = d.best[i];
+  if ((b >> 32) == 0) return;
+  const uint32_t v = ~(uint32_t)(b & 0xFFFFFFFFull);
+  const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const uint32_t lane = lane_id();
+  const uint64_t lo = d.inv_off[v], hi = d.inv_off[v + 1];
+  for (uint64_t j = lo + gw; j < hi; j += nw) {
+    const uint32_t s = d.inv[j];
+    if (s >= d.S || d.covered[s]) continue;  // warp-uniform
+    const uint32_t len = d.P.set_len[s];
+    const uint64_t off = d.P.set_off[s];
+    if (lane == 0) d.covered[s] = 1;  // s holds v once: no other warp has s
+    for (uint32_t e = lane; e < len; e += 32) {
+      const uint32_t u = d.P.vtx[off + e];
+      atomicSub(d.count + u, 1u);
+      d.dirty[u / SEL_CHUNK] = 1;
+    }
+  }
+}
+
 // ---- exclusive scan of u32 counts into u64 offsets (n+1 outputs) ----------
 constexpr int SCAN_THREADS = 1024;
 constexpr int SCAN_ITEMS = 4;
@@ -343,6 +469,24 @@ void launch_cover(const CoverLaunch &C, cudaStream_t stream) {
   count_launches(1);
   cover_kernel<<<C.blocks, 256, 0, stream>>>(C);
 }
+
+void launch_sel_init(const SelDesc *d, int blocks, cudaStream_t stream) {
+  count_launches(1);
+  sel_init_kernel<<<blocks, 256, 0, stream>>>(d);
+}
+void launch_sel_count(const SelDesc *d, int blocks, cudaStream_t stream) {
+  count_launches(1);
+  sel_count_kernel<<<blocks, 256, 0, stream>>>(d);
+}
+void launch_sel_pick(const SelDesc *d, uint32_t i, int blocks, cudaStream_t stream) {
+  count_launches(1);
+  sel_pick_kernel<<<blocks, 256, 0, stream>>>(d, i);
+}
+void launch_sel_cover(const SelDesc *d, uint32_t i, int blocks, cudaStream_t stream) {
+  count_launches(1);
+  sel_cover_kernel<<<blocks, 256, 0, stream>>>(d, i);
+}
+uint32_t sel_chunk_vertices() { return SEL_CHUNK; }
 
 void launch_argmax(const uint32_t *count, uint32_t n, unsigned long long *best,
                    int blocks, cudaStream_t stream) {

@@ -10,6 +10,7 @@ namespace rip {
 // Process-wide count of kernel launches issued by this library.
 uint64_t launch_counter();
 void count_launches(uint64_t n);
+void uncount_launches(uint64_t n);  // launches recorded into a CUDA graph, not run
 
 // Failure ids carry this bit when a set (or fused batch) was abandoned for
 // exceeding its edge-work cap rather than for lack of room.
@@ -34,6 +35,32 @@ struct SampleLaunch {
 };
 
 void launch_ic_plain(const SampleLaunch &L, cudaStream_t stream);
+
+// One IMM instance of a multi-instance launch.
+struct InstanceDesc {
+  DevGraph G;
+  DevPool P;
+  Key key;
+  uint64_t first;                 // set id of the instance's first set in this launch
+  uint64_t work_cap;              // IC edge-work cap per set (0 = none)
+  unsigned long long *first_bad;  // the instance pool's failure bookkeeping
+  unsigned long long *stats;      // the instance pool's counters [8]
+  uint32_t model;
+};
+struct MultiLaunch {
+  const InstanceDesc *inst = nullptr;
+  const uint32_t *prefix = nullptr;  // n_inst + 1 exclusive prefix of the set counts
+  uint32_t n_inst = 0, total = 0;
+  unsigned int *next = nullptr;
+  uint32_t *bitmaps = nullptr;       // per warp, bm_words (sized for the largest graph)
+  uint64_t bm_words = 0;
+  uint32_t *queues = nullptr;
+  uint32_t qcap = 0;
+  uint32_t *fail = nullptr;          // pairs (instance, rel | FAIL_BIG)
+  unsigned int *fail_count = nullptr;
+  int blocks = 0;
+};
+void launch_multi_sample(const MultiLaunch &L, cudaStream_t stream);
 void launch_lt_walk(const SampleLaunch &L, cudaStream_t stream);
 
 // Fused multi-colour IC BFS: one CTA (slot) per batch of `colors` sets.
@@ -134,6 +161,27 @@ void launch_cover(const CoverLaunch &C, cudaStream_t stream);
 void launch_make_heap(const uint32_t *count, uint32_t n, uint2 *heap, cudaStream_t stream);
 void launch_argmax(const uint32_t *count, uint32_t n, unsigned long long *best,
                    int blocks, cudaStream_t stream);
+
+// Device-only lowest-id picks of one served query (lives in device memory).
+struct SelDesc {
+  DevPool P;                       // the pool the query draws from
+  const uint64_t *inv_off;         // vertex -> sets index over the pool's sets
+  const uint32_t *inv;
+  uint64_t S;                      // select over sets [0, S)
+  uint32_t n, nchunks;             // vertices; chunks of sel_chunk_vertices()
+  uint32_t k;                      // picks
+  uint32_t *count;                 // nchunks * chunk entries (tail stays 0)
+  unsigned long long *cmax;        // per chunk: max key
+  uint8_t *dirty;                  // per chunk
+  uint8_t *covered;                // >= S rounded up to 16 bytes
+  unsigned long long *best;        // k keys: count << 32 | ~vertex
+  unsigned int *done_blocks;       // last-block counter of sel_pick
+};
+void launch_sel_init(const SelDesc *d, int blocks, cudaStream_t stream);
+void launch_sel_count(const SelDesc *d, int blocks, cudaStream_t stream);
+void launch_sel_pick(const SelDesc *d, uint32_t i, int blocks, cudaStream_t stream);
+void launch_sel_cover(const SelDesc *d, uint32_t i, int blocks, cudaStream_t stream);
+uint32_t sel_chunk_vertices();
 
 // Copies sets [first, first+count) into out[csr[i] ..] in set-id order.
 void launch_gather_sets(const DevPool &P, uint64_t first, uint64_t count,

@@ -344,3 +344,114 @@ class Pool:
                                    _ptr(seeds), ctypes.byref(ns), ctypes.byref(rec)),
                   "rip_imm_pool")
         return seeds[: ns.value].copy(), rec
+
+
+def sample_multi(ctx: Context, pools, seeds, counts) -> None:
+    """Extends every pool by counts[i] sets of seeds[i] in one launch
+    (``rip_sample_multi``); the sets equal what ``Pool.sample`` would add."""
+    n = len(pools)
+    hp = (ctypes.c_void_p * n)(*[p.h.value if hasattr(p.h, "value") else p.h for p in pools])
+    sd = np.ascontiguousarray(seeds, dtype=np.uint64)
+    ct = np.ascontiguousarray(counts, dtype=np.uint64)
+    check(lib.rip_sample_multi(ctx.h, hp, _ptr(sd), _ptr(ct), n), "rip_sample_multi", ctx.h)
+
+
+class Query:
+    """One IMM query (``rip_imm_query``) with its seed buffer."""
+
+    def __init__(self, graph: DeviceGraph, k: int, epsilon: float, l: float = 1.0,
+                 seed: int = 0, tiebreak: int = _lib.TIE_LOWEST_ID):
+        self.graph = graph
+        self.buf = np.zeros(max(k, 1), dtype=np.uint32)
+        self.q = _lib.ImmQuery()
+        self.q.graph = graph.h.value if hasattr(graph.h, "value") else graph.h
+        self.q.k, self.q.epsilon, self.q.l = k, epsilon, l
+        self.q.seed, self.q.tiebreak = seed, tiebreak
+        self.q.seeds = self.buf.ctypes.data
+        self.submitted_at = None
+
+    @property
+    def done(self) -> bool:
+        return bool(self.q.done)
+
+    @property
+    def status(self) -> int:
+        return self.q.status
+
+    @property
+    def seeds(self) -> np.ndarray:
+        return self.buf[: self.q.num_seeds].copy()
+
+    @property
+    def record(self):
+        return self.q.record
+
+    @property
+    def latency_ms(self) -> float:
+        return self.q.latency_ms
+
+
+def imm_batch(ctx: Context, queries) -> None:
+    """Runs the queries to completion as one continuous batch (``rip_imm_batch``)."""
+    n = len(queries)
+    arr = (_lib.ImmQuery * n)()
+    for i, q in enumerate(queries):
+        arr[i] = q.q
+    check(lib.rip_imm_batch(ctx.h, arr, n), "rip_imm_batch", ctx.h)
+    for i, q in enumerate(queries):
+        q.q = arr[i]
+
+
+class Server:
+    """Request loop over resident pools (``rip_server``): ``submit`` queues a
+    query, ``tick`` admits what fits and advances every admitted query by one
+    round."""
+
+    def __init__(self, ctx: Context, footprint_budget: int = 0, max_active: int = 16):
+        h = ctypes.c_void_p()
+        check(lib.rip_server_create(ctx.h, footprint_budget, max_active, ctypes.byref(h)),
+              "rip_server_create", ctx.h)
+        self.ctx, self.h = ctx, h
+        self._live = []
+        ctx._children.add(self)
+
+    def _invalidate(self) -> None:
+        self.h = None  # freed with its context
+
+    def submit(self, q: Query) -> Query:
+        check(lib.rip_server_submit(self.h, ctypes.byref(q.q)), "rip_server_submit", self.ctx.h)
+        self._live.append(q)
+        return q
+
+    def tick(self) -> int:
+        done = ctypes.c_uint32()
+        check(lib.rip_server_tick(self.h, ctypes.byref(done)), "rip_server_tick", self.ctx.h)
+        self._live = [q for q in self._live if not q.q.done]
+        return done.value
+
+    def pending(self) -> Tuple[int, int]:
+        a, qd = ctypes.c_uint32(), ctypes.c_uint32()
+        check(lib.rip_server_pending(self.h, ctypes.byref(a), ctypes.byref(qd)),
+              "rip_server_pending", self.ctx.h)
+        return a.value, qd.value
+
+    def stats(self) -> dict:
+        out = np.zeros(6, dtype=np.uint64)
+        check(lib.rip_server_stats(self.h, _ptr(out)), "rip_server_stats", self.ctx.h)
+        keys = ("ticks", "completed", "graph_launches", "pools", "admitted_bytes", "tick_us")
+        return {k: int(v) for k, v in zip(keys, out)}
+
+    def drain(self) -> None:
+        while any(self.pending()):
+            self.tick()
+
+    def close(self) -> None:
+        if self.h and self.ctx.h:
+            lib.rip_server_destroy(self.h)
+        self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
