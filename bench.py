@@ -52,6 +52,11 @@ WORKLOADS = {
     # p ~ U(0,0.1) and LT normalised weights, Poisson arrivals at 200 req/s
     # (seed 3), k log-uniform in [5,500], eps in {0.5,0.3,0.13}, IC/LT 50/50
     "s1": dict(name="serve_rmat18-24_poisson200", kind="serve"),
+    # R-MAT 2^24, 32*2^24 draws, weighted cascade p = 1/indeg, k=100,
+    # eps=0.13: full IMM with the autotuned sampler, plus each sampler
+    # (one set per warp, fused 64/128/256 colours) on the same fixed set range
+    "p3": dict(name="imm_ic_rmat24_deg32_wc_k100_eps0.13", kind="p3", scale=24,
+               draws=32 << 24, model="IC", k=100, eps=0.13),
 }
 METRIC = "RRR sets/s (full IMM)"
 
@@ -263,6 +268,8 @@ def main():
         return run_batch(args, w, world, rank, local)
     if w.get("kind") == "serve":
         return run_serve(args, w, world, rank, local)
+    if w.get("kind") == "p3":
+        return run_p3(args, w, world, rank, local)
     if args.impl == "reference":
         rc = reference_arm(args, w, world, rank)
         if world > 1:
@@ -328,6 +335,23 @@ def main():
     t_max = allreduce_max(elapsed_ms, world)
     sets_all = allreduce_sum(total_sets, world)
     value = sets_all / (t_max / 1e3)
+
+    # ---- the same IMM runs with the reference GPU path's tie-break ---------
+    # (lowest vertex id among equal counts, thrust::max_element): every pick
+    # stays on the device, one read-back per selection
+    torch.cuda.synchronize()
+    ev2, ev3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev2.record(stream)
+    low_sets = 0
+    for step in range(args.steps):
+        pool.clear()
+        _, rec = pool.imm(w["k"], w["eps"], 1.0, seed=seed_base + step,
+                          tiebreak=rb.TIE_LOWEST_ID)
+        low_sets += rec.total_sets
+    ev3.record(stream)
+    torch.cuda.synchronize()
+    low_ms = allreduce_max(ev2.elapsed_time(ev3), world)
+    low_value = allreduce_sum(low_sets, world) / (low_ms / 1e3)
 
     # ---- e2e through the public API: host graph -> device -> seeds ---------
     pin_idx = torch.from_numpy(g.index).pin_memory()
@@ -410,6 +434,11 @@ def main():
                                        "select": sel_ms / args.steps},
             "select_profile_per_step": {kk: vv / args.steps for kk, vv in sel_prof.items()},
             "sets_per_step": total_sets / args.steps,
+            "tiebreak": "reference CPU heap (CompareHeap lazy max-heap)",
+            "lowest_id_tiebreak": {"value": low_value, "unit": "sets/s",
+                                   "ms_per_step": low_ms / args.steps,
+                                   "note": "same IMM runs, reference GPU tie-break "
+                                           "(lowest id), picks on the device"},
         }
         print(json.dumps(line))
     pool.close()
@@ -452,10 +481,14 @@ def run_batch(args, w, world, rank, local):
             dg = rb.DeviceGraph.rmat_on_device(ctx, scale, deg << scale, model, wk, seed=i,
                                                weight_seed=100 + i, lo=0.0, hi=0.05)
         else:
-            hg = rb.HostGraph.erdos_renyi(1 << scale, deg << scale, seed=i)
-            hg = hg.with_weights(wk, seed=100 + i, lo=0.0, hi=0.05)
-            dg = rb.DeviceGraph(ctx, hg, model)
-        graphs.append(dict(dg=dg, scale=scale, deg=deg, kind=kind, model=model))
+            dg = rb.DeviceGraph.erdos_renyi_on_device(ctx, 1 << scale, deg << scale, model, wk,
+                                                      seed=i, weight_seed=100 + i, lo=0.0,
+                                                      hi=0.05)
+        graphs.append(dict(dg=dg, scale=scale, deg=deg, kind=kind, model=model, m=dg.m))
+    t_tune = time.perf_counter()
+    for gd in graphs:
+        gd["tuned"] = gd["dg"].autotune(seed=1, pilot=1024)["name"]
+    t_tune = time.perf_counter() - t_tune
     inst = []
     for j in range(64):
         gi = int(rng.integers(0, 16))
@@ -469,12 +502,19 @@ def run_batch(args, w, world, rank, local):
         return qs
 
     def plain(tag, limit_s=None):
+        """One instance at a time: a fresh pool, one set per warp, heavy IC
+        sets one CTA each, no multi-instance launch.  An instance whose pool
+        does not fit the device fails here as it does in the batch."""
         out, t0 = [], time.perf_counter()
         for x in inst:
             p = rb.Pool(graphs[x["g"]]["dg"])
-            seeds, rec = p.imm(x["k"], x["eps"], seed=x["seed"] + tag,
-                               tiebreak=rb.TIE_LOWEST_ID, sampler=rb.SAMPLER_PLAIN)
-            out.append((seeds, rec.total_sets))
+            p.heavy_batch(0)
+            try:
+                seeds, rec = p.imm(x["k"], x["eps"], seed=x["seed"] + tag,
+                                   tiebreak=rb.TIE_LOWEST_ID, sampler=rb.SAMPLER_PLAIN)
+                out.append((seeds, rec.total_sets))
+            except rb.RipError:
+                out.append((None, 0))
             p.close()
             if limit_s and time.perf_counter() - t0 > limit_s:
                 break
@@ -489,9 +529,11 @@ def run_batch(args, w, world, rank, local):
     t0 = time.perf_counter()
     sets = 0
     last = None
+    failed = 0
     for s in range(args.steps):
         last = batched(0 if s == 0 else 7 * s)
-        sets += sum(q.record.total_sets for q in last)
+        sets += sum(q.record.total_sets for q in last if q.status == 0)
+        failed += sum(1 for q in last if q.status != 0)
     torch.cuda.synchronize()
     t_b = time.perf_counter() - t0
     clk = clocks.stop()
@@ -504,7 +546,9 @@ def run_batch(args, w, world, rank, local):
     torch.cuda.synchronize()
     t_p = time.perf_counter() - t0
     first = batched(0)
-    same = all(np.array_equal(a[0], q.seeds) for a, q in zip(pl, first))
+    same = all(np.array_equal(a[0], q.seeds) for a, q in zip(pl, first)
+               if a[0] is not None and q.status == 0)
+    p_failed = sum(1 for a in pl if a[0] is None)
     p_sets = sum(x[1] for x in pl)
     line = {"metric": "RRR sets/s (64 batched IMM instances)", "value": sets / t_b,
             "unit": "sets/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
@@ -514,9 +558,11 @@ def run_batch(args, w, world, rank, local):
             "config": {"workload": w["name"], "instances": 64,
                        "graphs": [{k: v for k, v in g.items() if k != "dg"} for g in graphs],
                        "tiebreak": "lowest id (device picks)"},
+            "failed_instances_per_step": failed / max(args.steps, 1),
+            "autotune_s": t_tune,
             "plain_one_at_a_time": {"value": p_sets / t_p, "unit": "sets/s",
-                                    "instances": len(pl), "seconds": t_p,
-                                    "imm_per_s": len(pl) / t_p},
+                                    "instances": len(pl), "failed": p_failed,
+                                    "seconds": t_p, "imm_per_s": len(pl) / t_p},
             "batched_imm_per_s": 64 * args.steps / t_b,
             "speedup_vs_plain": (sets / t_b) / (p_sets / t_p),
             "same_seeds_as_plain": bool(same),
@@ -525,6 +571,80 @@ def run_batch(args, w, world, rank, local):
                     "note": "queries and seeds cross the host boundary; graphs resident"},
             "clocks": clk, "gpu_launches": launches}
     print(json.dumps(line))
+    ctx.close()
+    return 0
+
+
+def run_p3(args, w, world, rank, local):
+    import numpy as np
+    import torch
+    import ripples_b200 as rb
+    if _not_on_rank0(world, rank, args, w):
+        return 0
+    torch.cuda.set_device(local)
+    ctx = rb.Context(local)
+    t0 = time.perf_counter()
+    dg = rb.DeviceGraph.rmat_on_device(ctx, w["scale"], w["draws"], "IC", rb.WEIGHTS_WC, seed=0)
+    t_build = time.perf_counter() - t0
+    tune = dg.autotune(seed=1, pilot=8192)
+    peak, peak_kind = measured_peaks()
+    # each sampler on sets [0, count) of one seed (identical sets)
+    count = 1 << 18
+    samplers = {}
+    for name, smp, colors in [("plain", rb.SAMPLER_PLAIN, 64), ("fused64", rb.SAMPLER_FUSED, 64),
+                              ("fused128", rb.SAMPLER_FUSED, 128),
+                              ("fused256", rb.SAMPLER_FUSED, 256)]:
+        p = rb.Pool(dg)
+        p.configure(colors=colors)
+        p.sample(4096, seed=7, sampler=smp)  # warm-up: scratch, pool sizing
+        p.clear()
+        ctx.sync()
+        t1 = time.perf_counter()
+        p.sample(count, seed=7, sampler=smp)
+        ctx.sync()
+        dt = time.perf_counter() - t1
+        st = p.stats()
+        km, kn, _ = p.timing()
+        alg = 8 * int(st[0]) + 8 * int(st[1]) + 4 * int(st[3]) + 12 * int(st[2])
+        samplers[name] = {"sets_per_s": count / dt, "kernel_ms": km, "launches": kn,
+                          "alg_gb_per_s": alg / (km / 1e3) / 1e9 if km else None,
+                          "frac_of_hbm": (alg / (km / 1e3) / 1e9) / peak if km else None,
+                          "fusion_ratio": (int(st[4]) / int(st[0])) if st[0] else None,
+                          "mean_set": int(st[3]) / count}
+        p.close()
+    # full IMM runs, autotuned sampler
+    pool = rb.Pool(dg)
+    for i in range(args.warmup):
+        pool.clear()
+        pool.imm(w["k"], w["eps"], seed=100 + i, tiebreak=rb.TIE_LOWEST_ID)
+    clocks = ClockSampler(local)
+    clocks.start()
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    sets, thetas = 0, []
+    for s in range(args.steps):
+        pool.clear()
+        _, rec = pool.imm(w["k"], w["eps"], seed=s, tiebreak=rb.TIE_LOWEST_ID)
+        sets += rec.total_sets
+        thetas.append(int(rec.theta))
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t1
+    clk = clocks.stop()
+    line = {"metric": "RRR sets/s (full IMM)", "value": sets / dt, "unit": "sets/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True,
+            "scaling": "replicas only", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic R-MAT graph (seed 0), weighted cascade",
+            "config": {"workload": w["name"], "n": dg.n, "m": dg.m, "k": w["k"],
+                       "epsilon": w["eps"], "theta": thetas[0] if thetas else None,
+                       "tiebreak": "lowest id (device picks)"},
+            "autotune": tune, "graph_build_s": t_build,
+            "samplers_on_2^18_sets": samplers,
+            "fused_best_vs_plain": max(samplers[k]["sets_per_s"] for k in samplers
+                                       if k != "plain") / samplers["plain"]["sets_per_s"],
+            "clocks": clk}
+    print(json.dumps(line))
+    pool.close()
     ctx.close()
     return 0
 
@@ -547,6 +667,10 @@ def run_serve(args, w, world, rank, local):
         graphs[(sc, "LT")] = rb.DeviceGraph.rmat_on_device(
             ctx, sc, 16 << sc, "LT", rb.WEIGHTS_LT_NORMALIZED, seed=0, weight_seed=1)
     t_build = time.perf_counter() - t_build
+    t_tune = time.perf_counter()
+    tuned = {f"{sc}{m}": graphs[(sc, m)].autotune(seed=3, pilot=1024)["name"]
+             for sc in scales for m in ("IC",)}
+    t_tune = time.perf_counter() - t_tune
     rng = np.random.default_rng(3)
     N = args.serve_queries
     arrivals = np.cumsum(rng.exponential(1.0 / 200.0, size=N))
@@ -594,20 +718,26 @@ def run_serve(args, w, world, rank, local):
     # queries in arrival order until the time budget runs out
     torch.cuda.synchronize()
     tb = time.perf_counter()
-    base, same = [], True
+    base, same, base_ok = [], True, 0
     for i in range(N):
         s = spec[i]
         p = rb.Pool(graphs[(s["scale"], s["model"])])
+        p.heavy_batch(0)
         t1 = time.perf_counter()
-        seeds, rec = p.imm(s["k"], s["eps"], seed=3, tiebreak=rb.TIE_LOWEST_ID,
-                           sampler=rb.SAMPLER_PLAIN)
+        try:
+            seeds, rec = p.imm(s["k"], s["eps"], seed=3, tiebreak=rb.TIE_LOWEST_ID,
+                               sampler=rb.SAMPLER_PLAIN)
+            base_ok += 1
+            if qs[i].status == 0:
+                same = same and np.array_equal(seeds, qs[i].seeds)
+        except rb.RipError:
+            pass
         base.append(1e3 * (time.perf_counter() - t1))
         p.close()
-        same = same and qs[i].status == 0 and np.array_equal(seeds, qs[i].seeds)
         if time.perf_counter() - tb > args.baseline_seconds:
             break
     t_base = time.perf_counter() - tb
-    base_qps = len(base) / t_base
+    base_qps = base_ok / t_base
     line = {"metric": "IMM queries/s (serving loop)", "value": len(ok) / makespan,
             "unit": "queries/s", "n_gpus": 1, "steps": N, "warmup": 0,
             "ms_per_step": 1e3 * makespan / max(N, 1), "higher_is_better": True,
@@ -620,12 +750,14 @@ def run_serve(args, w, world, rank, local):
             "latency_ms": {"p50": _pct(lat, 50), "p99": _pct(lat, 99), "max": max(lat) if lat else None},
             "completed": len(ok), "failed": N - len(ok), "makespan_s": makespan,
             "plain_one_at_a_time": {"value": base_qps, "unit": "queries/s",
-                                    "queries": len(base), "seconds": t_base,
+                                    "queries": len(base), "completed": base_ok,
+                                    "seconds": t_base,
                                     "service_ms_p50": _pct(base, 50),
                                     "service_ms_p99": _pct(base, 99)},
             "speedup_vs_plain": (len(ok) / makespan) / base_qps if base_qps else None,
             "same_seeds_as_plain": bool(same),
-            "server": st, "graph_build_s": t_build,
+            "server": st, "graph_build_s": t_build, "autotune_s": t_tune,
+            "autotuned": tuned,
             "e2e": {"value": len(ok) / makespan, "unit": "queries/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": int(np.mean([4 * s["k"] for s in spec])),
                     "note": "queries and seeds cross the host boundary; graphs resident"},

@@ -58,7 +58,7 @@ extern "C" {
 #define RIP_TIE_LOWEST_ID 1
 
 /* IC sampler variants (LT always uses the walk kernel). */
-#define RIP_SAMPLER_AUTO 0   /* fused multi-colour BFS                        */
+#define RIP_SAMPLER_AUTO 0   /* the graph's autotuned choice (default: plain) */
 #define RIP_SAMPLER_PLAIN 1  /* one set per warp                              */
 #define RIP_SAMPLER_FUSED 2  /* fused multi-colour reverse BFS                */
 
@@ -113,6 +113,10 @@ int rip_graph_export(rip_graph *g, uint64_t *index, uint32_t *src);
 int rip_rmat_keys_device(rip_ctx *ctx, uint32_t scale, uint64_t first,
                          uint64_t count, double a, double b, double c,
                          uint64_t seed, uint64_t *d_keys);
+/* The same for Erdos-Renyi draws (uniform source and destination), the draws
+ * of rip_er_csr. */
+int rip_er_keys_device(rip_ctx *ctx, uint32_t n, uint64_t first, uint64_t count,
+                       uint64_t seed, uint64_t *d_keys);
 /* Builds a packed graph on the device from m sorted, unique (dst << 32 | src)
  * keys in device memory (no self-loops), with one of the RIP_WEIGHTS_* models
  * computed on the device exactly as rip_make_weights computes them. */
@@ -175,6 +179,38 @@ int rip_pool_configure(rip_pool *p, uint32_t colors, uint32_t slots,
  * 0 disables the hand-over.  Defaults 2^18 and 2^23.  Results do not depend on
  * these values. */
 int rip_pool_work_caps(rip_pool *p, uint64_t plain_cap, uint64_t fused_cap);
+
+/* Per-graph sampler autotuner.  Times `pilot` sets (0 = 2048) of `seed` on a
+ * scratch pool under each of RIP_TUNE_CANDIDATES IC configurations:
+ *   0 plain (one set per warp), heavy sets past 2^18 in-edges -> grid-wide BFS
+ *   1 plain, heavy past 2^14 in-edges -> grid-wide BFS
+ *   2 plain, heavy past 2^18 -> one CTA per set
+ *   3/4/5 fused 64/128/256 colours, batches past 2^23 -> heavy path
+ * writes the wall times to ms[] (may be null) and the fastest to *choice, and
+ * keeps it for the graph: pools created afterwards start from it and
+ * RIP_SAMPLER_AUTO runs it.  Untuned graphs run configuration 0 for AUTO.  LT
+ * graphs have one sampler (choice 0).  Sets never depend on the choice.  No
+ * reference counterpart (the reference fixes its GPU colour width). */
+#define RIP_TUNE_CANDIDATES 6
+int rip_graph_autotune(rip_graph *g, uint64_t seed, uint32_t pilot, double *ms, int *choice);
+
+/* IC sets whose edge work passes the caps above are grown either one
+ * 1024-thread CTA per set or, when at least `min_sets` of them are pending,
+ * 256 at a time by a multi-colour reverse BFS spread over the whole GPU (the
+ * regime of supercritical graphs, where many sets hold a large share of the
+ * graph and overlap).  Default 32; 0 = always one CTA per set.  Results do not
+ * depend on it.  No reference counterpart (the reference's GPU BFS,
+ * include/ripples/gpu/bfs.h:1338-1680, has one colour-batched path). */
+int rip_pool_heavy_batch(rip_pool *p, uint32_t min_sets);
+
+/* Reference-heap selection (RIP_TIE_REF_HEAP): after each pick the host
+ * fetches the current counts of the heap items keyed at least a threshold,
+ * first `percent` % of the previous gain (0 = adaptive, from the recent gain
+ * ratio), then -- if no fetched item still counts that much -- the largest
+ * fetched count, which covers every item the lazy pops can examine.  The seeds
+ * never depend on it.  No reference counterpart: the reference keeps every
+ * count on the host (streaming_find_most_influential.h:560-571). */
+int rip_pool_select_guess(rip_pool *p, uint32_t percent);
 
 /* ---- seed selection ------------------------------------------------------- */
 /* Greedy max coverage over sets [0, num_sets) of the pool.  Writes up to k

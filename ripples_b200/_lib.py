@@ -98,6 +98,7 @@ SIGNATURES = {
     "rip_graph_thresholds": (I32, [P, P]),
     "rip_graph_export": (I32, [P, P, P]),
     "rip_rmat_keys_device": (I32, [P, U32, U64, U64, DBL, DBL, DBL, U64, P]),
+    "rip_er_keys_device": (I32, [P, U32, U64, U64, U64, P]),
     "rip_graph_from_keys": (I32, [P, P, U64, U32, I32, U64, DBL, DBL, I32, PP]),
     "rip_pool_create": (I32, [P, P, PP]),
     "rip_pool_destroy": (I32, [P]),
@@ -110,6 +111,9 @@ SIGNATURES = {
     "rip_pool_timing": (I32, [P, ctypes.POINTER(DBL), ctypes.POINTER(U64), ctypes.POINTER(DBL)]),
     "rip_pool_configure": (I32, [P, U32, U32, U32]),
     "rip_pool_work_caps": (I32, [P, U64, U64]),
+    "rip_pool_select_guess": (I32, [P, U32]),
+    "rip_pool_heavy_batch": (I32, [P, U32]),
+    "rip_graph_autotune": (I32, [P, U64, U32, P, ctypes.POINTER(I32)]),
     "rip_select": (I32, [P, U64, U32, I32, P, P, ctypes.POINTER(U32), ctypes.POINTER(DBL)]),
     "rip_select_counts": (I32, [P, P]),
     "rip_selftest_heap": (I32, [U64, U32, U64]),

@@ -98,6 +98,8 @@ int rip_ctx_memory(rip_ctx *c, size_t *used, size_t *budget) {
 // ---------------------------------------------------------------------------
 static rip_graph *pool_graph(const rip_pool *p);
 
+static int build_lt_range(rip_ctx *c, rip_graph *g);
+
 extern "C" int rip_graph_upload(rip_ctx *c, const uint64_t *index,
                                 const uint32_t *src, const float *w, uint32_t n,
                                 uint64_t m, int model, rip_graph **out) {
@@ -164,14 +166,27 @@ extern "C" int rip_graph_upload(rip_ctx *c, const uint64_t *index,
   dfree(c, d_index);
   dfree(c, d_src);
   dfree(c, d_w);
+  if (rc == RIP_OK) rc = build_lt_range(c, g);
   if (rc != RIP_OK) {
     dfree(c, g->off);
     dfree(c, g->edges);
+    dfree(c, g->range);
     delete g;
     return rc;
   }
   c->graphs.push_back(g);
   *out = g;
+  return RIP_OK;
+}
+
+// The per-edge source ranges of an LT graph (after packing).
+static int build_lt_range(rip_ctx *c, rip_graph *g) {
+  if (g->model != RIP_MODEL_LT || g->m == 0) return RIP_OK;
+  TRY(dalloc(c, g->range, sizeof(uint2) * (size_t)g->m));
+  launch_lt_range(ptr<uint32_t>(g->off), ptr<uint2>(g->edges), g->m, ptr<uint2>(g->range),
+                  c->stream);
+  CK(c, cudaGetLastError());
+  CK(c, cudaStreamSynchronize(c->stream));
   return RIP_OK;
 }
 
@@ -203,14 +218,27 @@ static int pack_device_csr(rip_ctx *c, const uint64_t *d_index, const uint32_t *
     if (e == cudaSuccess) e = cudaGetLastError();
     if (e != cudaSuccess) rc = set_err(c, RIP_ERR_CUDA, "pack failed: %s", cudaGetErrorString(e));
   }
+  if (!rc) rc = build_lt_range(c, g);
   if (rc) {
     dfree(c, g->off);
     dfree(c, g->edges);
+    dfree(c, g->range);
     delete g;
     return rc;
   }
   c->graphs.push_back(g);
   *out = g;
+  return RIP_OK;
+}
+
+extern "C" int rip_er_keys_device(rip_ctx *c, uint32_t n, uint64_t first, uint64_t count,
+                                  uint64_t seed, uint64_t *d_keys) {
+  if (!c || n < 2 || (count && !d_keys)) return RIP_ERR_INVALID;
+  CK(c, cudaSetDevice(c->device));
+  if (count) launch_er_keys(n, first, count, seed, reinterpret_cast<unsigned long long *>(d_keys),
+                            c->stream);
+  CK(c, cudaGetLastError());
+  CK(c, cudaStreamSynchronize(c->stream));
   return RIP_OK;
 }
 
@@ -289,6 +317,7 @@ extern "C" int rip_graph_destroy(rip_graph *g) {
   erase_ptr(c->graphs, g);
   dfree(g->ctx, g->off);
   dfree(g->ctx, g->edges);
+  dfree(g->ctx, g->range);
   delete g;
   return RIP_OK;
 }
@@ -341,6 +370,13 @@ extern "C" int rip_pool_create(rip_ctx *c, rip_graph *g, rip_pool **out) {
     return rc;
   }
   cudaMemsetAsync(p->meta.p, 0, sizeof(PoolMeta), c->stream);
+  if (g->tuned.set) {
+    p->auto_sampler = g->tuned.sampler;
+    p->colors = g->tuned.colors;
+    p->cap_plain = g->tuned.cap_plain;
+    p->cap_fused = g->tuned.cap_fused;
+    p->giant_min = g->tuned.giant_min;
+  }
   c->pools.push_back(p);
   *out = p;
   return RIP_OK;
@@ -355,6 +391,8 @@ extern "C" int rip_pool_destroy(rip_pool *p) {
                    &p->scratch, &p->ids_a,     &p->ids_b,    &p->f_vis,
                    &p->f_pend,  &p->f_flag,    &p->f_log,    &p->f_order,
                    &p->b_scratch, &p->b_ids,   &p->d_heap,
+                   &p->g_state, &p->g_lists,   &p->g_col,
+                   &p->s_cmax,  &p->s_dirty,   &p->s_best,   &p->s_desc,
                    &p->count,   &p->inv_off,   &p->inv_cur,  &p->inv,
                    &p->covered,
                    &p->scan_sums, &p->sv_count, &p->sv_off, &p->sv_cur,
@@ -579,10 +617,114 @@ static int ensure_big_scratch(rip_pool *p, uint32_t slots, uint32_t qcap) {
   return RIP_OK;
 }
 
+// Grows the sets first+ids[i] 64*cw at a time, each batch by the whole grid
+// (kernels_giant.cu): one host round trip per BFS level for the frontier size.
+static int sample_giant(rip_pool *p, uint64_t seed, uint64_t first,
+                        const std::vector<uint32_t> &ids) {
+  rip_ctx *c = p->ctx;
+  rip_graph *g = p->g;
+  const size_t n = g->n;
+  constexpr uint32_t MAXCOL = 256, CWMAX = 4;
+  // state: vis | pend (n * 4 words each) | pflag (n); zero between batches
+  const size_t st_bytes = n * CWMAX * 8 * 2 + n * 4;
+  if (!p->g_state.p || p->g_state.bytes < st_bytes) {
+    TRY(dalloc(c, p->g_state, st_bytes));
+    CK(c, cudaMemsetAsync(p->g_state.p, 0, st_bytes, c->stream));
+  }
+  // lists: front | next | touched | ng (n u32 each) | masks (n * 4 words) |
+  // goff (n + 1) | scan sums
+  const size_t sums = scan_block_sums_needed((uint32_t)n);
+  const size_t li_bytes = n * 4 * 4 + n * CWMAX * 8 + (n + 1) * 8 + sums * 8;
+  TRY(dalloc(c, p->g_lists, li_bytes));
+  // per colour: set ids (u64) | starts (u64) | sizes | fill (u32) | counters
+  TRY(dalloc(c, p->g_col, MAXCOL * 24 + 256));
+  uint8_t *st = ptr<uint8_t>(p->g_state), *li = ptr<uint8_t>(p->g_lists),
+          *co = ptr<uint8_t>(p->g_col);
+  GiantLaunch L;
+  L.G = g->view();
+  L.P = p->view();
+  L.key = make_key(seed);
+  L.vis = reinterpret_cast<uint64_t *>(st);
+  L.pend = reinterpret_cast<uint64_t *>(st + n * CWMAX * 8);
+  L.pflag = reinterpret_cast<uint32_t *>(st + n * CWMAX * 16);
+  L.front = reinterpret_cast<uint32_t *>(li);
+  L.front_next = reinterpret_cast<uint32_t *>(li + n * 4);
+  L.touched = reinterpret_cast<uint32_t *>(li + n * 8);
+  L.ng = reinterpret_cast<uint32_t *>(li + n * 12);
+  L.masks = reinterpret_cast<uint64_t *>(li + n * 16);
+  L.goff = reinterpret_cast<uint64_t *>(li + n * 16 + n * CWMAX * 8);
+  uint64_t *d_sums = reinterpret_cast<uint64_t *>(li + n * 16 + n * CWMAX * 8 + (n + 1) * 8);
+  L.set_ids = reinterpret_cast<const uint64_t *>(co);
+  L.starts = reinterpret_cast<unsigned long long *>(co + MAXCOL * 8);
+  L.sizes = reinterpret_cast<uint32_t *>(co + MAXCOL * 16);
+  L.fill = reinterpret_cast<uint32_t *>(co + MAXCOL * 20);
+  L.ctr = reinterpret_cast<unsigned int *>(co + MAXCOL * 24);
+  L.stats = p->dmeta()->stats;
+  const int blocks = c->num_sms * 8;
+  std::vector<uint64_t> sid(MAXCOL);
+  std::vector<uint32_t> sizes(MAXCOL);
+  std::vector<unsigned long long> starts(MAXCOL);
+  for (size_t b0 = 0; b0 < ids.size(); b0 += MAXCOL) {
+    const uint32_t ncol = (uint32_t)std::min<size_t>(MAXCOL, ids.size() - b0);
+    const int cw = ncol <= 64 ? 1 : ncol <= 128 ? 2 : 4;
+    L.ncol = ncol;
+    for (uint32_t i = 0; i < ncol; ++i) sid[i] = first + ids[b0 + i];
+    CK(c, cudaEventRecord(c->ev0, c->stream));
+    CK(c, cudaMemcpyAsync(co, sid.data(), 8 * ncol, cudaMemcpyHostToDevice, c->stream));
+    CK(c, cudaMemsetAsync(L.ctr, 0, 16, c->stream));
+    CK(c, cudaMemsetAsync(L.sizes, 0, 4 * MAXCOL, c->stream));
+    launch_giant(0, cw, L, 0, 0, 1, c->stream);
+    unsigned int hc[2] = {0, 0};
+    CK(c, cudaMemcpyAsync(hc, L.ctr, 8, cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    uint32_t nf = hc[0];
+    for (uint32_t level = 1; nf > 0; ++level) {
+      launch_giant(1, cw, L, nf, level, blocks, c->stream);
+      launch_exclusive_scan(L.ng, L.goff, nf, d_sums, c->stream);
+      CK(c, cudaMemsetAsync(L.ctr, 0, 4, c->stream));
+      launch_giant(2, cw, L, nf, level, blocks, c->stream);
+      CK(c, cudaGetLastError());
+      CK(c, cudaMemcpyAsync(hc, L.ctr, 8, cudaMemcpyDeviceToHost, c->stream));
+      CK(c, cudaStreamSynchronize(c->stream));
+      std::swap(L.front, L.front_next);
+      nf = hc[0];
+    }
+    const uint32_t nt = hc[1];
+    launch_giant(3, cw, L, nt, 0, blocks, c->stream);
+    CK(c, cudaMemcpyAsync(sizes.data(), L.sizes, 4 * ncol, cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    uint64_t total = 0;
+    for (uint32_t i = 0; i < ncol; ++i) {
+      starts[i] = p->num_elems + total;
+      total += sizes[i];
+    }
+    TRY(ensure_elems(p, p->num_elems + total));
+    L.P = p->view();
+    CK(c, cudaMemcpyAsync(L.starts, starts.data(), 8 * ncol, cudaMemcpyHostToDevice,
+                          c->stream));
+    launch_giant(5, cw, L, 0, 0, 1, c->stream);
+    launch_giant(4, cw, L, nt, 0, blocks, c->stream);
+    CK(c, cudaGetLastError());
+    const unsigned long long cur = p->num_elems + total;
+    CK(c, cudaMemcpyAsync(&p->dmeta()->cursor, &cur, sizeof(cur), cudaMemcpyHostToDevice,
+                          c->stream));
+    CK(c, cudaEventRecord(c->ev1, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    p->num_elems = cur;
+    float kms = 0.f;
+    cudaEventElapsedTime(&kms, c->ev0, c->ev1);
+    p->kernel_ms += kms;
+    p->kernel_launches++;
+    p->big_sets += ncol;
+  }
+  return RIP_OK;
+}
+
 // Grows the sets first+ids[i], one 1024-thread CTA each.
 static int sample_big(rip_pool *p, uint64_t seed, uint64_t first,
                       const std::vector<uint32_t> &ids_in) {
   if (ids_in.empty()) return RIP_OK;
+  if (p->giant_min && ids_in.size() >= p->giant_min) return sample_giant(p, seed, first, ids_in);
   rip_ctx *c = p->ctx;
   rip_graph *g = p->g;
   const uint64_t bm_words = (((uint64_t)g->n + 31) / 32 + 7) & ~7ull;
@@ -823,6 +965,86 @@ extern "C" int rip_pool_work_caps(rip_pool *p, uint64_t plain_cap, uint64_t fuse
   return RIP_OK;
 }
 
+// Per-graph sampler autotuner: times a pilot of sets under each IC sampler
+// configuration on a scratch pool and keeps the fastest for the graph.
+extern "C" int rip_graph_autotune(rip_graph *g, uint64_t seed, uint32_t pilot, double *ms,
+                                  int *choice) {
+  if (!g) return RIP_ERR_INVALID;
+  rip_ctx *c = g->ctx;
+  struct Cand {
+    int sampler;
+    uint32_t colors;
+    uint64_t cap_plain, cap_fused;
+    uint32_t giant_min;
+  };
+  static const Cand cands[RIP_TUNE_CANDIDATES] = {
+      {RIP_SAMPLER_PLAIN, 64, 1ull << 18, 1ull << 23, 32},
+      {RIP_SAMPLER_PLAIN, 64, 1ull << 14, 1ull << 23, 32},
+      {RIP_SAMPLER_PLAIN, 64, 1ull << 18, 1ull << 23, 0},
+      {RIP_SAMPLER_FUSED, 64, 1ull << 18, 1ull << 23, 32},
+      {RIP_SAMPLER_FUSED, 128, 1ull << 18, 1ull << 23, 32},
+      {RIP_SAMPLER_FUSED, 256, 1ull << 18, 1ull << 23, 32},
+  };
+  if (ms)
+    for (int i = 0; i < RIP_TUNE_CANDIDATES; ++i) ms[i] = -1.0;
+  if (g->model != RIP_MODEL_IC) {  // one LT sampler: nothing to choose
+    g->tuned = rip_graph::Tuned{};
+    g->tuned.set = true;
+    if (choice) *choice = 0;
+    return RIP_OK;
+  }
+  pilot = std::max<uint32_t>(pilot ? pilot : 2048, 64);
+  int best = 0;
+  double best_ms = 0;
+  for (int i = 0; i < RIP_TUNE_CANDIDATES; ++i) {
+    rip_pool *p = nullptr;
+    TRY(rip_pool_create(c, g, &p));
+    p->auto_sampler = cands[i].sampler;
+    p->colors = cands[i].colors;
+    p->cap_plain = cands[i].cap_plain;
+    p->cap_fused = cands[i].cap_fused;
+    p->giant_min = cands[i].giant_min;
+    // a small warm-up sizes the scratch; the timed pilot follows it
+    int rc = rip_sample(p, seed, std::min<uint32_t>(pilot / 8, 256), RIP_SAMPLER_AUTO);
+    if (rc == RIP_OK) rc = rip_sync(c);
+    const auto t0 = clk::now();
+    if (rc == RIP_OK) rc = rip_sample(p, seed, pilot, RIP_SAMPLER_AUTO);
+    if (rc == RIP_OK) rc = rip_sync(c);
+    const double t = ms_since(t0);
+    rip_pool_destroy(p);
+    if (rc != RIP_OK) return rc;
+    if (ms) ms[i] = t;
+    if (i == 0 || t < best_ms) {
+      best = i;
+      best_ms = t;
+    }
+  }
+  g->tuned.set = true;
+  g->tuned.sampler = cands[best].sampler;
+  g->tuned.colors = cands[best].colors;
+  g->tuned.cap_plain = cands[best].cap_plain;
+  g->tuned.cap_fused = cands[best].cap_fused;
+  g->tuned.giant_min = cands[best].giant_min;
+  if (choice) *choice = best;
+  return RIP_OK;
+}
+
+// Number of heavy IC sets from which they are grown by the grid-wide
+// multi-colour BFS instead of one CTA each (0 = never).
+extern "C" int rip_pool_heavy_batch(rip_pool *p, uint32_t min_sets) {
+  if (!p) return RIP_ERR_INVALID;
+  p->giant_min = min_sets;
+  return RIP_OK;
+}
+
+// First-fetch threshold of reference-heap picks as a percentage of the
+// previous gain (0 = adaptive); the seeds do not depend on it.
+extern "C" int rip_pool_select_guess(rip_pool *p, uint32_t percent) {
+  if (!p || percent > 100) return RIP_ERR_INVALID;
+  p->cand_fixed = percent;
+  return RIP_OK;
+}
+
 extern "C" int rip_pool_configure(rip_pool *p, uint32_t colors, uint32_t slots,
                                   uint32_t log_capacity) {
   if (!p) return RIP_ERR_INVALID;
@@ -857,7 +1079,9 @@ extern "C" int rip_sample(rip_pool *p, uint64_t seed, uint64_t count,
   double mean = m.stats[2] ? (double)m.stats[3] / (double)m.stats[2] : 8.0;
   TRY(ensure_elems(p, p->num_elems + (uint64_t)(mean * 1.25 * count) + 1024));
   int rc;
-  if (p->g->model == RIP_MODEL_IC && sampler != RIP_SAMPLER_PLAIN)
+  const bool fused = sampler == RIP_SAMPLER_FUSED ||
+                     (sampler == RIP_SAMPLER_AUTO && p->auto_sampler == RIP_SAMPLER_FUSED);
+  if (p->g->model == RIP_MODEL_IC && fused)
     rc = sample_fused(p, seed, first, (uint32_t)count);
   else
     rc = sample_warp_per_set(p, seed, first, (uint32_t)count, nullptr);
@@ -965,6 +1189,63 @@ using RefQueue = std::priority_queue<HeapItem, std::vector<HeapItem>, CompareHea
 struct AdoptedQueue : RefQueue {
   explicit AdoptedQueue(std::vector<HeapItem> &&heap) { this->c = std::move(heap); }
   std::vector<HeapItem> release() { return std::move(this->c); }
+  const std::vector<HeapItem> &items() const { return this->c; }
+};
+
+// The vertices of every heap item keyed at least T (keys never grow
+// downwards, so subtrees whose root is keyed below T are skipped).  Returns
+// the count, or cap + 1 when more than cap items qualify.
+static uint32_t collect_at_least(const std::vector<HeapItem> &h, uint32_t T, uint32_t cap,
+                                 uint32_t *out, std::vector<uint32_t> &stack) {
+  const size_t len = h.size();
+  uint32_t cnt = 0;
+  stack.clear();
+  if (len && h[0].second >= T) stack.push_back(0);
+  while (!stack.empty()) {
+    const size_t i = stack.back();
+    stack.pop_back();
+    if (cnt == cap) return cap + 1;
+    out[cnt++] = h[i].first;
+    const size_t l = 2 * i + 1;
+    if (l < len && h[l].second >= T) stack.push_back((uint32_t)l);
+    if (l + 1 < len && h[l + 1].second >= T) stack.push_back((uint32_t)(l + 1));
+  }
+  return cnt;
+}
+
+// Open-addressing map vertex -> fetched count for one pick's candidates.
+struct CountMap {
+  std::vector<uint32_t> key, val;  // key = vertex + 1, 0 = empty
+  uint32_t mask = 0;
+  void reset(uint32_t items) {
+    uint32_t cap = 64;
+    while (cap < 2 * items) cap <<= 1;
+    if (key.size() < cap) {
+      key.assign(cap, 0u);
+      val.resize(cap);
+    } else {
+      std::fill(key.begin(), key.begin() + cap, 0u);
+    }
+    mask = cap - 1;
+  }
+  static uint32_t hash(uint32_t v) { return (v * 2654435761u) ^ (v >> 15); }
+  void put(uint32_t v, uint32_t c) {
+    uint32_t i = hash(v) & mask;
+    while (key[i] != 0u && key[i] != v + 1) i = (i + 1) & mask;
+    key[i] = v + 1;
+    val[i] = c;
+  }
+  bool get(uint32_t v, uint32_t &c) const {
+    uint32_t i = hash(v) & mask;
+    while (key[i] != 0u) {
+      if (key[i] == v + 1) {
+        c = val[i];
+        return true;
+      }
+      i = (i + 1) & mask;
+    }
+    return false;
+  }
 };
 
 // Bit-identical to std::make_heap(v.begin(), v.end(), CompareHeap{}), built
@@ -1039,11 +1320,28 @@ extern "C" int rip_selftest_heap(uint64_t n, uint32_t max_count, uint64_t seed) 
   return a == b ? 1 : 0;
 }
 
+// The counts left by the last selection still sit in the count buffer; bring
+// them to the host before anything overwrites that buffer.
+static int settle_last_counts(rip_pool *p) {
+  if (!p->have_last_counts || !p->last_counts_on_device) return RIP_OK;
+  rip_ctx *c = p->ctx;
+  p->last_counts.resize(p->g->n);
+  CK(c, cudaMemcpyAsync(p->last_counts.data(), p->count.p, sizeof(uint32_t) * (size_t)p->g->n,
+                        cudaMemcpyDeviceToHost, c->stream));
+  CK(c, cudaStreamSynchronize(c->stream));
+  p->last_counts_on_device = false;
+  return RIP_OK;
+}
+
 static int count_sets(rip_pool *p, uint64_t S) {
   rip_ctx *c = p->ctx;
   const uint32_t n = p->g->n;
-  TRY(dalloc(c, p->count, sizeof(uint32_t) * (size_t)n));
-  CK(c, cudaMemsetAsync(p->count.p, 0, sizeof(uint32_t) * (size_t)n, c->stream));
+  TRY(settle_last_counts(p));
+  // padded to whole chunks of the device picks (the tail stays zero)
+  const size_t chunk = sel_chunk_vertices();
+  const size_t padded = ((size_t)n + chunk - 1) / chunk * chunk;
+  TRY(dalloc(c, p->count, sizeof(uint32_t) * padded));
+  CK(c, cudaMemsetAsync(p->count.p, 0, sizeof(uint32_t) * padded, c->stream));
   launch_count(p->view(), S, ptr<uint32_t>(p->count), c->num_sms * 8, c->stream);
   CK(c, cudaGetLastError());
   return RIP_OK;
@@ -1065,6 +1363,7 @@ extern "C" int rip_select_counts(rip_pool *p, uint32_t *counts) {
   if (!p || !counts) return RIP_ERR_INVALID;
   if (!p->have_last_counts)
     return set_err(p->ctx, RIP_ERR_STATE, "no selection has run on this pool");
+  TRY(settle_last_counts(p));
   std::memcpy(counts, p->last_counts.data(), sizeof(uint32_t) * p->g->n);
   return RIP_OK;
 }
@@ -1088,6 +1387,7 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
   CK(c, cudaEventRecord(c->ev0, c->stream));
   const auto t_sel0 = clk::now();
   // 1. histogram, 2. vertex -> sets index
+  p->have_last_counts = false;  // superseded by this selection
   TRY(count_sets(p, S));
   TRY(dalloc(c, p->inv_off, sizeof(uint64_t) * ((size_t)n + 1)));
   TRY(dalloc(c, p->inv_cur, sizeof(uint64_t) * ((size_t)n + 1)));
@@ -1126,9 +1426,9 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
   hcount.resize(n);
   if (!c->h_pairs) c->h_pairs = new PinnedMem();
   if (!c->h_count) c->h_count = new PinnedMem();
-  // mapped: the cover kernel writes its decrement reports (vertex ids) here
-  const uint32_t max_reports = std::max<uint32_t>(2 * n, 1u << 21);
-  TRY(c->h_pairs->ensure(c, 16 + sizeof(uint32_t) * (size_t)max_reports, true));
+  // mapped: candidate vertex ids in, their counts out (reference-heap picks)
+  constexpr uint32_t CAND_CAP = 1u << 16;
+  TRY(c->h_pairs->ensure(c, 16 + 2 * sizeof(uint32_t) * (size_t)CAND_CAP, true));
   TRY(c->h_count->ensure(c, sizeof(uint32_t) * (size_t)n));
   PinnedMem &h_pairs = *c->h_pairs, &h_count = *c->h_count;
 
@@ -1136,58 +1436,23 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
   std::vector<uint32_t> out_seeds;
   std::vector<uint64_t> out_gains;
 
-  // Initial counts: the heap's keys, and |sets containing v| (the length of
-  // v's inverted list) for sizing each pick's cover grid.
-  CK(c, cudaMemcpyAsync(h_count.p, p->count.p, sizeof(uint32_t) * (size_t)n,
-                        cudaMemcpyDeviceToHost, c->stream));
-  CK(c, cudaStreamSynchronize(c->stream));
-  const uint32_t *init_count = static_cast<const uint32_t *>(h_count.p);
   p->sel_prof[0] += ms_since(t_sel0);
   p->sel_prof[6] += 1;
-  const double mean_len = S ? (double)P / (double)S : 1.0;
   const int max_blocks = c->num_sms * 4;
   unsigned char *hb = static_cast<unsigned char *>(h_pairs.p);
   unsigned char *db = static_cast<unsigned char *>(h_pairs.dev);
-  unsigned int *h_dn = reinterpret_cast<unsigned int *>(hb);  // pinned landing for dirty_n
-  // One pick: mark + decrement in one launch; with_pairs also streams the
-  // decremented vertex ids to mapped host memory.
-  auto cover = [&](uint32_t v, bool with_pairs) -> int {
+  // One pick: mark v's uncovered sets covered and decrement their members, one
+  // warp per set of v's inverted list (`gain` of them are still uncovered).
+  auto cover = [&](uint32_t v, uint64_t gain) -> int {
     C.vertex = v;
-    // one warp per set of v's inverted list, 8 warps per block
-    C.blocks = (int)std::min<uint64_t>(max_blocks * 4, std::max<uint64_t>(1, (init_count[v] + 7) / 8));
-    C.reports = with_pairs ? reinterpret_cast<uint32_t *>(db + 16) : nullptr;
-    C.max_reports = with_pairs ? max_reports : 0;
-    if (with_pairs) CK(c, cudaMemsetAsync(&dm->dirty_n, 0, sizeof(unsigned int), c->stream));
+    C.blocks = (int)std::min<uint64_t>(max_blocks * 4, std::max<uint64_t>(1, (gain + 7) / 8));
     launch_cover(C, c->stream);
     CK(c, cudaGetLastError());
     return RIP_OK;
   };
 
-  // After a pick: one synchronisation, then the host mirror applies one
-  // decrement per report (or takes the whole count array when the reports
-  // overflowed their buffer).
-  auto sync_dirty = [&]() -> int {
-    CK(c, cudaMemcpyAsync(h_dn, &dm->dirty_n, sizeof(unsigned int), cudaMemcpyDeviceToHost,
-                          c->stream));
-    CK(c, cudaStreamSynchronize(c->stream));
-    const auto t_a0 = clk::now();
-    const unsigned int dn = *reinterpret_cast<volatile unsigned int *>(h_dn);
-    if (dn > max_reports) {
-      CK(c, cudaMemcpyAsync(hcount.data(), p->count.p, sizeof(uint32_t) * (size_t)n,
-                            cudaMemcpyDeviceToHost, c->stream));
-      CK(c, cudaStreamSynchronize(c->stream));
-    } else {
-      const uint32_t *hr = reinterpret_cast<const uint32_t *>(hb + 16);
-      for (unsigned int i = 0; i < dn; ++i) hcount[hr[i]] -= 1;
-    }
-    p->sel_prof[5] += dn;
-    p->sel_prof[8] += ms_since(t_a0);
-    return RIP_OK;
-  };
-
   if (tiebreak == RIP_TIE_REF_HEAP) {
     const auto t_h0 = clk::now();
-    std::memcpy(hcount.data(), h_count.p, sizeof(uint32_t) * (size_t)n);
     // InitHeapStorage + std::priority_queue(cmp, std::move(storage)), as the
     // reference builds its heap (streaming_find_most_influential.h:541-544;
     // counting.h:196-206): the same heap, built level-parallel on the device
@@ -1216,56 +1481,149 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
     AdoptedQueue queue(std::move(storage));
     p->sel_prof[1] += ms_since(t_h0);
     const auto t_p0 = clk::now();
+    // The lazy pops of a pick only read the current counts of heap items keyed
+    // at least the pick's gain m (keys are stale upper bounds of the counts and
+    // m is the largest count).  After each cover the host fetches the counts
+    // of the items keyed >= T for a guess T below the previous gain; if one of
+    // them still counts >= T, then m >= T and the fetch covers every item the
+    // pops can reach.  Otherwise their largest count c is a lower bound of m
+    // and a second fetch with T = c is exact.  A pop outside the fetched items
+    // (not expected) falls back to the whole count array.
+    uint32_t *h_ids = reinterpret_cast<uint32_t *>(hb + 16);
+    uint32_t *h_cnt = h_ids + CAND_CAP;
+    const uint32_t *d_ids = reinterpret_cast<const uint32_t *>(db + 16);
+    uint32_t *d_cnt = reinterpret_cast<uint32_t *>(db + 16) + CAND_CAP;
+    CountMap cmap;
+    std::vector<uint32_t> stack;
+    // First pick: every key is still exact, so only the top is examined.
+    bool fresh_all = false, first = true;
+    if (!queue.empty()) {
+      cmap.reset(1);
+      cmap.put(queue.top().first, queue.top().second);
+    }
+    double ratio = 0.9;  // recent gain ratio g_i / g_{i-1}
+    auto fetch_all = [&]() -> int {
+      CK(c, cudaMemcpyAsync(h_count.p, p->count.p, sizeof(uint32_t) * (size_t)n,
+                            cudaMemcpyDeviceToHost, c->stream));
+      CK(c, cudaStreamSynchronize(c->stream));
+      std::memcpy(hcount.data(), h_count.p, sizeof(uint32_t) * (size_t)n);
+      fresh_all = true;
+      p->sel_prof[8] += 1;
+      return RIP_OK;
+    };
     while (out_seeds.size() < k && uncovered != 0) {
+      const auto t_g0 = clk::now();
+      if (!first) {
+        const uint64_t g_prev = out_gains.back();
+        const double guess = p->cand_fixed ? p->cand_fixed / 100.0 : 0.8 * ratio;
+        uint32_t T = (uint32_t)std::max<double>(1.0, std::floor((double)g_prev * guess));
+        for (int round = 0;; ++round) {
+          const uint32_t nc = collect_at_least(queue.items(), T, CAND_CAP, h_ids, stack);
+          if (nc > CAND_CAP) {
+            if (round == 0 && T < g_prev) {  // guess too low: raise it
+              T = (uint32_t)std::min<uint64_t>(g_prev, (uint64_t)T + (g_prev - T + 1) / 2);
+              continue;
+            }
+            TRY(fetch_all());
+            break;
+          }
+          launch_gather_counts(ptr<uint32_t>(p->count), d_ids, nc, d_cnt, c->stream);
+          CK(c, cudaGetLastError());
+          CK(c, cudaStreamSynchronize(c->stream));
+          p->sel_prof[5] += nc;
+          cmap.reset(nc);
+          uint32_t mc = 0;
+          for (uint32_t i = 0; i < nc; ++i) {
+            const uint32_t cv = *reinterpret_cast<volatile uint32_t *>(h_cnt + i);
+            cmap.put(h_ids[i], cv);
+            mc = std::max(mc, cv);
+          }
+          if (mc >= T || nc == queue.size()) break;
+          T = std::max<uint32_t>(mc, 1u);  // mc <= m < T: exact next round
+        }
+      }
+      p->sel_prof[7] += ms_since(t_g0);
       HeapItem element;
       const auto t_q0 = clk::now();
       for (;;) {  // getNextSeed, streaming_find_most_influential.h:560-571
         if (queue.empty())
           return set_err(c, RIP_ERR_STATE, "selection heap exhausted");
         element = queue.top();
+        uint32_t cur = 0;
+        if (fresh_all) {
+          cur = hcount[element.first];
+        } else if (!cmap.get(element.first, cur)) {
+          TRY(fetch_all());
+          cur = hcount[element.first];
+        }
         queue.pop();
         p->sel_prof[3] += 1;
-        if (element.second > hcount[element.first]) {
-          element.second = hcount[element.first];
+        if (element.second > cur) {
+          element.second = cur;
           queue.push(element);
           continue;
         }
         break;
       }
       p->sel_prof[9] += ms_since(t_q0);
+      if (!out_gains.empty() && out_gains.back())
+        ratio = std::min(1.0, (double)element.second / (double)out_gains.back());
       uncovered -= element.second;
       out_seeds.push_back(element.first);
       out_gains.push_back(element.second);
       if (out_seeds.size() == k) break;
-      const auto t_g0 = clk::now();
-      TRY(cover(element.first, true));
-      TRY(sync_dirty());
-      p->sel_prof[7] += ms_since(t_g0);
+      TRY(cover(element.first, element.second));
+      fresh_all = first = false;
     }
     p->sel_prof[2] += ms_since(t_p0);
     p->sel_prof[4] += out_seeds.size();
     p->heap_store = queue.release();
-  } else {
-    while (out_seeds.size() < k && uncovered != 0) {
-      CK(c, cudaMemsetAsync(&dm->best, 0, sizeof(unsigned long long), c->stream));
-      launch_argmax(ptr<uint32_t>(p->count), n, &dm->best, c->num_sms * 4, c->stream);
-      unsigned long long best = 0;
-      CK(c, cudaMemcpyAsync(&best, &dm->best, sizeof(best), cudaMemcpyDeviceToHost,
-                            c->stream));
-      CK(c, cudaStreamSynchronize(c->stream));
-      const uint32_t v = ~(uint32_t)(best & 0xFFFFFFFFull);
-      const uint64_t cnt = best >> 32;
-      uncovered -= cnt;
-      out_seeds.push_back(v);
-      out_gains.push_back(cnt);
-      if (out_seeds.size() == k) break;
-      TRY(cover(v, false));
-      // the lowest-id path keeps no host mirror; dirty bits are reset below
+  } else if (k > 0 && S > 0) {
+    // Lowest-id picks entirely on the device: k pick launches (cached chunk
+    // maxima, lowest id on ties) and k - 1 cover launches, one read-back.
+    const uint32_t chunk = sel_chunk_vertices();
+    const uint32_t nchunks = (uint32_t)(((uint64_t)n + chunk - 1) / chunk);
+    TRY(dalloc(c, p->s_cmax, (size_t)nchunks * 8));
+    TRY(dalloc(c, p->s_dirty, (size_t)nchunks));
+    TRY(dalloc(c, p->s_best, (size_t)k * 8 + 256));
+    TRY(dalloc(c, p->s_desc, sizeof(SelDesc)));
+    TRY(p->h_best.ensure(c, (size_t)k * 8));
+    SelDesc d;
+    d.P = p->view();
+    d.inv_off = ptr<uint64_t>(p->inv_off);
+    d.inv = ptr<uint32_t>(p->inv);
+    d.S = S;
+    d.n = n;
+    d.nchunks = nchunks;
+    d.k = k;
+    d.keep_counts = 1;
+    d.count = ptr<uint32_t>(p->count);
+    d.cmax = ptr<unsigned long long>(p->s_cmax);
+    d.dirty = ptr<uint8_t>(p->s_dirty);
+    d.covered = ptr<uint8_t>(p->covered);
+    d.best = ptr<unsigned long long>(p->s_best);
+    d.done_blocks = reinterpret_cast<unsigned int *>(ptr<uint8_t>(p->s_best) + (size_t)k * 8);
+    CK(c, cudaMemcpyAsync(p->s_desc.p, &d, sizeof(d), cudaMemcpyHostToDevice, c->stream));
+    const SelDesc *dd = ptr<SelDesc>(p->s_desc);
+    const int pick_blocks = (int)std::max<uint32_t>(1, std::min<uint32_t>((nchunks + 7) / 8,
+                                                                          c->num_sms * 4));
+    launch_sel_init(dd, c->num_sms, c->stream);
+    for (uint32_t i = 0; i < k; ++i) {
+      launch_sel_pick(dd, i, pick_blocks, c->stream);
+      if (i + 1 < k) launch_sel_cover(dd, i, max_blocks, c->stream);
     }
-    CK(c, cudaMemcpyAsync(h_count.p, p->count.p, sizeof(uint32_t) * (size_t)n,
-                          cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaGetLastError());
+    CK(c, cudaMemcpyAsync(p->h_best.p, p->s_best.p, (size_t)k * 8, cudaMemcpyDeviceToHost,
+                          c->stream));
     CK(c, cudaStreamSynchronize(c->stream));
-    std::memcpy(hcount.data(), h_count.p, sizeof(uint32_t) * (size_t)n);
+    const unsigned long long *hb8 = static_cast<const unsigned long long *>(p->h_best.p);
+    for (uint32_t i = 0; i < k && uncovered != 0; ++i) {
+      const uint64_t cnt = hb8[i] >> 32;
+      if (cnt == 0) break;
+      uncovered -= cnt;
+      out_seeds.push_back(~(uint32_t)(hb8[i] & 0xFFFFFFFFull));
+      out_gains.push_back(cnt);
+    }
   }
   CK(c, cudaEventRecord(c->ev1, c->stream));
   CK(c, cudaStreamSynchronize(c->stream));
@@ -1273,6 +1631,7 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
   cudaEventElapsedTime(&sms, c->ev0, c->ev1);
   p->select_kernel_ms += sms;
   p->have_last_counts = true;
+  p->last_counts_on_device = true;  // read back on demand (rip_select_counts)
   for (size_t i = 0; i < out_seeds.size(); ++i) {
     seeds[i] = out_seeds[i];
     if (gains) gains[i] = out_gains[i];

@@ -238,8 +238,18 @@ struct rip_graph {
   uint64_t m;
   int model;
   DevMem off, edges;
+  DevMem range;  // LT: per edge, the source's in-edge range
+  // IC sampler configuration picked by rip_graph_autotune (pools created
+  // afterwards start from it; RIP_SAMPLER_AUTO follows `sampler`)
+  struct Tuned {
+    bool set = false;
+    int sampler = RIP_SAMPLER_PLAIN;
+    uint32_t colors = 64, giant_min = 32;
+    uint64_t cap_plain = 1ull << 18, cap_fused = 1ull << 23;
+  } tuned;
   DevGraph view() {
-    return DevGraph{n, m, ptr<uint32_t>(off), ptr<uint2>(edges)};
+    return DevGraph{n, m, ptr<uint32_t>(off), ptr<uint2>(edges),
+                    range.p ? ptr<uint2>(range) : nullptr};
   }
 };
 
@@ -273,6 +283,10 @@ struct rip_pool {
   // CTA-per-set scratch for sets with very large edge work
   DevMem b_scratch, b_ids;
   uint32_t b_slots = 0, b_qcap = 0;
+  // grid-wide multi-colour BFS for the heavy sets (all-zero between batches)
+  DevMem g_state, g_lists, g_col;
+  uint32_t giant_min = 32;  // heavy sets that switch to the grid-wide BFS (0 = never)
+  int auto_sampler = RIP_SAMPLER_PLAIN;  // what RIP_SAMPLER_AUTO runs (IC)
   uint64_t cap_plain = 1ull << 18;  // in-edges per set before a warp hands it over
   uint64_t cap_fused = 1ull << 23;  // in-edges per fused batch before handing over
   uint64_t big_sets = 0;            // sets grown one CTA each (diagnostic)
@@ -287,14 +301,19 @@ struct rip_pool {
   DevMem sv_count, sv_off, sv_cur, sv_inv, sv_sums;
   uint64_t sv_sets = 0;
   std::vector<uint32_t> last_counts;
+  bool last_counts_on_device = false;  // last_counts still in `count` only
   bool have_last_counts = false;
   std::vector<HeapItem> heap_store;  // heap storage reused across selections
+  uint32_t cand_fixed = 0;           // first-fetch threshold, % of the last gain (0 = adaptive)
   void *heap_registered = nullptr;   // heap_store's buffer while page-locked
   size_t heap_registered_bytes = 0;
   DevMem d_heap;                     // heap built on the device
+  DevMem s_cmax, s_dirty, s_best, s_desc;  // device lowest-id picks
+  PinnedMem h_best;
   // selection profile: [0] count+index kernels and counts D2H, [1] heap build,
-  // [2] pick loop, [3] heap pops, [4] picks, [5] count reports, [6] selections,
-  // [7] ms in cover launch + sync, [8] ms applying reports, [9] ms in heap pops
+  // [2] pick loop, [3] heap pops, [4] picks, [5] candidate counts fetched,
+  // [6] selections, [7] ms covering + fetching candidate counts, [8] fetches
+  // of the whole count array from a pop outside the candidates, [9] ms in pops
   double sel_prof[12] = {0};
   // timing of sampler kernels (CUDA events on the context stream)
   double kernel_ms = 0.0;

@@ -14,7 +14,7 @@ namespace rip {
 
 namespace {
 
-constexpr uint32_t DOM_RMAT = 4, DOM_WEIGHT = 6;
+constexpr uint32_t DOM_RMAT = 4, DOM_ER = 5, DOM_WEIGHT = 6;
 
 __global__ void rmat_keys_kernel(uint32_t scale, uint64_t first, uint64_t count,
                                  uint32_t TA, uint32_t TB, uint32_t TC, Key key,
@@ -33,6 +33,20 @@ __global__ void rmat_keys_kernel(uint32_t scale, uint64_t first, uint64_t count,
       s |= rb << (scale - 1 - l);
       d |= cb << (scale - 1 - l);
     }
+    keys[j] = s == d ? ~0ull : (((unsigned long long)d << 32) | s);
+  }
+}
+
+// Erdos-Renyi draw i: src = mulhi(P(i; ER)[0], n), dst = mulhi(P(i; ER)[1], n),
+// as graphgen.cpp draws it.
+__global__ void er_keys_kernel(uint32_t n, uint64_t first, uint64_t count, Key key,
+                               unsigned long long *keys) {
+  for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < count;
+       j += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t i = first + j;
+    const u32x4 r = philox((uint32_t)i, (uint32_t)(i >> 32), 0u, DOM_ER << 24, key.k0, key.k1);
+    const uint32_t s = (uint32_t)(((uint64_t)r.x * n) >> 32);
+    const uint32_t d = (uint32_t)(((uint64_t)r.y * n) >> 32);
     keys[j] = s == d ? ~0ull : (((unsigned long long)d << 32) | s);
   }
 }
@@ -95,6 +109,12 @@ void launch_rmat_keys(uint32_t scale, uint64_t first, uint64_t count, double a, 
   rmat_keys_kernel<<<2368, 256, 0, stream>>>(scale, first, count, prob_u32_host(a),
                                              prob_u32_host(a + b), prob_u32_host(a + b + c),
                                              make_key(seed), keys);
+}
+
+void launch_er_keys(uint32_t n, uint64_t first, uint64_t count, uint64_t seed,
+                    unsigned long long *keys, cudaStream_t stream) {
+  count_launches(1);
+  er_keys_kernel<<<2368, 256, 0, stream>>>(n, first, count, make_key(seed), keys);
 }
 
 void launch_csr_from_keys(const unsigned long long *keys, uint64_t m, uint32_t n,

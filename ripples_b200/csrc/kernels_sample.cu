@@ -173,6 +173,10 @@ __device__ __forceinline__ SetOutcome ic_plain_set(const DevGraph &G, Key key, u
 }
 
 // One LT set: the single-predecessor walk from root(s) (see lt_walk_kernel).
+// With the graph's per-edge source ranges a step has one dependent round
+// trip: the picked edge's lane also holds the next vertex's in-edge range, so
+// that vertex's edges (degree <= 32: all of them) are requested right after the
+// pick, while the visited-bit atomic of the pick is still in flight.
 __device__ __forceinline__ SetOutcome lt_walk_set(const DevGraph &G, Key key, uint64_t s,
                                                   const WarpCtx &W) {
   const uint32_t lane = lane_id();
@@ -185,42 +189,66 @@ __device__ __forceinline__ SetOutcome lt_walk_set(const DevGraph &G, Key key, ui
   uint32_t qlen = 1;
   bool overflow = false;
   unsigned long long set_exp = 0, set_edges = 0;
-  uint32_t t = lt_threshold(key, s, cur);
   uint32_t lo = __ldg(G.off + cur), hi = __ldg(G.off + cur + 1);
+  // the current vertex's in-edges when it has at most 32 (lane j: edge lo + j)
+  bool have = false;
+  uint2 rec = make_uint2(0u, 0u), rng = make_uint2(0u, 0u);
   for (;;) {
     set_exp += (lane == 0);
     if (hi == lo) break;
-    // 32-ary search for the first edge whose cumulative threshold exceeds t
-    bool none = false;
-    while (hi - lo > 32) {
-      const uint32_t stride = (hi - lo + 31) / 32;
-      const uint32_t p = min(lo + (lane + 1) * stride - 1, hi - 1);
-      const bool pred = t < __ldg(&G.edges[p].y);
-      const uint32_t bal = __ballot_sync(FULL, pred);
-      set_edges += (lane == 0) ? 32 : 0;
-      if (bal == 0) {  // even the last edge's cumulative weight is <= t
-        none = true;
-        break;
+    const uint32_t t = lt_threshold(key, s, cur);
+    if (!have) {
+      // 32-ary search for the first edge whose cumulative threshold exceeds t
+      bool none = false;
+      while (hi - lo > 32) {
+        const uint32_t stride = (hi - lo + 31) / 32;
+        const uint32_t p = min(lo + (lane + 1) * stride - 1, hi - 1);
+        const bool pred = t < __ldg(&G.edges[p].y);
+        const uint32_t bal = __ballot_sync(FULL, pred);
+        set_edges += (lane == 0) ? 32 : 0;
+        if (bal == 0) {  // even the last edge's cumulative weight is <= t
+          none = true;
+          break;
+        }
+        const uint32_t L = __ffs(bal) - 1;
+        const uint32_t nlo = lo + L * stride;
+        hi = min(hi, lo + (L + 1) * stride);
+        lo = nlo;
       }
-      const uint32_t L = __ffs(bal) - 1;
-      const uint32_t nlo = lo + L * stride;
-      hi = min(hi, lo + (L + 1) * stride);
-      lo = nlo;
+      if (none) break;
+      const uint32_t e = lo + lane;
+      rec = make_uint2(0u, 0u);
+      if (e < hi) {
+        rec = __ldg(&G.edges[e]);
+        if (G.src_range) rng = __ldg(&G.src_range[e]);
+      }
     }
-    if (none) break;
-    const uint32_t e = lo + lane;
-    uint2 rec = make_uint2(0u, 0u);
-    if (e < hi) rec = __ldg(&G.edges[e]);
-    const uint32_t bal = __ballot_sync(FULL, e < hi && t < rec.y);
+    const uint32_t bal = __ballot_sync(FULL, lo + lane < hi && t < rec.y);
     set_edges += (lane == 0) ? (hi - lo) : 0;
     if (bal == 0) break;  // no in-edge picked: the walk ends here
-    const uint32_t u = __shfl_sync(FULL, rec.x, __ffs(bal) - 1);
+    const uint32_t L = __ffs(bal) - 1;
+    const uint32_t u = __shfl_sync(FULL, rec.x, L);
     uint32_t old = 0;
     const uint32_t bit = 1u << (u & 31);
     if (lane == 0) old = atomicOr(&W.bm[u >> 5], bit);
-    // next step's inputs, fetched while the atomic is in flight
-    const uint32_t t2 = lt_threshold(key, s, u);
-    const uint32_t lo2 = __ldg(G.off + u), hi2 = __ldg(G.off + u + 1);
+    uint32_t lo2, hi2;
+    if (G.src_range) {
+      lo2 = __shfl_sync(FULL, rng.x, L);
+      hi2 = __shfl_sync(FULL, rng.y, L);
+    } else {
+      lo2 = __ldg(G.off + u);
+      hi2 = __ldg(G.off + u + 1);
+    }
+    // u's in-edges, requested before the visited answer is consumed
+    have = G.src_range && hi2 - lo2 <= 32;
+    if (have) {
+      const uint32_t e = lo2 + lane;
+      rec = make_uint2(0u, 0u);
+      if (e < hi2) {
+        rec = __ldg(&G.edges[e]);
+        rng = __ldg(&G.src_range[e]);
+      }
+    }
     const uint32_t seen = __shfl_sync(FULL, old & bit, 0);
     if (seen) break;
     if (qlen + 1 > W.qcap) {
@@ -231,7 +259,6 @@ __device__ __forceinline__ SetOutcome lt_walk_set(const DevGraph &G, Key key, ui
     if (lane == 0) W.q[qlen] = u;
     ++qlen;
     cur = u;
-    t = t2;
     lo = lo2;
     hi = hi2;
   }

@@ -184,12 +184,14 @@ __global__ void __launch_bounds__(256) sel_init_kernel(const SelDesc *__restrict
   const SelDesc d = *dp;
   const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  const uint64_t n4 = (uint64_t)d.nchunks * (SEL_CHUNK / 4);
-  uint4 *c4 = reinterpret_cast<uint4 *>(d.count);
-  for (uint64_t i = tid; i < n4; i += stride) c4[i] = make_uint4(0, 0, 0, 0);
-  const uint64_t s16 = (d.S + 15) / 16;
-  uint4 *cv = reinterpret_cast<uint4 *>(d.covered);
-  for (uint64_t i = tid; i < s16; i += stride) cv[i] = make_uint4(0, 0, 0, 0);
+  if (!d.keep_counts) {
+    const uint64_t n4 = (uint64_t)d.nchunks * (SEL_CHUNK / 4);
+    uint4 *c4 = reinterpret_cast<uint4 *>(d.count);
+    for (uint64_t i = tid; i < n4; i += stride) c4[i] = make_uint4(0, 0, 0, 0);
+    const uint64_t s16 = (d.S + 15) / 16;
+    uint4 *cv = reinterpret_cast<uint4 *>(d.covered);
+    for (uint64_t i = tid; i < s16; i += stride) cv[i] = make_uint4(0, 0, 0, 0);
+  }
   for (uint64_t i = tid; i < d.nchunks; i += stride) d.dirty[i] = 1;
   for (uint64_t i = tid; i < d.k; i += stride) d.best[i] = 0ull;
   if (tid == 0) *d.done_blocks = 0;
@@ -286,6 +288,13 @@ __global__ void __launch_bounds__(256) sel_cover_kernel(const SelDesc *__restric
       d.dirty[u / SEL_CHUNK] = 1;
     }
   }
+}
+
+// out[i] = count[ids[i]] (ids and out may live in mapped host memory)
+__global__ void gather_counts_kernel(const uint32_t *__restrict__ count,
+                                     const uint32_t *ids, uint32_t m, uint32_t *out) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
+    out[i] = count[ids[i]];
 }
 
 // ---- exclusive scan of u32 counts into u64 offsets (n+1 outputs) ----------
@@ -487,6 +496,14 @@ void launch_sel_cover(const SelDesc *d, uint32_t i, int blocks, cudaStream_t str
   sel_cover_kernel<<<blocks, 256, 0, stream>>>(d, i);
 }
 uint32_t sel_chunk_vertices() { return SEL_CHUNK; }
+
+void launch_gather_counts(const uint32_t *count, const uint32_t *ids, uint32_t m,
+                          uint32_t *out, cudaStream_t stream) {
+  if (m == 0) return;
+  count_launches(1);
+  gather_counts_kernel<<<std::min<uint32_t>((m + 255) / 256, 148), 256, 0, stream>>>(count, ids,
+                                                                                     m, out);
+}
 
 void launch_argmax(const uint32_t *count, uint32_t n, unsigned long long *best,
                    int blocks, cudaStream_t stream) {

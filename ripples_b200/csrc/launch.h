@@ -36,6 +36,30 @@ struct SampleLaunch {
 
 void launch_ic_plain(const SampleLaunch &L, cudaStream_t stream);
 
+// A batch of up to 64*cw IC sets grown by the whole grid (kernels_giant.cu).
+struct GiantLaunch {
+  DevGraph G;
+  DevPool P;
+  Key key;
+  const uint64_t *set_ids = nullptr;   // ncol set ids (colour c = set_ids[c])
+  uint32_t ncol = 0;
+  uint64_t *vis = nullptr, *pend = nullptr;  // n * cw words each, zero between batches
+  uint32_t *pflag = nullptr;           // n, zero between batches
+  uint32_t *front = nullptr, *front_next = nullptr, *touched = nullptr;  // n each
+  uint64_t *masks = nullptr;           // n * cw: the current level's colours per entry
+  uint32_t *ng = nullptr;              // n: in-edge groups per entry
+  uint64_t *goff = nullptr;            // n + 1: exclusive scan of ng
+  unsigned int *ctr = nullptr;         // [0] next-frontier tail, [1] touched count
+  uint32_t *sizes = nullptr, *fill = nullptr;  // per colour
+  unsigned long long *starts = nullptr;        // per colour: pool offset
+  unsigned long long *stats = nullptr;         // the pool's counters
+};
+// what: 0 seed roots, 1 level prep (n_items = frontier size), 2 expand
+// (n_items = frontier size, level), 3 per-colour sizes, 4 scatter (n_items =
+// touched), 5 set offsets/lengths
+void launch_giant(int what, int cw, const GiantLaunch &L, uint32_t n_items, uint32_t level,
+                  int blocks, cudaStream_t s);
+
 // One IMM instance of a multi-instance launch.
 struct InstanceDesc {
   DevGraph G;
@@ -116,6 +140,8 @@ inline uint32_t prob_u32_host(double p) {
   if (y >= 4294967295.0) return 0xFFFFFFFFu;
   return (uint32_t)(uint64_t)y;
 }
+void launch_er_keys(uint32_t n, uint64_t first, uint64_t count, uint64_t seed,
+                    unsigned long long *keys, cudaStream_t stream);
 void launch_rmat_keys(uint32_t scale, uint64_t first, uint64_t count, double a, double b,
                       double c, uint64_t seed, unsigned long long *keys, cudaStream_t stream);
 void launch_csr_from_keys(const unsigned long long *keys, uint64_t m, uint32_t n,
@@ -127,6 +153,8 @@ void launch_weights(int kind, const uint64_t *index, uint32_t n, uint64_t seed, 
 void launch_pack_ic(const uint64_t *index, const float *w, uint32_t n,
                     uint64_t m, uint32_t *off, uint2 *edges, const uint32_t *src,
                     cudaStream_t stream);
+void launch_lt_range(const uint32_t *off, const uint2 *edges, uint64_t m, uint2 *range,
+                     cudaStream_t stream);
 void launch_pack_lt(const uint64_t *index, const float *w, uint32_t n,
                     uint64_t m, uint32_t *off, uint2 *edges, const uint32_t *src,
                     cudaStream_t stream);
@@ -170,6 +198,7 @@ struct SelDesc {
   uint64_t S;                      // select over sets [0, S)
   uint32_t n, nchunks;             // vertices; chunks of sel_chunk_vertices()
   uint32_t k;                      // picks
+  uint32_t keep_counts;            // 1: count and covered are already set up
   uint32_t *count;                 // nchunks * chunk entries (tail stays 0)
   unsigned long long *cmax;        // per chunk: max key
   uint8_t *dirty;                  // per chunk
@@ -182,6 +211,9 @@ void launch_sel_count(const SelDesc *d, int blocks, cudaStream_t stream);
 void launch_sel_pick(const SelDesc *d, uint32_t i, int blocks, cudaStream_t stream);
 void launch_sel_cover(const SelDesc *d, uint32_t i, int blocks, cudaStream_t stream);
 uint32_t sel_chunk_vertices();
+// out[i] = count[ids[i]], i < m
+void launch_gather_counts(const uint32_t *count, const uint32_t *ids, uint32_t m,
+                          uint32_t *out, cudaStream_t stream);
 
 // Copies sets [first, first+count) into out[csr[i] ..] in set-id order.
 void launch_gather_sets(const DevPool &P, uint64_t first, uint64_t count,

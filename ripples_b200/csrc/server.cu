@@ -51,6 +51,7 @@ struct Active {
   uint64_t S = 0;      // this round's selection prefix
   uint64_t delta = 0;  // sets a fresh run would sample this round
   uint64_t footprint = 0;
+  bool stalled = false;  // this tick: its pool could not grow; retried next tick
   clk::time_point t_sub, t_start, t_round;
   rip_imm_record R{};
   std::vector<uint32_t> picks;
@@ -186,6 +187,7 @@ int launch_round(rip_server *s, Active &a) {
   hd->n = (uint32_t)a.n;
   hd->nchunks = nchunks;
   hd->k = k;
+  hd->keep_counts = 0;
   hd->count = ptr<uint32_t>(sl.count);
   hd->cmax = ptr<unsigned long long>(sl.cmax);
   hd->dirty = ptr<uint8_t>(sl.dirty);
@@ -319,23 +321,6 @@ void evict_idle_pools(rip_server *s) {
     }
   }
   s->pools.swap(keep);
-}
-
-// Ends the admitted queries on pool p with `code` (the pool could not grow or
-// be indexed within the device budget); returns how many ended.
-uint32_t fail_pool_queries(rip_server *s, rip_pool *p, int code) {
-  uint32_t n = 0;
-  std::vector<Active> keep;
-  for (Active &a : s->active) {
-    if (a.pool == p) {
-      finish(s, a, code);
-      ++n;
-    } else {
-      keep.push_back(std::move(a));
-    }
-  }
-  s->active.swap(keep);
-  return n;
 }
 
 bool out_of_room(int rc) { return rc == RIP_ERR_NOMEM || rc == RIP_ERR_LIMIT; }
@@ -522,17 +507,25 @@ extern "C" int rip_server_tick(rip_server *s, uint32_t *completed) {
   if (!sp.empty()) {
     const int rc = rip_sample_multi(c, sp.data(), sseed.data(), scnt.data(), (uint32_t)sp.size());
     if (out_of_room(rc)) {
-      // free idle pools, then grow the pools one by one; queries on a pool
-      // that still does not fit end with the error
+      // Free idle pools, then grow the pools one by one.  A pool grows to its
+      // largest remaining request; when that does not fit, the queries asking
+      // for it wait for the next tick (other queries' pools may become idle
+      // and be freed by then) and the next largest request is tried.
       evict_idle_pools(s);
       for (size_t i = 0; i < sp.size(); ++i) {
-        uint64_t target = 0;
-        for (size_t j = 0; j < mp.size(); ++j)
-          if (mp[j] == sp[i]) target = need[j];
-        const uint64_t cnt = target > sp[i]->num_sets ? target - sp[i]->num_sets : 0;
-        const int r = cnt ? rip_sample_multi(c, &sp[i], &sseed[i], &cnt, 1) : RIP_OK;
-        if (out_of_room(r)) done_now += fail_pool_queries(s, sp[i], r);
-        else TRY(r);
+        for (;;) {
+          uint64_t target = 0;
+          for (Active &a : s->active)
+            if (a.pool == sp[i] && !a.stalled) target = std::max(target, a.S);
+          const uint64_t cnt = target > sp[i]->num_sets ? target - sp[i]->num_sets : 0;
+          const int r = cnt ? rip_sample_multi(c, &sp[i], &sseed[i], &cnt, 1) : RIP_OK;
+          if (!out_of_room(r)) {
+            TRY(r);
+            break;
+          }
+          for (Active &a : s->active)
+            if (a.pool == sp[i] && a.S == target) a.stalled = true;
+        }
       }
     } else {
       TRY(rc);
@@ -547,47 +540,34 @@ extern "C" int rip_server_tick(rip_server *s, uint32_t *completed) {
   }
   // 3. indexes, 4. selections
   bool any_dev = false;
-  for (size_t i = 0; i < s->active.size();) {
-    Active &a = s->active[i];
-    if (a.q->tiebreak != RIP_TIE_LOWEST_ID) {
-      ++i;
-      continue;
-    }
+  for (Active &a : s->active) {
+    if (a.stalled || a.q->tiebreak != RIP_TIE_LOWEST_ID) continue;
     const int r = extend_index(a.pool);
     if (out_of_room(r)) {
-      done_now += fail_pool_queries(s, a.pool, r);
-      i = 0;  // the active list changed
+      for (Active &b : s->active)
+        if (b.pool == a.pool) b.stalled = true;
       continue;
     }
     TRY(r);
     any_dev = true;
-    ++i;
   }
   if (any_dev) {
     const uint32_t chunk = sel_chunk_vertices();
-    std::vector<Active> keep;
     for (Active &a : s->active) {
-      if (a.q->tiebreak == RIP_TIE_LOWEST_ID) {
-        const int r = slot_buffers(s, s->slots[a.slot], (uint32_t)((a.n + chunk - 1) / chunk),
-                                   a.S, a.q->k);
-        if (out_of_room(r)) {
-          finish(s, a, r);
-          ++done_now;
-          continue;
-        }
-        TRY(r);
-      }
-      keep.push_back(std::move(a));
+      if (a.stalled || a.q->tiebreak != RIP_TIE_LOWEST_ID) continue;
+      const int r = slot_buffers(s, s->slots[a.slot], (uint32_t)((a.n + chunk - 1) / chunk),
+                                 a.S, a.q->k);
+      if (out_of_room(r)) a.stalled = true;
+      else TRY(r);
     }
-    s->active.swap(keep);
     CK(c, cudaStreamSynchronize(c->stream));
     for (Active &a : s->active)
-      if (a.q->tiebreak == RIP_TIE_LOWEST_ID) TRY(launch_round(s, a));
+      if (!a.stalled && a.q->tiebreak == RIP_TIE_LOWEST_ID) TRY(launch_round(s, a));
   }
   std::vector<double> fs(s->active.size(), 0.0);
   for (size_t i = 0; i < s->active.size(); ++i) {
     Active &a = s->active[i];
-    if (a.q->tiebreak != RIP_TIE_REF_HEAP) continue;
+    if (a.stalled || a.q->tiebreak != RIP_TIE_REF_HEAP) continue;
     a.picks.assign(a.q->k, 0);
     uint32_t ns = 0;
     TRY(rip_select(a.pool, a.S, a.q->k, RIP_TIE_REF_HEAP, a.picks.data(), nullptr, &ns,
@@ -596,7 +576,7 @@ extern "C" int rip_server_tick(rip_server *s, uint32_t *completed) {
   }
   for (size_t i = 0; i < s->active.size(); ++i) {
     Active &a = s->active[i];
-    if (a.q->tiebreak != RIP_TIE_LOWEST_ID) continue;
+    if (a.stalled || a.q->tiebreak != RIP_TIE_LOWEST_ID) continue;
     SelSlot &sl = s->slots[a.slot];
     CK(c, cudaStreamSynchronize(sl.st));
     read_round(sl, a.q->k, a.picks, a.gains);
@@ -604,10 +584,27 @@ extern "C" int rip_server_tick(rip_server *s, uint32_t *completed) {
     for (uint64_t g : a.gains) cov += g;
     fs[i] = a.S ? (double)cov / (double)a.S : 0.0;
   }
-  // 5. martingale steps, completions
+  // 5. martingale steps, completions.  When every admitted query waited for
+  // memory, nothing can free any: the one asking for the most sets ends.
+  bool progress = false;
+  size_t worst = 0;
+  for (size_t i = 0; i < s->active.size(); ++i) {
+    if (!s->active[i].stalled) progress = true;
+    if (s->active[i].S > s->active[worst].S) worst = i;
+  }
   std::vector<Active> keep;
   for (size_t i = 0; i < s->active.size(); ++i) {
     Active &a = s->active[i];
+    if (a.stalled) {
+      a.stalled = false;
+      if (!progress && i == worst) {
+        finish(s, a, RIP_ERR_NOMEM);
+        ++done_now;
+      } else {
+        keep.push_back(std::move(a));
+      }
+      continue;
+    }
     if (a.phase == 1) {
       a.R.select_ms = ms_since(a.t_round);
       a.q->f = fs[i];

@@ -179,16 +179,34 @@ class DeviceGraph:
         check(lib.rip_rmat_keys_device(ctx.h, scale, 0, num_edges, a, b, c, seed,
                                        ctypes.c_void_p(keys.data_ptr())),
               "rip_rmat_keys_device", ctx.h)
+        return cls._from_keys(ctx, keys, 1 << scale, model, weights, weight_seed, lo, hi)
+
+    @classmethod
+    def erdos_renyi_on_device(cls, ctx: Context, n: int, num_edges: int, model: str,
+                              weights: int, seed: int = 0, weight_seed: int = 1,
+                              lo: float = 0.0, hi: float = 1.0) -> "DeviceGraph":
+        """HostGraph.erdos_renyi(...).with_weights(...), built on the device."""
+        import torch
+        dev = torch.device("cuda", torch.cuda.current_device())
+        keys = torch.empty(num_edges, dtype=torch.int64, device=dev)
+        check(lib.rip_er_keys_device(ctx.h, n, 0, num_edges, seed,
+                                     ctypes.c_void_p(keys.data_ptr())),
+              "rip_er_keys_device", ctx.h)
+        return cls._from_keys(ctx, keys, n, model, weights, weight_seed, lo, hi)
+
+    @classmethod
+    def _from_keys(cls, ctx, keys, n, model, weights, weight_seed, lo, hi) -> "DeviceGraph":
+        import torch
         keys = torch.unique(keys[keys >= 0])  # drop self-loops (~0), sort, dedup
-        torch.cuda.synchronize(dev)
+        torch.cuda.synchronize(keys.device)
         h = ctypes.c_void_p()
         check(lib.rip_graph_from_keys(ctx.h, ctypes.c_void_p(keys.data_ptr()), keys.numel(),
-                                      1 << scale, weights, weight_seed, lo, hi, MODELS[model],
+                                      n, weights, weight_seed, lo, hi, MODELS[model],
                                       ctypes.byref(h)), "rip_graph_from_keys", ctx.h)
         m = keys.numel()
         del keys
         obj = cls.__new__(cls)
-        obj.ctx, obj.model, obj.n, obj.m, obj.h = ctx, model, 1 << scale, m, h
+        obj.ctx, obj.model, obj.n, obj.m, obj.h = ctx, model, n, m, h
         obj._pools = weakref.WeakSet()
         ctx._children.add(obj)
         return obj
@@ -199,6 +217,19 @@ class DeviceGraph:
         check(lib.rip_graph_export(self.h, _ptr(idx), _ptr(src)), "rip_graph_export",
               self.ctx.h)
         return idx, src[: self.m]
+
+    TUNE_NAMES = ("plain, heavy>2^18 grid BFS", "plain, heavy>2^14 grid BFS",
+                  "plain, heavy>2^18 CTA per set", "fused 64", "fused 128", "fused 256")
+
+    def autotune(self, seed: int = 0, pilot: int = 0) -> dict:
+        """Times each IC sampler configuration on a pilot of sets and keeps the
+        fastest for this graph (``rip_graph_autotune``)."""
+        ms = np.zeros(len(self.TUNE_NAMES), dtype=np.float64)
+        ch = ctypes.c_int()
+        check(lib.rip_graph_autotune(self.h, seed, pilot, _ptr(ms), ctypes.byref(ch)),
+              "rip_graph_autotune", self.ctx.h)
+        return {"choice": ch.value, "name": self.TUNE_NAMES[ch.value],
+                "ms": {n: float(t) for n, t in zip(self.TUNE_NAMES, ms) if t >= 0}}
 
     def thresholds(self) -> np.ndarray:
         out = np.empty(self.m, dtype=np.uint32)
@@ -254,6 +285,16 @@ class Pool:
         self._chk(lib.rip_pool_configure(self.h, colors, slots, log_capacity),
                   "rip_pool_configure")
 
+    def heavy_batch(self, min_sets: int) -> None:
+        """Heavy IC sets pending from which the grid-wide multi-colour BFS
+        grows them (0 = one CTA per set)."""
+        self._chk(lib.rip_pool_heavy_batch(self.h, min_sets), "rip_pool_heavy_batch")
+
+    def select_guess(self, percent: int) -> None:
+        """First-fetch threshold of reference-heap picks, % of the previous
+        gain (0 = adaptive)."""
+        self._chk(lib.rip_pool_select_guess(self.h, percent), "rip_pool_select_guess")
+
     def work_caps(self, plain: int, fused: int) -> None:
         self._chk(lib.rip_pool_work_caps(self.h, plain, fused), "rip_pool_work_caps")
 
@@ -307,8 +348,8 @@ class Pool:
     def select_profile(self) -> dict:
         out = np.zeros(12, dtype=np.float64)
         self._chk(lib.rip_select_profile(self.h, _ptr(out)), "rip_select_profile")
-        keys = ["prep_ms", "heap_ms", "picks_ms", "pops", "seeds", "reports", "selections",
-                "cover_sync_ms", "apply_ms", "pop_ms"]
+        keys = ["prep_ms", "heap_ms", "picks_ms", "pops", "seeds", "candidates", "selections",
+                "cover_fetch_ms", "full_fetches", "pop_ms"]
         return dict(zip(keys, out.tolist()))
 
     def count(self, num_sets: Optional[int] = None) -> np.ndarray:

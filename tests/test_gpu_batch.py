@@ -152,3 +152,23 @@ def test_server_rejects_bad_query(ctx, graphs):
     assert bad.done and bad.status == -1
     assert good.done and good.status == 0 and len(good.seeds) == 5
     srv.close()
+
+
+def test_autotune_picks_a_configuration_and_sets_stay_exact(ctx):
+    # a supercritical IC graph (heavy sets) and an LT graph
+    g = rb.HostGraph.rmat(12, 16 << 12, seed=3).with_weights(rb.WEIGHTS_UNIFORM, seed=4,
+                                                             lo=0.0, hi=0.3)
+    dg = rb.DeviceGraph(ctx, g, "IC")
+    r = dg.autotune(seed=5, pilot=512)
+    assert 0 <= r["choice"] < len(dg.TUNE_NAMES) and len(r["ms"]) == len(dg.TUNE_NAMES)
+    p = rb.Pool(dg)
+    p.sample(1500, seed=9)  # RIP_SAMPLER_AUTO: the tuned configuration
+    thr = O.pack("IC", g.index, g.weights)
+    ooff, ovtx, _ = O.sample("IC", g.n, g.index, g.src, thr, 9, 0, 1500)
+    off, vtx = p.export()
+    assert np.array_equal(off, ooff) and np.array_equal(vtx, ovtx)
+    p.close()
+    dg.close()
+    lt = rb.DeviceGraph(ctx, lt_graph(11), "LT")
+    assert lt.autotune(seed=1)["choice"] == 0
+    lt.close()

@@ -197,6 +197,53 @@ def test_selection_on_sampled_pool(ctx, tiebreak):
         assert f == of
 
 
+@pytest.mark.parametrize("guess", [1, 50, 0, 100])
+def test_reference_heap_candidate_fetch(ctx, guess):
+    # many vertices and heavy ties (LT walks are short, most counts are 1-3):
+    # whatever threshold the first fetch of a pick uses (too low: more items
+    # than the fetch holds; too high: a second, exact fetch), the seeds equal
+    # the reference heap's (the oracle's)
+    g = lt_graph(14, 4, seed=21)
+    dg, p = device_pool(ctx, g, "LT")
+    p.sample(30000, seed=5)
+    p.select_guess(guess)
+    off, vtx = p.export()
+    for k, S in [(300, 30000), (40, 9000)]:
+        f, seeds, gains = p.select(k, num_sets=S, tiebreak=rb.TIE_REF_HEAP)
+        of, oseeds, ogains, _ = O.select(g.n, off[: S + 1], vtx[: int(off[S])], k, 0)
+        assert seeds.tolist() == oseeds.tolist()
+        assert gains.tolist() == ogains.tolist() and f == of
+    # the counts after the last update step (every seed but a k-th one
+    # covered) come back on demand
+    covering = set(oseeds.tolist()[:-1] if len(oseeds) == k else oseeds.tolist())
+    want = np.zeros(g.n, np.int64)
+    for s in range(S):
+        members = vtx[int(off[s]):int(off[s + 1])]
+        if not covering.intersection(members.tolist()):
+            np.add.at(want, members.astype(np.int64), 1)
+    assert p.select_counts().tolist() == want.tolist()
+
+
+@pytest.mark.parametrize("scale,hi", [(13, 0.2), (11, 0.5)])
+def test_giant_component_sets_bit_exact(ctx, scale, hi):
+    """Supercritical IC (R-MAT, degree 16): a large share of the sets hold a
+    large share of the graph and go to the grid-wide multi-colour BFS in
+    batches of up to 256; they must equal the oracle's sets."""
+    g = rb.HostGraph.rmat(scale, 16 << scale, seed=3).with_weights(
+        rb.WEIGHTS_UNIFORM, seed=4, lo=0.0, hi=hi)
+    dg, p = device_pool(ctx, g, "IC", 64)
+    p.work_caps(1 << 12, 1 << 16)
+    p.sample(700, seed=21, sampler=rb.SAMPLER_PLAIN)
+    p.sample(300, seed=21, sampler=rb.SAMPLER_FUSED)
+    off, vtx = p.export()
+    ooff, ovtx, ost = oracle_sets(g, "IC", 21, 0, 1000)
+    assert_same_sets(off, vtx, ooff, ovtx)
+    lens = np.diff(off.astype(np.int64))
+    assert (lens > g.n // 20).sum() > 32  # the giant sets were there
+    st = p.stats()
+    assert st[2] == 1000 and st[3] == len(vtx) and st[5] == ost[1]
+
+
 def test_selection_stops_when_all_covered(ctx):
     dg = empty_graph(ctx, 10)
     p = rb.Pool(dg)
@@ -279,16 +326,26 @@ def test_device_graph_construction_matches_host(ctx, model, weights, lo, hi):
     assert np.array_equal(idx, hg.index) and np.array_equal(src, hg.src)
     assert np.array_equal(dg.thresholds(), O.pack(model, hg.index, hg.weights))
     dg.close()
+    eg = rb.HostGraph.erdos_renyi(3000, 40000, seed=6).with_weights(weights, seed=4, lo=lo, hi=hi)
+    de = rb.DeviceGraph.erdos_renyi_on_device(ctx, 3000, 40000, model, weights, seed=6,
+                                              weight_seed=4, lo=lo, hi=hi)
+    idx, src = de.export()
+    assert np.array_equal(idx, eg.index) and np.array_equal(src, eg.src)
+    assert np.array_equal(de.thresholds(), O.pack(model, eg.index, eg.weights))
+    de.close()
 
 
 @pytest.mark.parametrize("weights", [rb.WEIGHTS_UNIFORM, rb.WEIGHTS_WC])
 @pytest.mark.parametrize("sampler", [rb.SAMPLER_PLAIN, rb.SAMPLER_FUSED])
-def test_big_set_path_bit_exact(ctx, weights, sampler):
-    """Tiny edge-work budgets send most sets to the CTA-per-set sampler; the
-    sets must not change."""
+@pytest.mark.parametrize("heavy_batch", [0, 1])
+def test_big_set_path_bit_exact(ctx, weights, sampler, heavy_batch):
+    """Tiny edge-work budgets send most sets to the heavy-set samplers (one
+    CTA per set, or the grid-wide multi-colour BFS); the sets must not
+    change."""
     g = rb.HostGraph.rmat(12, 16 << 12, seed=8).with_weights(weights, seed=9, lo=0.0, hi=0.4)
     dg, p = device_pool(ctx, g, "IC", 64)
     p.work_caps(64, 256)
+    p.heavy_batch(heavy_batch)
     p.sample(3000, seed=12, sampler=sampler)
     off, vtx = p.export()
     ooff, ovtx, ost = oracle_sets(g, "IC", 12, 0, 3000)
