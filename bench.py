@@ -260,10 +260,18 @@ def main():
     ap.add_argument("--serve-queries", type=int, default=256)
     ap.add_argument("--serve-eps", default="0.5,0.3,0.13")
     ap.add_argument("--serve-max-active", type=int, default=32)
+    ap.add_argument("--serve-deadline", type=float, default=240.0,
+                    help="s1: seconds after which unfinished queries count as failed")
     ap.add_argument("--baseline-seconds", type=float, default=60.0)
+    ap.add_argument("--sampler-case", type=int, default=0,
+                    help="profiling case: one sampler launch of this many sets on the "
+                         "workload's graph (after a 1024-set pilot launch); prints its "
+                         "algorithmic bytes")
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
     world, rank, local = dist_setup()
+    if args.sampler_case:
+        return run_sampler_case(args, w, local)
     if w.get("kind") == "batch":
         return run_batch(args, w, world, rank, local)
     if w.get("kind") == "serve":
@@ -388,7 +396,7 @@ def main():
     # Algorithmic bytes: 8 B per vertex expansion (two u32 CSR offsets), 8 B
     # per in-edge record read (u32 source + u32 threshold), 4 B per pool
     # element written, 8 + 4 B per set (pool offset + length).
-    alg_bytes = 8 * int(st_tot[0]) + 8 * int(st_tot[1]) + 4 * int(st_tot[3]) + 12 * int(st_tot[2])
+    alg_bytes = alg_bytes_of(st_tot)
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (kern_ms / 1e3) / 1e9 if kern_ms > 0 else None
     kernel = "lt_walk_kernel" if w["model"] == "LT" else "ic_fused_kernel"
@@ -450,6 +458,39 @@ def main():
     return 0
 
 
+def alg_bytes_of(st):
+    """Algorithmic bytes of the sampler work in a pool's counters: 8 B per
+    vertex expansion (two CSR offsets), 8 B per in-edge record read (source +
+    threshold), 4 B per stored element, 12 B per stored set (offset + length)."""
+    return 8 * int(st[0]) + 8 * int(st[1]) + 4 * int(st[3]) + 12 * int(st[2])
+
+
+def run_sampler_case(args, w, local):
+    import torch
+    import ripples_b200 as rb
+    torch.cuda.set_device(local)
+    g = build_graph(w)
+    ctx = rb.Context(local)
+    dg = rb.DeviceGraph(ctx, g, w["model"])
+    pool = rb.Pool(dg)
+    pool.sample(1024, seed=5)
+    ctx.sync()
+    st0 = pool.stats()
+    km0, _, _ = pool.timing()
+    pool.sample(args.sampler_case, seed=5)
+    ctx.sync()
+    st = pool.stats() - st0
+    km, _, _ = pool.timing()
+    alg = alg_bytes_of(st)
+    print(json.dumps({"case": w["name"], "sets": args.sampler_case, "alg_bytes": alg,
+                      "kernel_ms": km - km0, "gb_per_s": alg / ((km - km0) / 1e3) / 1e9,
+                      "stats": [int(x) for x in st]}))
+    pool.close()
+    dg.close()
+    ctx.close()
+    return 0
+
+
 def _pct(xs, q):
     import numpy as np
     return float(np.percentile(np.asarray(xs, dtype=np.float64), q)) if xs else None
@@ -502,13 +543,13 @@ def run_batch(args, w, world, rank, local):
         return qs
 
     def plain(tag, limit_s=None):
-        """One instance at a time: a fresh pool, one set per warp, heavy IC
-        sets one CTA each, no multi-instance launch.  An instance whose pool
-        does not fit the device fails here as it does in the batch."""
+        """One instance at a time through rip_imm_pool: a fresh pool and the
+        same (autotuned) samplers as the batch, no multi-instance launch, no
+        shared rounds.  An instance whose pool does not fit the device fails
+        here as it does in the batch."""
         out, t0 = [], time.perf_counter()
         for x in inst:
             p = rb.Pool(graphs[x["g"]]["dg"])
-            p.heavy_batch(0)
             try:
                 seeds, rec = p.imm(x["k"], x["eps"], seed=x["seed"] + tag,
                                    tiebreak=rb.TIE_LOWEST_ID, sampler=rb.SAMPLER_PLAIN)
@@ -649,12 +690,18 @@ def run_p3(args, w, world, rank, local):
     return 0
 
 
+def _progress(t0, msg):
+    """Timestamped progress line on stderr (the JSON line stays on stdout)."""
+    print(f"[{time.perf_counter() - t0:8.2f}s] {msg}", file=sys.stderr, flush=True)
+
+
 def run_serve(args, w, world, rank, local):
     import numpy as np
     import torch
     import ripples_b200 as rb
     if _not_on_rank0(world, rank, args, w):
         return 0
+    t_run = time.perf_counter()
     torch.cuda.set_device(local)
     ctx = rb.Context(local)
     scales = [int(x) for x in args.serve_scales.split(",") if x]
@@ -667,9 +714,12 @@ def run_serve(args, w, world, rank, local):
         graphs[(sc, "LT")] = rb.DeviceGraph.rmat_on_device(
             ctx, sc, 16 << sc, "LT", rb.WEIGHTS_LT_NORMALIZED, seed=0, weight_seed=1)
     t_build = time.perf_counter() - t_build
+    _progress(t_run, f"graphs built ({t_build:.1f}s)")
     t_tune = time.perf_counter()
-    tuned = {f"{sc}{m}": graphs[(sc, m)].autotune(seed=3, pilot=1024)["name"]
-             for sc in scales for m in ("IC",)}
+    tuned = {}
+    for sc in scales:
+        tuned[f"{sc}IC"] = graphs[(sc, "IC")].autotune(seed=3, pilot=1024)["name"]
+        _progress(t_run, f"autotuned {sc}IC: {tuned[f'{sc}IC']}")
     t_tune = time.perf_counter() - t_tune
     rng = np.random.default_rng(3)
     N = args.serve_queries
@@ -691,6 +741,8 @@ def run_serve(args, w, world, rank, local):
     clocks.start()
     torch.cuda.synchronize()
     sub_t = [0.0] * N
+    ticks = 0
+    _progress(t_run, "serving")
     t0 = time.perf_counter()
     nxt = 0
     while True:
@@ -700,12 +752,23 @@ def run_serve(args, w, world, rank, local):
             sub_t[nxt] = now
             nxt += 1
         active, queued = srv.pending()
+        ticks += 1
+        if ticks % 20 == 0:
+            done_n = sum(1 for q in qs[:nxt] if q.done)
+            _progress(t_run, f"tick {ticks}: submitted {nxt} active {active} queued {queued} "
+                             f"done {done_n}")
+        if now > args.serve_deadline:
+            break
         if active == 0 and queued == 0:
             if nxt >= N:
                 break
             time.sleep(max(0.0, arrivals[nxt] - (time.perf_counter() - t0)))
             continue
+        t_tick = time.perf_counter()
         srv.tick()
+        t_tick = time.perf_counter() - t_tick
+        if t_tick > 1.0:
+            _progress(t_run, f"tick {ticks} took {t_tick:.1f}s (active {active})")
     torch.cuda.synchronize()
     makespan = time.perf_counter() - t0
     clk = clocks.stop()
@@ -722,7 +785,6 @@ def run_serve(args, w, world, rank, local):
     for i in range(N):
         s = spec[i]
         p = rb.Pool(graphs[(s["scale"], s["model"])])
-        p.heavy_batch(0)
         t1 = time.perf_counter()
         try:
             seeds, rec = p.imm(s["k"], s["eps"], seed=3, tiebreak=rb.TIE_LOWEST_ID,
@@ -733,6 +795,8 @@ def run_serve(args, w, world, rank, local):
         except rb.RipError:
             pass
         base.append(1e3 * (time.perf_counter() - t1))
+        _progress(t_run, f"baseline query {i} ({s['scale']} {s['model']} k={s['k']} "
+                         f"eps={s['eps']}): {base[-1]:.0f} ms")
         p.close()
         if time.perf_counter() - tb > args.baseline_seconds:
             break

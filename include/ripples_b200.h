@@ -331,8 +331,11 @@ int rip_server_submit(rip_server *s, rip_imm_query *q);
 int rip_server_tick(rip_server *s, uint32_t *completed);
 int rip_server_pending(const rip_server *s, uint32_t *active, uint32_t *queued);
 /* [0] ticks, [1] completed, [2] selection-graph launches, [3] resident pools,
- * [4] admitted footprint bytes, [5] microseconds spent in ticks */
-int rip_server_stats(const rip_server *s, uint64_t out[6]);
+ * [4] admitted footprint bytes, [5] microseconds spent in ticks, [6] times a
+ * query was suspended (every admitted query waited for memory: the largest
+ * went back to the queue, its pool freed, to restart later).  A query ends
+ * with RIP_ERR_NOMEM only when it does not fit even alone. */
+int rip_server_stats(const rip_server *s, uint64_t out[7]);
 
 /* ---- sampling without allocation ------------------------------------------- */
 /* No counterpart in the reference.  A variant of rip_sample's one-set-per-warp

@@ -98,8 +98,6 @@ int rip_ctx_memory(rip_ctx *c, size_t *used, size_t *budget) {
 // ---------------------------------------------------------------------------
 static rip_graph *pool_graph(const rip_pool *p);
 
-static int build_lt_range(rip_ctx *c, rip_graph *g);
-
 extern "C" int rip_graph_upload(rip_ctx *c, const uint64_t *index,
                                 const uint32_t *src, const float *w, uint32_t n,
                                 uint64_t m, int model, rip_graph **out) {
@@ -166,27 +164,14 @@ extern "C" int rip_graph_upload(rip_ctx *c, const uint64_t *index,
   dfree(c, d_index);
   dfree(c, d_src);
   dfree(c, d_w);
-  if (rc == RIP_OK) rc = build_lt_range(c, g);
   if (rc != RIP_OK) {
     dfree(c, g->off);
     dfree(c, g->edges);
-    dfree(c, g->range);
     delete g;
     return rc;
   }
   c->graphs.push_back(g);
   *out = g;
-  return RIP_OK;
-}
-
-// The per-edge source ranges of an LT graph (after packing).
-static int build_lt_range(rip_ctx *c, rip_graph *g) {
-  if (g->model != RIP_MODEL_LT || g->m == 0) return RIP_OK;
-  TRY(dalloc(c, g->range, sizeof(uint2) * (size_t)g->m));
-  launch_lt_range(ptr<uint32_t>(g->off), ptr<uint2>(g->edges), g->m, ptr<uint2>(g->range),
-                  c->stream);
-  CK(c, cudaGetLastError());
-  CK(c, cudaStreamSynchronize(c->stream));
   return RIP_OK;
 }
 
@@ -218,11 +203,9 @@ static int pack_device_csr(rip_ctx *c, const uint64_t *d_index, const uint32_t *
     if (e == cudaSuccess) e = cudaGetLastError();
     if (e != cudaSuccess) rc = set_err(c, RIP_ERR_CUDA, "pack failed: %s", cudaGetErrorString(e));
   }
-  if (!rc) rc = build_lt_range(c, g);
   if (rc) {
     dfree(c, g->off);
     dfree(c, g->edges);
-    dfree(c, g->range);
     delete g;
     return rc;
   }
@@ -317,7 +300,6 @@ extern "C" int rip_graph_destroy(rip_graph *g) {
   erase_ptr(c->graphs, g);
   dfree(g->ctx, g->off);
   dfree(g->ctx, g->edges);
-  dfree(g->ctx, g->range);
   delete g;
   return RIP_OK;
 }
@@ -1501,7 +1483,8 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
       cmap.reset(1);
       cmap.put(queue.top().first, queue.top().second);
     }
-    double ratio = 0.9;  // recent gain ratio g_i / g_{i-1}
+    double ratio = 0.9;   // recent gain ratio g_i / g_{i-1}
+    double margin = 0.9;  // guess = margin * ratio: lowered when a guess misses
     auto fetch_all = [&]() -> int {
       CK(c, cudaMemcpyAsync(h_count.p, p->count.p, sizeof(uint32_t) * (size_t)n,
                             cudaMemcpyDeviceToHost, c->stream));
@@ -1515,10 +1498,13 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
       const auto t_g0 = clk::now();
       if (!first) {
         const uint64_t g_prev = out_gains.back();
-        const double guess = p->cand_fixed ? p->cand_fixed / 100.0 : 0.8 * ratio;
+        const double guess = p->cand_fixed ? p->cand_fixed / 100.0 : margin * ratio;
         uint32_t T = (uint32_t)std::max<double>(1.0, std::floor((double)g_prev * guess));
         for (int round = 0;; ++round) {
+          const auto t_c0 = clk::now();
           const uint32_t nc = collect_at_least(queue.items(), T, CAND_CAP, h_ids, stack);
+          p->sel_prof[10] += ms_since(t_c0);
+          p->sel_prof[11] += 1;
           if (nc > CAND_CAP) {
             if (round == 0 && T < g_prev) {  // guess too low: raise it
               T = (uint32_t)std::min<uint64_t>(g_prev, (uint64_t)T + (g_prev - T + 1) / 2);
@@ -1538,8 +1524,12 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
             cmap.put(h_ids[i], cv);
             mc = std::max(mc, cv);
           }
-          if (mc >= T || nc == queue.size()) break;
+          if (mc >= T || nc == queue.size()) {
+            if (round == 0) margin = std::min(0.97, margin + 0.01);
+            break;
+          }
           T = std::max<uint32_t>(mc, 1u);  // mc <= m < T: exact next round
+          margin = std::max(0.5, margin - 0.05);
         }
       }
       p->sel_prof[7] += ms_since(t_g0);

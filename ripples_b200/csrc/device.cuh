@@ -19,9 +19,6 @@ struct DevGraph {
   uint64_t m;
   const uint32_t *off;
   const uint2 *edges;
-  // LT graphs: per edge, the source's in-edge range (off[src], off[src+1]);
-  // may be null (the walk then loads the offsets itself)
-  const uint2 *src_range = nullptr;
 };
 
 // Flat RRR pool: set s occupies vtx[set_off[s] .. set_off[s] + set_len[s]).

@@ -238,7 +238,6 @@ struct rip_graph {
   uint64_t m;
   int model;
   DevMem off, edges;
-  DevMem range;  // LT: per edge, the source's in-edge range
   // IC sampler configuration picked by rip_graph_autotune (pools created
   // afterwards start from it; RIP_SAMPLER_AUTO follows `sampler`)
   struct Tuned {
@@ -248,8 +247,7 @@ struct rip_graph {
     uint64_t cap_plain = 1ull << 18, cap_fused = 1ull << 23;
   } tuned;
   DevGraph view() {
-    return DevGraph{n, m, ptr<uint32_t>(off), ptr<uint2>(edges),
-                    range.p ? ptr<uint2>(range) : nullptr};
+    return DevGraph{n, m, ptr<uint32_t>(off), ptr<uint2>(edges)};
   }
 };
 
@@ -313,7 +311,8 @@ struct rip_pool {
   // selection profile: [0] count+index kernels and counts D2H, [1] heap build,
   // [2] pick loop, [3] heap pops, [4] picks, [5] candidate counts fetched,
   // [6] selections, [7] ms covering + fetching candidate counts, [8] fetches
-  // of the whole count array from a pop outside the candidates, [9] ms in pops
+  // of the whole count array from a pop outside the candidates, [9] ms in pops,
+  // [10] ms collecting candidates on the host, [11] candidate fetch rounds
   double sel_prof[12] = {0};
   // timing of sampler kernels (CUDA events on the context stream)
   double kernel_ms = 0.0;

@@ -104,25 +104,6 @@ void launch_pack_ic(const uint64_t *index, const float *w, uint32_t n,
   pack_ic_kernel<<<2368, 256, 0, stream>>>(src, w, m, pad4(m) + 4, edges);
 }
 
-// range[e] = (off[src_e], off[src_e + 1]): the in-edge range of edge e's
-// source, so an LT walk step that picks e can load the next vertex's in-edges
-// at once instead of first loading its offsets.
-__global__ void lt_range_kernel(const uint32_t *__restrict__ off,
-                                const uint2 *__restrict__ edges, uint64_t m, uint2 *range) {
-  for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < m;
-       e += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t u = edges[e].x;
-    range[e] = make_uint2(off[u], off[u + 1]);
-  }
-}
-
-void launch_lt_range(const uint32_t *off, const uint2 *edges, uint64_t m, uint2 *range,
-                     cudaStream_t stream) {
-  if (m == 0) return;
-  count_launches(1);
-  lt_range_kernel<<<2368, 256, 0, stream>>>(off, edges, m, range);
-}
-
 void launch_pack_lt(const uint64_t *index, const float *w, uint32_t n,
                     uint64_t m, uint32_t *off, uint2 *edges, const uint32_t *src,
                     cudaStream_t stream) {

@@ -173,10 +173,8 @@ __device__ __forceinline__ SetOutcome ic_plain_set(const DevGraph &G, Key key, u
 }
 
 // One LT set: the single-predecessor walk from root(s) (see lt_walk_kernel).
-// With the graph's per-edge source ranges a step has one dependent round
-// trip: the picked edge's lane also holds the next vertex's in-edge range, so
-// that vertex's edges (degree <= 32: all of them) are requested right after the
-// pick, while the visited-bit atomic of the pick is still in flight.
+// After a pick, the next vertex's offsets and (degree <= 32) its in-edges are
+// requested while the visited-bit atomic of the pick is still in flight.
 __device__ __forceinline__ SetOutcome lt_walk_set(const DevGraph &G, Key key, uint64_t s,
                                                   const WarpCtx &W) {
   const uint32_t lane = lane_id();
@@ -192,7 +190,7 @@ __device__ __forceinline__ SetOutcome lt_walk_set(const DevGraph &G, Key key, ui
   uint32_t lo = __ldg(G.off + cur), hi = __ldg(G.off + cur + 1);
   // the current vertex's in-edges when it has at most 32 (lane j: edge lo + j)
   bool have = false;
-  uint2 rec = make_uint2(0u, 0u), rng = make_uint2(0u, 0u);
+  uint2 rec = make_uint2(0u, 0u);
   for (;;) {
     set_exp += (lane == 0);
     if (hi == lo) break;
@@ -218,10 +216,7 @@ __device__ __forceinline__ SetOutcome lt_walk_set(const DevGraph &G, Key key, ui
       if (none) break;
       const uint32_t e = lo + lane;
       rec = make_uint2(0u, 0u);
-      if (e < hi) {
-        rec = __ldg(&G.edges[e]);
-        if (G.src_range) rng = __ldg(&G.src_range[e]);
-      }
+      if (e < hi) rec = __ldg(&G.edges[e]);
     }
     const uint32_t bal = __ballot_sync(FULL, lo + lane < hi && t < rec.y);
     set_edges += (lane == 0) ? (hi - lo) : 0;
@@ -231,23 +226,13 @@ __device__ __forceinline__ SetOutcome lt_walk_set(const DevGraph &G, Key key, ui
     uint32_t old = 0;
     const uint32_t bit = 1u << (u & 31);
     if (lane == 0) old = atomicOr(&W.bm[u >> 5], bit);
-    uint32_t lo2, hi2;
-    if (G.src_range) {
-      lo2 = __shfl_sync(FULL, rng.x, L);
-      hi2 = __shfl_sync(FULL, rng.y, L);
-    } else {
-      lo2 = __ldg(G.off + u);
-      hi2 = __ldg(G.off + u + 1);
-    }
+    const uint32_t lo2 = __ldg(G.off + u), hi2 = __ldg(G.off + u + 1);
     // u's in-edges, requested before the visited answer is consumed
-    have = G.src_range && hi2 - lo2 <= 32;
+    have = hi2 - lo2 <= 32;
     if (have) {
       const uint32_t e = lo2 + lane;
       rec = make_uint2(0u, 0u);
-      if (e < hi2) {
-        rec = __ldg(&G.edges[e]);
-        rng = __ldg(&G.src_range[e]);
-      }
+      if (e < hi2) rec = __ldg(&G.edges[e]);
     }
     const uint32_t seen = __shfl_sync(FULL, old & bit, 0);
     if (seen) break;

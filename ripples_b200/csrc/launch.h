@@ -153,8 +153,6 @@ void launch_weights(int kind, const uint64_t *index, uint32_t n, uint64_t seed, 
 void launch_pack_ic(const uint64_t *index, const float *w, uint32_t n,
                     uint64_t m, uint32_t *off, uint2 *edges, const uint32_t *src,
                     cudaStream_t stream);
-void launch_lt_range(const uint32_t *off, const uint2 *edges, uint64_t m, uint2 *range,
-                     cudaStream_t stream);
 void launch_pack_lt(const uint64_t *index, const float *w, uint32_t n,
                     uint64_t m, uint32_t *off, uint2 *edges, const uint32_t *src,
                     cudaStream_t stream);

@@ -70,7 +70,7 @@ struct rip_server {
   std::vector<SelSlot> slots;
   std::vector<int> free_slots;
   uint64_t admitted_bytes = 0;
-  uint64_t ticks = 0, completed = 0, graph_launches = 0;
+  uint64_t ticks = 0, completed = 0, graph_launches = 0, suspended = 0;
   double tick_ms = 0;
   std::map<rip_pool *, double> last_lb;  // per pool: LB of the last finished query
 };
@@ -272,6 +272,25 @@ void finish(rip_server *s, Active &a, int status) {
   if (a.slot >= 0) s->free_slots.push_back(a.slot);
 }
 
+// Takes an admitted query back to the end of the queue (it restarts from its
+// first round when admitted again) and frees its pool unless another admitted
+// query draws from it: the way out when every admitted query waits for memory.
+void suspend(rip_server *s, Active &a) {
+  s->admitted_bytes -= std::min(s->admitted_bytes, a.footprint);
+  if (a.slot >= 0) s->free_slots.push_back(a.slot);
+  s->queue.push_back({a.q, a.t_sub});
+  s->suspended++;
+  for (const Active &b : s->active)
+    if (&b != &a && b.pool == a.pool) return;
+  for (size_t i = 0; i < s->pools.size(); ++i)
+    if (s->pools[i].second == a.pool) {
+      s->last_lb.erase(a.pool);
+      rip_pool_destroy(a.pool);
+      s->pools.erase(s->pools.begin() + i);
+      return;
+    }
+}
+
 // Moves a query past the round just selected (imm.h:214-225 and :233-235).
 void advance(Active &a, double f) {
   if (a.phase == 0) {
@@ -415,7 +434,7 @@ extern "C" int rip_server_pending(const rip_server *s, uint32_t *active, uint32_
   return RIP_OK;
 }
 
-extern "C" int rip_server_stats(const rip_server *s, uint64_t out[6]) {
+extern "C" int rip_server_stats(const rip_server *s, uint64_t out[7]) {
   if (!s || !out) return RIP_ERR_INVALID;
   out[0] = s->ticks;
   out[1] = s->completed;
@@ -423,6 +442,7 @@ extern "C" int rip_server_stats(const rip_server *s, uint64_t out[6]) {
   out[3] = (uint64_t)s->pools.size();
   out[4] = s->admitted_bytes;
   out[5] = (uint64_t)(s->tick_ms * 1000.0);
+  out[6] = s->suspended;
   return RIP_OK;
 }
 
@@ -448,8 +468,17 @@ extern "C" int rip_server_tick(rip_server *s, uint32_t *completed) {
       ++done_now;
       continue;
     }
+    // admitted while its estimated footprint fits and the device is not
+    // already mostly in use; always when nothing else is admitted
+    const size_t in_use = c->used - std::min(c->used, c->cached);
+    if (!s->active.empty() && in_use > c->budget / 10 * 6) break;
     rip_pool *p = nullptr;
     TRY(pool_for(s, q->graph, q->seed, &p));
+    if (p->num_sets == 0) {  // a first slice of the pool measures its mean set size
+      const int r = rip_sample(p, q->seed, 256, RIP_SAMPLER_AUTO);
+      if (out_of_room(r) && !s->active.empty()) break;
+      if (r != RIP_OK && !out_of_room(r)) return r;
+    }
     const uint64_t fp = estimate_footprint(s, q, p);
     if (!s->active.empty() && s->admitted_bytes + fp > s->budget) break;
     s->queue.pop_front();
@@ -493,6 +522,33 @@ extern "C" int rip_server_tick(rip_server *s, uint32_t *completed) {
       need.push_back(0);
     }
     need[i] = std::max(need[i], a.S);
+  }
+  // A round whose pool would not fit the device even with nothing else on it
+  // ends its query now (RIP_ERR_LIMIT) instead of waiting for memory.
+  {
+    std::vector<Active> keep;
+    for (Active &a : s->active) {
+      const double per_set = mean_set_size(a.pool) * 8.0 + 13.0;
+      const double bytes = per_set * (double)a.S + (double)a.n * 24.0;
+      if (bytes > 0.9 * (double)c->budget) {
+        finish(s, a, RIP_ERR_LIMIT);
+        ++done_now;
+      } else {
+        keep.push_back(std::move(a));
+      }
+    }
+    s->active.swap(keep);
+    mp.clear();
+    need.clear();
+    for (Active &a : s->active) {
+      size_t i = 0;
+      while (i < mp.size() && mp[i] != a.pool) ++i;
+      if (i == mp.size()) {
+        mp.push_back(a.pool);
+        need.push_back(0);
+      }
+      need[i] = std::max(need[i], a.S);
+    }
   }
   std::vector<rip_pool *> sp;
   std::vector<uint64_t> sseed, scnt;
@@ -585,7 +641,7 @@ extern "C" int rip_server_tick(rip_server *s, uint32_t *completed) {
     fs[i] = a.S ? (double)cov / (double)a.S : 0.0;
   }
   // 5. martingale steps, completions.  When every admitted query waited for
-  // memory, nothing can free any: the one asking for the most sets ends.
+  // memory, the one asking for the most sets is suspended (or, alone, ends).
   bool progress = false;
   size_t worst = 0;
   for (size_t i = 0; i < s->active.size(); ++i) {
@@ -593,13 +649,18 @@ extern "C" int rip_server_tick(rip_server *s, uint32_t *completed) {
     if (s->active[i].S > s->active[worst].S) worst = i;
   }
   std::vector<Active> keep;
+  const size_t n_active = s->active.size();
   for (size_t i = 0; i < s->active.size(); ++i) {
     Active &a = s->active[i];
     if (a.stalled) {
       a.stalled = false;
       if (!progress && i == worst) {
-        finish(s, a, RIP_ERR_NOMEM);
-        ++done_now;
+        if (n_active > 1) {
+          suspend(s, a);  // frees memory for the others; it runs again later
+        } else {
+          finish(s, a, RIP_ERR_NOMEM);  // does not fit even alone
+          ++done_now;
+        }
       } else {
         keep.push_back(std::move(a));
       }

@@ -349,7 +349,7 @@ class Pool:
         out = np.zeros(12, dtype=np.float64)
         self._chk(lib.rip_select_profile(self.h, _ptr(out)), "rip_select_profile")
         keys = ["prep_ms", "heap_ms", "picks_ms", "pops", "seeds", "candidates", "selections",
-                "cover_fetch_ms", "full_fetches", "pop_ms"]
+                "cover_fetch_ms", "full_fetches", "pop_ms", "collect_ms", "fetch_rounds"]
         return dict(zip(keys, out.tolist()))
 
     def count(self, num_sets: Optional[int] = None) -> np.ndarray:
@@ -477,9 +477,10 @@ class Server:
         return a.value, qd.value
 
     def stats(self) -> dict:
-        out = np.zeros(6, dtype=np.uint64)
+        out = np.zeros(7, dtype=np.uint64)
         check(lib.rip_server_stats(self.h, _ptr(out)), "rip_server_stats", self.ctx.h)
-        keys = ("ticks", "completed", "graph_launches", "pools", "admitted_bytes", "tick_us")
+        keys = ("ticks", "completed", "graph_launches", "pools", "admitted_bytes", "tick_us",
+                "suspended")
         return {k: int(v) for k, v in zip(keys, out)}
 
     def drain(self) -> None:

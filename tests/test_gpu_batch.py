@@ -172,3 +172,28 @@ def test_autotune_picks_a_configuration_and_sets_stay_exact(ctx):
     lt = rb.DeviceGraph(ctx, lt_graph(11), "LT")
     assert lt.autotune(seed=1)["choice"] == 0
     lt.close()
+
+
+def test_server_suspends_under_memory_pressure_and_answers_stay_exact():
+    # a context whose budget fits one of these queries' pools at a time: the
+    # server must suspend one (its pool freed, restarted later) rather than
+    # fail it, and every answer must equal the query alone
+    small = rb.Context(0, hbm_budget=600 << 20)
+    g = lt_graph(16, 8, seed=31)
+    dg = rb.DeviceGraph(small, g, "LT")
+    specs = [(40, 0.12, 1), (30, 0.12, 2), (20, 0.2, 3)]
+    alone_res = []
+    for k, e, s in specs:
+        p = rb.Pool(dg)
+        seeds, rec = p.imm(k, e, seed=s, tiebreak=rb.TIE_LOWEST_ID)
+        alone_res.append((seeds.tolist(), rec.theta))
+        p.close()
+    srv = rb.Server(small, max_active=3)
+    qs = [srv.submit(rb.Query(dg, k, e, seed=s)) for k, e, s in specs]
+    srv.drain()
+    for q, (seeds, theta) in zip(qs, alone_res):
+        assert q.done and q.status == 0
+        assert q.seeds.tolist() == seeds and q.record.theta == theta
+    srv.close()
+    dg.close()
+    small.close()
