@@ -445,10 +445,15 @@ static int ensure_elems(rip_pool *p, uint64_t need) {
   return RIP_OK;
 }
 
-// Partitions the sampler scratch into `warps` x (bitmap + queue of qcap).
+// Partitions the sampler scratch into `warps` x (bitmap + queue of qcap).  LT
+// walks need no bitmap (revisits are found in the queue).
+static uint64_t scratch_bm_words(const rip_pool *p) {
+  return p->g->model == RIP_MODEL_LT ? 0 : (((uint64_t)p->g->n + 31) / 32 + 7) & ~7ull;
+}
+
 static int ensure_scratch(rip_pool *p, uint32_t warps, uint32_t qcap) {
   rip_ctx *c = p->ctx;
-  const uint64_t bm_words = (((uint64_t)p->g->n + 31) / 32 + 7) & ~7ull;
+  const uint64_t bm_words = scratch_bm_words(p);
   const uint64_t per = bm_words * 4 + (uint64_t)qcap * 4;
   const uint64_t bytes = per * warps;
   if (p->scratch.p && p->bm_words == bm_words && p->qcap == qcap &&
@@ -456,7 +461,7 @@ static int ensure_scratch(rip_pool *p, uint32_t warps, uint32_t qcap) {
     return RIP_OK;
   TRY(dalloc(c, p->scratch, bytes));
   // bitmaps must start all-zero; queue contents are don't-care
-  CK(c, cudaMemsetAsync(p->scratch.p, 0, bytes, c->stream));
+  if (bm_words) CK(c, cudaMemsetAsync(p->scratch.p, 0, bm_words * 4 * warps, c->stream));
   p->bm_words = bm_words;
   p->qcap = qcap;
   p->warps = warps;
@@ -465,9 +470,10 @@ static int ensure_scratch(rip_pool *p, uint32_t warps, uint32_t qcap) {
 
 static uint32_t default_warps(rip_pool *p, uint32_t qcap) {
   rip_ctx *c = p->ctx;
-  const uint64_t bm_bytes = ((((uint64_t)p->g->n + 31) / 32 + 7) & ~7ull) * 4;
+  const uint64_t bm_bytes = scratch_bm_words(p) * 4;
   const uint64_t per = bm_bytes + (uint64_t)qcap * 4;
-  uint64_t want = (uint64_t)c->num_sms * 32;  // 32 resident warps per SM
+  // LT walks: 64 resident warps per SM (latency-bound chains); IC: 32
+  uint64_t want = (uint64_t)c->num_sms * (p->g->model == RIP_MODEL_LT ? 64 : 32);
   size_t avail = c->budget > c->used ? c->budget - c->used : 0;
   uint64_t fit = (avail / 4) / per;  // scratch gets at most a quarter
   uint64_t w = std::min<uint64_t>(want, std::max<uint64_t>(fit, 8));
@@ -1175,22 +1181,26 @@ struct AdoptedQueue : RefQueue {
 };
 
 // The vertices of every heap item keyed at least T (keys never grow
-// downwards, so subtrees whose root is keyed below T are skipped).  Returns
-// the count, or cap + 1 when more than cap items qualify.
+// downwards, so subtrees whose root is keyed below T are skipped).  Walked
+// breadth first: the children of a queued node are prefetched when it is
+// queued, so the random reads into the heap array overlap.  Returns the
+// count, or cap + 1 when more than cap items qualify.
 static uint32_t collect_at_least(const std::vector<HeapItem> &h, uint32_t T, uint32_t cap,
-                                 uint32_t *out, std::vector<uint32_t> &stack) {
+                                 uint32_t *out, std::vector<uint32_t> &queue) {
   const size_t len = h.size();
   uint32_t cnt = 0;
-  stack.clear();
-  if (len && h[0].second >= T) stack.push_back(0);
-  while (!stack.empty()) {
-    const size_t i = stack.back();
-    stack.pop_back();
+  queue.clear();
+  if (len && h[0].second >= T) queue.push_back(0);
+  for (size_t head = 0; head < queue.size(); ++head) {
+    const size_t i = queue[head];
     if (cnt == cap) return cap + 1;
     out[cnt++] = h[i].first;
     const size_t l = 2 * i + 1;
-    if (l < len && h[l].second >= T) stack.push_back((uint32_t)l);
-    if (l + 1 < len && h[l + 1].second >= T) stack.push_back((uint32_t)(l + 1));
+    for (size_t c = l; c < l + 2 && c < len; ++c)
+      if (h[c].second >= T) {
+        queue.push_back((uint32_t)c);
+        if (2 * c + 1 < len) __builtin_prefetch(&h[2 * c + 1]);
+      }
   }
   return cnt;
 }

@@ -43,7 +43,8 @@ struct WarpCtx {
 // warp's bitmap.  Returns true when the set was stored; on a pool overflow
 // the reservation's offset is recorded in *first_bad.
 __device__ bool store_set(const WarpCtx &W, uint32_t qlen, bool overflow, uint64_t s,
-                          const DevPool &P, unsigned long long *first_bad) {
+                          const DevPool &P, unsigned long long *first_bad,
+                          bool clear_bitmap = true) {
   const uint32_t lane = lane_id();
   bool stored = false;
   if (!overflow) {
@@ -61,15 +62,16 @@ __device__ bool store_set(const WarpCtx &W, uint32_t qlen, bool overflow, uint64
       atomicMin(first_bad, b);
     }
   }
-  for (uint32_t i = lane; i < qlen; i += 32) W.bm[W.q[i] >> 5] = 0u;
+  if (clear_bitmap)
+    for (uint32_t i = lane; i < qlen; i += 32) W.bm[W.q[i] >> 5] = 0u;
   __syncwarp();
   return stored;
 }
 
 __device__ bool finish_set(const WarpCtx &W, uint32_t qlen, bool overflow,
                            uint64_t s, uint32_t rel, const DevPool &P,
-                           const FailList &F, bool big = false) {
-  const bool stored = store_set(W, qlen, overflow, s, P, F.first_bad_base);
+                           const FailList &F, bool big = false, bool clear_bitmap = true) {
+  const bool stored = store_set(W, qlen, overflow, s, P, F.first_bad_base, clear_bitmap);
   if (!stored && lane_id() == 0) F.ids[atomicAdd(F.count, 1u)] = big ? (rel | FAIL_BIG) : rel;
   __syncwarp();
   return stored;
@@ -173,16 +175,16 @@ __device__ __forceinline__ SetOutcome ic_plain_set(const DevGraph &G, Key key, u
 }
 
 // One LT set: the single-predecessor walk from root(s) (see lt_walk_kernel).
-// After a pick, the next vertex's offsets and (degree <= 32) its in-edges are
-// requested while the visited-bit atomic of the pick is still in flight.
+// A revisit is found by scanning the walk so far (the warp's queue, 32
+// entries per load, L1-resident): walks are short (tens of steps), so this
+// costs less than a visited-bitmap atomic and needs no bitmap at all.  After a
+// pick, the next vertex's offsets and (degree <= 32) its in-edges are
+// requested before the scan.
 __device__ __forceinline__ SetOutcome lt_walk_set(const DevGraph &G, Key key, uint64_t s,
                                                   const WarpCtx &W) {
   const uint32_t lane = lane_id();
   uint32_t cur = root_of(key, s, G.n);
-  if (lane == 0) {
-    W.q[0] = cur;
-    atomicOr(&W.bm[cur >> 5], 1u << (cur & 31));
-  }
+  if (lane == 0) W.q[0] = cur;
   __syncwarp();
   uint32_t qlen = 1;
   bool overflow = false;
@@ -221,27 +223,27 @@ __device__ __forceinline__ SetOutcome lt_walk_set(const DevGraph &G, Key key, ui
     const uint32_t bal = __ballot_sync(FULL, lo + lane < hi && t < rec.y);
     set_edges += (lane == 0) ? (hi - lo) : 0;
     if (bal == 0) break;  // no in-edge picked: the walk ends here
-    const uint32_t L = __ffs(bal) - 1;
-    const uint32_t u = __shfl_sync(FULL, rec.x, L);
-    uint32_t old = 0;
-    const uint32_t bit = 1u << (u & 31);
-    if (lane == 0) old = atomicOr(&W.bm[u >> 5], bit);
+    const uint32_t u = __shfl_sync(FULL, rec.x, __ffs(bal) - 1);
     const uint32_t lo2 = __ldg(G.off + u), hi2 = __ldg(G.off + u + 1);
-    // u's in-edges, requested before the visited answer is consumed
+    // u's in-edges, requested before the revisit scan
     have = hi2 - lo2 <= 32;
     if (have) {
       const uint32_t e = lo2 + lane;
       rec = make_uint2(0u, 0u);
       if (e < hi2) rec = __ldg(&G.edges[e]);
     }
-    const uint32_t seen = __shfl_sync(FULL, old & bit, 0);
+    bool seen = false;
+    for (uint32_t b = 0; b < qlen && !seen; b += 32) {
+      const uint32_t j = b + lane;
+      seen = __any_sync(FULL, j < qlen && W.q[j] == u);
+    }
     if (seen) break;
     if (qlen + 1 > W.qcap) {
-      if (lane == 0) W.bm[u >> 5] = 0u;
       overflow = true;
       break;
     }
     if (lane == 0) W.q[qlen] = u;
+    __syncwarp();
     ++qlen;
     cur = u;
     lo = lo2;
@@ -295,11 +297,10 @@ ic_plain_kernel(DevGraph G, DevPool P, Key key, uint64_t first, uint32_t count,
 // One walk per warp.  Each step needs the chosen in-edge of the current
 // vertex: a 32-ary search over the cumulative thresholds (one probe per lane
 // per round, log32(in-degree) rounds), finishing with one 8-byte load per lane
-// so the lane that holds the pick also holds its source id.  The visited-bit
-// atomic of the picked vertex is issued before that vertex's offsets and
-// threshold are fetched, and its result is only consumed afterwards, so the
-// two round trips overlap.
-__global__ void __launch_bounds__(256)
+// so the lane that holds the pick also holds its source id.  Walks are chains
+// of dependent loads, so the kernel is bound to 32 registers for 64 resident
+// warps per SM (and the host launches that many walks in flight).
+__global__ void __launch_bounds__(256, 8)
 lt_walk_kernel(DevGraph G, DevPool P, Key key, uint64_t first, uint32_t count,
                const uint32_t *ids, unsigned int *next, uint32_t *bitmaps,
                uint64_t bm_words, uint32_t *queues, uint32_t qcap, FailList F,
@@ -317,7 +318,7 @@ lt_walk_kernel(DevGraph G, DevPool P, Key key, uint64_t first, uint32_t count,
     const uint32_t rel = ids ? ids[idx] : idx;
     const uint64_t s = first + rel;
     const SetOutcome o = lt_walk_set(G, key, s, W);
-    if (finish_set(W, o.qlen, o.overflow, s, rel, P, F)) {
+    if (finish_set(W, o.qlen, o.overflow, s, rel, P, F, false, false)) {
       n_sets += (lane == 0);
       n_elems += (lane == 0) ? o.qlen : 0;
       n_exp += o.exp;
@@ -383,7 +384,7 @@ multi_sample_kernel(MultiLaunch L) {
     const uint64_t s = D.first + rel;
     const SetOutcome o = D.model == RIP_MODEL_IC ? ic_plain_set(D.G, D.key, s, W, D.work_cap)
                                                  : lt_walk_set(D.G, D.key, s, W);
-    if (store_set(W, o.qlen, o.overflow, s, D.P, D.first_bad)) {
+    if (store_set(W, o.qlen, o.overflow, s, D.P, D.first_bad, D.model == RIP_MODEL_IC)) {
       n_sets += 1;
       n_elems += o.qlen;
       n_exp += o.exp;
