@@ -263,6 +263,8 @@ def main():
     ap.add_argument("--serve-deadline", type=float, default=240.0,
                     help="s1: seconds after which unfinished queries count as failed")
     ap.add_argument("--baseline-seconds", type=float, default=60.0)
+    ap.add_argument("--case-scale", type=int, default=0,
+                    help="profiling case of the p3 workload: R-MAT scale (default 24)")
     ap.add_argument("--sampler-case", type=int, default=0,
                     help="profiling case: one sampler launch of this many sets on the "
                          "workload's graph (after a 1024-set pilot launch); prints its "
@@ -469,9 +471,12 @@ def run_sampler_case(args, w, local):
     import torch
     import ripples_b200 as rb
     torch.cuda.set_device(local)
-    g = build_graph(w)
     ctx = rb.Context(local)
-    dg = rb.DeviceGraph(ctx, g, w["model"])
+    if w.get("kind") == "p3":  # weighted-cascade R-MAT, 32 draws per vertex
+        scale = args.case_scale or w["scale"]
+        dg = rb.DeviceGraph.rmat_on_device(ctx, scale, 32 << scale, "IC", rb.WEIGHTS_WC, seed=0)
+    else:
+        dg = rb.DeviceGraph(ctx, build_graph(w), w["model"])
     pool = rb.Pool(dg)
     pool.sample(1024, seed=5)
     ctx.sync()
@@ -482,7 +487,8 @@ def run_sampler_case(args, w, local):
     st = pool.stats() - st0
     km, _, _ = pool.timing()
     alg = alg_bytes_of(st)
-    print(json.dumps({"case": w["name"], "sets": args.sampler_case, "alg_bytes": alg,
+    print(json.dumps({"case": w["name"], "n": dg.n, "m": dg.m, "sets": args.sampler_case,
+                      "alg_bytes": alg,
                       "kernel_ms": km - km0, "gb_per_s": alg / ((km - km0) / 1e3) / 1e9,
                       "stats": [int(x) for x in st]}))
     pool.close()

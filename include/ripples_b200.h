@@ -334,8 +334,10 @@ int rip_server_pending(const rip_server *s, uint32_t *active, uint32_t *queued);
  * [4] admitted footprint bytes, [5] microseconds spent in ticks, [6] times a
  * query was suspended (every admitted query waited for memory: the largest
  * went back to the queue, its pool freed, to restart later).  A query ends
- * with RIP_ERR_NOMEM only when it does not fit even alone. */
-int rip_server_stats(const rip_server *s, uint64_t out[7]);
+ * with RIP_ERR_NOMEM only when it does not fit even alone.  [7] microseconds
+ * sampling, [8] building the pools' vertex -> sets indexes, [9] indexing plus
+ * selecting (host-timed, with the synchronisations they need). */
+int rip_server_stats(const rip_server *s, uint64_t out[10]);
 
 /* ---- sampling without allocation ------------------------------------------- */
 /* No counterpart in the reference.  A variant of rip_sample's one-set-per-warp

@@ -652,6 +652,20 @@ static int sample_giant(rip_pool *p, uint64_t seed, uint64_t first,
   std::vector<uint64_t> sid(MAXCOL);
   std::vector<uint32_t> sizes(MAXCOL);
   std::vector<unsigned long long> starts(MAXCOL);
+  // A batch left unfinished by an error would leave masks and level stamps
+  // set: every error return clears the whole state first.
+  struct Clear {
+    rip_ctx *c;
+    void *p;
+    size_t bytes;
+    bool armed = true;
+    ~Clear() {
+      if (armed) {
+        cudaMemsetAsync(p, 0, bytes, c->stream);
+        cudaStreamSynchronize(c->stream);
+      }
+    }
+  } clear_on_error{c, p->g_state.p, st_bytes};
   for (size_t b0 = 0; b0 < ids.size(); b0 += MAXCOL) {
     const uint32_t ncol = (uint32_t)std::min<size_t>(MAXCOL, ids.size() - b0);
     const int cw = ncol <= 64 ? 1 : ncol <= 128 ? 2 : 4;
@@ -705,6 +719,7 @@ static int sample_giant(rip_pool *p, uint64_t seed, uint64_t first,
     p->kernel_launches++;
     p->big_sets += ncol;
   }
+  clear_on_error.armed = false;
   return RIP_OK;
 }
 

@@ -71,8 +71,9 @@ struct rip_server {
   std::vector<int> free_slots;
   uint64_t admitted_bytes = 0;
   uint64_t ticks = 0, completed = 0, graph_launches = 0, suspended = 0;
-  double tick_ms = 0;
+  double tick_ms = 0, sample_ms = 0, index_ms = 0, select_ms = 0;
   std::map<rip_pool *, double> last_lb;  // per pool: LB of the last finished query
+  std::map<rip_pool *, uint64_t> last_use;  // per pool: last tick a query drew from it
 };
 
 namespace {
@@ -285,6 +286,7 @@ void suspend(rip_server *s, Active &a) {
   for (size_t i = 0; i < s->pools.size(); ++i)
     if (s->pools[i].second == a.pool) {
       s->last_lb.erase(a.pool);
+      s->last_use.erase(a.pool);
       rip_pool_destroy(a.pool);
       s->pools.erase(s->pools.begin() + i);
       return;
@@ -336,6 +338,7 @@ void evict_idle_pools(rip_server *s) {
       keep.push_back(e);
     } else {
       s->last_lb.erase(e.second);
+      s->last_use.erase(e.second);
       rip_pool_destroy(e.second);
     }
   }
@@ -343,6 +346,32 @@ void evict_idle_pools(rip_server *s) {
 }
 
 bool out_of_room(int rc) { return rc == RIP_ERR_NOMEM || rc == RIP_ERR_LIMIT; }
+
+// Device bytes held by live allocations (the block cache is reusable).
+size_t in_use(rip_ctx *c) { return c->used - std::min(c->used, c->cached); }
+
+// Frees idle pools, least recently used first, until the live allocations
+// are at most `target` bytes; returns whether that was reached.
+bool evict_lru_until(rip_server *s, size_t target) {
+  rip_ctx *c = s->c;
+  while (in_use(c) > target) {
+    int best = -1;
+    for (size_t i = 0; i < s->pools.size(); ++i) {
+      rip_pool *p = s->pools[i].second;
+      bool active = false;  // queued queries re-create a freed pool when admitted
+      for (const Active &a : s->active) active = active || a.pool == p;
+      if (active) continue;
+      if (best < 0 || s->last_use[p] < s->last_use[s->pools[best].second]) best = (int)i;
+    }
+    if (best < 0) return false;
+    rip_pool *p = s->pools[best].second;
+    s->last_lb.erase(p);
+    s->last_use.erase(p);
+    rip_pool_destroy(p);
+    s->pools.erase(s->pools.begin() + best);
+  }
+  return true;
+}
 
 }  // namespace
 
@@ -434,7 +463,7 @@ extern "C" int rip_server_pending(const rip_server *s, uint32_t *active, uint32_
   return RIP_OK;
 }
 
-extern "C" int rip_server_stats(const rip_server *s, uint64_t out[7]) {
+extern "C" int rip_server_stats(const rip_server *s, uint64_t out[10]) {
   if (!s || !out) return RIP_ERR_INVALID;
   out[0] = s->ticks;
   out[1] = s->completed;
@@ -443,6 +472,9 @@ extern "C" int rip_server_stats(const rip_server *s, uint64_t out[7]) {
   out[4] = s->admitted_bytes;
   out[5] = (uint64_t)(s->tick_ms * 1000.0);
   out[6] = s->suspended;
+  out[7] = (uint64_t)(s->sample_ms * 1000.0);
+  out[8] = (uint64_t)(s->index_ms * 1000.0);
+  out[9] = (uint64_t)(s->select_ms * 1000.0);
   return RIP_OK;
 }
 
@@ -469,9 +501,9 @@ extern "C" int rip_server_tick(rip_server *s, uint32_t *completed) {
       continue;
     }
     // admitted while its estimated footprint fits and the device is not
-    // already mostly in use; always when nothing else is admitted
-    const size_t in_use = c->used - std::min(c->used, c->cached);
-    if (!s->active.empty() && in_use > c->budget / 10 * 6) break;
+    // already mostly in use (idle pools are freed, least recently used first,
+    // to make room); always when nothing else is admitted
+    if (!s->active.empty() && !evict_lru_until(s, c->budget / 10 * 6)) break;
     rip_pool *p = nullptr;
     TRY(pool_for(s, q->graph, q->seed, &p));
     if (p->num_sets == 0) {  // a first slice of the pool measures its mean set size
@@ -502,6 +534,7 @@ extern "C" int rip_server_tick(rip_server *s, uint32_t *completed) {
     if (completed) *completed = done_now;
     return RIP_OK;
   }
+  for (Active &a : s->active) s->last_use[a.pool] = s->ticks + 1;
   // 2. this round's prefixes and the pools' shortfalls, sampled in one launch
   std::vector<rip_pool *> mp;
   std::vector<uint64_t> need;
@@ -588,6 +621,7 @@ extern "C" int rip_server_tick(rip_server *s, uint32_t *completed) {
     }
   }
   const double gen_ms = ms_since(t_gen);
+  s->sample_ms += gen_ms;
   for (Active &a : s->active) {
     a.t_round = clk::now();
     if (a.phase == 0 && a.R.num_rounds < RIP_MAX_ROUNDS)
@@ -595,6 +629,7 @@ extern "C" int rip_server_tick(rip_server *s, uint32_t *completed) {
     if (a.phase == 1) a.R.generate_ms = a.delta ? gen_ms : 0.0;
   }
   // 3. indexes, 4. selections
+  const auto t_idx = clk::now();
   bool any_dev = false;
   for (Active &a : s->active) {
     if (a.stalled || a.q->tiebreak != RIP_TIE_LOWEST_ID) continue;
@@ -617,6 +652,7 @@ extern "C" int rip_server_tick(rip_server *s, uint32_t *completed) {
       else TRY(r);
     }
     CK(c, cudaStreamSynchronize(c->stream));
+    s->index_ms += ms_since(t_idx);
     for (Active &a : s->active)
       if (!a.stalled && a.q->tiebreak == RIP_TIE_LOWEST_ID) TRY(launch_round(s, a));
   }
@@ -640,6 +676,7 @@ extern "C" int rip_server_tick(rip_server *s, uint32_t *completed) {
     for (uint64_t g : a.gains) cov += g;
     fs[i] = a.S ? (double)cov / (double)a.S : 0.0;
   }
+  s->select_ms += ms_since(t_idx);
   // 5. martingale steps, completions.  When every admitted query waited for
   // memory, the one asking for the most sets is suspended (or, alone, ends).
   bool progress = false;

@@ -477,10 +477,10 @@ class Server:
         return a.value, qd.value
 
     def stats(self) -> dict:
-        out = np.zeros(7, dtype=np.uint64)
+        out = np.zeros(10, dtype=np.uint64)
         check(lib.rip_server_stats(self.h, _ptr(out)), "rip_server_stats", self.ctx.h)
         keys = ("ticks", "completed", "graph_launches", "pools", "admitted_bytes", "tick_us",
-                "suspended")
+                "suspended", "sample_us", "index_us", "index_select_us")
         return {k: int(v) for k, v in zip(keys, out)}
 
     def drain(self) -> None:
