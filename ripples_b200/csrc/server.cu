@@ -33,7 +33,9 @@ struct SelSlot {
   PinnedMem h_desc, h_best;
   uint32_t nchunk_cap = 0, k_cap = 0;
   uint64_t s_cap = 0;
-  // captured rounds by k: (graph, kernel nodes), oldest first
+  // captured rounds by k: (graph, kernel nodes), oldest first.  Kernels read
+  // every buffer through the descriptor, but the final copy node holds the
+  // best / h_best addresses: reallocating those drops the captured rounds.
   std::vector<std::pair<uint32_t, std::pair<cudaGraphExec_t, uint64_t>>> execs;
 };
 constexpr size_t MAX_GRAPHS_PER_SLOT = 8;
@@ -136,6 +138,9 @@ int slot_buffers(rip_server *s, SelSlot &sl, uint32_t nchunks, uint64_t S, uint3
     sl.s_cap = sl.covered.bytes;
   }
   if (k > sl.k_cap) {
+    // the captured rounds copy best -> h_best through the old buffers: drop them
+    for (auto &e : sl.execs) cudaGraphExecDestroy(e.second.first);
+    sl.execs.clear();
     TRY(dalloc(c, sl.best, (size_t)k * 8));
     TRY(sl.h_best.ensure(c, (size_t)k * 8));
     sl.k_cap = k;

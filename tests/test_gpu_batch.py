@@ -197,3 +197,19 @@ def test_server_suspends_under_memory_pressure_and_answers_stay_exact():
     srv.close()
     dg.close()
     small.close()
+
+
+def test_server_slot_reuse_across_k(ctx, graphs):
+    # one slot serves k = 10, then a larger k (its buffers grow), then k = 10
+    # again: the round captured for the first k must not reuse the old buffers
+    hs, dev = graphs
+    srv = rb.Server(ctx, max_active=1)
+    specs = [("lt12", 10, 0.5, 1), ("lt12", 60, 0.5, 1), ("lt12", 10, 0.4, 1),
+             ("ic12", 10, 0.5, 0), ("ic12", 70, 0.5, 0), ("ic12", 10, 0.5, 0)]
+    qs = [srv.submit(rb.Query(dev[n], k, e, seed=s)) for n, k, e, s in specs]
+    srv.drain()
+    for (n, k, e, s), q in zip(specs, qs):
+        assert q.done and q.status == 0
+        ref, rec = alone(dev, n, k, e, s, rb.TIE_LOWEST_ID)
+        assert q.seeds.tolist() == ref.tolist(), (n, k, e)
+    srv.close()
