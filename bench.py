@@ -779,8 +779,9 @@ def run_serve(args, w, world, rank, local):
     makespan = time.perf_counter() - t0
     clk = clocks.stop()
     launches = int(rb._lib.lib.rip_kernel_launches() - launches0)
-    ok = [q for q in qs if q.status == 0]
-    lat = [1e3 * (sub_t[i] - arrivals[i]) + qs[i].latency_ms for i in range(N) if qs[i].status == 0]
+    ok = [q for q in qs if q.done and q.status == 0]
+    lat = [1e3 * (sub_t[i] - arrivals[i]) + qs[i].latency_ms for i in range(N)
+           if qs[i].done and qs[i].status == 0]
     st = srv.stats()
     srv.close()
     # plain path, one query at a time (fresh pool, one set per warp), on the
@@ -796,7 +797,7 @@ def run_serve(args, w, world, rank, local):
             seeds, rec = p.imm(s["k"], s["eps"], seed=3, tiebreak=rb.TIE_LOWEST_ID,
                                sampler=rb.SAMPLER_PLAIN)
             base_ok += 1
-            if qs[i].status == 0:
+            if qs[i].done and qs[i].status == 0:
                 same = same and np.array_equal(seeds, qs[i].seeds)
         except rb.RipError:
             pass

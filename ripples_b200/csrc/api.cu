@@ -375,10 +375,14 @@ extern "C" int rip_pool_destroy(rip_pool *p) {
                    &p->b_scratch, &p->b_ids,   &p->d_heap,
                    &p->g_state, &p->g_lists,   &p->g_col,
                    &p->s_cmax,  &p->s_dirty,   &p->s_best,   &p->s_desc,
+
                    &p->count,   &p->inv_off,   &p->inv_cur,  &p->inv,
                    &p->covered,
-                   &p->scan_sums, &p->sv_count, &p->sv_off, &p->sv_cur,
-                   &p->sv_inv,  &p->sv_sums};
+                   &p->scan_sums, &p->sv_count, &p->sv_cur, &p->sv_sums};
+  for (ServeSegment &g : p->sv_segs) {
+    dfree(c, g.off);
+    dfree(c, g.inv);
+  }
   for (DevMem *m : all) dfree(c, *m);
   if (p->heap_registered) cudaHostUnregister(p->heap_registered);
   erase_ptr(c->pools, p);
@@ -396,6 +400,11 @@ extern "C" int rip_pool_clear(rip_pool *p) {
   for (double &x : p->sel_prof) x = 0.0;
   p->kernel_launches = 0;
   p->have_last_counts = false;
+  for (ServeSegment &g : p->sv_segs) {
+    dfree(c, g.off);
+    dfree(c, g.inv);
+  }
+  p->sv_segs.clear();
   p->sv_sets = 0;
   return RIP_OK;
 }
@@ -1603,10 +1612,12 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
     TRY(dalloc(c, p->s_best, (size_t)k * 8 + 256));
     TRY(dalloc(c, p->s_desc, sizeof(SelDesc)));
     TRY(p->h_best.ensure(c, (size_t)k * 8));
-    SelDesc d;
+    SelDesc d{};
     d.P = p->view();
-    d.inv_off = ptr<uint64_t>(p->inv_off);
-    d.inv = ptr<uint32_t>(p->inv);
+    d.seg_off[0] = ptr<uint64_t>(p->inv_off);
+    d.seg_inv[0] = ptr<uint32_t>(p->inv);
+    d.seg_first[0] = 0;
+    d.nseg = 1;
     d.S = S;
     d.n = n;
     d.nchunks = nchunks;
@@ -1618,6 +1629,8 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
     d.covered = ptr<uint8_t>(p->covered);
     d.best = ptr<unsigned long long>(p->s_best);
     d.done_blocks = reinterpret_cast<unsigned int *>(ptr<uint8_t>(p->s_best) + (size_t)k * 8);
+    d.acc = reinterpret_cast<unsigned long long *>(ptr<uint8_t>(p->s_best) + (size_t)k * 8 + 64);
+    d.total_elems = P;
     CK(c, cudaMemcpyAsync(p->s_desc.p, &d, sizeof(d), cudaMemcpyHostToDevice, c->stream));
     const SelDesc *dd = ptr<SelDesc>(p->s_desc);
     const int pick_blocks = (int)std::max<uint32_t>(1, std::min<uint32_t>((nchunks + 7) / 8,

@@ -251,6 +251,11 @@ struct rip_graph {
   }
 };
 
+struct ServeSegment {
+  DevMem off, inv;  // off u64[n + 1], inv u32[]: set ids in [first, last)
+  uint64_t first = 0, last = 0;
+};
+
 struct PoolMeta {  // device-side bookkeeping block (one D2H reads it all)
   unsigned long long cursor;
   unsigned long long first_bad;
@@ -295,8 +300,10 @@ struct rip_pool {
   DevMem count, inv_off, inv_cur, inv, covered,
       scan_sums;
   // vertex -> sets index over sets [0, sv_sets), shared by the served
-  // queries drawing from this pool (each filters to its own prefix)
-  DevMem sv_count, sv_off, sv_cur, sv_inv, sv_sums;
+  // queries drawing from this pool (each filters to its own prefix): one
+  // segment per growth step, merged into one past SEL_MAX_SEGMENTS
+  std::vector<ServeSegment> sv_segs;
+  DevMem sv_count, sv_cur, sv_sums;  // build scratch
   uint64_t sv_sets = 0;
   std::vector<uint32_t> last_counts;
   bool last_counts_on_device = false;  // last_counts still in `count` only

@@ -93,7 +93,7 @@ count_kernel(DevPool P, uint64_t S, uint32_t *count) {
 }
 
 __global__ void __launch_bounds__(256)
-inverted_kernel(DevPool P, uint64_t S, uint64_t *cursor, uint32_t *inv) {
+inverted_kernel(DevPool P, uint64_t S, uint64_t *cursor, uint32_t *inv, uint64_t base) {
   const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   for (uint64_t wb = gw * 32; wb < S; wb += nw * 32) {
@@ -107,7 +107,7 @@ inverted_kernel(DevPool P, uint64_t S, uint64_t *cursor, uint32_t *inv) {
             b = atomicAdd((unsigned long long *)cursor + v,
                           (unsigned long long)__popc(peers));
           b = __shfl_sync(FULL, b, leader);
-          if (valid) inv[b + __popc(peers & lanemask_lt())] = (uint32_t)s;
+          if (valid) inv[b + __popc(peers & lanemask_lt())] = (uint32_t)(base + s);
         });
   }
 }
@@ -194,13 +194,19 @@ __global__ void __launch_bounds__(256) sel_init_kernel(const SelDesc *__restrict
   }
   for (uint64_t i = tid; i < d.nchunks; i += stride) d.dirty[i] = 1;
   for (uint64_t i = tid; i < d.k; i += stride) d.best[i] = 0ull;
-  if (tid == 0) *d.done_blocks = 0;
+  if (tid == 0) {
+    *d.done_blocks = 0;
+    d.acc[2] = d.keep_counts ? d.total_elems : 0ull;
+    d.acc[3] = d.S;  // sets still uncovered
+    d.acc[4] = 0ull;
+  }
 }
 
 __global__ void __launch_bounds__(256) sel_count_kernel(const SelDesc *__restrict__ dp) {
   const SelDesc d = *dp;
   const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  unsigned long long elems = 0;
   for (uint64_t wb = gw * 32; wb < d.S; wb += nw * 32) {
     for_each_element(
         d.P, wb, d.S, [](uint64_t i) { return i; },
@@ -208,8 +214,11 @@ __global__ void __launch_bounds__(256) sel_count_kernel(const SelDesc *__restric
           const uint32_t peers = __match_any_sync(FULL, v);
           if (valid && (__ffs(peers) - 1) == (int)lane_id())
             atomicAdd(d.count + v, (uint32_t)__popc(peers));
+          elems += valid ? 1 : 0;
         });
   }
+  elems = warp_sum_u64(elems);
+  if (lane_id() == 0 && elems) atomicAdd(d.acc + 2, elems);
 }
 
 // Pick i: refresh the dirty chunk maxima (one warp per chunk), then the last
@@ -260,33 +269,90 @@ __global__ void __launch_bounds__(256) sel_pick_kernel(const SelDesc *__restrict
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) b = umax64(b, s_red[w]);
     d.best[i] = b;
     *d.done_blocks = 0;
+    // how the cover of this pick runs: its g sets hold about g x the mean
+    // uncovered set size; when that outweighs the rest, recounting the rest
+    // is less work than decrementing (either way the counts are exact)
+    const unsigned long long g = b >> 32, left = d.acc[2], sets = d.acc[3];
+    const unsigned long long est = sets ? (unsigned long long)((double)g * (double)left /
+                                                               (double)sets)
+                                        : 0ull;
+    d.acc[4] = (est > (left > est ? left - est : 0ull) + d.n / 4) ? 1ull : 0ull;
+    d.acc[3] = sets > g ? sets - g : 0ull;
   }
 }
 
-// After pick i: one warp per set of the seed's inverted list that lies in
-// [0, S) and is still uncovered; members are decremented and their chunks
-// marked dirty.
+// After pick i: mark the seed's still-uncovered sets in [0, S) covered (every
+// index segment).  Decrement mode (the pick's choice in acc[4] = 0): one warp
+// per set decrements its members and marks their chunks dirty.  Recount
+// mode: the sets are only marked, every count is cleared and every chunk
+// marked dirty, and sel_recount_kernel counts the sets left.  Both subtract
+// the covered sets' elements from acc[2] (elements of uncovered sets).
 __global__ void __launch_bounds__(256) sel_cover_kernel(const SelDesc *__restrict__ dp,
                                                         uint32_t i) {
   const SelDesc d = *dp;
   const unsigned long long b = d.best[i];
   if ((b >> 32) == 0) return;
   const uint32_t v = ~(uint32_t)(b & 0xFFFFFFFFull);
+  const bool recount = d.acc[4] != 0ull;
+  const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t gw = tid >> 5, nw = stride >> 5;
+  const uint32_t lane = lane_id();
+  unsigned long long elems = 0;
+  if (recount) {
+    uint4 *c4 = reinterpret_cast<uint4 *>(d.count);
+    const uint64_t n4 = (uint64_t)d.nchunks * (SEL_CHUNK / 4);
+    for (uint64_t x = tid; x < n4; x += stride) c4[x] = make_uint4(0, 0, 0, 0);
+    for (uint64_t x = tid; x < d.nchunks; x += stride) d.dirty[x] = 1;
+  }
+  for (uint32_t g = 0; g < d.nseg; ++g) {
+    if (d.seg_first[g] >= d.S) continue;  // the segment's sets are all >= S
+    const uint64_t lo = d.seg_off[g][v], hi = d.seg_off[g][v + 1];
+    if (recount) {  // one thread per entry: mark only
+      for (uint64_t j = lo + tid; j < hi; j += stride) {
+        const uint32_t s = d.seg_inv[g][j];
+        if (s < d.S && !d.covered[s]) {  // s holds v once: no other thread has s
+          d.covered[s] = 1;
+          elems += d.P.set_len[s];
+        }
+      }
+      continue;
+    }
+    for (uint64_t j = lo + gw; j < hi; j += nw) {  // one warp per entry
+      const uint32_t s = d.seg_inv[g][j];
+      if (s >= d.S || d.covered[s]) continue;  // warp-uniform
+      const uint32_t len = d.P.set_len[s];
+      const uint64_t so = d.P.set_off[s];
+      if (lane == 0) {
+        d.covered[s] = 1;
+        elems += len;
+      }
+      for (uint32_t e = lane; e < len; e += 32) {
+        const uint32_t u = d.P.vtx[so + e];
+        atomicSub(d.count + u, 1u);
+        d.dirty[u / SEL_CHUNK] = 1;
+      }
+    }
+  }
+  elems = warp_sum_u64(elems);
+  if (lane == 0 && elems) atomicAdd(d.acc + 2, (unsigned long long)0 - elems);  // acc[2] -= elems
+}
+
+// Recount mode only: count the members of every set in [0, S) still
+// uncovered.
+__global__ void __launch_bounds__(256) sel_recount_kernel(const SelDesc *__restrict__ dp) {
+  const SelDesc d = *dp;
+  if (d.acc[4] == 0ull) return;
   const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  const uint32_t lane = lane_id();
-  const uint64_t lo = d.inv_off[v], hi = d.inv_off[v + 1];
-  for (uint64_t j = lo + gw; j < hi; j += nw) {
-    const uint32_t s = d.inv[j];
-    if (s >= d.S || d.covered[s]) continue;  // warp-uniform
-    const uint32_t len = d.P.set_len[s];
-    const uint64_t off = d.P.set_off[s];
-    if (lane == 0) d.covered[s] = 1;  // s holds v once: no other warp has s
-    for (uint32_t e = lane; e < len; e += 32) {
-      const uint32_t u = d.P.vtx[off + e];
-      atomicSub(d.count + u, 1u);
-      d.dirty[u / SEL_CHUNK] = 1;
-    }
+  for (uint64_t wb = gw * 32; wb < d.S; wb += nw * 32) {
+    for_each_element(
+        d.P, wb, d.S, [&](uint64_t x) { return d.covered[x] ? ~0ull : x; },
+        [&](uint64_t, uint32_t v, bool valid) {
+          const uint32_t peers = __match_any_sync(FULL, v);
+          if (valid && (__ffs(peers) - 1) == (int)lane_id())
+            atomicAdd(d.count + v, (uint32_t)__popc(peers));
+        });
   }
 }
 
@@ -469,9 +535,9 @@ void launch_exclusive_scan(const uint32_t *in, uint64_t *out, uint32_t n,
 
 void launch_build_inverted(const DevPool &P, uint64_t num_sets,
                            uint64_t *cursor, uint32_t *inv, int blocks,
-                           cudaStream_t stream) {
+                           cudaStream_t stream, uint64_t base) {
   count_launches(1);
-  inverted_kernel<<<blocks, 256, 0, stream>>>(P, num_sets, cursor, inv);
+  inverted_kernel<<<blocks, 256, 0, stream>>>(P, num_sets, cursor, inv, base);
 }
 
 void launch_cover(const CoverLaunch &C, cudaStream_t stream) {
@@ -492,8 +558,9 @@ void launch_sel_pick(const SelDesc *d, uint32_t i, int blocks, cudaStream_t stre
   sel_pick_kernel<<<blocks, 256, 0, stream>>>(d, i);
 }
 void launch_sel_cover(const SelDesc *d, uint32_t i, int blocks, cudaStream_t stream) {
-  count_launches(1);
+  count_launches(2);
   sel_cover_kernel<<<blocks, 256, 0, stream>>>(d, i);
+  sel_recount_kernel<<<blocks, 256, 0, stream>>>(d);
 }
 uint32_t sel_chunk_vertices() { return SEL_CHUNK; }
 

@@ -163,9 +163,10 @@ void launch_count(const DevPool &P, uint64_t num_sets, uint32_t *count,
 void launch_exclusive_scan(const uint32_t *in, uint64_t *out, uint32_t n,
                            uint64_t *block_sums, cudaStream_t stream);
 size_t scan_block_sums_needed(uint32_t n);
+// inv receives base + (set index in P) for every element of sets [0, num_sets)
 void launch_build_inverted(const DevPool &P, uint64_t num_sets,
                            uint64_t *cursor, uint32_t *inv, int blocks,
-                           cudaStream_t stream);
+                           cudaStream_t stream, uint64_t base = 0);
 struct CoverLaunch {
   DevPool P;
   const uint64_t *inv_off;
@@ -189,10 +190,16 @@ void launch_argmax(const uint32_t *count, uint32_t n, unsigned long long *best,
                    int blocks, cudaStream_t stream);
 
 // Device-only lowest-id picks of one served query (lives in device memory).
+constexpr uint32_t SEL_MAX_SEGMENTS = 8;
 struct SelDesc {
   DevPool P;                       // the pool the query draws from
-  const uint64_t *inv_off;         // vertex -> sets index over the pool's sets
-  const uint32_t *inv;
+  // vertex -> sets index of the pool, as up to SEL_MAX_SEGMENTS segments, each
+  // over a range of set ids [seg_first[g], ...): v's sets in segment g are
+  // seg_inv[g][seg_off[g][v] .. seg_off[g][v + 1])
+  const uint64_t *seg_off[SEL_MAX_SEGMENTS];
+  const uint32_t *seg_inv[SEL_MAX_SEGMENTS];
+  uint64_t seg_first[SEL_MAX_SEGMENTS];
+  uint32_t nseg;
   uint64_t S;                      // select over sets [0, S)
   uint32_t n, nchunks;             // vertices; chunks of sel_chunk_vertices()
   uint32_t k;                      // picks
@@ -203,10 +210,17 @@ struct SelDesc {
   uint8_t *covered;                // >= S rounded up to 16 bytes
   unsigned long long *best;        // k keys: count << 32 | ~vertex
   unsigned int *done_blocks;       // last-block counter of sel_pick
+  unsigned long long *acc;         // [2] elements of the sets still uncovered,
+                                   // [3] sets still uncovered, [4] cover mode
+                                   // of the current pick (1 = recount)
+  uint64_t total_elems;            // elements of sets [0, S) (keep_counts)
 };
 void launch_sel_init(const SelDesc *d, int blocks, cudaStream_t stream);
 void launch_sel_count(const SelDesc *d, int blocks, cudaStream_t stream);
 void launch_sel_pick(const SelDesc *d, uint32_t i, int blocks, cudaStream_t stream);
+// Covers pick i's sets: marks them and decrements their members' counts or --
+// when they hold more elements than every set still uncovered -- recounts the
+// uncovered sets (2 launches; the pick decides which, on the device).
 void launch_sel_cover(const SelDesc *d, uint32_t i, int blocks, cudaStream_t stream);
 uint32_t sel_chunk_vertices();
 // out[i] = count[ids[i]], i < m

@@ -75,7 +75,6 @@ struct rip_server {
   uint64_t ticks = 0, completed = 0, graph_launches = 0, suspended = 0;
   double tick_ms = 0, sample_ms = 0, index_ms = 0, select_ms = 0;
   std::map<rip_pool *, double> last_lb;  // per pool: LB of the last finished query
-  std::map<rip_pool *, uint64_t> last_use;  // per pool: last tick a query drew from it
 };
 
 namespace {
@@ -134,8 +133,9 @@ int slot_buffers(rip_server *s, SelSlot &sl, uint32_t nchunks, uint64_t S, uint3
   }
   const uint64_t sb = ((S + 15) & ~15ull) + 16;
   if (sb > sl.s_cap) {
-    TRY(dalloc(c, sl.covered, std::max<uint64_t>(sb, sl.s_cap * 3 / 2)));
-    sl.s_cap = sl.covered.bytes;
+    const uint64_t cap = std::max<uint64_t>(sb, sl.s_cap * 3 / 2);
+    TRY(dalloc(c, sl.covered, cap));
+    sl.s_cap = cap;
   }
   if (k > sl.k_cap) {
     // the captured rounds copy best -> h_best through the old buffers: drop them
@@ -148,31 +148,54 @@ int slot_buffers(rip_server *s, SelSlot &sl, uint32_t nchunks, uint64_t S, uint3
   return RIP_OK;
 }
 
-// The vertex -> sets index of a pool over all the sets it holds.
+// The vertex -> sets index of a pool over all the sets it holds: the sets
+// added since the last call get a segment of their own (count, scan and
+// scatter over that range only); past SEL_MAX_SEGMENTS segments everything
+// is re-indexed as one.
 int extend_index(rip_pool *p) {
   rip_ctx *c = p->ctx;
   if (p->sv_sets == p->num_sets) return RIP_OK;
+  if (p->sv_segs.size() == SEL_MAX_SEGMENTS) {
+    for (ServeSegment &g : p->sv_segs) {
+      dfree(c, g.off);
+      dfree(c, g.inv);
+    }
+    p->sv_segs.clear();
+    p->sv_sets = 0;
+  }
   const uint32_t n = p->g->n;
-  const uint64_t S = p->num_sets;
+  const uint64_t first = p->sv_sets, S = p->num_sets - first;
+  // the pool viewed from set `first` on: set_off / set_len shifted
+  DevPool view = p->view();
+  view.set_off += first;
+  view.set_len += first;
+  ServeSegment seg;
+  seg.first = first;
+  seg.last = p->num_sets;
   TRY(dalloc(c, p->sv_count, sizeof(uint32_t) * (size_t)n));
   CK(c, cudaMemsetAsync(p->sv_count.p, 0, sizeof(uint32_t) * (size_t)n, c->stream));
-  launch_count(p->view(), S, ptr<uint32_t>(p->sv_count), c->num_sms * 8, c->stream);
-  TRY(dalloc(c, p->sv_off, sizeof(uint64_t) * ((size_t)n + 1)));
+  launch_count(view, S, ptr<uint32_t>(p->sv_count), c->num_sms * 8, c->stream);
+  TRY(dalloc(c, seg.off, sizeof(uint64_t) * ((size_t)n + 1)));
   TRY(dalloc(c, p->sv_cur, sizeof(uint64_t) * ((size_t)n + 1)));
   TRY(dalloc(c, p->sv_sums, sizeof(uint64_t) * scan_block_sums_needed(n)));
-  launch_exclusive_scan(ptr<uint32_t>(p->sv_count), ptr<uint64_t>(p->sv_off), n,
+  launch_exclusive_scan(ptr<uint32_t>(p->sv_count), ptr<uint64_t>(seg.off), n,
                         ptr<uint64_t>(p->sv_sums), c->stream);
   uint64_t P = 0;
-  CK(c, cudaMemcpyAsync(&P, ptr<uint64_t>(p->sv_off) + n, sizeof(uint64_t),
+  CK(c, cudaMemcpyAsync(&P, ptr<uint64_t>(seg.off) + n, sizeof(uint64_t),
                         cudaMemcpyDeviceToHost, c->stream));
-  CK(c, cudaMemcpyAsync(p->sv_cur.p, p->sv_off.p, sizeof(uint64_t) * ((size_t)n + 1),
+  CK(c, cudaMemcpyAsync(p->sv_cur.p, seg.off.p, sizeof(uint64_t) * ((size_t)n + 1),
                         cudaMemcpyDeviceToDevice, c->stream));
   CK(c, cudaStreamSynchronize(c->stream));
-  TRY(dalloc(c, p->sv_inv, sizeof(uint32_t) * std::max<uint64_t>(P, 1)));
-  launch_build_inverted(p->view(), S, ptr<uint64_t>(p->sv_cur), ptr<uint32_t>(p->sv_inv),
-                        c->num_sms * 8, c->stream);
+  int rc = dalloc(c, seg.inv, sizeof(uint32_t) * std::max<uint64_t>(P, 1));
+  if (rc != RIP_OK) {
+    dfree(c, seg.off);
+    return rc;
+  }
+  launch_build_inverted(view, S, ptr<uint64_t>(p->sv_cur), ptr<uint32_t>(seg.inv),
+                        c->num_sms * 8, c->stream, first);
   CK(c, cudaGetLastError());
-  p->sv_sets = S;
+  p->sv_segs.push_back(seg);
+  p->sv_sets = p->num_sets;
   return RIP_OK;
 }
 
@@ -187,8 +210,12 @@ int launch_round(rip_server *s, Active &a) {
   const uint32_t k = a.q->k;
   SelDesc *hd = static_cast<SelDesc *>(sl.h_desc.p);
   hd->P = p->view();
-  hd->inv_off = ptr<uint64_t>(p->sv_off);
-  hd->inv = ptr<uint32_t>(p->sv_inv);
+  hd->nseg = (uint32_t)p->sv_segs.size();
+  for (uint32_t g = 0; g < hd->nseg; ++g) {
+    hd->seg_off[g] = ptr<uint64_t>(p->sv_segs[g].off);
+    hd->seg_inv[g] = ptr<uint32_t>(p->sv_segs[g].inv);
+    hd->seg_first[g] = p->sv_segs[g].first;
+  }
   hd->S = a.S;
   hd->n = (uint32_t)a.n;
   hd->nchunks = nchunks;
@@ -200,6 +227,8 @@ int launch_round(rip_server *s, Active &a) {
   hd->covered = ptr<uint8_t>(sl.covered);
   hd->best = ptr<unsigned long long>(sl.best);
   hd->done_blocks = ptr<unsigned int>(sl.ctr);
+  hd->acc = reinterpret_cast<unsigned long long *>(ptr<uint8_t>(sl.ctr) + 64);
+  hd->total_elems = 0;
   CK(c, cudaMemcpyAsync(sl.desc.p, hd, sizeof(SelDesc), cudaMemcpyHostToDevice, sl.st));
   size_t gi = 0;
   while (gi < sl.execs.size() && sl.execs[gi].first != k) ++gi;
@@ -291,7 +320,6 @@ void suspend(rip_server *s, Active &a) {
   for (size_t i = 0; i < s->pools.size(); ++i)
     if (s->pools[i].second == a.pool) {
       s->last_lb.erase(a.pool);
-      s->last_use.erase(a.pool);
       rip_pool_destroy(a.pool);
       s->pools.erase(s->pools.begin() + i);
       return;
@@ -328,14 +356,11 @@ void advance(Active &a, double f) {
 bool pool_in_use(rip_server *s, rip_pool *p) {
   for (Active &a : s->active)
     if (a.pool == p) return true;
-  for (auto &e : s->pools)
-    if (e.second == p)
-      for (auto &q : s->queue)
-        if (q.first->graph == e.first.first && q.first->seed == e.first.second) return true;
   return false;
 }
 
-// Frees the pools no admitted or queued query draws from.
+// Frees the pools no admitted query draws from (a queued query re-creates
+// its pool when admitted): called only when a pool cannot grow.
 void evict_idle_pools(rip_server *s) {
   std::vector<std::pair<std::pair<rip_graph *, uint64_t>, rip_pool *>> keep;
   for (auto &e : s->pools) {
@@ -343,7 +368,6 @@ void evict_idle_pools(rip_server *s) {
       keep.push_back(e);
     } else {
       s->last_lb.erase(e.second);
-      s->last_use.erase(e.second);
       rip_pool_destroy(e.second);
     }
   }
@@ -354,29 +378,6 @@ bool out_of_room(int rc) { return rc == RIP_ERR_NOMEM || rc == RIP_ERR_LIMIT; }
 
 // Device bytes held by live allocations (the block cache is reusable).
 size_t in_use(rip_ctx *c) { return c->used - std::min(c->used, c->cached); }
-
-// Frees idle pools, least recently used first, until the live allocations
-// are at most `target` bytes; returns whether that was reached.
-bool evict_lru_until(rip_server *s, size_t target) {
-  rip_ctx *c = s->c;
-  while (in_use(c) > target) {
-    int best = -1;
-    for (size_t i = 0; i < s->pools.size(); ++i) {
-      rip_pool *p = s->pools[i].second;
-      bool active = false;  // queued queries re-create a freed pool when admitted
-      for (const Active &a : s->active) active = active || a.pool == p;
-      if (active) continue;
-      if (best < 0 || s->last_use[p] < s->last_use[s->pools[best].second]) best = (int)i;
-    }
-    if (best < 0) return false;
-    rip_pool *p = s->pools[best].second;
-    s->last_lb.erase(p);
-    s->last_use.erase(p);
-    rip_pool_destroy(p);
-    s->pools.erase(s->pools.begin() + best);
-  }
-  return true;
-}
 
 }  // namespace
 
@@ -506,9 +507,9 @@ extern "C" int rip_server_tick(rip_server *s, uint32_t *completed) {
       continue;
     }
     // admitted while its estimated footprint fits and the device is not
-    // already mostly in use (idle pools are freed, least recently used first,
-    // to make room); always when nothing else is admitted
-    if (!s->active.empty() && !evict_lru_until(s, c->budget / 10 * 6)) break;
+    // already mostly in use (resident pools stay: later queries reuse them);
+    // always when nothing else is admitted
+    if (!s->active.empty() && in_use(c) > c->budget / 20 * 17) break;
     rip_pool *p = nullptr;
     TRY(pool_for(s, q->graph, q->seed, &p));
     if (p->num_sets == 0) {  // a first slice of the pool measures its mean set size
@@ -539,7 +540,6 @@ extern "C" int rip_server_tick(rip_server *s, uint32_t *completed) {
     if (completed) *completed = done_now;
     return RIP_OK;
   }
-  for (Active &a : s->active) s->last_use[a.pool] = s->ticks + 1;
   // 2. this round's prefixes and the pools' shortfalls, sampled in one launch
   std::vector<rip_pool *> mp;
   std::vector<uint64_t> need;
@@ -567,7 +567,7 @@ extern "C" int rip_server_tick(rip_server *s, uint32_t *completed) {
     std::vector<Active> keep;
     for (Active &a : s->active) {
       const double per_set = mean_set_size(a.pool) * 8.0 + 13.0;
-      const double bytes = per_set * (double)a.S + (double)a.n * 24.0;
+      const double bytes = per_set * (double)a.S + (double)a.n * 96.0;
       if (bytes > 0.9 * (double)c->budget) {
         finish(s, a, RIP_ERR_LIMIT);
         ++done_now;

@@ -213,3 +213,20 @@ def test_server_slot_reuse_across_k(ctx, graphs):
         ref, rec = alone(dev, n, k, e, s, rb.TIE_LOWEST_ID)
         assert q.seeds.tolist() == ref.tolist(), (n, k, e)
     srv.close()
+
+
+def test_server_index_segments_and_merge(ctx, graphs):
+    # one pool grown by many later queries in turn (each needs more sets than
+    # the last): its vertex -> sets index gains a segment per growth step and
+    # is merged back into one past the segment limit; answers stay exact
+    hs, dev = graphs
+    srv = rb.Server(ctx, max_active=1)
+    specs = [("lt13", 5 + 4 * i, 0.5 - 0.03 * i, 7) for i in range(12)]
+    qs = [srv.submit(rb.Query(dev[n], k, e, seed=s)) for n, k, e, s in specs]
+    srv.drain()
+    for (n, k, e, s), q in zip(specs, qs):
+        assert q.done and q.status == 0
+        ref, rec = alone(dev, n, k, e, s, rb.TIE_LOWEST_ID)
+        assert q.seeds.tolist() == ref.tolist(), (k, e)
+        assert q.record.theta == rec.theta
+    srv.close()
