@@ -136,30 +136,42 @@ def dist_setup():
     return world, rank, local
 
 
-def allreduce_max(x, world):
+def _reduce(x, world, op_name):
+    """One float reduced over the ranks (NCCL on GPUs, gloo on CPU)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=getattr(dist.ReduceOp, op_name))
     return float(t.item())
+
+
+def allreduce_max(x, world):
+    return _reduce(x, world, "MAX")
 
 
 def allreduce_sum(x, world):
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    return _reduce(x, world, "SUM")
 
 
 def barrier(world):
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
+
+
+def replica_seed(rank, step):
+    """Sampler seed of a replica's step: ranks run independent IMM queries."""
+    return 1000003 * (rank + 1) + step
+
+
+def aggregate(sets, elapsed_ms, world):
+    """Whole-job throughput of the replicas: every rank's sets over the
+    slowest rank's device time."""
+    t_max = allreduce_max(elapsed_ms, world)
+    return allreduce_sum(sets, world) / (t_max / 1e3), t_max
 
 
 def run_reference_imm(bin_path, w, threads, parallel, timeout_s):
@@ -300,7 +312,7 @@ def main():
     stream = torch.cuda.ExternalStream(sp.value, device=torch.device("cuda", local))
     dg = rb.DeviceGraph(ctx, g, w["model"])
     pool = rb.Pool(dg)
-    seed_base = 1000003 * (rank + 1)
+    seed_base = replica_seed(rank, 0)
 
     def one_step(step):
         pool.clear()
@@ -342,9 +354,7 @@ def main():
     clk = clocks.stop()
     launches = int(rb._lib.lib.rip_kernel_launches() - launches0)
     elapsed_ms = ev0.elapsed_time(ev1)
-    t_max = allreduce_max(elapsed_ms, world)
-    sets_all = allreduce_sum(total_sets, world)
-    value = sets_all / (t_max / 1e3)
+    value, t_max = aggregate(total_sets, elapsed_ms, world)
 
     # ---- the same IMM runs with the reference GPU path's tie-break ---------
     # (lowest vertex id among equal counts, thrust::max_element): every pick
