@@ -385,6 +385,7 @@ extern "C" int rip_pool_destroy(rip_pool *p) {
   }
   for (DevMem *m : all) dfree(c, *m);
   if (p->heap_registered) cudaHostUnregister(p->heap_registered);
+  if (p->sel_graph.exec) cudaGraphExecDestroy(p->sel_graph.exec);
   erase_ptr(c->pools, p);
   delete p;
   return RIP_OK;
@@ -1635,14 +1636,46 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
     const SelDesc *dd = ptr<SelDesc>(p->s_desc);
     const int pick_blocks = (int)std::max<uint32_t>(1, std::min<uint32_t>((nchunks + 7) / 8,
                                                                           c->num_sms * 4));
-    launch_sel_init(dd, c->num_sms, c->stream);
-    for (uint32_t i = 0; i < k; ++i) {
-      launch_sel_pick(dd, i, pick_blocks, c->stream);
-      if (i + 1 < k) launch_sel_cover(dd, i, max_blocks, c->stream);
+    // The pick loop runs as one CUDA graph, captured once per (k, buffers):
+    // kernels read everything through the descriptor; the final copy node
+    // holds the best / h_best addresses, so moving those drops the graph.
+    SelGraph &sg = p->sel_graph;
+    if (sg.exec && (sg.k != k || sg.src != p->s_best.p || sg.dst != p->h_best.p ||
+                    sg.desc != p->s_desc.p || sg.pick_blocks != pick_blocks)) {
+      cudaGraphExecDestroy(sg.exec);
+      sg.exec = nullptr;
     }
-    CK(c, cudaGetLastError());
-    CK(c, cudaMemcpyAsync(p->h_best.p, p->s_best.p, (size_t)k * 8, cudaMemcpyDeviceToHost,
-                          c->stream));
+    if (!sg.exec) {
+      const uint64_t before = launch_counter();
+      cudaGraph_t graph = nullptr;
+      CK(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+      launch_sel_init(dd, c->num_sms, c->stream);
+      for (uint32_t i = 0; i < k; ++i) {
+        launch_sel_pick(dd, i, pick_blocks, c->stream);
+        if (i + 1 < k) launch_sel_cover(dd, i, max_blocks, c->stream);
+      }
+      cudaMemcpyAsync(p->h_best.p, p->s_best.p, (size_t)k * 8, cudaMemcpyDeviceToHost,
+                      c->stream);
+      const cudaError_t ce = cudaStreamEndCapture(c->stream, &graph);
+      sg.nodes = launch_counter() - before;
+      uncount_launches(sg.nodes);
+      if (ce != cudaSuccess)
+        return set_err(c, RIP_ERR_CUDA, "pick graph capture failed: %s", cudaGetErrorString(ce));
+      const cudaError_t ie = cudaGraphInstantiate(&sg.exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (ie != cudaSuccess) {
+        sg.exec = nullptr;
+        return set_err(c, RIP_ERR_CUDA, "pick graph instantiate failed: %s",
+                       cudaGetErrorString(ie));
+      }
+      sg.k = k;
+      sg.src = p->s_best.p;
+      sg.dst = p->h_best.p;
+      sg.desc = p->s_desc.p;
+      sg.pick_blocks = pick_blocks;
+    }
+    CK(c, cudaGraphLaunch(sg.exec, c->stream));
+    count_launches(sg.nodes);
     CK(c, cudaStreamSynchronize(c->stream));
     const unsigned long long *hb8 = static_cast<const unsigned long long *>(p->h_best.p);
     for (uint32_t i = 0; i < k && uncovered != 0; ++i) {

@@ -251,6 +251,15 @@ struct rip_graph {
   }
 };
 
+// A captured lowest-id pick loop and the addresses it was captured with.
+struct SelGraph {
+  cudaGraphExec_t exec = nullptr;
+  uint32_t k = 0;
+  int pick_blocks = 0;
+  void *src = nullptr, *dst = nullptr, *desc = nullptr;
+  uint64_t nodes = 0;
+};
+
 struct ServeSegment {
   DevMem off, inv;  // off u64[n + 1], inv u32[]: set ids in [first, last)
   uint64_t first = 0, last = 0;
@@ -315,6 +324,7 @@ struct rip_pool {
   DevMem d_heap;                     // heap built on the device
   DevMem s_cmax, s_dirty, s_best, s_desc;  // device lowest-id picks
   PinnedMem h_best;
+  SelGraph sel_graph;                // the captured pick loop
   // selection profile: [0] count+index kernels and counts D2H, [1] heap build,
   // [2] pick loop, [3] heap pops, [4] picks, [5] candidate counts fetched,
   // [6] selections, [7] ms covering + fetching candidate counts, [8] fetches
