@@ -56,7 +56,7 @@ int rip_ctx_destroy(rip_ctx *c) {
   dfree(c, c->m_scratch);
   dfree(c, c->m_table);
   dfree(c, c->m_fail);
-  delete c->h_pairs;
+  delete c->h_cand;
   delete c->h_count;
   delete c->h_meta;
   if (c->ev0) cudaEventDestroy(c->ev0);
@@ -1423,9 +1423,6 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
   CK(c, cudaGetLastError());
   TRY(dalloc(c, p->covered, std::max<uint64_t>(S, 1)));
   CK(c, cudaMemsetAsync(p->covered.p, 0, std::max<uint64_t>(S, 1), c->stream));
-  PoolMeta *dm = p->dmeta();
-  CK(c, cudaMemsetAsync(&dm->dirty_n, 0, sizeof(unsigned int), c->stream));
-  CK(c, cudaMemsetAsync(&dm->covered_sets, 0, sizeof(unsigned long long), c->stream));
 
   CoverLaunch C;
   C.P = p->view();
@@ -1433,21 +1430,17 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
   C.inv = ptr<uint32_t>(p->inv);
   C.covered = ptr<uint8_t>(p->covered);
   C.count = ptr<uint32_t>(p->count);
-  C.dirty_n = &dm->dirty_n;
-  C.covered_sets = &dm->covered_sets;
-  C.reports = nullptr;
-  C.max_reports = 0;
   C.blocks = c->num_sms * 4;
 
   std::vector<uint32_t> &hcount = p->last_counts;
   hcount.resize(n);
-  if (!c->h_pairs) c->h_pairs = new PinnedMem();
+  if (!c->h_cand) c->h_cand = new PinnedMem();
   if (!c->h_count) c->h_count = new PinnedMem();
   // mapped: candidate vertex ids in, their counts out (reference-heap picks)
   constexpr uint32_t CAND_CAP = 1u << 16;
-  TRY(c->h_pairs->ensure(c, 16 + 2 * sizeof(uint32_t) * (size_t)CAND_CAP, true));
+  TRY(c->h_cand->ensure(c, 16 + 2 * sizeof(uint32_t) * (size_t)CAND_CAP, true));
   TRY(c->h_count->ensure(c, sizeof(uint32_t) * (size_t)n));
-  PinnedMem &h_pairs = *c->h_pairs, &h_count = *c->h_count;
+  PinnedMem &h_cand = *c->h_cand, &h_count = *c->h_count;
 
   uint64_t uncovered = S;
   std::vector<uint32_t> out_seeds;
@@ -1456,8 +1449,8 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
   p->sel_prof[0] += ms_since(t_sel0);
   p->sel_prof[6] += 1;
   const int max_blocks = c->num_sms * 4;
-  unsigned char *hb = static_cast<unsigned char *>(h_pairs.p);
-  unsigned char *db = static_cast<unsigned char *>(h_pairs.dev);
+  unsigned char *hb = static_cast<unsigned char *>(h_cand.p);
+  unsigned char *db = static_cast<unsigned char *>(h_cand.dev);
   // One pick: mark v's uncovered sets covered and decrement their members, one
   // warp per set of v's inverted list (`gain` of them are still uncovered).
   auto cover = [&](uint32_t v, uint64_t gain) -> int {

@@ -58,7 +58,7 @@ struct rip_ctx {
   // or a new pool then costs no cudaMalloc); counted in `used`.
   std::vector<DevMem> cache;
   size_t cached = 0;
-  PinnedMem *h_pairs = nullptr;  // mapped: per-pick decrement reports
+  PinnedMem *h_cand = nullptr;   // mapped: reference-heap candidate ids and counts
   PinnedMem *h_count = nullptr;  // counts at the start of a selection
   // multi-instance sampler scratch (per warp: bitmap for the largest graph
   // of the launch + queue), instance table, failure pairs
@@ -271,10 +271,7 @@ struct PoolMeta {  // device-side bookkeeping block (one D2H reads it all)
   unsigned long long stats[8];
   unsigned int fail_count;
   unsigned int next;
-  unsigned int dirty_n;
   unsigned int fused_dirty;
-  unsigned long long best;
-  unsigned long long covered_sets;
 };
 
 struct rip_pool {

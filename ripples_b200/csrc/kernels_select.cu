@@ -11,15 +11,18 @@
 //                   contain the seed, instead of re-scanning the pool
 //                   (update_mask_kernel + count_uncovered_kernel,
 //                   src/gpu/find_most_influential.cc:74-98).
-// cover_kernel      after a pick: marks the seed's still-uncovered sets
-//                   covered and decrements the counts of their members
-//                   (UpdateCounters, include/ripples/counting.h:141-151),
-//                   reporting each decremented vertex straight to mapped host
-//                   memory so the host heap mirrors the counts exactly.
+// cover_kernel      after a reference-heap pick: marks the seed's
+//                   still-uncovered sets covered and decrements the counts of
+//                   their members (UpdateCounters,
+//                   include/ripples/counting.h:141-151).
+// gather_counts     the counts of the heap items a reference-heap pick can
+//                   examine, into mapped host memory.
 // heap kernels      the selection max-heap built on the device, level by
 //                   level, element for element the one std::make_heap builds.
-// argmax_kernel     max count, lowest vertex id on ties (thrust::max_element,
-//                   src/gpu/find_most_influential.cc:65-72).
+// sel_* kernels     lowest-id picks entirely on the device (max count, lowest
+//                   vertex id on ties, as thrust::max_element in
+//                   src/gpu/find_most_influential.cc:65-72): cached chunk
+//                   maxima, cover by decrement or recount.
 //
 // All per-set loops use the same warp-level load balancing: a warp takes 32
 // sets, scans their lengths and walks the concatenated elements 32 at a time,
@@ -114,52 +117,20 @@ inverted_kernel(DevPool P, uint64_t S, uint64_t *cursor, uint32_t *inv, uint64_t
 
 // One warp per set of the seed's inverted list.  A set holds each vertex
 // once, so its members are decremented with plain reductions (no result
-// needed, nothing to aggregate); when asked, every decrement is reported as
-// the vertex id into a slot range the warp reserves for the whole set, and
-// the host mirror applies count[u] -= 1 per report.
+// needed, nothing to aggregate).
 __global__ void __launch_bounds__(256) cover_kernel(CoverLaunch C) {
   const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   const uint32_t lane = lane_id();
   const uint64_t lo = C.inv_off[C.vertex], hi = C.inv_off[C.vertex + 1];
-  unsigned long long newly = 0;
   for (uint64_t i = lo + gw; i < hi; i += nw) {
     const uint32_t s = C.inv[i];
     if (C.covered[s]) continue;  // covered by an earlier seed (warp-uniform)
     const uint32_t len = C.P.set_len[s];
     const uint64_t off = C.P.set_off[s];
-    unsigned int base = 0;
-    if (lane == 0) {
-      C.covered[s] = 1;  // s holds the vertex once: no other warp has s
-      ++newly;
-      if (C.reports) base = atomicAdd(C.dirty_n, len);
-    }
-    base = __shfl_sync(FULL, base, 0);
-    for (uint32_t j = lane; j < len; j += 32) {
-      const uint32_t u = C.P.vtx[off + j];
-      atomicSub(C.count + u, 1u);
-      if (C.reports && base + j < C.max_reports) C.reports[base + j] = u;
-    }
+    if (lane == 0) C.covered[s] = 1;  // s holds the vertex once: no other warp has s
+    for (uint32_t j = lane; j < len; j += 32) atomicSub(C.count + C.P.vtx[off + j], 1u);
   }
-  newly = warp_sum_u64(newly);
-  if (lane == 0 && newly) atomicAdd(C.covered_sets, newly);
-}
-
-__global__ void argmax_kernel(const uint32_t *count, uint32_t n,
-                              unsigned long long *best) {
-  unsigned long long key = 0;
-  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n;
-       v += gridDim.x * blockDim.x) {
-    const unsigned long long k =
-        ((unsigned long long)count[v] << 32) | (unsigned long long)(~v);
-    key = k > key ? k : key;
-  }
-#pragma unroll
-  for (int d = 16; d > 0; d >>= 1) {
-    const unsigned long long o = __shfl_xor_sync(FULL, key, d);
-    key = o > key ? o : key;
-  }
-  if (lane_id() == 0 && key) atomicMax(best, key);
 }
 
 // ---- device-only picks (served queries) -----------------------------------
@@ -572,10 +543,5 @@ void launch_gather_counts(const uint32_t *count, const uint32_t *ids, uint32_t m
                                                                                      m, out);
 }
 
-void launch_argmax(const uint32_t *count, uint32_t n, unsigned long long *best,
-                   int blocks, cudaStream_t stream) {
-  count_launches(1);
-  argmax_kernel<<<blocks, 256, 0, stream>>>(count, n, best);
-}
 
 }  // namespace rip

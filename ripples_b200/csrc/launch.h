@@ -174,20 +174,13 @@ struct CoverLaunch {
   uint32_t vertex;
   uint8_t *covered;
   uint32_t *count;
-  unsigned int *dirty_n;
-  unsigned long long *covered_sets;  // running total of newly covered sets
-  // When set, every decrement reports its vertex here, at positions counted
-  // by dirty_n (reports past max_reports are dropped; dirty_n still counts).
-  uint32_t *reports;
-  uint32_t max_reports;
   int blocks;
 };
 void launch_cover(const CoverLaunch &C, cudaStream_t stream);
 // Builds the selection max-heap of {vertex, count} on the device, element for
 // element the heap std::make_heap builds (level-parallel).
 void launch_make_heap(const uint32_t *count, uint32_t n, uint2 *heap, cudaStream_t stream);
-void launch_argmax(const uint32_t *count, uint32_t n, unsigned long long *best,
-                   int blocks, cudaStream_t stream);
+
 
 // Device-only lowest-id picks of one served query (lives in device memory).
 constexpr uint32_t SEL_MAX_SEGMENTS = 8;
