@@ -380,19 +380,26 @@ def main():
     h2d = pin_idx.numel() * 8 + pin_src.numel() * 4 + pin_w.numel() * 4
     d2h = 4 * w["k"]
 
+    e2e_split = {"upload_ms": 0.0, "imm_ms": 0.0}
+
     def e2e_step(step):
+        t0 = time.perf_counter()
         gen_g = rb.HostGraph(g.n, pin_idx.numpy(), pin_src.numpy(), pin_w.numpy())
         gen = rb.B200RRRGenerator(gen_g, w["model"], seed=seed_base + 7919 + step, ctx=ctx)
+        t1 = time.perf_counter()
         CFG = rb.IMMConfiguration(k=w["k"], epsilon=w["eps"], diffusionModel=w["model"])
         rec = rb.IMMExecutionRecord()
         seeds = rb.IMM(gen_g, CFG, 1.0, gen, rec)
         n_sets = rec.TotalSets
         gen.pool.close()
         gen.graph.close()
+        e2e_split["upload_ms"] += 1e3 * (t1 - t0)
+        e2e_split["imm_ms"] += 1e3 * (time.perf_counter() - t1)
         return n_sets, seeds
 
     e2e_steps = max(1, min(args.steps, 3))
     e2e_step(-1)
+    e2e_split.update(upload_ms=0.0, imm_ms=0.0)
     barrier(world)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -439,7 +446,8 @@ def main():
                        "parallelism": f"replicas x{world}",
                        "l2": "graph (%d MB) and pool exceed L2 (126 MB)" % ((g.m * 8 + g.n * 4) >> 20)},
             "e2e": {"value": e2e_value, "unit": "sets/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "steps": e2e_steps},
+                    "d2h_bytes_per_step": d2h, "steps": e2e_steps,
+                    "split_ms_per_step": {kk: vv / e2e_steps for kk, vv in e2e_split.items()}},
             "roofline": {"bound": "hbm", "kernel": kernel,
                          "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
                          "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
@@ -552,10 +560,19 @@ def run_batch(args, w, world, rank, local):
         inst.append(dict(g=gi, k=int(rng.integers(10, 201)), eps=float(rng.uniform(0.1, 0.5)),
                          seed=10_000 + j))
 
+    server_stats = {}
+
     def batched(tag):
+        """All instances as one continuous batch (what rip_imm_batch runs),
+        through the server API so its phase timing can be reported."""
         qs = [rb.Query(graphs[x["g"]]["dg"], x["k"], x["eps"], seed=x["seed"] + tag)
               for x in inst]
-        rb.imm_batch(ctx, qs)
+        srv = rb.Server(ctx, max_active=len(qs))
+        for q in qs:
+            srv.submit(q)
+        srv.drain()
+        server_stats.update(srv.stats())
+        srv.close()
         return qs
 
     def plain(tag, limit_s=None):
@@ -616,6 +633,7 @@ def run_batch(args, w, world, rank, local):
                        "graphs": [{k: v for k, v in g.items() if k != "dg"} for g in graphs],
                        "tiebreak": "lowest id (device picks)"},
             "failed_instances_per_step": failed / max(args.steps, 1),
+            "server_last_step": dict(server_stats),
             "autotune_s": t_tune,
             "plain_one_at_a_time": {"value": p_sets / t_p, "unit": "sets/s",
                                     "instances": len(pl), "failed": p_failed,

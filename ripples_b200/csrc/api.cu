@@ -56,6 +56,7 @@ int rip_ctx_destroy(rip_ctx *c) {
   dfree(c, c->m_scratch);
   dfree(c, c->m_table);
   dfree(c, c->m_fail);
+  if (c->heap_registered) cudaHostUnregister(c->heap_registered);
   delete c->h_cand;
   delete c->h_count;
   delete c->h_meta;
@@ -110,15 +111,6 @@ extern "C" int rip_graph_upload(rip_ctx *c, const uint64_t *index,
                    (unsigned long long)m);
   if (index[0] != 0 || index[n] != m)
     return set_err(c, RIP_ERR_INVALID, "index[0] must be 0 and index[n] == m");
-  long bad = 0;
-#pragma omp parallel for reduction(+ : bad) schedule(static)
-  for (long long v = 0; v < (long long)n; ++v)
-    bad += index[v + 1] < index[v];
-#pragma omp parallel for reduction(+ : bad) schedule(static)
-  for (long long e = 0; e < (long long)m; ++e) bad += src[e] >= n;
-  if (bad)
-    return set_err(c, RIP_ERR_INVALID,
-                   "CSR not monotone or source id out of range (%ld bad)", bad);
   *out = nullptr;
   CK(c, cudaSetDevice(c->device));
   rip_graph *g = new rip_graph();
@@ -146,6 +138,21 @@ extern "C" int rip_graph_upload(rip_ctx *c, const uint64_t *index,
     if (e != cudaSuccess) {
       rc = set_err(c, RIP_ERR_CUDA, "graph upload copy failed: %s",
                    cudaGetErrorString(e));
+      break;
+    }
+    // validated on the device before anything indexes by it
+    unsigned long long bad = 0;  // counted in the first word of the edge buffer
+    launch_validate_csr(ptr<uint64_t>(d_index), ptr<uint32_t>(d_src), n, m,
+                        reinterpret_cast<unsigned long long *>(g->edges.p), c->stream);
+    e = cudaMemcpyAsync(&bad, g->edges.p, sizeof(bad), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) {
+      rc = set_err(c, RIP_ERR_CUDA, "graph validation failed: %s", cudaGetErrorString(e));
+      break;
+    }
+    if (bad) {
+      rc = set_err(c, RIP_ERR_INVALID,
+                   "CSR not monotone or source id out of range (%llu bad)", bad);
       break;
     }
     if (model == RIP_MODEL_IC)
@@ -384,7 +391,6 @@ extern "C" int rip_pool_destroy(rip_pool *p) {
     dfree(c, g.inv);
   }
   for (DevMem *m : all) dfree(c, *m);
-  if (p->heap_registered) cudaHostUnregister(p->heap_registered);
   if (p->sel_graph.exec) cudaGraphExecDestroy(p->sel_graph.exec);
   erase_ptr(c->pools, p);
   delete p;
@@ -1467,16 +1473,26 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
     // reference builds its heap (streaming_find_most_influential.h:541-544;
     // counting.h:196-206): the same heap, built level-parallel on the device
     // and downloaded into page-locked storage the queue adopts as is.
-    std::vector<HeapItem> storage = std::move(p->heap_store);
-    if (storage.capacity() < n || !p->heap_registered) {
-      if (p->heap_registered) cudaHostUnregister(p->heap_registered);
-      p->heap_registered = nullptr;
+    // The storage is the context's (page-locked once, reused by every pool);
+    // the guards hand it back on every way out of this block.
+    struct Lease {
+      rip_ctx *c;
+      std::vector<HeapItem> v;
+      explicit Lease(rip_ctx *c_) : c(c_), v(std::move(c_->heap_store)) {}
+      ~Lease() {
+        if (v.capacity()) c->heap_store = std::move(v);
+      }
+    } lease(c);
+    std::vector<HeapItem> &storage = lease.v;
+    if (storage.capacity() < n || !c->heap_registered) {
+      if (c->heap_registered) cudaHostUnregister(c->heap_registered);
+      c->heap_registered = nullptr;
+      std::vector<HeapItem>().swap(storage);
       storage.reserve(n);
       storage.resize(n);
       if (cudaHostRegister(storage.data(), sizeof(HeapItem) * storage.capacity(), 0) ==
           cudaSuccess) {
-        p->heap_registered = storage.data();
-        p->heap_registered_bytes = sizeof(HeapItem) * storage.capacity();
+        c->heap_registered = storage.data();
       } else {
         cudaGetLastError();  // pageable copy still works, only slower
       }
@@ -1489,6 +1505,11 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
                           cudaMemcpyDeviceToHost, c->stream));
     CK(c, cudaStreamSynchronize(c->stream));
     AdoptedQueue queue(std::move(storage));
+    struct Return {
+      rip_ctx *c;
+      AdoptedQueue &q;
+      ~Return() { c->heap_store = q.release(); }
+    } give_back{c, queue};
     p->sel_prof[1] += ms_since(t_h0);
     const auto t_p0 = clk::now();
     // The lazy pops of a pick only read the current counts of heap items keyed
@@ -1595,7 +1616,6 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
     }
     p->sel_prof[2] += ms_since(t_p0);
     p->sel_prof[4] += out_seeds.size();
-    p->heap_store = queue.release();
   } else if (k > 0 && S > 0) {
     // Lowest-id picks entirely on the device: k pick launches (cached chunk
     // maxima, lowest id on ties) and k - 1 cover launches, one read-back.

@@ -59,6 +59,10 @@ struct rip_ctx {
   std::vector<DevMem> cache;
   size_t cached = 0;
   PinnedMem *h_cand = nullptr;   // mapped: reference-heap candidate ids and counts
+  // reference-heap selection storage, shared by the context's pools (one
+  // selection runs at a time) and page-locked once
+  std::vector<HeapItem> heap_store;
+  void *heap_registered = nullptr;
   PinnedMem *h_count = nullptr;  // counts at the start of a selection
   // multi-instance sampler scratch (per warp: bitmap for the largest graph
   // of the launch + queue), instance table, failure pairs
@@ -314,10 +318,7 @@ struct rip_pool {
   std::vector<uint32_t> last_counts;
   bool last_counts_on_device = false;  // last_counts still in `count` only
   bool have_last_counts = false;
-  std::vector<HeapItem> heap_store;  // heap storage reused across selections
   uint32_t cand_fixed = 0;           // first-fetch threshold, % of the last gain (0 = adaptive)
-  void *heap_registered = nullptr;   // heap_store's buffer while page-locked
-  size_t heap_registered_bytes = 0;
   DevMem d_heap;                     // heap built on the device
   DevMem s_cmax, s_dirty, s_best, s_desc;  // device lowest-id picks
   PinnedMem h_best;

@@ -63,23 +63,45 @@ __global__ void pack_lt_kernel(const uint64_t *index, const uint32_t *src,
   const uint32_t lane = threadIdx.x & 31u;
   const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  for (uint64_t v = gw; v < n; v += nw) {
-    const uint64_t beg = index[v], end = index[v + 1];
-    uint64_t carry = 0;
-    for (uint64_t base = beg; base < end; base += 32) {
-      const uint64_t e = base + lane;
-      uint64_t x = e < end ? lt_fixed(w[e]) : 0ull;
-#pragma unroll
-      for (int d = 1; d < 32; d <<= 1) {
-        const uint64_t y = __shfl_up_sync(0xFFFFFFFFu, x, d);
-        if (lane >= (uint32_t)d) x = sat_add(x, y);
-      }
-      x = sat_add(x, carry);
-      if (e < end) {
-        const uint64_t c = x >> 8;
+  // 32 consecutive vertices per warp: a lane scans its own vertex when it has
+  // at most 32 in-edges (most vertices); the warp scans each larger one
+  // together, 32 edges per step with a shuffle scan
+  for (uint64_t v0 = gw * 32; v0 < n; v0 += nw * 32) {
+    const uint64_t v = v0 + lane;
+    uint64_t beg = 0, end = 0;
+    if (v < n) {
+      beg = index[v];
+      end = index[v + 1];
+    }
+    if (end - beg <= 32) {
+      uint64_t run = 0;
+      for (uint64_t e = beg; e < end; ++e) {
+        run = sat_add(run, lt_fixed(w[e]));
+        const uint64_t c = run >> 8;
         edges[e] = make_uint2(src[e], c > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)c);
       }
-      carry = __shfl_sync(0xFFFFFFFFu, x, 31);
+    }
+    uint32_t big = __ballot_sync(0xFFFFFFFFu, end - beg > 32);
+    while (big) {
+      const uint32_t L = __ffs(big) - 1;
+      big &= big - 1;
+      const uint64_t b = __shfl_sync(0xFFFFFFFFu, beg, L), t = __shfl_sync(0xFFFFFFFFu, end, L);
+      uint64_t carry = 0;
+      for (uint64_t base = b; base < t; base += 32) {
+        const uint64_t e = base + lane;
+        uint64_t x = e < t ? lt_fixed(w[e]) : 0ull;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+          const uint64_t y = __shfl_up_sync(0xFFFFFFFFu, x, d);
+          if (lane >= (uint32_t)d) x = sat_add(x, y);
+        }
+        x = sat_add(x, carry);
+        if (e < t) {
+          const uint64_t c = x >> 8;
+          edges[e] = make_uint2(src[e], c > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)c);
+        }
+        carry = __shfl_sync(0xFFFFFFFFu, x, 31);
+      }
     }
   }
   const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
@@ -102,6 +124,25 @@ void launch_pack_ic(const uint64_t *index, const float *w, uint32_t n,
   count_launches(2);
   pack_off_kernel<<<1184, 256, 0, stream>>>(index, n, off);
   pack_ic_kernel<<<2368, 256, 0, stream>>>(src, w, m, pad4(m) + 4, edges);
+}
+
+// *bad = entries with index[v + 1] < index[v] plus sources >= n
+__global__ void validate_csr_kernel(const uint64_t *index, const uint32_t *src, uint32_t n,
+                                    uint64_t m, unsigned long long *bad) {
+  const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  unsigned long long b = 0;
+  for (uint64_t v = tid; v < n; v += stride) b += index[v + 1] < index[v];
+  for (uint64_t e = tid; e < m; e += stride) b += src[e] >= n;
+  for (int d = 16; d > 0; d >>= 1) b += __shfl_xor_sync(0xFFFFFFFFu, b, d);
+  if ((threadIdx.x & 31u) == 0 && b) atomicAdd(bad, b);
+}
+
+void launch_validate_csr(const uint64_t *index, const uint32_t *src, uint32_t n, uint64_t m,
+                         unsigned long long *bad, cudaStream_t stream) {
+  count_launches(1);
+  cudaMemsetAsync(bad, 0, sizeof(*bad), stream);
+  validate_csr_kernel<<<2368, 256, 0, stream>>>(index, src, n, m, bad);
 }
 
 void launch_pack_lt(const uint64_t *index, const float *w, uint32_t n,

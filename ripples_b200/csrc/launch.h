@@ -153,6 +153,8 @@ void launch_weights(int kind, const uint64_t *index, uint32_t n, uint64_t seed, 
 void launch_pack_ic(const uint64_t *index, const float *w, uint32_t n,
                     uint64_t m, uint32_t *off, uint2 *edges, const uint32_t *src,
                     cudaStream_t stream);
+void launch_validate_csr(const uint64_t *index, const uint32_t *src, uint32_t n, uint64_t m,
+                         unsigned long long *bad, cudaStream_t stream);
 void launch_pack_lt(const uint64_t *index, const float *w, uint32_t n,
                     uint64_t m, uint32_t *off, uint2 *edges, const uint32_t *src,
                     cudaStream_t stream);
