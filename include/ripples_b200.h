@@ -181,18 +181,27 @@ int rip_pool_configure(rip_pool *p, uint32_t colors, uint32_t slots,
 int rip_pool_work_caps(rip_pool *p, uint64_t plain_cap, uint64_t fused_cap);
 
 /* Per-graph sampler autotuner.  Times `pilot` sets (0 = 2048) of `seed` on a
- * scratch pool under each of RIP_TUNE_CANDIDATES IC configurations:
+ * scratch pool under each of RIP_TUNE_CANDIDATES IC configurations (after a
+ * warm-up run, the faster of two timed runs):
  *   0 plain (one set per warp), heavy sets past 2^18 in-edges -> grid-wide BFS
  *   1 plain, heavy past 2^14 in-edges -> grid-wide BFS
  *   2 plain, heavy past 2^18 -> one CTA per set
  *   3/4/5 fused 64/128/256 colours, batches past 2^23 -> heavy path
+ *   6/7 as 0/2 with the one-set-per-warp kernel capped at 48 registers
+ *       (40 resident warps per SM instead of 32)
  * writes the wall times to ms[] (may be null) and the fastest to *choice, and
  * keeps it for the graph: pools created afterwards start from it and
  * RIP_SAMPLER_AUTO runs it.  Untuned graphs run configuration 0 for AUTO.  LT
  * graphs have one sampler (choice 0).  Sets never depend on the choice.  No
  * reference counterpart (the reference fixes its GPU colour width). */
-#define RIP_TUNE_CANDIDATES 6
+#define RIP_TUNE_CANDIDATES 8
 int rip_graph_autotune(rip_graph *g, uint64_t seed, uint32_t pilot, double *ms, int *choice);
+
+/* Variant of the one-set-per-warp IC kernel: 0 = no register cap (32 resident
+ * warps per SM), 5 = at most 48 registers (40 warps per SM).  Results do not
+ * depend on it; rip_graph_autotune chooses it per graph.  No reference
+ * counterpart. */
+int rip_pool_plain_occupancy(rip_pool *p, int blocks_per_sm);
 
 /* IC sets whose edge work passes the caps above are grown either one
  * 1024-thread CTA per set or, when at least `min_sets` of them are pending,

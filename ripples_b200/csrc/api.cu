@@ -365,6 +365,7 @@ extern "C" int rip_pool_create(rip_ctx *c, rip_graph *g, rip_pool **out) {
     p->cap_plain = g->tuned.cap_plain;
     p->cap_fused = g->tuned.cap_fused;
     p->giant_min = g->tuned.giant_min;
+    p->plain_occupancy = g->tuned.plain_occupancy;
   }
   c->pools.push_back(p);
   *out = p;
@@ -488,8 +489,10 @@ static uint32_t default_warps(rip_pool *p, uint32_t qcap) {
   rip_ctx *c = p->ctx;
   const uint64_t bm_bytes = scratch_bm_words(p) * 4;
   const uint64_t per = bm_bytes + (uint64_t)qcap * 4;
-  // LT walks: 64 resident warps per SM (latency-bound chains); IC: 32
-  uint64_t want = (uint64_t)c->num_sms * (p->g->model == RIP_MODEL_LT ? 64 : 32);
+  // LT walks: 64 resident warps per SM (latency-bound chains); IC: 32, or 40
+  // with the register-capped kernel variant
+  uint64_t want = (uint64_t)c->num_sms *
+                  (p->g->model == RIP_MODEL_LT ? 64 : p->plain_occupancy == 5 ? 40 : 32);
   size_t avail = c->budget > c->used ? c->budget - c->used : 0;
   uint64_t fit = (avail / 4) / per;  // scratch gets at most a quarter
   uint64_t w = std::min<uint64_t>(want, std::max<uint64_t>(fit, 8));
@@ -545,6 +548,7 @@ static int sample_warp_per_set(rip_pool *p, uint64_t seed, uint64_t first,
     L.F = FailList{ptr<uint32_t>(p->ids_a), &dm->fail_count, &dm->first_bad};
     L.st = Stats{dm->stats};
     L.threads = 256;
+    L.occupancy = p->plain_occupancy;
     const uint32_t active = std::min<uint32_t>(p->warps, todo);
     L.blocks = (int)std::max<uint32_t>(1, (active + 7) / 8);
     CK(c, cudaEventRecord(c->ev0, c->stream));
@@ -995,14 +999,17 @@ extern "C" int rip_graph_autotune(rip_graph *g, uint64_t seed, uint32_t pilot, d
     uint32_t colors;
     uint64_t cap_plain, cap_fused;
     uint32_t giant_min;
+    int occupancy;
   };
   static const Cand cands[RIP_TUNE_CANDIDATES] = {
-      {RIP_SAMPLER_PLAIN, 64, 1ull << 18, 1ull << 23, 32},
-      {RIP_SAMPLER_PLAIN, 64, 1ull << 14, 1ull << 23, 32},
-      {RIP_SAMPLER_PLAIN, 64, 1ull << 18, 1ull << 23, 0},
-      {RIP_SAMPLER_FUSED, 64, 1ull << 18, 1ull << 23, 32},
-      {RIP_SAMPLER_FUSED, 128, 1ull << 18, 1ull << 23, 32},
-      {RIP_SAMPLER_FUSED, 256, 1ull << 18, 1ull << 23, 32},
+      {RIP_SAMPLER_PLAIN, 64, 1ull << 18, 1ull << 23, 32, 0},
+      {RIP_SAMPLER_PLAIN, 64, 1ull << 14, 1ull << 23, 32, 0},
+      {RIP_SAMPLER_PLAIN, 64, 1ull << 18, 1ull << 23, 0, 0},
+      {RIP_SAMPLER_FUSED, 64, 1ull << 18, 1ull << 23, 32, 0},
+      {RIP_SAMPLER_FUSED, 128, 1ull << 18, 1ull << 23, 32, 0},
+      {RIP_SAMPLER_FUSED, 256, 1ull << 18, 1ull << 23, 32, 0},
+      {RIP_SAMPLER_PLAIN, 64, 1ull << 18, 1ull << 23, 32, 5},
+      {RIP_SAMPLER_PLAIN, 64, 1ull << 18, 1ull << 23, 0, 5},
   };
   if (ms)
     for (int i = 0; i < RIP_TUNE_CANDIDATES; ++i) ms[i] = -1.0;
@@ -1023,13 +1030,19 @@ extern "C" int rip_graph_autotune(rip_graph *g, uint64_t seed, uint32_t pilot, d
     p->cap_plain = cands[i].cap_plain;
     p->cap_fused = cands[i].cap_fused;
     p->giant_min = cands[i].giant_min;
-    // a small warm-up sizes the scratch; the timed pilot follows it
-    int rc = rip_sample(p, seed, std::min<uint32_t>(pilot / 8, 256), RIP_SAMPLER_AUTO);
+    p->plain_occupancy = cands[i].occupancy;
+    // a warm-up sizes every scratch buffer (heavy-set paths included); then
+    // the pilot runs twice on a cleared pool and the faster run counts
+    int rc = rip_sample(p, seed, pilot, RIP_SAMPLER_AUTO);
     if (rc == RIP_OK) rc = rip_sync(c);
-    const auto t0 = clk::now();
-    if (rc == RIP_OK) rc = rip_sample(p, seed, pilot, RIP_SAMPLER_AUTO);
-    if (rc == RIP_OK) rc = rip_sync(c);
-    const double t = ms_since(t0);
+    double t = 1e300;
+    for (int rep = 0; rep < 2 && rc == RIP_OK; ++rep) {
+      rc = rip_pool_clear(p);
+      const auto t0 = clk::now();
+      if (rc == RIP_OK) rc = rip_sample(p, seed, pilot, RIP_SAMPLER_AUTO);
+      if (rc == RIP_OK) rc = rip_sync(c);
+      t = std::min(t, ms_since(t0));
+    }
     rip_pool_destroy(p);
     if (rc != RIP_OK) return rc;
     if (ms) ms[i] = t;
@@ -1044,7 +1057,18 @@ extern "C" int rip_graph_autotune(rip_graph *g, uint64_t seed, uint32_t pilot, d
   g->tuned.cap_plain = cands[best].cap_plain;
   g->tuned.cap_fused = cands[best].cap_fused;
   g->tuned.giant_min = cands[best].giant_min;
+  g->tuned.plain_occupancy = cands[best].occupancy;
   if (choice) *choice = best;
+  return RIP_OK;
+}
+
+// Register/occupancy variant of the one-set-per-warp IC kernel (0 or 5).
+extern "C" int rip_pool_plain_occupancy(rip_pool *p, int blocks_per_sm) {
+  if (!p || (blocks_per_sm != 0 && blocks_per_sm != 5)) return RIP_ERR_INVALID;
+  if (p->plain_occupancy != blocks_per_sm) {
+    p->plain_occupancy = blocks_per_sm;
+    p->warps = 0;  // re-size the per-warp scratch for the new warp count
+  }
   return RIP_OK;
 }
 

@@ -249,6 +249,7 @@ struct rip_graph {
     int sampler = RIP_SAMPLER_PLAIN;
     uint32_t colors = 64, giant_min = 32;
     uint64_t cap_plain = 1ull << 18, cap_fused = 1ull << 23;
+    int plain_occupancy = 0;
   } tuned;
   DevGraph view() {
     return DevGraph{n, m, ptr<uint32_t>(off), ptr<uint2>(edges)};
@@ -300,6 +301,7 @@ struct rip_pool {
   DevMem g_state, g_lists, g_col;
   uint32_t giant_min = 32;  // heavy sets that switch to the grid-wide BFS (0 = never)
   int auto_sampler = RIP_SAMPLER_PLAIN;  // what RIP_SAMPLER_AUTO runs (IC)
+  int plain_occupancy = 0;   // IC one-set-per-warp kernel variant (0 or 5)
   uint64_t cap_plain = 1ull << 18;  // in-edges per set before a warp hands it over
   uint64_t cap_fused = 1ull << 23;  // in-edges per fused batch before handing over
   uint64_t big_sets = 0;            // sets grown one CTA each (diagnostic)

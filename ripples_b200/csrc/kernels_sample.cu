@@ -255,7 +255,10 @@ __device__ __forceinline__ SetOutcome lt_walk_set(const DevGraph &G, Key key, ui
 
 }  // namespace
 
-__global__ void __launch_bounds__(256)
+// MINB: resident blocks per SM the compiler must allow (1: no register cap;
+// 5: at most 48 registers, 40 warps per SM -- the autotuner picks per graph).
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB)
 ic_plain_kernel(DevGraph G, DevPool P, Key key, uint64_t first, uint32_t count,
                 const uint32_t *ids, unsigned int *next, uint32_t *bitmaps,
                 uint64_t bm_words, uint32_t *queues, uint32_t qcap,
@@ -406,9 +409,14 @@ void launch_multi_sample(const MultiLaunch &L, cudaStream_t stream) {
 
 void launch_ic_plain(const SampleLaunch &L, cudaStream_t stream) {
   count_launches(1);
-  ic_plain_kernel<<<L.blocks, L.threads, 0, stream>>>(
-      L.G, L.P, L.key, L.first, L.count, L.ids, L.next, L.bitmaps, L.bm_words,
-      L.queues, L.qcap, L.work_cap, L.F, L.st);
+  if (L.occupancy == 5)
+    ic_plain_kernel<5><<<L.blocks, L.threads, 0, stream>>>(
+        L.G, L.P, L.key, L.first, L.count, L.ids, L.next, L.bitmaps, L.bm_words,
+        L.queues, L.qcap, L.work_cap, L.F, L.st);
+  else
+    ic_plain_kernel<1><<<L.blocks, L.threads, 0, stream>>>(
+        L.G, L.P, L.key, L.first, L.count, L.ids, L.next, L.bitmaps, L.bm_words,
+        L.queues, L.qcap, L.work_cap, L.F, L.st);
 }
 
 void launch_lt_walk(const SampleLaunch &L, cudaStream_t stream) {

@@ -32,6 +32,7 @@ struct SampleLaunch {
   FailList F{};
   Stats st{};
   int blocks = 0, threads = 0;
+  int occupancy = 0;         // IC: 5 = the 48-register variant (40 warps per SM)
 };
 
 void launch_ic_plain(const SampleLaunch &L, cudaStream_t stream);

@@ -219,7 +219,9 @@ class DeviceGraph:
         return idx, src[: self.m]
 
     TUNE_NAMES = ("plain, heavy>2^18 grid BFS", "plain, heavy>2^14 grid BFS",
-                  "plain, heavy>2^18 CTA per set", "fused 64", "fused 128", "fused 256")
+                  "plain, heavy>2^18 CTA per set", "fused 64", "fused 128", "fused 256",
+                  "plain 40 warps/SM, heavy>2^18 grid BFS",
+                  "plain 40 warps/SM, heavy>2^18 CTA per set")
 
     def autotune(self, seed: int = 0, pilot: int = 0) -> dict:
         """Times each IC sampler configuration on a pilot of sets and keeps the
@@ -284,6 +286,11 @@ class Pool:
     def configure(self, colors: int = 64, slots: int = 0, log_capacity: int = 0) -> None:
         self._chk(lib.rip_pool_configure(self.h, colors, slots, log_capacity),
                   "rip_pool_configure")
+
+    def plain_occupancy(self, blocks_per_sm: int) -> None:
+        """One-set-per-warp IC kernel variant: 0 (no register cap) or 5."""
+        self._chk(lib.rip_pool_plain_occupancy(self.h, blocks_per_sm),
+                  "rip_pool_plain_occupancy")
 
     def heavy_batch(self, min_sets: int) -> None:
         """Heavy IC sets pending from which the grid-wide multi-colour BFS

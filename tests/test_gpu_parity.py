@@ -49,10 +49,12 @@ def test_thresholds_match_oracle(ctx):
         dg.close()
 
 
-@pytest.mark.parametrize("sampler,colors", SAMPLERS)
-def test_ic_sets_bit_exact(ctx, sampler, colors):
+@pytest.mark.parametrize("sampler,colors,occupancy", [s + (0,) for s in SAMPLERS] +
+                         [(rb.SAMPLER_PLAIN, 64, 5)])
+def test_ic_sets_bit_exact(ctx, sampler, colors, occupancy):
     g = ic_graph()
     dg, p = device_pool(ctx, g, "IC", colors)
+    p.plain_occupancy(occupancy)
     p.sample(3000, seed=7, sampler=sampler)
     off, vtx = p.export()
     ooff, ovtx, ost = oracle_sets(g, "IC", 7, 0, 3000)
