@@ -752,7 +752,7 @@ def run_serve(args, w, world, rank, local):
     t_tune = time.perf_counter()
     tuned = {}
     for sc in scales:
-        tuned[f"{sc}IC"] = graphs[(sc, "IC")].autotune(seed=3, pilot=1024)["name"]
+        tuned[f"{sc}IC"] = graphs[(sc, "IC")].autotune(seed=3, pilot=512)["name"]
         _progress(t_run, f"autotuned {sc}IC: {tuned[f'{sc}IC']}")
     t_tune = time.perf_counter() - t_tune
     rng = np.random.default_rng(3)

@@ -255,8 +255,9 @@ __device__ __forceinline__ SetOutcome lt_walk_set(const DevGraph &G, Key key, ui
 
 }  // namespace
 
-// MINB: resident blocks per SM the compiler must allow (1: no register cap;
-// 5: at most 48 registers, 40 warps per SM -- the autotuner picks per graph).
+// MINB: resident blocks per SM the compiler must allow (4: at most 64
+// registers, 32 warps per SM; 5: at most 48 registers, 40 warps per SM -- the
+// autotuner picks per graph).
 template <int MINB>
 __global__ void __launch_bounds__(256, MINB)
 ic_plain_kernel(DevGraph G, DevPool P, Key key, uint64_t first, uint32_t count,
@@ -414,7 +415,7 @@ void launch_ic_plain(const SampleLaunch &L, cudaStream_t stream) {
         L.G, L.P, L.key, L.first, L.count, L.ids, L.next, L.bitmaps, L.bm_words,
         L.queues, L.qcap, L.work_cap, L.F, L.st);
   else
-    ic_plain_kernel<1><<<L.blocks, L.threads, 0, stream>>>(
+    ic_plain_kernel<4><<<L.blocks, L.threads, 0, stream>>>(
         L.G, L.P, L.key, L.first, L.count, L.ids, L.next, L.bitmaps, L.bm_words,
         L.queues, L.qcap, L.work_cap, L.F, L.st);
 }
