@@ -346,3 +346,8 @@ struct rip_pool {
 // Ends the server queries on graph g and drops the servers' pools on it
 // (called before g is destroyed).
 void server_graph_gone(rip_ctx *c, rip_graph *g);
+
+template <typename T>
+inline void erase_ptr(std::vector<T *> &v, T *x) {
+  v.erase(std::remove(v.begin(), v.end(), x), v.end());
+}

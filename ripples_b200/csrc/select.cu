@@ -1,0 +1,526 @@
+// select.cu -- greedy max-coverage seed selection behind include/ripples_b200.h
+// (FindMostInfluentialSet, include/ripples/find_most_influential.h:176):
+// counts, inverted index, the reference CPU heap (exact, host pops with
+// device-fetched counts) and device-only lowest-id picks.
+#include "host.h"
+
+// ---------------------------------------------------------------------------
+// selection
+// ---------------------------------------------------------------------------
+namespace {
+using RefQueue = std::priority_queue<HeapItem, std::vector<HeapItem>, CompareHeap>;
+
+// std::priority_queue that adopts an already-heapified container instead of
+// running make_heap again (its container and comparator are protected
+// members).  pop/push are libstdc++'s own pop_heap/push_heap, as in the
+// reference.
+struct AdoptedQueue : RefQueue {
+  explicit AdoptedQueue(std::vector<HeapItem> &&heap) { this->c = std::move(heap); }
+  std::vector<HeapItem> release() { return std::move(this->c); }
+  const std::vector<HeapItem> &items() const { return this->c; }
+};
+
+// The vertices of every heap item keyed at least T (keys never grow
+// downwards, so subtrees whose root is keyed below T are skipped).  Walked
+// breadth first: the children of a queued node are prefetched when it is
+// queued, so the random reads into the heap array overlap.  Returns the
+// count, or cap + 1 when more than cap items qualify.
+static uint32_t collect_at_least(const std::vector<HeapItem> &h, uint32_t T, uint32_t cap,
+                                 uint32_t *out, std::vector<uint32_t> &queue) {
+  const size_t len = h.size();
+  uint32_t cnt = 0;
+  queue.clear();
+  if (len && h[0].second >= T) queue.push_back(0);
+  for (size_t head = 0; head < queue.size(); ++head) {
+    const size_t i = queue[head];
+    if (cnt == cap) return cap + 1;
+    out[cnt++] = h[i].first;
+    const size_t l = 2 * i + 1;
+    for (size_t c = l; c < l + 2 && c < len; ++c)
+      if (h[c].second >= T) {
+        queue.push_back((uint32_t)c);
+        if (2 * c + 1 < len) __builtin_prefetch(&h[2 * c + 1]);
+      }
+  }
+  return cnt;
+}
+
+// Open-addressing map vertex -> fetched count for one pick's candidates.
+struct CountMap {
+  std::vector<uint32_t> key, val;  // key = vertex + 1, 0 = empty
+  uint32_t mask = 0;
+  void reset(uint32_t items) {
+    uint32_t cap = 64;
+    while (cap < 2 * items) cap <<= 1;
+    if (key.size() < cap) {
+      key.assign(cap, 0u);
+      val.resize(cap);
+    } else {
+      std::fill(key.begin(), key.begin() + cap, 0u);
+    }
+    mask = cap - 1;
+  }
+  static uint32_t hash(uint32_t v) { return (v * 2654435761u) ^ (v >> 15); }
+  void put(uint32_t v, uint32_t c) {
+    uint32_t i = hash(v) & mask;
+    while (key[i] != 0u && key[i] != v + 1) i = (i + 1) & mask;
+    key[i] = v + 1;
+    val[i] = c;
+  }
+  bool get(uint32_t v, uint32_t &c) const {
+    uint32_t i = hash(v) & mask;
+    while (key[i] != 0u) {
+      if (key[i] == v + 1) {
+        c = val[i];
+        return true;
+      }
+      i = (i + 1) & mask;
+    }
+    return false;
+  }
+};
+
+// Bit-identical to std::make_heap(v.begin(), v.end(), CompareHeap{}), built
+// level by level in parallel.  libstdc++'s make_heap runs __adjust_heap on
+// every parent from (len-2)/2 down to 0; each call only touches the subtree
+// under its parent, and all parents at one depth have disjoint subtrees and
+// larger indices than every parent above them, so processing the depths from
+// the deepest up -- each depth in any order -- performs the same operations on
+// the same data.
+void parallel_make_heap(std::vector<HeapItem> &v) {
+  const std::ptrdiff_t len = (std::ptrdiff_t)v.size();
+  if (len < 2) return;
+  const std::ptrdiff_t last_parent = (len - 2) / 2;
+  int dmax = 0;
+  while ((((std::ptrdiff_t)2) << dmax) - 1 <= last_parent) ++dmax;
+  for (int d = dmax; d >= 0; --d) {
+    const std::ptrdiff_t lo = (((std::ptrdiff_t)1) << d) - 1;
+    const std::ptrdiff_t hi = std::min(last_parent, (((std::ptrdiff_t)2) << d) - 2);
+#pragma omp parallel for schedule(static) if (hi - lo > 8192)
+    for (std::ptrdiff_t p = hi; p >= lo; --p) {
+      HeapItem val = std::move(v[p]);
+      std::__adjust_heap(v.begin(), p, len, std::move(val),
+                         __gnu_cxx::__ops::_Iter_comp_iter<CompareHeap>(CompareHeap{}));
+    }
+  }
+}
+}  // namespace
+
+// Diagnostic: the device heap build against std::make_heap on n random
+// {vertex, count} items with counts in [0, max_count); 1 when identical.
+extern "C" int rip_selftest_heap_device(rip_ctx *c, uint64_t n, uint32_t max_count,
+                                        uint64_t seed) {
+  if (!c || n == 0 || n >= 0xFFFFFFFFull) return RIP_ERR_INVALID;
+  std::vector<uint32_t> cnt(n);
+  uint64_t x = seed * 6364136223846793005ull + 1442695040888963407ull;
+  for (uint64_t i = 0; i < n; ++i) {
+    x = x * 6364136223846793005ull + 1442695040888963407ull;
+    cnt[i] = (uint32_t)((x >> 33) % (max_count ? max_count : 1));
+  }
+  std::vector<HeapItem> ref(n), got(n);
+  for (uint64_t i = 0; i < n; ++i) ref[i] = {(uint32_t)i, cnt[i]};
+  std::make_heap(ref.begin(), ref.end(), CompareHeap{});
+  DevMem d_cnt, d_heap;
+  int rc = dalloc(c, d_cnt, 4 * n);
+  if (!rc) rc = dalloc(c, d_heap, 8 * n);
+  if (!rc) {
+    cudaMemcpyAsync(d_cnt.p, cnt.data(), 4 * n, cudaMemcpyHostToDevice, c->stream);
+    launch_make_heap(ptr<uint32_t>(d_cnt), (uint32_t)n, ptr<uint2>(d_heap), c->stream);
+    cudaMemcpyAsync(got.data(), d_heap.p, 8 * n, cudaMemcpyDeviceToHost, c->stream);
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess) rc = set_err(c, RIP_ERR_CUDA, "heap selftest: %s", cudaGetErrorString(e));
+  }
+  dfree(c, d_cnt);
+  dfree(c, d_heap);
+  if (rc) return rc;
+  return ref == got ? 1 : 0;
+}
+
+// Diagnostic: checks parallel_make_heap against std::make_heap on n random
+// counts drawn from [0, max_count) (many ties); returns 1 when identical.
+extern "C" int rip_selftest_heap(uint64_t n, uint32_t max_count, uint64_t seed) {
+  std::vector<HeapItem> a(n), b;
+  uint64_t x = seed * 6364136223846793005ull + 1442695040888963407ull;
+  for (uint64_t i = 0; i < n; ++i) {
+    x = x * 6364136223846793005ull + 1442695040888963407ull;
+    a[i] = {(uint32_t)i, (uint32_t)((x >> 33) % (max_count ? max_count : 1))};
+  }
+  b = a;
+  std::make_heap(b.begin(), b.end(), CompareHeap{});
+  parallel_make_heap(a);
+  return a == b ? 1 : 0;
+}
+
+// The counts left by the last selection still sit in the count buffer; bring
+// them to the host before anything overwrites that buffer.
+static int settle_last_counts(rip_pool *p) {
+  if (!p->have_last_counts || !p->last_counts_on_device) return RIP_OK;
+  rip_ctx *c = p->ctx;
+  p->last_counts.resize(p->g->n);
+  CK(c, cudaMemcpyAsync(p->last_counts.data(), p->count.p, sizeof(uint32_t) * (size_t)p->g->n,
+                        cudaMemcpyDeviceToHost, c->stream));
+  CK(c, cudaStreamSynchronize(c->stream));
+  p->last_counts_on_device = false;
+  return RIP_OK;
+}
+
+static int count_sets(rip_pool *p, uint64_t S) {
+  rip_ctx *c = p->ctx;
+  const uint32_t n = p->g->n;
+  TRY(settle_last_counts(p));
+  // padded to whole chunks of the device picks (the tail stays zero)
+  const size_t chunk = sel_chunk_vertices();
+  const size_t padded = ((size_t)n + chunk - 1) / chunk * chunk;
+  TRY(dalloc(c, p->count, sizeof(uint32_t) * padded));
+  CK(c, cudaMemsetAsync(p->count.p, 0, sizeof(uint32_t) * padded, c->stream));
+  launch_count(p->view(), S, ptr<uint32_t>(p->count), c->num_sms * 8, c->stream);
+  CK(c, cudaGetLastError());
+  return RIP_OK;
+}
+
+extern "C" int rip_count(rip_pool *p, uint64_t num_sets, uint32_t *counts) {
+  if (!p || !counts || num_sets > p->num_sets) return RIP_ERR_INVALID;
+  rip_ctx *c = p->ctx;
+  CK(c, cudaSetDevice(c->device));
+  TRY(count_sets(p, num_sets));
+  CK(c, cudaMemcpyAsync(counts, p->count.p, sizeof(uint32_t) * p->g->n,
+                        cudaMemcpyDeviceToHost, c->stream));
+  CK(c, cudaStreamSynchronize(c->stream));
+  return RIP_OK;
+}
+
+// Counts left by the last rip_select (after its last update step).
+extern "C" int rip_select_counts(rip_pool *p, uint32_t *counts) {
+  if (!p || !counts) return RIP_ERR_INVALID;
+  if (!p->have_last_counts)
+    return set_err(p->ctx, RIP_ERR_STATE, "no selection has run on this pool");
+  TRY(settle_last_counts(p));
+  std::memcpy(counts, p->last_counts.data(), sizeof(uint32_t) * p->g->n);
+  return RIP_OK;
+}
+
+extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
+                          uint32_t *seeds, uint64_t *gains, uint32_t *num_seeds,
+                          double *f) {
+  if (!p || (k && !seeds) || !num_seeds) return RIP_ERR_INVALID;
+  rip_ctx *c = p->ctx;
+  if (S > p->num_sets)
+    return set_err(c, RIP_ERR_INVALID, "rip_select: %llu sets requested, pool has %llu",
+                   (unsigned long long)S, (unsigned long long)p->num_sets);
+  if (tiebreak != RIP_TIE_REF_HEAP && tiebreak != RIP_TIE_LOWEST_ID)
+    return set_err(c, RIP_ERR_INVALID, "rip_select: unknown tie-break %d", tiebreak);
+  if (S >= (1ull << 32))
+    return set_err(c, RIP_ERR_LIMIT, "rip_select: at most 2^32-1 sets");
+  CK(c, cudaSetDevice(c->device));
+  const uint32_t n = p->g->n;
+  *num_seeds = 0;
+  if (f) *f = 0.0;
+  CK(c, cudaEventRecord(c->ev0, c->stream));
+  const auto t_sel0 = clk::now();
+  // 1. histogram, 2. vertex -> sets index
+  p->have_last_counts = false;  // superseded by this selection
+  TRY(count_sets(p, S));
+  TRY(dalloc(c, p->inv_off, sizeof(uint64_t) * ((size_t)n + 1)));
+  TRY(dalloc(c, p->inv_cur, sizeof(uint64_t) * ((size_t)n + 1)));
+  TRY(dalloc(c, p->scan_sums, sizeof(uint64_t) * scan_block_sums_needed(n)));
+  launch_exclusive_scan(ptr<uint32_t>(p->count), ptr<uint64_t>(p->inv_off), n,
+                        ptr<uint64_t>(p->scan_sums), c->stream);
+  uint64_t P = 0;
+  CK(c, cudaMemcpyAsync(&P, ptr<uint64_t>(p->inv_off) + n, sizeof(uint64_t),
+                        cudaMemcpyDeviceToHost, c->stream));
+  CK(c, cudaMemcpyAsync(p->inv_cur.p, p->inv_off.p, sizeof(uint64_t) * ((size_t)n + 1),
+                        cudaMemcpyDeviceToDevice, c->stream));
+  CK(c, cudaStreamSynchronize(c->stream));
+  TRY(dalloc(c, p->inv, sizeof(uint32_t) * std::max<uint64_t>(P, 1)));
+  launch_build_inverted(p->view(), S, ptr<uint64_t>(p->inv_cur), ptr<uint32_t>(p->inv),
+                        c->num_sms * 8, c->stream);
+  CK(c, cudaGetLastError());
+  TRY(dalloc(c, p->covered, std::max<uint64_t>(S, 1)));
+  CK(c, cudaMemsetAsync(p->covered.p, 0, std::max<uint64_t>(S, 1), c->stream));
+
+  CoverLaunch C;
+  C.P = p->view();
+  C.inv_off = ptr<uint64_t>(p->inv_off);
+  C.inv = ptr<uint32_t>(p->inv);
+  C.covered = ptr<uint8_t>(p->covered);
+  C.count = ptr<uint32_t>(p->count);
+  C.blocks = c->num_sms * 4;
+
+  std::vector<uint32_t> &hcount = p->last_counts;
+  hcount.resize(n);
+  if (!c->h_cand) c->h_cand = new PinnedMem();
+  if (!c->h_count) c->h_count = new PinnedMem();
+  // mapped: candidate vertex ids in, their counts out (reference-heap picks)
+  constexpr uint32_t CAND_CAP = 1u << 16;
+  TRY(c->h_cand->ensure(c, 16 + 2 * sizeof(uint32_t) * (size_t)CAND_CAP, true));
+  TRY(c->h_count->ensure(c, sizeof(uint32_t) * (size_t)n));
+  PinnedMem &h_cand = *c->h_cand, &h_count = *c->h_count;
+
+  uint64_t uncovered = S;
+  std::vector<uint32_t> out_seeds;
+  std::vector<uint64_t> out_gains;
+
+  p->sel_prof[0] += ms_since(t_sel0);
+  p->sel_prof[6] += 1;
+  const int max_blocks = c->num_sms * 4;
+  unsigned char *hb = static_cast<unsigned char *>(h_cand.p);
+  unsigned char *db = static_cast<unsigned char *>(h_cand.dev);
+  // One pick: mark v's uncovered sets covered and decrement their members, one
+  // warp per set of v's inverted list (`gain` of them are still uncovered).
+  auto cover = [&](uint32_t v, uint64_t gain) -> int {
+    C.vertex = v;
+    C.blocks = (int)std::min<uint64_t>(max_blocks * 4, std::max<uint64_t>(1, (gain + 7) / 8));
+    launch_cover(C, c->stream);
+    CK(c, cudaGetLastError());
+    return RIP_OK;
+  };
+
+  if (tiebreak == RIP_TIE_REF_HEAP) {
+    const auto t_h0 = clk::now();
+    // InitHeapStorage + std::priority_queue(cmp, std::move(storage)), as the
+    // reference builds its heap (streaming_find_most_influential.h:541-544;
+    // counting.h:196-206): the same heap, built level-parallel on the device
+    // and downloaded into page-locked storage the queue adopts as is.
+    // The storage is the context's (page-locked once, reused by every pool);
+    // the guards hand it back on every way out of this block.
+    struct Lease {
+      rip_ctx *c;
+      std::vector<HeapItem> v;
+      explicit Lease(rip_ctx *c_) : c(c_), v(std::move(c_->heap_store)) {}
+      ~Lease() {
+        if (v.capacity()) c->heap_store = std::move(v);
+      }
+    } lease(c);
+    std::vector<HeapItem> &storage = lease.v;
+    if (storage.capacity() < n || !c->heap_registered) {
+      if (c->heap_registered) cudaHostUnregister(c->heap_registered);
+      c->heap_registered = nullptr;
+      std::vector<HeapItem>().swap(storage);
+      storage.reserve(n);
+      storage.resize(n);
+      if (cudaHostRegister(storage.data(), sizeof(HeapItem) * storage.capacity(), 0) ==
+          cudaSuccess) {
+        c->heap_registered = storage.data();
+      } else {
+        cudaGetLastError();  // pageable copy still works, only slower
+      }
+    }
+    storage.resize(n);
+    TRY(dalloc(c, p->d_heap, sizeof(uint2) * (size_t)n));
+    launch_make_heap(ptr<uint32_t>(p->count), n, ptr<uint2>(p->d_heap), c->stream);
+    CK(c, cudaGetLastError());
+    CK(c, cudaMemcpyAsync(storage.data(), p->d_heap.p, sizeof(uint2) * (size_t)n,
+                          cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    AdoptedQueue queue(std::move(storage));
+    struct Return {
+      rip_ctx *c;
+      AdoptedQueue &q;
+      ~Return() { c->heap_store = q.release(); }
+    } give_back{c, queue};
+    p->sel_prof[1] += ms_since(t_h0);
+    const auto t_p0 = clk::now();
+    // The lazy pops of a pick only read the current counts of heap items keyed
+    // at least the pick's gain m (keys are stale upper bounds of the counts and
+    // m is the largest count).  After each cover the host fetches the counts
+    // of the items keyed >= T for a guess T below the previous gain; if one of
+    // them still counts >= T, then m >= T and the fetch covers every item the
+    // pops can reach.  Otherwise their largest count c is a lower bound of m
+    // and a second fetch with T = c is exact.  A pop outside the fetched items
+    // (not expected) falls back to the whole count array.
+    uint32_t *h_ids = reinterpret_cast<uint32_t *>(hb + 16);
+    uint32_t *h_cnt = h_ids + CAND_CAP;
+    const uint32_t *d_ids = reinterpret_cast<const uint32_t *>(db + 16);
+    uint32_t *d_cnt = reinterpret_cast<uint32_t *>(db + 16) + CAND_CAP;
+    CountMap cmap;
+    std::vector<uint32_t> stack;
+    // First pick: every key is still exact, so only the top is examined.
+    bool fresh_all = false, first = true;
+    if (!queue.empty()) {
+      cmap.reset(1);
+      cmap.put(queue.top().first, queue.top().second);
+    }
+    double ratio = 0.9;   // recent gain ratio g_i / g_{i-1}
+    double margin = 0.9;  // guess = margin * ratio: lowered when a guess misses
+    auto fetch_all = [&]() -> int {
+      CK(c, cudaMemcpyAsync(h_count.p, p->count.p, sizeof(uint32_t) * (size_t)n,
+                            cudaMemcpyDeviceToHost, c->stream));
+      CK(c, cudaStreamSynchronize(c->stream));
+      std::memcpy(hcount.data(), h_count.p, sizeof(uint32_t) * (size_t)n);
+      fresh_all = true;
+      p->sel_prof[8] += 1;
+      return RIP_OK;
+    };
+    while (out_seeds.size() < k && uncovered != 0) {
+      const auto t_g0 = clk::now();
+      if (!first) {
+        const uint64_t g_prev = out_gains.back();
+        const double guess = p->cand_fixed ? p->cand_fixed / 100.0 : margin * ratio;
+        uint32_t T = (uint32_t)std::max<double>(1.0, std::floor((double)g_prev * guess));
+        for (int round = 0;; ++round) {
+          const auto t_c0 = clk::now();
+          const uint32_t nc = collect_at_least(queue.items(), T, CAND_CAP, h_ids, stack);
+          p->sel_prof[10] += ms_since(t_c0);
+          p->sel_prof[11] += 1;
+          if (nc > CAND_CAP) {
+            if (round == 0 && T < g_prev) {  // guess too low: raise it
+              T = (uint32_t)std::min<uint64_t>(g_prev, (uint64_t)T + (g_prev - T + 1) / 2);
+              continue;
+            }
+            TRY(fetch_all());
+            break;
+          }
+          launch_gather_counts(ptr<uint32_t>(p->count), d_ids, nc, d_cnt, c->stream);
+          CK(c, cudaGetLastError());
+          CK(c, cudaStreamSynchronize(c->stream));
+          p->sel_prof[5] += nc;
+          cmap.reset(nc);
+          uint32_t mc = 0;
+          for (uint32_t i = 0; i < nc; ++i) {
+            const uint32_t cv = *reinterpret_cast<volatile uint32_t *>(h_cnt + i);
+            cmap.put(h_ids[i], cv);
+            mc = std::max(mc, cv);
+          }
+          if (mc >= T || nc == queue.size()) {
+            if (round == 0) margin = std::min(0.97, margin + 0.01);
+            break;
+          }
+          T = std::max<uint32_t>(mc, 1u);  // mc <= m < T: exact next round
+          margin = std::max(0.5, margin - 0.05);
+        }
+      }
+      p->sel_prof[7] += ms_since(t_g0);
+      HeapItem element;
+      const auto t_q0 = clk::now();
+      for (;;) {  // getNextSeed, streaming_find_most_influential.h:560-571
+        if (queue.empty())
+          return set_err(c, RIP_ERR_STATE, "selection heap exhausted");
+        element = queue.top();
+        uint32_t cur = 0;
+        if (fresh_all) {
+          cur = hcount[element.first];
+        } else if (!cmap.get(element.first, cur)) {
+          TRY(fetch_all());
+          cur = hcount[element.first];
+        }
+        queue.pop();
+        p->sel_prof[3] += 1;
+        if (element.second > cur) {
+          element.second = cur;
+          queue.push(element);
+          continue;
+        }
+        break;
+      }
+      p->sel_prof[9] += ms_since(t_q0);
+      if (!out_gains.empty() && out_gains.back())
+        ratio = std::min(1.0, (double)element.second / (double)out_gains.back());
+      uncovered -= element.second;
+      out_seeds.push_back(element.first);
+      out_gains.push_back(element.second);
+      if (out_seeds.size() == k) break;
+      TRY(cover(element.first, element.second));
+      fresh_all = first = false;
+    }
+    p->sel_prof[2] += ms_since(t_p0);
+    p->sel_prof[4] += out_seeds.size();
+  } else if (k > 0 && S > 0) {
+    // Lowest-id picks entirely on the device: k pick launches (cached chunk
+    // maxima, lowest id on ties) and k - 1 cover launches, one read-back.
+    const uint32_t chunk = sel_chunk_vertices();
+    const uint32_t nchunks = (uint32_t)(((uint64_t)n + chunk - 1) / chunk);
+    TRY(dalloc(c, p->s_cmax, (size_t)nchunks * 8));
+    TRY(dalloc(c, p->s_dirty, (size_t)nchunks));
+    TRY(dalloc(c, p->s_best, (size_t)k * 8 + 256));
+    TRY(dalloc(c, p->s_desc, sizeof(SelDesc)));
+    TRY(p->h_best.ensure(c, (size_t)k * 8));
+    SelDesc d{};
+    d.P = p->view();
+    d.seg_off[0] = ptr<uint64_t>(p->inv_off);
+    d.seg_inv[0] = ptr<uint32_t>(p->inv);
+    d.seg_first[0] = 0;
+    d.nseg = 1;
+    d.S = S;
+    d.n = n;
+    d.nchunks = nchunks;
+    d.k = k;
+    d.keep_counts = 1;
+    d.count = ptr<uint32_t>(p->count);
+    d.cmax = ptr<unsigned long long>(p->s_cmax);
+    d.dirty = ptr<uint8_t>(p->s_dirty);
+    d.covered = ptr<uint8_t>(p->covered);
+    d.best = ptr<unsigned long long>(p->s_best);
+    d.done_blocks = reinterpret_cast<unsigned int *>(ptr<uint8_t>(p->s_best) + (size_t)k * 8);
+    d.acc = reinterpret_cast<unsigned long long *>(ptr<uint8_t>(p->s_best) + (size_t)k * 8 + 64);
+    d.total_elems = P;
+    CK(c, cudaMemcpyAsync(p->s_desc.p, &d, sizeof(d), cudaMemcpyHostToDevice, c->stream));
+    const SelDesc *dd = ptr<SelDesc>(p->s_desc);
+    const int pick_blocks = (int)std::max<uint32_t>(1, std::min<uint32_t>((nchunks + 7) / 8,
+                                                                          c->num_sms * 4));
+    // The pick loop runs as one CUDA graph, captured once per (k, buffers):
+    // kernels read everything through the descriptor; the final copy node
+    // holds the best / h_best addresses, so moving those drops the graph.
+    SelGraph &sg = p->sel_graph;
+    if (sg.exec && (sg.k != k || sg.src != p->s_best.p || sg.dst != p->h_best.p ||
+                    sg.desc != p->s_desc.p || sg.pick_blocks != pick_blocks)) {
+      cudaGraphExecDestroy(sg.exec);
+      sg.exec = nullptr;
+    }
+    if (!sg.exec) {
+      const uint64_t before = launch_counter();
+      cudaGraph_t graph = nullptr;
+      CK(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+      launch_sel_init(dd, c->num_sms, c->stream);
+      for (uint32_t i = 0; i < k; ++i) {
+        launch_sel_pick(dd, i, pick_blocks, c->stream);
+        if (i + 1 < k) launch_sel_cover(dd, i, max_blocks, c->stream);
+      }
+      cudaMemcpyAsync(p->h_best.p, p->s_best.p, (size_t)k * 8, cudaMemcpyDeviceToHost,
+                      c->stream);
+      const cudaError_t ce = cudaStreamEndCapture(c->stream, &graph);
+      sg.nodes = launch_counter() - before;
+      uncount_launches(sg.nodes);
+      if (ce != cudaSuccess)
+        return set_err(c, RIP_ERR_CUDA, "pick graph capture failed: %s", cudaGetErrorString(ce));
+      const cudaError_t ie = cudaGraphInstantiate(&sg.exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (ie != cudaSuccess) {
+        sg.exec = nullptr;
+        return set_err(c, RIP_ERR_CUDA, "pick graph instantiate failed: %s",
+                       cudaGetErrorString(ie));
+      }
+      sg.k = k;
+      sg.src = p->s_best.p;
+      sg.dst = p->h_best.p;
+      sg.desc = p->s_desc.p;
+      sg.pick_blocks = pick_blocks;
+    }
+    CK(c, cudaGraphLaunch(sg.exec, c->stream));
+    count_launches(sg.nodes);
+    CK(c, cudaStreamSynchronize(c->stream));
+    const unsigned long long *hb8 = static_cast<const unsigned long long *>(p->h_best.p);
+    for (uint32_t i = 0; i < k && uncovered != 0; ++i) {
+      const uint64_t cnt = hb8[i] >> 32;
+      if (cnt == 0) break;
+      uncovered -= cnt;
+      out_seeds.push_back(~(uint32_t)(hb8[i] & 0xFFFFFFFFull));
+      out_gains.push_back(cnt);
+    }
+  }
+  CK(c, cudaEventRecord(c->ev1, c->stream));
+  CK(c, cudaStreamSynchronize(c->stream));
+  float sms = 0.f;
+  cudaEventElapsedTime(&sms, c->ev0, c->ev1);
+  p->select_kernel_ms += sms;
+  p->have_last_counts = true;
+  p->last_counts_on_device = true;  // read back on demand (rip_select_counts)
+  for (size_t i = 0; i < out_seeds.size(); ++i) {
+    seeds[i] = out_seeds[i];
+    if (gains) gains[i] = out_gains[i];
+  }
+  *num_seeds = (uint32_t)out_seeds.size();
+  if (f) *f = S ? double(S - uncovered) / (double)S : 0.0;
+  return RIP_OK;
+}
+
