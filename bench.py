@@ -311,6 +311,7 @@ def main():
     rb._lib.check(rb._lib.lib.rip_ctx_stream(ctx.h, ctypes.byref(sp)), "rip_ctx_stream")
     stream = torch.cuda.ExternalStream(sp.value, device=torch.device("cuda", local))
     dg = rb.DeviceGraph(ctx, g, w["model"])
+    tune = dg.autotune(seed=1, pilot=2048) if w["model"] == "IC" else None  # setup, untimed
     pool = rb.Pool(dg)
     seed_base = replica_seed(rank, 0)
 
@@ -418,7 +419,9 @@ def main():
     alg_bytes = alg_bytes_of(st_tot)
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (kern_ms / 1e3) / 1e9 if kern_ms > 0 else None
-    kernel = "lt_walk_kernel" if w["model"] == "LT" else "ic_fused_kernel"
+    kernel = ("lt_walk_kernel" if w["model"] == "LT" else
+              "ic_fused_kernel" if tune and tune["name"].startswith("fused") else
+              "ic_plain_kernel")
     traffic = None
     prof = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(prof):
@@ -462,6 +465,7 @@ def main():
                                        "select": sel_ms / args.steps},
             "select_profile_per_step": {kk: vv / args.steps for kk, vv in sel_prof.items()},
             "sets_per_step": total_sets / args.steps,
+            "autotune": tune,
             "tiebreak": "reference CPU heap (CompareHeap lazy max-heap)",
             "lowest_id_tiebreak": {"value": low_value, "unit": "sets/s",
                                    "ms_per_step": low_ms / args.steps,
