@@ -362,3 +362,48 @@ def test_device_heap_is_libstdcxx_make_heap(ctx, n, max_count, seed):
     """rip_select builds its max-heap on the device; it must equal
     std::make_heap element for element (ties included)."""
     assert rb._lib.lib.rip_selftest_heap_device(ctx.h, n, max_count, seed) == 1
+
+
+@pytest.mark.parametrize("model", ["IC", "LT"])
+@pytest.mark.parametrize("case", ["no_edges", "pair", "triangle", "isolated_tail"])
+def test_corner_graphs_match_oracle(ctx, model, case):
+    """Graphs at the edges of the input space: no edges at all (every set is
+    its root), two and three vertices, and a small graph whose last vertices
+    have no in- or out-edges.  Sets, IMM seeds and theta equal the oracle's,
+    under every sampler and both tie-breaks."""
+    if case == "no_edges":
+        g = rb.HostGraph.from_edges(5, [], [], np.zeros(0, np.float32))
+    elif case == "pair":
+        g = rb.HostGraph.from_edges(2, [0, 1], [1, 0], np.array([0.9, 0.4], np.float32))
+    elif case == "triangle":
+        g = rb.HostGraph.from_edges(3, [0, 1, 2, 0], [1, 2, 0, 2],
+                                    np.array([0.7, 0.5, 1.0, 0.3], np.float32))
+    else:
+        e = rb.HostGraph.rmat(6, 256, seed=4)
+        src, dst = e.transpose_edges()
+        g = rb.HostGraph.from_edges(80, src, dst, np.full(len(src), 0.3, np.float32))
+    if model == "LT":
+        g = g.with_weights(rb.WEIGHTS_LT_NORMALIZED, seed=5) if g.m else g
+    thr = O.pack(model, g.index, g.weights)
+    samplers = [rb.SAMPLER_PLAIN, rb.SAMPLER_FUSED] if model == "IC" else [rb.SAMPLER_AUTO]
+    for sampler in samplers:
+        dg, p = device_pool(ctx, g, model)
+        p.sample(700, seed=2, sampler=sampler)
+        off, vtx = p.export()
+        ooff, ovtx, _ = O.sample(model, g.n, g.index, g.src, thr, 2, 0, 700)
+        assert_same_sets(off, vtx, ooff, ovtx)
+        for tie in (rb.TIE_REF_HEAP, rb.TIE_LOWEST_ID):
+            k = min(3, g.n)
+            f, seeds, gains = p.select(k + 2, tiebreak=tie)  # k beyond what can add coverage
+            of, oseeds, ogains, _ = O.select(g.n, off, vtx, k + 2, tie)
+            assert seeds.tolist() == oseeds.tolist() and f == of
+        p.close()
+        dg.close()
+    for tie in (rb.TIE_REF_HEAP, rb.TIE_LOWEST_ID):
+        dg = rb.DeviceGraph(ctx, g, model)
+        q = rb.Pool(dg)
+        seeds, rec = q.imm(2, 0.5, seed=3, tiebreak=tie)
+        o = O.imm(model, g.n, g.index, g.src, thr, 2, 0.5, seed=3, tiebreak=tie)
+        assert seeds.tolist() == o["seeds"] and rec.theta == o["theta"], (case, tie)
+        q.close()
+        dg.close()
