@@ -11,8 +11,9 @@
 //             colours that reached them last level) and count their in-edge
 //             groups;
 //   scan    : exclusive scan of the group counts (one global work list);
-//   expand  : one thread per aligned 4-edge group, its owner found by binary
-//             search in the scan; for every colour of the owner's mask one
+//   expand  : one thread per aligned 4-edge group, its owner found by one
+//             binary search per warp in the scan and a short walk per lane;
+//             for every colour of the owner's mask one
 //             Philox call flips the four edges' coins; live edges OR the
 //             colour into the source's visited mask, and colours new to it go
 //             to its pending mask and put it on the next level's frontier
@@ -120,14 +121,26 @@ __global__ void __launch_bounds__(256) giant_expand_kernel(GiantLaunch L, uint32
     for (int t = 0; t < 4; ++t)
 #pragma unroll
       for (int w = 0; w < CW; ++w) live[t][w] = 0;
-    if (valid) {
-      // owner: the last entry i with goff[i] <= j
-      uint32_t lo = 0, hi = nf;
-      while (hi - lo > 1) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (L.goff[mid] <= j) lo = mid;
-        else hi = mid;
+    // owner of j: the last entry i with goff[i] <= j.  One binary search per
+    // warp (for its first j), then each lane walks forward from there: the
+    // warp's 32 consecutive groups span few entries
+    uint32_t wlo = 0;
+    {
+      const uint64_t j0 = __shfl_sync(FULL, j, 0);
+      if (lane_id() == 0 && j0 < total) {
+        uint32_t lo = 0, hi = nf;
+        while (hi - lo > 1) {
+          const uint32_t mid = (lo + hi) >> 1;
+          if (L.goff[mid] <= j0) lo = mid;
+          else hi = mid;
+        }
+        wlo = lo;
       }
+      wlo = __shfl_sync(FULL, wlo, 0);
+    }
+    if (valid) {
+      uint32_t lo = wlo;
+      while (lo + 1 < nf && L.goff[lo + 1] <= j) ++lo;
       const uint32_t v = L.front[lo];
       const uint32_t beg = __ldg(L.G.off + v), end = __ldg(L.G.off + v + 1);
       const uint32_t g = (beg >> 2) + (uint32_t)(j - L.goff[lo]);
