@@ -237,12 +237,14 @@ int rip_select(rip_pool *p, uint64_t num_sets, uint32_t k, int tiebreak,
  * (the reference's known-answer test, test/cuda_find_most_influential.cc:84-167). */
 int rip_select_counts(rip_pool *p, uint32_t *counts);
 
-/* Diagnostic breakdown of the rip_select calls on this pool: out[0] ms in
- * counting/indexing kernels + count download, out[1] ms building the heap,
- * out[2] ms in the pick loop, out[3] heap pops, out[4] seeds picked,
- * out[5] (vertex, count) reports applied, out[6] selections, out[7] ms in
- * cover launches + syncs (includes out[8]), out[8] ms applying reports,
- * out[9] ms in heap pops. */
+/* Diagnostic breakdown of the rip_select calls on this pool: out[0] ms
+ * enqueueing the counting/indexing kernels, out[1] ms until the heap is on
+ * the host (includes those kernels), out[2] ms in the pick loop, out[3] heap
+ * pops, out[4] seeds picked, out[5] candidate counts fetched, out[6]
+ * selections, out[7] ms covering and fetching candidate counts (includes
+ * out[10]), out[8] fetches of the whole count array, out[9] ms in heap pops,
+ * out[10] ms collecting candidates on the host, out[11] fetch rounds.  The
+ * heap fields are those of the reference-heap tie-break. */
 int rip_select_profile(rip_pool *p, double out[12]);
 
 /* Diagnostic: builds a heap of n random (vertex, count) entries, counts in
