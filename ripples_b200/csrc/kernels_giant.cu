@@ -175,7 +175,9 @@ __global__ void __launch_bounds__(256) giant_expand_kernel(GiantLaunch L, uint32
       bool added = false;
 #pragma unroll
       for (int w = 0; w < CW; ++w) {
-        if (live[t][w]) {
+        // a plain read first: visited bits only get set, so colours it shows
+        // need no atomic (most live edges late in a giant BFS)
+        if (live[t][w] && (live[t][w] & ~__ldcg(&L.vis[(size_t)u[t] * CW + w]))) {
           const uint64_t old =
               atomicOr((unsigned long long *)&L.vis[(size_t)u[t] * CW + w], live[t][w]);
           const uint64_t add = live[t][w] & ~old;
