@@ -382,6 +382,7 @@ def main():
     d2h = 4 * w["k"]
 
     e2e_split = {"upload_ms": 0.0, "imm_ms": 0.0}
+    e2e_step_ms = []
 
     def e2e_step(step):
         t0 = time.perf_counter()
@@ -394,13 +395,16 @@ def main():
         n_sets = rec.TotalSets
         gen.pool.close()
         gen.graph.close()
+        t2 = time.perf_counter()
         e2e_split["upload_ms"] += 1e3 * (t1 - t0)
-        e2e_split["imm_ms"] += 1e3 * (time.perf_counter() - t1)
+        e2e_split["imm_ms"] += 1e3 * (t2 - t1)
+        e2e_step_ms.append(round(1e3 * (t2 - t0), 2))
         return n_sets, seeds
 
-    e2e_steps = max(1, min(args.steps, 3))
+    e2e_steps = max(1, min(args.steps, 10))
     e2e_step(-1)
     e2e_split.update(upload_ms=0.0, imm_ms=0.0)
+    e2e_step_ms.clear()
     barrier(world)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -450,7 +454,8 @@ def main():
                        "l2": "graph (%d MB) and pool exceed L2 (126 MB)" % ((g.m * 8 + g.n * 4) >> 20)},
             "e2e": {"value": e2e_value, "unit": "sets/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": e2e_steps,
-                    "split_ms_per_step": {kk: vv / e2e_steps for kk, vv in e2e_split.items()}},
+                    "split_ms_per_step": {kk: vv / e2e_steps for kk, vv in e2e_split.items()},
+                    "step_ms": e2e_step_ms},
             "roofline": {"bound": "hbm", "kernel": kernel,
                          "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
                          "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
@@ -810,6 +815,18 @@ def run_serve(args, w, world, rank, local):
     torch.cuda.synchronize()
     makespan = time.perf_counter() - t0
     clk = clocks.stop()
+    for i, q in enumerate(qs):  # per-query account on stderr
+        if not q.done:
+            continue
+        r = q.record
+        nr = min(r.num_rounds, 64)
+        gen = r.generate_ms + sum(r.round_generate_ms[j] for j in range(nr))
+        sel = r.select_ms + sum(r.round_select_ms[j] for j in range(nr))
+        s = spec[i]
+        _progress(t_run, f"query {i} ({s['scale']} {s['model']} k={s['k']} eps={s['eps']}): "
+                         f"status {q.status} theta {r.theta} elements {r.pool_elements} "
+                         f"rounds {r.num_rounds} latency {q.latency_ms:.0f} ms "
+                         f"queue {q.q.queue_ms:.0f} generate {gen:.0f} select {sel:.0f}")
     launches = int(rb._lib.lib.rip_kernel_launches() - launches0)
     ok = [q for q in qs if q.done and q.status == 0]
     lat = [1e3 * (sub_t[i] - arrivals[i]) + qs[i].latency_ms for i in range(N)

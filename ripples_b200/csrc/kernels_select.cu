@@ -80,6 +80,22 @@ __device__ __forceinline__ void for_each_element(const DevPool &P,
   }
 }
 
+// One occurrence per valid lane, called by all lanes of the warp.  When the
+// warp's 32 elements come from one set they are distinct vertices (a set
+// holds each vertex once) and every lane adds 1; otherwise lanes holding the
+// same vertex are grouped with __match_any_sync and one leader adds the group
+// size.  Lanes past the last element carry the last set's id.
+__device__ __forceinline__ void add_occurrence(uint32_t *count, uint64_t s, uint32_t v,
+                                               bool valid) {
+  if (__shfl_sync(FULL, s, 0) == __shfl_sync(FULL, s, 31)) {
+    if (valid) atomicAdd(count + v, 1u);
+    return;
+  }
+  const uint32_t peers = __match_any_sync(FULL, v);
+  if (valid && (__ffs(peers) - 1) == (int)lane_id())
+    atomicAdd(count + v, (uint32_t)__popc(peers));
+}
+
 __global__ void __launch_bounds__(256)
 count_kernel(DevPool P, uint64_t S, uint32_t *count) {
   const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
@@ -87,11 +103,7 @@ count_kernel(DevPool P, uint64_t S, uint32_t *count) {
   for (uint64_t wb = gw * 32; wb < S; wb += nw * 32) {
     for_each_element(
         P, wb, S, [](uint64_t i) { return i; },
-        [&](uint64_t, uint32_t v, bool valid) {
-          const uint32_t peers = __match_any_sync(FULL, v);
-          if (valid && (__ffs(peers) - 1) == (int)lane_id())
-            atomicAdd(count + v, (uint32_t)__popc(peers));
-        });
+        [&](uint64_t s, uint32_t v, bool valid) { add_occurrence(count, s, v, valid); });
   }
 }
 
@@ -103,6 +115,11 @@ inverted_kernel(DevPool P, uint64_t S, uint64_t *cursor, uint32_t *inv, uint64_t
     for_each_element(
         P, wb, S, [](uint64_t i) { return i; },
         [&](uint64_t s, uint32_t v, bool valid) {
+          if (__shfl_sync(FULL, s, 0) == __shfl_sync(FULL, s, 31)) {  // distinct vertices
+            if (valid)
+              inv[atomicAdd((unsigned long long *)cursor + v, 1ull)] = (uint32_t)(base + s);
+            return;
+          }
           const uint32_t peers = __match_any_sync(FULL, v);
           const uint32_t leader = __ffs(peers) - 1;
           unsigned long long b = 0;
@@ -181,10 +198,8 @@ __global__ void __launch_bounds__(256) sel_count_kernel(const SelDesc *__restric
   for (uint64_t wb = gw * 32; wb < d.S; wb += nw * 32) {
     for_each_element(
         d.P, wb, d.S, [](uint64_t i) { return i; },
-        [&](uint64_t, uint32_t v, bool valid) {
-          const uint32_t peers = __match_any_sync(FULL, v);
-          if (valid && (__ffs(peers) - 1) == (int)lane_id())
-            atomicAdd(d.count + v, (uint32_t)__popc(peers));
+        [&](uint64_t s, uint32_t v, bool valid) {
+          add_occurrence(d.count, s, v, valid);
           elems += valid ? 1 : 0;
         });
   }
@@ -319,11 +334,7 @@ __global__ void __launch_bounds__(256) sel_recount_kernel(const SelDesc *__restr
   for (uint64_t wb = gw * 32; wb < d.S; wb += nw * 32) {
     for_each_element(
         d.P, wb, d.S, [&](uint64_t x) { return d.covered[x] ? ~0ull : x; },
-        [&](uint64_t, uint32_t v, bool valid) {
-          const uint32_t peers = __match_any_sync(FULL, v);
-          if (valid && (__ffs(peers) - 1) == (int)lane_id())
-            atomicAdd(d.count + v, (uint32_t)__popc(peers));
-        });
+        [&](uint64_t s, uint32_t v, bool valid) { add_occurrence(d.count, s, v, valid); });
   }
 }
 

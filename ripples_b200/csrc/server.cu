@@ -13,7 +13,9 @@
 //
 // One tick advances every admitted query by one round:
 //   1. admit queued queries while slots are free and their estimated
-//      footprint (new sets x mean set size + selection buffers) fits;
+//      footprint (new sets x mean set size + selection buffers) fits; past
+//      a query that must wait, only queries whose resident pool already
+//      holds their estimated theta;
 //   2. sample every pool's shortfall in one multi-instance launch;
 //   3. extend each pool's vertex -> sets index to the sets it now holds;
 //   4. run each lowest-id query's round as one CUDA graph on its slot's
@@ -22,6 +24,7 @@
 //   5. advance each query's martingale; finished queries are written back.
 #include <deque>
 #include <map>
+#include <set>
 
 #include "host.h"
 
@@ -33,12 +36,16 @@ struct SelSlot {
   PinnedMem h_desc, h_best;
   uint32_t nchunk_cap = 0, k_cap = 0;
   uint64_t s_cap = 0;
-  // captured rounds by k: (graph, kernel nodes), oldest first.  Kernels read
+  // captured rounds by k and grid class: (graph, kernel nodes), oldest first.  Kernels read
   // every buffer through the descriptor, but the final copy node holds the
   // best / h_best addresses: reallocating those drops the captured rounds.
-  std::vector<std::pair<uint32_t, std::pair<cudaGraphExec_t, uint64_t>>> execs;
+  std::vector<std::pair<uint64_t, std::pair<cudaGraphExec_t, uint64_t>>> execs;
 };
 constexpr size_t MAX_GRAPHS_PER_SLOT = 8;
+// rounds over more elements than this run on full-occupancy grids
+constexpr double WIDE_ROUND_ELEMENTS = 64.0 * 1024 * 1024;
+// queued queries looked at per tick for admission
+constexpr size_t MAX_ADMISSION_SCAN = 1024;
 
 struct Active {
   rip_imm_query *q = nullptr;
@@ -75,6 +82,8 @@ struct rip_server {
   uint64_t ticks = 0, completed = 0, graph_launches = 0, suspended = 0;
   double tick_ms = 0, sample_ms = 0, index_ms = 0, select_ms = 0;
   std::map<rip_pool *, double> last_lb;  // per pool: LB of the last finished query
+  bool pressure = false;  // the last tick had a query waiting for memory
+  std::set<rip_imm_query *> resumed;  // suspended once: admitted only in arrival order
 };
 
 namespace {
@@ -113,6 +122,24 @@ uint64_t estimate_footprint(rip_server *s, rip_imm_query *q, rip_pool *p) {
   const double per_set = mean_set_size(p) * 8.0 + 12.0 + 1.0;
   const uint64_t grow = theta > p->num_sets ? theta - p->num_sets : 0;
   return (uint64_t)(per_set * (double)grow) + (uint64_t)n * 4 + theta + 8ull * q->k;
+}
+
+// The server's pool for (graph, seed) when one is resident, else null.
+rip_pool *resident_pool(rip_server *s, rip_graph *g, uint64_t seed) {
+  for (auto &e : s->pools)
+    if (e.first.first == g && e.first.second == seed) return e.second;
+  return nullptr;
+}
+
+// True when the pool already holds the theta the query is estimated to need
+// (from the lower bound of the last query that finished on the pool).
+bool holds_estimate(rip_server *s, rip_imm_query *q, rip_pool *p) {
+  auto it = s->last_lb.find(p);
+  if (it == s->last_lb.end() || !(it->second > 0)) return false;
+  const uint64_t n = q->graph->n;
+  const double lp = q->l * (1 + 1 / std::log2((double)n));
+  const uint64_t theta = rip_theta(q->epsilon, lp, q->k, it->second, n);
+  return theta + theta / 4 <= p->num_sets;  // a margin: the bound came from another k
 }
 
 int slot_buffers(rip_server *s, SelSlot &sl, uint32_t nchunks, uint64_t S, uint32_t k) {
@@ -230,8 +257,14 @@ int launch_round(rip_server *s, Active &a) {
   hd->acc = reinterpret_cast<unsigned long long *>(ptr<uint8_t>(sl.ctr) + 64);
   hd->total_elems = 0;
   CK(c, cudaMemcpyAsync(sl.desc.p, hd, sizeof(SelDesc), cudaMemcpyHostToDevice, sl.st));
+  // Rounds over many elements take full-occupancy grids for the count and
+  // the covers (one such round fills the device by itself); small rounds
+  // keep small grids so that many slots' rounds share the device.  The
+  // captured rounds are keyed by k and the grid class.
+  const bool wide = mean_set_size(p) * (double)a.S > WIDE_ROUND_ELEMENTS;
+  const uint64_t key = (uint64_t)k | (wide ? 1ull << 32 : 0ull);
   size_t gi = 0;
-  while (gi < sl.execs.size() && sl.execs[gi].first != k) ++gi;
+  while (gi < sl.execs.size() && sl.execs[gi].first != key) ++gi;
   if (gi == sl.execs.size()) {
     if (sl.execs.size() == MAX_GRAPHS_PER_SLOT) {
       cudaGraphExecDestroy(sl.execs.front().second.first);
@@ -239,14 +272,16 @@ int launch_round(rip_server *s, Active &a) {
     }
     const SelDesc *d = ptr<SelDesc>(sl.desc);
     const int blocks = std::max(8, c->num_sms / 2);
+    const int count_blocks = wide ? c->num_sms * 8 : blocks * 2;
+    const int cover_blocks = wide ? c->num_sms * 4 : blocks;
     const uint64_t before = launch_counter();
     cudaGraph_t g = nullptr;
     CK(c, cudaStreamBeginCapture(sl.st, cudaStreamCaptureModeThreadLocal));
     launch_sel_init(d, blocks, sl.st);
-    launch_sel_count(d, blocks * 2, sl.st);
+    launch_sel_count(d, count_blocks, sl.st);
     for (uint32_t i = 0; i < k; ++i) {
       launch_sel_pick(d, i, blocks, sl.st);
-      if (i + 1 < k) launch_sel_cover(d, i, blocks, sl.st);
+      if (i + 1 < k) launch_sel_cover(d, i, cover_blocks, sl.st);
     }
     cudaMemcpyAsync(sl.h_best.p, sl.best.p, (size_t)k * 8, cudaMemcpyDeviceToHost, sl.st);
     const cudaError_t e = cudaStreamEndCapture(sl.st, &g);
@@ -261,7 +296,7 @@ int launch_round(rip_server *s, Active &a) {
     if (ie != cudaSuccess)
       return set_err(c, RIP_ERR_CUDA, "selection graph instantiate failed: %s",
                      cudaGetErrorString(ie));
-    sl.execs.push_back({k, {exec, nodes}});
+    sl.execs.push_back({key, {exec, nodes}});
     gi = sl.execs.size() - 1;
   }
   CK(c, cudaGraphLaunch(sl.execs[gi].second.first, sl.st));
@@ -302,6 +337,7 @@ void finish(rip_server *s, Active &a, int status) {
   }
   q->latency_ms = ms_since(a.t_sub);
   q->done = 1;
+  s->resumed.erase(q);
   s->completed++;
   s->admitted_bytes -= std::min(s->admitted_bytes, a.footprint);
   if (a.slot >= 0) s->free_slots.push_back(a.slot);
@@ -314,6 +350,7 @@ void suspend(rip_server *s, Active &a) {
   s->admitted_bytes -= std::min(s->admitted_bytes, a.footprint);
   if (a.slot >= 0) s->free_slots.push_back(a.slot);
   s->queue.push_back({a.q, a.t_sub});
+  s->resumed.insert(a.q);
   s->suspended++;
   for (const Active &b : s->active)
     if (&b != &a && b.pool == a.pool) return;
@@ -490,36 +527,73 @@ extern "C" int rip_server_tick(rip_server *s, uint32_t *completed) {
   CK(c, cudaSetDevice(c->device));
   const auto t_tick = clk::now();
   uint32_t done_now = 0;
-  // 1. admission
-  while (!s->queue.empty() && !s->free_slots.empty()) {
-    rip_imm_query *q = s->queue.front().first;
+  // 1. admission, in arrival order.  Once a query has to wait (no room for
+  // its pool to grow), later queries are still admitted when their pool is
+  // resident and already holds the theta their estimate asks for: they add
+  // selection buffers only, so they cannot delay the waiting query's growth.
+  // Not while the last tick had a query waiting for memory: the waiting
+  // queries drain first (suspension frees pools), so a suspended query is
+  // not taken straight back.
+  bool head_waits = false;
+  size_t scanned = 0;
+  for (auto it = s->queue.begin();
+       it != s->queue.end() && !s->free_slots.empty() && scanned < MAX_ADMISSION_SCAN;
+       ++scanned) {
+    rip_imm_query *q = it->first;
     const bool bad = !q->graph || q->graph->ctx != c || q->k == 0 || !q->seeds ||
                      !(q->epsilon > 0) || q->graph->n < 2 ||
                      (q->tiebreak != RIP_TIE_LOWEST_ID && q->tiebreak != RIP_TIE_REF_HEAP);
     Active a;
     a.q = q;
-    a.t_sub = s->queue.front().second;
+    a.t_sub = it->second;
     if (bad) {
-      s->queue.pop_front();
+      it = s->queue.erase(it);
       a.t_start = clk::now();
       finish(s, a, RIP_ERR_INVALID);
       ++done_now;
       continue;
     }
-    // admitted while its estimated footprint fits and the device is not
-    // already mostly in use (resident pools stay: later queries reuse them);
-    // always when nothing else is admitted
-    if (!s->active.empty() && in_use(c) > c->budget / 20 * 17) break;
     rip_pool *p = nullptr;
-    TRY(pool_for(s, q->graph, q->seed, &p));
-    if (p->num_sets == 0) {  // a first slice of the pool measures its mean set size
-      const int r = rip_sample(p, q->seed, 256, RIP_SAMPLER_AUTO);
-      if (out_of_room(r) && !s->active.empty()) break;
-      if (r != RIP_OK && !out_of_room(r)) return r;
+    uint64_t fp = 0;
+    if (!head_waits) {
+      // admitted while its estimated footprint fits and the device is not
+      // already mostly in use (resident pools stay: later queries reuse
+      // them); always when nothing else is admitted
+      if (!s->active.empty() && in_use(c) > c->budget / 20 * 17) {
+        head_waits = true;
+        ++it;
+        continue;
+      }
+      TRY(pool_for(s, q->graph, q->seed, &p));
+      if (p->num_sets == 0) {  // a first slice of the pool measures its mean set size
+        const int r = rip_sample(p, q->seed, 256, RIP_SAMPLER_AUTO);
+        if (out_of_room(r) && !s->active.empty()) {
+          head_waits = true;
+          ++it;
+          continue;
+        }
+        if (r != RIP_OK && !out_of_room(r)) return r;
+      }
+      fp = estimate_footprint(s, q, p);
+      if (!s->active.empty() && s->admitted_bytes + fp > s->budget) {
+        head_waits = true;
+        ++it;
+        continue;
+      }
+    } else {
+      if (s->pressure) break;
+      p = resident_pool(s, q->graph, q->seed);
+      if (!p || s->resumed.count(q) || !holds_estimate(s, q, p)) {
+        ++it;
+        continue;
+      }
+      fp = estimate_footprint(s, q, p);
+      if (s->admitted_bytes + fp > s->budget) {
+        ++it;
+        continue;
+      }
     }
-    const uint64_t fp = estimate_footprint(s, q, p);
-    if (!s->active.empty() && s->admitted_bytes + fp > s->budget) break;
-    s->queue.pop_front();
+    it = s->queue.erase(it);
     a.pool = p;
     a.slot = s->free_slots.back();
     s->free_slots.pop_back();
@@ -686,8 +760,10 @@ extern "C" int rip_server_tick(rip_server *s, uint32_t *completed) {
   // memory, the one asking for the most sets is suspended (or, alone, ends).
   bool progress = false;
   size_t worst = 0;
+  s->pressure = false;
   for (size_t i = 0; i < s->active.size(); ++i) {
     if (!s->active[i].stalled) progress = true;
+    else s->pressure = true;
     if (s->active[i].S > s->active[worst].S) worst = i;
   }
   std::vector<Active> keep;
