@@ -592,12 +592,13 @@ def run_batch(args, w, world, rank, local):
         out, t0 = [], time.perf_counter()
         for x in inst:
             p = rb.Pool(graphs[x["g"]]["dg"])
+            ti = time.perf_counter()
             try:
                 seeds, rec = p.imm(x["k"], x["eps"], seed=x["seed"] + tag,
                                    tiebreak=rb.TIE_LOWEST_ID, sampler=rb.SAMPLER_PLAIN)
-                out.append((seeds, rec.total_sets))
+                out.append((seeds, rec.total_sets, 1e3 * (time.perf_counter() - ti)))
             except rb.RipError:
-                out.append((None, 0))
+                out.append((None, 0, 1e3 * (time.perf_counter() - ti)))
             p.close()
             if limit_s and time.perf_counter() - t0 > limit_s:
                 break
@@ -631,6 +632,16 @@ def run_batch(args, w, world, rank, local):
     first = batched(0)
     same = all(np.array_equal(a[0], q.seeds) for a, q in zip(pl, first)
                if a[0] is not None and q.status == 0)
+    for j, q in enumerate(first):  # per-instance account on stderr
+        x, gd, r = inst[j], graphs[inst[j]["g"]], q.record
+        nr = min(r.num_rounds, 64)
+        gen = r.generate_ms + sum(r.round_generate_ms[i] for i in range(nr))
+        sel = r.select_ms + sum(r.round_select_ms[i] for i in range(nr))
+        pms = f"{pl[j][2]:.0f}" if j < len(pl) else "-"
+        print(f"instance {j} ({gd['scale']} {gd['kind']} deg {gd['deg']} {gd['model']} "
+              f"k={x['k']} eps={x['eps']:.2f}): status {q.status} theta {r.theta} "
+              f"elements {r.pool_elements} rounds {r.num_rounds} batched {r.total_ms:.0f} ms "
+              f"(generate {gen:.0f} select {sel:.0f}) plain {pms} ms", file=sys.stderr)
     p_failed = sum(1 for a in pl if a[0] is None)
     p_sets = sum(x[1] for x in pl)
     line = {"metric": "RRR sets/s (64 batched IMM instances)", "value": sets / t_b,
