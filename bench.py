@@ -57,6 +57,12 @@ WORKLOADS = {
     # (one set per warp, fused 64/128/256 colours) on the same fixed set range
     "p3": dict(name="imm_ic_rmat24_deg32_wc_k100_eps0.13", kind="p3", scale=24,
                draws=32 << 24, model="IC", k=100, eps=0.13),
+    # forward Monte Carlo spread (rip_spread_ic) of the 50 vertices of largest
+    # out-degree on R-MAT 2^20 (16*2^20 draws, IC p ~ U(0,0.1)), 20000
+    # replicas a step; the reference's own simulator timed beside it
+    "spread": dict(name="spread_ic_rmat20_deg16_k50", kind="spread", scale=20,
+                   draws=16 << 20, model="IC", weights="uniform_0_0.1", k=50,
+                   replicas=20000),
 }
 METRIC = "RRR sets/s (full IMM)"
 
@@ -292,6 +298,8 @@ def main():
         return run_serve(args, w, world, rank, local)
     if w.get("kind") == "p3":
         return run_p3(args, w, world, rank, local)
+    if w.get("kind") == "spread":
+        return run_spread(args, w, world, rank, local)
     if args.impl == "reference":
         rc = reference_arm(args, w, world, rank)
         if world > 1:
@@ -740,6 +748,95 @@ def run_p3(args, w, world, rank, local):
             "clocks": clk}
     print(json.dumps(line))
     pool.close()
+    ctx.close()
+    return 0
+
+
+def run_spread(args, w, world, rank, local):
+    import ctypes
+    import numpy as np
+    import torch
+    import ripples_b200 as rb
+    if _not_on_rank0(world, rank, args, w):
+        return 0
+    torch.cuda.set_device(local)
+    g = build_graph(w)
+    f = g.forward()
+    ctx = rb.Context(local)
+    sp = ctypes.c_void_p()
+    rb._lib.check(rb._lib.lib.rip_ctx_stream(ctx.h, ctypes.byref(sp)), "rip_ctx_stream")
+    stream = torch.cuda.ExternalStream(sp.value, device=torch.device("cuda", local))
+    dg = rb.DeviceGraph(ctx, f, "IC")
+    outdeg = np.diff(f.index).astype(np.int64)
+    seeds = np.lexsort((np.arange(g.n), -outdeg))[: w["k"]].astype(np.uint32)
+    R = w["replicas"]
+    for i in range(args.warmup):
+        rb.spread_ic(dg, seeds, R // 10, seed=1000 + i)
+    launches0 = rb._lib.lib.rip_kernel_launches()
+    clocks = ClockSampler(local)
+    clocks.start()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    means, dev_ms, wall = [], 0.0, 0.0
+    for step in range(args.steps):
+        t0 = time.perf_counter()
+        ev0.record(stream)
+        means.append(rb.spread_ic(dg, seeds, R, seed=step))
+        ev1.record(stream)
+        ev1.synchronize()
+        wall += time.perf_counter() - t0
+        dev_ms += ev0.elapsed_time(ev1)
+    clk = clocks.stop()
+    launches = int(rb._lib.lib.rip_kernel_launches() - launches0)
+    # algorithmic bytes of one replica: 8 (two offsets) + 8 per out-edge
+    # record of every reached vertex.  The oracle reproduces replicas 0..7 of
+    # step 0 bit for bit, and their reached vertices' out-edges give the mean.
+    from oracle import oracle as O
+    thr = O.pack("IC", f.index, f.weights)
+    sample_reps = 8
+    s_mean, _, s_edges = O.spread_ic(f.n, f.index, f.src, thr, seeds, sample_reps, seed=0,
+                                     with_edges=True)
+    alg_per_replica = 8.0 * s_mean + 8.0 * s_edges / sample_reps
+    mean = float(np.mean(means))
+    value = R * args.steps / (dev_ms / 1e3)
+    peak, peak_kind = measured_peaks()
+    # the reference's simulator (ripples::simulate) on one host core, a
+    # bounded sample of replicas
+    cpu = None
+    if O.reference() is not None:
+        tmpd = tempfile.mkdtemp()
+        path = os.path.join(tmpd, "fwd.bin")
+        g.write_binary(path, backward=False)
+        reps_cpu = 20
+        t0 = time.perf_counter()
+        ref_mean = O.reference().ref_simulate(path.encode(), 0, seeds.ctypes.data, len(seeds),
+                                              reps_cpu, 0)
+        t_cpu = time.perf_counter() - t0
+        shutil.rmtree(tmpd, ignore_errors=True)
+        cpu = {"value": reps_cpu / t_cpu, "unit": "replicas/s", "cores": 1, "kind": "reference",
+               "sample": f"{reps_cpu} replicas of ripples::simulate (IC) on the same graph and "
+                         f"seeds, {1e3 * t_cpu:.0f} ms; its mean spread {ref_mean:.1f}"}
+    line = {"metric": "IC spread replicas/s (forward Monte Carlo)", "value": value,
+            "unit": "replicas/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
+            "scaling": "replicas only", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic R-MAT graph (seed 0) and weights (seed 1), forward CSR",
+            "config": {"workload": w["name"], "n": g.n, "m": g.m, "k": w["k"],
+                       "replicas_per_step": R,
+                       "l2": "graph (130 MB) exceeds L2 (126 MB); per-CTA bitmaps and queues"},
+            "mean_spread": mean, "reached_vertices_per_s": mean * value,
+            "e2e": {"value": R * args.steps / wall, "unit": "replicas/s",
+                    "h2d_bytes_per_step": 4 * len(seeds), "d2h_bytes_per_step": 8,
+                    "note": "one rip_spread_ic call per step: seeds in, mean out"},
+            "roofline": {"bound": "hbm", "kernel": "ic_spread_kernel",
+                         "achieved": alg_per_replica * value / 1e9, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s",
+                         "frac": alg_per_replica * value / 1e9 / peak, "traffic": None,
+                         "alg_bytes_per_replica": alg_per_replica,
+                         "alg_note": "mean over replicas 0-7 of step 0 (oracle, bit-exact)"},
+            "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches}
+    print(json.dumps(line))
+    dg.close()
     ctx.close()
     return 0
 

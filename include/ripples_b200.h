@@ -292,6 +292,23 @@ int rip_imm_pool(rip_pool *p, uint32_t k, double epsilon, double l,
                  uint64_t seed, int tiebreak, int sampler, uint32_t *seeds,
                  uint32_t *num_seeds, rip_imm_record *record);
 
+/* ---- spread of a seed set ------------------------------------------------- */
+/* Forward Monte Carlo spread under IC: the mean number of vertices a seed set
+ * reaches (seeds included) over `replicas` independent cascades, as the
+ * replica loop of tools/simulator.cc:139-149 over ripples::simulate
+ * (include/ripples/diffusion_simulation.h:73-127) measures it.
+ *   g       : an IC graph uploaded with the FORWARD CSR -- index over source
+ *             vertices, src[] holding each out-edge's target, weights p(u->v)
+ *             (rip_graph_upload's arrays for the transposed graph).
+ *   seeds   : k vertex ids < n (a repeated id counts once).
+ *   sizes   : optional host array of `replicas` entries: the reached count of
+ *             each replica.  Replica r is a pure function of (seed, r).
+ * Edge e fires in replica r iff P(e>>2, r; seed, SIM_IC)[e&3] < threshold(e):
+ * the same distribution as the reference's uniform01 <= p(u->v) draws, not the
+ * same draws.  Returns RIP_ERR_INVALID for an LT graph or a seed >= n. */
+int rip_spread_ic(rip_graph *g, const uint32_t *seeds, uint32_t k,
+                  uint64_t replicas, uint64_t seed, uint32_t *sizes, double *spread);
+
 /* ---- batching and serving --------------------------------------------------- */
 /* No counterpart in the reference (its GenerateRRRSets, include/ripples/
  * generate_rrr_sets.h:60-120, fills one instance's sets per call).  Extends

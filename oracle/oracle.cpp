@@ -25,6 +25,8 @@
 //     so equal-count ties resolve identically.
 //   * The lowest-id argmax tie-break of the reference's GPU seed selection,
 //     src/gpu/find_most_influential.cc:65-72 (thrust::max_element).
+//   * Forward IC spread of a seed set, replica by replica:
+//     include/ripples/diffusion_simulation.h:73-127 (run_simulation, IC).
 //   * IMM theta math and the martingale loop: include/ripples/imm.h:77-128
 //     (ThetaPrime, InvThetaPrime, Theta), :145-260 (Sampling), :768-860 (IMM),
 //     include/ripples/utility.h:84-87 (logBinomial).
@@ -54,7 +56,7 @@
 
 namespace {
 
-enum : uint32_t { DOM_ROOT = 1, DOM_IC = 2, DOM_LT = 3 };
+enum : uint32_t { DOM_ROOT = 1, DOM_IC = 2, DOM_LT = 3, DOM_SIM_IC = 7 };
 
 void philox4x32_10(const uint32_t ctr_in[4], const uint32_t key_in[2],
                    uint32_t out[4]) {
@@ -109,6 +111,19 @@ uint32_t ic_coin(uint64_t seed, uint64_t s, uint64_t e) {
   ctr[1] = (uint32_t)(g >> 32);
   ctr[2] = (uint32_t)s;
   ctr[3] = (DOM_IC << 24) | (uint32_t)((s >> 32) & 0xFFFFFFu);
+  philox4x32_10(ctr, key, out);
+  return out[e & 3];
+}
+
+// Forward spread simulation coin of edge e in replica r (its own domain).
+uint32_t sim_ic_coin(uint64_t seed, uint64_t r, uint64_t e) {
+  uint32_t key[2], ctr[4], out[4];
+  make_key(seed, key);
+  uint64_t g = e >> 2;
+  ctr[0] = (uint32_t)g;
+  ctr[1] = (uint32_t)(g >> 32);
+  ctr[2] = (uint32_t)r;
+  ctr[3] = (DOM_SIM_IC << 24) | (uint32_t)((r >> 32) & 0xFFFFFFu);
   philox4x32_10(ctr, key, out);
   return out[e & 3];
 }
@@ -395,6 +410,45 @@ void *orc_sample(int model, uint32_t n, const uint64_t *index,
     stats[1] = st.edges_scanned;
   }
   return p;
+}
+
+// Forward IC spread: replica r is a BFS from the seeds over the forward CSR
+// (index over sources, dst[e] the target of out-edge e) in which edge e fires
+// iff sim_ic_coin(seed, r, e) < thr[e]; sizes[r] = vertices reached, seeds
+// included (include/ripples/diffusion_simulation.h:73-127).  Returns the sum
+// of the sizes; *edges (optional) = out-edges of reached vertices, summed.
+uint64_t orc_spread_ic(uint32_t n, const uint64_t *index, const uint32_t *dst,
+                       const uint32_t *thr, const uint32_t *seeds, uint32_t k,
+                       uint64_t replicas, uint64_t seed, uint32_t *sizes,
+                       uint64_t *edges) {
+  uint64_t n_edges = 0;
+  std::vector<uint64_t> stamp(n, ~0ull);
+  std::vector<uint32_t> queue;
+  uint64_t total = 0;
+  for (uint64_t r = 0; r < replicas; ++r) {
+    queue.clear();
+    for (uint32_t i = 0; i < k; ++i)
+      if (stamp[seeds[i]] != r) {
+        stamp[seeds[i]] = r;
+        queue.push_back(seeds[i]);
+      }
+    for (size_t head = 0; head < queue.size(); ++head) {
+      const uint32_t u = queue[head];
+      n_edges += index[u + 1] - index[u];
+      for (uint64_t e = index[u]; e < index[u + 1]; ++e) {
+        const uint32_t v = dst[e];
+        if (stamp[v] == r) continue;  // coins are pure: skipping is exact
+        if (sim_ic_coin(seed, r, e) < thr[e]) {
+          stamp[v] = r;
+          queue.push_back(v);
+        }
+      }
+    }
+    if (sizes) sizes[r] = (uint32_t)queue.size();
+    total += queue.size();
+  }
+  if (edges) *edges = n_edges;
+  return total;
 }
 
 uint64_t orc_pool_elements(void *h) { return ((Pool *)h)->vtx.size(); }

@@ -43,6 +43,7 @@ def _load_oracle() -> ctypes.CDLL:
         "orc_pack_ic": (None, [P, U64, P]),
         "orc_pack_lt": (None, [P, U32, P, P]),
         "orc_sample": (P, [I32, U32, P, P, P, U64, U64, U64, P]),
+        "orc_spread_ic": (U64, [U32, P, P, P, P, U32, U64, U64, P, ctypes.POINTER(U64)]),
         "orc_pool_elements": (U64, [P]),
         "orc_pool_sets": (U64, [P]),
         "orc_pool_copy": (None, [P, P, P]),
@@ -109,6 +110,32 @@ def sample(model: str, n: int, index: np.ndarray, src: np.ndarray, thr: np.ndarr
     L.orc_pool_copy(h, _ptr(off), _ptr(vtx))
     L.orc_pool_free(h)
     return off, vtx[:ne], st
+
+
+def spread_ic(n: int, index: np.ndarray, dst: np.ndarray, thr: np.ndarray, seeds,
+              replicas: int, seed: int = 0, with_edges: bool = False):
+    """Forward IC spread over the forward CSR (index over sources, dst the
+    out-edge targets, IC thresholds): (mean reached count, per-replica
+    counts), plus the out-edges of the reached vertices summed over the
+    replicas with ``with_edges``."""
+    idx = np.ascontiguousarray(index, dtype=np.uint64)
+    d = np.ascontiguousarray(dst, dtype=np.uint32)
+    t = np.ascontiguousarray(thr, dtype=np.uint32)
+    if d.size == 0:
+        d = np.zeros(1, np.uint32)
+        t = np.zeros(1, np.uint32)
+    sd = np.ascontiguousarray(seeds, dtype=np.uint32)
+    k = int(sd.size)
+    if k == 0:
+        sd = np.zeros(1, np.uint32)
+    sizes = np.zeros(max(replicas, 1), dtype=np.uint32)
+    edges = ctypes.c_uint64()
+    total = L.orc_spread_ic(n, _ptr(idx), _ptr(d), _ptr(t), _ptr(sd), k, replicas, seed,
+                            _ptr(sizes), ctypes.byref(edges))
+    mean = total / replicas if replicas else 0.0
+    if with_edges:
+        return mean, sizes[:replicas], edges.value
+    return mean, sizes[:replicas]
 
 
 def select(n: int, offsets: np.ndarray, vertices: np.ndarray, k: int, tiebreak: int = 0):

@@ -1,0 +1,139 @@
+// kernels_spread.cu -- forward Monte Carlo spread of a seed set under IC.
+//
+// The reference measures the quality of a seed set with ripples::simulate
+// (include/ripples/diffusion_simulation.h:73-127, driven replica by replica
+// by tools/simulator.cc): a BFS from the seeds over the forward graph in
+// which edge u -> v fires with probability p(u -> v), the spread being the
+// number of vertices reached, seeds included.  Here one 1024-thread CTA runs
+// one replica at a time with the level loop of the one-CTA-per-heavy-set
+// sampler: a level's entries are taken 1024 at a time, a block scan turns
+// their 4-edge group counts into offsets and all warps stride over the
+// concatenated groups.  The coin of forward edge e in replica r is
+// sim_ic_coins(key, e >> 2, r)[e & 3]: a replica's reached set is a pure
+// function of (seed, r), whatever the visiting order.
+#include "device.cuh"
+#include "launch.h"
+
+namespace rip {
+
+namespace {
+
+constexpr int SIM_THREADS = 1024;
+constexpr int SIM_WARPS = SIM_THREADS / 32;
+
+__device__ uint32_t sim_block_scan(uint32_t x, uint32_t *warp_tot, uint32_t *total) {
+  const uint32_t lane = lane_id(), wid = threadIdx.x >> 5;
+  const uint32_t incl = warp_incl_scan(x);
+  if (lane == 31) warp_tot[wid] = incl;
+  __syncthreads();
+  if (wid == 0) {
+    const uint32_t t = lane < SIM_WARPS ? warp_tot[lane] : 0u;
+    const uint32_t ti = warp_incl_scan(t);
+    if (lane < SIM_WARPS) warp_tot[lane] = ti - t;
+    if (lane == 31) *total = ti;
+  }
+  __syncthreads();
+  const uint32_t r = warp_tot[wid] + incl - x;
+  __syncthreads();
+  return r;
+}
+
+__global__ void __launch_bounds__(SIM_THREADS)
+ic_spread_kernel(SpreadLaunch L) {
+  __shared__ uint32_t s_off[SIM_THREADS + 1];
+  __shared__ uint32_t s_beg[SIM_THREADS], s_end[SIM_THREADS];
+  __shared__ uint32_t s_warp[SIM_WARPS];
+  __shared__ uint32_t s_qlen, s_total;
+  __shared__ unsigned long long s_rep;
+
+  const uint32_t tid = threadIdx.x;
+  uint32_t *bm = L.bitmaps + (size_t)blockIdx.x * L.bm_words;
+  uint32_t *q = L.queues + (size_t)blockIdx.x * L.qcap;
+  unsigned long long reached = 0;
+
+  for (;;) {
+    if (tid == 0) {
+      s_rep = atomicAdd(L.next, 1ull);
+      s_qlen = 0;
+    }
+    __syncthreads();
+    const uint64_t r = s_rep;
+    if (r >= L.replicas) break;
+    // the seeds are the first level (a repeated seed is queued once)
+    for (uint32_t i = tid; i < L.k; i += SIM_THREADS) {
+      const uint32_t v = L.seeds[i];
+      const uint32_t bit = 1u << (v & 31);
+      if (!(atomicOr(&bm[v >> 5], bit) & bit)) {
+        const uint32_t pos = atomicAdd(&s_qlen, 1u);
+        if (pos < L.qcap) q[pos] = v;
+      }
+    }
+    __syncthreads();
+    uint32_t lo = 0, hi = min(s_qlen, L.qcap);
+    while (lo < hi) {
+      for (uint32_t cb = lo; cb < hi; cb += SIM_THREADS) {
+        const uint32_t e = cb + tid;
+        uint32_t beg = 0, end = 0;
+        if (e < hi) {
+          const uint32_t v = q[e];
+          beg = __ldg(L.G.off + v);
+          end = __ldg(L.G.off + v + 1);
+        }
+        s_beg[tid] = beg;
+        s_end[tid] = end;
+        const uint32_t ng = group_count(beg, end);
+        s_off[tid] = sim_block_scan(ng, s_warp, &s_total);
+        if (tid == 0) s_off[SIM_THREADS] = s_total;
+        __syncthreads();
+        const uint32_t total = s_off[SIM_THREADS];
+        for (uint32_t j = tid; j < total; j += SIM_THREADS) {
+          uint32_t a = 0, b = SIM_THREADS;  // entry a: s_off[a] <= j < s_off[a + 1]
+          while (b - a > 1) {
+            const uint32_t mid = (a + b) >> 1;
+            if (s_off[mid] <= j) a = mid;
+            else b = mid;
+          }
+          const uint32_t ob = s_beg[a], oe = s_end[a];
+          const uint32_t g = (ob >> 2) + (j - s_off[a]);
+          uint2 rec[4];
+          load_group(L.G.edges, g, rec);
+          const u32x4 c = sim_ic_coins(L.key, g, r);
+#pragma unroll
+          for (int t = 0; t < 4; ++t) {
+            const uint32_t ed = (g << 2) + t;
+            if (ed >= ob && ed < oe && lane_of(c, t) < rec[t].y) {
+              const uint32_t u = rec[t].x;
+              const uint32_t bit = 1u << (u & 31);
+              if (!(atomicOr(&bm[u >> 5], bit) & bit)) {
+                const uint32_t pos = atomicAdd(&s_qlen, 1u);
+                if (pos < L.qcap) q[pos] = u;
+              }
+            }
+          }
+        }
+        __syncthreads();
+      }
+      lo = hi;
+      hi = min(s_qlen, L.qcap);
+      __syncthreads();
+    }
+    // every vertex is queued at most once, so qlen <= n = qcap
+    const uint32_t qlen = min(s_qlen, L.qcap);
+    if (tid == 0) {
+      if (L.sizes) L.sizes[r] = qlen;
+      reached += qlen;
+    }
+    for (uint32_t i = tid; i < qlen; i += SIM_THREADS) bm[q[i] >> 5] = 0u;
+    __syncthreads();
+  }
+  if (tid == 0 && reached) atomicAdd(L.total, reached);
+}
+
+}  // namespace
+
+void launch_ic_spread(const SpreadLaunch &L, cudaStream_t stream) {
+  count_launches(1);
+  ic_spread_kernel<<<L.blocks, SIM_THREADS, 0, stream>>>(L);
+}
+
+}  // namespace rip

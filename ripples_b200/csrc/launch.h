@@ -130,6 +130,24 @@ struct BigLaunch {
   int blocks = 0;
 };
 void launch_ic_bigset(const BigLaunch &L, cudaStream_t stream);
+
+// Forward IC spread simulation (kernels_spread.cu): one CTA per replica.
+struct SpreadLaunch {
+  DevGraph G{};                   // forward CSR: edges[e] = {target, threshold}
+  Key key{};
+  const uint32_t *seeds = nullptr;  // k vertex ids < n
+  uint32_t k = 0;
+  uint64_t replicas = 0;
+  unsigned long long *next = nullptr;   // replica counter (zeroed)
+  unsigned long long *total = nullptr;  // sum of reached counts (zeroed)
+  uint32_t *sizes = nullptr;      // per replica reached count, or null
+  uint32_t *bitmaps = nullptr;    // per CTA slot, bm_words words, all-zero
+  uint64_t bm_words = 0;
+  uint32_t *queues = nullptr;     // per CTA slot, qcap = n entries
+  uint32_t qcap = 0;
+  int blocks = 0;
+};
+void launch_ic_spread(const SpreadLaunch &L, cudaStream_t stream);
 void launch_ic_fused(const FusedLaunch &L, cudaStream_t stream);
 // Resident fused CTAs per SM for a colour width (occupancy API).
 int fused_ctas_per_sm(uint32_t colors);

@@ -14,6 +14,9 @@
 //   coin(s, e)         = P(g_lo, g_hi, s_lo, IC<<24 | s_hi)[e & 3],  g = e >> 2
 //   lt_threshold(s, v) = P(v, 0, s_lo, LT<<24 | s_hi)[0]
 // (s_hi = bits 32..55 of the set id; set ids are limited to 2^56.)
+// Forward Monte Carlo spread simulation draws from domains of its own, keyed
+// by the replica id r instead of a set id:
+//   sim_coin(r, e)     = P(g_lo, g_hi, r_lo, SIM_IC<<24 | r_hi)[e & 3]
 #pragma once
 #include <stdint.h>
 
@@ -25,7 +28,7 @@
 
 namespace rip {
 
-enum : uint32_t { DOM_ROOT = 1, DOM_IC = 2, DOM_LT = 3 };
+enum : uint32_t { DOM_ROOT = 1, DOM_IC = 2, DOM_LT = 3, DOM_SIM_IC = 7 };
 
 RIP_HD void mulhilo32(uint32_t a, uint32_t b, uint32_t &hi, uint32_t &lo) {
 #if defined(__CUDA_ARCH__)
@@ -100,6 +103,12 @@ RIP_HD uint32_t root_of(Key k, uint64_t s, uint32_t n) {
 RIP_HD u32x4 ic_coins(Key k, uint64_t g, uint64_t s) {
   return philox((uint32_t)g, (uint32_t)(g >> 32), (uint32_t)s,
                 set_hi(s, DOM_IC), k.k0, k.k1);
+}
+
+// Coins for the 4 forward edges 4g .. 4g+3 in spread replica r.
+RIP_HD u32x4 sim_ic_coins(Key k, uint64_t g, uint64_t r) {
+  return philox((uint32_t)g, (uint32_t)(g >> 32), (uint32_t)r,
+                set_hi(r, DOM_SIM_IC), k.k0, k.k1);
 }
 
 RIP_HD uint32_t lt_threshold(Key k, uint64_t s, uint32_t v) {

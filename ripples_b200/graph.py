@@ -101,6 +101,13 @@ class HostGraph:
                                    _ptr(self.src), _ptr(self.weights), 1 if backward else 0),
               "rip_write_binary")
 
+    def forward(self) -> "HostGraph":
+        """The forward CSR of the same graph in this class's layout: ``index``
+        over source vertices, ``src`` holding each out-edge's target (ordered
+        by target id), ``weights`` p(u -> v) -- what ``rip_spread_ic`` takes."""
+        s, d = self.transpose_edges()
+        return HostGraph.from_edges(self.n, d, s, self.weights)
+
     def transpose_edges(self) -> Tuple[np.ndarray, np.ndarray]:
         """(src, dst) arrays of the directed edges, in backward-CSR order."""
         dst = np.repeat(np.arange(self.n, dtype=np.uint32), np.diff(self.index).astype(np.int64))
@@ -402,6 +409,20 @@ def sample_multi(ctx: Context, pools, seeds, counts) -> None:
     sd = np.ascontiguousarray(seeds, dtype=np.uint64)
     ct = np.ascontiguousarray(counts, dtype=np.uint64)
     check(lib.rip_sample_multi(ctx.h, hp, _ptr(sd), _ptr(ct), n), "rip_sample_multi", ctx.h)
+
+
+def spread_ic(graph: DeviceGraph, seeds, replicas: int, seed: int = 0,
+              with_sizes: bool = False):
+    """Forward Monte Carlo spread of ``seeds`` under IC (``rip_spread_ic``):
+    ``graph`` is an IC ``DeviceGraph`` of the FORWARD CSR
+    (``HostGraph.forward()``).  Returns the mean reached count, and with
+    ``with_sizes`` also each replica's count."""
+    sd = np.ascontiguousarray(seeds, dtype=np.uint32)
+    sizes = np.zeros(max(replicas, 1), dtype=np.uint32) if with_sizes else None
+    out = ctypes.c_double()
+    check(lib.rip_spread_ic(graph.h, _ptr(sd) if sd.size else None, int(sd.size), replicas, seed,
+                            _ptr(sizes), ctypes.byref(out)), "rip_spread_ic", graph.ctx.h)
+    return (out.value, sizes[:replicas]) if with_sizes else out.value
 
 
 class Query:

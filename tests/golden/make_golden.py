@@ -17,6 +17,8 @@ Outputs (small, committed):
   sampler_reference.npz per-vertex occurrence counts and set sizes of the
                         reference's sequential IC / LT samplers on fixed graphs
                         (trng interface shim as the random stream)
+  spread_reference.json mean IC spread of fixed seed sets measured by the
+                        reference's simulator (ripples::simulate)
 The karate graph (karate.tsv, 78 edges) is the reference's
 test-data/karate.tsv / test/rrr_set_generation.cc:63-79 edge list.
 """
@@ -151,6 +153,51 @@ def sampler_reference():
     np.savez_compressed(os.path.join(OUT, "sampler_reference.npz"), **out)
 
 
+SPREAD_CASES = [
+    # name, graph builder arguments, seed choice, replicas
+    dict(name="karate_ic", graph="karate", seeds="top2", replicas=100000),
+    dict(name="rmat12_ic", graph=dict(scale=12, draws=8 << 12, seed=7, wseed=8, hi=0.2),
+         seeds="top10", replicas=20000),
+    dict(name="rmat14_ic", graph=dict(scale=14, draws=1 << 18, seed=0, wseed=1, hi=0.1),
+         seeds="top20", replicas=5000),
+]
+
+
+def spread_graph(case) -> "rb.HostGraph":
+    if case["graph"] == "karate":
+        return karate_graph()
+    p = case["graph"]
+    return rb.HostGraph.rmat(p["scale"], p["draws"], seed=p["seed"]).with_weights(
+        rb.WEIGHTS_UNIFORM, seed=p["wseed"], lo=0.0, hi=p["hi"])
+
+
+def spread_seeds(g, choice) -> np.ndarray:
+    """The `choice` = "topK" vertices of largest out-degree (ties: lower id)."""
+    k = int(choice[3:])
+    outdeg = np.bincount(g.src, minlength=g.n)
+    return np.lexsort((np.arange(g.n), -outdeg))[:k].astype(np.uint32)
+
+
+def spread_reference():
+    """Mean IC spread of fixed seed sets measured by the reference's own
+    simulator (ripples::simulate, include/ripples/diffusion_simulation.h:73-127,
+    driven as tools/simulator.cc does), for pinning the forward-spread
+    restatement."""
+    tmp = tempfile.mkdtemp()
+    R = O.reference()
+    rows = []
+    for case in SPREAD_CASES:
+        g = spread_graph(case)
+        seeds = spread_seeds(g, case["seeds"])
+        path = os.path.join(tmp, case["name"] + "_fwd.bin")
+        g.write_binary(path, backward=False)
+        spread = R.ref_simulate(path.encode(), 0, seeds.ctypes.data, len(seeds),
+                                case["replicas"], 0)
+        rows.append(dict(case, seeds_list=[int(x) for x in seeds], spread=spread))
+    with open(os.path.join(OUT, "spread_reference.json"), "w") as fh:
+        json.dump(rows, fh, indent=1)
+
+
 def karate_graph() -> "rb.HostGraph":
     e = np.loadtxt(os.path.join(OUT, "karate.tsv"), dtype=np.float64)
     src = e[:, 0].astype(np.int64) - 1  # 1-based ids in the file
@@ -164,4 +211,5 @@ if __name__ == "__main__":
     theta_values()
     kat_counting()
     sampler_reference()
+    spread_reference()
     print("golden fixtures written to", OUT)
