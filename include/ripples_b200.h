@@ -308,6 +308,17 @@ int rip_imm_pool(rip_pool *p, uint32_t k, double epsilon, double l,
  * same draws.  Returns RIP_ERR_INVALID for an LT graph or a seed >= n. */
 int rip_spread_ic(rip_graph *g, const uint32_t *seeds, uint32_t k,
                   uint64_t replicas, uint64_t seed, uint32_t *sizes, double *spread);
+/* Forward Monte Carlo spread under LT, the live-edge form of
+ * include/ripples/diffusion_simulation.h:129-178's threshold model: in replica
+ * r vertex v keeps the first in-edge j (CSR order of `bwd`) with
+ * P(v, 0, r; seed, SIM_LT)[0] < cum[j] (the LT sampler's cumulative
+ * thresholds), or none; v is reached iff that edge's source is.
+ *   fwd : the forward CSR, uploaded as an IC graph (its weights are unused).
+ *   bwd : the same graph's backward CSR uploaded with RIP_MODEL_LT (the graph
+ *         IMM runs on).
+ * Other arguments and results as rip_spread_ic. */
+int rip_spread_lt(rip_graph *fwd, rip_graph *bwd, const uint32_t *seeds, uint32_t k,
+                  uint64_t replicas, uint64_t seed, uint32_t *sizes, double *spread);
 
 /* ---- batching and serving --------------------------------------------------- */
 /* No counterpart in the reference (its GenerateRRRSets, include/ripples/

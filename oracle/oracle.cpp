@@ -25,8 +25,9 @@
 //     so equal-count ties resolve identically.
 //   * The lowest-id argmax tie-break of the reference's GPU seed selection,
 //     src/gpu/find_most_influential.cc:65-72 (thrust::max_element).
-//   * Forward IC spread of a seed set, replica by replica:
-//     include/ripples/diffusion_simulation.h:73-127 (run_simulation, IC).
+//   * Forward spread of a seed set, replica by replica:
+//     include/ripples/diffusion_simulation.h:73-127 (IC) and :129-178 (LT,
+//     restated in its live-edge form).
 //   * IMM theta math and the martingale loop: include/ripples/imm.h:77-128
 //     (ThetaPrime, InvThetaPrime, Theta), :145-260 (Sampling), :768-860 (IMM),
 //     include/ripples/utility.h:84-87 (logBinomial).
@@ -56,7 +57,7 @@
 
 namespace {
 
-enum : uint32_t { DOM_ROOT = 1, DOM_IC = 2, DOM_LT = 3, DOM_SIM_IC = 7 };
+enum : uint32_t { DOM_ROOT = 1, DOM_IC = 2, DOM_LT = 3, DOM_SIM_IC = 7, DOM_SIM_LT = 8 };
 
 void philox4x32_10(const uint32_t ctr_in[4], const uint32_t key_in[2],
                    uint32_t out[4]) {
@@ -126,6 +127,18 @@ uint32_t sim_ic_coin(uint64_t seed, uint64_t r, uint64_t e) {
   ctr[3] = (DOM_SIM_IC << 24) | (uint32_t)((r >> 32) & 0xFFFFFFu);
   philox4x32_10(ctr, key, out);
   return out[e & 3];
+}
+
+// Forward LT spread: the threshold of vertex v in replica r (its own domain).
+uint32_t sim_lt_threshold(uint64_t seed, uint64_t r, uint32_t v) {
+  uint32_t key[2], ctr[4], out[4];
+  make_key(seed, key);
+  ctr[0] = v;
+  ctr[1] = 0;
+  ctr[2] = (uint32_t)r;
+  ctr[3] = (DOM_SIM_LT << 24) | (uint32_t)((r >> 32) & 0xFFFFFFu);
+  philox4x32_10(ctr, key, out);
+  return out[0];
 }
 
 uint32_t lt_threshold(uint64_t seed, uint64_t s, uint32_t v) {
@@ -448,6 +461,47 @@ uint64_t orc_spread_ic(uint32_t n, const uint64_t *index, const uint32_t *dst,
     total += queue.size();
   }
   if (edges) *edges = n_edges;
+  return total;
+}
+
+// Forward LT spread in the live-edge form of the threshold model
+// (include/ripples/diffusion_simulation.h:129-178; Kempe, Kleinberg, Tardos,
+// KDD'03): in replica r vertex v keeps the first in-edge j of the backward
+// CSR (bindex, bsrc, cum: the LT sampler's cumulative thresholds) with
+// sim_lt_threshold(seed, r, v) < cum[j], or none, and v is reached iff that
+// in-edge's source is.  BFS from the seeds over the forward CSR (findex,
+// fdst).  Returns the sum of the reached counts.
+uint64_t orc_spread_lt(uint32_t n, const uint64_t *findex, const uint32_t *fdst,
+                       const uint64_t *bindex, const uint32_t *bsrc, const uint32_t *cum,
+                       const uint32_t *seeds, uint32_t k, uint64_t replicas, uint64_t seed,
+                       uint32_t *sizes) {
+  std::vector<uint64_t> stamp(n, ~0ull);
+  std::vector<uint32_t> queue;
+  uint64_t total = 0;
+  for (uint64_t r = 0; r < replicas; ++r) {
+    queue.clear();
+    for (uint32_t i = 0; i < k; ++i)
+      if (stamp[seeds[i]] != r) {
+        stamp[seeds[i]] = r;
+        queue.push_back(seeds[i]);
+      }
+    for (size_t head = 0; head < queue.size(); ++head) {
+      const uint32_t u = queue[head];
+      for (uint64_t e = findex[u]; e < findex[u + 1]; ++e) {
+        const uint32_t v = fdst[e];
+        if (stamp[v] == r) continue;
+        const uint32_t t = sim_lt_threshold(seed, r, v);
+        uint64_t j = bindex[v];
+        while (j < bindex[v + 1] && !(t < cum[j])) ++j;  // first j, CSR order
+        if (j < bindex[v + 1] && bsrc[j] == u) {
+          stamp[v] = r;
+          queue.push_back(v);
+        }
+      }
+    }
+    if (sizes) sizes[r] = (uint32_t)queue.size();
+    total += queue.size();
+  }
   return total;
 }
 

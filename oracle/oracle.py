@@ -44,6 +44,7 @@ def _load_oracle() -> ctypes.CDLL:
         "orc_pack_lt": (None, [P, U32, P, P]),
         "orc_sample": (P, [I32, U32, P, P, P, U64, U64, U64, P]),
         "orc_spread_ic": (U64, [U32, P, P, P, P, U32, U64, U64, P, ctypes.POINTER(U64)]),
+        "orc_spread_lt": (U64, [U32, P, P, P, P, P, P, U32, U64, U64, P]),
         "orc_pool_elements": (U64, [P]),
         "orc_pool_sets": (U64, [P]),
         "orc_pool_copy": (None, [P, P, P]),
@@ -136,6 +137,28 @@ def spread_ic(n: int, index: np.ndarray, dst: np.ndarray, thr: np.ndarray, seeds
     if with_edges:
         return mean, sizes[:replicas], edges.value
     return mean, sizes[:replicas]
+
+
+def spread_lt(g, seeds, replicas: int, seed: int = 0) -> Tuple[float, np.ndarray]:
+    """Forward LT spread (live-edge form) on backward HostGraph ``g`` with LT
+    weights: (mean reached count, per-replica counts)."""
+    f = g.forward()
+    cum = pack("LT", g.index, g.weights)
+    fi = np.ascontiguousarray(f.index, dtype=np.uint64)
+    fd = np.ascontiguousarray(f.src, dtype=np.uint32)
+    bi = np.ascontiguousarray(g.index, dtype=np.uint64)
+    bs = np.ascontiguousarray(g.src, dtype=np.uint32)
+    c = np.ascontiguousarray(cum, dtype=np.uint32)
+    if fd.size == 0:
+        fd, bs, c = (np.zeros(1, np.uint32) for _ in range(3))
+    sd = np.ascontiguousarray(seeds, dtype=np.uint32)
+    k = int(sd.size)
+    if k == 0:
+        sd = np.zeros(1, np.uint32)
+    sizes = np.zeros(max(replicas, 1), dtype=np.uint32)
+    total = L.orc_spread_lt(g.n, _ptr(fi), _ptr(fd), _ptr(bi), _ptr(bs), _ptr(c), _ptr(sd), k,
+                            replicas, seed, _ptr(sizes))
+    return (total / replicas if replicas else 0.0), sizes[:replicas]
 
 
 def select(n: int, offsets: np.ndarray, vertices: np.ndarray, k: int, tiebreak: int = 0):

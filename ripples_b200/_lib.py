@@ -127,6 +127,7 @@ SIGNATURES = {
                            ctypes.POINTER(ImmRecord)]),
     "rip_sample_multi": (I32, [P, P, P, P, U32]),
     "rip_spread_ic": (I32, [P, P, U32, U64, U64, P, ctypes.POINTER(ctypes.c_double)]),
+    "rip_spread_lt": (I32, [P, P, P, U32, U64, U64, P, ctypes.POINTER(ctypes.c_double)]),
     "rip_imm_batch": (I32, [P, ctypes.POINTER(ImmQuery), U32]),
     "rip_server_create": (I32, [P, SZ, U32, PP]),
     "rip_server_destroy": (I32, [P]),

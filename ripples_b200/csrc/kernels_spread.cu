@@ -1,16 +1,23 @@
-// kernels_spread.cu -- forward Monte Carlo spread of a seed set under IC.
+// kernels_spread.cu -- forward Monte Carlo spread of a seed set (IC, LT).
 //
 // The reference measures the quality of a seed set with ripples::simulate
-// (include/ripples/diffusion_simulation.h:73-127, driven replica by replica
-// by tools/simulator.cc): a BFS from the seeds over the forward graph in
-// which edge u -> v fires with probability p(u -> v), the spread being the
-// number of vertices reached, seeds included.  Here one 1024-thread CTA runs
-// one replica at a time with the level loop of the one-CTA-per-heavy-set
-// sampler: a level's entries are taken 1024 at a time, a block scan turns
-// their 4-edge group counts into offsets and all warps stride over the
-// concatenated groups.  The coin of forward edge e in replica r is
-// sim_ic_coins(key, e >> 2, r)[e & 3]: a replica's reached set is a pure
-// function of (seed, r), whatever the visiting order.
+// (include/ripples/diffusion_simulation.h:73-178, driven replica by replica
+// by tools/simulator.cc); the spread is the number of vertices reached,
+// seeds included.  Here one 1024-thread CTA runs one replica at a time with
+// the level loop of the one-CTA-per-heavy-set sampler: a level's entries are
+// taken 1024 at a time, a block scan turns their 4-edge group counts into
+// offsets and all warps stride over the concatenated groups of out-edges.
+//   IC: out-edge e of a reached vertex fires in replica r iff
+//       sim_ic_coins(key, e >> 2, r)[e & 3] < threshold(e) (BFS over live
+//       edges, diffusion_simulation.h:73-127).
+//   LT: the live-edge form of the threshold model (Kempe, Kleinberg, Tardos,
+//       KDD'03): vertex v keeps at most one in-edge -- the first j of its
+//       in-list with sim_lt_threshold(key, r, v) < cum[j], cum being the
+//       fixed-point cumulative in-weights the LT sampler uses -- and v is
+//       reached iff the source of that in-edge is reached.  The reached set
+//       has the distribution of diffusion_simulation.h:129-178's.
+// Either way a replica's reached set is a pure function of (seed, r),
+// whatever the visiting order.
 #include "device.cuh"
 #include "launch.h"
 
@@ -38,10 +45,32 @@ __device__ uint32_t sim_block_scan(uint32_t x, uint32_t *warp_tot, uint32_t *tot
   return r;
 }
 
-__global__ void __launch_bounds__(SIM_THREADS)
-ic_spread_kernel(SpreadLaunch L) {
+constexpr uint32_t NO_VERTEX = 0xFFFFFFFFu;
+
+// LT: the source of the in-edge vertex v keeps in replica r, or NO_VERTEX.
+// cum is non-decreasing along the in-list, so the first j with t < cum[j] is
+// found by binary search.
+__device__ __forceinline__ uint32_t lt_kept_source(const DevGraph &B, Key key, uint64_t r,
+                                                   uint32_t v) {
+  const uint32_t lo = __ldg(B.off + v), hi = __ldg(B.off + v + 1);
+  if (lo == hi) return NO_VERTEX;
+  const uint32_t t = sim_lt_threshold(key, r, v);
+  if (!(t < __ldg(B.edges + (hi - 1)).y)) return NO_VERTEX;  // keeps no in-edge
+  uint32_t a = lo, b = hi - 1;  // cum[b] > t
+  while (a < b) {
+    const uint32_t mid = (a + b) >> 1;
+    if (__ldg(B.edges + mid).y > t) b = mid;
+    else a = mid + 1;
+  }
+  return __ldg(B.edges + a).x;
+}
+
+template <bool LT>
+__global__ void __launch_bounds__(SIM_THREADS, 1)
+spread_kernel(SpreadLaunch L) {
   __shared__ uint32_t s_off[SIM_THREADS + 1];
   __shared__ uint32_t s_beg[SIM_THREADS], s_end[SIM_THREADS];
+  __shared__ uint32_t s_v[LT ? SIM_THREADS : 1];  // LT: the entry's vertex
   __shared__ uint32_t s_warp[SIM_WARPS];
   __shared__ uint32_t s_qlen, s_total;
   __shared__ unsigned long long s_rep;
@@ -78,6 +107,7 @@ ic_spread_kernel(SpreadLaunch L) {
           const uint32_t v = q[e];
           beg = __ldg(L.G.off + v);
           end = __ldg(L.G.off + v + 1);
+          if (LT) s_v[tid] = v;
         }
         s_beg[tid] = beg;
         s_end[tid] = end;
@@ -97,16 +127,34 @@ ic_spread_kernel(SpreadLaunch L) {
           const uint32_t g = (ob >> 2) + (j - s_off[a]);
           uint2 rec[4];
           load_group(L.G.edges, g, rec);
-          const u32x4 c = sim_ic_coins(L.key, g, r);
+          if (LT) {
+            const uint32_t from = s_v[a];
 #pragma unroll
-          for (int t = 0; t < 4; ++t) {
-            const uint32_t ed = (g << 2) + t;
-            if (ed >= ob && ed < oe && lane_of(c, t) < rec[t].y) {
+            for (int t = 0; t < 4; ++t) {
+              const uint32_t ed = (g << 2) + t;
+              if (ed < ob || ed >= oe) continue;
               const uint32_t u = rec[t].x;
               const uint32_t bit = 1u << (u & 31);
+              // a plain read first: reached bits are only ever set
+              if ((__ldcg(&bm[u >> 5]) & bit) || lt_kept_source(L.B, L.key, r, u) != from)
+                continue;
               if (!(atomicOr(&bm[u >> 5], bit) & bit)) {
                 const uint32_t pos = atomicAdd(&s_qlen, 1u);
                 if (pos < L.qcap) q[pos] = u;
+              }
+            }
+          } else {
+            const u32x4 c = sim_ic_coins(L.key, g, r);
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+              const uint32_t ed = (g << 2) + t;
+              if (ed >= ob && ed < oe && lane_of(c, t) < rec[t].y) {
+                const uint32_t u = rec[t].x;
+                const uint32_t bit = 1u << (u & 31);
+                if (!(atomicOr(&bm[u >> 5], bit) & bit)) {
+                  const uint32_t pos = atomicAdd(&s_qlen, 1u);
+                  if (pos < L.qcap) q[pos] = u;
+                }
               }
             }
           }
@@ -131,9 +179,10 @@ ic_spread_kernel(SpreadLaunch L) {
 
 }  // namespace
 
-void launch_ic_spread(const SpreadLaunch &L, cudaStream_t stream) {
+void launch_spread(const SpreadLaunch &L, bool lt, cudaStream_t stream) {
   count_launches(1);
-  ic_spread_kernel<<<L.blocks, SIM_THREADS, 0, stream>>>(L);
+  if (lt) spread_kernel<true><<<L.blocks, SIM_THREADS, 0, stream>>>(L);
+  else spread_kernel<false><<<L.blocks, SIM_THREADS, 0, stream>>>(L);
 }
 
 }  // namespace rip

@@ -131,9 +131,10 @@ struct BigLaunch {
 };
 void launch_ic_bigset(const BigLaunch &L, cudaStream_t stream);
 
-// Forward IC spread simulation (kernels_spread.cu): one CTA per replica.
+// Forward spread simulation (kernels_spread.cu): one CTA per replica.
 struct SpreadLaunch {
-  DevGraph G{};                   // forward CSR: edges[e] = {target, threshold}
+  DevGraph G{};                   // forward CSR: edges[e] = {target, IC threshold}
+  DevGraph B{};                   // LT only: backward CSR, edges[j] = {source, cumulative}
   Key key{};
   const uint32_t *seeds = nullptr;  // k vertex ids < n
   uint32_t k = 0;
@@ -147,7 +148,7 @@ struct SpreadLaunch {
   uint32_t qcap = 0;
   int blocks = 0;
 };
-void launch_ic_spread(const SpreadLaunch &L, cudaStream_t stream);
+void launch_spread(const SpreadLaunch &L, bool lt, cudaStream_t stream);
 void launch_ic_fused(const FusedLaunch &L, cudaStream_t stream);
 // Resident fused CTAs per SM for a colour width (occupancy API).
 int fused_ctas_per_sm(uint32_t colors);

@@ -17,6 +17,7 @@
 // Forward Monte Carlo spread simulation draws from domains of its own, keyed
 // by the replica id r instead of a set id:
 //   sim_coin(r, e)     = P(g_lo, g_hi, r_lo, SIM_IC<<24 | r_hi)[e & 3]
+//   sim_lt_thr(r, v)   = P(v, 0, r_lo, SIM_LT<<24 | r_hi)[0]
 #pragma once
 #include <stdint.h>
 
@@ -28,7 +29,7 @@
 
 namespace rip {
 
-enum : uint32_t { DOM_ROOT = 1, DOM_IC = 2, DOM_LT = 3, DOM_SIM_IC = 7 };
+enum : uint32_t { DOM_ROOT = 1, DOM_IC = 2, DOM_LT = 3, DOM_SIM_IC = 7, DOM_SIM_LT = 8 };
 
 RIP_HD void mulhilo32(uint32_t a, uint32_t b, uint32_t &hi, uint32_t &lo) {
 #if defined(__CUDA_ARCH__)
@@ -109,6 +110,11 @@ RIP_HD u32x4 ic_coins(Key k, uint64_t g, uint64_t s) {
 RIP_HD u32x4 sim_ic_coins(Key k, uint64_t g, uint64_t r) {
   return philox((uint32_t)g, (uint32_t)(g >> 32), (uint32_t)r,
                 set_hi(r, DOM_SIM_IC), k.k0, k.k1);
+}
+
+// Threshold of vertex v in LT spread replica r.
+RIP_HD uint32_t sim_lt_threshold(Key k, uint64_t r, uint32_t v) {
+  return philox(v, 0u, (uint32_t)r, set_hi(r, DOM_SIM_LT), k.k0, k.k1).x;
 }
 
 RIP_HD uint32_t lt_threshold(Key k, uint64_t s, uint32_t v) {

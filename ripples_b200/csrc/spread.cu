@@ -1,27 +1,25 @@
-// spread.cu -- forward Monte Carlo spread of a seed set under IC (host side).
+// spread.cu -- forward Monte Carlo spread of a seed set (host side).
 //
-// rip_spread_ic replaces the replica loop of tools/simulator.cc:139-149 over
-// ripples::simulate (include/ripples/diffusion_simulation.h:73-127): the
-// expected number of vertices a seed set reaches, averaged over replicas,
-// with every replica's reached count available for variance estimates.
+// rip_spread_ic / rip_spread_lt replace the replica loop of
+// tools/simulator.cc:139-149 over ripples::simulate
+// (include/ripples/diffusion_simulation.h:73-178): the expected number of
+// vertices a seed set reaches, averaged over replicas, with every replica's
+// reached count available for variance estimates.
 #include "host.h"
 
-extern "C" int rip_spread_ic(rip_graph *g, const uint32_t *seeds, uint32_t k,
-                             uint64_t replicas, uint64_t seed, uint32_t *sizes,
-                             double *spread) {
-  if (!g) return RIP_ERR_INVALID;
+namespace {
+
+int spread_run(rip_graph *g, rip_graph *b, const uint32_t *seeds, uint32_t k,
+               uint64_t replicas, uint64_t seed, uint32_t *sizes, double *spread,
+               const char *who) {
   rip_ctx *c = g->ctx;
-  if ((k && !seeds) || !spread)
-    return set_err(c, RIP_ERR_INVALID, "rip_spread_ic: null argument");
-  if (g->model != RIP_MODEL_IC)
-    return set_err(c, RIP_ERR_INVALID,
-                   "rip_spread_ic: the graph must be an IC graph holding the forward CSR");
+  if ((k && !seeds) || !spread) return set_err(c, RIP_ERR_INVALID, "%s: null argument", who);
   for (uint32_t i = 0; i < k; ++i)
     if (seeds[i] >= g->n)
-      return set_err(c, RIP_ERR_INVALID, "rip_spread_ic: seed %u out of range (n = %u)",
-                     seeds[i], g->n);
+      return set_err(c, RIP_ERR_INVALID, "%s: seed %u out of range (n = %u)", who, seeds[i],
+                     g->n);
   if (replicas >= (1ull << 56))
-    return set_err(c, RIP_ERR_LIMIT, "rip_spread_ic: at most 2^56 replicas");
+    return set_err(c, RIP_ERR_LIMIT, "%s: at most 2^56 replicas", who);
   *spread = 0.0;
   if (replicas == 0 || g->n == 0) return RIP_OK;
   CK(c, cudaSetDevice(c->device));
@@ -57,6 +55,7 @@ extern "C" int rip_spread_ic(rip_graph *g, const uint32_t *seeds, uint32_t k,
 
   SpreadLaunch L;
   L.G = g->view();
+  if (b) L.B = b->view();
   L.key = make_key(seed);
   L.seeds = ptr<uint32_t>(B.d_seeds);
   L.k = k;
@@ -69,7 +68,7 @@ extern "C" int rip_spread_ic(rip_graph *g, const uint32_t *seeds, uint32_t k,
   L.queues = L.bitmaps + slots * bm_words;
   L.qcap = g->n;
   L.blocks = (int)slots;
-  launch_ic_spread(L, c->stream);
+  launch_spread(L, b != nullptr, c->stream);
   CK(c, cudaGetLastError());
   unsigned long long total = 0;
   CK(c, cudaMemcpyAsync(&total, L.total, sizeof(total), cudaMemcpyDeviceToHost, c->stream));
@@ -79,4 +78,29 @@ extern "C" int rip_spread_ic(rip_graph *g, const uint32_t *seeds, uint32_t k,
   CK(c, cudaStreamSynchronize(c->stream));
   *spread = (double)total / (double)replicas;
   return RIP_OK;
+}
+
+}  // namespace
+
+extern "C" int rip_spread_ic(rip_graph *g, const uint32_t *seeds, uint32_t k,
+                             uint64_t replicas, uint64_t seed, uint32_t *sizes,
+                             double *spread) {
+  if (!g) return RIP_ERR_INVALID;
+  if (g->model != RIP_MODEL_IC)
+    return set_err(g->ctx, RIP_ERR_INVALID,
+                   "rip_spread_ic: the graph must be an IC graph holding the forward CSR");
+  return spread_run(g, nullptr, seeds, k, replicas, seed, sizes, spread, "rip_spread_ic");
+}
+
+extern "C" int rip_spread_lt(rip_graph *fwd, rip_graph *bwd, const uint32_t *seeds,
+                             uint32_t k, uint64_t replicas, uint64_t seed, uint32_t *sizes,
+                             double *spread) {
+  if (!fwd || !bwd) return RIP_ERR_INVALID;
+  if (bwd->model != RIP_MODEL_LT || fwd->ctx != bwd->ctx)
+    return set_err(fwd->ctx, RIP_ERR_INVALID,
+                   "rip_spread_lt: bwd must be the graph's LT upload in the same context");
+  if (fwd->n != bwd->n || fwd->m != bwd->m)
+    return set_err(fwd->ctx, RIP_ERR_INVALID,
+                   "rip_spread_lt: forward and backward CSR differ in size");
+  return spread_run(fwd, bwd, seeds, k, replicas, seed, sizes, spread, "rip_spread_lt");
 }

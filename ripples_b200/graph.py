@@ -425,6 +425,21 @@ def spread_ic(graph: DeviceGraph, seeds, replicas: int, seed: int = 0,
     return (out.value, sizes[:replicas]) if with_sizes else out.value
 
 
+def spread_lt(forward: DeviceGraph, backward: DeviceGraph, seeds, replicas: int,
+              seed: int = 0, with_sizes: bool = False):
+    """Forward Monte Carlo spread of ``seeds`` under LT (``rip_spread_lt``):
+    ``forward`` holds the forward CSR (``HostGraph.forward()``, any model),
+    ``backward`` is the same graph's LT ``DeviceGraph``.  Returns the mean
+    reached count, and with ``with_sizes`` also each replica's count."""
+    sd = np.ascontiguousarray(seeds, dtype=np.uint32)
+    sizes = np.zeros(max(replicas, 1), dtype=np.uint32) if with_sizes else None
+    out = ctypes.c_double()
+    check(lib.rip_spread_lt(forward.h, backward.h, _ptr(sd) if sd.size else None, int(sd.size),
+                            replicas, seed, _ptr(sizes), ctypes.byref(out)), "rip_spread_lt",
+          forward.ctx.h)
+    return (out.value, sizes[:replicas]) if with_sizes else out.value
+
+
 class Query:
     """One IMM query (``rip_imm_query``) with its seed buffer."""
 

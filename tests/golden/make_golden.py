@@ -17,8 +17,8 @@ Outputs (small, committed):
   sampler_reference.npz per-vertex occurrence counts and set sizes of the
                         reference's sequential IC / LT samplers on fixed graphs
                         (trng interface shim as the random stream)
-  spread_reference.json mean IC spread of fixed seed sets measured by the
-                        reference's simulator (ripples::simulate)
+  spread_reference.json mean IC / LT spread of fixed seed sets measured by
+                        the reference's simulator (ripples::simulate)
 The karate graph (karate.tsv, 78 edges) is the reference's
 test-data/karate.tsv / test/rrr_set_generation.cc:63-79 edge list.
 """
@@ -154,21 +154,32 @@ def sampler_reference():
 
 
 SPREAD_CASES = [
-    # name, graph builder arguments, seed choice, replicas
-    dict(name="karate_ic", graph="karate", seeds="top2", replicas=100000),
-    dict(name="rmat12_ic", graph=dict(scale=12, draws=8 << 12, seed=7, wseed=8, hi=0.2),
+    # name, model, graph builder arguments, seed choice, replicas
+    dict(name="karate_ic", model="IC", graph="karate", seeds="top2", replicas=100000),
+    dict(name="rmat12_ic", model="IC", graph=dict(scale=12, draws=8 << 12, seed=7, wseed=8,
+                                                  hi=0.2),
          seeds="top10", replicas=20000),
-    dict(name="rmat14_ic", graph=dict(scale=14, draws=1 << 18, seed=0, wseed=1, hi=0.1),
+    dict(name="rmat14_ic", model="IC", graph=dict(scale=14, draws=1 << 18, seed=0, wseed=1,
+                                                  hi=0.1),
          seeds="top20", replicas=5000),
+    dict(name="karate_lt", model="LT", graph="karate", seeds="top2", replicas=50000),
+    dict(name="rmat10_lt", model="LT", graph=dict(scale=10, draws=8 << 10, seed=7, wseed=8),
+         seeds="top10", replicas=5000),
+    dict(name="rmat12_lt", model="LT", graph=dict(scale=12, draws=8 << 12, seed=5, wseed=6),
+         seeds="top10", replicas=12000),
 ]
 
 
 def spread_graph(case) -> "rb.HostGraph":
+    lt = case.get("model", "IC") == "LT"
     if case["graph"] == "karate":
-        return karate_graph()
+        g = karate_graph()
+        return g.with_weights(rb.WEIGHTS_LT_NORMALIZED, seed=9) if lt else g
     p = case["graph"]
-    return rb.HostGraph.rmat(p["scale"], p["draws"], seed=p["seed"]).with_weights(
-        rb.WEIGHTS_UNIFORM, seed=p["wseed"], lo=0.0, hi=p["hi"])
+    g = rb.HostGraph.rmat(p["scale"], p["draws"], seed=p["seed"])
+    if lt:
+        return g.with_weights(rb.WEIGHTS_LT_NORMALIZED, seed=p["wseed"])
+    return g.with_weights(rb.WEIGHTS_UNIFORM, seed=p["wseed"], lo=0.0, hi=p["hi"])
 
 
 def spread_seeds(g, choice) -> np.ndarray:
@@ -179,10 +190,10 @@ def spread_seeds(g, choice) -> np.ndarray:
 
 
 def spread_reference():
-    """Mean IC spread of fixed seed sets measured by the reference's own
-    simulator (ripples::simulate, include/ripples/diffusion_simulation.h:73-127,
+    """Mean IC / LT spread of fixed seed sets measured by the reference's own
+    simulator (ripples::simulate, include/ripples/diffusion_simulation.h:73-178,
     driven as tools/simulator.cc does), for pinning the forward-spread
-    restatement."""
+    restatements."""
     tmp = tempfile.mkdtemp()
     R = O.reference()
     rows = []
@@ -191,8 +202,8 @@ def spread_reference():
         seeds = spread_seeds(g, case["seeds"])
         path = os.path.join(tmp, case["name"] + "_fwd.bin")
         g.write_binary(path, backward=False)
-        spread = R.ref_simulate(path.encode(), 0, seeds.ctypes.data, len(seeds),
-                                case["replicas"], 0)
+        spread = R.ref_simulate(path.encode(), 0 if case["model"] == "IC" else 1,
+                                seeds.ctypes.data, len(seeds), case["replicas"], 0)
         rows.append(dict(case, seeds_list=[int(x) for x in seeds], spread=spread))
     with open(os.path.join(OUT, "spread_reference.json"), "w") as fh:
         json.dump(rows, fh, indent=1)

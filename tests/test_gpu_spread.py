@@ -1,6 +1,7 @@
-"""The device forward IC spread simulator (rip_spread_ic): every replica's
-reached count bit-exact against the oracle's restatement, and the mean
-against the spread the reference's own simulator measured (golden)."""
+"""The device forward spread simulators (rip_spread_ic, rip_spread_lt):
+every replica's reached count bit-exact against the oracle's restatement,
+and the mean against the spread the reference's own simulator measured
+(golden)."""
 import json
 import os
 import sys
@@ -61,7 +62,8 @@ def test_spread_karate_bit_exact(ctx):
         dg.close()
 
 
-@pytest.mark.parametrize("name", ["karate_ic", "rmat12_ic", "rmat14_ic"])
+@pytest.mark.parametrize("name", ["karate_ic", "rmat12_ic", "rmat14_ic", "karate_lt",
+                                  "rmat10_lt", "rmat12_lt"])
 def test_spread_matches_reference_simulator(ctx, name):
     # The device mean over many replicas against the reference simulator's
     # mean for the same seeds: within 4 standard errors and within 1%.
@@ -72,15 +74,56 @@ def test_spread_matches_reference_simulator(ctx, name):
     g = M.spread_graph(case)
     seeds = np.asarray(case["seeds_list"], np.uint32)
     dg = forward_device(ctx, g)
+    bg = rb.DeviceGraph(ctx, g, "LT") if case["model"] == "LT" else None
     try:
         reps = 200000
-        mean, sizes = rb.spread_ic(dg, seeds, reps, seed=17, with_sizes=True)
+        if bg is None:
+            mean, sizes = rb.spread_ic(dg, seeds, reps, seed=17, with_sizes=True)
+        else:
+            mean, sizes = rb.spread_lt(dg, bg, seeds, reps, seed=17, with_sizes=True)
     finally:
+        if bg is not None:
+            bg.close()
         dg.close()
     sd = float(np.std(sizes.astype(np.float64)))
     se = sd * np.sqrt(1.0 / reps + 1.0 / case["replicas"])
     assert abs(mean - case["spread"]) <= 4 * se + 1e-9, (mean, case["spread"], se)
     assert abs(mean - case["spread"]) / case["spread"] < 0.01
+
+
+@pytest.mark.parametrize("scale,deg,kind,seeds,replicas", [
+    (10, 8, "normalized", [0, 8, 64, 128], 256),
+    (12, 16, "normalized", [0, 1, 2, 3, 4, 5, 6, 7], 64),
+    (11, 8, "partial", [3, 3, 9], 128),   # in-weights sum below 1: some keep no edge
+])
+def test_spread_lt_bit_exact_vs_oracle(ctx, scale, deg, kind, seeds, replicas):
+    g = rb.HostGraph.rmat(scale, deg << scale, seed=scale + 1)
+    if kind == "normalized":
+        g = g.with_weights(rb.WEIGHTS_LT_NORMALIZED, seed=scale + 60)
+    else:
+        g = g.with_weights(rb.WEIGHTS_UNIFORM, seed=scale + 60, lo=0.0, hi=0.1)
+    fg, bg = forward_device(ctx, g), rb.DeviceGraph(ctx, g, "LT")
+    try:
+        mean, sizes = rb.spread_lt(fg, bg, seeds, replicas, seed=23, with_sizes=True)
+        o_mean, o_sizes = O.spread_lt(g, seeds, replicas, seed=23)
+        assert np.array_equal(sizes, o_sizes)
+        assert mean == pytest.approx(o_mean, rel=0, abs=1e-9)
+    finally:
+        bg.close()
+        fg.close()
+
+
+def test_spread_lt_karate_bit_exact(ctx):
+    from conftest import karate
+    g = karate().with_weights(rb.WEIGHTS_LT_NORMALIZED, seed=9)
+    fg, bg = forward_device(ctx, g), rb.DeviceGraph(ctx, g, "LT")
+    try:
+        _, sizes = rb.spread_lt(fg, bg, [0, 33], 5000, seed=4, with_sizes=True)
+        _, o_sizes = O.spread_lt(g, [0, 33], 5000, seed=4)
+        assert np.array_equal(sizes, o_sizes)
+    finally:
+        bg.close()
+        fg.close()
 
 
 def test_spread_arguments(ctx):
@@ -96,6 +139,16 @@ def test_spread_arguments(ctx):
             rb.spread_ic(dg, [g.n], 10)  # out of range: rejected on the host
         with pytest.raises(rb.RipError):
             rb.spread_ic(lt, [1], 10)    # IC only
+        with pytest.raises(rb.RipError):
+            rb.spread_lt(dg, dg, [1], 10)  # the backward graph must be the LT upload
+        small = rb.DeviceGraph(ctx, rb.HostGraph.rmat(6, 4 << 6, seed=1).with_weights(
+            rb.WEIGHTS_LT_NORMALIZED, seed=2), "LT")
+        try:
+            with pytest.raises(rb.RipError):
+                rb.spread_lt(dg, small, [1], 10)  # forward and backward differ
+        finally:
+            small.close()
+        assert rb.spread_lt(dg, lt, [1], 10) >= 1.0  # the same graph: fine
         # the context stays usable after the rejections
         assert rb.spread_ic(dg, [1], 10) >= 1.0
     finally:
