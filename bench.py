@@ -470,6 +470,10 @@ def main():
                          "traffic": traffic,
                          "alg_bytes_per_launch": alg_bytes / max(kern_n, 1),
                          "launches": kern_n, "kernel_ms": kern_ms},
+            # sum over sets of the in-degrees of their members (per-set
+            # semantics, fused expansions counted per colour) over the
+            # sampler kernels' time
+            "traversed_edges_per_s": int(st_tot[5]) / (kern_ms / 1e3) if kern_ms > 0 else None,
             "cpu_baseline": base,
             "clocks": clk,
             "gpu_launches": launches,
@@ -713,6 +717,7 @@ def run_p3(args, w, world, rank, local):
                           "alg_gb_per_s": alg / (km / 1e3) / 1e9 if km else None,
                           "frac_of_hbm": (alg / (km / 1e3) / 1e9) / peak if km else None,
                           "fusion_ratio": (int(st[4]) / int(st[0])) if st[0] else None,
+                          "traversed_edges_per_s": int(st[5]) / (km / 1e3) if km else None,
                           "mean_set": int(st[3]) / count}
         p.close()
     # full IMM runs, autotuned sampler
