@@ -450,6 +450,39 @@ int rip_write_binary(const char *path, uint32_t n, uint64_t m,
                      const float *w, int backward);
 void rip_free(void *ptr);
 
+/* ---- graph input files (host) ---------------------------------------------- */
+/* Weight distributions for unweighted TSV input (--distribution). */
+enum { RIP_DIST_UNIFORM = 0, RIP_DIST_NORMAL = 1, RIP_DIST_CONST = 2 };
+
+typedef struct rip_tsv_options {
+  int weighted;     /* third column holds the weight (-w) */
+  int undirected;   /* also add the reverse of every edge (-u) */
+  int renumber;     /* ids to 0..n-1 in sorted order (0: --disable-renumbering) */
+  int model;        /* RIP_MODEL_LT: generated weights normalised per source */
+  int distribution; /* RIP_DIST_* for generated weights */
+  double mean, variance, scale;  /* normal / const parameters; scale factor <= 1 */
+} rip_tsv_options;
+
+/* Reads a TSV edge list into the backward CSR (GraphBwd) the reference builds
+ * from it: include/ripples/loaders.h:138-296 (parsing, generated weights and
+ * their LT normalisation per source with a "not taking" mass, loaders.h:
+ * 169-191) and the Graph constructor (include/ripples/graph.h:520-620:
+ * renumbering, in-edges by source id).  Generated weights come from a Philox
+ * stream, not trng (same distributions, not the same draws).  Outputs are
+ * malloc'd arrays released with rip_free: index u64[n+1], src u32[m],
+ * w f32[m], reverse_map u32[n] (internal id -> input id, Graph::convertID).
+ * Returns RIP_ERR_INVALID with rip_read_error() text for an unreadable file
+ * or bad options. */
+int rip_read_tsv(const char *path, const rip_tsv_options *opt, uint32_t *n, uint64_t *m,
+                 uint64_t **index, uint32_t **src, float **w, uint32_t **reverse_map);
+/* Reads the reference binary format (include/ripples/graph.h:854-995,
+ * backward direction, float weights), weights multiplied by `scale` when it
+ * is below 1.  Outputs as rip_read_tsv. */
+int rip_read_binary(const char *path, double scale, uint32_t *n, uint64_t *m,
+                    uint64_t **index, uint32_t **src, float **w, uint32_t **reverse_map);
+/* Message for the last failed rip_read_* call on the calling thread. */
+const char *rip_read_error(void);
+
 #ifdef __cplusplus
 }
 #endif

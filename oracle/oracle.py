@@ -232,6 +232,8 @@ def reference() -> Optional[ctypes.CDLL]:
             "ref_pool_copy": (None, [P, P, P]),
             "ref_pool_free": (None, [P]),
             "ref_simulate": (DBL, [ctypes.c_char_p, I32, P, U32, U64, U64]),
+            "ref_graph_load_tsv": (P, [ctypes.c_char_p, I32, I32, I32]),
+            "ref_graph_copy": (None, [P, P, P, P, P]),
         }
         for k, (r, a) in sig.items():
             f = getattr(R, k)
@@ -251,6 +253,23 @@ def ref_select(n: int, offsets, vertices, k: int, omp: bool = True, threads: int
     ns = R.ref_select(n, len(off) - 1, _ptr(off), _ptr(vtx), k, 1 if omp else 0, threads,
                       _ptr(seeds), ctypes.byref(f))
     return f.value, seeds[:ns].copy()
+
+
+def ref_load_tsv(path: str, undirected: bool, lt: bool, renumber: bool):
+    """The reference's weighted TSV loader + GraphBwd: (n, index, src, w,
+    reverse_map)."""
+    R = reference()
+    g = R.ref_graph_load_tsv(path.encode(), int(undirected), int(lt), int(renumber))
+    try:
+        n, m = R.ref_graph_nodes(g), R.ref_graph_edges(g)
+        idx = np.zeros(n + 1, np.uint64)
+        src = np.zeros(max(m, 1), np.uint32)
+        w = np.zeros(max(m, 1), np.float32)
+        rmap = np.zeros(max(n, 1), np.uint32)
+        R.ref_graph_copy(g, _ptr(idx), _ptr(src), _ptr(w), _ptr(rmap))
+        return n, idx, src[:m], w[:m], rmap[:n]
+    finally:
+        R.ref_graph_free(g)
 
 
 def ref_sample(bin_path: str, model: str, count: int, seed: int = 0):

@@ -14,6 +14,9 @@
 //                      (include/ripples/generate_rrr_sets.h:186-198), with the
 //                      project's trng interface shim as the random stream.
 //   ref_simulate    -> ripples::simulate (include/ripples/diffusion_simulation.h)
+//   ref_graph_load_tsv / ref_graph_copy
+//                   -> the sequential TSV loader (include/ripples/loaders.h:138-196)
+//                      and the GraphBwd constructor (include/ripples/graph.h:506-620)
 #include <cstdint>
 #include <cstring>
 #include <string>
@@ -25,6 +28,7 @@
 #include "ripples/imm.h"
 #include "ripples/imm_interface.h"
 #include "ripples/diffusion_simulation.h"
+#include "ripples/loaders.h"
 #include "spdlog/sinks/stdout_color_sinks.h"
 
 namespace {
@@ -115,6 +119,43 @@ void *ref_graph_load(const char *path) {
 void ref_graph_free(void *g) { delete (ripples::GraphBwd *)g; }
 uint64_t ref_graph_nodes(void *g) { return ((ripples::GraphBwd *)g)->num_nodes(); }
 uint64_t ref_graph_edges(void *g) { return ((ripples::GraphBwd *)g)->num_edges(); }
+
+// Loads an unweighted TSV edge list with the reference's sequential loader
+// (include/ripples/loaders.h:138-196; weights from the shim's uniform01
+// stream, LT weights normalised per source) into the GraphBwd its constructor
+// builds (include/ripples/graph.h:506-620), renumbering when `renumber`.
+// (The weighted loader, loaders.h:211-296, parses its per-thread chunk buffer
+// as an unterminated C string, so it is not used here.)
+void *ref_graph_load_tsv(const char *path, int undirected, int lt, int renumber) {
+  ensure_console();
+  using E = ripples::Edge<uint32_t, float>;
+  trng::lcg64 lcg;
+  lcg.seed(0UL);
+  lcg.split(2, 0);
+  ripples::WeightGenerator<trng::lcg64, trng::uniform01_dist<float>, float> gen(lcg, 1.0f);
+  std::vector<E> edges;
+  if (lt)
+    edges = ripples::load<E>(std::string(path), undirected != 0, gen, ripples::edge_list_tsv{},
+                             ripples::linear_threshold_tag{});
+  else
+    edges = ripples::load<E>(std::string(path), undirected != 0, gen, ripples::edge_list_tsv{},
+                             ripples::independent_cascade_tag{});
+  return new ripples::GraphBwd(edges.begin(), edges.end(), renumber != 0);
+}
+
+// The graph's CSR and id map: index u64[n+1], src u32[m], w f32[m],
+// reverse_map u32[n] (internal id -> input id, Graph::convertID).
+void ref_graph_copy(void *g, uint64_t *index, uint32_t *src, float *w, uint32_t *reverse_map) {
+  auto &G = *(ripples::GraphBwd *)g;
+  const uint64_t n = G.num_nodes(), m = G.num_edges();
+  const auto *idx = G.csr_index();
+  for (uint64_t v = 0; v <= n; ++v) index[v] = (uint64_t)idx[v];
+  for (uint64_t e = 0; e < m; ++e) {
+    src[e] = G.csr_edges()[e];
+    w[e] = G.csr_weights()[e];
+  }
+  for (uint64_t v = 0; v < n; ++v) reverse_map[v] = G.convertID((uint32_t)v);
+}
 
 // Samples `count` sets with the reference sequential sampler; model 0 = IC,
 // 1 = LT.  Writes the total element count to *nelem and returns a handle to

@@ -25,6 +25,7 @@ ERR = {
 }
 
 MODEL_IC, MODEL_LT = 0, 1
+DIST_UNIFORM, DIST_NORMAL, DIST_CONST = 0, 1, 2
 TIE_REF_HEAP, TIE_LOWEST_ID = 0, 1
 SAMPLER_AUTO, SAMPLER_PLAIN, SAMPLER_FUSED = 0, 1, 2
 WEIGHTS_UNIFORM, WEIGHTS_LT_NORMALIZED, WEIGHTS_WC = 0, 1, 2
@@ -55,6 +56,19 @@ class ImmRecord(ctypes.Structure):
         ("total_sets", ctypes.c_uint64),
         ("pool_elements", ctypes.c_uint64),
         ("rrr_set_bytes", ctypes.c_uint64),
+    ]
+
+
+class TsvOptions(ctypes.Structure):
+    _fields_ = [
+        ("weighted", ctypes.c_int),
+        ("undirected", ctypes.c_int),
+        ("renumber", ctypes.c_int),
+        ("model", ctypes.c_int),
+        ("distribution", ctypes.c_int),
+        ("mean", ctypes.c_double),
+        ("variance", ctypes.c_double),
+        ("scale", ctypes.c_double),
     ]
 
 
@@ -147,6 +161,11 @@ SIGNATURES = {
     "rip_make_weights": (I32, [I32, U32, P, U64, U64, DBL, DBL, P]),
     "rip_write_binary": (I32, [ctypes.c_char_p, U32, U64, P, P, P, I32]),
     "rip_free": (None, [P]),
+    "rip_read_tsv": (I32, [ctypes.c_char_p, ctypes.POINTER(TsvOptions), ctypes.POINTER(U32),
+                           ctypes.POINTER(U64), P, P, P, P]),
+    "rip_read_binary": (I32, [ctypes.c_char_p, ctypes.c_double, ctypes.POINTER(U32),
+                              ctypes.POINTER(U64), P, P, P, P]),
+    "rip_read_error": (ctypes.c_char_p, []),
 }
 
 

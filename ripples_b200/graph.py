@@ -18,7 +18,7 @@ from typing import Optional, Sequence, Tuple
 import numpy as np
 
 from . import _lib
-from ._lib import check, lib
+from ._lib import RipError, check, lib
 
 
 def _ptr(a: Optional[np.ndarray]):
@@ -86,6 +86,52 @@ class HostGraph:
         if weights is not None:
             w = np.asarray(weights, dtype=np.float32)[order]
         return cls(n, idx, s.astype(np.uint32), w)
+
+    @staticmethod
+    def _from_read(rc, n, m, pi, ps, pw, pm, where) -> Tuple["HostGraph", np.ndarray]:
+        if rc != 0:
+            raise RipError(rc, where, (lib.rip_read_error() or b"").decode())
+        n, m = n.value, m.value
+
+        def take(p, ctype, count, dtype):
+            a = (np.ctypeslib.as_array(ctypes.cast(p, ctypes.POINTER(ctype)), shape=(count,)).copy()
+                 if count else np.zeros(0, dtype=dtype))
+            lib.rip_free(p)
+            return a
+        idx = take(pi, ctypes.c_uint64, n + 1, np.uint64)
+        src = take(ps, ctypes.c_uint32, m, np.uint32)
+        w = take(pw, ctypes.c_float, m, np.float32)
+        rmap = take(pm, ctypes.c_uint32, n, np.uint32)
+        return HostGraph(n, idx, src, w), rmap
+
+    @classmethod
+    def read_tsv(cls, path: str, weighted: bool = False, undirected: bool = False,
+                 renumber: bool = True, model: str = "IC", distribution: str = "uniform",
+                 mean: float = 0.5, variance: float = 1.0,
+                 scale: float = 1.0) -> Tuple["HostGraph", np.ndarray]:
+        """A TSV edge list read as the reference's loader and Graph constructor
+        build its GraphBwd (``rip_read_tsv``); returns (graph, reverse id map)."""
+        dist = {"uniform": _lib.DIST_UNIFORM, "normal": _lib.DIST_NORMAL,
+                "const": _lib.DIST_CONST}.get(distribution, -1)
+        o = _lib.TsvOptions(int(weighted), int(undirected), int(renumber), MODELS[model], dist,
+                            mean, variance, scale)
+        n, m = ctypes.c_uint32(), ctypes.c_uint64()
+        pi, ps, pw, pm = (ctypes.c_void_p() for _ in range(4))
+        rc = lib.rip_read_tsv(path.encode(), ctypes.byref(o), ctypes.byref(n), ctypes.byref(m),
+                              ctypes.byref(pi), ctypes.byref(ps), ctypes.byref(pw),
+                              ctypes.byref(pm))
+        return cls._from_read(rc, n, m, pi, ps, pw, pm, "rip_read_tsv")
+
+    @classmethod
+    def read_binary(cls, path: str, scale: float = 1.0) -> Tuple["HostGraph", np.ndarray]:
+        """The reference binary format (``rip_read_binary``); returns (graph,
+        reverse id map)."""
+        n, m = ctypes.c_uint32(), ctypes.c_uint64()
+        pi, ps, pw, pm = (ctypes.c_void_p() for _ in range(4))
+        rc = lib.rip_read_binary(path.encode(), scale, ctypes.byref(n), ctypes.byref(m),
+                                 ctypes.byref(pi), ctypes.byref(ps), ctypes.byref(pw),
+                                 ctypes.byref(pm))
+        return cls._from_read(rc, n, m, pi, ps, pw, pm, "rip_read_binary")
 
     def with_weights(self, kind: int, seed: int = 1, lo: float = 0.0,
                      hi: float = 1.0) -> "HostGraph":

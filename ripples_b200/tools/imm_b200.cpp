@@ -20,7 +20,8 @@
 // (no -w) are drawn from the library's Philox stream (seed 0): U(0,1),
 // truncated normal(mean, variance) on [0,1), or a constant; for LT they are
 // normalised per source with an extra random "not taking" mass, as the
-// reference loader does (loaders.h:169-191).
+// reference loader does (loaders.h:169-191).  Reading is the library's
+// (rip_read_tsv / rip_read_binary).
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -35,7 +36,6 @@
 #include <vector>
 
 #include "ripples_b200.h"
-#include "../csrc/philox.cuh"
 
 namespace {
 
@@ -112,130 +112,42 @@ struct Graph {  // backward CSR + id map
   std::vector<uint32_t> reverse_map;  // internal id -> input id
 };
 
-double unif(uint64_t ctr) {
-  rip::u32x4 r = rip::philox((uint32_t)ctr, (uint32_t)(ctr >> 32), 0u, 7u << 24, 0u, 0u);
-  return (double)(r.x >> 8) * (1.0 / 16777216.0);
-}
-
-float gen_weight(const Options &o, uint64_t &ctr) {
-  if (o.distribution == "const") return (float)o.mean;
-  if (o.distribution == "normal") {
-    for (int it = 0; it < 1000; ++it) {
-      double u1 = unif(ctr++), u2 = unif(ctr++);
-      if (u1 <= 0.0) continue;
-      double z = std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2);
-      double x = o.mean + o.variance * z;
-      if (x >= 0.0 && x < 1.0) return (float)x;
-    }
-    return 0.0f;
-  }
-  if (o.distribution != "uniform") usage("Unsupported distribution");
-  return (float)unif(ctr++);
-}
-
-struct Edge {
-  uint32_t s, d;
-  float w;
-};
-
-Graph load_tsv(const Options &o) {
-  std::ifstream in(o.input);
-  if (!in) usage(("cannot open " + o.input).c_str());
-  std::vector<Edge> edges;
-  uint64_t ctr = 0;
-  std::string line;
-  while (std::getline(in, line)) {
-    if (line.empty() || line.find('%') != std::string::npos ||
-        line.find('#') != std::string::npos)
-      continue;
-    std::istringstream ss(line);
-    uint64_t s, d;
-    float w = 0.0f;
-    if (!(ss >> s >> d)) continue;
-    if (o.weighted) ss >> w;
-    else w = gen_weight(o, ctr);
-    edges.push_back({(uint32_t)s, (uint32_t)d, w});
-    if (o.undirected) edges.push_back({(uint32_t)d, (uint32_t)s, o.weighted ? w : gen_weight(o, ctr)});
-  }
-  if (!o.weighted && o.model == "LT") {
-    // normalise per source with a random "not taking" mass (loaders.h:169-191)
-    std::stable_sort(edges.begin(), edges.end(),
-                     [](const Edge &a, const Edge &b) { return a.s < b.s; });
-    for (size_t b = 0; b < edges.size();) {
-      size_t e = b;
-      while (e < edges.size() && edges[e].s == edges[b].s) ++e;
-      float total = gen_weight(o, ctr);
-      for (size_t i = b; i < e; ++i) total += edges[i].w;
-      for (size_t i = b; i < e; ++i) edges[i].w /= total;
-      b = e;
-    }
-  }
-  if (o.scale < 1.0)
-    for (auto &e : edges) e.w = (float)(e.w * o.scale);
-  Graph G;
-  std::vector<uint32_t> ids;
-  uint32_t maxid = 0;
-  for (auto &e : edges) maxid = std::max(maxid, std::max(e.s, e.d));
-  if (o.no_renumber) {
-    G.n = edges.empty() ? 0 : maxid + 1;
-    G.reverse_map.resize(G.n);
-    for (uint32_t v = 0; v < G.n; ++v) G.reverse_map[v] = v;
+// The graph through the library's readers (rip_read_tsv / rip_read_binary):
+// the reference loader's parsing, generated weights and renumbering.
+Graph load_graph(const Options &o) {
+  uint32_t n = 0;
+  uint64_t m = 0, *index = nullptr;
+  uint32_t *src = nullptr, *reverse_map = nullptr;
+  float *w = nullptr;
+  int rc;
+  if (o.reload) {
+    rc = rip_read_binary(o.input.c_str(), o.scale, &n, &m, &index, &src, &w, &reverse_map);
   } else {
-    for (auto &e : edges) {
-      ids.push_back(e.s);
-      ids.push_back(e.d);
-    }
-    std::sort(ids.begin(), ids.end());
-    ids.erase(std::unique(ids.begin(), ids.end()), ids.end());
-    G.n = (uint32_t)ids.size();
-    G.reverse_map = ids;
-    auto id = [&](uint32_t x) {
-      return (uint32_t)(std::lower_bound(ids.begin(), ids.end(), x) - ids.begin());
-    };
-    for (auto &e : edges) {
-      e.s = id(e.s);
-      e.d = id(e.d);
-    }
+    rip_tsv_options t;
+    t.weighted = o.weighted;
+    t.undirected = o.undirected;
+    t.renumber = !o.no_renumber;
+    t.model = o.model == "LT" ? RIP_MODEL_LT : RIP_MODEL_IC;
+    t.distribution = o.distribution == "uniform"  ? RIP_DIST_UNIFORM
+                     : o.distribution == "normal" ? RIP_DIST_NORMAL
+                     : o.distribution == "const"  ? RIP_DIST_CONST
+                                                  : -1;
+    t.mean = o.mean;
+    t.variance = o.variance;
+    t.scale = o.scale;
+    rc = rip_read_tsv(o.input.c_str(), &t, &n, &m, &index, &src, &w, &reverse_map);
   }
-  // backward CSR: in-edges of each destination, by source id
-  std::stable_sort(edges.begin(), edges.end(), [](const Edge &a, const Edge &b) {
-    return a.d != b.d ? a.d < b.d : a.s < b.s;
-  });
-  G.index.assign((size_t)G.n + 1, 0);
-  for (auto &e : edges) G.index[e.d + 1]++;
-  for (uint32_t v = 0; v < G.n; ++v) G.index[v + 1] += G.index[v];
-  G.src.resize(edges.size());
-  G.w.resize(edges.size());
-  for (size_t i = 0; i < edges.size(); ++i) {
-    G.src[i] = edges[i].s;
-    G.w[i] = edges[i].w;
-  }
-  return G;
-}
-
-Graph load_binary(const Options &o) {
-  std::ifstream in(o.input, std::ios::binary);
-  if (!in) usage(("cannot open " + o.input).c_str());
-  uint64_t hdr[5];
-  in.read(reinterpret_cast<char *>(hdr), sizeof(hdr));
-  if (!in || hdr[0] != 0xc0ffeeull) usage("The endianess check failed when reloading the input binary.");
-  if (hdr[1] != 0xa1ccac0full)
-    usage("You are loading a binary that is not compatible with the algorithm you are trying to run.");
-  if (hdr[2] != 32ull) usage("The weight type in the binary file is not float.");
+  if (rc != RIP_OK) usage(rip_read_error());
   Graph G;
-  G.n = (uint32_t)hdr[3];
-  const uint64_t m = hdr[4];
-  G.reverse_map.resize(G.n);
-  G.index.resize((size_t)G.n + 1);
-  G.src.resize(m);
-  G.w.resize(m);
-  in.read(reinterpret_cast<char *>(G.reverse_map.data()), 4ull * G.n);
-  in.read(reinterpret_cast<char *>(G.index.data()), 8ull * (G.n + 1));
-  in.read(reinterpret_cast<char *>(G.src.data()), 4ull * m);
-  in.read(reinterpret_cast<char *>(G.w.data()), 4ull * m);
-  if (!in) usage("truncated binary graph");
-  if (o.scale < 1.0)
-    for (auto &x : G.w) x = (float)(x * o.scale);
+  G.n = n;
+  G.index.assign(index, index + (size_t)n + 1);
+  G.src.assign(src, src + m);
+  G.w.assign(w, w + m);
+  G.reverse_map.assign(reverse_map, reverse_map + n);
+  rip_free(index);
+  rip_free(src);
+  rip_free(w);
+  rip_free(reverse_map);
   return G;
 }
 
@@ -263,7 +175,7 @@ int main(int argc, char **argv) {
   const Options o = parse(argc, argv);
   using clk = std::chrono::high_resolution_clock;
   auto t0 = clk::now();
-  Graph G = o.reload ? load_binary(o) : load_tsv(o);
+  Graph G = load_graph(o);
   const double load_ms = std::chrono::duration<double, std::milli>(clk::now() - t0).count();
   std::fprintf(stderr, "[imm_b200] Loading took %.0fms: %u nodes, %zu edges\n", load_ms, G.n,
                G.src.size());

@@ -144,3 +144,106 @@ def test_parallel_heap_is_libstdcxx_make_heap(n, max_count, seed):
     std::make_heap element for element (the reference's tie-break depends on
     the exact heap layout), including with heavy ties."""
     assert _lib.lib.rip_selftest_heap(n, max_count, seed) == 1
+
+
+# ---- graph input files (rip_read_tsv / rip_read_binary) ---------------------
+
+def _write(path, text):
+    with open(path, "w") as fh:
+        fh.write(text)
+    return str(path)
+
+
+@pytest.mark.parametrize("undirected,renumber,lt", [(u, r, l) for u in (0, 1) for r in (0, 1)
+                                                    for l in (0, 1)])
+def test_read_tsv_structure_matches_reference_loader(tmp_path, undirected, renumber, lt):
+    # The graph the reference's sequential loader and GraphBwd constructor
+    # build from the same file: n, offsets, id map and each vertex's in-edge
+    # sources (the reference fills in-lists in parallel; here they are sorted
+    # by source id).  LT generated weights: per-source sums below 1 on both
+    # sides (the "not taking" mass).
+    from oracle import oracle as O
+    if O.reference() is None:
+        pytest.skip("oracle/_ref not built")
+    rng = np.random.default_rng(7)
+    lines = ["# header", "% comment"]
+    for i in range(2000):
+        s, t = rng.integers(0, 1500, size=2)
+        lines.append(f"{s}\t{t}")
+        if i % 101 == 0:
+            lines.append("")
+    p = _write(tmp_path / "g.tsv", "\n".join(lines) + "\n")
+    n, idx, src, w, rmap = O.ref_load_tsv(p, undirected, lt, renumber)
+    g, rmap2 = rb.HostGraph.read_tsv(p, undirected=bool(undirected), renumber=bool(renumber),
+                                     model="LT" if lt else "IC")
+    assert n == g.n and np.array_equal(idx, g.index) and np.array_equal(rmap, rmap2)
+    for v in range(n):
+        assert sorted(src[idx[v]:idx[v + 1]].tolist()) == \
+            g.src[g.index[v]:g.index[v + 1]].tolist()
+    assert (g.weights >= 0).all() and (g.weights < 1).all()
+    if lt:
+        for s_, w_ in ((src, w), (g.src, g.weights)):
+            out = np.zeros(n)
+            np.add.at(out, s_, w_)
+            assert out.max() < 1.0 + 1e-6
+
+
+def test_read_tsv_weighted_options(tmp_path):
+    p = _write(tmp_path / "w.tsv", "# c\n10 20 0.5\n20 30 0.25\n\n% x\n50 10 0.75\n10 20 0.125\n")
+    g, rmap = rb.HostGraph.read_tsv(p, weighted=True)
+    assert g.n == 4 and rmap.tolist() == [10, 20, 30, 50]
+    assert g.index.tolist() == [0, 1, 3, 4, 4]       # in-edges of 10, 20, 30, 50
+    assert g.src.tolist() == [3, 0, 0, 1]            # by source id, duplicates kept
+    assert g.weights.tolist() == [0.75, 0.5, 0.125, 0.25]
+    g2, _ = rb.HostGraph.read_tsv(p, weighted=True, undirected=True)
+    assert g2.m == 8
+    for v in range(g2.n):  # the reverse edge carries the same weight
+        for e in range(int(g2.index[v]), int(g2.index[v + 1])):
+            u = int(g2.src[e])
+            back = [float(g2.weights[f]) for f in range(int(g2.index[u]), int(g2.index[u + 1]))
+                    if int(g2.src[f]) == v]
+            assert float(g2.weights[e]) in back
+    g3, rmap3 = rb.HostGraph.read_tsv(p, weighted=True, renumber=False, scale=0.5)
+    assert g3.n == 51 and np.array_equal(rmap3, np.arange(51))
+    assert sorted(g3.weights.tolist()) == [0.0625, 0.125, 0.25, 0.375]
+
+
+def test_read_tsv_generated_weights_and_errors(tmp_path):
+    p = _write(tmp_path / "u.tsv", "".join(f"{i} {(i * 7) % 50}\n" for i in range(200)))
+    a, _ = rb.HostGraph.read_tsv(p)
+    b, _ = rb.HostGraph.read_tsv(p)
+    assert np.array_equal(a.weights, b.weights)   # one deterministic stream
+    c, _ = rb.HostGraph.read_tsv(p, distribution="const", mean=0.3)
+    assert np.allclose(c.weights, 0.3)
+    d, _ = rb.HostGraph.read_tsv(p, distribution="normal", mean=0.4, variance=0.1)
+    assert (d.weights >= 0).all() and (d.weights < 1).all()
+    with pytest.raises(rb.RipError, match="cannot open"):
+        rb.HostGraph.read_tsv(str(tmp_path / "missing.tsv"))
+    with pytest.raises(rb.RipError, match="Unsupported distribution"):
+        rb.HostGraph.read_tsv(p, distribution="pareto")
+    with pytest.raises(rb.RipError, match="scale factor"):
+        rb.HostGraph.read_tsv(p, scale=2.0)
+
+
+def test_read_binary_round_trip_and_errors(tmp_path):
+    g = rb.HostGraph.rmat(9, 4000, seed=4).with_weights(rb.WEIGHTS_UNIFORM, seed=1, lo=0, hi=1)
+    p = str(tmp_path / "g.bin")
+    g.write_binary(p)
+    h, rmap = rb.HostGraph.read_binary(p)
+    assert h.n == g.n and np.array_equal(rmap, np.arange(g.n))
+    assert np.array_equal(h.index, g.index) and np.array_equal(h.src, g.src)
+    assert np.array_equal(h.weights, g.weights)
+    h2, _ = rb.HostGraph.read_binary(p, scale=0.5)
+    assert np.array_equal(h2.weights, (g.weights * 0.5).astype(np.float32))
+    raw = open(p, "rb").read()
+    bad = str(tmp_path / "bad.bin")
+    open(bad, "wb").write(b"\x00" * 8 + raw[8:])
+    with pytest.raises(rb.RipError, match="endianess"):
+        rb.HostGraph.read_binary(bad)
+    open(bad, "wb").write(raw[: len(raw) - 12])
+    with pytest.raises(rb.RipError, match="truncated"):
+        rb.HostGraph.read_binary(bad)
+    pf = str(tmp_path / "f.bin")
+    g.write_binary(pf, backward=False)  # the forward direction is another format id
+    with pytest.raises(rb.RipError, match="not compatible"):
+        rb.HostGraph.read_binary(pf)
