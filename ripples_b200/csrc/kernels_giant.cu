@@ -130,7 +130,7 @@ __global__ void __launch_bounds__(256) giant_expand_kernel(GiantLaunch L, uint32
       if (lane_id() == 0 && j0 < total) {
         uint32_t lo = 0, hi = nf;
         while (hi - lo > 1) {
-          const uint32_t mid = (lo + hi) >> 1;
+          const uint32_t mid = lo + ((hi - lo) >> 1);
           if (L.goff[mid] <= j0) lo = mid;
           else hi = mid;
         }

@@ -58,7 +58,7 @@ __device__ __forceinline__ uint32_t lt_kept_source(const DevGraph &B, Key key, u
   if (!(t < __ldg(B.edges + (hi - 1)).y)) return NO_VERTEX;  // keeps no in-edge
   uint32_t a = lo, b = hi - 1;  // cum[b] > t
   while (a < b) {
-    const uint32_t mid = (a + b) >> 1;
+    const uint32_t mid = a + ((b - a) >> 1);  // edge ids reach 2^32: no a + b
     if (__ldg(B.edges + mid).y > t) b = mid;
     else a = mid + 1;
   }
