@@ -427,6 +427,14 @@ int64_t rip_inv_theta_prime(int64_t rr_size, double epsilon_prime, double l,
 uint64_t rip_theta(double epsilon, double l, uint64_t k, double lower_bound,
                    uint64_t n);
 double rip_log_binomial(uint64_t n, uint64_t k);
+/* OPIM-C sample sizes and bounds, exactly include/ripples/opimc.h:60-98 in its
+ * float arithmetic: theta_max (eq. 16), theta_0 (eq. 17), the lower bound of a
+ * seed set's spread from its coverage of R2 (eq. 5) and the upper bound of the
+ * optimum from the greedy coverage of R1 (eq. 8). */
+uint64_t rip_opimc_theta_max(uint64_t n, float epsilon, uint64_t k, float delta);
+uint64_t rip_opimc_theta_zero(uint64_t n, float epsilon, uint64_t k, float delta);
+float rip_opimc_lower_bound(uint64_t coverage, float delta2, uint64_t n, uint64_t theta);
+float rip_opimc_upper_bound(uint64_t coverage, float delta1, uint64_t n, uint64_t theta);
 
 /* ---- graph construction helpers (host) ------------------------------------- */
 /* R-MAT (Chakrabarti, Zhan, Faloutsos, SDM'04) edge sampling with quadrant

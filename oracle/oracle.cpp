@@ -25,6 +25,8 @@
 //     so equal-count ties resolve identically.
 //   * The lowest-id argmax tie-break of the reference's GPU seed selection,
 //     src/gpu/find_most_influential.cc:65-72 (thrust::max_element).
+//   * OPIM-C: include/ripples/opimc.h:60-98 (sample sizes and bounds, float
+//     arithmetic), :101-118 (coverage of a seed set), :150-243 (the driver).
 //   * Forward spread of a seed set, replica by replica:
 //     include/ripples/diffusion_simulation.h:73-127 (IC) and :129-178 (LT,
 //     restated in its live-edge form).
@@ -369,6 +371,52 @@ void sample_range(const Graph &G, int model, uint64_t seed, uint64_t first,
   }
 }
 
+// OPIM-C (include/ripples/opimc.h:150-243; Tang, Tang, Xiao, Yuan, SIGMOD'18)
+// over the oracle's samplers and selection.  Pool R1 holds the sets of key
+// `seed`, pool R2 those of key seed + R2_KEY_OFFSET, both ids [0, theta).
+// Bounds in the reference's float arithmetic (opimc.h:60-98).
+constexpr uint64_t R2_KEY_OFFSET = 0x9E3779B97F4A7C15ull;
+constexpr float OPIMC_A = 0.6321203113733684f;
+
+float opimc_theta_helper(size_t n, size_t k, float delta) {
+  float B = OPIMC_A * std::sqrt(std::log(6.0 / delta));
+  float C = std::sqrt(OPIMC_A * (logBinomial(n, k) + std::log(6.0 / delta)));
+  float D = (B + C) * (B + C);
+  return 2 * D;
+}
+
+// (unqualified log / sqrt on float arguments, as the reference calls them)
+float opimc_lower(size_t coverage, float delta2, size_t n, size_t theta) {
+  float A = log(1 / delta2);
+  float B = sqrt(coverage + 2 * A / 9);
+  float C = sqrt(A / 2);
+  float D = (B - C) * (B - C);
+  float E = A / 18;
+  return (float(n) / theta) * (D - E);
+}
+
+float opimc_upper(size_t coverage, float delta1, size_t n, size_t theta) {
+  float B = coverage / OPIMC_A;
+  float C = log(1 / delta1) / 2;
+  float D = sqrt(B + C);
+  double r = std::sqrt((double)C);  // (D + sqrt(C))^2 evaluates in double
+  float E = (float)((D + r) * (D + r));
+  return (float(n) / theta) * E;
+}
+
+uint64_t coverage_of(const Pool &P, uint64_t nsets, const std::vector<uint32_t> &seeds) {
+  std::vector<uint32_t> S(seeds);
+  std::sort(S.begin(), S.end());
+  uint64_t covered = 0;
+  for (uint64_t s = 0; s < nsets; ++s)
+    for (uint64_t j = P.off[s]; j < P.off[s + 1]; ++j)
+      if (std::binary_search(S.begin(), S.end(), P.vtx[j])) {
+        ++covered;
+        break;
+      }
+  return covered;
+}
+
 }  // namespace
 
 extern "C" {
@@ -503,6 +551,70 @@ uint64_t orc_spread_lt(uint32_t n, const uint64_t *findex, const uint32_t *fdst,
     total += queue.size();
   }
   return total;
+}
+
+// OPIM-C's coverage check (include/ripples/opimc.h:101-118, FindCoverage):
+// the number of sets [0, nsets) holding at least one of the k seeds.
+uint64_t orc_find_coverage(uint64_t nsets, const uint64_t *off, const uint32_t *vtx,
+                           const uint32_t *seeds, uint32_t k) {
+  std::vector<uint32_t> S(seeds, seeds + k);
+  std::sort(S.begin(), S.end());
+  uint64_t covered = 0;
+  for (uint64_t s = 0; s < nsets; ++s)
+    for (uint64_t j = off[s]; j < off[s + 1]; ++j)
+      if (std::binary_search(S.begin(), S.end(), vtx[j])) {
+        ++covered;
+        break;
+      }
+  return covered;
+}
+
+// OPIM-C driver; returns the number of seeds written.  theta_out: the final
+// pool size; rounds: selections run; thetas[0..1] = theta_0, theta_max.
+uint32_t orc_opimc(int model, uint32_t n, const uint64_t *index, const uint32_t *src,
+                   const uint32_t *thr, uint32_t k, float epsilon, float delta,
+                   uint64_t seed, int tiebreak, uint32_t *seeds, uint64_t *theta_out,
+                   uint32_t *rounds, uint64_t *thetas) {
+  Graph G{n, index, src, thr};
+  Pool R1, R2;
+  SampleStats st;
+  size_t theta = (size_t)std::ceil(opimc_theta_helper(n, k, delta));
+  const size_t theta_max =
+      (size_t)std::ceil(n * opimc_theta_helper(n, k, delta) / (epsilon * epsilon * k));
+  thetas[0] = theta;
+  thetas[1] = theta_max;
+  sample_range(G, model, seed, 0, theta, R1, st);
+  sample_range(G, model, seed + R2_KEY_OFFSET, 0, theta, R2, st);
+  const size_t i_max = (size_t)std::ceil(std::log2(theta_max / theta));
+  const float d = delta / (3 * i_max);
+  std::vector<uint32_t> result;
+  uint32_t r = 0;
+  for (;; ++r) {
+    SelectResult S = select_sets(n, theta, R1.off.data(), R1.vtx.data(), k, tiebreak);
+    const size_t cov1 = (size_t)(S.f * theta);  // the reference scales f back
+    const size_t cov2 = coverage_of(R2, theta, S.seeds);
+    const float upper = opimc_upper(cov1, d, n, theta);
+    const float lower = opimc_lower(cov2, d, n, theta);
+    result = S.seeds;
+    if (lower / upper >= (OPIMC_A - epsilon)) break;
+    if (theta >= theta_max) break;  // the paper's cap; the reference has none
+    const size_t grow = theta;  // theta doubles
+    sample_range(G, model, seed, theta, grow, R1, st);
+    sample_range(G, model, seed + R2_KEY_OFFSET, theta, grow, R2, st);
+    theta *= 2;
+  }
+  for (size_t i = 0; i < result.size(); ++i) seeds[i] = result[i];
+  *theta_out = theta;
+  *rounds = r + 1;
+  return (uint32_t)result.size();
+}
+
+void orc_opimc_math(uint64_t n, float epsilon, uint64_t k, float delta, uint64_t coverage,
+                    uint64_t theta, uint64_t *thetas, float *bounds) {
+  thetas[0] = (uint64_t)std::ceil(opimc_theta_helper(n, k, delta));
+  thetas[1] = (uint64_t)std::ceil(n * opimc_theta_helper(n, k, delta) / (epsilon * epsilon * k));
+  bounds[0] = opimc_lower(coverage, delta, n, theta);
+  bounds[1] = opimc_upper(coverage, delta, n, theta);
 }
 
 uint64_t orc_pool_elements(void *h) { return ((Pool *)h)->vtx.size(); }

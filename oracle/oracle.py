@@ -45,6 +45,10 @@ def _load_oracle() -> ctypes.CDLL:
         "orc_sample": (P, [I32, U32, P, P, P, U64, U64, U64, P]),
         "orc_spread_ic": (U64, [U32, P, P, P, P, U32, U64, U64, P, ctypes.POINTER(U64)]),
         "orc_spread_lt": (U64, [U32, P, P, P, P, P, P, U32, U64, U64, P]),
+        "orc_find_coverage": (U64, [U64, P, P, P, U32]),
+        "orc_opimc": (U32, [I32, U32, P, P, P, U32, ctypes.c_float, ctypes.c_float, U64, I32, P,
+                            ctypes.POINTER(U64), ctypes.POINTER(U32), P]),
+        "orc_opimc_math": (None, [U64, ctypes.c_float, U64, ctypes.c_float, U64, U64, P, P]),
         "orc_pool_elements": (U64, [P]),
         "orc_pool_sets": (U64, [P]),
         "orc_pool_copy": (None, [P, P, P]),
@@ -161,6 +165,53 @@ def spread_lt(g, seeds, replicas: int, seed: int = 0) -> Tuple[float, np.ndarray
     return (total / replicas if replicas else 0.0), sizes[:replicas]
 
 
+def opimc(model: str, n: int, index, src, thr, k: int, epsilon: float, delta: float,
+          seed: int = 0, tiebreak: int = 0) -> dict:
+    """OPIM-C (include/ripples/opimc.h:150-243) over the oracle: seeds, the
+    final pool size, rounds, theta_0 and theta_max."""
+    idx = np.ascontiguousarray(index, dtype=np.uint64)
+    s = np.ascontiguousarray(src, dtype=np.uint32)
+    t = np.ascontiguousarray(thr, dtype=np.uint32)
+    seeds = np.zeros(max(k, 1), np.uint32)
+    theta, rounds = ctypes.c_uint64(), ctypes.c_uint32()
+    th = np.zeros(2, np.uint64)
+    ns = L.orc_opimc(0 if model == "IC" else 1, n, _ptr(idx), _ptr(s), _ptr(t), k, epsilon, delta,
+                     seed, tiebreak, _ptr(seeds), ctypes.byref(theta), ctypes.byref(rounds),
+                     _ptr(th))
+    return dict(seeds=seeds[:ns].tolist(), theta=theta.value, rounds=rounds.value,
+                theta_zero=int(th[0]), theta_max=int(th[1]))
+
+
+def opimc_math(n, epsilon, k, delta, coverage, theta):
+    th = np.zeros(2, np.uint64)
+    b = np.zeros(2, np.float32)
+    L.orc_opimc_math(n, epsilon, k, delta, coverage, theta, _ptr(th), _ptr(b))
+    return int(th[0]), int(th[1]), b
+
+
+def find_coverage(offsets, vertices, seeds) -> int:
+    """Sets holding at least one seed (OPIM-C's FindCoverage)."""
+    off = np.ascontiguousarray(offsets, dtype=np.uint64)
+    vtx = np.ascontiguousarray(vertices, dtype=np.uint32)
+    sd = np.ascontiguousarray(seeds, dtype=np.uint32)
+    if vtx.size == 0:
+        vtx = np.zeros(1, np.uint32)
+    k = int(sd.size)
+    if k == 0:
+        sd = np.zeros(1, np.uint32)
+    return int(L.orc_find_coverage(len(off) - 1, _ptr(off), _ptr(vtx), _ptr(sd), k))
+
+
+def ref_find_coverage(offsets, vertices, seeds) -> int:
+    R = reference()
+    off = np.ascontiguousarray(offsets, dtype=np.uint64)
+    vtx = np.ascontiguousarray(vertices, dtype=np.uint32)
+    sd = np.ascontiguousarray(seeds, dtype=np.uint32)
+    if vtx.size == 0:
+        vtx = np.zeros(1, np.uint32)
+    return int(R.ref_find_coverage(len(off) - 1, _ptr(off), _ptr(vtx), _ptr(sd), int(len(seeds))))
+
+
 def select(n: int, offsets: np.ndarray, vertices: np.ndarray, k: int, tiebreak: int = 0):
     """Greedy max coverage; returns (f, seeds, gains, uncovered).
     tiebreak 0 = reference CPU lazy heap, 1 = lowest id."""
@@ -233,6 +284,11 @@ def reference() -> Optional[ctypes.CDLL]:
             "ref_pool_free": (None, [P]),
             "ref_simulate": (DBL, [ctypes.c_char_p, I32, P, U32, U64, U64]),
             "ref_graph_load_tsv": (P, [ctypes.c_char_p, I32, I32, I32]),
+            "ref_opimc_theta_max": (U64, [U64, ctypes.c_float, U64, ctypes.c_float]),
+            "ref_opimc_theta_zero": (U64, [U64, ctypes.c_float, U64, ctypes.c_float]),
+            "ref_opimc_lower_bound": (ctypes.c_float, [U64, ctypes.c_float, U64, U64]),
+            "ref_opimc_upper_bound": (ctypes.c_float, [U64, ctypes.c_float, U64, U64]),
+            "ref_find_coverage": (U64, [U64, P, P, P, U32]),
             "ref_graph_copy": (None, [P, P, P, P, P]),
         }
         for k, (r, a) in sig.items():

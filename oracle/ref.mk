@@ -16,12 +16,15 @@ DEFS     := -DNDEBUG -DSORTING=1 -DREORDERING=1 -DRIPPLES_ENABLE_FLOAT_WEIGHTS=1
 INC      := -I$(REF)/include -Ioracle/shims -I$(SPDLOG) -I$(NLOHMANN)
 FLAGS    := -O3 -fopenmp -std=c++17 -w $(DEFS) $(INC)
 
-all: $(OUT)/imm $(OUT)/simulator $(OUT)/libref_harness.so $(OUT)/adapter_imm
+all: $(OUT)/imm $(OUT)/opimc $(OUT)/simulator $(OUT)/libref_harness.so $(OUT)/adapter_imm
 
 $(OUT):
 	mkdir -p $(OUT)
 
 $(OUT)/imm: $(REF)/tools/imm.cc | $(OUT)
+	$(REFCXX) $(FLAGS) $< -o $@
+
+$(OUT)/opimc: $(REF)/tools/opimc.cc | $(OUT)
 	$(REFCXX) $(FLAGS) $< -o $@
 
 $(OUT)/simulator: $(REF)/tools/simulator.cc | $(OUT)

@@ -14,6 +14,8 @@
 //                      (include/ripples/generate_rrr_sets.h:186-198), with the
 //                      project's trng interface shim as the random stream.
 //   ref_simulate    -> ripples::simulate (include/ripples/diffusion_simulation.h)
+//   ref_opimc_*, ref_find_coverage
+//                   -> include/ripples/opimc.h:60-118
 //   ref_graph_load_tsv / ref_graph_copy
 //                   -> the sequential TSV loader (include/ripples/loaders.h:138-196)
 //                      and the GraphBwd constructor (include/ripples/graph.h:506-620)
@@ -29,6 +31,7 @@
 #include "ripples/imm_interface.h"
 #include "ripples/diffusion_simulation.h"
 #include "ripples/loaders.h"
+#include "ripples/opimc.h"
 #include "spdlog/sinks/stdout_color_sinks.h"
 
 namespace {
@@ -119,6 +122,27 @@ void *ref_graph_load(const char *path) {
 void ref_graph_free(void *g) { delete (ripples::GraphBwd *)g; }
 uint64_t ref_graph_nodes(void *g) { return ((ripples::GraphBwd *)g)->num_nodes(); }
 uint64_t ref_graph_edges(void *g) { return ((ripples::GraphBwd *)g)->num_edges(); }
+
+// OPIM-C arithmetic (include/ripples/opimc.h:60-98) and FindCoverage
+// (:101-118): the number of sets holding at least one seed.
+uint64_t ref_opimc_theta_max(uint64_t n, float eps, uint64_t k, float delta) {
+  return ripples::ThetaMax(n, eps, k, delta);
+}
+uint64_t ref_opimc_theta_zero(uint64_t n, float eps, uint64_t k, float delta) {
+  return ripples::ThetaZero(n, eps, k, delta);
+}
+float ref_opimc_lower_bound(uint64_t cov, float delta2, uint64_t n, uint64_t theta) {
+  return ripples::LowerBound(cov, delta2, n, theta);
+}
+float ref_opimc_upper_bound(uint64_t cov, float delta1, uint64_t n, uint64_t theta) {
+  return ripples::UpperBound(cov, delta1, n, theta);
+}
+uint64_t ref_find_coverage(uint64_t nsets, const uint64_t *off, const uint32_t *vtx,
+                           const uint32_t *seeds, uint32_t k) {
+  RRRsets RR = make_sets(nsets, off, vtx);
+  std::vector<uint32_t> S(seeds, seeds + k);
+  return ripples::FindCoverage(RR, S);
+}
 
 // Loads an unweighted TSV edge list with the reference's sequential loader
 // (include/ripples/loaders.h:138-196; weights from the shim's uniform01

@@ -166,6 +166,10 @@ SIGNATURES = {
     "rip_read_binary": (I32, [ctypes.c_char_p, ctypes.c_double, ctypes.POINTER(U32),
                               ctypes.POINTER(U64), P, P, P, P]),
     "rip_read_error": (ctypes.c_char_p, []),
+    "rip_opimc_theta_max": (U64, [U64, ctypes.c_float, U64, ctypes.c_float]),
+    "rip_opimc_theta_zero": (U64, [U64, ctypes.c_float, U64, ctypes.c_float]),
+    "rip_opimc_lower_bound": (ctypes.c_float, [U64, ctypes.c_float, U64, U64]),
+    "rip_opimc_upper_bound": (ctypes.c_float, [U64, ctypes.c_float, U64, U64]),
 }
 
 

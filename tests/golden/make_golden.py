@@ -19,6 +19,8 @@ Outputs (small, committed):
                         (trng interface shim as the random stream)
   spread_reference.json mean IC / LT spread of fixed seed sets measured by
                         the reference's simulator (ripples::simulate)
+  opimc_values.json     the reference's OPIM-C sample sizes and bounds on a
+                        grid (include/ripples/opimc.h:60-98), floats as bits
 The karate graph (karate.tsv, 78 edges) is the reference's
 test-data/karate.tsv / test/rrr_set_generation.cc:63-79 edge list.
 """
@@ -209,6 +211,33 @@ def spread_reference():
         json.dump(rows, fh, indent=1)
 
 
+def opimc_values():
+    """The reference's OPIM-C arithmetic (include/ripples/opimc.h:60-98) on a
+    grid: theta_max, theta_0 and the two bounds (floats stored bit for bit)."""
+    import itertools
+    import struct
+    R = O.reference()
+    fbits = lambda x: struct.unpack("<I", struct.pack("<f", x))[0]
+    rows = {"theta": [], "bounds": []}
+    for n, eps, k, delta in itertools.product([34, 1000, 16384, 1 << 20, 1 << 24, 3000017],
+                                              [0.05, 0.1, 0.13, 0.3, 0.5], [1, 5, 50, 100, 500],
+                                              [0.01, 1e-3, 1.0 / 16384]):
+        rows["theta"].append([n, fbits(eps), k, fbits(delta),
+                              int(R.ref_opimc_theta_max(n, eps, k, delta)),
+                              int(R.ref_opimc_theta_zero(n, eps, k, delta))])
+    rng = np.random.default_rng(3)
+    for _ in range(2000):
+        n = int(rng.integers(10, 1 << 24))
+        theta = int(rng.integers(1, 10 ** 7))
+        cov = int(rng.integers(0, theta + 1))
+        d = float(rng.choice([0.01, 0.001, 1e-4, 0.0333]))
+        rows["bounds"].append([cov, fbits(d), n, theta,
+                               fbits(R.ref_opimc_lower_bound(cov, d, n, theta)),
+                               fbits(R.ref_opimc_upper_bound(cov, d, n, theta))])
+    with open(os.path.join(OUT, "opimc_values.json"), "w") as fh:
+        json.dump(rows, fh)
+
+
 def karate_graph() -> "rb.HostGraph":
     e = np.loadtxt(os.path.join(OUT, "karate.tsv"), dtype=np.float64)
     src = e[:, 0].astype(np.int64) - 1  # 1-based ids in the file
@@ -223,4 +252,5 @@ if __name__ == "__main__":
     kat_counting()
     sampler_reference()
     spread_reference()
+    opimc_values()
     print("golden fixtures written to", OUT)

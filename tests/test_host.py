@@ -247,3 +247,21 @@ def test_read_binary_round_trip_and_errors(tmp_path):
     g.write_binary(pf, backward=False)  # the forward direction is another format id
     with pytest.raises(rb.RipError, match="not compatible"):
         rb.HostGraph.read_binary(pf)
+
+
+def test_opimc_arithmetic_matches_reference_golden():
+    # theta_max, theta_0 and the two bounds of OPIM-C bit for bit against
+    # the reference (include/ripples/opimc.h:60-98, golden grid).
+    import json
+    from conftest import GOLDEN
+    with open(os.path.join(GOLDEN, "opimc_values.json")) as fh:
+        rows = json.load(fh)
+    f = lambda bits: struct.unpack("<f", struct.pack("<I", bits))[0]
+    lib = _lib.lib
+    for n, eps, k, delta, tmax, tzero in rows["theta"]:
+        assert lib.rip_opimc_theta_max(n, f(eps), k, f(delta)) == tmax
+        assert lib.rip_opimc_theta_zero(n, f(eps), k, f(delta)) == tzero
+    bits = lambda x: struct.unpack("<I", struct.pack("<f", x))[0]
+    for cov, d, n, theta, lo, up in rows["bounds"]:
+        assert bits(lib.rip_opimc_lower_bound(cov, f(d), n, theta)) == lo
+        assert bits(lib.rip_opimc_upper_bound(cov, f(d), n, theta)) == up

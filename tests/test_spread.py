@@ -57,3 +57,57 @@ def test_spread_within_one_percent_of_reference(tmp_path, model, scale, draws, k
     s_ref = R.ref_simulate(fwd.encode(), m, np.asarray(ref, np.uint32).ctypes.data, k, reps, 0)
     s_our = R.ref_simulate(fwd.encode(), m, np.asarray(ours, np.uint32).ctypes.data, k, reps, 0)
     assert abs(s_our - s_ref) / s_ref < 0.01, (s_our, s_ref)
+
+
+OPIMC_EXE = os.path.join(ROOT, "oracle", "_ref", "opimc")
+
+
+@pytest.mark.parametrize("eps", [0.5, 0.2])
+def test_opimc_matches_reference_tool(tmp_path, eps):
+    # OPIM-C (include/ripples/opimc.h:150-243) restated over the oracle
+    # against the reference's own opimc tool on the 2^14-vertex IC
+    # configuration: theta_0 and theta_max equal, and the spread of the two
+    # seed sets, both measured by the reference's simulate, within 1%.
+    R = O.reference()
+    if R is None or not os.path.exists(OPIMC_EXE):
+        pytest.skip("oracle/_ref not built")
+    g = rb.HostGraph.rmat(14, 1 << 18, seed=0).with_weights(rb.WEIGHTS_UNIFORM, seed=1,
+                                                             lo=0.0, hi=0.1)
+    bwd, fwd = str(tmp_path / "g.bin"), str(tmp_path / "gf.bin")
+    g.write_binary(bwd, backward=True)
+    g.write_binary(fwd, backward=False)
+    out = str(tmp_path / "opimc.json")
+    subprocess.run([OPIMC_EXE, "-i", bwd, "--reload-binary", "-d", "IC", "-k", "20", "-e",
+                    str(eps), "--delta", "0.05", "-o", out, "-p"], check=True,
+                   stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL,
+                   env=dict(os.environ, OMP_NUM_THREADS="4"), timeout=600)
+    with open(out) as fh:
+        rec = json.load(fh)[0]
+    thr = O.pack("IC", g.index, g.weights)
+    ours = O.opimc("IC", g.n, g.index, g.src, thr, 20, eps, 0.05, seed=0)
+    assert ours["theta_zero"] == rec["ThetaZero"] and ours["theta_max"] == rec["ThetaMax"]
+    assert len(ours["seeds"]) == len(rec["Seeds"]) == 20
+    s_ref = R.ref_simulate(fwd.encode(), 0, np.asarray(rec["Seeds"], np.uint32).ctypes.data,
+                           20, 3000, 0)
+    s_our = R.ref_simulate(fwd.encode(), 0, np.asarray(ours["seeds"], np.uint32).ctypes.data,
+                           20, 3000, 0)
+    assert abs(s_our - s_ref) / s_ref < 0.01, (s_our, s_ref)
+
+
+def test_opimc_oracle_arithmetic_matches_reference():
+    R = O.reference()
+    if R is None:
+        pytest.skip("oracle/_ref not built")
+    rng = np.random.default_rng(9)
+    for _ in range(2000):
+        n = int(rng.integers(100, 1 << 24))
+        k = int(rng.integers(1, 200))
+        eps = float(rng.choice([0.05, 0.1, 0.3]))
+        d = float(rng.choice([0.05, 0.01, 0.001]))
+        theta = int(rng.integers(1, 10 ** 7))
+        cov = int(rng.integers(0, theta + 1))
+        t0, tm, b = O.opimc_math(n, eps, k, d, cov, theta)
+        assert t0 == R.ref_opimc_theta_zero(n, eps, k, d)
+        assert tm == R.ref_opimc_theta_max(n, eps, k, d)
+        assert np.float32(R.ref_opimc_lower_bound(cov, d, n, theta)) == b[0]
+        assert np.float32(R.ref_opimc_upper_bound(cov, d, n, theta)) == b[1]
