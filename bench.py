@@ -243,6 +243,78 @@ def reference_arm(args, w, world, rank):
     return 0
 
 
+def reference_arm_other(args, w, world, rank):
+    """The reference arm of the non-default workloads.  spread: the replica
+    loop of the reference's simulator tool (tools/simulator.cc:139-149 over
+    ripples::simulate, built from its sources) on all host cores, replicas of
+    the same seeds on the same forward graph.
+    batch / serve: the reference has no batching or serving path, and p3 (one
+    IMM on a 2^24-vertex, 521 M-edge graph) runs for hours on host cores: those
+    print an unavailable line."""
+    if rank != 0:
+        return 0
+    kind = w["kind"]
+    if kind != "spread":
+        why = {"batch": "the reference runs one IMM instance per process (no batching path)",
+               "serve": "the reference has no request loop (no serving path)",
+               "p3": "one reference IMM on the 2^24-vertex, 521 M-edge graph takes hours "
+                     "on host cores"}[kind]
+        print(json.dumps({"impl": "reference", "unavailable": why}))
+        return 0
+    sys.path.insert(0, ROOT)
+    from oracle import oracle as O
+    R = O.reference()
+    if R is None:
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref not built (make -f oracle/ref.mk needs the reference "
+                          "sources)"}))
+        return 0
+    import numpy as np
+    g = build_graph(w)
+    f = g.forward()
+    outdeg = np.diff(f.index).astype(np.int64)
+    seeds = np.lexsort((np.arange(g.n), -outdeg))[: w["k"]].astype(np.uint32)
+    tmp = tempfile.mkdtemp()
+    path = os.path.join(tmp, "fwd.bin")
+    g.write_binary(path, backward=False)
+    cores = os.cpu_count() or 1
+    reps = max(cores * 8, 64)  # a bounded sample: a few seconds of all cores
+
+    def run(r):
+        t0 = time.perf_counter()
+        mean = R.ref_simulate_parallel(path.encode(), 0 if w["model"] == "IC" else 1,
+                                       seeds.ctypes.data, len(seeds), r)
+        return time.perf_counter() - t0, mean
+
+    for _ in range(args.warmup):
+        run(cores)
+    tot_s, means = 0.0, []
+    for _ in range(args.steps):
+        dt, m = run(reps)
+        tot_s += dt
+        means.append(m)
+    value = reps * args.steps / tot_s
+    shutil.rmtree(tmp, ignore_errors=True)
+    print(json.dumps({
+        "impl": "reference", "metric": "IC spread replicas/s (forward Monte Carlo)",
+        "value": value, "unit": "replicas/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * tot_s / args.steps,
+        "higher_is_better": True, "scaling": "replicas only", "vs_baseline": None,
+        "dtype": "u32", "data": "synthetic R-MAT graph (seed 0) and weights (seed 1), forward "
+                                "binary format",
+        "config": {"workload": w["name"], "n": g.n, "m": g.m, "k": w["k"],
+                   "replicas_per_step": reps,
+                   "reference_path": "simulator's OpenMP replica loop"},
+        "mean_spread": float(np.mean(means)),
+        "cpu_baseline": {"value": value, "unit": "replicas/s", "cores": cores,
+                         "kind": "reference",
+                         "sample": f"{args.steps} runs of the simulator's replica loop, "
+                                   f"{reps} replicas each, graph load included"},
+        "e2e": {"value": value, "unit": "replicas/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0}}))
+    return 0
+
+
 def cpu_baseline(w, g, budget_s=30.0):
     """The reference's own CPU imm on this box's host cores (one IMM run)."""
     exe = os.path.join(ROOT, "oracle", "_ref", "imm")
@@ -290,6 +362,12 @@ def main():
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
     world, rank, local = dist_setup()
+    if args.impl == "reference" and w.get("kind") in ("batch", "serve", "p3", "spread"):
+        rc = reference_arm_other(args, w, world, rank)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return rc
     if args.sampler_case:
         return run_sampler_case(args, w, local)
     if w.get("kind") == "batch":

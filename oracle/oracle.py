@@ -283,6 +283,7 @@ def reference() -> Optional[ctypes.CDLL]:
             "ref_pool_copy": (None, [P, P, P]),
             "ref_pool_free": (None, [P]),
             "ref_simulate": (DBL, [ctypes.c_char_p, I32, P, U32, U64, U64]),
+            "ref_simulate_parallel": (DBL, [ctypes.c_char_p, I32, P, U32, U64]),
             "ref_graph_load_tsv": (P, [ctypes.c_char_p, I32, I32, I32]),
             "ref_opimc_theta_max": (U64, [U64, ctypes.c_float, U64, ctypes.c_float]),
             "ref_opimc_theta_zero": (U64, [U64, ctypes.c_float, U64, ctypes.c_float]),

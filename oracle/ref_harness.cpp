@@ -14,6 +14,7 @@
 //                      (include/ripples/generate_rrr_sets.h:186-198), with the
 //                      project's trng interface shim as the random stream.
 //   ref_simulate    -> ripples::simulate (include/ripples/diffusion_simulation.h)
+//   ref_simulate_parallel -> the replica loop of tools/simulator.cc:139-149
 //   ref_opimc_*, ref_find_coverage
 //                   -> include/ripples/opimc.h:60-118
 //   ref_graph_load_tsv / ref_graph_copy
@@ -122,6 +123,39 @@ void *ref_graph_load(const char *path) {
 void ref_graph_free(void *g) { delete (ripples::GraphBwd *)g; }
 uint64_t ref_graph_nodes(void *g) { return ((ripples::GraphBwd *)g)->num_nodes(); }
 uint64_t ref_graph_edges(void *g) { return ((ripples::GraphBwd *)g)->num_edges(); }
+
+// The replica loop of tools/simulator.cc:139-149 (OpenMP over replicas, one
+// trng stream per thread split as the tool splits them) without the tool's
+// log sink (a rotating sink of max size 0, which the vendored spdlog
+// rejects).  Returns the mean activated count.
+double ref_simulate_parallel(const char *fwd_path, int model, const uint32_t *seeds,
+                             uint32_t nseeds, uint64_t replicas) {
+  ensure_console();
+  ripples::GraphFwd G;
+  G.load_binary(fwd_path);
+  std::vector<uint32_t> S(seeds, seeds + nseeds);
+  G.transformID(S.begin(), S.end(), S.begin());
+  std::vector<trng::lcg64> generator(omp_get_max_threads());
+#pragma omp parallel
+  {
+    generator[omp_get_thread_num()].seed(0UL);
+    generator[omp_get_thread_num()].split(2, 1);
+    generator[omp_get_thread_num()].split(omp_get_num_threads(), omp_get_thread_num());
+  }
+  std::vector<size_t> reached(replicas);
+#pragma omp parallel for schedule(dynamic)
+  for (uint64_t i = 0; i < replicas; ++i) {
+    if (model == 0)
+      reached[i] = ripples::simulate(G, S.begin(), S.end(), generator[omp_get_thread_num()],
+                                     ripples::independent_cascade_tag{}).first;
+    else
+      reached[i] = ripples::simulate(G, S.begin(), S.end(), generator[omp_get_thread_num()],
+                                     ripples::linear_threshold_tag{}).first;
+  }
+  double acc = 0.0;
+  for (size_t x : reached) acc += (double)x;
+  return replicas ? acc / (double)replicas : 0.0;
+}
 
 // OPIM-C arithmetic (include/ripples/opimc.h:60-98) and FindCoverage
 // (:101-118): the number of sets holding at least one seed.

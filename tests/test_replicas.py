@@ -65,3 +65,19 @@ def test_reference_arm_runs_on_rank_zero_only():
         warmup, steps = 1, 1
     # a rank other than 0 returns at once, without building or timing anything
     assert bench.reference_arm(Args(), bench.WORKLOADS["lt20"], world=2, rank=1) == 0
+
+
+@pytest.mark.parametrize("workload", ["b1", "s1", "p3"])
+def test_reference_arm_of_other_workloads(workload, capsys):
+    # batching, serving and the 2^24 IMM have no runnable reference
+    # counterpart: one unavailable line, exit 0, no GPU path taken
+    sys.path.insert(0, ROOT)
+    import json
+    import bench
+
+    class Args:
+        warmup, steps = 1, 1
+    assert bench.reference_arm_other(Args(), bench.WORKLOADS[workload], world=1, rank=0) == 0
+    line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["unavailable"]
+    assert bench.reference_arm_other(Args(), bench.WORKLOADS[workload], world=2, rank=1) == 0
