@@ -114,9 +114,10 @@ extern "C" int rip_read_tsv(const char *path, const rip_tsv_options *o, uint32_t
                           o->distribution == RIP_DIST_NORMAL ||
                           o->distribution == RIP_DIST_CONST;
   std::vector<Edge> edges;
-  uint64_t ctr = 0;
+  uint64_t ctr = 0, lineno = 0;
   std::string line;
   while (std::getline(in, line)) {
+    ++lineno;
     if (line.empty() || line.find('%') != std::string::npos ||
         line.find('#') != std::string::npos)
       continue;
@@ -124,6 +125,8 @@ extern "C" int rip_read_tsv(const char *path, const rip_tsv_options *o, uint32_t
     uint64_t s, d;
     float w = 0.0f;
     if (!(ss >> s >> d)) continue;
+    if (s >= 0xFFFFFFFFull || d >= 0xFFFFFFFFull)  // ids are u32 with ~0 reserved
+      return read_fail("vertex id above 2^32 - 2 on line " + std::to_string(lineno));
     if (o->weighted) {
       ss >> w;
     } else {

@@ -223,6 +223,9 @@ def test_read_tsv_generated_weights_and_errors(tmp_path):
         rb.HostGraph.read_tsv(p, distribution="pareto")
     with pytest.raises(rb.RipError, match="scale factor"):
         rb.HostGraph.read_tsv(p, scale=2.0)
+    big = _write(tmp_path / "big.tsv", "1 2\n3 4294967295\n")
+    with pytest.raises(rb.RipError, match="line 2"):
+        rb.HostGraph.read_tsv(big)
 
 
 def test_read_binary_round_trip_and_errors(tmp_path):
