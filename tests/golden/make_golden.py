@@ -138,6 +138,9 @@ def sampler_reference():
             rb.WEIGHTS_UNIFORM, seed=4, lo=0.0, hi=0.3), "IC"),
         "rmat10_lt": (rb.HostGraph.rmat(10, 8 << 10, seed=5).with_weights(
             rb.WEIGHTS_LT_NORMALIZED, seed=6), "LT"),
+        # weighted cascade p = 1/indeg, the 2^24 IC workload's weight model
+        "rmat10_wc": (rb.HostGraph.rmat(10, 16 << 10, seed=9).with_weights(rb.WEIGHTS_WC),
+                      "IC"),
     }
     for name, (g, model) in graphs.items():
         path = os.path.join(tmp, name + ".bin")
