@@ -303,11 +303,15 @@ int rip_imm_pool(rip_pool *p, uint32_t k, double epsilon, double l,
  *   seeds   : k vertex ids < n (a repeated id counts once).
  *   sizes   : optional host array of `replicas` entries: the reached count of
  *             each replica.  Replica r is a pure function of (seed, r).
+ *   levels  : optional host array of `replicas` entries: the BFS levels of
+ *             each replica, the seeds' level included (the second member of
+ *             the pair ripples::simulate returns).
  * Edge e fires in replica r iff P(e>>2, r; seed, SIM_IC)[e&3] < threshold(e):
  * the same distribution as the reference's uniform01 <= p(u->v) draws, not the
  * same draws.  Returns RIP_ERR_INVALID for an LT graph or a seed >= n. */
 int rip_spread_ic(rip_graph *g, const uint32_t *seeds, uint32_t k,
-                  uint64_t replicas, uint64_t seed, uint32_t *sizes, double *spread);
+                  uint64_t replicas, uint64_t seed, uint32_t *sizes, uint32_t *levels,
+                  double *spread);
 /* Forward Monte Carlo spread under LT, the live-edge form of
  * include/ripples/diffusion_simulation.h:129-178's threshold model: in replica
  * r vertex v keeps the first in-edge j (CSR order of `bwd`) with
@@ -318,7 +322,8 @@ int rip_spread_ic(rip_graph *g, const uint32_t *seeds, uint32_t k,
  *         IMM runs on).
  * Other arguments and results as rip_spread_ic. */
 int rip_spread_lt(rip_graph *fwd, rip_graph *bwd, const uint32_t *seeds, uint32_t k,
-                  uint64_t replicas, uint64_t seed, uint32_t *sizes, double *spread);
+                  uint64_t replicas, uint64_t seed, uint32_t *sizes, uint32_t *levels,
+                  double *spread);
 
 /* ---- batching and serving --------------------------------------------------- */
 /* No counterpart in the reference (its GenerateRRRSets, include/ripples/
@@ -488,6 +493,15 @@ int rip_read_tsv(const char *path, const rip_tsv_options *opt, uint32_t *n, uint
  * is below 1.  Outputs as rip_read_tsv. */
 int rip_read_binary(const char *path, double scale, uint32_t *n, uint64_t *m,
                     uint64_t **index, uint32_t **src, float **w, uint32_t **reverse_map);
+/* The forward direction of the same format (the simulator's input: index
+ * over sources, dst u32[m] the out-edge targets). */
+int rip_read_binary_forward(const char *path, double scale, uint32_t *n, uint64_t *m,
+                            uint64_t **index, uint32_t **dst, float **w, uint32_t **reverse_map);
+/* The CSR of the transposed graph (include/ripples/graph.h:787-832): in-lists
+ * become out-lists and back, each ordered by the other endpoint (stable),
+ * weights carried along; malloc'd outputs released with rip_free. */
+int rip_transpose_csr(uint32_t n, uint64_t m, const uint64_t *index, const uint32_t *adj,
+                      const float *w, uint64_t **index_out, uint32_t **adj_out, float **w_out);
 /* Message for the last failed rip_read_* call on the calling thread. */
 const char *rip_read_error(void);
 

@@ -481,7 +481,7 @@ void *orc_sample(int model, uint32_t n, const uint64_t *index,
 uint64_t orc_spread_ic(uint32_t n, const uint64_t *index, const uint32_t *dst,
                        const uint32_t *thr, const uint32_t *seeds, uint32_t k,
                        uint64_t replicas, uint64_t seed, uint32_t *sizes,
-                       uint64_t *edges) {
+                       uint64_t *edges, uint32_t *levels) {
   uint64_t n_edges = 0;
   std::vector<uint64_t> stamp(n, ~0ull);
   std::vector<uint32_t> queue;
@@ -493,36 +493,34 @@ uint64_t orc_spread_ic(uint32_t n, const uint64_t *index, const uint32_t *dst,
         stamp[seeds[i]] = r;
         queue.push_back(seeds[i]);
       }
-    for (size_t head = 0; head < queue.size(); ++head) {
-      const uint32_t u = queue[head];
-      n_edges += index[u + 1] - index[u];
-      for (uint64_t e = index[u]; e < index[u + 1]; ++e) {
-        const uint32_t v = dst[e];
-        if (stamp[v] == r) continue;  // coins are pure: skipping is exact
-        if (sim_ic_coin(seed, r, e) < thr[e]) {
-          stamp[v] = r;
-          queue.push_back(v);
+    uint32_t lev = 0;
+    for (size_t head = 0; head < queue.size(); ++lev) {  // one BFS level per pass
+      const size_t end = queue.size();
+      for (; head < end; ++head) {
+        const uint32_t u = queue[head];
+        n_edges += index[u + 1] - index[u];
+        for (uint64_t e = index[u]; e < index[u + 1]; ++e) {
+          const uint32_t v = dst[e];
+          if (stamp[v] == r) continue;  // coins are pure: skipping is exact
+          if (sim_ic_coin(seed, r, e) < thr[e]) {
+            stamp[v] = r;
+            queue.push_back(v);
+          }
         }
       }
     }
     if (sizes) sizes[r] = (uint32_t)queue.size();
+    if (levels) levels[r] = lev;
     total += queue.size();
   }
   if (edges) *edges = n_edges;
   return total;
 }
 
-// Forward LT spread in the live-edge form of the threshold model
-// (include/ripples/diffusion_simulation.h:129-178; Kempe, Kleinberg, Tardos,
-// KDD'03): in replica r vertex v keeps the first in-edge j of the backward
-// CSR (bindex, bsrc, cum: the LT sampler's cumulative thresholds) with
-// sim_lt_threshold(seed, r, v) < cum[j], or none, and v is reached iff that
-// in-edge's source is.  BFS from the seeds over the forward CSR (findex,
-// fdst).  Returns the sum of the reached counts.
 uint64_t orc_spread_lt(uint32_t n, const uint64_t *findex, const uint32_t *fdst,
                        const uint64_t *bindex, const uint32_t *bsrc, const uint32_t *cum,
                        const uint32_t *seeds, uint32_t k, uint64_t replicas, uint64_t seed,
-                       uint32_t *sizes) {
+                       uint32_t *sizes, uint32_t *levels) {
   std::vector<uint64_t> stamp(n, ~0ull);
   std::vector<uint32_t> queue;
   uint64_t total = 0;
@@ -533,21 +531,26 @@ uint64_t orc_spread_lt(uint32_t n, const uint64_t *findex, const uint32_t *fdst,
         stamp[seeds[i]] = r;
         queue.push_back(seeds[i]);
       }
-    for (size_t head = 0; head < queue.size(); ++head) {
-      const uint32_t u = queue[head];
-      for (uint64_t e = findex[u]; e < findex[u + 1]; ++e) {
-        const uint32_t v = fdst[e];
-        if (stamp[v] == r) continue;
-        const uint32_t t = sim_lt_threshold(seed, r, v);
-        uint64_t j = bindex[v];
-        while (j < bindex[v + 1] && !(t < cum[j])) ++j;  // first j, CSR order
-        if (j < bindex[v + 1] && bsrc[j] == u) {
-          stamp[v] = r;
-          queue.push_back(v);
+    uint32_t lev = 0;
+    for (size_t head = 0; head < queue.size(); ++lev) {
+      const size_t end = queue.size();
+      for (; head < end; ++head) {
+        const uint32_t u = queue[head];
+        for (uint64_t e = findex[u]; e < findex[u + 1]; ++e) {
+          const uint32_t v = fdst[e];
+          if (stamp[v] == r) continue;
+          const uint32_t t = sim_lt_threshold(seed, r, v);
+          uint64_t j = bindex[v];
+          while (j < bindex[v + 1] && !(t < cum[j])) ++j;  // first j, CSR order
+          if (j < bindex[v + 1] && bsrc[j] == u) {
+            stamp[v] = r;
+            queue.push_back(v);
+          }
         }
       }
     }
     if (sizes) sizes[r] = (uint32_t)queue.size();
+    if (levels) levels[r] = lev;
     total += queue.size();
   }
   return total;

@@ -43,8 +43,8 @@ def _load_oracle() -> ctypes.CDLL:
         "orc_pack_ic": (None, [P, U64, P]),
         "orc_pack_lt": (None, [P, U32, P, P]),
         "orc_sample": (P, [I32, U32, P, P, P, U64, U64, U64, P]),
-        "orc_spread_ic": (U64, [U32, P, P, P, P, U32, U64, U64, P, ctypes.POINTER(U64)]),
-        "orc_spread_lt": (U64, [U32, P, P, P, P, P, P, U32, U64, U64, P]),
+        "orc_spread_ic": (U64, [U32, P, P, P, P, U32, U64, U64, P, ctypes.POINTER(U64), P]),
+        "orc_spread_lt": (U64, [U32, P, P, P, P, P, P, U32, U64, U64, P, P]),
         "orc_find_coverage": (U64, [U64, P, P, P, U32]),
         "orc_opimc": (U32, [I32, U32, P, P, P, U32, ctypes.c_float, ctypes.c_float, U64, I32, P,
                             ctypes.POINTER(U64), ctypes.POINTER(U32), P]),
@@ -118,7 +118,8 @@ def sample(model: str, n: int, index: np.ndarray, src: np.ndarray, thr: np.ndarr
 
 
 def spread_ic(n: int, index: np.ndarray, dst: np.ndarray, thr: np.ndarray, seeds,
-              replicas: int, seed: int = 0, with_edges: bool = False):
+              replicas: int, seed: int = 0, with_edges: bool = False,
+              with_levels: bool = False):
     """Forward IC spread over the forward CSR (index over sources, dst the
     out-edge targets, IC thresholds): (mean reached count, per-replica
     counts), plus the out-edges of the reached vertices summed over the
@@ -135,15 +136,19 @@ def spread_ic(n: int, index: np.ndarray, dst: np.ndarray, thr: np.ndarray, seeds
         sd = np.zeros(1, np.uint32)
     sizes = np.zeros(max(replicas, 1), dtype=np.uint32)
     edges = ctypes.c_uint64()
+    levels = np.zeros(max(replicas, 1), dtype=np.uint32)
     total = L.orc_spread_ic(n, _ptr(idx), _ptr(d), _ptr(t), _ptr(sd), k, replicas, seed,
-                            _ptr(sizes), ctypes.byref(edges))
+                            _ptr(sizes), ctypes.byref(edges), _ptr(levels))
     mean = total / replicas if replicas else 0.0
+    out = [mean, sizes[:replicas]]
     if with_edges:
-        return mean, sizes[:replicas], edges.value
-    return mean, sizes[:replicas]
+        out.append(edges.value)
+    if with_levels:
+        out.append(levels[:replicas])
+    return tuple(out)
 
 
-def spread_lt(g, seeds, replicas: int, seed: int = 0) -> Tuple[float, np.ndarray]:
+def spread_lt(g, seeds, replicas: int, seed: int = 0, with_levels: bool = False):
     """Forward LT spread (live-edge form) on backward HostGraph ``g`` with LT
     weights: (mean reached count, per-replica counts)."""
     f = g.forward()
@@ -160,9 +165,13 @@ def spread_lt(g, seeds, replicas: int, seed: int = 0) -> Tuple[float, np.ndarray
     if k == 0:
         sd = np.zeros(1, np.uint32)
     sizes = np.zeros(max(replicas, 1), dtype=np.uint32)
+    levels = np.zeros(max(replicas, 1), dtype=np.uint32)
     total = L.orc_spread_lt(g.n, _ptr(fi), _ptr(fd), _ptr(bi), _ptr(bs), _ptr(c), _ptr(sd), k,
-                            replicas, seed, _ptr(sizes))
-    return (total / replicas if replicas else 0.0), sizes[:replicas]
+                            replicas, seed, _ptr(sizes), _ptr(levels))
+    mean = total / replicas if replicas else 0.0
+    if with_levels:
+        return mean, sizes[:replicas], levels[:replicas]
+    return mean, sizes[:replicas]
 
 
 def opimc(model: str, n: int, index, src, thr, k: int, epsilon: float, delta: float,
@@ -284,6 +293,7 @@ def reference() -> Optional[ctypes.CDLL]:
             "ref_pool_free": (None, [P]),
             "ref_simulate": (DBL, [ctypes.c_char_p, I32, P, U32, U64, U64]),
             "ref_simulate_parallel": (DBL, [ctypes.c_char_p, I32, P, U32, U64]),
+            "ref_simulate_levels": (DBL, [ctypes.c_char_p, I32, P, U32, U64, U64]),
             "ref_graph_load_tsv": (P, [ctypes.c_char_p, I32, I32, I32]),
             "ref_opimc_theta_max": (U64, [U64, ctypes.c_float, U64, ctypes.c_float]),
             "ref_opimc_theta_zero": (U64, [U64, ctypes.c_float, U64, ctypes.c_float]),

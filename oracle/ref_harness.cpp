@@ -278,4 +278,29 @@ double ref_simulate(const char *fwd_path, int model, const uint32_t *seeds,
   return acc / (double)replicas;
 }
 
+// The mean of the second member of ripples::simulate's result (BFS levels /
+// rounds, the seeds' included), replicas as ref_simulate runs them.
+double ref_simulate_levels(const char *fwd_path, int model, const uint32_t *seeds,
+                           uint32_t nseeds, uint64_t replicas, uint64_t seed) {
+  ensure_console();
+  ripples::GraphFwd G;
+  G.load_binary(fwd_path);
+  std::vector<uint32_t> S(seeds, seeds + nseeds);
+  trng::lcg64 gen;
+  gen.seed(seed);
+  gen.split(2, 1);
+  double acc = 0.0;
+  for (uint64_t r = 0; r < replicas; ++r) {
+    std::pair<size_t, size_t> res;
+    if (model == 0)
+      res = ripples::simulate(G, S.begin(), S.end(), gen,
+                              ripples::independent_cascade_tag{});
+    else
+      res = ripples::simulate(G, S.begin(), S.end(), gen,
+                              ripples::linear_threshold_tag{});
+    acc += (double)res.second;
+  }
+  return acc / (double)replicas;
+}
+
 }  // extern "C"

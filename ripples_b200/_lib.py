@@ -140,8 +140,8 @@ SIGNATURES = {
     "rip_imm_pool": (I32, [P, U32, DBL, DBL, U64, I32, I32, P, ctypes.POINTER(U32),
                            ctypes.POINTER(ImmRecord)]),
     "rip_sample_multi": (I32, [P, P, P, P, U32]),
-    "rip_spread_ic": (I32, [P, P, U32, U64, U64, P, ctypes.POINTER(ctypes.c_double)]),
-    "rip_spread_lt": (I32, [P, P, P, U32, U64, U64, P, ctypes.POINTER(ctypes.c_double)]),
+    "rip_spread_ic": (I32, [P, P, U32, U64, U64, P, P, ctypes.POINTER(ctypes.c_double)]),
+    "rip_spread_lt": (I32, [P, P, P, U32, U64, U64, P, P, ctypes.POINTER(ctypes.c_double)]),
     "rip_imm_batch": (I32, [P, ctypes.POINTER(ImmQuery), U32]),
     "rip_server_create": (I32, [P, SZ, U32, PP]),
     "rip_server_destroy": (I32, [P]),
@@ -166,6 +166,9 @@ SIGNATURES = {
     "rip_read_binary": (I32, [ctypes.c_char_p, ctypes.c_double, ctypes.POINTER(U32),
                               ctypes.POINTER(U64), P, P, P, P]),
     "rip_read_error": (ctypes.c_char_p, []),
+    "rip_read_binary_forward": (I32, [ctypes.c_char_p, ctypes.c_double, ctypes.POINTER(U32),
+                                      ctypes.POINTER(U64), P, P, P, P]),
+    "rip_transpose_csr": (I32, [U32, U64, P, P, P, P, P, P]),
     "rip_opimc_theta_max": (U64, [U64, ctypes.c_float, U64, ctypes.c_float]),
     "rip_opimc_theta_zero": (U64, [U64, ctypes.c_float, U64, ctypes.c_float]),
     "rip_opimc_lower_bound": (ctypes.c_float, [U64, ctypes.c_float, U64, U64]),

@@ -23,6 +23,8 @@ OBJ = os.path.join(PKG, "_lib", "obj")
 LIB = os.path.join(PKG, "_lib", "libripples_b200.so")
 TOOL = os.path.join(PKG, "_lib", "imm_b200")
 TOOL_SRC = os.path.join(PKG, "tools", "imm_b200.cpp")
+SIM_TOOL = os.path.join(PKG, "_lib", "simulator_b200")
+SIM_TOOL_SRC = os.path.join(PKG, "tools", "simulator_b200.cpp")
 INCLUDE = os.path.join(ROOT, "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -81,16 +83,18 @@ def build(verbose: bool = False) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
-    # the drop-in imm command-line tool (host C++ over the C ABI)
-    if _stale(TOOL, [TOOL_SRC, LIB] + _headers()):
-        cxx = shutil.which("g++") or "g++"
-        cmd = [cxx, "-O2", "-std=c++17", "-I" + INCLUDE, TOOL_SRC, "-o", TOOL,
-               "-L" + os.path.dirname(LIB), "-lripples_b200", "-Wl,-rpath,$ORIGIN"]
-        if verbose:
-            print(" ".join(cmd), flush=True)
-        r = subprocess.run(cmd, capture_output=True, text=True)
-        if r.returncode != 0:
-            raise RuntimeError(f"imm_b200 build failed:\n{r.stdout}\n{r.stderr}")
+    # the drop-in imm and simulator command-line tools (host C++ over the C ABI)
+    for tool, src in ((TOOL, TOOL_SRC), (SIM_TOOL, SIM_TOOL_SRC)):
+        if _stale(tool, [src, LIB] + _headers()):
+            cxx = shutil.which("g++") or "g++"
+            cmd = [cxx, "-O2", "-std=c++17", "-I" + INCLUDE, src, "-o", tool,
+                   "-L" + os.path.dirname(LIB), "-lripples_b200", "-Wl,-rpath,$ORIGIN"]
+            if verbose:
+                print(" ".join(cmd), flush=True)
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            if r.returncode != 0:
+                raise RuntimeError(f"{os.path.basename(tool)} build failed:\n{r.stdout}\n"
+                                   f"{r.stderr}")
     return LIB
 
 

@@ -17,7 +17,9 @@
 //                    "not taking" mass, as loaders.h:169-191 does.
 //   rip_read_binary  the reference binary format (include/ripples/
 //                    graph.h:854-995, backward direction): header, id map,
-//                    offsets, sources, float weights.
+//                    offsets, sources, float weights; rip_read_binary_forward
+//                    the forward direction (the simulator's input).
+//   rip_transpose_csr  backward <-> forward CSR on the host (graph.h:787-832).
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -196,9 +198,13 @@ extern "C" int rip_read_tsv(const char *path, const rip_tsv_options *o, uint32_t
                   map_out);
 }
 
-extern "C" int rip_read_binary(const char *path, double scale, uint32_t *n_out,
-                               uint64_t *m_out, uint64_t **index_out, uint32_t **src_out,
-                               float **w_out, uint32_t **map_out) {
+namespace {
+
+// The reference binary format in one direction: magic 0xa1ccac0f for the
+// backward CSR (in-edges), 0xf0cacc1a for the forward one (out-edges).
+int read_binary(const char *path, uint64_t magic, double scale, uint32_t *n_out,
+                uint64_t *m_out, uint64_t **index_out, uint32_t **src_out, float **w_out,
+                uint32_t **map_out) {
   if (!path || !n_out || !m_out || !index_out || !src_out || !w_out || !map_out)
     return read_fail("rip_read_binary: null argument");
   std::ifstream in(path, std::ios::binary);
@@ -207,7 +213,7 @@ extern "C" int rip_read_binary(const char *path, double scale, uint32_t *n_out,
   in.read(reinterpret_cast<char *>(hdr), sizeof(hdr));
   if (!in || hdr[0] != 0xc0ffeeull)
     return read_fail("The endianess check failed when reloading the input binary.");
-  if (hdr[1] != 0xa1ccac0full)
+  if (hdr[1] != magic)
     return read_fail(
         "You are loading a binary that is not compatible with the algorithm you are trying to "
         "run.");
@@ -229,4 +235,59 @@ extern "C" int rip_read_binary(const char *path, double scale, uint32_t *n_out,
     for (auto &x : w) x = (float)(x * scale);
   return hand_out(n, index, src, w, reverse_map, n_out, m_out, index_out, src_out, w_out,
                   map_out);
+}
+
+}  // namespace
+
+extern "C" int rip_read_binary(const char *path, double scale, uint32_t *n_out,
+                               uint64_t *m_out, uint64_t **index_out, uint32_t **src_out,
+                               float **w_out, uint32_t **map_out) {
+  return read_binary(path, 0xa1ccac0full, scale, n_out, m_out, index_out, src_out, w_out,
+                     map_out);
+}
+
+extern "C" int rip_read_binary_forward(const char *path, double scale, uint32_t *n_out,
+                                       uint64_t *m_out, uint64_t **index_out,
+                                       uint32_t **dst_out, float **w_out, uint32_t **map_out) {
+  return read_binary(path, 0xf0cacc1aull, scale, n_out, m_out, index_out, dst_out, w_out,
+                     map_out);
+}
+
+// The CSR of the transposed graph: out-lists become in-lists and back, each
+// list ordered by the other endpoint's id (stable: parallel edges keep their
+// order), weights carried along.
+extern "C" int rip_transpose_csr(uint32_t n, uint64_t m, const uint64_t *index,
+                                 const uint32_t *adj, const float *w, uint64_t **index_out,
+                                 uint32_t **adj_out, float **w_out) {
+  if ((n && !index) || (m && (!adj || !w)) || !index_out || !adj_out || !w_out)
+    return read_fail("rip_transpose_csr: null argument");
+  std::vector<uint64_t> t_index((size_t)n + 1, 0);
+  for (uint64_t e = 0; e < m; ++e) {
+    if (adj[e] >= n) return read_fail("rip_transpose_csr: vertex out of range");
+    t_index[adj[e] + 1]++;
+  }
+  for (uint32_t v = 0; v < n; ++v) t_index[v + 1] += t_index[v];
+  std::vector<uint64_t> cursor(t_index.begin(), t_index.begin() + n);
+  std::vector<uint32_t> t_adj(m);
+  std::vector<float> t_w(m);
+  for (uint32_t v = 0; v < n; ++v)  // v ascending: each new list is ordered by v
+    for (uint64_t e = index[v]; e < index[v + 1]; ++e) {
+      const uint64_t at = cursor[adj[e]]++;
+      t_adj[at] = v;
+      t_w[at] = w[e];
+    }
+  uint64_t *pi = copy_out(t_index);
+  uint32_t *pa = copy_out(t_adj);
+  float *pw = copy_out(t_w);
+  if (!pi || !pa || !pw) {
+    std::free(pi);
+    std::free(pa);
+    std::free(pw);
+    g_read_error = "out of host memory";
+    return RIP_ERR_NOMEM;
+  }
+  *index_out = pi;
+  *adj_out = pa;
+  *w_out = pw;
+  return RIP_OK;
 }

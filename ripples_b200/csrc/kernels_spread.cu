@@ -98,8 +98,9 @@ spread_kernel(SpreadLaunch L) {
       }
     }
     __syncthreads();
-    uint32_t lo = 0, hi = min(s_qlen, L.qcap);
+    uint32_t lo = 0, hi = min(s_qlen, L.qcap), levels = 0;
     while (lo < hi) {
+      ++levels;  // one BFS level (the seeds are the first)
       for (uint32_t cb = lo; cb < hi; cb += SIM_THREADS) {
         const uint32_t e = cb + tid;
         uint32_t beg = 0, end = 0;
@@ -169,6 +170,7 @@ spread_kernel(SpreadLaunch L) {
     const uint32_t qlen = min(s_qlen, L.qcap);
     if (tid == 0) {
       if (L.sizes) L.sizes[r] = qlen;
+      if (L.levels) L.levels[r] = levels;
       reached += qlen;
     }
     for (uint32_t i = tid; i < qlen; i += SIM_THREADS) bm[q[i] >> 5] = 0u;

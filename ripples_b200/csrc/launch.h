@@ -142,6 +142,7 @@ struct SpreadLaunch {
   unsigned long long *next = nullptr;   // replica counter (zeroed)
   unsigned long long *total = nullptr;  // sum of reached counts (zeroed)
   uint32_t *sizes = nullptr;      // per replica reached count, or null
+  uint32_t *levels = nullptr;     // per replica BFS levels (seeds' included), or null
   uint32_t *bitmaps = nullptr;    // per CTA slot, bm_words words, all-zero
   uint64_t bm_words = 0;
   uint32_t *queues = nullptr;     // per CTA slot, qcap = n entries

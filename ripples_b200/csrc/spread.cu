@@ -10,8 +10,8 @@
 namespace {
 
 int spread_run(rip_graph *g, rip_graph *b, const uint32_t *seeds, uint32_t k,
-               uint64_t replicas, uint64_t seed, uint32_t *sizes, double *spread,
-               const char *who) {
+               uint64_t replicas, uint64_t seed, uint32_t *sizes, uint32_t *levels,
+               double *spread, const char *who) {
   rip_ctx *c = g->ctx;
   if ((k && !seeds) || !spread) return set_err(c, RIP_ERR_INVALID, "%s: null argument", who);
   for (uint32_t i = 0; i < k; ++i)
@@ -35,18 +35,20 @@ int spread_run(rip_graph *g, rip_graph *b, const uint32_t *seeds, uint32_t k,
 
   struct Buffers {
     rip_ctx *c;
-    DevMem scratch, ctr, d_seeds, d_sizes;
+    DevMem scratch, ctr, d_seeds, d_sizes, d_levels;
     ~Buffers() {
       dfree(c, scratch);
       dfree(c, ctr);
       dfree(c, d_seeds);
       dfree(c, d_sizes);
+      dfree(c, d_levels);
     }
-  } B{c, {}, {}, {}, {}};
+  } B{c, {}, {}, {}, {}, {}};
   TRY(dalloc(c, B.scratch, slots * per_slot));
   TRY(dalloc(c, B.ctr, 2 * sizeof(unsigned long long)));
   TRY(dalloc(c, B.d_seeds, sizeof(uint32_t) * std::max<uint32_t>(k, 1)));
   if (sizes) TRY(dalloc(c, B.d_sizes, sizeof(uint32_t) * replicas));
+  if (levels) TRY(dalloc(c, B.d_levels, sizeof(uint32_t) * replicas));
   CK(c, cudaMemsetAsync(B.scratch.p, 0, slots * bm_words * 4, c->stream));
   CK(c, cudaMemsetAsync(B.ctr.p, 0, 2 * sizeof(unsigned long long), c->stream));
   if (k)
@@ -63,6 +65,7 @@ int spread_run(rip_graph *g, rip_graph *b, const uint32_t *seeds, uint32_t k,
   L.next = ptr<unsigned long long>(B.ctr);
   L.total = L.next + 1;
   L.sizes = sizes ? ptr<uint32_t>(B.d_sizes) : nullptr;
+  L.levels = levels ? ptr<uint32_t>(B.d_levels) : nullptr;
   L.bitmaps = ptr<uint32_t>(B.scratch);
   L.bm_words = bm_words;
   L.queues = L.bitmaps + slots * bm_words;
@@ -75,6 +78,9 @@ int spread_run(rip_graph *g, rip_graph *b, const uint32_t *seeds, uint32_t k,
   if (sizes)
     CK(c, cudaMemcpyAsync(sizes, B.d_sizes.p, sizeof(uint32_t) * replicas,
                           cudaMemcpyDeviceToHost, c->stream));
+  if (levels)
+    CK(c, cudaMemcpyAsync(levels, B.d_levels.p, sizeof(uint32_t) * replicas,
+                          cudaMemcpyDeviceToHost, c->stream));
   CK(c, cudaStreamSynchronize(c->stream));
   *spread = (double)total / (double)replicas;
   return RIP_OK;
@@ -84,17 +90,18 @@ int spread_run(rip_graph *g, rip_graph *b, const uint32_t *seeds, uint32_t k,
 
 extern "C" int rip_spread_ic(rip_graph *g, const uint32_t *seeds, uint32_t k,
                              uint64_t replicas, uint64_t seed, uint32_t *sizes,
-                             double *spread) {
+                             uint32_t *levels, double *spread) {
   if (!g) return RIP_ERR_INVALID;
   if (g->model != RIP_MODEL_IC)
     return set_err(g->ctx, RIP_ERR_INVALID,
                    "rip_spread_ic: the graph must be an IC graph holding the forward CSR");
-  return spread_run(g, nullptr, seeds, k, replicas, seed, sizes, spread, "rip_spread_ic");
+  return spread_run(g, nullptr, seeds, k, replicas, seed, sizes, levels, spread,
+                    "rip_spread_ic");
 }
 
 extern "C" int rip_spread_lt(rip_graph *fwd, rip_graph *bwd, const uint32_t *seeds,
                              uint32_t k, uint64_t replicas, uint64_t seed, uint32_t *sizes,
-                             double *spread) {
+                             uint32_t *levels, double *spread) {
   if (!fwd || !bwd) return RIP_ERR_INVALID;
   if (bwd->model != RIP_MODEL_LT || fwd->ctx != bwd->ctx)
     return set_err(fwd->ctx, RIP_ERR_INVALID,
@@ -102,5 +109,6 @@ extern "C" int rip_spread_lt(rip_graph *fwd, rip_graph *bwd, const uint32_t *see
   if (fwd->n != bwd->n || fwd->m != bwd->m)
     return set_err(fwd->ctx, RIP_ERR_INVALID,
                    "rip_spread_lt: forward and backward CSR differ in size");
-  return spread_run(fwd, bwd, seeds, k, replicas, seed, sizes, spread, "rip_spread_lt");
+  return spread_run(fwd, bwd, seeds, k, replicas, seed, sizes, levels, spread,
+                    "rip_spread_lt");
 }

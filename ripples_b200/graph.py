@@ -123,15 +123,39 @@ class HostGraph:
         return cls._from_read(rc, n, m, pi, ps, pw, pm, "rip_read_tsv")
 
     @classmethod
-    def read_binary(cls, path: str, scale: float = 1.0) -> Tuple["HostGraph", np.ndarray]:
-        """The reference binary format (``rip_read_binary``); returns (graph,
-        reverse id map)."""
+    def read_binary(cls, path: str, scale: float = 1.0,
+                    forward: bool = False) -> Tuple["HostGraph", np.ndarray]:
+        """The reference binary format (``rip_read_binary``; with ``forward``
+        the forward direction, ``rip_read_binary_forward``, whose CSR is indexed
+        by source); returns (graph, reverse id map)."""
         n, m = ctypes.c_uint32(), ctypes.c_uint64()
         pi, ps, pw, pm = (ctypes.c_void_p() for _ in range(4))
-        rc = lib.rip_read_binary(path.encode(), scale, ctypes.byref(n), ctypes.byref(m),
-                                 ctypes.byref(pi), ctypes.byref(ps), ctypes.byref(pw),
-                                 ctypes.byref(pm))
+        fn = lib.rip_read_binary_forward if forward else lib.rip_read_binary
+        rc = fn(path.encode(), scale, ctypes.byref(n), ctypes.byref(m), ctypes.byref(pi),
+                ctypes.byref(ps), ctypes.byref(pw), ctypes.byref(pm))
         return cls._from_read(rc, n, m, pi, ps, pw, pm, "rip_read_binary")
+
+    def transposed(self) -> "HostGraph":
+        """The CSR of the transposed graph (``rip_transpose_csr``): in-lists
+        become out-lists, each ordered by the other endpoint."""
+        pi, pa, pw = (ctypes.c_void_p() for _ in range(3))
+        idx = np.ascontiguousarray(self.index, dtype=np.uint64)
+        adj = np.ascontiguousarray(self.src, dtype=np.uint32)
+        w = np.ascontiguousarray(self.weights if self.weights is not None
+                                 else np.zeros(self.m, np.float32), dtype=np.float32)
+        rc = lib.rip_transpose_csr(self.n, self.m, _ptr(idx), _ptr(adj), _ptr(w),
+                                   ctypes.byref(pi), ctypes.byref(pa), ctypes.byref(pw))
+        if rc != 0:
+            raise RipError(rc, "rip_transpose_csr", (lib.rip_read_error() or b"").decode())
+
+        def take(p, ctype, count, dtype):
+            a = (np.ctypeslib.as_array(ctypes.cast(p, ctypes.POINTER(ctype)), shape=(count,)).copy()
+                 if count else np.zeros(0, dtype=dtype))
+            lib.rip_free(p)
+            return a
+        return HostGraph(self.n, take(pi, ctypes.c_uint64, self.n + 1, np.uint64),
+                         take(pa, ctypes.c_uint32, self.m, np.uint32),
+                         take(pw, ctypes.c_float, self.m, np.float32))
 
     def with_weights(self, kind: int, seed: int = 1, lo: float = 0.0,
                      hi: float = 1.0) -> "HostGraph":
@@ -458,32 +482,44 @@ def sample_multi(ctx: Context, pools, seeds, counts) -> None:
 
 
 def spread_ic(graph: DeviceGraph, seeds, replicas: int, seed: int = 0,
-              with_sizes: bool = False):
+              with_sizes: bool = False, with_levels: bool = False):
     """Forward Monte Carlo spread of ``seeds`` under IC (``rip_spread_ic``):
     ``graph`` is an IC ``DeviceGraph`` of the FORWARD CSR
     (``HostGraph.forward()``).  Returns the mean reached count, and with
-    ``with_sizes`` also each replica's count."""
+    ``with_sizes`` / ``with_levels`` also each replica's count / BFS levels."""
     sd = np.ascontiguousarray(seeds, dtype=np.uint32)
     sizes = np.zeros(max(replicas, 1), dtype=np.uint32) if with_sizes else None
+    levels = np.zeros(max(replicas, 1), dtype=np.uint32) if with_levels else None
     out = ctypes.c_double()
     check(lib.rip_spread_ic(graph.h, _ptr(sd) if sd.size else None, int(sd.size), replicas, seed,
-                            _ptr(sizes), ctypes.byref(out)), "rip_spread_ic", graph.ctx.h)
-    return (out.value, sizes[:replicas]) if with_sizes else out.value
+                            _ptr(sizes), _ptr(levels), ctypes.byref(out)), "rip_spread_ic",
+          graph.ctx.h)
+    return _spread_result(out.value, sizes, levels, replicas)
+
+
+def _spread_result(mean, sizes, levels, replicas):
+    res = [mean]
+    if sizes is not None:
+        res.append(sizes[:replicas])
+    if levels is not None:
+        res.append(levels[:replicas])
+    return res[0] if len(res) == 1 else tuple(res)
 
 
 def spread_lt(forward: DeviceGraph, backward: DeviceGraph, seeds, replicas: int,
-              seed: int = 0, with_sizes: bool = False):
+              seed: int = 0, with_sizes: bool = False, with_levels: bool = False):
     """Forward Monte Carlo spread of ``seeds`` under LT (``rip_spread_lt``):
     ``forward`` holds the forward CSR (``HostGraph.forward()``, any model),
     ``backward`` is the same graph's LT ``DeviceGraph``.  Returns the mean
     reached count, and with ``with_sizes`` also each replica's count."""
     sd = np.ascontiguousarray(seeds, dtype=np.uint32)
     sizes = np.zeros(max(replicas, 1), dtype=np.uint32) if with_sizes else None
+    levels = np.zeros(max(replicas, 1), dtype=np.uint32) if with_levels else None
     out = ctypes.c_double()
     check(lib.rip_spread_lt(forward.h, backward.h, _ptr(sd) if sd.size else None, int(sd.size),
-                            replicas, seed, _ptr(sizes), ctypes.byref(out)), "rip_spread_lt",
-          forward.ctx.h)
-    return (out.value, sizes[:replicas]) if with_sizes else out.value
+                            replicas, seed, _ptr(sizes), _ptr(levels), ctypes.byref(out)),
+          "rip_spread_lt", forward.ctx.h)
+    return _spread_result(out.value, sizes, levels, replicas)
 
 
 class Query:

@@ -41,9 +41,13 @@ def test_spread_bit_exact_vs_oracle(ctx, scale, deg, hi, seeds, replicas):
         g = g.with_weights(rb.WEIGHTS_UNIFORM, seed=scale + 50, lo=0.0, hi=hi)
     dg = forward_device(ctx, g)
     try:
-        mean, sizes = rb.spread_ic(dg, seeds, replicas, seed=21, with_sizes=True)
-        o_mean, o_sizes = oracle_spread(g, seeds, replicas, seed=21)
-        assert np.array_equal(sizes, o_sizes)
+        mean, sizes, levels = rb.spread_ic(dg, seeds, replicas, seed=21, with_sizes=True,
+                                           with_levels=True)
+        f = g.forward()
+        thr = O.pack("IC", f.index, f.weights)
+        o_mean, o_sizes, o_levels = O.spread_ic(f.n, f.index, f.src, thr, seeds, replicas,
+                                                seed=21, with_levels=True)
+        assert np.array_equal(sizes, o_sizes) and np.array_equal(levels, o_levels)
         assert mean == pytest.approx(o_mean, rel=0, abs=1e-9)
         assert rb.spread_ic(dg, seeds, replicas, seed=21) == mean  # without the sizes
     finally:
@@ -104,9 +108,10 @@ def test_spread_lt_bit_exact_vs_oracle(ctx, scale, deg, kind, seeds, replicas):
         g = g.with_weights(rb.WEIGHTS_UNIFORM, seed=scale + 60, lo=0.0, hi=0.1)
     fg, bg = forward_device(ctx, g), rb.DeviceGraph(ctx, g, "LT")
     try:
-        mean, sizes = rb.spread_lt(fg, bg, seeds, replicas, seed=23, with_sizes=True)
-        o_mean, o_sizes = O.spread_lt(g, seeds, replicas, seed=23)
-        assert np.array_equal(sizes, o_sizes)
+        mean, sizes, levels = rb.spread_lt(fg, bg, seeds, replicas, seed=23, with_sizes=True,
+                                           with_levels=True)
+        o_mean, o_sizes, o_levels = O.spread_lt(g, seeds, replicas, seed=23, with_levels=True)
+        assert np.array_equal(sizes, o_sizes) and np.array_equal(levels, o_levels)
         assert mean == pytest.approx(o_mean, rel=0, abs=1e-9)
     finally:
         bg.close()

@@ -268,3 +268,23 @@ def test_opimc_arithmetic_matches_reference_golden():
     for cov, d, n, theta, lo, up in rows["bounds"]:
         assert bits(lib.rip_opimc_lower_bound(cov, f(d), n, theta)) == lo
         assert bits(lib.rip_opimc_upper_bound(cov, f(d), n, theta)) == up
+
+
+def test_transpose_and_forward_binary(tmp_path):
+    # rip_transpose_csr gives the forward CSR HostGraph.forward() builds (and
+    # back), and the forward binary format reads back as that CSR
+    g = rb.HostGraph.rmat(9, 4000, seed=5).with_weights(rb.WEIGHTS_UNIFORM, seed=2, lo=0, hi=1)
+    f = g.forward()
+    t = g.transposed()
+    assert np.array_equal(t.index, f.index) and np.array_equal(t.src, f.src)
+    assert np.array_equal(t.weights, f.weights)
+    back = t.transposed()
+    assert np.array_equal(back.index, g.index) and np.array_equal(back.src, g.src)
+    assert np.array_equal(back.weights, g.weights)
+    p = str(tmp_path / "gf.bin")
+    g.write_binary(p, backward=False)
+    h, rmap = rb.HostGraph.read_binary(p, forward=True)
+    assert np.array_equal(h.index, f.index) and np.array_equal(h.src, f.src)
+    assert np.array_equal(h.weights, f.weights) and np.array_equal(rmap, np.arange(g.n))
+    with pytest.raises(rb.RipError, match="not compatible"):
+        rb.HostGraph.read_binary(p)  # a forward file is not a backward one
