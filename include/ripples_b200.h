@@ -325,6 +325,32 @@ int rip_spread_lt(rip_graph *fwd, rip_graph *bwd, const uint32_t *seeds, uint32_
                   uint64_t replicas, uint64_t seed, uint32_t *sizes, uint32_t *levels,
                   double *spread);
 
+/* ---- OPIM-C --------------------------------------------------------------- */
+/* FindCoverage (include/ripples/opimc.h:101-118): the number of sets among the
+ * pool's first num_sets holding at least one of the k seeds. */
+int rip_coverage(rip_pool *p, uint64_t num_sets, const uint32_t *seeds, uint32_t k,
+                 uint64_t *covered);
+
+typedef struct rip_opimc_record {
+  uint64_t theta_zero, theta_max;  /* eq. (17), (16) */
+  uint64_t theta;                  /* final sets per pool */
+  uint32_t rounds;                 /* selections run */
+  uint64_t coverage1, coverage2;   /* of the last round: greedy on R1, seeds on R2 */
+  float lower, upper;              /* the last round's bounds (eq. 5, 8) */
+  double total_ms;
+} rip_opimc_record;
+
+/* OPIM-C (include/ripples/opimc.h:150-243) on two pools of one graph: R1 holds
+ * the sets of key `seed`, R2 those of key seed + 0x9E3779B97F4A7C15, both
+ * cleared first and grown from theta_0 sets, doubling, until the lower bound
+ * of the seeds' spread (their coverage of R2) reaches (1 - 1/e - epsilon)
+ * times the upper bound of the optimum (the greedy coverage of R1), or theta
+ * reaches theta_max (the paper's cap; the reference has none).  Seeds are
+ * picked on R1 with `tiebreak`. */
+int rip_opimc_pool(rip_pool *r1, rip_pool *r2, uint32_t k, float epsilon, float delta,
+                   uint64_t seed, int tiebreak, int sampler, uint32_t *seeds,
+                   uint32_t *num_seeds, rip_opimc_record *record);
+
 /* ---- batching and serving --------------------------------------------------- */
 /* No counterpart in the reference (its GenerateRRRSets, include/ripples/
  * generate_rrr_sets.h:60-120, fills one instance's sets per call).  Extends

@@ -9,7 +9,7 @@ from ._lib import (MODEL_IC, MODEL_LT, SAMPLER_AUTO, SAMPLER_FUSED, SAMPLER_PLAI
                    TIE_LOWEST_ID, TIE_REF_HEAP, WEIGHTS_LT_NORMALIZED, WEIGHTS_UNIFORM,
                    WEIGHTS_WC, RipError)
 from .graph import (Context, DeviceGraph, HostGraph, Pool, Query, Server, imm_batch, sample_multi,
-                    spread_ic, spread_lt)
+                    opimc, spread_ic, spread_lt)
 from .imm import (B200RRRGenerator, FindMostInfluentialSet, GenerateRRRSets, IMM,
                   IMMConfiguration, IMMExecutionRecord, independent_cascade_tag,
                   linear_threshold_tag, omp_parallel_tag, sequential_tag)

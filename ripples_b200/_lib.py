@@ -72,6 +72,20 @@ class TsvOptions(ctypes.Structure):
     ]
 
 
+class OpimcRecord(ctypes.Structure):
+    _fields_ = [
+        ("theta_zero", ctypes.c_uint64),
+        ("theta_max", ctypes.c_uint64),
+        ("theta", ctypes.c_uint64),
+        ("rounds", ctypes.c_uint32),
+        ("coverage1", ctypes.c_uint64),
+        ("coverage2", ctypes.c_uint64),
+        ("lower", ctypes.c_float),
+        ("upper", ctypes.c_float),
+        ("total_ms", ctypes.c_double),
+    ]
+
+
 class ImmQuery(ctypes.Structure):
     _fields_ = [
         ("graph", ctypes.c_void_p),
@@ -169,6 +183,9 @@ SIGNATURES = {
     "rip_read_binary_forward": (I32, [ctypes.c_char_p, ctypes.c_double, ctypes.POINTER(U32),
                                       ctypes.POINTER(U64), P, P, P, P]),
     "rip_transpose_csr": (I32, [U32, U64, P, P, P, P, P, P]),
+    "rip_coverage": (I32, [P, U64, P, U32, ctypes.POINTER(U64)]),
+    "rip_opimc_pool": (I32, [P, P, U32, ctypes.c_float, ctypes.c_float, U64, I32, I32, P,
+                             ctypes.POINTER(U32), ctypes.POINTER(OpimcRecord)]),
     "rip_opimc_theta_max": (U64, [U64, ctypes.c_float, U64, ctypes.c_float]),
     "rip_opimc_theta_zero": (U64, [U64, ctypes.c_float, U64, ctypes.c_float]),
     "rip_opimc_lower_bound": (ctypes.c_float, [U64, ctypes.c_float, U64, U64]),

@@ -107,6 +107,27 @@ count_kernel(DevPool P, uint64_t S, uint32_t *count) {
   }
 }
 
+// Sets of [0, S) holding at least one marked vertex (OPIM-C's FindCoverage,
+// include/ripples/opimc.h:101-118): bit (s - window) of `hit` is set when a
+// member of set s is marked; each warp adds the covered sets of its window.
+__global__ void __launch_bounds__(256)
+coverage_kernel(DevPool P, uint64_t S, const uint32_t *marked, unsigned long long *covered) {
+  const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  unsigned long long mine = 0;
+  for (uint64_t wb = gw * 32; wb < S; wb += nw * 32) {
+    uint32_t hit = 0;
+    for_each_element(
+        P, wb, S, [](uint64_t i) { return i; },
+        [&](uint64_t s, uint32_t v, bool valid) {
+          const bool m = valid && ((__ldg(marked + (v >> 5)) >> (v & 31)) & 1u);
+          hit |= __reduce_or_sync(FULL, m ? 1u << (uint32_t)(s - wb) : 0u);
+        });
+    mine += __popc(hit);
+  }
+  if (lane_id() == 0 && mine) atomicAdd(covered, mine);
+}
+
 __global__ void __launch_bounds__(256)
 inverted_kernel(DevPool P, uint64_t S, uint64_t *cursor, uint32_t *inv, uint64_t base) {
   const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
@@ -525,6 +546,12 @@ void launch_build_inverted(const DevPool &P, uint64_t num_sets,
 void launch_cover(const CoverLaunch &C, cudaStream_t stream) {
   count_launches(1);
   cover_kernel<<<C.blocks, 256, 0, stream>>>(C);
+}
+
+void launch_coverage(const DevPool &P, uint64_t S, const uint32_t *marked,
+                     unsigned long long *covered, int blocks, cudaStream_t stream) {
+  count_launches(1);
+  coverage_kernel<<<blocks, 256, 0, stream>>>(P, S, marked, covered);
 }
 
 void launch_sel_init(const SelDesc *d, int blocks, cudaStream_t stream) {

@@ -231,6 +231,9 @@ struct SelDesc {
                                    // of the current pick (1 = recount)
   uint64_t total_elems;            // elements of sets [0, S) (keep_counts)
 };
+// Sets of [0, S) holding a vertex whose bit is set in `marked` (n bits).
+void launch_coverage(const DevPool &P, uint64_t S, const uint32_t *marked,
+                     unsigned long long *covered, int blocks, cudaStream_t stream);
 void launch_sel_init(const SelDesc *d, int blocks, cudaStream_t stream);
 void launch_sel_count(const SelDesc *d, int blocks, cudaStream_t stream);
 void launch_sel_pick(const SelDesc *d, uint32_t i, int blocks, cudaStream_t stream);

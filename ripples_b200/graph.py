@@ -460,6 +460,16 @@ class Pool:
         self._chk(lib.rip_select_counts(self.h, _ptr(out)), "rip_select_counts")
         return out
 
+    def coverage(self, seeds, num_sets: Optional[int] = None) -> int:
+        """Sets among the first ``num_sets`` holding at least one of ``seeds``
+        (``rip_coverage``, OPIM-C's FindCoverage)."""
+        sd = np.ascontiguousarray(seeds, dtype=np.uint32)
+        out = ctypes.c_uint64()
+        self._chk(lib.rip_coverage(self.h, self.num_sets if num_sets is None else num_sets,
+                                   _ptr(sd) if sd.size else None, int(sd.size),
+                                   ctypes.byref(out)), "rip_coverage")
+        return out.value
+
     def imm(self, k: int, epsilon: float, l: float = 1.0, seed: int = 0,
             tiebreak: int = _lib.TIE_REF_HEAP, sampler: int = _lib.SAMPLER_AUTO):
         seeds = np.zeros(max(k, 1), dtype=np.uint32)
@@ -504,6 +514,18 @@ def _spread_result(mean, sizes, levels, replicas):
     if levels is not None:
         res.append(levels[:replicas])
     return res[0] if len(res) == 1 else tuple(res)
+
+
+def opimc(r1: Pool, r2: Pool, k: int, epsilon: float, delta: float, seed: int = 0,
+          tiebreak: int = _lib.TIE_REF_HEAP, sampler: int = _lib.SAMPLER_AUTO):
+    """OPIM-C on two pools of one graph (``rip_opimc_pool``): (seeds, record)."""
+    seeds = np.zeros(max(k, 1), dtype=np.uint32)
+    ns = ctypes.c_uint32()
+    rec = _lib.OpimcRecord()
+    check(lib.rip_opimc_pool(r1.h, r2.h, k, epsilon, delta, seed, tiebreak, sampler,
+                             _ptr(seeds), ctypes.byref(ns), ctypes.byref(rec)),
+          "rip_opimc_pool", r1.graph.ctx.h)
+    return seeds[: ns.value].copy(), rec
 
 
 def spread_lt(forward: DeviceGraph, backward: DeviceGraph, seeds, replicas: int,
