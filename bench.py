@@ -1,10 +1,14 @@
 """Benchmark: RRR sets/s of full IMM runs on one or more B200s.
 
-Default workload (N=1): plain IMM under the LT model on a directed R-MAT graph
-with 2^20 vertices and 16*2^20 edge draws (a,b,c,d = .57,.19,.19,.05, seed 0,
-self-loops and duplicates removed), in-weights U(0,1) normalised per
-destination, k=50, epsilon=0.3.  Other workloads: --workload ic14 (R-MAT 2^14,
-2^18 draws, IC p ~ U(0,0.1), k=20, eps=0.5).
+Default workload (N=1): plain IMM under the IC model on a directed R-MAT graph
+with 2^24 vertices and 32*2^24 edge draws (a,b,c,d = .57,.19,.19,.05, seed 0,
+self-loops and duplicates removed: m = 520 761 423), weighted-cascade
+probabilities p = 1/in-degree(dst), k=100, epsilon=0.13, seeds chosen with the
+reference CPU heap's tie-break.  Other workloads: --workload lt20 (R-MAT 2^20,
+16*2^20 draws, LT in-weights U(0,1) normalised per destination, k=50,
+epsilon=0.3), ic14 (R-MAT 2^14, 2^18 draws, IC p ~ U(0,0.1), k=20,
+epsilon=0.5), ic24_samplers (each IC sampler on one fixed set range of the
+2^24 graph), b1 (batching), s1 (serving), spread (forward Monte Carlo).
 
 One step = one complete IMM (martingale theta estimation + final sampling +
 final greedy selection) from an empty RRR pool, with a fresh sampler seed each
@@ -18,9 +22,16 @@ only"): each rank runs its own independent IMM query (its own seeds), and
 `value` aggregates the ranks' sets -- weak scaling, no collective on the data
 path.
 
---impl reference runs the reference's own CPU imm (built from its sources into
-oracle/_ref/ by oracle/ref.mk) on the same graph, written in the reference's
-binary format, on rank 0 only.
+--impl reference runs the reference's own CPU implementation (built from its
+sources into oracle/_ref/ by oracle/ref.mk) on rank 0 only, on the same graph
+written in the reference's binary format by the oracle's generator (the
+process never loads this package's library):
+  IC: the imm tool's `-p --rrsets N` sampling path (GenerateRRRSets over an
+      ICStreamingGenerator on every host thread), N sized so a step takes a
+      few seconds: sets/s of sampling alone, an upper bound of the reference's
+      full-IMM rate (its selection time is left out).
+  LT: the sequential imm (`-p` runs IC coin flips on its CPU workers,
+      include/ripples/batched_add_rrrset.h:231-245), full IMM runs, 1 core.
 """
 from __future__ import annotations
 
@@ -39,6 +50,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOADS = {
+    "ic24": dict(name="imm_ic_rmat24_deg32_wc_k100_eps0.13", scale=24, draws=32 << 24,
+                 model="IC", k=100, eps=0.13, weights="wc"),
     "lt20": dict(name="imm_lt_rmat20_deg16_k50_eps0.3", scale=20, draws=16 << 20, model="LT",
                  k=50, eps=0.3, weights="lt_normalized"),
     "ic14": dict(name="imm_ic_rmat14_2^18_k20_eps0.5", scale=14, draws=1 << 18, model="IC",
@@ -55,8 +68,8 @@ WORKLOADS = {
     # R-MAT 2^24, 32*2^24 draws, weighted cascade p = 1/indeg, k=100,
     # eps=0.13: full IMM with the autotuned sampler, plus each sampler
     # (one set per warp, fused 64/128/256 colours) on the same fixed set range
-    "p3": dict(name="imm_ic_rmat24_deg32_wc_k100_eps0.13", kind="p3", scale=24,
-               draws=32 << 24, model="IC", k=100, eps=0.13),
+    "ic24_samplers": dict(name="samplers_ic_rmat24_deg32_wc", kind="p3", scale=24,
+                          draws=32 << 24, model="IC", k=100, eps=0.13),
     # forward Monte Carlo spread (rip_spread_ic) of the 50 vertices of largest
     # out-degree on R-MAT 2^20 (16*2^20 draws, IC p ~ U(0,0.1)), 20000
     # replicas a step; the reference's own simulator timed beside it
@@ -67,9 +80,20 @@ WORKLOADS = {
 METRIC = "RRR sets/s (full IMM)"
 
 
+RMAT_ABC = (0.57, 0.19, 0.19)
+
+
+def workload_config(w, n, m):
+    """The `config` object of both arms' lines (identical by construction)."""
+    return {"workload": w["name"], "model": w["model"], "k": w["k"], "epsilon": w["eps"],
+            "n": n, "m": m, "weights": w["weights"],
+            "graph": "R-MAT 2^%d, %d draws, a,b,c = %s, seed 0, no self-loops or duplicates"
+                     % (w["scale"], w["draws"], ",".join(str(x) for x in RMAT_ABC))}
+
+
 def build_graph(w):
     import ripples_b200 as rb
-    g = rb.HostGraph.rmat(w["scale"], w["draws"], 0.57, 0.19, 0.19, seed=0)
+    g = rb.HostGraph.rmat(w["scale"], w["draws"], *RMAT_ABC, seed=0)
     if w["weights"] == "lt_normalized":
         return g.with_weights(rb.WEIGHTS_LT_NORMALIZED, seed=1)
     if w["weights"] == "wc":
@@ -198,48 +222,95 @@ def run_reference_imm(bin_path, w, threads, parallel, timeout_s):
     return sets, float(rec["Total"]), rec
 
 
+def oracle_graph(w):
+    """The workload's graph drawn by the oracle's generator (tests pin it equal
+    to the library's host builder), so the reference arm never loads this
+    package's library.  Returns (n, index, src, weights)."""
+    from oracle import oracle as O
+    kind, lo, hi = {"wc": ("wc", 0.0, 0.0), "lt_normalized": ("lt_normalized", 0.0, 0.0),
+                    "uniform_0_0.1": ("uniform", 0.0, 0.1)}[w["weights"]]
+    return O.rmat_graph(w["scale"], w["draws"], *RMAT_ABC, seed=0, weights=kind, weight_seed=1,
+                        lo=lo, hi=hi)
+
+
+def reference_sampling(path, steps, warmup, target_s):
+    """The reference's `imm -p -d IC --rrsets N` sampling path (tools/imm.cc:
+    224-262: GenerateRRRSets over an ICStreamingGenerator with one CPU worker
+    per host thread) through the harness built from its sources, the graph
+    loaded once.  N is a multiple of 64 sets per thread sized so one call takes
+    about target_s.  Returns (N, [ms of each timed call], threads)."""
+    import ctypes
+    from oracle import oracle as O
+    R = O.reference()
+    threads = os.cpu_count() or 1
+    g = R.ref_graph_load(path.encode())
+    try:
+        unit = 64 * threads
+        ne = ctypes.c_uint64()
+        ms = R.ref_generate_parallel(g, unit, 0, ctypes.byref(ne))  # sizing call
+        N = max(unit, int(target_s * 1e3 / max(ms, 1e-3)) * unit)
+        for i in range(warmup):
+            R.ref_generate_parallel(g, N, 1 + i, ctypes.byref(ne))
+        times = [R.ref_generate_parallel(g, N, 1000 + i, ctypes.byref(ne)) for i in range(steps)]
+    finally:
+        R.ref_graph_free(g)
+    return N, times, threads
+
+
 def reference_arm(args, w, world, rank):
     if rank != 0:
         return 0
+    from oracle import oracle as O
     exe = os.path.join(ROOT, "oracle", "_ref", "imm")
-    if not os.path.exists(exe):
+    if not os.path.exists(exe) or O.reference() is None:
         print(json.dumps({"impl": "reference", "unavailable":
-                          "oracle/_ref/imm not built (make -f oracle/ref.mk needs the "
+                          "oracle/_ref not built (make -f oracle/ref.mk needs the "
                           "reference sources)"}))
         return 0
-    g = build_graph(w)
+    n, index, src, wts = oracle_graph(w)
+    m = len(src)
     tmp = tempfile.mkdtemp()
     path = os.path.join(tmp, "graph.bin")
-    g.write_binary(path, backward=True)
-    cores = os.cpu_count() or 1
-    # The reference's LT sampler is only correct on its sequential path: the
-    # parallel CPU workers run IC coin flips whatever the model
-    # (include/ripples/batched_add_rrrset.h:231-245).  IC runs use all cores.
-    parallel = w["model"] == "IC"
-    threads = cores if parallel else 1
-    for _ in range(args.warmup):
-        run_reference_imm(path, w, threads, parallel, 600)
-    tot_sets, tot_ms = 0, 0.0
-    for _ in range(args.steps):
-        s, ms, rec = run_reference_imm(path, w, threads, parallel, 600)
-        tot_sets += s
-        tot_ms += ms
+    O.write_binary(path, n, index, src, wts)
+    del index, src, wts
+    config = workload_config(w, n, m)
+    if w["model"] == "IC":
+        # a step: one bounded GenerateRRRSets call, the whole run a few minutes
+        per_step = min(5.0, max(1.0, 150.0 / max(1, args.steps + args.warmup)))
+        N, times, threads = reference_sampling(path, args.steps, args.warmup, per_step)
+        tot_sets, tot_ms = N * len(times), sum(times)
+        path_note = ("imm -p --rrsets %d (GenerateRRRSets, ICStreamingGenerator, %d CPU "
+                     "workers): sampling only, theta-capped" % (N, threads))
+        sample = (f"{args.steps} calls of the reference's parallel GenerateRRRSets, {N} sets "
+                  f"each, on all {threads} host threads (graph loaded once)")
+    else:
+        # The reference's LT sampler is only correct on its sequential path:
+        # the parallel CPU workers run IC coin flips whatever the model
+        # (include/ripples/batched_add_rrrset.h:231-245).
+        threads = 1
+        for _ in range(args.warmup):
+            run_reference_imm(path, w, threads, False, 600)
+        tot_sets, tot_ms = 0, 0.0
+        for _ in range(args.steps):
+            s_, ms, rec = run_reference_imm(path, w, threads, False, 600)
+            tot_sets += s_
+            tot_ms += ms
+        path_note = "imm (sequential), full IMM runs"
+        sample = f"{args.steps} full IMM runs of the workload, sequential imm"
+    shutil.rmtree(tmp, ignore_errors=True)
     value = tot_sets / (tot_ms / 1e3)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "sets/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
+            "ms_per_step": tot_ms / max(args.steps, 1), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32",
-            "data": "synthetic R-MAT (seed 0), written in the reference binary format",
-            "config": {"workload": w["name"], "model": w["model"], "k": w["k"],
-                       "epsilon": w["eps"], "n": g.n, "m": g.m,
-                       "reference_path": "imm -p" if parallel else "imm (sequential)"},
+            "data": "synthetic R-MAT (seed 0) from the oracle's generator, written in the "
+                    "reference binary format",
+            "config": config, "reference_path": path_note,
             "cpu_baseline": {"value": value, "unit": "sets/s", "cores": threads,
-                             "kind": "reference",
-                             "sample": f"{args.steps} full IMM runs of the workload"},
+                             "kind": "reference", "sample": sample},
             "e2e": {"value": value, "unit": "sets/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
-    shutil.rmtree(tmp, ignore_errors=True)
     return 0
 
 
@@ -257,8 +328,8 @@ def reference_arm_other(args, w, world, rank):
     if kind != "spread":
         why = {"batch": "the reference runs one IMM instance per process (no batching path)",
                "serve": "the reference has no request loop (no serving path)",
-               "p3": "one reference IMM on the 2^24-vertex, 521 M-edge graph takes hours "
-                     "on host cores"}[kind]
+               "p3": "this workload compares the library's samplers with one another; the "
+                     "reference arm of the 2^24 graph is --workload ic24"}[kind]
         print(json.dumps({"impl": "reference", "unavailable": why}))
         return 0
     sys.path.insert(0, ROOT)
@@ -315,26 +386,34 @@ def reference_arm_other(args, w, world, rank):
     return 0
 
 
-def cpu_baseline(w, g, budget_s=30.0):
-    """The reference's own CPU imm on this box's host cores (one IMM run)."""
+def cpu_baseline(w, g, budget_s=10.0):
+    """The reference's own CPU path on this box's host cores, a bounded sample:
+    IC -- its parallel sampler (the imm tool's -p --rrsets path) on every host
+    thread, about budget_s of work; LT -- one full sequential imm run."""
+    from oracle import oracle as O
     exe = os.path.join(ROOT, "oracle", "_ref", "imm")
-    if not os.path.exists(exe):
+    if not os.path.exists(exe) or O.reference() is None:
         return None
     tmp = tempfile.mkdtemp()
     path = os.path.join(tmp, "graph.bin")
     g.write_binary(path, backward=True)
-    parallel = w["model"] == "IC"
-    threads = (os.cpu_count() or 1) if parallel else 1
     try:
-        s, ms, rec = run_reference_imm(path, w, threads, parallel, max(60, budget_s * 4))
+        if w["model"] == "IC":
+            N, times, threads = reference_sampling(path, 1, 0, budget_s)
+            return {"value": N / (times[0] / 1e3), "unit": "sets/s", "cores": threads,
+                    "kind": "reference",
+                    "sample": f"{N} sets ({times[0]:.0f} ms) of the reference's parallel "
+                              f"GenerateRRRSets (imm -p --rrsets path) on {threads} threads: "
+                              f"sampling only"}
+        s_, ms, rec = run_reference_imm(path, w, 1, False, max(60, budget_s * 12))
+        return {"value": s_ / (ms / 1e3), "unit": "sets/s", "cores": 1, "kind": "reference",
+                "sample": f"one full IMM run ({s_} sets, {ms:.0f} ms) with the reference's "
+                          f"sequential imm built from its sources"}
     except (subprocess.TimeoutExpired, subprocess.CalledProcessError) as e:
-        return {"value": None, "unit": "sets/s", "cores": threads, "kind": "reference",
+        return {"value": None, "unit": "sets/s", "cores": None, "kind": "reference",
                 "sample": f"failed: {type(e).__name__}"}
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
-    return {"value": s / (ms / 1e3), "unit": "sets/s", "cores": threads, "kind": "reference",
-            "sample": f"one full IMM run ({s} sets, {ms:.0f} ms) with the reference's "
-                      f"{'parallel' if parallel else 'sequential'} imm built from its sources"}
 
 
 def main():
@@ -343,7 +422,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="lt20", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="ic24", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--serve-scales", default="18,20,22,24",
                     help="s1: R-MAT scales of the resident graphs")
@@ -448,9 +527,10 @@ def main():
     # stays on the device, one read-back per selection
     torch.cuda.synchronize()
     ev2, ev3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    low_steps = max(1, min(args.steps, 5))
     ev2.record(stream)
     low_sets = 0
-    for step in range(args.steps):
+    for step in range(low_steps):
         pool.clear()
         _, rec = pool.imm(w["k"], w["eps"], 1.0, seed=seed_base + step,
                           tiebreak=rb.TIE_LOWEST_ID)
@@ -459,6 +539,7 @@ def main():
     torch.cuda.synchronize()
     low_ms = allreduce_max(ev2.elapsed_time(ev3), world)
     low_value = allreduce_sum(low_sets, world) / (low_ms / 1e3)
+    low_ms_per_step = low_ms / low_steps
 
     # ---- e2e through the public API: host graph -> device -> seeds ---------
     pin_idx = torch.from_numpy(g.index).pin_memory()
@@ -487,7 +568,7 @@ def main():
         e2e_step_ms.append(round(1e3 * (t2 - t0), 2))
         return n_sets, seeds
 
-    e2e_steps = max(1, min(args.steps, 10))
+    e2e_steps = max(1, min(args.steps, 5 if g.m > (1 << 28) else 10))
     e2e_step(-1)
     e2e_split.update(upload_ms=0.0, imm_ms=0.0)
     e2e_step_ms.clear()
@@ -533,11 +614,10 @@ def main():
             "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32",
             "data": "synthetic R-MAT graph (seed 0) and weights (seed 1); fresh sampler seed per step",
-            "config": {"workload": w["name"], "model": w["model"], "k": w["k"],
-                       "epsilon": w["eps"], "n": g.n, "m": g.m,
-                       "theta": thetas[0] if thetas else None,
-                       "parallelism": f"replicas x{world}",
-                       "l2": "graph (%d MB) and pool exceed L2 (126 MB)" % ((g.m * 8 + g.n * 4) >> 20)},
+            "config": workload_config(w, g.n, g.m),
+            "theta": thetas[0] if thetas else None,
+            "parallelism": f"replicas x{world}",
+            "l2": "graph (%d MB) and pool exceed L2 (126 MB)" % ((g.m * 8 + g.n * 4) >> 20),
             "e2e": {"value": e2e_value, "unit": "sets/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": e2e_steps,
                     "split_ms_per_step": {kk: vv / e2e_steps for kk, vv in e2e_split.items()},
@@ -563,7 +643,7 @@ def main():
             "autotune": tune,
             "tiebreak": "reference CPU heap (CompareHeap lazy max-heap)",
             "lowest_id_tiebreak": {"value": low_value, "unit": "sets/s",
-                                   "ms_per_step": low_ms / args.steps,
+                                   "ms_per_step": low_ms_per_step, "steps": low_steps,
                                    "note": "same IMM runs, reference GPU tie-break "
                                            "(lowest id), picks on the device"},
         }

@@ -3,8 +3,10 @@
 // CPU restatement of the pnnl/ripples IMM hot path, used exclusively as the
 // checker by tests/, __graft_entry__.smoke() and the cpu_baseline leg of
 // bench.py.  Nothing in the product (ripples_b200/) links, loads or calls this
-// file.  It is single-threaded scalar C++ on purpose: simple enough to read
-// against the reference line by line.
+// file.  The algorithms are scalar C++ on purpose: simple enough to read
+// against the reference line by line.  Only loops over independent items
+// (sets listed by id, edge draws, per-vertex weights) run on several host
+// threads, which leaves every result unchanged.
 //
 // What it restates (reference paths are relative to the ripples project):
 //   * Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as
@@ -57,9 +59,15 @@
 #include <vector>
 #include <sys/types.h>
 
+#include <omp.h>
+#include <parallel/algorithm>
+
 namespace {
 
-enum : uint32_t { DOM_ROOT = 1, DOM_IC = 2, DOM_LT = 3, DOM_SIM_IC = 7, DOM_SIM_LT = 8 };
+enum : uint32_t {
+  DOM_ROOT = 1, DOM_IC = 2, DOM_LT = 3, DOM_RMAT = 4, DOM_ER = 5, DOM_WEIGHT = 6,
+  DOM_SIM_IC = 7, DOM_SIM_LT = 8
+};
 
 void philox4x32_10(const uint32_t ctr_in[4], const uint32_t key_in[2],
                    uint32_t out[4]) {
@@ -259,6 +267,56 @@ void sample_lt_one(const Graph &G, uint64_t seed, uint64_t s,
     out.push_back(u);
     cur = u;
   }
+  std::sort(out.begin(), out.end());
+}
+
+
+// One set (IC or LT) with a visited bitmap the caller owns: the bits of the
+// set's members are cleared again before returning, so one bitmap serves any
+// number of sets.  Same semantics as sample_ic_one / sample_lt_one.
+void sample_one_bits(const Graph &G, int model, uint64_t seed, uint64_t s,
+                     std::vector<uint64_t> &bits, std::vector<uint32_t> &out) {
+  auto test_set = [&](uint32_t v) {
+    uint64_t &w = bits[v >> 6];
+    const uint64_t b = 1ull << (v & 63);
+    const bool was = (w & b) != 0;
+    w |= b;
+    return was;
+  };
+  out.clear();
+  uint32_t r = root_of(seed, s, G.n);
+  out.push_back(r);
+  test_set(r);
+  if (model == 0) {
+    for (size_t head = 0; head < out.size(); ++head) {
+      const uint32_t v = out[head];
+      for (uint64_t e = G.index[v]; e < G.index[v + 1]; ++e) {
+        const uint32_t u = G.src[e];
+        if (bits[u >> 6] & (1ull << (u & 63))) continue;
+        if (ic_coin(seed, s, e) < G.thr[e]) {
+          test_set(u);
+          out.push_back(u);
+        }
+      }
+    }
+  } else {
+    uint32_t cur = r;
+    for (;;) {
+      const uint32_t t = lt_threshold(seed, s, cur);
+      uint64_t sel = UINT64_MAX;
+      for (uint64_t e = G.index[cur]; e < G.index[cur + 1]; ++e)
+        if (t < G.thr[e]) {
+          sel = e;
+          break;
+        }
+      if (sel == UINT64_MAX) break;
+      const uint32_t u = G.src[sel];
+      if (test_set(u)) break;
+      out.push_back(u);
+      cur = u;
+    }
+  }
+  for (uint32_t v : out) bits[v >> 6] &= ~(1ull << (v & 63));
   std::sort(out.begin(), out.end());
 }
 
@@ -712,5 +770,115 @@ int orc_imm(int model, uint32_t n, const uint64_t *index, const uint32_t *src,
   *total_sets = pool.off.size() - 1;
   return 0;
 }
+
+// Samples the sets whose ids are listed: pool set i is set ids[i].  Sets are
+// pure functions of (seed, id), so they are drawn in parallel over the host
+// threads (one n-bit visited bitmap per thread).
+void *orc_sample_ids(int model, uint32_t n, const uint64_t *index, const uint32_t *src,
+                     const uint32_t *thr, uint64_t seed, const uint64_t *ids,
+                     uint64_t count) {
+  Graph G{n, index, src, thr};
+  std::vector<std::vector<uint32_t>> sets(count);
+#pragma omp parallel
+  {
+    std::vector<uint64_t> bits(((size_t)n + 63) / 64, 0);
+#pragma omp for schedule(dynamic, 1)
+    for (uint64_t i = 0; i < count; ++i) sample_one_bits(G, model, seed, ids[i], bits, sets[i]);
+  }
+  Pool *p = new Pool();
+  for (auto &one : sets) {
+    p->vtx.insert(p->vtx.end(), one.begin(), one.end());
+    p->off.push_back(p->vtx.size());
+  }
+  return p;
+}
+
+// ---- synthetic input graphs ------------------------------------------------
+// The R-MAT (Chakrabarti, Zhan, Faloutsos, SDM'04) and Erdos-Renyi draws and
+// weight models the library's host graph builders use, restated so that the
+// reference's input files can be written without loading the library:
+//   R-MAT draw i, level l: quadrant from P(i_lo, i_hi, l/4, RMAT<<24)[l%4]
+//     against the cumulative thresholds of a, a+b, a+b+c (u32 fixed point);
+//     bit l of (src, dst) from most significant down; self-loops dropped.
+//   keys (dst<<32 | src) sorted and de-duplicated = the backward CSR.
+//   weights of CSR edge e from P(e_lo, e_hi, 0, WEIGHT<<24)[0] >> 8 / 2^24.
+int orc_rmat_csr(uint32_t scale, uint64_t draws, double a, double b, double c,
+                 uint64_t seed, uint64_t **index_out, uint32_t **src_out, uint64_t *m_out) {
+  if (scale == 0 || scale > 31) return -1;
+  const uint32_t n = 1u << scale;
+  const uint32_t TA = prob_to_u32(a), TB = prob_to_u32(a + b), TC = prob_to_u32(a + b + c);
+  uint32_t key[2];
+  make_key(seed, key);
+  std::vector<uint64_t> keys(draws, ~0ull);
+#pragma omp parallel for schedule(static)
+  for (uint64_t i = 0; i < draws; ++i) {
+    uint32_t s = 0, d = 0, rnd[4] = {0, 0, 0, 0};
+    for (uint32_t l = 0; l < scale; ++l) {
+      if ((l & 3) == 0) {
+        const uint32_t ctr[4] = {(uint32_t)i, (uint32_t)(i >> 32), l >> 2, DOM_RMAT << 24};
+        philox4x32_10(ctr, key, rnd);
+      }
+      const uint32_t u = rnd[l & 3];
+      const uint32_t row = u >= TB;                          // quadrants c, d
+      const uint32_t col = (u >= TA && u < TB) || u >= TC;   // quadrants b, d
+      s |= row << (scale - 1 - l);
+      d |= col << (scale - 1 - l);
+    }
+    if (s != d) keys[i] = ((uint64_t)d << 32) | s;
+  }
+  __gnu_parallel::sort(keys.begin(), keys.end());
+  keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
+  if (!keys.empty() && keys.back() == ~0ull) keys.pop_back();  // the dropped self-loops
+  const uint64_t m = keys.size();
+  uint64_t *index = (uint64_t *)std::calloc((size_t)n + 1, sizeof(uint64_t));
+  uint32_t *src = (uint32_t *)std::malloc(sizeof(uint32_t) * (m ? m : 1));
+  if (!index || !src) {
+    std::free(index);
+    std::free(src);
+    return -1;
+  }
+#pragma omp parallel for schedule(static)
+  for (uint64_t e = 0; e < m; ++e) src[e] = (uint32_t)keys[e];
+  for (uint64_t e = 0; e < m; ++e) index[(keys[e] >> 32) + 1]++;
+  for (uint32_t v = 0; v < n; ++v) index[v + 1] += index[v];
+  *index_out = index;
+  *src_out = src;
+  *m_out = m;
+  return 0;
+}
+
+// kind 0: U(lo, hi) per edge; 1: U(0,1) normalised per destination (sum in
+// double over the float draws, CSR order); 2: weighted cascade 1/in-degree.
+int orc_make_weights(int kind, uint32_t n, const uint64_t *index, uint64_t seed, double lo,
+                     double hi, float *w) {
+  uint32_t key[2];
+  make_key(seed, key);
+  auto unif = [&](uint64_t e) {
+    uint32_t rnd[4];
+    const uint32_t ctr[4] = {(uint32_t)e, (uint32_t)(e >> 32), 0, DOM_WEIGHT << 24};
+    philox4x32_10(ctr, key, rnd);
+    return (double)(rnd[0] >> 8) / 16777216.0;
+  };
+  if (kind < 0 || kind > 2) return -1;
+#pragma omp parallel for schedule(dynamic, 4096)
+  for (uint64_t v = 0; v < n; ++v) {
+    const uint64_t b = index[v], e1 = index[v + 1];
+    if (kind == 0) {
+      for (uint64_t e = b; e < e1; ++e) w[e] = (float)(lo + (hi - lo) * unif(e));
+    } else if (kind == 1) {
+      double sum = 0.0;
+      for (uint64_t e = b; e < e1; ++e) {
+        w[e] = (float)unif(e);
+        sum += (double)w[e];
+      }
+      for (uint64_t e = b; e < e1; ++e) w[e] = sum > 0.0 ? (float)((double)w[e] / sum) : 0.0f;
+    } else {
+      for (uint64_t e = b; e < e1; ++e) w[e] = (float)(1.0 / (double)(e1 - b));
+    }
+  }
+  return 0;
+}
+
+void orc_free(void *p) { std::free(p); }
 
 }  // extern "C"

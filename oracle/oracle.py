@@ -43,6 +43,11 @@ def _load_oracle() -> ctypes.CDLL:
         "orc_pack_ic": (None, [P, U64, P]),
         "orc_pack_lt": (None, [P, U32, P, P]),
         "orc_sample": (P, [I32, U32, P, P, P, U64, U64, U64, P]),
+        "orc_sample_ids": (P, [I32, U32, P, P, P, U64, P, U64]),
+        "orc_rmat_csr": (I32, [U32, U64, DBL, DBL, DBL, U64, ctypes.POINTER(P), ctypes.POINTER(P),
+                               ctypes.POINTER(U64)]),
+        "orc_make_weights": (I32, [I32, U32, P, U64, DBL, DBL, P]),
+        "orc_free": (None, [P]),
         "orc_spread_ic": (U64, [U32, P, P, P, P, U32, U64, U64, P, ctypes.POINTER(U64), P]),
         "orc_spread_lt": (U64, [U32, P, P, P, P, P, P, U32, U64, U64, P, P]),
         "orc_find_coverage": (U64, [U64, P, P, P, U32]),
@@ -115,6 +120,64 @@ def sample(model: str, n: int, index: np.ndarray, src: np.ndarray, thr: np.ndarr
     L.orc_pool_copy(h, _ptr(off), _ptr(vtx))
     L.orc_pool_free(h)
     return off, vtx[:ne], st
+
+
+def sample_ids(model: str, n: int, index: np.ndarray, src: np.ndarray, thr: np.ndarray,
+               seed: int, ids) -> Tuple[np.ndarray, np.ndarray]:
+    """The sets with the listed ids as CSR (offsets, vertices), each sorted;
+    drawn in parallel over the host threads."""
+    idx = np.ascontiguousarray(index, dtype=np.uint64)
+    s = np.ascontiguousarray(src, dtype=np.uint32)
+    t = np.ascontiguousarray(thr, dtype=np.uint32)
+    if s.size == 0:
+        s = np.zeros(1, np.uint32)
+        t = np.zeros(1, np.uint32)
+    ids = np.ascontiguousarray(ids, dtype=np.uint64)
+    h = L.orc_sample_ids(0 if model == "IC" else 1, n, _ptr(idx), _ptr(s), _ptr(t), seed,
+                         _ptr(ids), len(ids))
+    ns, ne = L.orc_pool_sets(h), L.orc_pool_elements(h)
+    off = np.zeros(ns + 1, dtype=np.uint64)
+    vtx = np.zeros(max(ne, 1), dtype=np.uint32)
+    L.orc_pool_copy(h, _ptr(off), _ptr(vtx))
+    L.orc_pool_free(h)
+    return off, vtx[:ne]
+
+
+WEIGHT_KINDS = {"uniform": 0, "lt_normalized": 1, "wc": 2}
+
+
+def rmat_graph(scale: int, draws: int, a: float = 0.57, b: float = 0.19, c: float = 0.19,
+               seed: int = 0, weights: str = "uniform", weight_seed: int = 1,
+               lo: float = 0.0, hi: float = 0.1):
+    """An R-MAT graph drawn as the library's host builder draws it, as the
+    backward CSR (n, index u64[n+1], src u32[m], weights f32[m])."""
+    pi, ps, m = P(), P(), U64()
+    if L.orc_rmat_csr(scale, draws, a, b, c, seed, ctypes.byref(pi), ctypes.byref(ps),
+                      ctypes.byref(m)) != 0:
+        raise MemoryError("orc_rmat_csr failed")
+    n, mm = 1 << scale, m.value
+    try:
+        index = np.ctypeslib.as_array(ctypes.cast(pi, ctypes.POINTER(U64)), (n + 1,)).copy()
+        src = np.ctypeslib.as_array(ctypes.cast(ps, ctypes.POINTER(U32)), (max(mm, 1),))[:mm].copy()
+    finally:
+        L.orc_free(pi)
+        L.orc_free(ps)
+    w = np.zeros(max(mm, 1), dtype=np.float32)
+    if L.orc_make_weights(WEIGHT_KINDS[weights], n, _ptr(index), weight_seed, lo, hi, _ptr(w)):
+        raise ValueError("orc_make_weights failed")
+    return n, index, src, w[:mm]
+
+
+def write_binary(path: str, n: int, index, src, w) -> None:
+    """The reference's binary graph format (include/ripples/graph.h:700-771),
+    backward direction, float weights, identity id map."""
+    m = len(src)
+    with open(path, "wb") as fh:
+        np.asarray([0xc0ffee, 0xa1ccac0f, 32, n, m], dtype=np.uint64).tofile(fh)
+        np.arange(n, dtype=np.uint32).tofile(fh)
+        np.ascontiguousarray(index, dtype=np.uint64).tofile(fh)
+        np.ascontiguousarray(src, dtype=np.uint32).tofile(fh)
+        np.ascontiguousarray(w, dtype=np.float32).tofile(fh)
 
 
 def spread_ic(n: int, index: np.ndarray, dst: np.ndarray, thr: np.ndarray, seeds,
@@ -301,6 +364,8 @@ def reference() -> Optional[ctypes.CDLL]:
             "ref_opimc_upper_bound": (ctypes.c_float, [U64, ctypes.c_float, U64, U64]),
             "ref_find_coverage": (U64, [U64, P, P, P, U32]),
             "ref_graph_copy": (None, [P, P, P, P, P]),
+            "ref_generate_parallel": (DBL, [P, U64, U64, ctypes.POINTER(U64)]),
+            "ref_imm_sequential": (U32, [P, I32, U32, DBL, U64, P]),
         }
         for k, (r, a) in sig.items():
             f = getattr(R, k)

@@ -17,6 +17,12 @@
 //   ref_simulate_parallel -> the replica loop of tools/simulator.cc:139-149
 //   ref_opimc_*, ref_find_coverage
 //                   -> include/ripples/opimc.h:60-118
+//   ref_generate_parallel -> the imm tool's `-p --rrsets N` path
+//                      (tools/imm.cc:224-262): an ICStreamingGenerator over
+//                      every OpenMP thread and one GenerateRRRSets call,
+//                      omp_parallel_tag (generate_rrr_sets.h:214-224)
+//   ref_imm_sequential -> the imm tool's sequential path (tools/imm.cc:313-323,
+//                      ripples::IMM with sequential_tag) with a chosen seed
 //   ref_graph_load_tsv / ref_graph_copy
 //                   -> the sequential TSV loader (include/ripples/loaders.h:138-196)
 //                      and the GraphBwd constructor (include/ripples/graph.h:506-620)
@@ -29,7 +35,9 @@
 #include "ripples/generate_rrr_sets.h"
 #include "ripples/graph.h"
 #include "ripples/imm.h"
+#include "ripples/imm_configuration.h"
 #include "ripples/imm_interface.h"
+#include "ripples/streaming_rrr_generator.h"
 #include "ripples/diffusion_simulation.h"
 #include "ripples/loaders.h"
 #include "ripples/opimc.h"
@@ -301,6 +309,61 @@ double ref_simulate_levels(const char *fwd_path, int model, const uint32_t *seed
     acc += (double)res.second;
   }
   return acc / (double)replicas;
+}
+
+// The imm tool's `-p --rrsets N` sampling (tools/imm.cc:224-262 with
+// CFG.num_rr_sets = count): master lcg64 seeded `seed` and split(2, 1), an
+// ICStreamingGenerator with one CPU worker per OpenMP thread, no GPU workers,
+// the default 64-colour CPU batches, then GenerateRRRSets over `count`
+// pre-inserted empty sets.  Returns the milliseconds of that call alone (the
+// tool's ThetaEstimationGenerateRRR entry) and the element count.
+double ref_generate_parallel(void *g, uint64_t count, uint64_t seed, uint64_t *nelem) {
+  ensure_console();
+  auto &G = *(ripples::GraphBwd *)g;
+  trng::lcg64 generator;
+  generator.seed(seed);
+  generator.split(2, 1);
+  const size_t workers = omp_get_max_threads();
+  std::unordered_map<size_t, size_t> worker_to_gpu;
+  ripples::ICStreamingGenerator se(G, generator, workers, 0, 0, 64, 64, worker_to_gpu, 1.0f);
+  ripples::IMMExecutionRecord R;
+  ripples::RRRsetAllocator<uint32_t> allocator;
+  std::vector<ripples::RRRset<ripples::GraphBwd>> RR;
+  const auto t0 = std::chrono::high_resolution_clock::now();
+  RR.insert(RR.end(), count, ripples::RRRset<ripples::GraphBwd>(allocator));
+  ripples::GenerateRRRSets(G, se, RR.end() - count, RR.end(), R,
+                           ripples::independent_cascade_tag{}, ripples::omp_parallel_tag{});
+  const auto t1 = std::chrono::high_resolution_clock::now();
+  uint64_t tot = 0;
+  for (auto &s : RR) tot += s.size();
+  *nelem = tot;
+  return std::chrono::duration<double, std::milli>(t1 - t0).count();
+}
+
+// The imm tool's sequential IMM (tools/imm.cc:313-323) with the master
+// lcg64 seeded `seed` instead of 0.  model 0 = IC, 1 = LT.  Writes the seeds
+// (input ids) and returns their number.
+uint32_t ref_imm_sequential(void *g, int model, uint32_t k, double epsilon, uint64_t seed,
+                            uint32_t *seeds_out) {
+  ensure_console();
+  auto &G = *(ripples::GraphBwd *)g;
+  ripples::IMMConfiguration CFG;
+  CFG.k = k;
+  CFG.epsilon = epsilon;
+  trng::lcg64 generator;
+  generator.seed(seed);
+  generator.split(2, 1);
+  ripples::IMMExecutionRecord R;
+  std::vector<uint32_t> seeds;
+  if (model == 0)
+    seeds = ripples::IMM(G, CFG, 1.0, generator, R, ripples::independent_cascade_tag{},
+                         ripples::sequential_tag{});
+  else
+    seeds = ripples::IMM(G, CFG, 1.0, generator, R, ripples::linear_threshold_tag{},
+                         ripples::sequential_tag{});
+  G.convertID(seeds.begin(), seeds.end(), seeds.begin());
+  for (size_t i = 0; i < seeds.size(); ++i) seeds_out[i] = seeds[i];
+  return (uint32_t)seeds.size();
 }
 
 }  // extern "C"

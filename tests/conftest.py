@@ -39,6 +39,43 @@ def golden_kat():
 
 
 @pytest.fixture(scope="session")
+def golden_wc16():
+    """The reference sequential sampler's counts on R-MAT 2^16, weighted
+    cascade (tests/golden/make_golden.py, WC16), with the graph rebuilt from
+    its parameters by the oracle's generator."""
+    from oracle import oracle as O
+    z = dict(np.load(os.path.join(GOLDEN, "sampler_reference_wc16.npz")))
+    scale, draws, seed = (int(x) for x in z["params"])
+    n, idx, src, w = O.rmat_graph(scale, draws, seed=seed, weights="wc")
+    return dict(z, n=n, index=idx, src=src, w=w, scale=scale, draws=draws, seed=seed)
+
+
+def chi2_homogeneity(a, b, min_expected=20):
+    """Chi-square test that two count vectors come from one distribution;
+    cells with fewer than 2 * min_expected joint counts are pooled."""
+    from scipy import stats
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    keep = (a + b) >= 2 * min_expected
+    table = np.vstack([np.append(a[keep], a[~keep].sum()), np.append(b[keep], b[~keep].sum())])
+    table = table[:, table.sum(axis=0) > 0]
+    chi2, p, dof, _ = stats.chi2_contingency(table)
+    return chi2, p, dof
+
+
+def assert_same_distribution(freq, sizes, ref_freq, ref_size_hist):
+    """North-star check 3: per-vertex occurrence frequencies within a
+    chi-square bound (p > 1e-4) and mean RRR size within 1% of the reference
+    sampler's."""
+    chi2, p, dof = chi2_homogeneity(freq, ref_freq)
+    assert p > 1e-4, (chi2, dof, p)
+    hist = np.asarray(ref_size_hist, np.float64)
+    ref_mean = (hist * np.arange(len(hist))).sum() / hist.sum()
+    mean = float(np.mean(sizes))
+    assert abs(mean - ref_mean) / ref_mean < 0.01, (mean, ref_mean)
+
+
+@pytest.fixture(scope="session")
 def golden_sampler():
     return dict(np.load(os.path.join(GOLDEN, "sampler_reference.npz")))
 

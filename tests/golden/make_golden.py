@@ -158,6 +158,29 @@ def sampler_reference():
     np.savez_compressed(os.path.join(OUT, "sampler_reference.npz"), **out)
 
 
+# Weighted cascade on R-MAT 2^16 (32 draws per vertex), the 2^24 IC
+# workload's weight model at a size where 2 M reference sets make the 1% mean
+# size bound a 3-sigma test.  The graph is rebuilt from these parameters by the
+# tests (oracle.rmat_graph), so the fixture holds only the reference's counts.
+WC16 = dict(scale=16, draws=32 << 16, seed=0, nsets=2_000_000, sampler_seed=0)
+
+
+def sampler_reference_wc16():
+    n, idx, src, w = O.rmat_graph(WC16["scale"], WC16["draws"], seed=WC16["seed"],
+                                  weights="wc")
+    tmp = tempfile.mkdtemp()
+    path = os.path.join(tmp, "wc16.bin")
+    O.write_binary(path, n, idx, src, w)
+    off, vtx = O.ref_sample(path, "IC", WC16["nsets"], seed=WC16["sampler_seed"])
+    sizes = np.diff(off).astype(np.int64)
+    np.savez_compressed(os.path.join(OUT, "sampler_reference_wc16.npz"),
+                        freq=np.bincount(vtx, minlength=n).astype(np.uint64),
+                        size_hist=np.bincount(sizes).astype(np.uint64),
+                        nsets=np.array([WC16["nsets"]], np.uint64),
+                        params=np.array([WC16["scale"], WC16["draws"], WC16["seed"]],
+                                        np.uint64))
+
+
 SPREAD_CASES = [
     # name, model, graph builder arguments, seed choice, replicas
     dict(name="karate_ic", model="IC", graph="karate", seeds="top2", replicas=100000),
@@ -254,6 +277,7 @@ if __name__ == "__main__":
     theta_values()
     kat_counting()
     sampler_reference()
+    sampler_reference_wc16()
     spread_reference()
     opimc_values()
     print("golden fixtures written to", OUT)
