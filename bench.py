@@ -541,6 +541,28 @@ def main():
     low_value = allreduce_sum(low_sets, world) / (low_ms / 1e3)
     low_ms_per_step = low_ms / low_steps
 
+    # ---- the IC samplers with and without per-vertex uniform thresholds ----
+    # (the same sets either way; untimed by the headline)
+    uniform_cmp = None
+    if w["model"] == "IC" and dg.uniform_thresholds():
+        uniform_cmp = {}
+        for label, on in (("on", True), ("off", False)):
+            dg.uniform_thresholds(on)
+            p2 = rb.Pool(dg)
+            p2.sample(1 << 14, seed=77)
+            p2.clear()
+            torch.cuda.synchronize()
+            t_u = time.perf_counter()
+            p2.sample(1 << 18, seed=77)
+            torch.cuda.synchronize()
+            t_u = time.perf_counter() - t_u
+            km_u, _, _ = p2.timing()
+            st_u = p2.stats()
+            uniform_cmp[label] = {"sets_per_s": (1 << 18) / t_u, "kernel_ms": km_u,
+                                  "alg_gb_per_s": alg_bytes_of(st_u, on) / (km_u / 1e3) / 1e9}
+            p2.close()
+        dg.uniform_thresholds(True)
+
     # ---- e2e through the public API: host graph -> device -> seeds ---------
     pin_idx = torch.from_numpy(g.index).pin_memory()
     pin_src = torch.from_numpy(g.src).pin_memory()
@@ -587,7 +609,8 @@ def main():
     # Algorithmic bytes: 8 B per vertex expansion (two u32 CSR offsets), 8 B
     # per in-edge record read (u32 source + u32 threshold), 4 B per pool
     # element written, 8 + 4 B per set (pool offset + length).
-    alg_bytes = alg_bytes_of(st_tot)
+    vthr = bool(dg.uniform_thresholds()) if w["model"] == "IC" else False
+    alg_bytes = alg_bytes_of(st_tot, vthr)
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (kern_ms / 1e3) / 1e9 if kern_ms > 0 else None
     kernel = ("lt_walk_kernel" if w["model"] == "LT" else
@@ -641,6 +664,8 @@ def main():
             "select_profile_per_step": {kk: vv / args.steps for kk, vv in sel_prof.items()},
             "sets_per_step": total_sets / args.steps,
             "autotune": tune,
+            "uniform_thresholds_2^18_sets": uniform_cmp,
+            "branching": dg.branching if w["model"] == "IC" else None,
             "tiebreak": "reference CPU heap (CompareHeap lazy max-heap)",
             "lowest_id_tiebreak": {"value": low_value, "unit": "sets/s",
                                    "ms_per_step": low_ms_per_step, "steps": low_steps,
@@ -657,11 +682,15 @@ def main():
     return 0
 
 
-def alg_bytes_of(st):
+def alg_bytes_of(st, vthr=False):
     """Algorithmic bytes of the sampler work in a pool's counters: 8 B per
     vertex expansion (two CSR offsets), 8 B per in-edge record read (source +
-    threshold), 4 B per stored element, 12 B per stored set (offset + length)."""
-    return 8 * int(st[0]) + 8 * int(st[1]) + 4 * int(st[3]) + 12 * int(st[2])
+    threshold), 4 B per stored element, 12 B per stored set (offset + length).
+    With per-vertex uniform thresholds (vthr) an expansion also reads its
+    vertex's threshold (4 B), the records of uniform in-lists are not read
+    (counter 6) and only their live edges' sources are (4 B each, counter 7)."""
+    return (8 * int(st[0]) + 8 * (int(st[1]) - int(st[6])) + 4 * int(st[7]) +
+            4 * int(st[3]) + 12 * int(st[2]) + (4 * int(st[0]) if vthr else 0))
 
 
 def run_sampler_case(args, w, local):
@@ -669,7 +698,8 @@ def run_sampler_case(args, w, local):
     import ripples_b200 as rb
     torch.cuda.set_device(local)
     ctx = rb.Context(local)
-    if w.get("kind") == "p3":  # weighted-cascade R-MAT, 32 draws per vertex
+    if w.get("kind") == "p3" or w["name"].startswith("imm_ic_rmat24"):
+        # weighted-cascade R-MAT, 32 draws per vertex
         scale = args.case_scale or w["scale"]
         dg = rb.DeviceGraph.rmat_on_device(ctx, scale, 32 << scale, "IC", rb.WEIGHTS_WC, seed=0)
     else:
@@ -683,7 +713,7 @@ def run_sampler_case(args, w, local):
     ctx.sync()
     st = pool.stats() - st0
     km, _, _ = pool.timing()
-    alg = alg_bytes_of(st)
+    alg = alg_bytes_of(st, w["model"] == "IC" and dg.uniform_thresholds())
     print(json.dumps({"case": w["name"], "n": dg.n, "m": dg.m, "sets": args.sampler_case,
                       "alg_bytes": alg,
                       "kernel_ms": km - km0, "gb_per_s": alg / ((km - km0) / 1e3) / 1e9,
@@ -870,7 +900,7 @@ def run_p3(args, w, world, rank, local):
         dt = time.perf_counter() - t1
         st = p.stats()
         km, kn, _ = p.timing()
-        alg = 8 * int(st[0]) + 8 * int(st[1]) + 4 * int(st[3]) + 12 * int(st[2])
+        alg = alg_bytes_of(st, bool(dg.uniform_thresholds()))
         samplers[name] = {"sets_per_s": count / dt, "kernel_ms": km, "launches": kn,
                           "alg_gb_per_s": alg / (km / 1e3) / 1e9 if km else None,
                           "frac_of_hbm": (alg / (km / 1e3) / 1e9) / peak if km else None,

@@ -158,7 +158,10 @@ int rip_pool_import(rip_pool *p, const uint64_t *offsets,
  * number of sets it served), stats[1] = in-edges read, stats[2] = sets
  * written, stats[3] = pool elements written, stats[4] = per-set expansions
  * (sum over sets of vertices expanded), stats[5] = per-set in-edges
- * (sum over sets of in-edges of the expanded vertices). */
+ * (sum over sets of in-edges of the expanded vertices), stats[6] = in-edges
+ * of uniform-threshold lists (coins drawn against the vertex's threshold,
+ * records not read; see rip_graph_uniform_thresholds), stats[7] = live edges
+ * of those lists (their source id read). */
 int rip_pool_stats(rip_pool *p, uint64_t stats[8]);
 
 /* Kernel time (CUDA events on the context stream) spent in the sampler
@@ -197,6 +200,23 @@ int rip_pool_work_caps(rip_pool *p, uint64_t plain_cap, uint64_t fused_cap);
 #define RIP_TUNE_CANDIDATES 8
 int rip_graph_autotune(rip_graph *g, uint64_t seed, uint32_t pilot, double *ms, int *choice);
 
+/* Per-vertex uniform IC thresholds.  When every in-edge of a vertex has the
+ * same threshold (weighted cascade, p = 1/in-degree, makes all of them so),
+ * the IC samplers draw that vertex's coins against the one value and read the
+ * source id of a live edge only -- not the 8-byte record of every in-edge.
+ * rip_graph_upload / rip_graph_from_keys build the per-vertex array when such
+ * in-lists (two or more edges) hold at least half of the edges, and turn it
+ * on.  enable: 1 on, 0 off, -1 leave as is; *available (may be null): 1 when
+ * the array exists.  Sets never depend on it.  No reference counterpart (the
+ * reference reads each edge's weight, include/ripples/add_rrrset.h:128-135). */
+int rip_graph_uniform_thresholds(rip_graph *g, int enable, int *available);
+/* The branching factor of a reverse BFS on an IC graph, measured at upload:
+ * the expected number of live in-edges of an edge's source,
+ * sum over edges (u->v) of sum_{w->u} p(w->u), divided by m (0 for LT graphs).
+ * Above 1.1 sets grow large and overlap, and untuned pools grow heavy sets with
+ * the grid-wide BFS (rip_pool_heavy_batch).  No reference counterpart. */
+int rip_graph_branching(const rip_graph *g, double *branching);
+
 /* Variant of the one-set-per-warp IC kernel: 0 = no register cap (32 resident
  * warps per SM), 5 = at most 48 registers (40 warps per SM).  Results do not
  * depend on it; rip_graph_autotune chooses it per graph.  No reference
@@ -207,8 +227,11 @@ int rip_pool_plain_occupancy(rip_pool *p, int blocks_per_sm);
  * 1024-thread CTA per set or, when at least `min_sets` of them are pending,
  * 256 at a time by a multi-colour reverse BFS spread over the whole GPU (the
  * regime of supercritical graphs, where many sets hold a large share of the
- * graph and overlap).  Default 32; 0 = always one CTA per set.  Results do not
- * depend on it.  No reference counterpart (the reference's GPU BFS,
+ * graph and overlap).  Default 32 on IC graphs whose reverse BFS is
+ * supercritical -- the expected live in-edges of an edge's source,
+ * sum over edges (u->v) of sum_{w->u} p(w->u) / m, above 1.1 -- else 0
+ * (weighted cascade: at most 1); 0 = always one CTA per set.  An autotuned graph's pools start from its
+ * tuned value.  Results do not depend on it.  No reference counterpart (the reference's GPU BFS,
  * include/ripples/gpu/bfs.h:1338-1680, has one colour-batched path). */
 int rip_pool_heavy_batch(rip_pool *p, uint32_t min_sets);
 
@@ -427,17 +450,25 @@ int rip_server_stats(const rip_server *s, uint64_t out[10]);
  *            d_vertices[d_set_offsets[i] .. + d_set_lengths[i]) (members in
  *            discovery order, not sorted); *num_elements = elements written.
  *            Sets are bit-identical to rip_sample's for the same seed and ids.
- *   Limits : count <= RIP_STATIC_MAX_SETS per call; n such that eight warps'
- *            n-bit bitmaps plus queues fit in the array (about 24 million
- *            vertices); larger requests return RIP_ERR_LIMIT, as does a
- *            vertex_capacity too small for the sets (message from
- *            rip_static_last_error()).
+ *   Limits : count <= RIP_STATIC_MAX_SETS per call.  IC: n such that eight
+ *            warps' n-bit bitmaps plus queues fit in the array (about 24
+ *            million vertices); LT walks keep no bitmap (any n; a walk may
+ *            reach about 786 000 vertices).  Larger requests return
+ *            RIP_ERR_LIMIT, as does a vertex_capacity too small for the sets
+ *            (message from rip_static_last_error()).
+ *   Speed  : the array is split into as many warps as fit (at most 32 per SM):
+ *            IC gets 120 warps at n = 2^20 and 8 at n = 2^24, against the
+ *            4 736 rip_sample runs on a B200, so large graphs sample far more
+ *            slowly here.
  *   Rules  : the first call on a device looks up the array's address with
- *            cudaGetSymbolAddress; make it before any stream capture.  Every
- *            call shares the array and it keeps the last call's contents (each
- *            call re-zeroes what must start at zero); calls that overlap on the
- *            GPU race, so serialise them.  `stream` is a cudaStream_t (NULL =
- *            legacy default stream); the call returns after it synchronises. */
+ *            cudaGetSymbolAddress and the device's SM count; make that first
+ *            call before any stream capture.  The cached address belongs to
+ *            the device's primary context: do not call again after a
+ *            cudaDeviceReset of that device.  Every call shares the array and
+ *            it keeps the last call's contents (each call re-zeroes what must
+ *            start at zero); calls that overlap on the GPU race, so serialise
+ *            them.  `stream` is a cudaStream_t (NULL = legacy default stream);
+ *            every call synchronises it before returning. */
 #define RIP_STATIC_SCRATCH_BYTES (32u << 20)
 #define RIP_STATIC_MAX_SETS (1u << 20)
 int rip_sample_static(const uint32_t *d_off, const void *d_edges, uint32_t n,

@@ -6,7 +6,9 @@
 # Flags mirror the reference's default compile definitions (CMakeLists.txt:57-67).
 #
 #   make -f oracle/ref.mk            (from the repository root)
-REF      ?= /root/reference
+# The sources are found through REF, else RIPPLES_REFERENCE_DIR from the
+# environment, else the recipe's default location.
+REF      ?= $(or $(RIPPLES_REFERENCE_DIR),/root/reference)
 SITE     ?= $(shell python -c "import site;print(site.getsitepackages()[0])")
 SPDLOG   ?= $(SITE)/flashinfer/data/spdlog/include
 NLOHMANN ?= $(SITE)/include/cudnn_frontend/thirdparty

@@ -14,11 +14,17 @@ constexpr uint32_t FULL = 0xFFFFFFFFu;
 //   LT: threshold = floor(cumulative in-weight up to e * 2^32)
 // off has n+1 entries; edges is padded with {0, 0} records to a multiple of 4
 // and 32-byte aligned so a 4-edge group is one aligned 32-byte read.
+// vthr (IC graphs, optional): vthr[v] != 0 when every in-edge of v has the
+// threshold vthr[v] (weighted cascade: p = 1/in-degree); the IC samplers then
+// compare v's coins against it and read only the sources of live edges.
+// 0 means "read each edge's own threshold" (a uniform threshold of 0, an
+// in-list that never fires, is stored as 0 too: still exact, only slower).
 struct DevGraph {
   uint32_t n;
   uint64_t m;
   const uint32_t *off;
   const uint2 *edges;
+  const uint32_t *vthr = nullptr;
 };
 
 // Flat RRR pool: set s occupies vtx[set_off[s] .. set_off[s] + set_len[s]).

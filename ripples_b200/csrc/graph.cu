@@ -6,6 +6,46 @@
 // graph
 // ---------------------------------------------------------------------------
 
+// IC graphs: the per-vertex uniform thresholds, kept when uniform in-lists of
+// two or more edges hold at least half of the edges (weighted cascade: all of
+// them); the IC samplers then skip the threshold reads of those lists.  The
+// same pass measures the branching factor of a reverse BFS, which picks the
+// heavy-set default of untuned graphs.
+static int setup_vthr(rip_ctx *c, rip_graph *g) {
+  if (g->model != RIP_MODEL_IC || g->m == 0) return RIP_OK;
+  DevMem sums, lam;
+  int rc = dalloc(c, g->vthr, sizeof(uint32_t) * (size_t)g->n);
+  if (!rc) rc = dalloc(c, lam, sizeof(float) * (size_t)g->n);
+  if (!rc) rc = dalloc(c, sums, 2 * sizeof(unsigned long long));
+  if (rc) {  // an optional speed-up: without room for it the graph still works
+    dfree(c, g->vthr);
+    dfree(c, lam);
+    dfree(c, sums);
+    return RIP_OK;
+  }
+  launch_uniform_threshold(ptr<uint32_t>(g->off), ptr<uint2>(g->edges), g->n, g->m,
+                           ptr<uint32_t>(g->vthr), ptr<float>(lam),
+                           ptr<unsigned long long>(sums), c->stream);
+  unsigned long long h[2] = {0, 0};
+  cudaError_t e = cudaMemcpyAsync(h, sums.p, sizeof(h), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  dfree(c, sums);
+  dfree(c, lam);
+  if (e != cudaSuccess) {
+    dfree(c, g->vthr);
+    return set_err(c, RIP_ERR_CUDA, "uniform thresholds: %s", cudaGetErrorString(e));
+  }
+  if (2 * h[0] < g->m) dfree(c, g->vthr);
+  g->use_vthr = g->vthr.p != nullptr;
+  double total = 0.0;
+  std::memcpy(&total, &h[1], sizeof(total));
+  g->branching = total / (double)g->m;
+  // grid-wide multi-colour BFS for heavy sets only where sets grow large and
+  // overlap (a supercritical reverse BFS); else one CTA per heavy set
+  g->default_giant_min = g->branching > kSupercritical ? 32u : 0u;
+  return RIP_OK;
+}
+
 extern "C" int rip_graph_upload(rip_ctx *c, const uint64_t *index,
                                 const uint32_t *src, const float *w, uint32_t n,
                                 uint64_t m, int model, rip_graph **out) {
@@ -78,9 +118,11 @@ extern "C" int rip_graph_upload(rip_ctx *c, const uint64_t *index,
   dfree(c, d_index);
   dfree(c, d_src);
   dfree(c, d_w);
+  if (rc == RIP_OK) rc = setup_vthr(c, g);
   if (rc != RIP_OK) {
     dfree(c, g->off);
     dfree(c, g->edges);
+    dfree(c, g->vthr);
     delete g;
     return rc;
   }
@@ -112,9 +154,11 @@ static int pack_device_csr(rip_ctx *c, const uint64_t *d_index, const uint32_t *
     if (e == cudaSuccess) e = cudaGetLastError();
     if (e != cudaSuccess) rc = set_err(c, RIP_ERR_CUDA, "pack failed: %s", cudaGetErrorString(e));
   }
+  if (!rc) rc = setup_vthr(c, g);
   if (rc) {
     dfree(c, g->off);
     dfree(c, g->edges);
+    dfree(c, g->vthr);
     delete g;
     return rc;
   }
@@ -209,6 +253,7 @@ extern "C" int rip_graph_destroy(rip_graph *g) {
   erase_ptr(c->graphs, g);
   dfree(g->ctx, g->off);
   dfree(g->ctx, g->edges);
+  dfree(g->ctx, g->vthr);
   delete g;
   return RIP_OK;
 }
@@ -235,3 +280,15 @@ extern "C" int rip_graph_thresholds(rip_graph *g, uint32_t *thr) {
   return RIP_OK;
 }
 
+extern "C" int rip_graph_uniform_thresholds(rip_graph *g, int enable, int *available) {
+  if (!g) return RIP_ERR_INVALID;
+  if (available) *available = g->vthr.p != nullptr;
+  if (enable >= 0) g->use_vthr = enable && g->vthr.p != nullptr;
+  return RIP_OK;
+}
+
+extern "C" int rip_graph_branching(const rip_graph *g, double *branching) {
+  if (!g || !branching) return RIP_ERR_INVALID;
+  *branching = g->branching;
+  return RIP_OK;
+}

@@ -236,12 +236,28 @@ struct PinnedMem {
 };
 
 
+// Branching factor above which untuned IC graphs grow heavy sets with the
+// grid-wide multi-colour BFS (sets large and overlapping) rather than one CTA
+// per set.
+constexpr double kSupercritical = 1.1;
+
 struct rip_graph {
   rip_ctx *ctx;
   uint32_t n;
   uint64_t m;
   int model;
   DevMem off, edges;
+  // per-vertex uniform IC thresholds (DevGraph::vthr); allocated only when
+  // uniform in-lists hold at least half of the edges, and used while
+  // use_vthr is set
+  DevMem vthr;
+  bool use_vthr = false;
+  // IC: branching factor of a reverse BFS -- the expected live in-edges of
+  // an edge's source, sum over edges of lambda(src) / m with lambda(u) the
+  // sum of u's in-edge probabilities -- and the heavy-set batch size pools of
+  // an untuned graph start with (rip_pool_heavy_batch)
+  double branching = 0.0;
+  uint32_t default_giant_min = 32;
   // IC sampler configuration picked by rip_graph_autotune (pools created
   // afterwards start from it; RIP_SAMPLER_AUTO follows `sampler`)
   struct Tuned {
@@ -252,7 +268,8 @@ struct rip_graph {
     int plain_occupancy = 0;
   } tuned;
   DevGraph view() {
-    return DevGraph{n, m, ptr<uint32_t>(off), ptr<uint2>(edges)};
+    return DevGraph{n, m, ptr<uint32_t>(off), ptr<uint2>(edges),
+                    use_vthr && vthr.p ? ptr<uint32_t>(vthr) : nullptr};
   }
 };
 

@@ -43,15 +43,15 @@ __device__ uint32_t big_block_scan(uint32_t x, uint32_t *warp_tot, uint32_t *tot
 __global__ void __launch_bounds__(BIG_THREADS)
 ic_bigset_kernel(BigLaunch L) {
   __shared__ uint32_t s_off[BIG_THREADS + 1];  // exclusive group offsets of the chunk
-  __shared__ uint32_t s_beg[BIG_THREADS], s_end[BIG_THREADS];
+  __shared__ uint32_t s_beg[BIG_THREADS], s_end[BIG_THREADS], s_vt[BIG_THREADS];
   __shared__ uint32_t s_warp[BIG_WARPS];
   __shared__ uint32_t s_idx, s_qlen, s_overflow, s_total;
-  __shared__ unsigned long long s_edges, s_base;
+  __shared__ unsigned long long s_edges, s_uedges, s_usrc, s_base;
 
   const uint32_t tid = threadIdx.x;
   uint32_t *bm = L.bitmaps + (size_t)blockIdx.x * L.bm_words;
   uint32_t *q = L.queues + (size_t)blockIdx.x * L.qcap;
-  unsigned long long n_exp = 0, n_edges = 0, n_sets = 0, n_elems = 0;
+  unsigned long long n_exp = 0, n_edges = 0, n_sets = 0, n_elems = 0, n_uedges = 0, n_usrc = 0;
 
   for (;;) {
     if (tid == 0) s_idx = atomicAdd(L.next, 1u);
@@ -67,21 +67,26 @@ ic_bigset_kernel(BigLaunch L) {
       s_qlen = 1;
       s_overflow = 0;
       s_edges = 0;
+      s_uedges = 0;
+      s_usrc = 0;
     }
     __syncthreads();
     uint32_t lo = 0, hi = 1;
     while (lo < hi && !s_overflow) {
       for (uint32_t cb = lo; cb < hi; cb += BIG_THREADS) {
         const uint32_t e = cb + tid;
-        uint32_t beg = 0, end = 0;
+        uint32_t beg = 0, end = 0, vt = 0;
         if (e < hi) {
           const uint32_t v = q[e];
           beg = __ldg(L.G.off + v);
           end = __ldg(L.G.off + v + 1);
+          if (L.G.vthr) vt = __ldg(L.G.vthr + v);
           atomicAdd(&s_edges, (unsigned long long)(end - beg));
+          if (vt) atomicAdd(&s_uedges, (unsigned long long)(end - beg));
         }
         s_beg[tid] = beg;
         s_end[tid] = end;
+        s_vt[tid] = vt;
         const uint32_t ng = group_count(beg, end);
         s_off[tid] = big_block_scan(ng, s_warp, &s_total);
         if (tid == 0) s_off[BIG_THREADS] = s_total;
@@ -95,16 +100,20 @@ ic_bigset_kernel(BigLaunch L) {
             if (s_off[mid] <= j) a = mid;
             else b = mid;
           }
-          const uint32_t ob = s_beg[a], oe = s_end[a];
+          const uint32_t ob = s_beg[a], oe = s_end[a], ovt = s_vt[a];
           const uint32_t g = (ob >> 2) + (j - s_off[a]);
-          uint2 rec[4];
-          load_group(L.G.edges, g, rec);
+          uint2 rec[4] = {};
+          if (!ovt) load_group(L.G.edges, g, rec);  // else: uniform threshold
           const u32x4 c = ic_coins(L.key, g, s);
 #pragma unroll
           for (int t = 0; t < 4; ++t) {
             const uint32_t ed = (g << 2) + t;
-            if (ed >= ob && ed < oe && lane_of(c, t) < rec[t].y) {
-              const uint32_t u = rec[t].x;
+            if (ed >= ob && ed < oe && lane_of(c, t) < (ovt ? ovt : rec[t].y)) {
+              uint32_t u = rec[t].x;
+              if (ovt) {
+                u = __ldg(&L.G.edges[ed].x);
+                atomicAdd(&s_usrc, 1ull);
+              }
               const uint32_t bit = 1u << (u & 31);
               if (!(atomicOr(&bm[u >> 5], bit) & bit)) {
                 const uint32_t pos = atomicAdd(&s_qlen, 1u);
@@ -153,6 +162,8 @@ ic_bigset_kernel(BigLaunch L) {
         n_elems += qlen;
         n_exp += qlen;
         n_edges += s_edges;
+        n_uedges += s_uedges;
+        n_usrc += s_usrc;
       } else {
         L.F.ids[atomicAdd(L.F.count, 1u)] = rel;
       }
@@ -166,6 +177,8 @@ ic_bigset_kernel(BigLaunch L) {
     atomicAdd(L.st.v + 3, n_elems);
     atomicAdd(L.st.v + 4, n_exp);
     atomicAdd(L.st.v + 5, n_edges);
+    if (n_uedges) atomicAdd(L.st.v + 6, n_uedges);
+    if (n_usrc) atomicAdd(L.st.v + 7, n_usrc);
   }
 }
 

@@ -145,6 +145,59 @@ void launch_validate_csr(const uint64_t *index, const uint32_t *src, uint32_t n,
   validate_csr_kernel<<<2368, 256, 0, stream>>>(index, src, n, m, bad);
 }
 
+// vthr[v] = the threshold every in-edge of v shares, else 0; lam[v] = the
+// expected number of live in-edges of v (sum of its thresholds / 2^32).  One
+// warp per vertex.  sums[0] += in-degrees of the uniform vertices with at
+// least two in-edges (the edge reads the IC samplers can skip).
+__global__ void uniform_threshold_kernel(const uint32_t *off, const uint2 *edges, uint32_t n,
+                                         uint32_t *vthr, float *lam, unsigned long long *sums) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  unsigned long long cov = 0;
+  for (uint64_t v = warp; v < n; v += warps) {
+    const uint32_t beg = off[v], end = off[v + 1];
+    const uint32_t t = end > beg ? edges[beg].y : 0u;
+    bool same = true;
+    unsigned long long tsum = 0;
+    for (uint32_t e = beg + lane; e < end; e += 32) {
+      const uint32_t x = edges[e].y;
+      same = same && x == t;
+      tsum += x;
+    }
+    same = __all_sync(0xFFFFFFFFu, same);
+    for (int d = 16; d > 0; d >>= 1) tsum += __shfl_xor_sync(0xFFFFFFFFu, tsum, d);
+    if (lane == 0) {
+      vthr[v] = same ? t : 0u;
+      lam[v] = (float)((double)tsum * (1.0 / 4294967296.0));
+      if (same && t && end - beg >= 2) cov += end - beg;
+    }
+  }
+  if (lane == 0 && cov) atomicAdd(sums, cov);
+}
+
+// *total (a double) += lam[source] over every edge: divided by m it is the
+// branching factor of a reverse BFS (the expected live in-edges of the vertex
+// an edge leads to).
+__global__ void branching_kernel(const uint2 *edges, uint64_t m, const float *lam,
+                                 double *total) {
+  const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  double acc = 0.0;
+  for (uint64_t e = tid; e < m; e += stride) acc += (double)lam[edges[e].x];
+  for (int d = 16; d > 0; d >>= 1) acc += __shfl_xor_sync(0xFFFFFFFFu, acc, d);
+  if ((threadIdx.x & 31u) == 0 && acc != 0.0) atomicAdd(total, acc);
+}
+
+void launch_uniform_threshold(const uint32_t *off, const uint2 *edges, uint32_t n, uint64_t m,
+                              uint32_t *vthr, float *lam, unsigned long long *sums,
+                              cudaStream_t stream) {
+  count_launches(2);
+  cudaMemsetAsync(sums, 0, 2 * sizeof(*sums), stream);
+  uniform_threshold_kernel<<<2368, 256, 0, stream>>>(off, edges, n, vthr, lam, sums);
+  branching_kernel<<<2368, 256, 0, stream>>>(edges, m, lam, reinterpret_cast<double *>(sums + 1));
+}
+
 void launch_pack_lt(const uint64_t *index, const float *w, uint32_t n,
                     uint64_t m, uint32_t *off, uint2 *edges, const uint32_t *src,
                     cudaStream_t stream) {

@@ -81,6 +81,9 @@ struct SetOutcome {
   uint32_t qlen;
   bool overflow, big;
   unsigned long long exp, edges;  // per-set work (valid on lane 0 / summed over lanes)
+  // IC, summed over lanes: in-edges of uniform-threshold lists (coins drawn,
+  // records not read) and live edges of those lists (source id read)
+  unsigned long long uedges = 0, usrc = 0;
 };
 
 // One IC set: reverse BFS from root(s) over live in-edges, warp-cooperative,
@@ -98,16 +101,19 @@ __device__ __forceinline__ SetOutcome ic_plain_set(const DevGraph &G, Key key, u
   uint32_t qlen = 1, head = 0;
   bool overflow = false, big = false;
   unsigned long long set_exp = 0, set_edges = 0, warp_edges = 0;
+  uint32_t set_uedges = 0, set_usrc = 0;  // a set's edges are fewer than m < 2^32
 
   while (head < qlen && !overflow) {
     const uint32_t take = min(32u, qlen - head);
-    uint32_t beg = 0, end = 0, ng = 0;
+    uint32_t beg = 0, end = 0, ng = 0, vt = 0;
     if (lane < take) {
       const uint32_t v = W.q[head + lane];
       beg = __ldg(G.off + v);
       end = __ldg(G.off + v + 1);
+      if (G.vthr) vt = __ldg(G.vthr + v);
       ng = group_count(beg, end);
       set_edges += end - beg;
+      if (vt) set_uedges += end - beg;
     }
     set_exp += (lane == 0) ? take : 0;
     const uint32_t incl = warp_incl_scan(ng);
@@ -126,20 +132,26 @@ __device__ __forceinline__ SetOutcome ic_plain_set(const DevGraph &G, Key key, u
       const uint32_t oe = __shfl_sync(FULL, end, owner);
       const uint32_t oexcl = __shfl_sync(FULL, incl, owner) -
                              __shfl_sync(FULL, ng, owner);
+      // the owner's uniform threshold (0: read each edge's record)
+      const uint32_t ovt = __shfl_sync(FULL, vt, owner);
       uint32_t nu[4];
       bool isnew[4];
       if (valid) {
         const uint32_t g = (ob >> 2) + (j - oexcl);
-        uint2 rec[4];
-        load_group(G.edges, g, rec);
+        uint2 rec[4] = {};
+        if (!ovt) load_group(G.edges, g, rec);
         const u32x4 c = ic_coins(key, g, s);
 #pragma unroll
         for (int t = 0; t < 4; ++t) {
           const uint32_t e = (g << 2) + t;
-          const bool live = e >= ob && e < oe && lane_of(c, t) < rec[t].y;
+          const bool live = e >= ob && e < oe && lane_of(c, t) < (ovt ? ovt : rec[t].y);
           isnew[t] = false;
           nu[t] = rec[t].x;
           if (live) {
+            if (ovt) {
+              nu[t] = __ldg(&G.edges[e].x);
+              ++set_usrc;
+            }
             const uint32_t bit = 1u << (nu[t] & 31);
             const uint32_t old = atomicOr(&W.bm[nu[t] >> 5], bit);
             isnew[t] = !(old & bit);
@@ -171,7 +183,7 @@ __device__ __forceinline__ SetOutcome ic_plain_set(const DevGraph &G, Key key, u
     }
     head += take;
   }
-  return SetOutcome{qlen, overflow, big, set_exp, set_edges};
+  return SetOutcome{qlen, overflow, big, set_exp, set_edges, set_uedges, set_usrc};
 }
 
 // One LT set: the single-predecessor walk from root(s) (see lt_walk_kernel).
@@ -267,7 +279,7 @@ ic_plain_kernel(DevGraph G, DevPool P, Key key, uint64_t first, uint32_t count,
   const uint32_t lane = lane_id();
   const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   WarpCtx W{bitmaps + w * bm_words, queues + w * (uint64_t)qcap, qcap};
-  unsigned long long n_exp = 0, n_edges = 0, n_sets = 0, n_elems = 0;
+  unsigned long long n_exp = 0, n_edges = 0, n_sets = 0, n_elems = 0, n_uedges = 0, n_usrc = 0;
 
   for (;;) {
     uint32_t idx = 0;
@@ -282,12 +294,16 @@ ic_plain_kernel(DevGraph G, DevPool P, Key key, uint64_t first, uint32_t count,
       n_elems += (lane == 0) ? o.qlen : 0;
       n_exp += o.exp;
       n_edges += o.edges;
+      n_uedges += o.uedges;
+      n_usrc += o.usrc;
     }
   }
   n_exp = warp_sum_u64(n_exp);
   n_edges = warp_sum_u64(n_edges);
   n_sets = warp_sum_u64(n_sets);
   n_elems = warp_sum_u64(n_elems);
+  n_uedges = warp_sum_u64(n_uedges);
+  n_usrc = warp_sum_u64(n_usrc);
   if (lane == 0) {
     atomicAdd(st.v + 0, n_exp);
     atomicAdd(st.v + 1, n_edges);
@@ -295,6 +311,8 @@ ic_plain_kernel(DevGraph G, DevPool P, Key key, uint64_t first, uint32_t count,
     atomicAdd(st.v + 3, n_elems);
     atomicAdd(st.v + 4, n_exp);
     atomicAdd(st.v + 5, n_edges);
+    if (n_uedges) atomicAdd(st.v + 6, n_uedges);
+    if (n_usrc) atomicAdd(st.v + 7, n_usrc);
   }
 }
 
@@ -354,9 +372,10 @@ multi_sample_kernel(MultiLaunch L) {
   WarpCtx W{L.bitmaps + w * L.bm_words, L.queues + w * (uint64_t)L.qcap, L.qcap};
   // counters of the instance the warp is on, flushed when it moves on
   uint32_t cur = ~0u;
-  unsigned long long n_exp = 0, n_edges = 0, n_sets = 0, n_elems = 0;
+  unsigned long long n_exp = 0, n_edges = 0, n_sets = 0, n_elems = 0, n_uedges = 0, n_usrc = 0;
   auto flush = [&]() {
     const unsigned long long e = warp_sum_u64(n_exp), d = warp_sum_u64(n_edges);
+    const unsigned long long ue = warp_sum_u64(n_uedges), us = warp_sum_u64(n_usrc);
     if (lane == 0 && cur != ~0u && n_sets) {
       unsigned long long *st = L.inst[cur].stats;
       atomicAdd(st + 0, e);
@@ -365,8 +384,10 @@ multi_sample_kernel(MultiLaunch L) {
       atomicAdd(st + 3, n_elems);
       atomicAdd(st + 4, e);
       atomicAdd(st + 5, d);
+      if (ue) atomicAdd(st + 6, ue);
+      if (us) atomicAdd(st + 7, us);
     }
-    n_exp = n_edges = n_sets = n_elems = 0;
+    n_exp = n_edges = n_sets = n_elems = n_uedges = n_usrc = 0;
   };
   for (;;) {
     uint32_t idx = 0;
@@ -393,6 +414,8 @@ multi_sample_kernel(MultiLaunch L) {
       n_elems += o.qlen;
       n_exp += o.exp;
       n_edges += o.edges;
+      n_uedges += o.uedges;
+      n_usrc += o.usrc;
     } else if (lane == 0) {
       const unsigned int f = atomicAdd(L.fail_count, 1u);
       L.fail[2 * f] = a;

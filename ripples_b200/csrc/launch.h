@@ -179,6 +179,12 @@ void launch_validate_csr(const uint64_t *index, const uint32_t *src, uint32_t n,
 void launch_pack_lt(const uint64_t *index, const float *w, uint32_t n,
                     uint64_t m, uint32_t *off, uint2 *edges, const uint32_t *src,
                     cudaStream_t stream);
+// Per-vertex uniform IC thresholds (DevGraph::vthr); sums[0] = the edges they
+// cover, sums[1] holds a double whose value / m is the branching factor of a
+// reverse BFS (zero bits are 0.0).  lam is n floats of scratch.
+void launch_uniform_threshold(const uint32_t *off, const uint2 *edges, uint32_t n, uint64_t m,
+                              uint32_t *vthr, float *lam, unsigned long long *sums,
+                              cudaStream_t stream);
 
 // Selection.
 void launch_count(const DevPool &P, uint64_t num_sets, uint32_t *count,

@@ -28,6 +28,7 @@ extern "C" int rip_pool_create(rip_ctx *c, rip_graph *g, rip_pool **out) {
     return rc;
   }
   cudaMemsetAsync(p->meta.p, 0, sizeof(PoolMeta), c->stream);
+  p->giant_min = g->default_giant_min;
   if (g->tuned.set) {
     p->auto_sampler = g->tuned.sampler;
     p->colors = g->tuned.colors;

@@ -16,11 +16,23 @@
 //   * g_static_scratch is RIP_STATIC_SCRATCH_BYTES (32 MiB); every GPU that
 //     loads this library holds it until the process exits.
 //   * At most RIP_STATIC_MAX_SETS sets per call, and n small enough that
-//     eight warps' n-bit bitmaps plus queues fit in the scratch; larger
-//     requests are rejected with RIP_ERR_LIMIT and a message.
+//     eight warps' scratch fits in the array: IC needs an n-bit bitmap plus a
+//     queue per warp (n up to about 24 million vertices), LT only the queue
+//     (its walks find revisits by scanning it).  Larger requests are rejected
+//     with RIP_ERR_LIMIT and a message.
+//   * Throughput follows the array size: the scratch is split into as many
+//     warps as fit, at most 32 per SM.  With 24 MiB left after the id lists,
+//     IC on n = 2^20 gets 120 warps (192 KiB each; rip_sample runs 4 736 on a
+//     B200) and on n = 2^24 the minimum of 8, so large graphs sample far
+//     slower than through rip_sample.  LT warps hold a 64 KiB queue each
+//     (376 warps at any n); a walk may grow to about 786 000 vertices.
 //   * The first call on a device looks up the array's device address with
-//     cudaGetSymbolAddress (with that device current) and caches it; make
-//     that first call before any stream capture.
+//     cudaGetSymbolAddress (with that device current) and the device's SM
+//     count, and caches both; make that first call before any stream capture.
+//     Every call then synchronises `stream` before it returns.
+//   * The cached address belongs to the device's primary context: after a
+//     cudaDeviceReset on that device the process must not call this entry
+//     point again.
 //   * All calls share the one array and it keeps the last call's contents;
 //     each call re-zeroes what must start at zero (counters, bitmaps).  Calls
 //     whose work overlaps on the GPU (other streams, other host threads on the
@@ -55,6 +67,7 @@ struct StaticMeta {  // at the start of g_static_scratch
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 void *g_addr[kMaxDevices] = {};
+int g_sms[kMaxDevices] = {};
 thread_local std::string g_err;
 
 int fail(int code, const char *fmt, ...) {
@@ -67,8 +80,9 @@ int fail(int code, const char *fmt, ...) {
   return code;
 }
 
-// Device address of g_static_scratch on the current device (set up once).
-int scratch_address(unsigned char **out) {
+// Device address of g_static_scratch on the current device and the device's
+// SM count (set up once per device).
+int scratch_address(unsigned char **out, int *sms) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return fail(RIP_ERR_CUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
@@ -80,9 +94,15 @@ int scratch_address(unsigned char **out) {
     if (e != cudaSuccess || !p)
       return fail(RIP_ERR_CUDA, "cudaGetSymbolAddress(g_static_scratch): %s",
                   cudaGetErrorString(e));
+    int count = 0;
+    e = cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess || count <= 0)
+      return fail(RIP_ERR_CUDA, "cudaDeviceGetAttribute(SM count): %s", cudaGetErrorString(e));
+    g_sms[dev] = count;
     g_addr[dev] = p;
   }
   *out = static_cast<unsigned char *>(g_addr[dev]);
+  *sms = g_sms[dev];
   return RIP_OK;
 }
 
@@ -114,7 +134,8 @@ extern "C" int rip_sample_static(const uint32_t *d_off, const void *d_edges,
   if (count == 0) return RIP_OK;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   unsigned char *base = nullptr;
-  int rc = scratch_address(&base);
+  int sms = 0;
+  int rc = scratch_address(&base, &sms);
   if (rc != RIP_OK) return rc;
 
   StaticMeta *meta = reinterpret_cast<StaticMeta *>(base);
@@ -122,15 +143,16 @@ extern "C" int rip_sample_static(const uint32_t *d_off, const void *d_edges,
                       reinterpret_cast<uint32_t *>(base + kMetaBytes + kIdsBytes)};
   unsigned char *work = base + kMetaBytes + 2 * kIdsBytes;
   const size_t work_bytes = RIP_STATIC_SCRATCH_BYTES - kMetaBytes - 2 * kIdsBytes;
-  const uint64_t bm_words = (((uint64_t)n + 31) / 32 + 7) & ~7ull;
+  // IC warps keep an n-bit visited bitmap; LT walks need none
+  const uint64_t bm_words = model == RIP_MODEL_IC ? (((uint64_t)n + 31) / 32 + 7) & ~7ull : 0;
   const uint64_t bm_bytes = bm_words * 4;
 
-  // Partition: as many warps as fit (multiple of 8, up to 32 per SM's worth
-  // of a B200), each with an n-bit bitmap and a queue of qcap entries.
+  // Partition: as many warps as fit (multiple of 8, at most 32 per SM of this
+  // device), each with its bitmap and a queue of qcap entries.
   uint32_t qcap = n < (1u << 14) ? n : (1u << 14);
   auto warps_for = [&](uint32_t q) -> uint64_t {
     uint64_t w = work_bytes / (bm_bytes + 4ull * q);
-    if (w > 148 * 32) w = 148 * 32;
+    if (w > (uint64_t)sms * 32) w = (uint64_t)sms * 32;
     return w & ~7ull;
   };
   if (warps_for(qcap) < 8)
@@ -143,10 +165,17 @@ extern "C" int rip_sample_static(const uint32_t *d_off, const void *d_edges,
     return fail(RIP_ERR_CUDA, "cudaMemsetAsync(meta) failed");
   SampleLaunch L;
   L.G = DevGraph{n, m, d_off, static_cast<const uint2 *>(d_edges)};
-  // the kernels index the set arrays by absolute set id: shift the caller's
-  // buffers so entry `first` lands at index 0
-  L.P = DevPool{d_vertices, &meta->cursor, vertex_capacity, d_set_offsets - first,
-                d_set_lengths - first};
+  // The kernels index the set arrays by absolute set id, so they get the
+  // caller's buffers moved back by `first` entries: entry `first` is then the
+  // caller's index 0, and only ids in [first, first + count) are written.  The
+  // moved addresses are formed in integer arithmetic (the pointer arithmetic
+  // would leave the buffers' bounds) and are never dereferenced below `first`.
+  auto moved_back = [first](void *ptr, size_t elem) {
+    return reinterpret_cast<uintptr_t>(ptr) - (uintptr_t)(first * elem);
+  };
+  L.P = DevPool{d_vertices, &meta->cursor, vertex_capacity,
+                reinterpret_cast<uint64_t *>(moved_back(d_set_offsets, sizeof(uint64_t))),
+                reinterpret_cast<uint32_t *>(moved_back(d_set_lengths, sizeof(uint32_t)))};
   L.key = make_key(seed);
   L.first = first;
   L.next = &meta->next;
@@ -160,7 +189,7 @@ extern "C" int rip_sample_static(const uint32_t *d_off, const void *d_edges,
                   "rip_sample_static: a set outgrew the queues the static scratch can hold "
                   "for n = %u", n);
     // bitmaps must start all-zero; this region may have held queues before
-    if (cudaMemsetAsync(work, 0, warps * bm_bytes, s) != cudaSuccess ||
+    if ((bm_bytes && cudaMemsetAsync(work, 0, warps * bm_bytes, s) != cudaSuccess) ||
         cudaMemsetAsync(&meta->fail_count, 0, sizeof(unsigned int), s) != cudaSuccess ||
         cudaMemsetAsync(&meta->next, 0, sizeof(unsigned int), s) != cudaSuccess ||
         cudaMemsetAsync(&meta->first_bad, 0xFF, sizeof(unsigned long long), s) != cudaSuccess)

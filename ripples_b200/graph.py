@@ -288,6 +288,24 @@ class DeviceGraph:
         ctx._children.add(obj)
         return obj
 
+    def uniform_thresholds(self, enable: Optional[bool] = None) -> bool:
+        """Whether the per-vertex uniform IC thresholds exist
+        (``rip_graph_uniform_thresholds``); ``enable`` turns their use on or
+        off (sets never depend on it)."""
+        avail = ctypes.c_int()
+        check(lib.rip_graph_uniform_thresholds(self.h, -1 if enable is None else int(enable),
+                                               ctypes.byref(avail)),
+              "rip_graph_uniform_thresholds", self.ctx.h)
+        return bool(avail.value)
+
+    @property
+    def branching(self) -> float:
+        """Branching factor of a reverse BFS (IC; ``rip_graph_branching``)."""
+        b = ctypes.c_double()
+        check(lib.rip_graph_branching(self.h, ctypes.byref(b)), "rip_graph_branching",
+              self.ctx.h)
+        return b.value
+
     def export(self) -> Tuple[np.ndarray, np.ndarray]:
         idx = np.zeros(self.n + 1, dtype=np.uint64)
         src = np.zeros(max(self.m, 1), dtype=np.uint32)

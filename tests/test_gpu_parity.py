@@ -407,3 +407,64 @@ def test_corner_graphs_match_oracle(ctx, model, case):
         assert seeds.tolist() == o["seeds"] and rec.theta == o["theta"], (case, tie)
         q.close()
         dg.close()
+
+
+def mixed_uniform_graph(scale=12, deg=16, seed=31):
+    """Weighted cascade on two vertices in three, U(0, 0.3) per edge on the
+    rest: uniform in-lists hold about two thirds of the edges, so the graph
+    keeps per-vertex uniform thresholds and the samplers meet both kinds of
+    list in one set."""
+    g = rb.HostGraph.rmat(scale, deg << scale, seed=seed)
+    wc = g.with_weights(rb.WEIGHTS_WC).weights
+    un = g.with_weights(rb.WEIGHTS_UNIFORM, seed=seed + 1, lo=0.0, hi=0.3).weights
+    dst = np.repeat(np.arange(g.n), np.diff(g.index).astype(np.int64))
+    return rb.HostGraph(g.n, g.index, g.src, np.where(dst % 3 == 0, un, wc).astype(np.float32))
+
+
+@pytest.mark.parametrize("path", ["plain", "cta_per_set", "multi"])
+def test_uniform_thresholds_match_oracle(ctx, path):
+    g = mixed_uniform_graph()
+    dg = rb.DeviceGraph(ctx, g, "IC")
+    assert dg.uniform_thresholds()  # built at upload, on
+    ooff, ovtx, ost = oracle_sets(g, "IC", 17, 0, 3000)
+    try:
+        for enable in (True, False):
+            dg.uniform_thresholds(enable)
+            p = rb.Pool(dg)
+            if path == "cta_per_set":
+                p.work_caps(64, 1 << 23)  # nearly every set goes to the CTA-per-set kernel
+                p.heavy_batch(0)
+            if path == "multi":
+                rb.sample_multi(ctx, [p], [17], [3000])
+            else:
+                p.sample(3000, seed=17, sampler=rb.SAMPLER_PLAIN)
+            off, vtx = p.export()
+            assert_same_sets(off, vtx, ooff, ovtx)
+            st = p.stats()
+            assert st[5] == ost[1]  # coins drawn for every in-edge of every member
+            # records of uniform lists are skipped only when switched on
+            assert (st[6] > 0) == enable and (st[7] > 0) == enable
+            p.close()
+    finally:
+        dg.close()
+
+
+def test_uniform_thresholds_only_where_they_pay(ctx):
+    # U(0, 0.3) per edge: only in-lists of one edge are uniform, far from half
+    # of the edges, so no per-vertex array is kept
+    dg = rb.DeviceGraph(ctx, ic_graph(12), "IC")
+    assert not dg.uniform_thresholds()
+    dg.close()
+    # weighted cascade: every list is uniform, and a reverse BFS is at most
+    # critical (an edge's source has one live in-edge on average, or none)
+    g = rb.HostGraph.rmat(12, 8 << 12, seed=3).with_weights(rb.WEIGHTS_WC)
+    dg = rb.DeviceGraph(ctx, g, "IC")
+    assert dg.uniform_thresholds()
+    lam = np.bincount(np.repeat(np.arange(g.n), np.diff(g.index).astype(np.int64)),
+                      weights=g.weights.astype(np.float64), minlength=g.n)
+    assert abs(dg.branching - lam[g.src].mean()) < 1e-3 and dg.branching <= 1.0 + 1e-6
+    dg.close()
+    # LT graphs never keep one
+    dg = rb.DeviceGraph(ctx, lt_graph(10), "LT")
+    assert not dg.uniform_thresholds()
+    dg.close()

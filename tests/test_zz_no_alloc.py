@@ -8,8 +8,11 @@ rip_sample_static takes the packed graph and the output buffers in their own
 device memory and keeps its scratch in a fixed static device array.  This
 test builds those buffers with torch (outside the call), runs two calls in a
 row through the C ABI, and checks every set against what rip_sample -- the
-allocating entry point -- produces for the same seed and set ids: the sets
-must be identical, bit for bit.
+allocating entry point -- produces for the same seed and set ids, and against
+the CPU oracle: the sets must be identical, bit for bit.  A second case grows
+sets past the 16 384-entry queues the array starts with, so the entry point
+must re-run them with wider queues (fewer warps) and still return the same
+sets.
 """
 import ctypes
 
@@ -17,6 +20,7 @@ import numpy as np
 import pytest
 
 import ripples_b200 as rb
+from oracle import oracle as O
 from ripples_b200 import _lib
 
 pytestmark = pytest.mark.gpu
@@ -72,13 +76,35 @@ def test_static_sampling_matches_rip_sample(ctx, model):
     pool.sample(count, seed=seed, sampler=rb.SAMPLER_PLAIN)
     off, vtx = pool.export()
     expected = [vtx[off[i]:off[i + 1]] for i in range(2 * count)]
+    thr = O.pack(model, g.index, g.weights)
+    ooff, ovtx, _ = O.sample(model, g.n, g.index, g.src, thr, seed, 0, 2 * count)
     capacity = int(off[-1]) + 1024
     # two calls in a row: sets [0, count) then [count, 2*count)
     for call in range(2):
         got = run_static(d_off, d_edges, g, model, seed, call * count, count, capacity)
         for i, s in enumerate(got):
-            assert np.array_equal(s, expected[call * count + i]), (call, i)
+            j = call * count + i
+            assert np.array_equal(s, expected[j]), (call, i)
+            assert np.array_equal(s, ovtx[ooff[j]:ooff[j + 1]]), (call, i)
     pool.close()
+    dg.close()
+
+
+def test_static_sampling_retries_sets_past_the_first_queues(ctx):
+    # R-MAT 2^16 with p ~ U(0, 0.5): about two live in-edges per vertex, so
+    # many sets hold a large share of the graph, more than the 16 384 entries
+    # of the queues the scratch is first split into
+    g = rb.HostGraph.rmat(16, 8 << 16, seed=5).with_weights(rb.WEIGHTS_UNIFORM, seed=6, lo=0.0,
+                                                             hi=0.5)
+    seed, count = 9, 200
+    dg, d_off, d_edges = packed_graph(ctx, g, "IC")
+    thr = O.pack("IC", g.index, g.weights)
+    ooff, ovtx, _ = O.sample("IC", g.n, g.index, g.src, thr, seed, 0, count)
+    for call in range(2):
+        got = run_static(d_off, d_edges, g, "IC", seed, 0, count, count * g.n)
+        assert max(len(x) for x in got) > (1 << 14)
+        for i, x in enumerate(got):
+            assert np.array_equal(x, ovtx[ooff[i]:ooff[i + 1]]), (call, i)
     dg.close()
 
 
