@@ -89,6 +89,12 @@ const char *rip_version(void);
 int rip_ctx_stream(rip_ctx *ctx, void **stream);
 /* Number of kernels this library has launched in the process so far. */
 uint64_t rip_kernel_launches(void);
+/* Measured ceiling of the IC coin function on this device: coins per second
+ * of a kernel that only draws coins (Philox4x32-10, four per block) the way a
+ * uniform-threshold in-list is expanded, at full occupancy, no memory
+ * traffic.  The roofline of the samplers on weighted-cascade graphs, which
+ * are bound by this arithmetic rather than by HBM.  No reference counterpart. */
+int rip_coin_rate(rip_ctx *ctx, double *coins_per_s);
 
 /* ---- graph ---------------------------------------------------------------- */
 /* Uploads a backward CSR (GraphBwd) and packs it for the kernels: weights are

@@ -122,6 +122,7 @@ SIGNATURES = {
     "rip_kernel_launches": (U64, []),
     "rip_graph_uniform_thresholds": (I32, [P, I32, ctypes.POINTER(I32)]),
     "rip_graph_branching": (I32, [P, ctypes.POINTER(ctypes.c_double)]),
+    "rip_coin_rate": (I32, [P, ctypes.POINTER(ctypes.c_double)]),
     "rip_graph_upload": (I32, [P, P, P, P, U32, U64, I32, PP]),
     "rip_graph_destroy": (I32, [P]),
     "rip_graph_info": (I32, [P, ctypes.POINTER(U32), ctypes.POINTER(U64), ctypes.POINTER(I32)]),

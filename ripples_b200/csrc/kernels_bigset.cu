@@ -20,6 +20,9 @@ namespace {
 
 constexpr int BIG_THREADS = 1024;
 constexpr int BIG_WARPS = BIG_THREADS / 32;
+// In-lists of at least this many 4-edge groups are swept by the whole CTA, one
+// list at a time.
+constexpr uint32_t kLongCTA = 1024;
 
 // Exclusive block scan of one u32 per thread; returns the exclusive value and
 // writes the block total to *total.  Uses `warp_tot` (BIG_WARPS entries).
@@ -45,7 +48,8 @@ ic_bigset_kernel(BigLaunch L) {
   __shared__ uint32_t s_off[BIG_THREADS + 1];  // exclusive group offsets of the chunk
   __shared__ uint32_t s_beg[BIG_THREADS], s_end[BIG_THREADS], s_vt[BIG_THREADS];
   __shared__ uint32_t s_warp[BIG_WARPS];
-  __shared__ uint32_t s_idx, s_qlen, s_overflow, s_total;
+  __shared__ uint32_t s_long[BIG_THREADS];  // entries of the chunk with long in-lists
+  __shared__ uint32_t s_idx, s_qlen, s_overflow, s_total, s_nlong;
   __shared__ unsigned long long s_edges, s_uedges, s_usrc, s_base;
 
   const uint32_t tid = threadIdx.x;
@@ -72,10 +76,35 @@ ic_bigset_kernel(BigLaunch L) {
     }
     __syncthreads();
     uint32_t lo = 0, hi = 1;
+    // Coins of group g of the in-list [ob, oe) (uniform threshold ovt, or 0:
+    // each record's own); newly reached sources go to the queue.
+    auto expand_group = [&](uint32_t g, uint32_t ob, uint32_t oe, uint32_t ovt) {
+      uint2 rec[4] = {};
+      if (!ovt) load_group(L.G.edges, g, rec);  // else: uniform threshold
+      const u32x4 c = ic_coins(L.key, g, s);
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const uint32_t ed = (g << 2) + t;
+        if (ed >= ob && ed < oe && lane_of(c, t) < (ovt ? ovt : rec[t].y)) {
+          uint32_t u = rec[t].x;
+          if (ovt) {
+            u = __ldg(&L.G.edges[ed].x);
+            atomicAdd(&s_usrc, 1ull);
+          }
+          const uint32_t bit = 1u << (u & 31);
+          if (!(atomicOr(&bm[u >> 5], bit) & bit)) {
+            const uint32_t pos = atomicAdd(&s_qlen, 1u);
+            if (pos < L.qcap) q[pos] = u;
+            else s_overflow = 1;
+          }
+        }
+      }
+    };
     while (lo < hi && !s_overflow) {
       for (uint32_t cb = lo; cb < hi; cb += BIG_THREADS) {
         const uint32_t e = cb + tid;
         uint32_t beg = 0, end = 0, vt = 0;
+        if (tid == 0) s_nlong = 0;
         if (e < hi) {
           const uint32_t v = q[e];
           beg = __ldg(L.G.off + v);
@@ -88,40 +117,36 @@ ic_bigset_kernel(BigLaunch L) {
         s_end[tid] = end;
         s_vt[tid] = vt;
         const uint32_t ng = group_count(beg, end);
-        s_off[tid] = big_block_scan(ng, s_warp, &s_total);
+        const bool lng = ng >= kLongCTA;
+        s_off[tid] = big_block_scan(lng ? 0u : ng, s_warp, &s_total);  // syncs
         if (tid == 0) s_off[BIG_THREADS] = s_total;
+        if (lng) s_long[atomicAdd(&s_nlong, 1u)] = tid;
         __syncthreads();
-        const uint32_t total = s_off[BIG_THREADS];
-        for (uint32_t j = tid; j < total; j += BIG_THREADS) {
-          // entry a: s_off[a] <= j < s_off[a + 1]
-          uint32_t a = 0, b = BIG_THREADS;
-          while (b - a > 1) {
-            const uint32_t mid = (a + b) >> 1;
-            if (s_off[mid] <= j) a = mid;
-            else b = mid;
-          }
+        // long in-lists (hubs): all threads sweep one list at a time
+        const uint32_t nlong = s_nlong;
+        for (uint32_t li = 0; li < nlong; ++li) {
+          const uint32_t a = s_long[li];
           const uint32_t ob = s_beg[a], oe = s_end[a], ovt = s_vt[a];
-          const uint32_t g = (ob >> 2) + (j - s_off[a]);
-          uint2 rec[4] = {};
-          if (!ovt) load_group(L.G.edges, g, rec);  // else: uniform threshold
-          const u32x4 c = ic_coins(L.key, g, s);
-#pragma unroll
-          for (int t = 0; t < 4; ++t) {
-            const uint32_t ed = (g << 2) + t;
-            if (ed >= ob && ed < oe && lane_of(c, t) < (ovt ? ovt : rec[t].y)) {
-              uint32_t u = rec[t].x;
-              if (ovt) {
-                u = __ldg(&L.G.edges[ed].x);
-                atomicAdd(&s_usrc, 1ull);
-              }
-              const uint32_t bit = 1u << (u & 31);
-              if (!(atomicOr(&bm[u >> 5], bit) & bit)) {
-                const uint32_t pos = atomicAdd(&s_qlen, 1u);
-                if (pos < L.qcap) q[pos] = u;
-                else s_overflow = 1;
-              }
+          const uint32_t g_last = (oe - 1) >> 2;
+          for (uint32_t g = (ob >> 2) + tid; g <= g_last; g += BIG_THREADS)
+            expand_group(g, ob, oe, ovt);
+        }
+        // the other lists through their concatenated groups: entry a holds
+        // group j when s_off[a] <= j < s_off[a + 1]; a thread's j only grows,
+        // so its entry cursor only moves forward
+        const uint32_t total = s_off[BIG_THREADS];
+        uint32_t a = 0;
+        for (uint32_t j = tid; j < total; j += BIG_THREADS) {
+          if (s_off[a + 1] <= j) {
+            uint32_t b = BIG_THREADS;
+            while (b - a > 1) {
+              const uint32_t mid = (a + b) >> 1;
+              if (s_off[mid] <= j) a = mid;
+              else b = mid;
             }
           }
+          const uint32_t ob = s_beg[a];
+          expand_group((ob >> 2) + (j - s_off[a]), ob, s_end[a], s_vt[a]);
         }
         __syncthreads();
       }

@@ -33,6 +33,10 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
   return m;
 }
 
+// In-lists of at least this many 4-edge groups are swept by a whole warp (or
+// CTA) at a time instead of sharing it with other lists.
+constexpr uint32_t kLongGroups = 64;
+
 struct WarpCtx {
   uint32_t *bm;  // visited bitmap, ceil(n/32) words
   uint32_t *q;   // queue, qcap entries
@@ -103,6 +107,50 @@ __device__ __forceinline__ SetOutcome ic_plain_set(const DevGraph &G, Key key, u
   unsigned long long set_exp = 0, set_edges = 0, warp_edges = 0;
   uint32_t set_uedges = 0, set_usrc = 0;  // a set's edges are fewer than m < 2^32
 
+  // Appends this lane's newly reached vertices of one 4-edge group to the
+  // queue (warp-wide, in lane order per edge slot); on queue overflow the set
+  // is abandoned and the bits of vertices that will never be queued cleared.
+  auto append = [&](const bool isnew[4], const uint32_t nu[4]) {
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const uint32_t bal = __ballot_sync(FULL, isnew[t]);
+      if (bal == 0) continue;
+      const uint32_t cnt = __popc(bal);
+      if (overflow || qlen + cnt > W.qcap) {
+        if (isnew[t]) W.bm[nu[t] >> 5] = 0u;
+        overflow = true;
+        continue;
+      }
+      if (isnew[t]) W.q[qlen + __popc(bal & lanemask_lt())] = nu[t];
+      qlen += cnt;
+    }
+  };
+  // Draws the coins of group g of the in-list [ob, oe) (uniform threshold
+  // ovt, or 0: each record's own), marks the live sources in the bitmap and
+  // reports which were not yet there.
+  auto expand_group = [&](uint32_t g, uint32_t ob, uint32_t oe, uint32_t ovt, bool isnew[4],
+                          uint32_t nu[4]) {
+    uint2 rec[4] = {};
+    if (!ovt) load_group(G.edges, g, rec);
+    const u32x4 c = ic_coins(key, g, s);
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const uint32_t e = (g << 2) + t;
+      const bool live = e >= ob && e < oe && lane_of(c, t) < (ovt ? ovt : rec[t].y);
+      isnew[t] = false;
+      nu[t] = rec[t].x;
+      if (live) {
+        if (ovt) {
+          nu[t] = __ldg(&G.edges[e].x);
+          ++set_usrc;
+        }
+        const uint32_t bit = 1u << (nu[t] & 31);
+        const uint32_t old = atomicOr(&W.bm[nu[t] >> 5], bit);
+        isnew[t] = !(old & bit);
+      }
+    }
+  };
+
   while (head < qlen && !overflow) {
     const uint32_t take = min(32u, qlen - head);
     uint32_t beg = 0, end = 0, ng = 0, vt = 0;
@@ -116,69 +164,51 @@ __device__ __forceinline__ SetOutcome ic_plain_set(const DevGraph &G, Key key, u
       if (vt) set_uedges += end - beg;
     }
     set_exp += (lane == 0) ? take : 0;
-    const uint32_t incl = warp_incl_scan(ng);
-    const uint32_t total = __shfl_sync(FULL, incl, 31);
-    warp_edges += (unsigned long long)total * 4;
+    {
+      const uint32_t all = warp_incl_scan(ng);
+      warp_edges += (unsigned long long)__shfl_sync(FULL, all, 31) * 4;
+    }
     if (work_cap && warp_edges > work_cap) {
       // too much edge work for one warp: leave the set to a whole CTA
       overflow = big = true;
       break;
     }
+    // Long in-lists (hubs) are swept by the whole warp, one list at a time:
+    // lane j takes groups j, j + 32, ... of the list, with no owner search.
+    uint32_t longs = __ballot_sync(FULL, ng >= kLongGroups);
+    while (longs && !overflow) {
+      const uint32_t L = __ffs(longs) - 1;
+      longs &= longs - 1;
+      const uint32_t lb = __shfl_sync(FULL, beg, L), le = __shfl_sync(FULL, end, L);
+      const uint32_t lvt = __shfl_sync(FULL, vt, L);
+      const uint32_t g_last = (le - 1) >> 2;
+      for (uint32_t base = lb >> 2; base <= g_last && !overflow; base += 32) {
+        const uint32_t g = base + lane;
+        uint32_t nu[4] = {0, 0, 0, 0};
+        bool isnew[4] = {false, false, false, false};
+        if (g <= g_last) expand_group(g, lb, le, lvt, isnew, nu);
+        // live edges are rare on hub lists: one vote skips the four ballots
+        if (__any_sync(FULL, isnew[0] || isnew[1] || isnew[2] || isnew[3])) append(isnew, nu);
+        __syncwarp();
+      }
+    }
+    // The shorter lists share the warp through their concatenated groups:
+    // group j belongs to the lane whose scanned range holds it.
+    const uint32_t ngs = ng >= kLongGroups ? 0u : ng;
+    const uint32_t incl = warp_incl_scan(ngs);
+    const uint32_t total = __shfl_sync(FULL, incl, 31);
     for (uint32_t base = 0; base < total && !overflow; base += 32) {
       const uint32_t j = base + lane;
       const bool valid = j < total;
       const uint32_t owner = warp_find_owner(incl, valid ? j : total - 1);
       const uint32_t ob = __shfl_sync(FULL, beg, owner);
       const uint32_t oe = __shfl_sync(FULL, end, owner);
-      const uint32_t oexcl = __shfl_sync(FULL, incl, owner) -
-                             __shfl_sync(FULL, ng, owner);
-      // the owner's uniform threshold (0: read each edge's record)
+      const uint32_t oexcl = __shfl_sync(FULL, incl, owner) - __shfl_sync(FULL, ngs, owner);
       const uint32_t ovt = __shfl_sync(FULL, vt, owner);
-      uint32_t nu[4];
-      bool isnew[4];
-      if (valid) {
-        const uint32_t g = (ob >> 2) + (j - oexcl);
-        uint2 rec[4] = {};
-        if (!ovt) load_group(G.edges, g, rec);
-        const u32x4 c = ic_coins(key, g, s);
-#pragma unroll
-        for (int t = 0; t < 4; ++t) {
-          const uint32_t e = (g << 2) + t;
-          const bool live = e >= ob && e < oe && lane_of(c, t) < (ovt ? ovt : rec[t].y);
-          isnew[t] = false;
-          nu[t] = rec[t].x;
-          if (live) {
-            if (ovt) {
-              nu[t] = __ldg(&G.edges[e].x);
-              ++set_usrc;
-            }
-            const uint32_t bit = 1u << (nu[t] & 31);
-            const uint32_t old = atomicOr(&W.bm[nu[t] >> 5], bit);
-            isnew[t] = !(old & bit);
-          }
-        }
-      } else {
-#pragma unroll
-        for (int t = 0; t < 4; ++t) {
-          isnew[t] = false;
-          nu[t] = 0;
-        }
-      }
-#pragma unroll
-      for (int t = 0; t < 4; ++t) {
-        const uint32_t bal = __ballot_sync(FULL, isnew[t]);
-        if (bal == 0) continue;
-        const uint32_t cnt = __popc(bal);
-        if (overflow || qlen + cnt > W.qcap) {
-          // Abandon the set: clear the bits of vertices that will never
-          // reach the queue (queued ones are cleared by store_set).
-          if (isnew[t]) W.bm[nu[t] >> 5] = 0u;
-          overflow = true;
-          continue;
-        }
-        if (isnew[t]) W.q[qlen + __popc(bal & lanemask_lt())] = nu[t];
-        qlen += cnt;
-      }
+      uint32_t nu[4] = {0, 0, 0, 0};
+      bool isnew[4] = {false, false, false, false};
+      if (valid) expand_group((ob >> 2) + (j - oexcl), ob, oe, ovt, isnew, nu);
+      append(isnew, nu);
       __syncwarp();
     }
     head += take;

@@ -211,6 +211,14 @@ class Context:
     def sync(self) -> None:
         check(lib.rip_sync(self.h), "rip_sync", self.h)
 
+    def coin_rate(self) -> float:
+        """Measured coins per second of the IC coin function alone
+        (``rip_coin_rate``): the ceiling of the samplers on uniform-threshold
+        graphs."""
+        r = ctypes.c_double()
+        check(lib.rip_coin_rate(self.h, ctypes.byref(r)), "rip_coin_rate", self.h)
+        return r.value
+
     def memory(self) -> Tuple[int, int]:
         used, budget = ctypes.c_size_t(), ctypes.c_size_t()
         check(lib.rip_ctx_memory(self.h, ctypes.byref(used), ctypes.byref(budget)),
