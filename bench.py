@@ -476,7 +476,7 @@ def main():
     rb._lib.check(rb._lib.lib.rip_ctx_stream(ctx.h, ctypes.byref(sp)), "rip_ctx_stream")
     stream = torch.cuda.ExternalStream(sp.value, device=torch.device("cuda", local))
     dg = rb.DeviceGraph(ctx, g, w["model"])
-    tune = dg.autotune(seed=1, pilot=2048) if w["model"] == "IC" else None  # setup, untimed
+    tune = dg.autotune(seed=1, pilot=32768) if w["model"] == "IC" else None  # setup, untimed
     pool = rb.Pool(dg)
     seed_base = replica_seed(rank, 0)
 

@@ -189,21 +189,28 @@ int rip_pool_configure(rip_pool *p, uint32_t colors, uint32_t slots,
  * these values. */
 int rip_pool_work_caps(rip_pool *p, uint64_t plain_cap, uint64_t fused_cap);
 
-/* Per-graph sampler autotuner.  Times `pilot` sets (0 = 2048) of `seed` on a
- * scratch pool under each of RIP_TUNE_CANDIDATES IC configurations (after a
- * warm-up run, the faster of two timed runs):
+/* Per-graph sampler autotuner.  Times sets of `seed` on a scratch pool under
+ * each of RIP_TUNE_CANDIDATES IC configurations (after a warm-up run, the
+ * faster of two timed runs): every candidate on the first min(pilot, 2048)
+ * sets, then the candidates within twice the best of that screen on all
+ * `pilot` sets (0 = 2048; large graphs want tens of thousands, so that the
+ * heavy sets fill the GPU as they do at full size):
  *   0 plain (one set per warp), heavy sets past 2^18 in-edges -> grid-wide BFS
  *   1 plain, heavy past 2^14 in-edges -> grid-wide BFS
  *   2 plain, heavy past 2^18 -> one CTA per set
  *   3/4/5 fused 64/128/256 colours, batches past 2^23 -> heavy path
  *   6/7 as 0/2 with the one-set-per-warp kernel capped at 48 registers
  *       (40 resident warps per SM instead of 32)
- * writes the wall times to ms[] (may be null) and the fastest to *choice, and
+ *   8/9 as 2 with 512- / 256-thread CTAs for the heavy sets (2 / 4 sets
+ *       growing per SM instead of 1: the block-shape axis; candidates 0-2
+ *       use 1024-thread CTAs, 6-7 512-thread ones)
+ * writes the wall times to ms[] (may be null; a candidate dropped after the
+ * screen keeps its screen time) and the fastest to *choice, and
  * keeps it for the graph: pools created afterwards start from it and
  * RIP_SAMPLER_AUTO runs it.  Untuned graphs run configuration 0 for AUTO.  LT
  * graphs have one sampler (choice 0).  Sets never depend on the choice.  No
  * reference counterpart (the reference fixes its GPU colour width). */
-#define RIP_TUNE_CANDIDATES 8
+#define RIP_TUNE_CANDIDATES 10
 int rip_graph_autotune(rip_graph *g, uint64_t seed, uint32_t pilot, double *ms, int *choice);
 
 /* Per-vertex uniform IC thresholds.  When every in-edge of a vertex has the
@@ -240,6 +247,12 @@ int rip_pool_plain_occupancy(rip_pool *p, int blocks_per_sm);
  * tuned value.  Results do not depend on it.  No reference counterpart (the reference's GPU BFS,
  * include/ripples/gpu/bfs.h:1338-1680, has one colour-batched path). */
 int rip_pool_heavy_batch(rip_pool *p, uint32_t min_sets);
+
+/* Block shape of the one-CTA-per-set kernel for heavy IC sets: 256, 512 or
+ * 1024 threads (default 512; an autotuned graph's pools start from its tuned
+ * value).  Smaller CTAs grow more sets per SM at once, each with fewer
+ * threads.  Results do not depend on it.  No reference counterpart. */
+int rip_pool_heavy_block(rip_pool *p, uint32_t threads);
 
 /* Reference-heap selection (RIP_TIE_REF_HEAP): after each pick the host
  * fetches the current counts of the heap items keyed at least a threshold,

@@ -52,6 +52,82 @@ constexpr int model_of() {
   return std::is_same<std::decay_t<Tag>, linear_threshold_tag>::value ? RIP_MODEL_LT
                                                                       : RIP_MODEL_IC;
 }
+
+// Records that carry GenerateRRRSetsRecord::WalkIterations
+// (include/ripples/generate_rrr_sets_record.h:69-91) get one iteration entry
+// per generate() call; other record types are left alone.
+template <typename R, typename = void>
+struct has_walk_iterations : std::false_type {};
+template <typename R>
+struct has_walk_iterations<R, std::void_t<decltype(std::declval<R &>().WalkIterations)>>
+    : std::true_type {};
+
+template <typename R>
+void record_walk(R &rec, uint64_t sets, double total_ms, double kernel_ms, double d2h_ms,
+                 double post_ms) {
+  if constexpr (has_walk_iterations<R>::value) {
+    using Iter = typename decltype(rec.WalkIterations)::value_type;
+    using Gpu = typename decltype(std::declval<Iter &>().GPUWalks)::value_type;
+    using ms = std::chrono::duration<double, std::milli>;
+    using ns = std::chrono::nanoseconds;
+    Iter it;
+    it.NumSets = sets;
+    it.Total = std::chrono::duration_cast<decltype(it.Total)>(ms(total_ms));
+    Gpu g;
+    g.NumSets = sets;
+    g.Total = std::chrono::duration_cast<decltype(g.Total)>(ms(total_ms));
+    g.Kernel = std::chrono::duration_cast<ns>(ms(kernel_ms));
+    g.D2H = std::chrono::duration_cast<ns>(ms(d2h_ms));
+    g.Post = std::chrono::duration_cast<ns>(ms(post_ms));
+    it.GPUWalks.push_back(g);
+    rec.WalkIterations.push_back(std::move(it));
+  }
+}
+
+// One device context per (host thread, device) for FindMostInfluentialSet on
+// host-held sets: an edgeless graph of the right vertex count and a pool the
+// sets are imported into, kept between calls so a martingale loop driven by
+// the reference pays the set-up once.
+struct SelectionContext {
+  rip_ctx *ctx = nullptr;
+  rip_graph *graph = nullptr;
+  rip_pool *pool = nullptr;
+  int device = -1;
+  uint32_t n = 0;
+  ~SelectionContext() {
+    if (ctx) rip_ctx_destroy(ctx);  // frees the pool and the graph too
+  }
+  void prepare(int dev, uint32_t nodes) {
+    if (ctx && dev != device) {
+      rip_ctx_destroy(ctx);
+      ctx = nullptr;
+    }
+    if (!ctx) {
+      check(rip_ctx_create(dev, 0, &ctx), nullptr, "rip_ctx_create");
+      device = dev;
+      graph = nullptr;
+      pool = nullptr;
+    }
+    if (graph && n != nodes) {
+      check(rip_graph_destroy(graph), ctx, "rip_graph_destroy");  // its pool goes too
+      graph = nullptr;
+      pool = nullptr;
+    }
+    if (!graph) {
+      std::vector<uint64_t> index((size_t)nodes + 1, 0);
+      check(rip_graph_upload(ctx, index.data(), nullptr, nullptr, nodes, 0, RIP_MODEL_IC,
+                             &graph),
+            ctx, "rip_graph_upload");
+      n = nodes;
+    }
+    if (!pool) check(rip_pool_create(ctx, graph, &pool), ctx, "rip_pool_create");
+    check(rip_pool_clear(pool), ctx, "rip_pool_clear");
+  }
+};
+inline SelectionContext &selection_context() {
+  thread_local SelectionContext sc;
+  return sc;
+}
 }  // namespace b200_detail
 
 // Owns a device context, the uploaded backward CSR and a device RRR pool.
@@ -81,22 +157,37 @@ class B200RRRGenerator {
     if (ctx_) rip_ctx_destroy(ctx_);  // frees the pool and the graph too
   }
 
-  // Fills [begin, end) -- empty sets the caller inserted -- with new sets.
+  // Fills [begin, end) -- empty sets the caller inserted -- with new sets, and
+  // adds one WalkIterations entry to the record (one GPU walk: sampling
+  // kernels, the copy back, filling the caller's sets).
   template <typename ItrTy, typename RecordTy>
-  void generate(ItrTy begin, ItrTy end, RecordTy &) {
+  void generate(ItrTy begin, ItrTy end, RecordTy &record) {
+    using clk = std::chrono::steady_clock;
+    const auto t0 = clk::now();
     const uint64_t count = std::distance(begin, end);
     uint64_t first = 0;
+    double k0 = 0, k1 = 0, sel = 0;
+    uint64_t launches = 0;
     b200_detail::check(rip_pool_info(pool_, &first, nullptr), ctx_, "rip_pool_info");
+    b200_detail::check(rip_pool_timing(pool_, &k0, &launches, &sel), ctx_, "rip_pool_timing");
     b200_detail::check(rip_sample(pool_, seed_, count, sampler_), ctx_, "rip_sample");
+    b200_detail::check(rip_sync(ctx_), ctx_, "rip_sync");
+    const auto t1 = clk::now();
     std::vector<uint64_t> off(count + 1);
     b200_detail::check(rip_pool_export(pool_, first, count, off.data(), nullptr), ctx_,
                        "rip_pool_export");
     std::vector<uint32_t> vtx(off[count]);
     b200_detail::check(rip_pool_export(pool_, first, count, off.data(), vtx.data()), ctx_,
                        "rip_pool_export");
+    const auto t2 = clk::now();
     uint64_t i = 0;
     for (ItrTy it = begin; it != end; ++it, ++i)
       it->assign(vtx.begin() + off[i], vtx.begin() + off[i + 1]);
+    const auto t3 = clk::now();
+    b200_detail::check(rip_pool_timing(pool_, &k1, &launches, &sel), ctx_, "rip_pool_timing");
+    using ms = std::chrono::duration<double, std::milli>;
+    b200_detail::record_walk(record, count, ms(t3 - t0).count(), k1 - k0,
+                             ms(t2 - t1).count(), ms(t3 - t2).count());
   }
 
   bool isGpuEnabled() const { return true; }
@@ -121,27 +212,22 @@ void GenerateRRRSets(const GraphTy &, B200RRRGenerator<GraphTy> &gen, ItrTy begi
   gen.generate(begin, end, record);
 }
 
-// Seed selection on the GPU over the sets in [rrr_begin, rrr_end): they are
-// copied to a temporary device pool (the library's own pools select in place
-// with rip_select).  Sets are not reordered.
+// Seed selection on the GPU over the sets in [rrr_begin, rrr_end), with the
+// reference CPU heap's tie-break: the sets are imported into a device pool
+// that is kept (with its context) per host thread and device between calls,
+// and are not reordered.  The record gets one Counting entry (the device
+// selection: counting, heap, picks and count updates) and one Pivoting entry
+// of zero (no partitioning), as the sequential reference pushes one of each
+// (include/ripples/find_most_influential.h:169-172).  enableGPU and
+// CFG.seed_select_max_workers / seed_select_max_gpu_workers are accepted for
+// the reference's signature; selection always runs on the device.
 template <typename GraphTy, typename ConfTy, typename RRRsetsItr>
 std::pair<double, std::vector<typename GraphTy::vertex_type>> FindMostInfluentialSet(
     const GraphTy &G, const ConfTy &CFG, RRRsetsItr rrr_begin, RRRsetsItr rrr_end,
-    FindMostInfluentialSetRecord &, bool, b200_tag &&, int device = 0) {
-  rip_ctx *ctx = nullptr;
-  b200_detail::check(rip_ctx_create(device, 0, &ctx), nullptr, "rip_ctx_create");
-  struct Guard {
-    rip_ctx *c;
-    ~Guard() { rip_ctx_destroy(c); }
-  } guard{ctx};
-  const uint32_t n = (uint32_t)G.num_nodes();
-  std::vector<uint64_t> index(n + 1, 0);
-  rip_graph *g = nullptr;
-  b200_detail::check(rip_graph_upload(ctx, index.data(), nullptr, nullptr, n, 0,
-                                      RIP_MODEL_IC, &g),
-                     ctx, "rip_graph_upload");
-  rip_pool *p = nullptr;
-  b200_detail::check(rip_pool_create(ctx, g, &p), ctx, "rip_pool_create");
+    FindMostInfluentialSetRecord &record, bool, b200_tag &&, int device = 0) {
+  using clk = std::chrono::steady_clock;
+  b200_detail::SelectionContext &sc = b200_detail::selection_context();
+  sc.prepare(device, (uint32_t)G.num_nodes());
   const uint64_t S = std::distance(rrr_begin, rrr_end);
   std::vector<uint64_t> off(S + 1, 0);
   std::vector<uint32_t> vtx;
@@ -150,14 +236,22 @@ std::pair<double, std::vector<typename GraphTy::vertex_type>> FindMostInfluentia
     off[i + 1] = off[i] + it->size();
     vtx.insert(vtx.end(), it->begin(), it->end());
   }
-  b200_detail::check(rip_pool_import(p, off.data(), vtx.empty() ? nullptr : vtx.data(), S),
-                     ctx, "rip_pool_import");
+  b200_detail::check(
+      rip_pool_import(sc.pool, off.data(), vtx.empty() ? nullptr : vtx.data(), S), sc.ctx,
+      "rip_pool_import");
   const uint32_t k = (uint32_t)CFG.k;
   std::vector<uint32_t> seeds(k ? k : 1);
   uint32_t ns = 0;
   double f = 0;
-  b200_detail::check(rip_select(p, S, k, RIP_TIE_REF_HEAP, seeds.data(), nullptr, &ns, &f),
-                     ctx, "rip_select");
+  const auto t0 = clk::now();
+  b200_detail::check(
+      rip_select(sc.pool, S, k, RIP_TIE_REF_HEAP, seeds.data(), nullptr, &ns, &f), sc.ctx,
+      "rip_select");
+  using ms = std::chrono::duration<double, std::milli>;
+  record.Counting.push_back(
+      std::chrono::duration_cast<typename FindMostInfluentialSetRecord::ex_time_ms>(
+          ms(clk::now() - t0)));
+  record.Pivoting.push_back(typename FindMostInfluentialSetRecord::ex_time_ms(0));
   std::vector<typename GraphTy::vertex_type> result(seeds.begin(), seeds.begin() + ns);
   return {f, result};
 }

@@ -144,6 +144,7 @@ SIGNATURES = {
     "rip_pool_work_caps": (I32, [P, U64, U64]),
     "rip_pool_select_guess": (I32, [P, U32]),
     "rip_pool_heavy_batch": (I32, [P, U32]),
+    "rip_pool_heavy_block": (I32, [P, U32]),
     "rip_pool_plain_occupancy": (I32, [P, I32]),
     "rip_graph_autotune": (I32, [P, U64, U32, P, ctypes.POINTER(I32)]),
     "rip_select": (I32, [P, U64, U32, I32, P, P, ctypes.POINTER(U32), ctypes.POINTER(DBL)]),

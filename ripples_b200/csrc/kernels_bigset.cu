@@ -4,13 +4,14 @@
 // many hubs and read millions of in-edge records each (on an R-MAT graph with
 // 2^20 vertices 1% of the sets carry ~40% of the edge work).  One warp per set
 // (ic_plain_kernel) or one warp per frontier entry (ic_fused_kernel) walks a
-// hub's in-list alone, so those sets set the kernel's length.  Here one
-// 1024-thread CTA grows one such set: level by level, the level's entries are
-// taken 1024 at a time, a block scan turns their 4-edge group counts into
-// offsets, and all 32 warps stride over the concatenated groups (each thread
-// finds its entry by binary search in shared memory) -- a hub's in-list is
-// split over the whole CTA.  Levels are separated by __syncthreads only.
-// Coins are the same (set, edge)-keyed Philox draws as every other sampler.
+// hub's in-list alone, so those sets set the kernel's length.  Here one CTA
+// grows one such set: level by level, the level's entries are taken a CTA's
+// width at a time; in-lists of at least that many 4-edge groups (hubs) are
+// swept by all threads one list at a time, and the others through their
+// concatenated groups (a block scan turns group counts into offsets; each
+// thread finds its entry with a forward-only cursor in shared memory).
+// Levels are separated by __syncthreads only.  Coins are the same
+// (set, edge)-keyed Philox draws as every other sampler.
 #include "device.cuh"
 #include "launch.h"
 
@@ -18,15 +19,17 @@ namespace rip {
 
 namespace {
 
-constexpr int BIG_THREADS = 1024;
-constexpr int BIG_WARPS = BIG_THREADS / 32;
-// In-lists of at least this many 4-edge groups are swept by the whole CTA, one
-// list at a time.
-constexpr uint32_t kLongCTA = 1024;
+// Block shapes: 256, 512 or 1024 threads (at 64 registers a thread: 4, 2 or
+// 1 CTA per SM, each growing its own set -- smaller CTAs let one set's barrier
+// waits overlap another's work; the autotuner picks per graph).  In-lists of
+// at least BIG_THREADS 4-edge groups are swept by the whole CTA, one list at
+// a time.
 
 // Exclusive block scan of one u32 per thread; returns the exclusive value and
 // writes the block total to *total.  Uses `warp_tot` (BIG_WARPS entries).
+template <int BIG_THREADS>
 __device__ uint32_t big_block_scan(uint32_t x, uint32_t *warp_tot, uint32_t *total) {
+  constexpr int BIG_WARPS = BIG_THREADS / 32;
   const uint32_t lane = lane_id(), wid = threadIdx.x >> 5;
   const uint32_t incl = warp_incl_scan(x);
   if (lane == 31) warp_tot[wid] = incl;
@@ -43,8 +46,11 @@ __device__ uint32_t big_block_scan(uint32_t x, uint32_t *warp_tot, uint32_t *tot
   return r;
 }
 
-__global__ void __launch_bounds__(BIG_THREADS)
+template <int BIG_THREADS>
+__global__ void __launch_bounds__(BIG_THREADS, 1024 / BIG_THREADS)
 ic_bigset_kernel(BigLaunch L) {
+  constexpr int BIG_WARPS = BIG_THREADS / 32;
+  constexpr uint32_t kLongCTA = BIG_THREADS;
   __shared__ uint32_t s_off[BIG_THREADS + 1];  // exclusive group offsets of the chunk
   __shared__ uint32_t s_beg[BIG_THREADS], s_end[BIG_THREADS], s_vt[BIG_THREADS];
   __shared__ uint32_t s_warp[BIG_WARPS];
@@ -118,7 +124,7 @@ ic_bigset_kernel(BigLaunch L) {
         s_vt[tid] = vt;
         const uint32_t ng = group_count(beg, end);
         const bool lng = ng >= kLongCTA;
-        s_off[tid] = big_block_scan(lng ? 0u : ng, s_warp, &s_total);  // syncs
+        s_off[tid] = big_block_scan<BIG_THREADS>(lng ? 0u : ng, s_warp, &s_total);  // syncs
         if (tid == 0) s_off[BIG_THREADS] = s_total;
         if (lng) s_long[atomicAdd(&s_nlong, 1u)] = tid;
         __syncthreads();
@@ -211,7 +217,12 @@ ic_bigset_kernel(BigLaunch L) {
 
 void launch_ic_bigset(const BigLaunch &L, cudaStream_t stream) {
   count_launches(1);
-  ic_bigset_kernel<<<L.blocks, BIG_THREADS, 0, stream>>>(L);
+  if (L.threads == 256)
+    ic_bigset_kernel<256><<<L.blocks, 256, 0, stream>>>(L);
+  else if (L.threads == 512)
+    ic_bigset_kernel<512><<<L.blocks, 512, 0, stream>>>(L);
+  else
+    ic_bigset_kernel<1024><<<L.blocks, 1024, 0, stream>>>(L);
 }
 
 }  // namespace rip

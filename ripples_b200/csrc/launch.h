@@ -128,6 +128,7 @@ struct BigLaunch {
   FailList F{};
   Stats st{};
   int blocks = 0;
+  int threads = 1024;             // block shape: 256, 512 or 1024
 };
 void launch_ic_bigset(const BigLaunch &L, cudaStream_t stream);
 

@@ -36,6 +36,7 @@ extern "C" int rip_pool_create(rip_ctx *c, rip_graph *g, rip_pool **out) {
     p->cap_fused = g->tuned.cap_fused;
     p->giant_min = g->tuned.giant_min;
     p->plain_occupancy = g->tuned.plain_occupancy;
+    p->big_threads = g->tuned.big_threads;
   }
   c->pools.push_back(p);
   *out = p;
@@ -426,8 +427,9 @@ static int sample_big(rip_pool *p, uint64_t seed, uint64_t first,
     const size_t per = bm_words * 4 + (size_t)q * 4;
     size_t avail = c->budget > c->used ? c->budget - c->used : 0;
     avail += p->b_scratch.bytes;
-    return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)c->num_sms,
-                                                               (avail / 4) / per));
+    // one slot per resident CTA: 1024 / big_threads of them per SM
+    const uint64_t max_slots = (uint64_t)c->num_sms * (1024u / p->big_threads);
+    return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(max_slots, (avail / 4) / per));
   };
   TRY(ensure_big_scratch(p, slots_for(qcap), qcap));
   std::vector<uint32_t> ids = ids_in;
@@ -454,6 +456,7 @@ static int sample_big(rip_pool *p, uint64_t seed, uint64_t first,
     L.F = FailList{ptr<uint32_t>(p->b_ids) + ids.size(), &dm->fail_count, &dm->first_bad};
     L.st = Stats{dm->stats};
     L.blocks = (int)std::min<uint32_t>(p->b_slots, (uint32_t)ids.size());
+    L.threads = (int)p->big_threads;
     CK(c, cudaEventRecord(c->ev0, c->stream));
     launch_ic_bigset(L, c->stream);
     CK(c, cudaGetLastError());
@@ -670,16 +673,19 @@ extern "C" int rip_graph_autotune(rip_graph *g, uint64_t seed, uint32_t pilot, d
     uint64_t cap_plain, cap_fused;
     uint32_t giant_min;
     int occupancy;
+    uint32_t big_threads;
   };
   static const Cand cands[RIP_TUNE_CANDIDATES] = {
-      {RIP_SAMPLER_PLAIN, 64, 1ull << 18, 1ull << 23, 32, 0},
-      {RIP_SAMPLER_PLAIN, 64, 1ull << 14, 1ull << 23, 32, 0},
-      {RIP_SAMPLER_PLAIN, 64, 1ull << 18, 1ull << 23, 0, 0},
-      {RIP_SAMPLER_FUSED, 64, 1ull << 18, 1ull << 23, 32, 0},
-      {RIP_SAMPLER_FUSED, 128, 1ull << 18, 1ull << 23, 32, 0},
-      {RIP_SAMPLER_FUSED, 256, 1ull << 18, 1ull << 23, 32, 0},
-      {RIP_SAMPLER_PLAIN, 64, 1ull << 18, 1ull << 23, 32, 5},
-      {RIP_SAMPLER_PLAIN, 64, 1ull << 18, 1ull << 23, 0, 5},
+      {RIP_SAMPLER_PLAIN, 64, 1ull << 18, 1ull << 23, 32, 0, 1024},
+      {RIP_SAMPLER_PLAIN, 64, 1ull << 14, 1ull << 23, 32, 0, 1024},
+      {RIP_SAMPLER_PLAIN, 64, 1ull << 18, 1ull << 23, 0, 0, 1024},
+      {RIP_SAMPLER_FUSED, 64, 1ull << 18, 1ull << 23, 32, 0, 1024},
+      {RIP_SAMPLER_FUSED, 128, 1ull << 18, 1ull << 23, 32, 0, 1024},
+      {RIP_SAMPLER_FUSED, 256, 1ull << 18, 1ull << 23, 32, 0, 1024},
+      {RIP_SAMPLER_PLAIN, 64, 1ull << 18, 1ull << 23, 32, 5, 512},
+      {RIP_SAMPLER_PLAIN, 64, 1ull << 18, 1ull << 23, 0, 5, 512},
+      {RIP_SAMPLER_PLAIN, 64, 1ull << 18, 1ull << 23, 0, 0, 512},
+      {RIP_SAMPLER_PLAIN, 64, 1ull << 18, 1ull << 23, 0, 0, 256},
   };
   if (ms)
     for (int i = 0; i < RIP_TUNE_CANDIDATES; ++i) ms[i] = -1.0;
@@ -689,10 +695,14 @@ extern "C" int rip_graph_autotune(rip_graph *g, uint64_t seed, uint32_t pilot, d
     if (choice) *choice = 0;
     return RIP_OK;
   }
+  // Two phases: every candidate on a short screen of the pilot's first sets,
+  // then those within twice the best screen time on the whole pilot (on large
+  // graphs the heavy sets of a short run are too few to fill the GPU, which
+  // hides what the heavy-set paths cost at full size).  Each timing is the
+  // faster of two runs after a warm-up that sizes every scratch buffer.
   pilot = std::max<uint32_t>(pilot ? pilot : 2048, 64);
-  int best = 0;
-  double best_ms = 0;
-  for (int i = 0; i < RIP_TUNE_CANDIDATES; ++i) {
+  const uint32_t screen = std::min<uint32_t>(pilot, 2048);
+  auto time_cand = [&](int i, uint32_t sets, double *out) -> int {
     rip_pool *p = nullptr;
     TRY(rip_pool_create(c, g, &p));
     p->auto_sampler = cands[i].sampler;
@@ -701,22 +711,38 @@ extern "C" int rip_graph_autotune(rip_graph *g, uint64_t seed, uint32_t pilot, d
     p->cap_fused = cands[i].cap_fused;
     p->giant_min = cands[i].giant_min;
     p->plain_occupancy = cands[i].occupancy;
-    // a warm-up sizes every scratch buffer (heavy-set paths included); then
-    // the pilot runs twice on a cleared pool and the faster run counts
-    int rc = rip_sample(p, seed, pilot, RIP_SAMPLER_AUTO);
+    p->big_threads = cands[i].big_threads;
+    int rc = rip_sample(p, seed, sets, RIP_SAMPLER_AUTO);
     if (rc == RIP_OK) rc = rip_sync(c);
     double t = 1e300;
     for (int rep = 0; rep < 2 && rc == RIP_OK; ++rep) {
       rc = rip_pool_clear(p);
       const auto t0 = clk::now();
-      if (rc == RIP_OK) rc = rip_sample(p, seed, pilot, RIP_SAMPLER_AUTO);
+      if (rc == RIP_OK) rc = rip_sample(p, seed, sets, RIP_SAMPLER_AUTO);
       if (rc == RIP_OK) rc = rip_sync(c);
       t = std::min(t, ms_since(t0));
     }
     rip_pool_destroy(p);
-    if (rc != RIP_OK) return rc;
-    if (ms) ms[i] = t;
-    if (i == 0 || t < best_ms) {
+    *out = t;
+    return rc;
+  };
+  double t_screen[RIP_TUNE_CANDIDATES];
+  double screen_best = 1e300;
+  for (int i = 0; i < RIP_TUNE_CANDIDATES; ++i) {
+    TRY(time_cand(i, screen, &t_screen[i]));
+    screen_best = std::min(screen_best, t_screen[i]);
+    if (ms) ms[i] = t_screen[i];
+  }
+  int best = 0;
+  double best_ms = 1e300;
+  for (int i = 0; i < RIP_TUNE_CANDIDATES; ++i) {
+    double t = t_screen[i];
+    if (pilot > screen) {
+      if (t_screen[i] > 2.0 * screen_best) continue;  // out after the screen
+      TRY(time_cand(i, pilot, &t));
+      if (ms) ms[i] = t;
+    }
+    if (t < best_ms) {
       best = i;
       best_ms = t;
     }
@@ -728,6 +754,7 @@ extern "C" int rip_graph_autotune(rip_graph *g, uint64_t seed, uint32_t pilot, d
   g->tuned.cap_fused = cands[best].cap_fused;
   g->tuned.giant_min = cands[best].giant_min;
   g->tuned.plain_occupancy = cands[best].occupancy;
+  g->tuned.big_threads = cands[best].big_threads;
   if (choice) *choice = best;
   return RIP_OK;
 }
@@ -747,6 +774,13 @@ extern "C" int rip_pool_plain_occupancy(rip_pool *p, int blocks_per_sm) {
 extern "C" int rip_pool_heavy_batch(rip_pool *p, uint32_t min_sets) {
   if (!p) return RIP_ERR_INVALID;
   p->giant_min = min_sets;
+  return RIP_OK;
+}
+
+// Block shape of the CTA-per-set kernel for heavy IC sets.
+extern "C" int rip_pool_heavy_block(rip_pool *p, uint32_t threads) {
+  if (!p || (threads != 256 && threads != 512 && threads != 1024)) return RIP_ERR_INVALID;
+  p->big_threads = threads;
   return RIP_OK;
 }
 

@@ -322,9 +322,11 @@ class DeviceGraph:
         return idx, src[: self.m]
 
     TUNE_NAMES = ("plain, heavy>2^18 grid BFS", "plain, heavy>2^14 grid BFS",
-                  "plain, heavy>2^18 CTA per set", "fused 64", "fused 128", "fused 256",
-                  "plain 40 warps/SM, heavy>2^18 grid BFS",
-                  "plain 40 warps/SM, heavy>2^18 CTA per set")
+                  "plain, heavy>2^18 CTA per set, 1024-thread CTAs", "fused 64", "fused 128",
+                  "fused 256", "plain 40 warps/SM, heavy>2^18 grid BFS",
+                  "plain 40 warps/SM, heavy>2^18 CTA per set, 512-thread CTAs",
+                  "plain, heavy>2^18 CTA per set, 512-thread CTAs",
+                  "plain, heavy>2^18 CTA per set, 256-thread CTAs")
 
     def autotune(self, seed: int = 0, pilot: int = 0) -> dict:
         """Times each IC sampler configuration on a pilot of sets and keeps the
@@ -399,6 +401,11 @@ class Pool:
         """Heavy IC sets pending from which the grid-wide multi-colour BFS
         grows them (0 = one CTA per set)."""
         self._chk(lib.rip_pool_heavy_batch(self.h, min_sets), "rip_pool_heavy_batch")
+
+    def heavy_block(self, threads: int) -> None:
+        """Block shape (256/512/1024 threads) of the CTA-per-set kernel for
+        heavy IC sets."""
+        self._chk(lib.rip_pool_heavy_block(self.h, threads), "rip_pool_heavy_block")
 
     def select_guess(self, percent: int) -> None:
         """First-fetch threshold of reference-heap picks, % of the previous

@@ -5,10 +5,11 @@
 // Loads a reference-format binary graph with ripples::GraphBwd::load_binary,
 // then, through the adapter only:
 //   1. ripples::IMM(G, CFG, 1, gen, R, <model>_tag{}, b200_tag{})
-//   2. ripples::GenerateRRRSets(G, gen2, begin, end, R, <model>_tag{}, b200_tag{})
+//   2. ripples::GenerateRRRSets(G, gen2, begin, end, R2, <model>_tag{}, b200_tag{})
 //      on caller-inserted empty sets, then
-//      ripples::FindMostInfluentialSet(G, CFG, begin, end, R, true, b200_tag{})
-// and prints one JSON object with the results.
+//      ripples::FindMostInfluentialSet(G, CFG, begin, end, R2, true, b200_tag{})
+//      on all of them and again on the first half
+// and prints one JSON object with the results and the record's entries.
 //   usage: adapter_imm <graph.bin> <IC|LT> <k> <epsilon> <seed> <nsets>
 #include <cstdio>
 #include <cstdlib>
@@ -38,9 +39,14 @@ int run(const ripples::GraphBwd &G, int model, size_t k, double eps, uint64_t se
 
   ripples::B200RRRGenerator<ripples::GraphBwd> gen2(G, model, seed);
   ripples::RRRsets<ripples::GraphBwd> RR(nsets);
-  ripples::GenerateRRRSets(G, gen2, RR.begin(), RR.end(), R, Tag{}, ripples::b200_tag{});
-  auto S = ripples::FindMostInfluentialSet(G, CFG, RR.begin(), RR.end(), R, true,
+  ripples::IMMExecutionRecord R2;
+  ripples::GenerateRRRSets(G, gen2, RR.begin(), RR.end(), R2, Tag{}, ripples::b200_tag{});
+  auto S = ripples::FindMostInfluentialSet(G, CFG, RR.begin(), RR.end(), R2, true,
                                            ripples::b200_tag{});
+  // a second selection in the same process, on the first half of the sets:
+  // the adapter's cached device context is reused
+  auto S2 = ripples::FindMostInfluentialSet(G, CFG, RR.begin(), RR.begin() + nsets / 2, R2,
+                                            true, ripples::b200_tag{});
   uint64_t elems = 0;
   bool sorted = true;
   for (auto &s : RR) {
@@ -57,7 +63,14 @@ int run(const ripples::GraphBwd &G, int model, size_t k, double eps, uint64_t se
               RR.size(), (unsigned long long)elems, sorted ? "true" : "false", S.first);
   for (size_t i = 0; i < S.second.size(); ++i)
     std::printf("%s%u", i ? ", " : "", S.second[i]);
-  std::printf("]}\n");
+  std::printf("], \"half_f\": %.17g, \"half_seeds\": [", S2.first);
+  for (size_t i = 0; i < S2.second.size(); ++i)
+    std::printf("%s%u", i ? ", " : "", S2.second[i]);
+  std::printf("], \"counting\": %zu, \"pivoting\": %zu, \"walk_iterations\": %zu, "
+              "\"walk_sets\": %zu, \"gpu_walks\": %zu}\n",
+              R2.Counting.size(), R2.Pivoting.size(), R2.WalkIterations.size(),
+              R2.WalkIterations.empty() ? (size_t)0 : R2.WalkIterations[0].NumSets,
+              R2.WalkIterations.empty() ? (size_t)0 : R2.WalkIterations[0].GPUWalks.size());
   return 0;
 }
 

@@ -39,3 +39,10 @@ def test_adapter_through_reference_api(tmp_path, model):
     assert r["sets"] == nsets and r["elements"] == len(vtx) and r["sorted"]
     f, seeds, _, _ = O.select(g.n, off, vtx, k, 0)
     assert r["select_seeds"] == seeds.tolist() and r["f"] == f
+    half = nsets // 2
+    f2, seeds2, _, _ = O.select(g.n, off[:half + 1], vtx[:int(off[half])], k, 0)
+    assert r["half_seeds"] == seeds2.tolist() and r["half_f"] == f2
+    # the record: one walk iteration (one GPU walk) for the one GenerateRRRSets
+    # call, one Counting and one Pivoting entry per FindMostInfluentialSet
+    assert r["walk_iterations"] == 1 and r["walk_sets"] == nsets and r["gpu_walks"] == 1
+    assert r["counting"] == 2 and r["pivoting"] == 2

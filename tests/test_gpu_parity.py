@@ -468,3 +468,24 @@ def test_uniform_thresholds_only_where_they_pay(ctx):
     dg = rb.DeviceGraph(ctx, lt_graph(10), "LT")
     assert not dg.uniform_thresholds()
     dg.close()
+
+
+@pytest.mark.parametrize("threads", [256, 512, 1024])
+def test_cta_per_set_block_shapes_match_oracle(ctx, threads):
+    # R-MAT 2^16 with 16 draws per vertex: the largest in-lists pass 1024
+    # 4-edge groups, so every block shape sweeps some lists with the whole CTA
+    g = mixed_uniform_graph(scale=16, deg=16, seed=41)
+    assert np.diff(g.index).max() >= 4 * 1024
+    dg = rb.DeviceGraph(ctx, g, "IC")
+    p = rb.Pool(dg)
+    try:
+        p.work_caps(64, 1 << 23)  # nearly every set goes to the CTA-per-set kernel
+        p.heavy_batch(0)
+        p.heavy_block(threads)
+        p.sample(600, seed=23, sampler=rb.SAMPLER_PLAIN)
+        off, vtx = p.export()
+        ooff, ovtx, _ = oracle_sets(g, "IC", 23, 0, 600)
+        assert_same_sets(off, vtx, ooff, ovtx)
+    finally:
+        p.close()
+        dg.close()
