@@ -69,7 +69,13 @@ WORKLOADS = {
     # eps=0.13: full IMM with the autotuned sampler, plus each sampler
     # (one set per warp, fused 64/128/256 colours) on the same fixed set range
     "ic24_samplers": dict(name="samplers_ic_rmat24_deg32_wc", kind="p3", scale=24,
-                          draws=32 << 24, model="IC", k=100, eps=0.13),
+                          draws=32 << 24, model="IC", k=100, eps=0.13, weights="wc",
+                          sets=1 << 18),
+    # the serving workload's 2^24 IC graph (degree 16, p ~ U(0, 0.1)): a
+    # supercritical reverse BFS, sets large and overlapping
+    "ic24u_samplers": dict(name="samplers_ic_rmat24_deg16_u0.1", kind="p3", scale=24,
+                           draws=16 << 24, model="IC", k=100, eps=0.13,
+                           weights="uniform_0_0.1", sets=1 << 12),
     # forward Monte Carlo spread (rip_spread_ic) of the 50 vertices of largest
     # out-degree on R-MAT 2^20 (16*2^20 draws, IC p ~ U(0,0.1)), 20000
     # replicas a step; the reference's own simulator timed beside it
@@ -615,7 +621,7 @@ def main():
     achieved = alg_bytes / (kern_ms / 1e3) / 1e9 if kern_ms > 0 else None
     kernel = ("lt_walk_kernel" if w["model"] == "LT" else
               "ic_fused_kernel" if tune and tune["name"].startswith("fused") else
-              "ic_plain_kernel")
+              "ic_plain_kernel + ic_bigset_kernel (every IC sampler launch)")
     traffic = None
     prof = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(prof):
@@ -625,6 +631,15 @@ def main():
             # DRAM bytes per algorithmic byte from the ncu capture, applied to
             # this run's average launch
             traffic = tr["dram_bytes_per_alg_byte"] * alg_bytes / kern_n
+
+    coin_roofline = None
+    if w["model"] == "IC" and kern_ms > 0:
+        coin_peak = ctx.coin_rate()
+        coins = int(st_tot[5]) / (kern_ms / 1e3)
+        coin_roofline = {"bound": "coin arithmetic (Philox4x32-10, integer issue)",
+                         "kernel": kernel, "achieved": coins, "peak": coin_peak,
+                         "peak_kind": "measured (coin-only kernel, same run)",
+                         "unit": "coins/s", "frac": coins / coin_peak if coin_peak else None}
 
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -655,6 +670,11 @@ def main():
             # semantics, fused expansions counted per colour) over the
             # sampler kernels' time
             "traversed_edges_per_s": int(st_tot[5]) / (kern_ms / 1e3) if kern_ms > 0 else None,
+            # IC samplers draw one coin per in-edge of every member; on
+            # uniform-threshold graphs they read almost nothing else, so the
+            # ceiling is the coin function's own rate on this GPU, measured
+            # here by a coin-only kernel at full occupancy (rip_coin_rate)
+            "compute_roofline": coin_roofline,
             "cpu_baseline": base,
             "clocks": clk,
             "gpu_launches": launches,
@@ -698,10 +718,16 @@ def run_sampler_case(args, w, local):
     import ripples_b200 as rb
     torch.cuda.set_device(local)
     ctx = rb.Context(local)
-    if w.get("kind") == "p3" or w["name"].startswith("imm_ic_rmat24"):
-        # weighted-cascade R-MAT, 32 draws per vertex
+    if w.get("scale") == 24:
+        # the 2^24 graphs, built on the device (smaller with --case-scale, same
+        # draws per vertex)
         scale = args.case_scale or w["scale"]
-        dg = rb.DeviceGraph.rmat_on_device(ctx, scale, 32 << scale, "IC", rb.WEIGHTS_WC, seed=0)
+        draws = w["draws"] >> (w["scale"] - scale)
+        if w["weights"] == "wc":
+            dg = rb.DeviceGraph.rmat_on_device(ctx, scale, draws, "IC", rb.WEIGHTS_WC, seed=0)
+        else:
+            dg = rb.DeviceGraph.rmat_on_device(ctx, scale, draws, "IC", rb.WEIGHTS_UNIFORM,
+                                               seed=0, weight_seed=1, lo=0.0, hi=0.1)
     else:
         dg = rb.DeviceGraph(ctx, build_graph(w), w["model"])
     pool = rb.Pool(dg)
@@ -871,6 +897,10 @@ def run_batch(args, w, world, rank, local):
 
 
 def run_p3(args, w, world, rank, local):
+    """Each IC sampler on one fixed range of sets of a 2^24-vertex R-MAT graph
+    (identical sets whatever the sampler): one set per warp with heavy sets
+    one CTA each, the same with heavy sets grown by the grid-wide multi-colour
+    BFS, and the fused multi-colour BFS at 64/128/256 colours."""
     import numpy as np
     import torch
     import ripples_b200 as rb
@@ -879,19 +909,28 @@ def run_p3(args, w, world, rank, local):
     torch.cuda.set_device(local)
     ctx = rb.Context(local)
     t0 = time.perf_counter()
-    dg = rb.DeviceGraph.rmat_on_device(ctx, w["scale"], w["draws"], "IC", rb.WEIGHTS_WC, seed=0)
+    scale = args.case_scale or w["scale"]
+    draws = w["draws"] >> (w["scale"] - scale)
+    if w["weights"] == "wc":
+        dg = rb.DeviceGraph.rmat_on_device(ctx, scale, draws, "IC", rb.WEIGHTS_WC, seed=0)
+    else:
+        dg = rb.DeviceGraph.rmat_on_device(ctx, scale, draws, "IC", rb.WEIGHTS_UNIFORM, seed=0,
+                                           weight_seed=1, lo=0.0, hi=0.1)
     t_build = time.perf_counter() - t0
-    tune = dg.autotune(seed=1, pilot=8192)
     peak, peak_kind = measured_peaks()
-    # each sampler on sets [0, count) of one seed (identical sets)
-    count = 1 << 18
+    count = w["sets"]
     samplers = {}
-    for name, smp, colors in [("plain", rb.SAMPLER_PLAIN, 64), ("fused64", rb.SAMPLER_FUSED, 64),
-                              ("fused128", rb.SAMPLER_FUSED, 128),
-                              ("fused256", rb.SAMPLER_FUSED, 256)]:
+    clocks = ClockSampler(local)
+    clocks.start()
+    for name, smp, colors, heavy in [("plain, heavy sets one CTA each", rb.SAMPLER_PLAIN, 64, 0),
+                                     ("plain, heavy sets grid-wide BFS", rb.SAMPLER_PLAIN, 64, 32),
+                                     ("fused64", rb.SAMPLER_FUSED, 64, 32),
+                                     ("fused128", rb.SAMPLER_FUSED, 128, 32),
+                                     ("fused256", rb.SAMPLER_FUSED, 256, 32)]:
         p = rb.Pool(dg)
         p.configure(colors=colors)
-        p.sample(4096, seed=7, sampler=smp)  # warm-up: scratch, pool sizing
+        p.heavy_batch(heavy)
+        p.sample(max(256, count // 16), seed=7, sampler=smp)  # warm-up: scratch, pool sizing
         p.clear()
         ctx.sync()
         t1 = time.perf_counter()
@@ -908,39 +947,21 @@ def run_p3(args, w, world, rank, local):
                           "traversed_edges_per_s": int(st[5]) / (km / 1e3) if km else None,
                           "mean_set": int(st[3]) / count}
         p.close()
-    # full IMM runs, autotuned sampler
-    pool = rb.Pool(dg)
-    for i in range(args.warmup):
-        pool.clear()
-        pool.imm(w["k"], w["eps"], seed=100 + i, tiebreak=rb.TIE_LOWEST_ID)
-    clocks = ClockSampler(local)
-    clocks.start()
-    torch.cuda.synchronize()
-    t1 = time.perf_counter()
-    sets, thetas = 0, []
-    for s in range(args.steps):
-        pool.clear()
-        _, rec = pool.imm(w["k"], w["eps"], seed=s, tiebreak=rb.TIE_LOWEST_ID)
-        sets += rec.total_sets
-        thetas.append(int(rec.theta))
-    torch.cuda.synchronize()
-    dt = time.perf_counter() - t1
     clk = clocks.stop()
-    line = {"metric": "RRR sets/s (full IMM)", "value": sets / dt, "unit": "sets/s",
-            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True,
-            "scaling": "replicas only", "vs_baseline": None, "dtype": "u32",
-            "data": "synthetic R-MAT graph (seed 0), weighted cascade",
-            "config": {"workload": w["name"], "n": dg.n, "m": dg.m, "k": w["k"],
-                       "epsilon": w["eps"], "theta": thetas[0] if thetas else None,
-                       "tiebreak": "lowest id (device picks)"},
-            "autotune": tune, "graph_build_s": t_build,
-            "samplers_on_2^18_sets": samplers,
-            "fused_best_vs_plain": max(samplers[k]["sets_per_s"] for k in samplers
-                                       if k != "plain") / samplers["plain"]["sets_per_s"],
+    plain = samplers["plain, heavy sets one CTA each"]["sets_per_s"]
+    line = {"metric": "RRR sets/s (one sampler launch series)", "value": plain,
+            "unit": "sets/s", "n_gpus": 1, "steps": 1, "warmup": 1,
+            "higher_is_better": True, "scaling": "replicas only", "vs_baseline": None,
+            "dtype": "u32",
+            "data": "synthetic R-MAT graph (seed 0), " + ("weighted cascade" if w["weights"] == "wc"
+                                                          else "IC p ~ U(0, 0.1) (seed 1)"),
+            "config": {"workload": w["name"], "n": dg.n, "m": dg.m, "sets": count,
+                       "branching": dg.branching,
+                       "uniform_thresholds": bool(dg.uniform_thresholds())},
+            "graph_build_s": t_build, "samplers": samplers,
+            "best_vs_plain": {k: v["sets_per_s"] / plain for k, v in samplers.items()},
             "clocks": clk}
     print(json.dumps(line))
-    pool.close()
     ctx.close()
     return 0
 

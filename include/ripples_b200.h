@@ -130,6 +130,23 @@ int rip_graph_from_keys(rip_ctx *ctx, const uint64_t *d_keys, uint64_t m,
                         uint32_t n, int weights, uint64_t weight_seed, double lo,
                         double hi, int model, rip_graph **out);
 
+/* Builds a packed graph on the device from a host edge list -- m directed
+ * edges src[e] -> dst[e] with weight w[e], as a TSV file gives them
+ * (rip_read_tsv_edges) -- doing on the GPU what the reference's Graph
+ * constructor and get_transpose do on the host (include/ripples/graph.h:
+ * 506-620, 787-832): with `renumber`, ids become 0..n-1 in sorted order of
+ * the distinct endpoints (rip_graph_id_map gives the map back), else
+ * n = largest id + 1; each vertex's in-list is ordered by source id, parallel
+ * edges in input order; weights are packed for `model` as rip_graph_upload
+ * packs them.  The result equals rip_graph_upload of rip_read_tsv's CSR for
+ * the same file.  Limits: m < 2^32 - 4, n < 2^32 - 1. */
+int rip_graph_from_edges(rip_ctx *ctx, const uint32_t *src, const uint32_t *dst,
+                         const float *w, uint64_t m, int renumber, int model,
+                         rip_graph **out);
+/* Internal id -> input id of a graph's vertices (n entries; the identity for
+ * graphs not renumbered by rip_graph_from_edges), Graph::convertID's map. */
+int rip_graph_id_map(const rip_graph *g, uint32_t *map);
+
 /* ---- RRR pool --------------------------------------------------------------- */
 /* A device-resident, growable flat pool of RRR sets, addressed by set id
  * 0, 1, 2, ...  Replaces RRRsets = std::vector<std::vector<uint32_t>>
@@ -564,6 +581,14 @@ typedef struct rip_tsv_options {
  * or bad options. */
 int rip_read_tsv(const char *path, const rip_tsv_options *opt, uint32_t *n, uint64_t *m,
                  uint64_t **index, uint32_t **src, float **w, uint32_t **reverse_map);
+/* The edge list of a TSV file before any CSR is built: parsing, generated
+ * weights, undirected doubling, the LT per-source normalisation and the scale
+ * factor exactly as rip_read_tsv applies them (include/ripples/loaders.h:
+ * 138-196), in input ids.  Outputs are malloc'd arrays of m entries released
+ * with rip_free; rip_graph_from_edges builds the graph from them on the
+ * device. */
+int rip_read_tsv_edges(const char *path, const rip_tsv_options *opt, uint64_t *m,
+                       uint32_t **src, uint32_t **dst, float **w);
 /* Reads the reference binary format (include/ripples/graph.h:854-995,
  * backward direction, float weights), weights multiplied by `scale` when it
  * is below 1.  Outputs as rip_read_tsv. */

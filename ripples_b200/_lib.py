@@ -122,6 +122,8 @@ SIGNATURES = {
     "rip_kernel_launches": (U64, []),
     "rip_graph_uniform_thresholds": (I32, [P, I32, ctypes.POINTER(I32)]),
     "rip_graph_branching": (I32, [P, ctypes.POINTER(ctypes.c_double)]),
+    "rip_graph_from_edges": (I32, [P, P, P, P, U64, I32, I32, PP]),
+    "rip_graph_id_map": (I32, [P, P]),
     "rip_coin_rate": (I32, [P, ctypes.POINTER(ctypes.c_double)]),
     "rip_graph_upload": (I32, [P, P, P, P, U32, U64, I32, PP]),
     "rip_graph_destroy": (I32, [P]),
@@ -179,6 +181,8 @@ SIGNATURES = {
     "rip_make_weights": (I32, [I32, U32, P, U64, U64, DBL, DBL, P]),
     "rip_write_binary": (I32, [ctypes.c_char_p, U32, U64, P, P, P, I32]),
     "rip_free": (None, [P]),
+    "rip_read_tsv_edges": (I32, [ctypes.c_char_p, ctypes.POINTER(TsvOptions),
+                                 ctypes.POINTER(U64), P, P, P]),
     "rip_read_tsv": (I32, [ctypes.c_char_p, ctypes.POINTER(TsvOptions), ctypes.POINTER(U32),
                            ctypes.POINTER(U64), P, P, P, P]),
     "rip_read_binary": (I32, [ctypes.c_char_p, ctypes.c_double, ctypes.POINTER(U32),

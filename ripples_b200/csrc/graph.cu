@@ -132,7 +132,7 @@ extern "C" int rip_graph_upload(rip_ctx *c, const uint64_t *index,
 }
 
 // Packs index/src/weights already in device memory into a new graph.
-static int pack_device_csr(rip_ctx *c, const uint64_t *d_index, const uint32_t *d_src,
+int pack_device_csr(rip_ctx *c, const uint64_t *d_index, const uint32_t *d_src,
                            const float *d_w, uint32_t n, uint64_t m, int model,
                            rip_graph **out) {
   rip_graph *g = new rip_graph();

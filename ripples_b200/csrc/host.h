@@ -247,6 +247,9 @@ struct rip_graph {
   uint64_t m;
   int model;
   DevMem off, edges;
+  // internal id -> input id when the graph was built from an edge list with
+  // renumbering (rip_graph_from_edges); empty: the identity
+  std::vector<uint32_t> reverse_map;
   // per-vertex uniform IC thresholds (DevGraph::vthr); allocated only when
   // uniform in-lists hold at least half of the edges, and used while
   // use_vthr is set
@@ -273,6 +276,11 @@ struct rip_graph {
                     use_vthr && vthr.p ? ptr<uint32_t>(vthr) : nullptr};
   }
 };
+// Packs a backward CSR already in device memory (index u64[n+1], src u32[m],
+// weights f32[m]) into a new graph of the context (graph.cu).
+int pack_device_csr(rip_ctx *c, const uint64_t *d_index, const uint32_t *d_src,
+                    const float *d_w, uint32_t n, uint64_t m, int model, rip_graph **out);
+
 
 // A captured lowest-id pick loop and the addresses it was captured with.
 struct SelGraph {

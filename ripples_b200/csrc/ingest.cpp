@@ -104,18 +104,18 @@ int hand_out(uint32_t n, const std::vector<uint64_t> &index, const std::vector<u
 
 extern "C" const char *rip_read_error(void) { return g_read_error.c_str(); }
 
-extern "C" int rip_read_tsv(const char *path, const rip_tsv_options *o, uint32_t *n_out,
-                            uint64_t *m_out, uint64_t **index_out, uint32_t **src_out,
-                            float **w_out, uint32_t **map_out) {
-  if (!path || !o || !n_out || !m_out || !index_out || !src_out || !w_out || !map_out)
-    return read_fail("rip_read_tsv: null argument");
+namespace {
+
+// The edge list of a TSV file as include/ripples/loaders.h:138-196 reads it:
+// parsing, generated weights, undirected doubling, the LT normalisation per
+// source and the scale factor -- everything before the Graph constructor.
+int parse_tsv(const char *path, const rip_tsv_options *o, std::vector<Edge> &edges) {
   if (o->scale > 1.0) return read_fail("The scale factor must be <= 1.0");
   std::ifstream in(path);
   if (!in) return read_fail(std::string("cannot open ") + path);
   const bool known_dist = o->distribution == RIP_DIST_UNIFORM ||
                           o->distribution == RIP_DIST_NORMAL ||
                           o->distribution == RIP_DIST_CONST;
-  std::vector<Edge> edges;
   uint64_t ctr = 0, lineno = 0;
   std::string line;
   while (std::getline(in, line)) {
@@ -154,6 +154,51 @@ extern "C" int rip_read_tsv(const char *path, const rip_tsv_options *o, uint32_t
   }
   if (o->scale < 1.0)
     for (auto &e : edges) e.w = (float)(e.w * o->scale);
+  return RIP_OK;
+}
+
+}  // namespace
+
+extern "C" int rip_read_tsv_edges(const char *path, const rip_tsv_options *o, uint64_t *m_out,
+                                  uint32_t **src_out, uint32_t **dst_out, float **w_out) {
+  if (!path || !o || !m_out || !src_out || !dst_out || !w_out)
+    return read_fail("rip_read_tsv_edges: null argument");
+  std::vector<Edge> edges;
+  const int rc = parse_tsv(path, o, edges);
+  if (rc != RIP_OK) return rc;
+  std::vector<uint32_t> s(edges.size()), d(edges.size());
+  std::vector<float> w(edges.size());
+  for (size_t i = 0; i < edges.size(); ++i) {
+    s[i] = edges[i].s;
+    d[i] = edges[i].d;
+    w[i] = edges[i].w;
+  }
+  uint32_t *ps = copy_out(s), *pd = copy_out(d);
+  float *pw = copy_out(w);
+  if (!ps || !pd || !pw) {
+    std::free(ps);
+    std::free(pd);
+    std::free(pw);
+    g_read_error = "out of host memory";
+    return RIP_ERR_NOMEM;
+  }
+  *m_out = edges.size();
+  *src_out = ps;
+  *dst_out = pd;
+  *w_out = pw;
+  return RIP_OK;
+}
+
+extern "C" int rip_read_tsv(const char *path, const rip_tsv_options *o, uint32_t *n_out,
+                            uint64_t *m_out, uint64_t **index_out, uint32_t **src_out,
+                            float **w_out, uint32_t **map_out) {
+  if (!path || !o || !n_out || !m_out || !index_out || !src_out || !w_out || !map_out)
+    return read_fail("rip_read_tsv: null argument");
+  std::vector<Edge> edges;
+  {
+    const int rc = parse_tsv(path, o, edges);
+    if (rc != RIP_OK) return rc;
+  }
   uint32_t n = 0;
   std::vector<uint32_t> reverse_map;
   uint32_t maxid = 0;

@@ -122,6 +122,36 @@ class HostGraph:
                               ctypes.byref(pm))
         return cls._from_read(rc, n, m, pi, ps, pw, pm, "rip_read_tsv")
 
+    @staticmethod
+    def read_tsv_edges(path: str, weighted: bool = False, undirected: bool = False,
+                       model: str = "IC", distribution: str = "uniform", mean: float = 0.5,
+                       variance: float = 1.0,
+                       scale: float = 1.0) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
+        """A TSV file's edge list before any CSR is built (``rip_read_tsv_edges``):
+        (src, dst, weights) in input ids, for ``DeviceGraph.from_edges``."""
+        dist = {"uniform": _lib.DIST_UNIFORM, "normal": _lib.DIST_NORMAL,
+                "const": _lib.DIST_CONST}.get(distribution, -1)
+        o = _lib.TsvOptions(int(weighted), int(undirected), 1, MODELS[model], dist, mean,
+                            variance, scale)
+        m = ctypes.c_uint64()
+        ps, pd, pw = (ctypes.c_void_p() for _ in range(3))
+        rc = lib.rip_read_tsv_edges(path.encode(), ctypes.byref(o), ctypes.byref(m),
+                                    ctypes.byref(ps), ctypes.byref(pd), ctypes.byref(pw))
+        if rc != 0:
+            raise RipError(rc, "rip_read_tsv_edges", (lib.rip_read_error() or b"").decode())
+        mm = m.value
+        try:
+            src = np.ctypeslib.as_array(ctypes.cast(ps, ctypes.POINTER(ctypes.c_uint32)),
+                                        shape=(max(mm, 1),))[:mm].copy()
+            dst = np.ctypeslib.as_array(ctypes.cast(pd, ctypes.POINTER(ctypes.c_uint32)),
+                                        shape=(max(mm, 1),))[:mm].copy()
+            w = np.ctypeslib.as_array(ctypes.cast(pw, ctypes.POINTER(ctypes.c_float)),
+                                      shape=(max(mm, 1),))[:mm].copy()
+        finally:
+            for x in (ps, pd, pw):
+                lib.rip_free(x)
+        return src, dst, w
+
     @classmethod
     def read_binary(cls, path: str, scale: float = 1.0,
                     forward: bool = False) -> Tuple["HostGraph", np.ndarray]:
@@ -305,6 +335,33 @@ class DeviceGraph:
                                                ctypes.byref(avail)),
               "rip_graph_uniform_thresholds", self.ctx.h)
         return bool(avail.value)
+
+    @classmethod
+    def from_edges(cls, ctx: "Context", src, dst, weights, model: str,
+                   renumber: bool = True) -> "DeviceGraph":
+        """The graph built on the device from a host edge list
+        (``rip_graph_from_edges``): renumbering, transpose and packing on the
+        GPU.  ``id_map()`` gives internal id -> input id."""
+        self = cls.__new__(cls)
+        s = np.ascontiguousarray(src, dtype=np.uint32)
+        d = np.ascontiguousarray(dst, dtype=np.uint32)
+        w = np.ascontiguousarray(weights, dtype=np.float32)
+        h = ctypes.c_void_p()
+        check(lib.rip_graph_from_edges(ctx.h, _ptr(s), _ptr(d), _ptr(w), len(s),
+                                       int(renumber), MODELS[model], ctypes.byref(h)),
+              "rip_graph_from_edges", ctx.h)
+        n, m = ctypes.c_uint32(), ctypes.c_uint64()
+        check(lib.rip_graph_info(h, ctypes.byref(n), ctypes.byref(m), None), "rip_graph_info",
+              ctx.h)
+        self.ctx, self.model, self.n, self.m, self.h = ctx, model, n.value, m.value, h
+        self._pools = weakref.WeakSet()
+        ctx._children.add(self)
+        return self
+
+    def id_map(self) -> np.ndarray:
+        out = np.zeros(max(self.n, 1), dtype=np.uint32)
+        check(lib.rip_graph_id_map(self.h, _ptr(out)), "rip_graph_id_map", self.ctx.h)
+        return out[: self.n]
 
     @property
     def branching(self) -> float:

@@ -228,6 +228,26 @@ def test_read_tsv_generated_weights_and_errors(tmp_path):
         rb.HostGraph.read_tsv(big)
 
 
+def test_read_tsv_edges_is_the_readers_edge_list(tmp_path):
+    # rip_read_tsv_edges stops before the Graph constructor: renumbering its
+    # edges (sorted distinct ids) and ordering them by (destination, source),
+    # stably, gives rip_read_tsv's CSR -- what rip_graph_from_edges does on the
+    # device.
+    rng = np.random.default_rng(3)
+    lines = [f"{a}\t{b}\t{rng.random():.6f}" for a, b in rng.integers(5, 900, size=(1500, 2))]
+    p = _write(tmp_path / "e.tsv", "# c\n" + "\n".join(lines) + "\n")
+    for undirected in (False, True):
+        s, d, w = rb.HostGraph.read_tsv_edges(p, weighted=True, undirected=undirected)
+        g, rmap = rb.HostGraph.read_tsv(p, weighted=True, undirected=undirected)
+        ids = np.unique(np.concatenate([s, d]))
+        assert np.array_equal(ids, rmap)
+        rs, rd = np.searchsorted(ids, s), np.searchsorted(ids, d)
+        order = np.lexsort((rs, rd))  # stable: by destination, then source
+        assert np.array_equal(rs[order].astype(np.uint32), g.src)
+        assert np.array_equal(w[order], g.weights)
+        assert np.array_equal(np.searchsorted(rd[order], np.arange(g.n + 1)), g.index)
+
+
 def test_read_binary_round_trip_and_errors(tmp_path):
     g = rb.HostGraph.rmat(9, 4000, seed=4).with_weights(rb.WEIGHTS_UNIFORM, seed=1, lo=0, hi=1)
     p = str(tmp_path / "g.bin")
