@@ -4,6 +4,7 @@
 // macros.
 #pragma once
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdarg>
@@ -59,6 +60,9 @@ struct rip_ctx {
   std::vector<DevMem> cache;
   size_t cached = 0;
   PinnedMem *h_cand = nullptr;   // mapped: reference-heap candidate ids and counts
+  // last epoch a cover-and-gather kernel published in h_cand's first word
+  // (unique per context, so a flag left by an earlier pick never matches)
+  uint32_t cg_epoch = 0;
   // reference-heap selection storage, shared by the context's pools (one
   // selection runs at a time) and page-locked once
   std::vector<HeapItem> heap_store;
@@ -350,6 +354,10 @@ struct rip_pool {
   uint32_t cand_fixed = 0;           // first-fetch threshold, % of the last gain (0 = adaptive)
   DevMem d_heap;                     // heap built on the device
   DevMem s_cmax, s_dirty, s_best, s_desc;  // device lowest-id picks
+  // reference-heap picks: completion ticket of the cover-and-gather kernel
+  // (zero between launches)
+  DevMem cg_done;
+  bool cg_done_zeroed = false;
   PinnedMem h_best;
   SelGraph sel_graph;                // the captured pick loop
   // selection profile: [0] count+index kernels and counts D2H, [1] heap build,

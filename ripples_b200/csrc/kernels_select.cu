@@ -171,6 +171,46 @@ __global__ void __launch_bounds__(256) cover_kernel(CoverLaunch C) {
   }
 }
 
+// A reference-heap pick in one launch: cover_kernel's work, then the last
+// block to finish (a completion ticket in *done) gathers the current counts of
+// the host's candidates for the next pick into `out` (mapped host memory),
+// resets the ticket and publishes `epoch` in *flag after a system-wide fence,
+// so the host polls one word instead of synchronising the stream.
+__global__ void __launch_bounds__(256) cover_gather_kernel(CoverLaunch C, const uint32_t *ids,
+                                                           uint32_t nids, uint32_t *out,
+                                                           unsigned int *done,
+                                                           volatile unsigned int *flag,
+                                                           unsigned int epoch) {
+  const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const uint32_t lane = lane_id();
+  const uint64_t lo = C.inv_off[C.vertex], hi = C.inv_off[C.vertex + 1];
+  for (uint64_t i = lo + gw; i < hi; i += nw) {
+    const uint32_t s = C.inv[i];
+    if (C.covered[s]) continue;
+    const uint32_t len = C.P.set_len[s];
+    const uint64_t off = C.P.set_off[s];
+    if (lane == 0) C.covered[s] = 1;
+    for (uint32_t j = lane; j < len; j += 32) atomicSub(C.count + C.P.vtx[off + j], 1u);
+  }
+  __shared__ bool s_last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();  // this block's decrements before its ticket
+    s_last = atomicAdd(done, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();  // every other block's decrements are visible from here
+  for (uint32_t i = threadIdx.x; i < nids; i += blockDim.x) out[i] = __ldcg(C.count + ids[i]);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    *done = 0u;
+    __threadfence_system();
+    *flag = epoch;
+  }
+}
+
 // ---- device-only picks (served queries) -----------------------------------
 // Every kernel reads its buffers from a SelDesc in device memory, so one
 // captured CUDA graph serves every round of a query: the host rewrites the
@@ -546,6 +586,13 @@ void launch_build_inverted(const DevPool &P, uint64_t num_sets,
 void launch_cover(const CoverLaunch &C, cudaStream_t stream) {
   count_launches(1);
   cover_kernel<<<C.blocks, 256, 0, stream>>>(C);
+}
+
+void launch_cover_gather(const CoverLaunch &C, const uint32_t *ids, uint32_t nids,
+                         uint32_t *out, unsigned int *done, unsigned int *flag,
+                         unsigned int epoch, cudaStream_t stream) {
+  count_launches(1);
+  cover_gather_kernel<<<C.blocks, 256, 0, stream>>>(C, ids, nids, out, done, flag, epoch);
 }
 
 void launch_coverage(const DevPool &P, uint64_t S, const uint32_t *marked,

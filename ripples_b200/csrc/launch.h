@@ -207,6 +207,11 @@ struct CoverLaunch {
   int blocks;
 };
 void launch_cover(const CoverLaunch &C, cudaStream_t stream);
+// The cover, then the last block gathers count[ids[i]] (i < nids) into out,
+// resets *done (a zeroed device word) and writes epoch to *flag (mapped).
+void launch_cover_gather(const CoverLaunch &C, const uint32_t *ids, uint32_t nids,
+                         uint32_t *out, unsigned int *done, unsigned int *flag,
+                         unsigned int epoch, cudaStream_t stream);
 // Builds the selection max-heap of {vertex, count} on the device, element for
 // element the heap std::make_heap builds (level-parallel).
 void launch_make_heap(const uint32_t *count, uint32_t n, uint2 *heap, cudaStream_t stream);

@@ -247,8 +247,9 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
   C.count = ptr<uint32_t>(p->count);
   C.blocks = c->num_sms * 4;
 
-  std::vector<uint32_t> &hcount = p->last_counts;
-  hcount.resize(n);
+  // whole-array count fetches land in the context's page-locked buffer and
+  // are read there (no second host copy)
+  const uint32_t *hcount = nullptr;
   if (!c->h_cand) c->h_cand = new PinnedMem();
   if (!c->h_count) c->h_count = new PinnedMem();
   // mapped: candidate vertex ids in, their counts out (reference-heap picks)
@@ -347,33 +348,69 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
       CK(c, cudaMemcpyAsync(h_count.p, p->count.p, sizeof(uint32_t) * (size_t)n,
                             cudaMemcpyDeviceToHost, c->stream));
       CK(c, cudaStreamSynchronize(c->stream));
-      std::memcpy(hcount.data(), h_count.p, sizeof(uint32_t) * (size_t)n);
+      hcount = static_cast<const uint32_t *>(h_count.p);
       fresh_all = true;
       p->sel_prof[8] += 1;
       return RIP_OK;
+    };
+    // The next pick's first candidate fetch rides on the cover: its items are
+    // collected before the cover is launched (the heap and the last gain are
+    // final once the seed is chosen) and, when few enough, the cover kernel's
+    // last block gathers their counts and raises a flag the host polls.
+    constexpr uint32_t FUSED_MAX = 2048;  // one block reads the ids over the bus
+    TRY(dalloc(c, p->cg_done, sizeof(unsigned int)));
+    if (!p->cg_done_zeroed) {
+      CK(c, cudaMemsetAsync(p->cg_done.p, 0, sizeof(unsigned int), c->stream));
+      p->cg_done_zeroed = true;
+    }
+    volatile unsigned int *h_flag = reinterpret_cast<volatile unsigned int *>(hb);
+    unsigned int *d_flag = reinterpret_cast<unsigned int *>(db);
+    bool prefetched = false;  // h_ids / h_cnt hold round 0 of the next pick
+    uint32_t pre_T = 0, pre_nc = 0;
+    auto first_T = [&](uint64_t g_prev) {
+      const double guess = p->cand_fixed ? p->cand_fixed / 100.0 : margin * ratio;
+      return (uint32_t)std::max<double>(1.0, std::floor((double)g_prev * guess));
+    };
+    // round-0 collect at T (raised once while too many items qualify);
+    // returns the count, CAND_CAP + 1 when still too many
+    auto collect0 = [&](uint64_t g_prev, uint32_t &T) -> uint32_t {
+      for (;;) {
+        const auto t_c0 = clk::now();
+        const uint32_t nc = collect_at_least(queue.items(), T, CAND_CAP, h_ids, stack);
+        p->sel_prof[10] += ms_since(t_c0);
+        if (nc > CAND_CAP && T < g_prev) {
+          T = (uint32_t)std::min<uint64_t>(g_prev, (uint64_t)T + (g_prev - T + 1) / 2);
+          continue;
+        }
+        return nc;
+      }
     };
     while (out_seeds.size() < k && uncovered != 0) {
       const auto t_g0 = clk::now();
       if (!first) {
         const uint64_t g_prev = out_gains.back();
-        const double guess = p->cand_fixed ? p->cand_fixed / 100.0 : margin * ratio;
-        uint32_t T = (uint32_t)std::max<double>(1.0, std::floor((double)g_prev * guess));
+        uint32_t T = prefetched ? pre_T : first_T(g_prev);
         for (int round = 0;; ++round) {
-          const auto t_c0 = clk::now();
-          const uint32_t nc = collect_at_least(queue.items(), T, CAND_CAP, h_ids, stack);
-          p->sel_prof[10] += ms_since(t_c0);
+          uint32_t nc;
+          if (round == 0 && prefetched) {
+            nc = pre_nc;
+          } else if (round == 0) {
+            nc = collect0(g_prev, T);
+          } else {
+            const auto t_c0 = clk::now();
+            nc = collect_at_least(queue.items(), T, CAND_CAP, h_ids, stack);
+            p->sel_prof[10] += ms_since(t_c0);
+          }
           p->sel_prof[11] += 1;
           if (nc > CAND_CAP) {
-            if (round == 0 && T < g_prev) {  // guess too low: raise it
-              T = (uint32_t)std::min<uint64_t>(g_prev, (uint64_t)T + (g_prev - T + 1) / 2);
-              continue;
-            }
             TRY(fetch_all());
             break;
           }
-          launch_gather_counts(ptr<uint32_t>(p->count), d_ids, nc, d_cnt, c->stream);
-          CK(c, cudaGetLastError());
-          CK(c, cudaStreamSynchronize(c->stream));
+          if (!(round == 0 && prefetched)) {
+            launch_gather_counts(ptr<uint32_t>(p->count), d_ids, nc, d_cnt, c->stream);
+            CK(c, cudaGetLastError());
+            CK(c, cudaStreamSynchronize(c->stream));
+          }
           p->sel_prof[5] += nc;
           cmap.reset(nc);
           uint32_t mc = 0;
@@ -389,6 +426,7 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
           T = std::max<uint32_t>(mc, 1u);  // mc <= m < T: exact next round
           margin = std::max(0.5, margin - 0.05);
         }
+        prefetched = false;
       }
       p->sel_prof[7] += ms_since(t_g0);
       HeapItem element;
@@ -420,7 +458,36 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
       out_seeds.push_back(element.first);
       out_gains.push_back(element.second);
       if (out_seeds.size() == k) break;
-      TRY(cover(element.first, element.second));
+      const auto t_f0 = clk::now();
+      pre_T = first_T(element.second);
+      pre_nc = collect0(element.second, pre_T);
+      if (pre_nc <= FUSED_MAX) {
+        C.vertex = element.first;
+        C.blocks = (int)std::min<uint64_t>(max_blocks * 4,
+                                           std::max<uint64_t>(1, (element.second + 7) / 8));
+        // epochs count per context: the mapped buffer is the context's
+        const unsigned int epoch = ++c->cg_epoch;
+        *h_flag = 0u;  // the buffer's first word may hold anything before this
+        launch_cover_gather(C, d_ids, pre_nc, d_cnt, ptr<unsigned int>(p->cg_done), d_flag,
+                            epoch, c->stream);
+        CK(c, cudaGetLastError());
+        // poll the flag; a stream synchronise covers the (unexpected) case of
+        // a flag that does not arrive within a second
+        const auto t_w0 = clk::now();
+        while (*h_flag != epoch) {
+          if (ms_since(t_w0) > 1000.0) {
+            CK(c, cudaStreamSynchronize(c->stream));
+            if (*h_flag != epoch)
+              return set_err(c, RIP_ERR_DEVICE, "pick flag not raised after the cover");
+            break;
+          }
+        }
+        std::atomic_thread_fence(std::memory_order_acquire);
+        prefetched = true;
+      } else {
+        TRY(cover(element.first, element.second));
+      }
+      p->sel_prof[7] += ms_since(t_f0);
       fresh_all = first = false;
     }
     p->sel_prof[2] += ms_since(t_p0);
