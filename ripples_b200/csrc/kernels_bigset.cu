@@ -84,10 +84,10 @@ ic_bigset_kernel(BigLaunch L) {
     uint32_t lo = 0, hi = 1;
     // Coins of group g of the in-list [ob, oe) (uniform threshold ovt, or 0:
     // each record's own); newly reached sources go to the queue.
-    auto expand_group = [&](uint32_t g, uint32_t ob, uint32_t oe, uint32_t ovt) {
-      uint2 rec[4] = {};
-      if (!ovt) load_group(L.G.edges, g, rec);  // else: uniform threshold
-      const u32x4 c = ic_coins(L.key, g, s);
+    // The live edges of group g given its coins c (and, for a list without a
+    // uniform threshold, its records).
+    auto apply_coins = [&](uint32_t g, uint32_t ob, uint32_t oe, uint32_t ovt, const u32x4 &c,
+                           const uint2 rec[4]) {
 #pragma unroll
       for (int t = 0; t < 4; ++t) {
         const uint32_t ed = (g << 2) + t;
@@ -105,6 +105,11 @@ ic_bigset_kernel(BigLaunch L) {
           }
         }
       }
+    };
+    auto expand_group = [&](uint32_t g, uint32_t ob, uint32_t oe, uint32_t ovt) {
+      uint2 rec[4] = {};
+      if (!ovt) load_group(L.G.edges, g, rec);  // else: uniform threshold
+      apply_coins(g, ob, oe, ovt, ic_coins(L.key, g, s), rec);
     };
     while (lo < hi && !s_overflow) {
       for (uint32_t cb = lo; cb < hi; cb += BIG_THREADS) {
@@ -134,8 +139,22 @@ ic_bigset_kernel(BigLaunch L) {
           const uint32_t a = s_long[li];
           const uint32_t ob = s_beg[a], oe = s_end[a], ovt = s_vt[a];
           const uint32_t g_last = (oe - 1) >> 2;
-          for (uint32_t g = (ob >> 2) + tid; g <= g_last; g += BIG_THREADS)
-            expand_group(g, ob, oe, ovt);
+          if (ovt) {
+            // uniform threshold: nothing to load, two coin blocks in flight
+            // per thread so their dependent Philox rounds interleave
+            const uint2 none[4] = {};
+            uint32_t g = (ob >> 2) + tid;
+            for (; g + BIG_THREADS <= g_last; g += 2 * BIG_THREADS) {
+              const u32x4 c0 = ic_coins(L.key, g, s);
+              const u32x4 c1 = ic_coins(L.key, g + BIG_THREADS, s);
+              apply_coins(g, ob, oe, ovt, c0, none);
+              apply_coins(g + BIG_THREADS, ob, oe, ovt, c1, none);
+            }
+            if (g <= g_last) apply_coins(g, ob, oe, ovt, ic_coins(L.key, g, s), none);
+          } else {
+            for (uint32_t g = (ob >> 2) + tid; g <= g_last; g += BIG_THREADS)
+              expand_group(g, ob, oe, ovt);
+          }
         }
         // the other lists through their concatenated groups: entry a holds
         // group j when s_off[a] <= j < s_off[a + 1]; a thread's j only grows,

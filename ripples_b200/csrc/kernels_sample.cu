@@ -128,11 +128,8 @@ __device__ __forceinline__ SetOutcome ic_plain_set(const DevGraph &G, Key key, u
   // Draws the coins of group g of the in-list [ob, oe) (uniform threshold
   // ovt, or 0: each record's own), marks the live sources in the bitmap and
   // reports which were not yet there.
-  auto expand_group = [&](uint32_t g, uint32_t ob, uint32_t oe, uint32_t ovt, bool isnew[4],
-                          uint32_t nu[4]) {
-    uint2 rec[4] = {};
-    if (!ovt) load_group(G.edges, g, rec);
-    const u32x4 c = ic_coins(key, g, s);
+  auto apply_coins = [&](uint32_t g, uint32_t ob, uint32_t oe, uint32_t ovt, const u32x4 &c,
+                         const uint2 rec[4], bool isnew[4], uint32_t nu[4]) {
 #pragma unroll
     for (int t = 0; t < 4; ++t) {
       const uint32_t e = (g << 2) + t;
@@ -149,6 +146,12 @@ __device__ __forceinline__ SetOutcome ic_plain_set(const DevGraph &G, Key key, u
         isnew[t] = !(old & bit);
       }
     }
+  };
+  auto expand_group = [&](uint32_t g, uint32_t ob, uint32_t oe, uint32_t ovt, bool isnew[4],
+                          uint32_t nu[4]) {
+    uint2 rec[4] = {};
+    if (!ovt) load_group(G.edges, g, rec);
+    apply_coins(g, ob, oe, ovt, ic_coins(key, g, s), rec, isnew, nu);
   };
 
   while (head < qlen && !overflow) {
