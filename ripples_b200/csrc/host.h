@@ -273,7 +273,7 @@ struct rip_graph {
     uint32_t colors = 64, giant_min = 32;
     uint64_t cap_plain = 1ull << 18, cap_fused = 1ull << 23;
     int plain_occupancy = 0;
-    uint32_t big_threads = 512;
+    uint32_t big_threads = 256;
   } tuned;
   DevGraph view() {
     return DevGraph{n, m, ptr<uint32_t>(off), ptr<uint2>(edges),
@@ -335,7 +335,7 @@ struct rip_pool {
   uint64_t cap_plain = 1ull << 18;  // in-edges per set before a warp hands it over
   uint64_t cap_fused = 1ull << 23;  // in-edges per fused batch before handing over
   uint64_t big_sets = 0;            // sets grown one CTA each (diagnostic)
-  uint32_t big_threads = 512;       // block shape of the CTA-per-set kernel (256/512/1024)
+  uint32_t big_threads = 256;       // block shape of the CTA-per-set kernel (128-1024)
   uint32_t colors = 64;      // fused colour width (64/128/256)
   uint32_t fused_slots = 0;  // 0 = size from the budget
   uint32_t lcap_pref = 0;    // 0 = default frontier-log capacity

@@ -19,8 +19,8 @@ namespace rip {
 
 namespace {
 
-// Block shapes: 256, 512 or 1024 threads (at 64 registers a thread: 4, 2 or
-// 1 CTA per SM, each growing its own set -- smaller CTAs let one set's barrier
+// Block shapes: 128, 256, 512 or 1024 threads (at 64 registers a thread: 8,
+// 4, 2 or 1 CTA per SM, each growing its own set -- smaller CTAs let one set's barrier
 // waits overlap another's work; the autotuner picks per graph).  In-lists of
 // at least BIG_THREADS 4-edge groups are swept by the whole CTA, one list at
 // a time.
@@ -236,7 +236,9 @@ ic_bigset_kernel(BigLaunch L) {
 
 void launch_ic_bigset(const BigLaunch &L, cudaStream_t stream) {
   count_launches(1);
-  if (L.threads == 256)
+  if (L.threads == 128)
+    ic_bigset_kernel<128><<<L.blocks, 128, 0, stream>>>(L);
+  else if (L.threads == 256)
     ic_bigset_kernel<256><<<L.blocks, 256, 0, stream>>>(L);
   else if (L.threads == 512)
     ic_bigset_kernel<512><<<L.blocks, 512, 0, stream>>>(L);

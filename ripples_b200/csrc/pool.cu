@@ -682,10 +682,10 @@ extern "C" int rip_graph_autotune(rip_graph *g, uint64_t seed, uint32_t pilot, d
       {RIP_SAMPLER_FUSED, 64, 1ull << 18, 1ull << 23, 32, 0, 1024},
       {RIP_SAMPLER_FUSED, 128, 1ull << 18, 1ull << 23, 32, 0, 1024},
       {RIP_SAMPLER_FUSED, 256, 1ull << 18, 1ull << 23, 32, 0, 1024},
-      {RIP_SAMPLER_PLAIN, 64, 1ull << 18, 1ull << 23, 32, 5, 512},
-      {RIP_SAMPLER_PLAIN, 64, 1ull << 18, 1ull << 23, 0, 5, 512},
-      {RIP_SAMPLER_PLAIN, 64, 1ull << 18, 1ull << 23, 0, 0, 512},
+      {RIP_SAMPLER_PLAIN, 64, 1ull << 18, 1ull << 23, 32, 5, 256},
+      {RIP_SAMPLER_PLAIN, 64, 1ull << 18, 1ull << 23, 0, 5, 256},
       {RIP_SAMPLER_PLAIN, 64, 1ull << 18, 1ull << 23, 0, 0, 256},
+      {RIP_SAMPLER_PLAIN, 64, 1ull << 16, 1ull << 23, 0, 0, 256},
   };
   if (ms)
     for (int i = 0; i < RIP_TUNE_CANDIDATES; ++i) ms[i] = -1.0;
@@ -779,7 +779,8 @@ extern "C" int rip_pool_heavy_batch(rip_pool *p, uint32_t min_sets) {
 
 // Block shape of the CTA-per-set kernel for heavy IC sets.
 extern "C" int rip_pool_heavy_block(rip_pool *p, uint32_t threads) {
-  if (!p || (threads != 256 && threads != 512 && threads != 1024)) return RIP_ERR_INVALID;
+  if (!p || (threads != 128 && threads != 256 && threads != 512 && threads != 1024))
+    return RIP_ERR_INVALID;
   p->big_threads = threads;
   return RIP_OK;
 }

@@ -381,9 +381,9 @@ class DeviceGraph:
     TUNE_NAMES = ("plain, heavy>2^18 grid BFS", "plain, heavy>2^14 grid BFS",
                   "plain, heavy>2^18 CTA per set, 1024-thread CTAs", "fused 64", "fused 128",
                   "fused 256", "plain 40 warps/SM, heavy>2^18 grid BFS",
-                  "plain 40 warps/SM, heavy>2^18 CTA per set, 512-thread CTAs",
-                  "plain, heavy>2^18 CTA per set, 512-thread CTAs",
-                  "plain, heavy>2^18 CTA per set, 256-thread CTAs")
+                  "plain 40 warps/SM, heavy>2^18 CTA per set, 256-thread CTAs",
+                  "plain, heavy>2^18 CTA per set, 256-thread CTAs",
+                  "plain, heavy>2^16 CTA per set, 256-thread CTAs")
 
     def autotune(self, seed: int = 0, pilot: int = 0) -> dict:
         """Times each IC sampler configuration on a pilot of sets and keeps the

@@ -470,7 +470,7 @@ def test_uniform_thresholds_only_where_they_pay(ctx):
     dg.close()
 
 
-@pytest.mark.parametrize("threads", [256, 512, 1024])
+@pytest.mark.parametrize("threads", [128, 256, 512, 1024])
 def test_cta_per_set_block_shapes_match_oracle(ctx, threads):
     # R-MAT 2^16 with 16 draws per vertex: the largest in-lists pass 1024
     # 4-edge groups, so every block shape sweeps some lists with the whole CTA
