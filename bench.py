@@ -432,10 +432,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--serve-scales", default="18,20,22,24",
                     help="s1: R-MAT scales of the resident graphs")
-    ap.add_argument("--serve-queries", type=int, default=256)
+    ap.add_argument("--serve-queries", type=int, default=64)
+    ap.add_argument("--serve-tiebreak", default="lowest_id", choices=["lowest_id", "ref_heap"],
+                    help="s1: tie-break of every query, served and plain")
     ap.add_argument("--serve-eps", default="0.5,0.3,0.13")
     ap.add_argument("--serve-max-active", type=int, default=32)
-    ap.add_argument("--serve-deadline", type=float, default=240.0,
+    ap.add_argument("--serve-deadline", type=float, default=600.0,
                     help="s1: seconds after which unfinished queries count as failed")
     ap.add_argument("--baseline-seconds", type=float, default=60.0)
     ap.add_argument("--case-scale", type=int, default=0,
@@ -852,7 +854,7 @@ def run_batch(args, w, world, rank, local):
     plain(12345, limit_s=5)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    pl = plain(0, limit_s=args.baseline_seconds)
+    pl = plain(0)
     torch.cuda.synchronize()
     t_p = time.perf_counter() - t0
     first = batched(0)
@@ -1100,7 +1102,9 @@ def run_serve(args, w, world, rank, local):
     used, budget = ctx.memory()
     fp_budget = min(150 << 30, int(0.8 * budget))
     srv = rb.Server(ctx, footprint_budget=fp_budget, max_active=args.serve_max_active)
-    qs = [rb.Query(graphs[(s["scale"], s["model"])], s["k"], s["eps"], seed=3) for s in spec]
+    tie = rb.TIE_REF_HEAP if args.serve_tiebreak == "ref_heap" else rb.TIE_LOWEST_ID
+    qs = [rb.Query(graphs[(s["scale"], s["model"])], s["k"], s["eps"], seed=3, tiebreak=tie)
+          for s in spec]
     launches0 = rb._lib.lib.rip_kernel_launches()
     clocks = ClockSampler(local)
     clocks.start()
@@ -1155,8 +1159,9 @@ def run_serve(args, w, world, rank, local):
            if qs[i].done and qs[i].status == 0]
     st = srv.stats()
     srv.close()
-    # plain path, one query at a time (fresh pool, one set per warp), on the
-    # queries in arrival order until the time budget runs out
+    # plain path, one query at a time (a fresh pool each, one set per warp,
+    # the same tie-break): every query of the same stream, in arrival order,
+    # so both arms serve the identical workload
     torch.cuda.synchronize()
     tb = time.perf_counter()
     base, same, base_ok = [], True, 0
@@ -1165,7 +1170,7 @@ def run_serve(args, w, world, rank, local):
         p = rb.Pool(graphs[(s["scale"], s["model"])])
         t1 = time.perf_counter()
         try:
-            seeds, rec = p.imm(s["k"], s["eps"], seed=3, tiebreak=rb.TIE_LOWEST_ID,
+            seeds, rec = p.imm(s["k"], s["eps"], seed=3, tiebreak=tie,
                                sampler=rb.SAMPLER_PLAIN)
             base_ok += 1
             if qs[i].done and qs[i].status == 0:
@@ -1176,8 +1181,6 @@ def run_serve(args, w, world, rank, local):
         _progress(t_run, f"baseline query {i} ({s['scale']} {s['model']} k={s['k']} "
                          f"eps={s['eps']}): {base[-1]:.0f} ms")
         p.close()
-        if time.perf_counter() - tb > args.baseline_seconds:
-            break
     t_base = time.perf_counter() - tb
     base_qps = base_ok / t_base
     line = {"metric": "IMM queries/s (serving loop)", "value": len(ok) / makespan,
@@ -1191,6 +1194,7 @@ def run_serve(args, w, world, rank, local):
                        "footprint_budget_gb": fp_budget / 2**30},
             "latency_ms": {"p50": _pct(lat, 50), "p99": _pct(lat, 99), "max": max(lat) if lat else None},
             "completed": len(ok), "failed": N - len(ok), "makespan_s": makespan,
+            "tiebreak": args.serve_tiebreak,
             "plain_one_at_a_time": {"value": base_qps, "unit": "queries/s",
                                     "queries": len(base), "completed": base_ok,
                                     "seconds": t_base,
