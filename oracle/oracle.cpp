@@ -40,7 +40,10 @@
 // independently):
 //   key                 = (seed & 0xffffffff, seed >> 32)
 //   root(s)             = mulhi64(u64(P(s_lo, 0, 0, ROOT<<24 | s_hi)), n)
-//   coin(s, e)          = P(g_lo, g_hi, s_lo, IC<<24 | s_hi)[e & 3], g = e >> 2
+//   coin(s, e)          = coarse(s, e) << 16 | fine(s, e)
+//   coarse(s, e)        = 16-bit half (e & 1) of word (e >> 1) & 3 of
+//                         P(b_lo, b_hi, s_lo, IC<<24 | s_hi),  b = e >> 3
+//   fine(s, e)          = P(e_lo, e_hi, s_lo, IC_FINE<<24 | s_hi)[0] & 0xffff
 //   lt_threshold(s, v)  = P(v, 0, s_lo, LT<<24 | s_hi)[0]
 //   IC edge e live for set s  <=>  coin(s, e) < thr[e]
 //   thr[e] = clamp(floor(w_e * 2^32), 0, 2^32-1)
@@ -66,7 +69,7 @@ namespace {
 
 enum : uint32_t {
   DOM_ROOT = 1, DOM_IC = 2, DOM_LT = 3, DOM_RMAT = 4, DOM_ER = 5, DOM_WEIGHT = 6,
-  DOM_SIM_IC = 7, DOM_SIM_LT = 8
+  DOM_SIM_IC = 7, DOM_SIM_LT = 8, DOM_IC_FINE = 9
 };
 
 void philox4x32_10(const uint32_t ctr_in[4], const uint32_t key_in[2],
@@ -114,16 +117,39 @@ uint32_t root_of(uint64_t seed, uint64_t s, uint32_t n) {
   return (uint32_t)(((unsigned __int128)u * n) >> 64);
 }
 
-uint32_t ic_coin(uint64_t seed, uint64_t s, uint64_t e) {
+uint32_t ic_coarse(uint64_t seed, uint64_t s, uint64_t e) {
   uint32_t key[2], ctr[4], out[4];
   make_key(seed, key);
-  uint64_t g = e >> 2;
-  ctr[0] = (uint32_t)g;
-  ctr[1] = (uint32_t)(g >> 32);
+  const uint64_t b = e >> 3;
+  ctr[0] = (uint32_t)b;
+  ctr[1] = (uint32_t)(b >> 32);
   ctr[2] = (uint32_t)s;
   ctr[3] = (DOM_IC << 24) | (uint32_t)((s >> 32) & 0xFFFFFFu);
   philox4x32_10(ctr, key, out);
-  return out[e & 3];
+  const uint32_t w = out[(e >> 1) & 3];
+  return (e & 1) ? (w >> 16) : (w & 0xFFFFu);
+}
+
+uint32_t ic_fine(uint64_t seed, uint64_t s, uint64_t e) {
+  uint32_t key[2], ctr[4], out[4];
+  make_key(seed, key);
+  ctr[0] = (uint32_t)e;
+  ctr[1] = (uint32_t)(e >> 32);
+  ctr[2] = (uint32_t)s;
+  ctr[3] = (DOM_IC_FINE << 24) | (uint32_t)((s >> 32) & 0xFFFFFFu);
+  philox4x32_10(ctr, key, out);
+  return out[0] & 0xFFFFu;
+}
+
+// The full 32-bit coin of edge e for set s.
+uint32_t ic_coin(uint64_t seed, uint64_t s, uint64_t e) {
+  return (ic_coarse(seed, s, e) << 16) | ic_fine(seed, s, e);
+}
+
+// coin(s, e) < thr, drawing the fine half only on a coarse tie.
+bool ic_live(uint64_t seed, uint64_t s, uint64_t e, uint32_t thr) {
+  const uint32_t c = ic_coarse(seed, s, e), th = thr >> 16;
+  return c < th || (c == th && ic_fine(seed, s, e) < (thr & 0xFFFFu));
 }
 
 // Forward spread simulation coin of edge e in replica r (its own domain).
@@ -232,7 +258,7 @@ void sample_ic_one(const Graph &G, uint64_t seed, uint64_t s,
       st.edges_scanned++;
       uint32_t u = G.src[e];
       if (stamp[u] == tag) continue;  // coins are pure: skipping is exact
-      if (ic_coin(seed, s, e) < G.thr[e]) {
+      if (ic_live(seed, s, e, G.thr[e])) {
         stamp[u] = tag;
         out.push_back(u);
       }
@@ -293,7 +319,7 @@ void sample_one_bits(const Graph &G, int model, uint64_t seed, uint64_t s,
       for (uint64_t e = G.index[v]; e < G.index[v + 1]; ++e) {
         const uint32_t u = G.src[e];
         if (bits[u >> 6] & (1ull << (u & 63))) continue;
-        if (ic_coin(seed, s, e) < G.thr[e]) {
+        if (ic_live(seed, s, e, G.thr[e])) {
           test_set(u);
           out.push_back(u);
         }

@@ -79,6 +79,20 @@ __device__ __forceinline__ uint32_t warp_find_owner(uint32_t incl, uint32_t j) {
   return lo;
 }
 
+// Lane-wise minimum of two pairs of 16-bit halves.
+__device__ __forceinline__ uint32_t vmin_u16x2(uint32_t a, uint32_t b) {
+  uint32_t d;
+  asm("min.u16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+  return d;
+}
+
+// Smallest of the eight coarse coins of a block: when it exceeds a uniform
+// threshold's coarse half, no edge of the block is live and none ties.
+__device__ __forceinline__ uint32_t block_min16(const u32x4 &c) {
+  const uint32_t m = vmin_u16x2(vmin_u16x2(c.x, c.y), vmin_u16x2(c.z, c.w));
+  return min(m & 0xFFFFu, m >> 16);
+}
+
 // Number of 4-edge groups covering [beg, end).
 __device__ __forceinline__ uint32_t group_count(uint32_t beg, uint32_t end) {
   return end > beg ? ((end - 1) >> 2) - (beg >> 2) + 1 : 0;

@@ -11,7 +11,8 @@
 // concatenated groups (a block scan turns group counts into offsets; each
 // thread finds its entry with a forward-only cursor in shared memory).
 // Levels are separated by __syncthreads only.  Coins are the same
-// (set, edge)-keyed Philox draws as every other sampler.
+// (set, edge)-keyed Philox draws as every other sampler; on lists with a
+// uniform threshold a thread takes whole 8-edge coin blocks.
 #include "device.cuh"
 #include "launch.h"
 
@@ -84,32 +85,69 @@ ic_bigset_kernel(BigLaunch L) {
     uint32_t lo = 0, hi = 1;
     // Coins of group g of the in-list [ob, oe) (uniform threshold ovt, or 0:
     // each record's own); newly reached sources go to the queue.
-    // The live edges of group g given its coins c (and, for a list without a
-    // uniform threshold, its records).
+    // Source u of a live edge joins the set (and the queue) unless there.
+    auto reach = [&](uint32_t u) {
+      const uint32_t bit = 1u << (u & 31);
+      if (!(atomicOr(&bm[u >> 5], bit) & bit)) {
+        const uint32_t pos = atomicAdd(&s_qlen, 1u);
+        if (pos < L.qcap) q[pos] = u;
+        else s_overflow = 1;
+      }
+    };
+    // The live edges of group g given its coin block c (the group is half
+    // of the 8-edge block g >> 1) and, for a list without a uniform
+    // threshold, its records.
     auto apply_coins = [&](uint32_t g, uint32_t ob, uint32_t oe, uint32_t ovt, const u32x4 &c,
                            const uint2 rec[4]) {
+      const uint32_t hb = (g & 1u) << 2;
+      uint32_t live = 0, tie = 0;
 #pragma unroll
       for (int t = 0; t < 4; ++t) {
         const uint32_t ed = (g << 2) + t;
-        if (ed >= ob && ed < oe && lane_of(c, t) < (ovt ? ovt : rec[t].y)) {
+        const uint32_t th = (ovt ? ovt : rec[t].y) >> 16, cc = coarse_of(c, hb + t);
+        if (ed >= ob && ed < oe) {
+          if (cc < th) live |= 1u << t;
+          else if (cc == th) tie |= 1u << t;
+        }
+      }
+      while (tie) {  // a coarse tie, one edge in 65 536: the fine half decides
+        const uint32_t t = __ffs(tie) - 1;
+        tie &= tie - 1;
+        const uint32_t thr = ovt ? ovt
+                                 : (t == 0 ? rec[0].y : t == 1 ? rec[1].y : t == 2 ? rec[2].y : rec[3].y);
+        if (ic_fine_call(L.key, (g << 2) + t, s) < (thr & 0xFFFFu)) live |= 1u << t;
+      }
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const uint32_t ed = (g << 2) + t;
+        if (live & (1u << t)) {
           uint32_t u = rec[t].x;
           if (ovt) {
             u = __ldg(&L.G.edges[ed].x);
             atomicAdd(&s_usrc, 1ull);
           }
-          const uint32_t bit = 1u << (u & 31);
-          if (!(atomicOr(&bm[u >> 5], bit) & bit)) {
-            const uint32_t pos = atomicAdd(&s_qlen, 1u);
-            if (pos < L.qcap) q[pos] = u;
-            else s_overflow = 1;
-          }
+          reach(u);
+        }
+      }
+    };
+    // The live edges of the 8-edge block b of a uniform-threshold list.
+    auto apply_block = [&](uint32_t b, uint32_t ob, uint32_t oe, uint32_t ovt, const u32x4 &c) {
+      const uint32_t th = ovt >> 16;
+      if (block_min16(c) > th) return;  // nothing live, no tie
+#pragma unroll
+      for (int h = 0; h < 8; ++h) {
+        const uint32_t cc = coarse_of(c, h), ed = (b << 3) + h;
+        if (cc <= th && ed >= ob && ed < oe &&
+            (cc < th || ic_fine_call(L.key, ed, s) < (ovt & 0xFFFFu))) {
+          atomicAdd(&s_usrc, 1ull);
+          reach(__ldg(&L.G.edges[ed].x));
         }
       }
     };
     auto expand_group = [&](uint32_t g, uint32_t ob, uint32_t oe, uint32_t ovt) {
       uint2 rec[4] = {};
       if (!ovt) load_group(L.G.edges, g, rec);  // else: uniform threshold
-      apply_coins(g, ob, oe, ovt, ic_coins(L.key, g, s), rec);
+      apply_coins(g, ob, oe, ovt, ic_block(L.key, g >> 1, s), rec);
     };
     while (lo < hi && !s_overflow) {
       for (uint32_t cb = lo; cb < hi; cb += BIG_THREADS) {
@@ -140,17 +178,18 @@ ic_bigset_kernel(BigLaunch L) {
           const uint32_t ob = s_beg[a], oe = s_end[a], ovt = s_vt[a];
           const uint32_t g_last = (oe - 1) >> 2;
           if (ovt) {
-            // uniform threshold: nothing to load, two coin blocks in flight
-            // per thread so their dependent Philox rounds interleave
-            const uint2 none[4] = {};
-            uint32_t g = (ob >> 2) + tid;
-            for (; g + BIG_THREADS <= g_last; g += 2 * BIG_THREADS) {
-              const u32x4 c0 = ic_coins(L.key, g, s);
-              const u32x4 c1 = ic_coins(L.key, g + BIG_THREADS, s);
-              apply_coins(g, ob, oe, ovt, c0, none);
-              apply_coins(g + BIG_THREADS, ob, oe, ovt, c1, none);
+            // uniform threshold: nothing to load; a thread takes whole
+            // 8-edge coin blocks, two in flight so their dependent Philox
+            // rounds interleave
+            const uint32_t b_last = (oe - 1) >> 3;
+            uint32_t b = (ob >> 3) + tid;
+            for (; b + BIG_THREADS <= b_last; b += 2 * BIG_THREADS) {
+              const u32x4 c0 = ic_block(L.key, b, s);
+              const u32x4 c1 = ic_block(L.key, b + BIG_THREADS, s);
+              apply_block(b, ob, oe, ovt, c0);
+              apply_block(b + BIG_THREADS, ob, oe, ovt, c1);
             }
-            if (g <= g_last) apply_coins(g, ob, oe, ovt, ic_coins(L.key, g, s), none);
+            if (b <= b_last) apply_block(b, ob, oe, ovt, ic_block(L.key, b, s));
           } else {
             for (uint32_t g = (ob >> 2) + tid; g <= g_last; g += BIG_THREADS)
               expand_group(g, ob, oe, ovt);

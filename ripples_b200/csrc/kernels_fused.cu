@@ -172,12 +172,31 @@ ic_fused_kernel(FusedLaunch L) {
                 while (mm) {
                   const int bi = __ffsll((long long)mm) - 1;
                   mm &= mm - 1;
-                  const u32x4 cn = ic_coins(L.key, g, s_set[w * 64 + bi]);
+                  const uint64_t sid = s_set[w * 64 + bi];
+                  // this group's four coarse coins: half of the 8-edge block
+                  const u32x4 cb = ic_block(L.key, g >> 1, sid);
+                  const uint32_t hb = (g & 1u) << 2;
                   const uint64_t bit = 1ull << bi;
-                  if (inr[0] && cn.x < rec[0].y) live[0][w] |= bit;
-                  if (inr[1] && cn.y < rec[1].y) live[1][w] |= bit;
-                  if (inr[2] && cn.z < rec[2].y) live[2][w] |= bit;
-                  if (inr[3] && cn.w < rec[3].y) live[3][w] |= bit;
+                  uint32_t tie = 0;
+#pragma unroll
+                  for (int t = 0; t < 4; ++t) {
+                    const uint32_t th = rec[t].y >> 16, cc = coarse_of(cb, hb + t);
+                    if (inr[t]) {
+                      if (cc < th) live[t][w] |= bit;
+                      else if (cc == th) tie |= 1u << t;
+                    }
+                  }
+                  while (tie) {  // a coarse tie, one edge in 65 536: the fine half decides
+                    const uint32_t t = __ffs(tie) - 1;
+                    tie &= tie - 1;
+                    const uint32_t thr = t == 0 ? rec[0].y : t == 1 ? rec[1].y : t == 2 ? rec[2].y : rec[3].y;
+                    if (ic_fine_call(L.key, (g << 2) + t, sid) < (thr & 0xFFFFu)) {
+                      if (t == 0) live[0][w] |= bit;
+                      else if (t == 1) live[1][w] |= bit;
+                      else if (t == 2) live[2][w] |= bit;
+                      else live[3][w] |= bit;
+                    }
+                  }
                 }
               }
             }

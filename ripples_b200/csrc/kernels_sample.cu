@@ -110,33 +110,52 @@ __device__ __forceinline__ SetOutcome ic_plain_set(const DevGraph &G, Key key, u
   // Appends this lane's newly reached vertices of one 4-edge group to the
   // queue (warp-wide, in lane order per edge slot); on queue overflow the set
   // is abandoned and the bits of vertices that will never be queued cleared.
+  auto append_one = [&](bool isnew, uint32_t nu) {
+    const uint32_t bal = __ballot_sync(FULL, isnew);
+    if (bal == 0) return;
+    const uint32_t cnt = __popc(bal);
+    if (overflow || qlen + cnt > W.qcap) {
+      if (isnew) W.bm[nu >> 5] = 0u;
+      overflow = true;
+      return;
+    }
+    if (isnew) W.q[qlen + __popc(bal & lanemask_lt())] = nu;
+    qlen += cnt;
+  };
   auto append = [&](const bool isnew[4], const uint32_t nu[4]) {
 #pragma unroll
-    for (int t = 0; t < 4; ++t) {
-      const uint32_t bal = __ballot_sync(FULL, isnew[t]);
-      if (bal == 0) continue;
-      const uint32_t cnt = __popc(bal);
-      if (overflow || qlen + cnt > W.qcap) {
-        if (isnew[t]) W.bm[nu[t] >> 5] = 0u;
-        overflow = true;
-        continue;
-      }
-      if (isnew[t]) W.q[qlen + __popc(bal & lanemask_lt())] = nu[t];
-      qlen += cnt;
-    }
+    for (int t = 0; t < 4; ++t) append_one(isnew[t], nu[t]);
   };
   // Draws the coins of group g of the in-list [ob, oe) (uniform threshold
-  // ovt, or 0: each record's own), marks the live sources in the bitmap and
-  // reports which were not yet there.
+  // ovt, or 0: each record's own) from the group's half of its 8-edge coin
+  // block, marks the live sources in the bitmap and reports which were not
+  // yet there.
   auto apply_coins = [&](uint32_t g, uint32_t ob, uint32_t oe, uint32_t ovt, const u32x4 &c,
                          const uint2 rec[4], bool isnew[4], uint32_t nu[4]) {
+    const uint32_t hb = (g & 1u) << 2;
+    uint32_t live = 0, tie = 0;
 #pragma unroll
     for (int t = 0; t < 4; ++t) {
       const uint32_t e = (g << 2) + t;
-      const bool live = e >= ob && e < oe && lane_of(c, t) < (ovt ? ovt : rec[t].y);
+      const uint32_t th = (ovt ? ovt : rec[t].y) >> 16, cc = coarse_of(c, hb + t);
+      if (e >= ob && e < oe) {
+        if (cc < th) live |= 1u << t;
+        else if (cc == th) tie |= 1u << t;
+      }
+    }
+    while (tie) {  // a coarse tie, one edge in 65 536: the fine half decides
+      const uint32_t t = __ffs(tie) - 1;
+      tie &= tie - 1;
+      const uint32_t thr = ovt ? ovt
+                               : (t == 0 ? rec[0].y : t == 1 ? rec[1].y : t == 2 ? rec[2].y : rec[3].y);
+      if (ic_fine_call(key, (g << 2) + t, s) < (thr & 0xFFFFu)) live |= 1u << t;
+    }
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const uint32_t e = (g << 2) + t;
       isnew[t] = false;
       nu[t] = rec[t].x;
-      if (live) {
+      if (live & (1u << t)) {
         if (ovt) {
           nu[t] = __ldg(&G.edges[e].x);
           ++set_usrc;
@@ -151,7 +170,7 @@ __device__ __forceinline__ SetOutcome ic_plain_set(const DevGraph &G, Key key, u
                           uint32_t nu[4]) {
     uint2 rec[4] = {};
     if (!ovt) load_group(G.edges, g, rec);
-    apply_coins(g, ob, oe, ovt, ic_coins(key, g, s), rec, isnew, nu);
+    apply_coins(g, ob, oe, ovt, ic_block(key, g >> 1, s), rec, isnew, nu);
   };
 
   while (head < qlen && !overflow) {
@@ -184,6 +203,48 @@ __device__ __forceinline__ SetOutcome ic_plain_set(const DevGraph &G, Key key, u
       longs &= longs - 1;
       const uint32_t lb = __shfl_sync(FULL, beg, L), le = __shfl_sync(FULL, end, L);
       const uint32_t lvt = __shfl_sync(FULL, vt, L);
+      if (lvt) {
+        // uniform threshold: lane j takes 8-edge coin blocks j, j + 32, ...
+        // (one Philox block for eight coins, no records read); the few live
+        // edges are then appended one per lane per pass
+        const uint32_t th = lvt >> 16, tf = lvt & 0xFFFFu;
+        const uint32_t b_last = (le - 1) >> 3;
+        for (uint32_t base = lb >> 3; base <= b_last && !overflow; base += 32) {
+          const uint32_t b = base + lane;
+          uint32_t live = 0, tie = 0;
+          const u32x4 c = ic_block(key, b, s);
+          if (b <= b_last && block_min16(c) <= th) {  // else: nothing live, no tie
+#pragma unroll
+            for (int h = 0; h < 8; ++h) {
+              const uint32_t cc = coarse_of(c, h), e = (b << 3) + h;
+              if (cc <= th && e >= lb && e < le) {
+                if (cc < th) live |= 1u << h;
+                else tie |= 1u << h;
+              }
+            }
+          }
+          while (tie) {  // coarse ties: the fine half decides
+            const uint32_t h = __ffs(tie) - 1;
+            tie &= tie - 1;
+            if (ic_fine_call(key, (b << 3) + h, s) < tf) live |= 1u << h;
+          }
+          while (__any_sync(FULL, live != 0)) {
+            bool isnew = false;
+            uint32_t nu = 0;
+            if (live) {
+              const uint32_t e = (b << 3) + (__ffs(live) - 1);
+              live &= live - 1;
+              nu = __ldg(&G.edges[e].x);
+              ++set_usrc;
+              const uint32_t bit = 1u << (nu & 31);
+              isnew = !(atomicOr(&W.bm[nu >> 5], bit) & bit);
+            }
+            append_one(isnew, nu);
+          }
+          __syncwarp();
+        }
+        continue;
+      }
       const uint32_t g_last = (le - 1) >> 2;
       for (uint32_t base = lb >> 2; base <= g_last && !overflow; base += 32) {
         const uint32_t g = base + lane;

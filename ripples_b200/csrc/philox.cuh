@@ -11,8 +11,16 @@
 // bit-identical RRR sets whatever order they visit edges in.
 //   key                = (seed_lo, seed_hi)
 //   root(s)            = mulhi64(P(s_lo, 0, 0, ROOT<<24 | s_hi)[0..1], n)
-//   coin(s, e)         = P(g_lo, g_hi, s_lo, IC<<24 | s_hi)[e & 3],  g = e >> 2
+//   coin(s, e)         = coarse(s, e) << 16 | fine(s, e)   (32 bits)
+//   coarse(s, e)       = 16-bit half (e & 1) of word (e >> 1) & 3 of
+//                        P(b_lo, b_hi, s_lo, IC<<24 | s_hi),  b = e >> 3
+//   fine(s, e)         = low 16 bits of P(e_lo, e_hi, s_lo, IC_FINE<<24 | s_hi)[0]
 //   lt_threshold(s, v) = P(v, 0, s_lo, LT<<24 | s_hi)[0]
+// An IC edge is live iff coin < threshold: coarse < thr >> 16, or
+// coarse == thr >> 16 and fine < thr & 0xFFFF.  One Philox block thus
+// carries the coarse halves of eight edges, and the fine half is drawn for
+// one edge in 65 536 (a coarse tie); the coin is still an exactly uniform
+// 32-bit draw per (set, edge), compared with the same threshold.
 // (s_hi = bits 32..55 of the set id; set ids are limited to 2^56.)
 // Forward Monte Carlo spread simulation draws from domains of its own, keyed
 // by the replica id r instead of a set id:
@@ -29,7 +37,14 @@
 
 namespace rip {
 
-enum : uint32_t { DOM_ROOT = 1, DOM_IC = 2, DOM_LT = 3, DOM_SIM_IC = 7, DOM_SIM_LT = 8 };
+enum : uint32_t {
+  DOM_ROOT = 1,
+  DOM_IC = 2,
+  DOM_LT = 3,
+  DOM_SIM_IC = 7,
+  DOM_SIM_LT = 8,
+  DOM_IC_FINE = 9
+};
 
 RIP_HD void mulhilo32(uint32_t a, uint32_t b, uint32_t &hi, uint32_t &lo) {
 #if defined(__CUDA_ARCH__)
@@ -100,10 +115,35 @@ RIP_HD uint32_t root_of(Key k, uint64_t s, uint32_t n) {
 #endif
 }
 
-// Coins for the 4 edges 4g .. 4g+3 of set s.
-RIP_HD u32x4 ic_coins(Key k, uint64_t g, uint64_t s) {
-  return philox((uint32_t)g, (uint32_t)(g >> 32), (uint32_t)s,
+// Coarse coins of the 8 edges 8b .. 8b+7 of set s: edge 8b + h is half
+// h & 1 of word h >> 1 (coarse_of).
+RIP_HD u32x4 ic_block(Key k, uint64_t b, uint64_t s) {
+  return philox((uint32_t)b, (uint32_t)(b >> 32), (uint32_t)s,
                 set_hi(s, DOM_IC), k.k0, k.k1);
+}
+
+// Fine (low) 16 bits of the coin of edge e of set s.
+RIP_HD uint32_t ic_fine(Key k, uint64_t e, uint64_t s) {
+  return philox((uint32_t)e, (uint32_t)(e >> 32), (uint32_t)s,
+                set_hi(s, DOM_IC_FINE), k.k0, k.k1).x & 0xFFFFu;
+}
+
+#if defined(__CUDACC__)
+// The fine half is drawn on one coarse tie in 65 536: out of line on the
+// device, so the samplers' hot loops carry one Philox body, not two.
+static __device__ __noinline__ uint32_t ic_fine_call(Key k, uint64_t e, uint64_t s) {
+  return ic_fine(k, e, s);
+}
+#endif
+
+// Live test of edge e with coarse coin `coarse` against threshold thr.
+RIP_HD bool ic_live(Key k, uint64_t s, uint64_t e, uint32_t coarse, uint32_t thr) {
+  const uint32_t th = thr >> 16;
+#if defined(__CUDA_ARCH__)
+  return coarse < th || (coarse == th && ic_fine_call(k, e, s) < (thr & 0xFFFFu));
+#else
+  return coarse < th || (coarse == th && ic_fine(k, e, s) < (thr & 0xFFFFu));
+#endif
 }
 
 // Coins for the 4 forward edges 4g .. 4g+3 in spread replica r.
@@ -123,6 +163,12 @@ RIP_HD uint32_t lt_threshold(Key k, uint64_t s, uint32_t v) {
 
 RIP_HD uint32_t lane_of(const u32x4 &r, uint32_t i) {
   return i == 0 ? r.x : i == 1 ? r.y : i == 2 ? r.z : r.w;
+}
+
+// Coarse coin h (0..7) of a block.
+RIP_HD uint32_t coarse_of(const u32x4 &blk, uint32_t h) {
+  const uint32_t w = lane_of(blk, h >> 1);
+  return (h & 1) ? (w >> 16) : (w & 0xFFFFu);
 }
 
 }  // namespace rip
