@@ -98,6 +98,11 @@ __device__ __forceinline__ uint32_t group_count(uint32_t beg, uint32_t end) {
   return end > beg ? ((end - 1) >> 2) - (beg >> 2) + 1 : 0;
 }
 
+// Number of 8-edge coin blocks covering [beg, end).
+__device__ __forceinline__ uint32_t block_count(uint32_t beg, uint32_t end) {
+  return end > beg ? ((end - 1) >> 3) - (beg >> 3) + 1 : 0;
+}
+
 // Loads the 4 edge records of group g (32-byte aligned).
 __device__ __forceinline__ void load_group(const uint2 *edges, uint32_t g,
                                            uint2 rec[4]) {

@@ -6,13 +6,13 @@
 // (ic_plain_kernel) or one warp per frontier entry (ic_fused_kernel) walks a
 // hub's in-list alone, so those sets set the kernel's length.  Here one CTA
 // grows one such set: level by level, the level's entries are taken a CTA's
-// width at a time; in-lists of at least that many 4-edge groups (hubs) are
-// swept by all threads one list at a time, and the others through their
-// concatenated groups (a block scan turns group counts into offsets; each
+// width at a time; in-lists of at least that many 8-edge coin blocks (hubs)
+// are swept by all threads one list at a time, and the others through their
+// concatenated blocks (a block scan turns block counts into offsets; each
 // thread finds its entry with a forward-only cursor in shared memory).
 // Levels are separated by __syncthreads only.  Coins are the same
-// (set, edge)-keyed Philox draws as every other sampler; on lists with a
-// uniform threshold a thread takes whole 8-edge coin blocks.
+// (set, edge)-keyed Philox draws as every other sampler; a thread takes
+// whole 8-edge coin blocks (one Philox block each).
 #include "device.cuh"
 #include "launch.h"
 
@@ -23,8 +23,8 @@ namespace {
 // Block shapes: 128, 256, 512 or 1024 threads (at 64 registers a thread: 8,
 // 4, 2 or 1 CTA per SM, each growing its own set -- smaller CTAs let one set's barrier
 // waits overlap another's work; the autotuner picks per graph).  In-lists of
-// at least BIG_THREADS 4-edge groups are swept by the whole CTA, one list at
-// a time.
+// at least BIG_THREADS coin blocks are swept by the whole CTA, one list at a
+// time.
 
 // Exclusive block scan of one u32 per thread; returns the exclusive value and
 // writes the block total to *total.  Uses `warp_tot` (BIG_WARPS entries).
@@ -52,7 +52,7 @@ __global__ void __launch_bounds__(BIG_THREADS, 1024 / BIG_THREADS)
 ic_bigset_kernel(BigLaunch L) {
   constexpr int BIG_WARPS = BIG_THREADS / 32;
   constexpr uint32_t kLongCTA = BIG_THREADS;
-  __shared__ uint32_t s_off[BIG_THREADS + 1];  // exclusive group offsets of the chunk
+  __shared__ uint32_t s_off[BIG_THREADS + 1];  // exclusive coin-block offsets of the chunk
   __shared__ uint32_t s_beg[BIG_THREADS], s_end[BIG_THREADS], s_vt[BIG_THREADS];
   __shared__ uint32_t s_warp[BIG_WARPS];
   __shared__ uint32_t s_long[BIG_THREADS];  // entries of the chunk with long in-lists
@@ -83,8 +83,6 @@ ic_bigset_kernel(BigLaunch L) {
     }
     __syncthreads();
     uint32_t lo = 0, hi = 1;
-    // Coins of group g of the in-list [ob, oe) (uniform threshold ovt, or 0:
-    // each record's own); newly reached sources go to the queue.
     // Source u of a live edge joins the set (and the queue) unless there.
     auto reach = [&](uint32_t u) {
       const uint32_t bit = 1u << (u & 31);
@@ -94,60 +92,57 @@ ic_bigset_kernel(BigLaunch L) {
         else s_overflow = 1;
       }
     };
-    // The live edges of group g given its coin block c (the group is half
-    // of the 8-edge block g >> 1) and, for a list without a uniform
-    // threshold, its records.
-    auto apply_coins = [&](uint32_t g, uint32_t ob, uint32_t oe, uint32_t ovt, const u32x4 &c,
-                           const uint2 rec[4]) {
-      const uint32_t hb = (g & 1u) << 2;
+    // The live edges of 8-edge coin block b of the in-list [ob, oe) given
+    // its coarse coins c: against the list's uniform threshold ovt (a block
+    // usually cleared by its smallest coin) or, when ovt is 0, each record's
+    // own (records two at a time; a pair past the list's end is not read:
+    // the record array ends on a 4-edge boundary); a coarse tie (one edge in
+    // 65 536) draws the fine half.  Sources of live edges are read then.
+    auto expand_block = [&](uint32_t b, uint32_t ob, uint32_t oe, uint32_t ovt, const u32x4 &c) {
       uint32_t live = 0, tie = 0;
+      if (ovt) {
+        const uint32_t th = ovt >> 16;
+        if (block_min16(c) > th) return;  // nothing live, no tie
 #pragma unroll
-      for (int t = 0; t < 4; ++t) {
-        const uint32_t ed = (g << 2) + t;
-        const uint32_t th = (ovt ? ovt : rec[t].y) >> 16, cc = coarse_of(c, hb + t);
-        if (ed >= ob && ed < oe) {
-          if (cc < th) live |= 1u << t;
-          else if (cc == th) tie |= 1u << t;
-        }
-      }
-      while (tie) {  // a coarse tie, one edge in 65 536: the fine half decides
-        const uint32_t t = __ffs(tie) - 1;
-        tie &= tie - 1;
-        const uint32_t thr = ovt ? ovt
-                                 : (t == 0 ? rec[0].y : t == 1 ? rec[1].y : t == 2 ? rec[2].y : rec[3].y);
-        if (ic_fine_call(L.key, (g << 2) + t, s) < (thr & 0xFFFFu)) live |= 1u << t;
-      }
-#pragma unroll
-      for (int t = 0; t < 4; ++t) {
-        const uint32_t ed = (g << 2) + t;
-        if (live & (1u << t)) {
-          uint32_t u = rec[t].x;
-          if (ovt) {
-            u = __ldg(&L.G.edges[ed].x);
-            atomicAdd(&s_usrc, 1ull);
+        for (int h = 0; h < 8; ++h) {
+          const uint32_t cc = coarse_of(c, h), ed = (b << 3) + h;
+          if (cc <= th && ed >= ob && ed < oe) {
+            if (cc < th) live |= 1u << h;
+            else tie |= 1u << h;
           }
-          reach(u);
         }
-      }
-    };
-    // The live edges of the 8-edge block b of a uniform-threshold list.
-    auto apply_block = [&](uint32_t b, uint32_t ob, uint32_t oe, uint32_t ovt, const u32x4 &c) {
-      const uint32_t th = ovt >> 16;
-      if (block_min16(c) > th) return;  // nothing live, no tie
+      } else {
+        const uint4 *rp = reinterpret_cast<const uint4 *>(L.G.edges + ((size_t)b << 3));
 #pragma unroll
-      for (int h = 0; h < 8; ++h) {
-        const uint32_t cc = coarse_of(c, h), ed = (b << 3) + h;
-        if (cc <= th && ed >= ob && ed < oe &&
-            (cc < th || ic_fine_call(L.key, ed, s) < (ovt & 0xFFFFu))) {
-          atomicAdd(&s_usrc, 1ull);
-          reach(__ldg(&L.G.edges[ed].x));
+        for (int qq = 0; qq < 4; ++qq) {
+          const uint32_t e0 = (b << 3) + 2 * qq;
+          if (e0 < oe && e0 + 1 >= ob) {
+            const uint4 r = __ldg(rp + qq);
+            const uint32_t c0 = coarse_of(c, 2 * qq), c1 = coarse_of(c, 2 * qq + 1);
+            if (e0 >= ob) {
+              if (c0 < (r.y >> 16)) live |= 1u << (2 * qq);
+              else if (c0 == (r.y >> 16)) tie |= 1u << (2 * qq);
+            }
+            if (e0 + 1 < oe) {
+              if (c1 < (r.w >> 16)) live |= 2u << (2 * qq);
+              else if (c1 == (r.w >> 16)) tie |= 2u << (2 * qq);
+            }
+          }
         }
       }
-    };
-    auto expand_group = [&](uint32_t g, uint32_t ob, uint32_t oe, uint32_t ovt) {
-      uint2 rec[4] = {};
-      if (!ovt) load_group(L.G.edges, g, rec);  // else: uniform threshold
-      apply_coins(g, ob, oe, ovt, ic_block(L.key, g >> 1, s), rec);
+      while (tie) {
+        const uint32_t h = __ffs(tie) - 1;
+        tie &= tie - 1;
+        const uint32_t ed = (b << 3) + h;
+        const uint32_t thr = ovt ? ovt : __ldg(&L.G.edges[ed].y);
+        if (ic_fine_call(L.key, ed, s) < (thr & 0xFFFFu)) live |= 1u << h;
+      }
+      while (live) {
+        const uint32_t ed = (b << 3) + (__ffs(live) - 1);
+        live &= live - 1;
+        if (ovt) atomicAdd(&s_usrc, 1ull);
+        reach(__ldg(&L.G.edges[ed].x));
+      }
     };
     while (lo < hi && !s_overflow) {
       for (uint32_t cb = lo; cb < hi; cb += BIG_THREADS) {
@@ -165,52 +160,46 @@ ic_bigset_kernel(BigLaunch L) {
         s_beg[tid] = beg;
         s_end[tid] = end;
         s_vt[tid] = vt;
-        const uint32_t ng = group_count(beg, end);
-        const bool lng = ng >= kLongCTA;
-        s_off[tid] = big_block_scan<BIG_THREADS>(lng ? 0u : ng, s_warp, &s_total);  // syncs
+        const uint32_t nb = block_count(beg, end);
+        const bool lng = nb >= kLongCTA;
+        s_off[tid] = big_block_scan<BIG_THREADS>(lng ? 0u : nb, s_warp, &s_total);  // syncs
         if (tid == 0) s_off[BIG_THREADS] = s_total;
         if (lng) s_long[atomicAdd(&s_nlong, 1u)] = tid;
         __syncthreads();
-        // long in-lists (hubs): all threads sweep one list at a time
+        // long in-lists (hubs): all threads sweep one list at a time, a
+        // thread taking whole coin blocks, two in flight so that their
+        // dependent Philox rounds interleave
         const uint32_t nlong = s_nlong;
         for (uint32_t li = 0; li < nlong; ++li) {
           const uint32_t a = s_long[li];
           const uint32_t ob = s_beg[a], oe = s_end[a], ovt = s_vt[a];
-          const uint32_t g_last = (oe - 1) >> 2;
-          if (ovt) {
-            // uniform threshold: nothing to load; a thread takes whole
-            // 8-edge coin blocks, two in flight so their dependent Philox
-            // rounds interleave
-            const uint32_t b_last = (oe - 1) >> 3;
-            uint32_t b = (ob >> 3) + tid;
-            for (; b + BIG_THREADS <= b_last; b += 2 * BIG_THREADS) {
-              const u32x4 c0 = ic_block(L.key, b, s);
-              const u32x4 c1 = ic_block(L.key, b + BIG_THREADS, s);
-              apply_block(b, ob, oe, ovt, c0);
-              apply_block(b + BIG_THREADS, ob, oe, ovt, c1);
-            }
-            if (b <= b_last) apply_block(b, ob, oe, ovt, ic_block(L.key, b, s));
-          } else {
-            for (uint32_t g = (ob >> 2) + tid; g <= g_last; g += BIG_THREADS)
-              expand_group(g, ob, oe, ovt);
+          const uint32_t b_last = (oe - 1) >> 3;
+          uint32_t b = (ob >> 3) + tid;
+          for (; b + BIG_THREADS <= b_last; b += 2 * BIG_THREADS) {
+            const u32x4 c0 = ic_block(L.key, b, s);
+            const u32x4 c1 = ic_block(L.key, b + BIG_THREADS, s);
+            expand_block(b, ob, oe, ovt, c0);
+            expand_block(b + BIG_THREADS, ob, oe, ovt, c1);
           }
+          if (b <= b_last) expand_block(b, ob, oe, ovt, ic_block(L.key, b, s));
         }
-        // the other lists through their concatenated groups: entry a holds
-        // group j when s_off[a] <= j < s_off[a + 1]; a thread's j only grows,
-        // so its entry cursor only moves forward
+        // the other lists through their concatenated coin blocks: entry a
+        // holds block j when s_off[a] <= j < s_off[a + 1]; a thread's j only
+        // grows, so its entry cursor only moves forward
         const uint32_t total = s_off[BIG_THREADS];
         uint32_t a = 0;
         for (uint32_t j = tid; j < total; j += BIG_THREADS) {
           if (s_off[a + 1] <= j) {
-            uint32_t b = BIG_THREADS;
-            while (b - a > 1) {
-              const uint32_t mid = (a + b) >> 1;
+            uint32_t hi2 = BIG_THREADS;
+            while (hi2 - a > 1) {
+              const uint32_t mid = (a + hi2) >> 1;
               if (s_off[mid] <= j) a = mid;
-              else b = mid;
+              else hi2 = mid;
             }
           }
           const uint32_t ob = s_beg[a];
-          expand_group((ob >> 2) + (j - s_off[a]), ob, s_end[a], s_vt[a]);
+          const uint32_t b = (ob >> 3) + (j - s_off[a]);
+          expand_block(b, ob, s_end[a], s_vt[a], ic_block(L.key, b, s));
         }
         __syncthreads();
       }

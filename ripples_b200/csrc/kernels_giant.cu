@@ -8,14 +8,13 @@
 // grid: every vertex carries a visited and a pending colour mask, and each
 // level runs as
 //   prep    : the level's frontier entries take their pending masks (for the
-//             colours that reached them last level) and count their in-edge
-//             groups;
+//             colours that reached them last level) and count their 8-edge
+//             coin blocks;
 //   scan    : exclusive scan of the group counts (one global work list);
-//   expand  : one thread per aligned 4-edge group, its owner found by one
-//             binary search per warp in the scan and a short walk per lane;
-//             for every colour of the owner's mask one
-//             Philox block (the group's half of its 8-edge coin block)
-//             gives the four edges' coarse coins; live edges OR the
+//   expand  : one thread per aligned 8-edge coin block, its owner found by
+//             one binary search per warp in the scan and a short walk per
+//             lane; for every colour of the owner's mask one Philox block
+//             gives the eight edges' coarse coins; live edges OR the
 //             colour into the source's visited mask, and colours new to it go
 //             to its pending mask and put it on the next level's frontier
 //             (once per level: a per-vertex level stamp).
@@ -71,7 +70,7 @@ __global__ void __launch_bounds__(256) giant_seed_kernel(GiantLaunch L) {
 }
 
 // Level prep: entry i of the frontier takes its vertex's pending colours and
-// counts its in-edge groups.
+// counts its 8-edge coin blocks.
 template <int CW>
 __global__ void __launch_bounds__(256) giant_prep_kernel(GiantLaunch L, uint32_t nf) {
   unsigned long long exp = 0, edges = 0, sexp = 0, sedges = 0;
@@ -88,7 +87,7 @@ __global__ void __launch_bounds__(256) giant_prep_kernel(GiantLaunch L, uint32_t
     uint32_t ng = 0;
     if (pc) {
       const uint32_t beg = __ldg(L.G.off + v), end = __ldg(L.G.off + v + 1);
-      ng = group_count(beg, end);
+      ng = block_count(beg, end);
       exp += 1;
       edges += end - beg;
       sexp += pc;
@@ -116,15 +115,13 @@ __global__ void __launch_bounds__(256) giant_expand_kernel(GiantLaunch L, uint32
   for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < total; base += stride) {
     const uint64_t j = base + threadIdx.x;
     const bool valid = j < total;
-    uint32_t u[4] = {0, 0, 0, 0};
-    uint64_t live[4][CW];
+    uint32_t u[8], thr[8];
 #pragma unroll
-    for (int t = 0; t < 4; ++t)
-#pragma unroll
-      for (int w = 0; w < CW; ++w) live[t][w] = 0;
+    for (int h = 0; h < 8; ++h) u[h] = thr[h] = 0;
+    uint32_t addm = 0;  // edges whose source gained a colour
     // owner of j: the last entry i with goff[i] <= j.  One binary search per
     // warp (for its first j), then each lane walks forward from there: the
-    // warp's 32 consecutive groups span few entries
+    // warp's 32 consecutive blocks span few entries
     uint32_t wlo = 0;
     {
       const uint64_t j0 = __shfl_sync(FULL, j, 0);
@@ -144,46 +141,74 @@ __global__ void __launch_bounds__(256) giant_expand_kernel(GiantLaunch L, uint32
       while (lo + 1 < nf && L.goff[lo + 1] <= j) ++lo;
       const uint32_t v = L.front[lo];
       const uint32_t beg = __ldg(L.G.off + v), end = __ldg(L.G.off + v + 1);
-      const uint32_t g = (beg >> 2) + (uint32_t)(j - L.goff[lo]);
-      uint2 rec[4];
-      load_group(L.G.edges, g, rec);
-      bool inr[4];
+      // an 8-edge coin block: its two 4-edge record groups (the second only
+      // when it holds an edge of this list: the record array ends on a
+      // 4-edge boundary)
+      const uint32_t b = (beg >> 3) + (uint32_t)(j - L.goff[lo]);
+      uint2 rec[8];
+      load_group(L.G.edges, 2 * b, rec);
+      if (((2 * b + 1) << 2) < end) {
+        load_group(L.G.edges, 2 * b + 1, rec + 4);
+      } else {
 #pragma unroll
-      for (int t = 0; t < 4; ++t) {
-        const uint32_t e = (g << 2) + t;
-        inr[t] = e >= beg && e < end && rec[t].y != 0u;
-        u[t] = rec[t].x;
+        for (int h = 4; h < 8; ++h) rec[h] = make_uint2(0u, 0u);
       }
-      if (inr[0] | inr[1] | inr[2] | inr[3]) {
+      uint32_t inr = 0;
+#pragma unroll
+      for (int h = 0; h < 8; ++h) {
+        const uint32_t e = (b << 3) + h;
+        if (e >= beg && e < end && rec[h].y != 0u) inr |= 1u << h;
+        u[h] = rec[h].x;
+        thr[h] = rec[h].y;
+      }
+      if (inr) {
 #pragma unroll
         for (int w = 0; w < CW; ++w) {
+          // one Philox block per colour gives the eight edges' coarse coins
+          uint64_t live[8];
+#pragma unroll
+          for (int h = 0; h < 8; ++h) live[h] = 0;
           uint64_t mm = L.masks[(size_t)lo * CW + w];
           while (mm) {
             const int bi = __ffsll((long long)mm) - 1;
             mm &= mm - 1;
             const uint64_t sid = L.set_ids[w * 64 + bi];
-            // this group's four coarse coins: half of the 8-edge block
-            const u32x4 cb = ic_block(L.key, g >> 1, sid);
-            const uint32_t hb = (g & 1u) << 2;
+            const u32x4 cb = ic_block(L.key, b, sid);
             const uint64_t bit = 1ull << bi;
             uint32_t tie = 0;
 #pragma unroll
-            for (int t = 0; t < 4; ++t) {
-              const uint32_t th = rec[t].y >> 16, cc = coarse_of(cb, hb + t);
-              if (inr[t]) {
-                if (cc < th) live[t][w] |= bit;
-                else if (cc == th) tie |= 1u << t;
+            for (int h = 0; h < 8; ++h) {
+              const uint32_t th = thr[h] >> 16, cc = coarse_of(cb, h);
+              if (inr & (1u << h)) {
+                if (cc < th) live[h] |= bit;
+                else if (cc == th) tie |= 1u << h;
               }
             }
             while (tie) {  // a coarse tie, one edge in 65 536: the fine half decides
-              const uint32_t t = __ffs(tie) - 1;
+              const uint32_t h = __ffs(tie) - 1;
               tie &= tie - 1;
-              const uint32_t thr = t == 0 ? rec[0].y : t == 1 ? rec[1].y : t == 2 ? rec[2].y : rec[3].y;
-              if (ic_fine_call(L.key, (g << 2) + t, sid) < (thr & 0xFFFFu)) {
-                if (t == 0) live[0][w] |= bit;
-                else if (t == 1) live[1][w] |= bit;
-                else if (t == 2) live[2][w] |= bit;
-                else live[3][w] |= bit;
+              uint32_t t = thr[0];
+#pragma unroll
+              for (int q = 1; q < 8; ++q)
+                if (h == (uint32_t)q) t = thr[q];
+              if (ic_fine_call(L.key, (b << 3) + h, sid) < (t & 0xFFFFu)) {
+#pragma unroll
+                for (int q = 0; q < 8; ++q)
+                  if (h == (uint32_t)q) live[q] |= bit;
+              }
+            }
+          }
+#pragma unroll
+          for (int h = 0; h < 8; ++h) {
+            // a plain read first: visited bits only get set, so colours it
+            // shows need no atomic (most live edges late in a giant BFS)
+            if (live[h] && (live[h] & ~__ldcg(&L.vis[(size_t)u[h] * CW + w]))) {
+              const uint64_t old =
+                  atomicOr((unsigned long long *)&L.vis[(size_t)u[h] * CW + w], live[h]);
+              const uint64_t add = live[h] & ~old;
+              if (add) {
+                atomicOr((unsigned long long *)&L.pend[(size_t)u[h] * CW + w], add);
+                addm |= 1u << h;
               }
             }
           }
@@ -191,26 +216,12 @@ __global__ void __launch_bounds__(256) giant_expand_kernel(GiantLaunch L, uint32
       }
     }
 #pragma unroll
-    for (int t = 0; t < 4; ++t) {
-      bool added = false;
-#pragma unroll
-      for (int w = 0; w < CW; ++w) {
-        // a plain read first: visited bits only get set, so colours it shows
-        // need no atomic (most live edges late in a giant BFS)
-        if (live[t][w] && (live[t][w] & ~__ldcg(&L.vis[(size_t)u[t] * CW + w]))) {
-          const uint64_t old =
-              atomicOr((unsigned long long *)&L.vis[(size_t)u[t] * CW + w], live[t][w]);
-          const uint64_t add = live[t][w] & ~old;
-          if (add) {
-            atomicOr((unsigned long long *)&L.pend[(size_t)u[t] * CW + w], add);
-            added = true;
-          }
-        }
-      }
+    for (int h = 0; h < 8; ++h) {
+      const bool added = (addm >> h) & 1u;
       uint32_t oldf = level + 1;
-      if (added) oldf = atomicExch(&L.pflag[u[t]], level + 1);
-      warp_append(added && oldf == 0u, u[t], L.touched, L.ctr + 1);
-      warp_append(added && oldf != level + 1, u[t], L.front_next, L.ctr + 0);
+      if (added) oldf = atomicExch(&L.pflag[u[h]], level + 1);
+      warp_append(added && oldf == 0u, u[h], L.touched, L.ctr + 1);
+      warp_append(added && oldf != level + 1, u[h], L.front_next, L.ctr + 0);
     }
   }
 }

@@ -33,9 +33,9 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
   return m;
 }
 
-// In-lists of at least this many 4-edge groups are swept by a whole warp (or
-// CTA) at a time instead of sharing it with other lists.
-constexpr uint32_t kLongGroups = 64;
+// In-lists of at least this many 8-edge coin blocks are swept by a whole
+// warp at a time instead of sharing it with other lists.
+constexpr uint32_t kLongBlocks = 32;
 
 struct WarpCtx {
   uint32_t *bm;  // visited bitmap, ceil(n/32) words
@@ -107,9 +107,9 @@ __device__ __forceinline__ SetOutcome ic_plain_set(const DevGraph &G, Key key, u
   unsigned long long set_exp = 0, set_edges = 0, warp_edges = 0;
   uint32_t set_uedges = 0, set_usrc = 0;  // a set's edges are fewer than m < 2^32
 
-  // Appends this lane's newly reached vertices of one 4-edge group to the
-  // queue (warp-wide, in lane order per edge slot); on queue overflow the set
-  // is abandoned and the bits of vertices that will never be queued cleared.
+  // Appends this lane's newly reached vertex (if any) to the queue,
+  // warp-wide in lane order; on queue overflow the set is abandoned and the
+  // bits of vertices that will never be queued cleared.
   auto append_one = [&](bool isnew, uint32_t nu) {
     const uint32_t bal = __ballot_sync(FULL, isnew);
     if (bal == 0) return;
@@ -122,73 +122,91 @@ __device__ __forceinline__ SetOutcome ic_plain_set(const DevGraph &G, Key key, u
     if (isnew) W.q[qlen + __popc(bal & lanemask_lt())] = nu;
     qlen += cnt;
   };
-  auto append = [&](const bool isnew[4], const uint32_t nu[4]) {
-#pragma unroll
-    for (int t = 0; t < 4; ++t) append_one(isnew[t], nu[t]);
-  };
-  // Draws the coins of group g of the in-list [ob, oe) (uniform threshold
-  // ovt, or 0: each record's own) from the group's half of its 8-edge coin
-  // block, marks the live sources in the bitmap and reports which were not
-  // yet there.
-  auto apply_coins = [&](uint32_t g, uint32_t ob, uint32_t oe, uint32_t ovt, const u32x4 &c,
-                         const uint2 rec[4], bool isnew[4], uint32_t nu[4]) {
-    const uint32_t hb = (g & 1u) << 2;
+  // Live edges (bit h: edge 8b + h) of 8-edge coin block b of the in-list
+  // [ob, oe): one Philox block gives the eight coarse coins, compared with
+  // the list's uniform threshold ovt (a whole block usually cleared by its
+  // smallest coin) or, when ovt is 0, with each record's own threshold; a
+  // coarse tie (one edge in 65 536) draws the fine half.
+  auto block_live = [&](uint32_t b, uint32_t ob, uint32_t oe, uint32_t ovt) -> uint32_t {
+    const u32x4 c = ic_block(key, b, s);
     uint32_t live = 0, tie = 0;
+    if (ovt) {
+      const uint32_t th = ovt >> 16;
+      if (block_min16(c) <= th) {
 #pragma unroll
-    for (int t = 0; t < 4; ++t) {
-      const uint32_t e = (g << 2) + t;
-      const uint32_t th = (ovt ? ovt : rec[t].y) >> 16, cc = coarse_of(c, hb + t);
-      if (e >= ob && e < oe) {
-        if (cc < th) live |= 1u << t;
-        else if (cc == th) tie |= 1u << t;
-      }
-    }
-    while (tie) {  // a coarse tie, one edge in 65 536: the fine half decides
-      const uint32_t t = __ffs(tie) - 1;
-      tie &= tie - 1;
-      const uint32_t thr = ovt ? ovt
-                               : (t == 0 ? rec[0].y : t == 1 ? rec[1].y : t == 2 ? rec[2].y : rec[3].y);
-      if (ic_fine_call(key, (g << 2) + t, s) < (thr & 0xFFFFu)) live |= 1u << t;
-    }
-#pragma unroll
-    for (int t = 0; t < 4; ++t) {
-      const uint32_t e = (g << 2) + t;
-      isnew[t] = false;
-      nu[t] = rec[t].x;
-      if (live & (1u << t)) {
-        if (ovt) {
-          nu[t] = __ldg(&G.edges[e].x);
-          ++set_usrc;
+        for (int h = 0; h < 8; ++h) {
+          const uint32_t cc = coarse_of(c, h), e = (b << 3) + h;
+          if (cc <= th && e >= ob && e < oe) {
+            if (cc < th) live |= 1u << h;
+            else tie |= 1u << h;
+          }
         }
-        const uint32_t bit = 1u << (nu[t] & 31);
-        const uint32_t old = atomicOr(&W.bm[nu[t] >> 5], bit);
-        isnew[t] = !(old & bit);
+      }
+    } else {
+      // records two at a time; a pair past the list's end is not read (the
+      // record array ends on a 4-edge boundary, not an 8-edge one)
+      const uint4 *rp = reinterpret_cast<const uint4 *>(G.edges + ((size_t)b << 3));
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const uint32_t e0 = (b << 3) + 2 * q;
+        if (e0 < oe && e0 + 1 >= ob) {
+          const uint4 r = __ldg(rp + q);
+          const uint32_t c0 = coarse_of(c, 2 * q), c1 = coarse_of(c, 2 * q + 1);
+          if (e0 >= ob) {
+            if (c0 < (r.y >> 16)) live |= 1u << (2 * q);
+            else if (c0 == (r.y >> 16)) tie |= 1u << (2 * q);
+          }
+          if (e0 + 1 < oe) {
+            if (c1 < (r.w >> 16)) live |= 2u << (2 * q);
+            else if (c1 == (r.w >> 16)) tie |= 2u << (2 * q);
+          }
+        }
       }
     }
+    while (tie) {
+      const uint32_t h = __ffs(tie) - 1;
+      tie &= tie - 1;
+      const uint32_t e = (b << 3) + h;
+      const uint32_t thr = ovt ? ovt : __ldg(&G.edges[e].y);
+      if (ic_fine_call(key, e, s) < (thr & 0xFFFFu)) live |= 1u << h;
+    }
+    return live;
   };
-  auto expand_group = [&](uint32_t g, uint32_t ob, uint32_t oe, uint32_t ovt, bool isnew[4],
-                          uint32_t nu[4]) {
-    uint2 rec[4] = {};
-    if (!ovt) load_group(G.edges, g, rec);
-    apply_coins(g, ob, oe, ovt, ic_block(key, g >> 1, s), rec, isnew, nu);
+  // Marks the sources of a block's live edges in the bitmap and queues the
+  // new ones: one live edge per lane per pass, every lane voting (live edges
+  // are few; a record's source is read again, from L1).
+  auto take_live = [&](uint32_t b, uint32_t live, bool uniform) {
+    while (__any_sync(FULL, live != 0)) {
+      bool isnew = false;
+      uint32_t nu = 0;
+      if (live) {
+        const uint32_t e = (b << 3) + (__ffs(live) - 1);
+        live &= live - 1;
+        nu = __ldg(&G.edges[e].x);
+        if (uniform) ++set_usrc;
+        const uint32_t bit = 1u << (nu & 31);
+        isnew = !(atomicOr(&W.bm[nu >> 5], bit) & bit);
+      }
+      append_one(isnew, nu);
+    }
   };
 
   while (head < qlen && !overflow) {
     const uint32_t take = min(32u, qlen - head);
-    uint32_t beg = 0, end = 0, ng = 0, vt = 0;
+    uint32_t beg = 0, end = 0, nb = 0, vt = 0;
     if (lane < take) {
       const uint32_t v = W.q[head + lane];
       beg = __ldg(G.off + v);
       end = __ldg(G.off + v + 1);
       if (G.vthr) vt = __ldg(G.vthr + v);
-      ng = group_count(beg, end);
+      nb = block_count(beg, end);
       set_edges += end - beg;
       if (vt) set_uedges += end - beg;
     }
     set_exp += (lane == 0) ? take : 0;
     {
-      const uint32_t all = warp_incl_scan(ng);
-      warp_edges += (unsigned long long)__shfl_sync(FULL, all, 31) * 4;
+      const uint32_t all = warp_incl_scan(nb);
+      warp_edges += (unsigned long long)__shfl_sync(FULL, all, 31) * 8;
     }
     if (work_cap && warp_edges > work_cap) {
       // too much edge work for one warp: leave the set to a whole CTA
@@ -196,70 +214,25 @@ __device__ __forceinline__ SetOutcome ic_plain_set(const DevGraph &G, Key key, u
       break;
     }
     // Long in-lists (hubs) are swept by the whole warp, one list at a time:
-    // lane j takes groups j, j + 32, ... of the list, with no owner search.
-    uint32_t longs = __ballot_sync(FULL, ng >= kLongGroups);
+    // lane j takes coin blocks j, j + 32, ... of the list, no owner search.
+    uint32_t longs = __ballot_sync(FULL, nb >= kLongBlocks);
     while (longs && !overflow) {
       const uint32_t L = __ffs(longs) - 1;
       longs &= longs - 1;
       const uint32_t lb = __shfl_sync(FULL, beg, L), le = __shfl_sync(FULL, end, L);
       const uint32_t lvt = __shfl_sync(FULL, vt, L);
-      if (lvt) {
-        // uniform threshold: lane j takes 8-edge coin blocks j, j + 32, ...
-        // (one Philox block for eight coins, no records read); the few live
-        // edges are then appended one per lane per pass
-        const uint32_t th = lvt >> 16, tf = lvt & 0xFFFFu;
-        const uint32_t b_last = (le - 1) >> 3;
-        for (uint32_t base = lb >> 3; base <= b_last && !overflow; base += 32) {
-          const uint32_t b = base + lane;
-          uint32_t live = 0, tie = 0;
-          const u32x4 c = ic_block(key, b, s);
-          if (b <= b_last && block_min16(c) <= th) {  // else: nothing live, no tie
-#pragma unroll
-            for (int h = 0; h < 8; ++h) {
-              const uint32_t cc = coarse_of(c, h), e = (b << 3) + h;
-              if (cc <= th && e >= lb && e < le) {
-                if (cc < th) live |= 1u << h;
-                else tie |= 1u << h;
-              }
-            }
-          }
-          while (tie) {  // coarse ties: the fine half decides
-            const uint32_t h = __ffs(tie) - 1;
-            tie &= tie - 1;
-            if (ic_fine_call(key, (b << 3) + h, s) < tf) live |= 1u << h;
-          }
-          while (__any_sync(FULL, live != 0)) {
-            bool isnew = false;
-            uint32_t nu = 0;
-            if (live) {
-              const uint32_t e = (b << 3) + (__ffs(live) - 1);
-              live &= live - 1;
-              nu = __ldg(&G.edges[e].x);
-              ++set_usrc;
-              const uint32_t bit = 1u << (nu & 31);
-              isnew = !(atomicOr(&W.bm[nu >> 5], bit) & bit);
-            }
-            append_one(isnew, nu);
-          }
-          __syncwarp();
-        }
-        continue;
-      }
-      const uint32_t g_last = (le - 1) >> 2;
-      for (uint32_t base = lb >> 2; base <= g_last && !overflow; base += 32) {
-        const uint32_t g = base + lane;
-        uint32_t nu[4] = {0, 0, 0, 0};
-        bool isnew[4] = {false, false, false, false};
-        if (g <= g_last) expand_group(g, lb, le, lvt, isnew, nu);
-        // live edges are rare on hub lists: one vote skips the four ballots
-        if (__any_sync(FULL, isnew[0] || isnew[1] || isnew[2] || isnew[3])) append(isnew, nu);
+      const uint32_t b_last = (le - 1) >> 3;
+      for (uint32_t base = lb >> 3; base <= b_last && !overflow; base += 32) {
+        const uint32_t b = base + lane;
+        const uint32_t live = b <= b_last ? block_live(b, lb, le, lvt) : 0u;
+        take_live(b, live, lvt != 0);
         __syncwarp();
       }
     }
-    // The shorter lists share the warp through their concatenated groups:
-    // group j belongs to the lane whose scanned range holds it.
-    const uint32_t ngs = ng >= kLongGroups ? 0u : ng;
-    const uint32_t incl = warp_incl_scan(ngs);
+    // The shorter lists share the warp through their concatenated coin
+    // blocks: block j belongs to the lane whose scanned range holds it.
+    const uint32_t nbs = nb >= kLongBlocks ? 0u : nb;
+    const uint32_t incl = warp_incl_scan(nbs);
     const uint32_t total = __shfl_sync(FULL, incl, 31);
     for (uint32_t base = 0; base < total && !overflow; base += 32) {
       const uint32_t j = base + lane;
@@ -267,12 +240,11 @@ __device__ __forceinline__ SetOutcome ic_plain_set(const DevGraph &G, Key key, u
       const uint32_t owner = warp_find_owner(incl, valid ? j : total - 1);
       const uint32_t ob = __shfl_sync(FULL, beg, owner);
       const uint32_t oe = __shfl_sync(FULL, end, owner);
-      const uint32_t oexcl = __shfl_sync(FULL, incl, owner) - __shfl_sync(FULL, ngs, owner);
+      const uint32_t oexcl = __shfl_sync(FULL, incl, owner) - __shfl_sync(FULL, nbs, owner);
       const uint32_t ovt = __shfl_sync(FULL, vt, owner);
-      uint32_t nu[4] = {0, 0, 0, 0};
-      bool isnew[4] = {false, false, false, false};
-      if (valid) expand_group((ob >> 2) + (j - oexcl), ob, oe, ovt, isnew, nu);
-      append(isnew, nu);
+      const uint32_t b = (ob >> 3) + (j - oexcl);
+      const uint32_t live = valid ? block_live(b, ob, oe, ovt) : 0u;
+      take_live(b, live, ovt != 0);
       __syncwarp();
     }
     head += take;
