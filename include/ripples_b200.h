@@ -218,7 +218,7 @@ int rip_pool_work_caps(rip_pool *p, uint64_t plain_cap, uint64_t fused_cap);
  *   3/4/5 fused 64/128/256 colours, batches past 2^23 -> heavy path
  *   6/7 as 0/2 with the one-set-per-warp kernel capped at 48 registers
  *       (40 resident warps per SM instead of 32)
- *   8 as 2 with 256-thread CTAs for the heavy sets (4 sets growing per SM
+ *   8 as 2 with 256-thread CTAs for the heavy sets (5 sets growing per SM
  *       instead of 1: the block-shape axis; candidates 0-2 use 1024-thread
  *       CTAs, 6-7 256-thread ones), 9 the same with heavy sets from 2^16
  *       in-edges
@@ -267,9 +267,9 @@ int rip_pool_plain_occupancy(rip_pool *p, int blocks_per_sm);
 int rip_pool_heavy_batch(rip_pool *p, uint32_t min_sets);
 
 /* Block shape of the one-CTA-per-set kernel for heavy IC sets: 128, 256, 512
- * or 1024 threads (default 256; an autotuned graph's pools start from its
- * tuned value).  Smaller CTAs grow more sets per SM at once, each with fewer
- * threads.  Results do not depend on it.  No reference counterpart. */
+ * or 1024 threads, 10, 5, 2 or 1 of them resident per SM (default 256; an
+ * autotuned graph's pools start from its tuned value).  Smaller CTAs grow
+ * more sets per SM at once, each with fewer threads.  Results do not depend on it.  No reference counterpart. */
 int rip_pool_heavy_block(rip_pool *p, uint32_t threads);
 
 /* Reference-heap selection (RIP_TIE_REF_HEAP): after each pick the host

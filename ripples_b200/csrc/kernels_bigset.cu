@@ -20,11 +20,12 @@ namespace rip {
 
 namespace {
 
-// Block shapes: 128, 256, 512 or 1024 threads (at 64 registers a thread: 8,
-// 4, 2 or 1 CTA per SM, each growing its own set -- smaller CTAs let one set's barrier
-// waits overlap another's work; the autotuner picks per graph).  In-lists of
-// at least BIG_THREADS coin blocks are swept by the whole CTA, one list at a
-// time.
+// Block shapes: 128, 256, 512 or 1024 threads, kBigCtasPerSm of them
+// resident per SM (10, 5, 2 or 1: at most 48, 48, 64 or 64 registers a
+// thread), each growing its own set -- more resident CTAs let one set's
+// barrier waits overlap another's work; the autotuner picks the shape per
+// graph.  In-lists of at least BIG_THREADS coin blocks are swept by the
+// whole CTA, one list at a time.
 
 // Exclusive block scan of one u32 per thread; returns the exclusive value and
 // writes the block total to *total.  Uses `warp_tot` (BIG_WARPS entries).
@@ -48,7 +49,7 @@ __device__ uint32_t big_block_scan(uint32_t x, uint32_t *warp_tot, uint32_t *tot
 }
 
 template <int BIG_THREADS>
-__global__ void __launch_bounds__(BIG_THREADS, 1024 / BIG_THREADS)
+__global__ void __launch_bounds__(BIG_THREADS, kBigCtasPerSm(BIG_THREADS))
 ic_bigset_kernel(BigLaunch L) {
   constexpr int BIG_WARPS = BIG_THREADS / 32;
   constexpr uint32_t kLongCTA = BIG_THREADS;

@@ -130,6 +130,11 @@ struct BigLaunch {
   int blocks = 0;
   int threads = 1024;             // block shape: 256, 512 or 1024
 };
+// Resident CTAs per SM of each heavy-set block shape (the kernel's launch
+// bounds and the number of heavy-set scratch slots per SM).
+constexpr int kBigCtasPerSm(int threads) {
+  return threads == 128 ? 10 : threads == 256 ? 5 : threads == 512 ? 2 : 1;
+}
 void launch_ic_bigset(const BigLaunch &L, cudaStream_t stream);
 
 // Forward spread simulation (kernels_spread.cu): one CTA per replica.

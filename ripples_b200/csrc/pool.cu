@@ -427,8 +427,8 @@ static int sample_big(rip_pool *p, uint64_t seed, uint64_t first,
     const size_t per = bm_words * 4 + (size_t)q * 4;
     size_t avail = c->budget > c->used ? c->budget - c->used : 0;
     avail += p->b_scratch.bytes;
-    // one slot per resident CTA: 1024 / big_threads of them per SM
-    const uint64_t max_slots = (uint64_t)c->num_sms * (1024u / p->big_threads);
+    // one slot per resident CTA
+    const uint64_t max_slots = (uint64_t)c->num_sms * kBigCtasPerSm((int)p->big_threads);
     return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(max_slots, (avail / 4) / per));
   };
   TRY(ensure_big_scratch(p, slots_for(qcap), qcap));
