@@ -47,6 +47,8 @@
 //   lt_threshold(s, v)  = P(v, 0, s_lo, LT<<24 | s_hi)[0]
 //   IC edge e live for set s  <=>  coin(s, e) < thr[e]
 //   thr[e] = clamp(floor(w_e * 2^32), 0, 2^32-1)
+//   forward spread, replica r: sim_coin(r, e) as coin(s, e) with r for s
+//   and the SIM_IC / SIM_IC_FINE domains
 //   LT: first in-edge j of v (CSR order) with threshold < cum[j],
 //       W_i = floor(clamp(w_i, 0, 2) * 2^40)            (exact, 64-bit)
 //       cum[j] = min(min(sum_{i<=j} W_i, 2^41) >> 8, 2^32-1)
@@ -69,7 +71,7 @@ namespace {
 
 enum : uint32_t {
   DOM_ROOT = 1, DOM_IC = 2, DOM_LT = 3, DOM_RMAT = 4, DOM_ER = 5, DOM_WEIGHT = 6,
-  DOM_SIM_IC = 7, DOM_SIM_LT = 8, DOM_IC_FINE = 9
+  DOM_SIM_IC = 7, DOM_SIM_LT = 8, DOM_IC_FINE = 9, DOM_SIM_IC_FINE = 10
 };
 
 void philox4x32_10(const uint32_t ctr_in[4], const uint32_t key_in[2],
@@ -152,17 +154,36 @@ bool ic_live(uint64_t seed, uint64_t s, uint64_t e, uint32_t thr) {
   return c < th || (c == th && ic_fine(seed, s, e) < (thr & 0xFFFFu));
 }
 
-// Forward spread simulation coin of edge e in replica r (its own domain).
-uint32_t sim_ic_coin(uint64_t seed, uint64_t r, uint64_t e) {
+// Forward spread simulation coin of edge e in replica r (its own domains):
+// coarse << 16 | fine, as ic_coin.
+uint32_t sim_ic_coarse(uint64_t seed, uint64_t r, uint64_t e) {
   uint32_t key[2], ctr[4], out[4];
   make_key(seed, key);
-  uint64_t g = e >> 2;
-  ctr[0] = (uint32_t)g;
-  ctr[1] = (uint32_t)(g >> 32);
+  const uint64_t b = e >> 3;
+  ctr[0] = (uint32_t)b;
+  ctr[1] = (uint32_t)(b >> 32);
   ctr[2] = (uint32_t)r;
   ctr[3] = (DOM_SIM_IC << 24) | (uint32_t)((r >> 32) & 0xFFFFFFu);
   philox4x32_10(ctr, key, out);
-  return out[e & 3];
+  const uint32_t w = out[(e >> 1) & 3];
+  return (e & 1) ? (w >> 16) : (w & 0xFFFFu);
+}
+
+uint32_t sim_ic_fine(uint64_t seed, uint64_t r, uint64_t e) {
+  uint32_t key[2], ctr[4], out[4];
+  make_key(seed, key);
+  ctr[0] = (uint32_t)e;
+  ctr[1] = (uint32_t)(e >> 32);
+  ctr[2] = (uint32_t)r;
+  ctr[3] = (DOM_SIM_IC_FINE << 24) | (uint32_t)((r >> 32) & 0xFFFFFFu);
+  philox4x32_10(ctr, key, out);
+  return out[0] & 0xFFFFu;
+}
+
+// sim coin(r, e) < thr, drawing the fine half only on a coarse tie.
+bool sim_ic_live(uint64_t seed, uint64_t r, uint64_t e, uint32_t thr) {
+  const uint32_t c = sim_ic_coarse(seed, r, e), th = thr >> 16;
+  return c < th || (c == th && sim_ic_fine(seed, r, e) < (thr & 0xFFFFu));
 }
 
 // Forward LT spread: the threshold of vertex v in replica r (its own domain).
@@ -559,7 +580,7 @@ void *orc_sample(int model, uint32_t n, const uint64_t *index,
 
 // Forward IC spread: replica r is a BFS from the seeds over the forward CSR
 // (index over sources, dst[e] the target of out-edge e) in which edge e fires
-// iff sim_ic_coin(seed, r, e) < thr[e]; sizes[r] = vertices reached, seeds
+// iff sim_ic_live(seed, r, e, thr[e]); sizes[r] = vertices reached, seeds
 // included (include/ripples/diffusion_simulation.h:73-127).  Returns the sum
 // of the sizes; *edges (optional) = out-edges of reached vertices, summed.
 uint64_t orc_spread_ic(uint32_t n, const uint64_t *index, const uint32_t *dst,
@@ -586,7 +607,7 @@ uint64_t orc_spread_ic(uint32_t n, const uint64_t *index, const uint32_t *dst,
         for (uint64_t e = index[u]; e < index[u + 1]; ++e) {
           const uint32_t v = dst[e];
           if (stamp[v] == r) continue;  // coins are pure: skipping is exact
-          if (sim_ic_coin(seed, r, e) < thr[e]) {
+          if (sim_ic_live(seed, r, e, thr[e])) {
             stamp[v] = r;
             queue.push_back(v);
           }

@@ -103,6 +103,70 @@ __device__ __forceinline__ uint32_t block_count(uint32_t beg, uint32_t end) {
   return end > beg ? ((end - 1) >> 3) - (beg >> 3) + 1 : 0;
 }
 
+// Coin blocks of a launch: from the key (its schedule added in registers)
+// or from round keys the kernel keeps in parameter space.
+struct KeyCoins {
+  Key k;
+  __device__ __forceinline__ u32x4 block(uint64_t b, uint64_t s) const { return ic_block(k, b, s); }
+};
+struct RoundKeyCoins {
+  const RoundKeys &rk;
+  __device__ __forceinline__ u32x4 block(uint64_t b, uint64_t s) const {
+    return ic_block_rk(rk, b, s);
+  }
+};
+
+// Live edges (bit h: edge 8b + h) of 8-edge coin block b of the in-list
+// [ob, oe) for set s, given the block's coarse coins c: compared with the
+// list's uniform threshold ovt (a whole block usually cleared by its smallest
+// coin) or, when ovt is 0, with each record's own threshold (records read two
+// at a time; a pair past the list's end is not read: the record array ends
+// on a 4-edge boundary, not an 8-edge one).  A coarse tie (one edge in
+// 65 536) draws the fine half.
+__device__ __forceinline__ uint32_t ic_block_live(const DevGraph &G, Key key, uint64_t s,
+                                                  uint32_t b, uint32_t ob, uint32_t oe,
+                                                  uint32_t ovt, const u32x4 &c) {
+  uint32_t live = 0, tie = 0;
+  if (ovt) {
+    const uint32_t th = ovt >> 16;
+    if (block_min16(c) > th) return 0u;
+#pragma unroll
+    for (int h = 0; h < 8; ++h) {
+      const uint32_t cc = coarse_of(c, h), e = (b << 3) + h;
+      if (cc <= th && e >= ob && e < oe) {
+        if (cc < th) live |= 1u << h;
+        else tie |= 1u << h;
+      }
+    }
+  } else {
+    const uint4 *rp = reinterpret_cast<const uint4 *>(G.edges + ((size_t)b << 3));
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const uint32_t e0 = (b << 3) + 2 * q;
+      if (e0 < oe && e0 + 1 >= ob) {
+        const uint4 r = __ldg(rp + q);
+        const uint32_t c0 = coarse_of(c, 2 * q), c1 = coarse_of(c, 2 * q + 1);
+        if (e0 >= ob) {
+          if (c0 < (r.y >> 16)) live |= 1u << (2 * q);
+          else if (c0 == (r.y >> 16)) tie |= 1u << (2 * q);
+        }
+        if (e0 + 1 < oe) {
+          if (c1 < (r.w >> 16)) live |= 2u << (2 * q);
+          else if (c1 == (r.w >> 16)) tie |= 2u << (2 * q);
+        }
+      }
+    }
+  }
+  while (tie) {
+    const uint32_t h = __ffs(tie) - 1;
+    tie &= tie - 1;
+    const uint32_t e = (b << 3) + h;
+    const uint32_t thr = ovt ? ovt : __ldg(&G.edges[e].y);
+    if (ic_fine_call(key, e, s) < (thr & 0xFFFFu)) live |= 1u << h;
+  }
+  return live;
+}
+
 // Loads the 4 edge records of group g (32-byte aligned).
 __device__ __forceinline__ void load_group(const uint2 *edges, uint32_t g,
                                            uint2 rec[4]) {

@@ -50,7 +50,7 @@ __device__ uint32_t big_block_scan(uint32_t x, uint32_t *warp_tot, uint32_t *tot
 
 template <int BIG_THREADS>
 __global__ void __launch_bounds__(BIG_THREADS, kBigCtasPerSm(BIG_THREADS))
-ic_bigset_kernel(BigLaunch L) {
+ic_bigset_kernel(const __grid_constant__ BigLaunch L) {
   constexpr int BIG_WARPS = BIG_THREADS / 32;
   constexpr uint32_t kLongCTA = BIG_THREADS;
   __shared__ uint32_t s_off[BIG_THREADS + 1];  // exclusive coin-block offsets of the chunk
@@ -93,51 +93,10 @@ ic_bigset_kernel(BigLaunch L) {
         else s_overflow = 1;
       }
     };
-    // The live edges of 8-edge coin block b of the in-list [ob, oe) given
-    // its coarse coins c: against the list's uniform threshold ovt (a block
-    // usually cleared by its smallest coin) or, when ovt is 0, each record's
-    // own (records two at a time; a pair past the list's end is not read:
-    // the record array ends on a 4-edge boundary); a coarse tie (one edge in
-    // 65 536) draws the fine half.  Sources of live edges are read then.
+    // The live edges of 8-edge coin block b of the in-list [ob, oe) given its
+    // coarse coins c; their sources are read then and reached.
     auto expand_block = [&](uint32_t b, uint32_t ob, uint32_t oe, uint32_t ovt, const u32x4 &c) {
-      uint32_t live = 0, tie = 0;
-      if (ovt) {
-        const uint32_t th = ovt >> 16;
-        if (block_min16(c) > th) return;  // nothing live, no tie
-#pragma unroll
-        for (int h = 0; h < 8; ++h) {
-          const uint32_t cc = coarse_of(c, h), ed = (b << 3) + h;
-          if (cc <= th && ed >= ob && ed < oe) {
-            if (cc < th) live |= 1u << h;
-            else tie |= 1u << h;
-          }
-        }
-      } else {
-        const uint4 *rp = reinterpret_cast<const uint4 *>(L.G.edges + ((size_t)b << 3));
-#pragma unroll
-        for (int qq = 0; qq < 4; ++qq) {
-          const uint32_t e0 = (b << 3) + 2 * qq;
-          if (e0 < oe && e0 + 1 >= ob) {
-            const uint4 r = __ldg(rp + qq);
-            const uint32_t c0 = coarse_of(c, 2 * qq), c1 = coarse_of(c, 2 * qq + 1);
-            if (e0 >= ob) {
-              if (c0 < (r.y >> 16)) live |= 1u << (2 * qq);
-              else if (c0 == (r.y >> 16)) tie |= 1u << (2 * qq);
-            }
-            if (e0 + 1 < oe) {
-              if (c1 < (r.w >> 16)) live |= 2u << (2 * qq);
-              else if (c1 == (r.w >> 16)) tie |= 2u << (2 * qq);
-            }
-          }
-        }
-      }
-      while (tie) {
-        const uint32_t h = __ffs(tie) - 1;
-        tie &= tie - 1;
-        const uint32_t ed = (b << 3) + h;
-        const uint32_t thr = ovt ? ovt : __ldg(&L.G.edges[ed].y);
-        if (ic_fine_call(L.key, ed, s) < (thr & 0xFFFFu)) live |= 1u << h;
-      }
+      uint32_t live = ic_block_live(L.G, L.key, s, b, ob, oe, ovt, c);
       while (live) {
         const uint32_t ed = (b << 3) + (__ffs(live) - 1);
         live &= live - 1;
@@ -177,12 +136,12 @@ ic_bigset_kernel(BigLaunch L) {
           const uint32_t b_last = (oe - 1) >> 3;
           uint32_t b = (ob >> 3) + tid;
           for (; b + BIG_THREADS <= b_last; b += 2 * BIG_THREADS) {
-            const u32x4 c0 = ic_block(L.key, b, s);
-            const u32x4 c1 = ic_block(L.key, b + BIG_THREADS, s);
+            const u32x4 c0 = ic_block_rk(L.rk, b, s);
+            const u32x4 c1 = ic_block_rk(L.rk, b + BIG_THREADS, s);
             expand_block(b, ob, oe, ovt, c0);
             expand_block(b + BIG_THREADS, ob, oe, ovt, c1);
           }
-          if (b <= b_last) expand_block(b, ob, oe, ovt, ic_block(L.key, b, s));
+          if (b <= b_last) expand_block(b, ob, oe, ovt, ic_block_rk(L.rk, b, s));
         }
         // the other lists through their concatenated coin blocks: entry a
         // holds block j when s_off[a] <= j < s_off[a + 1]; a thread's j only
@@ -200,7 +159,7 @@ ic_bigset_kernel(BigLaunch L) {
           }
           const uint32_t ob = s_beg[a];
           const uint32_t b = (ob >> 3) + (j - s_off[a]);
-          expand_block(b, ob, s_end[a], s_vt[a], ic_block(L.key, b, s));
+          expand_block(b, ob, s_end[a], s_vt[a], ic_block_rk(L.rk, b, s));
         }
         __syncthreads();
       }
@@ -263,8 +222,10 @@ ic_bigset_kernel(BigLaunch L) {
 
 }  // namespace
 
-void launch_ic_bigset(const BigLaunch &L, cudaStream_t stream) {
+void launch_ic_bigset(const BigLaunch &L0, cudaStream_t stream) {
   count_launches(1);
+  BigLaunch L = L0;
+  L.rk = round_keys(L.key);
   if (L.threads == 128)
     ic_bigset_kernel<128><<<L.blocks, 128, 0, stream>>>(L);
   else if (L.threads == 256)

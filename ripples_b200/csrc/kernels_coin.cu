@@ -16,13 +16,14 @@ namespace rip {
 namespace {
 
 __global__ void __launch_bounds__(256)
-coin_rate_kernel(Key key, uint32_t blocks_per_thread, uint32_t thr, unsigned long long *live) {
+coin_rate_kernel(const __grid_constant__ RoundKeys rk, Key key, uint32_t blocks_per_thread,
+                 uint32_t thr, unsigned long long *live) {
   const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   const uint64_t s = tid;                                 // one set per thread
   const uint64_t b0 = tid * (uint64_t)blocks_per_thread;  // its own coin blocks
   uint32_t cnt = 0;
   for (uint32_t i = 0; i < blocks_per_thread; ++i) {
-    const u32x4 c = ic_block(key, b0 + i, s);
+    const u32x4 c = ic_block_rk(rk, b0 + i, s);
     if (block_min16(c) <= (thr >> 16)) {  // as the samplers: most blocks stop here
 #pragma unroll
       for (int h = 0; h < 8; ++h)
@@ -46,12 +47,13 @@ extern "C" int rip_coin_rate(rip_ctx *c, double *coins_per_s) {
   const int blocks = c->num_sms * 8;  // 64 resident warps per SM
   const uint32_t cblocks = 1024;
   const Key key = make_key(0x5EEDull);
+  const RoundKeys rk = round_keys(key);
   CK(c, cudaMemsetAsync(live.p, 0, sizeof(unsigned long long), c->stream));
   count_launches(2);
-  coin_rate_kernel<<<blocks, 256, 0, c->stream>>>(key, cblocks, 1u << 20,
+  coin_rate_kernel<<<blocks, 256, 0, c->stream>>>(rk, key, cblocks, 1u << 20,
                                                   ptr<unsigned long long>(live));
   CK(c, cudaEventRecord(c->ev0, c->stream));
-  coin_rate_kernel<<<blocks, 256, 0, c->stream>>>(key, cblocks, 1u << 20,
+  coin_rate_kernel<<<blocks, 256, 0, c->stream>>>(rk, key, cblocks, 1u << 20,
                                                   ptr<unsigned long long>(live));
   CK(c, cudaEventRecord(c->ev1, c->stream));
   CK(c, cudaEventSynchronize(c->ev1));

@@ -108,8 +108,8 @@ __global__ void __launch_bounds__(256) giant_prep_kernel(GiantLaunch L, uint32_t
 }
 
 template <int CW>
-__global__ void __launch_bounds__(256) giant_expand_kernel(GiantLaunch L, uint32_t nf,
-                                                           uint32_t level) {
+__global__ void __launch_bounds__(256) giant_expand_kernel(const __grid_constant__ GiantLaunch L,
+                                                           uint32_t nf, uint32_t level) {
   const uint64_t total = L.goff[nf];
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < total; base += stride) {
@@ -173,7 +173,7 @@ __global__ void __launch_bounds__(256) giant_expand_kernel(GiantLaunch L, uint32
             const int bi = __ffsll((long long)mm) - 1;
             mm &= mm - 1;
             const uint64_t sid = L.set_ids[w * 64 + bi];
-            const u32x4 cb = ic_block(L.key, b, sid);
+            const u32x4 cb = ic_block_rk(L.rk, b, sid);
             const uint64_t bit = 1ull << bi;
             uint32_t tie = 0;
 #pragma unroll
@@ -330,8 +330,10 @@ static void giant_launch(int what, const GiantLaunch &L, uint32_t n_items, uint3
   }
 }
 
-void launch_giant(int what, int cw, const GiantLaunch &L, uint32_t n_items, uint32_t level,
+void launch_giant(int what, int cw, const GiantLaunch &L0, uint32_t n_items, uint32_t level,
                   int blocks, cudaStream_t s) {
+  GiantLaunch L = L0;
+  L.rk = round_keys(L.key);
   if (cw == 1) giant_launch<1>(what, L, n_items, level, blocks, s);
   else if (cw == 2) giant_launch<2>(what, L, n_items, level, blocks, s);
   else giant_launch<4>(what, L, n_items, level, blocks, s);

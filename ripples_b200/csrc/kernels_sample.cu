@@ -93,8 +93,10 @@ struct SetOutcome {
 // One IC set: reverse BFS from root(s) over live in-edges, warp-cooperative,
 // members in discovery order in W.q.  Sets past `work_cap` in-edges (when
 // nonzero) are abandoned with big = true.
-__device__ __forceinline__ SetOutcome ic_plain_set(const DevGraph &G, Key key, uint64_t s,
-                                                   const WarpCtx &W, uint64_t work_cap) {
+template <class Coins>
+__device__ __forceinline__ SetOutcome ic_plain_set(const DevGraph &G, Key key, const Coins &coins,
+                                                   uint64_t s, const WarpCtx &W,
+                                                   uint64_t work_cap) {
   const uint32_t lane = lane_id();
   const uint32_t root = root_of(key, s, G.n);
   if (lane == 0) {
@@ -122,55 +124,8 @@ __device__ __forceinline__ SetOutcome ic_plain_set(const DevGraph &G, Key key, u
     if (isnew) W.q[qlen + __popc(bal & lanemask_lt())] = nu;
     qlen += cnt;
   };
-  // Live edges (bit h: edge 8b + h) of 8-edge coin block b of the in-list
-  // [ob, oe): one Philox block gives the eight coarse coins, compared with
-  // the list's uniform threshold ovt (a whole block usually cleared by its
-  // smallest coin) or, when ovt is 0, with each record's own threshold; a
-  // coarse tie (one edge in 65 536) draws the fine half.
   auto block_live = [&](uint32_t b, uint32_t ob, uint32_t oe, uint32_t ovt) -> uint32_t {
-    const u32x4 c = ic_block(key, b, s);
-    uint32_t live = 0, tie = 0;
-    if (ovt) {
-      const uint32_t th = ovt >> 16;
-      if (block_min16(c) <= th) {
-#pragma unroll
-        for (int h = 0; h < 8; ++h) {
-          const uint32_t cc = coarse_of(c, h), e = (b << 3) + h;
-          if (cc <= th && e >= ob && e < oe) {
-            if (cc < th) live |= 1u << h;
-            else tie |= 1u << h;
-          }
-        }
-      }
-    } else {
-      // records two at a time; a pair past the list's end is not read (the
-      // record array ends on a 4-edge boundary, not an 8-edge one)
-      const uint4 *rp = reinterpret_cast<const uint4 *>(G.edges + ((size_t)b << 3));
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const uint32_t e0 = (b << 3) + 2 * q;
-        if (e0 < oe && e0 + 1 >= ob) {
-          const uint4 r = __ldg(rp + q);
-          const uint32_t c0 = coarse_of(c, 2 * q), c1 = coarse_of(c, 2 * q + 1);
-          if (e0 >= ob) {
-            if (c0 < (r.y >> 16)) live |= 1u << (2 * q);
-            else if (c0 == (r.y >> 16)) tie |= 1u << (2 * q);
-          }
-          if (e0 + 1 < oe) {
-            if (c1 < (r.w >> 16)) live |= 2u << (2 * q);
-            else if (c1 == (r.w >> 16)) tie |= 2u << (2 * q);
-          }
-        }
-      }
-    }
-    while (tie) {
-      const uint32_t h = __ffs(tie) - 1;
-      tie &= tie - 1;
-      const uint32_t e = (b << 3) + h;
-      const uint32_t thr = ovt ? ovt : __ldg(&G.edges[e].y);
-      if (ic_fine_call(key, e, s) < (thr & 0xFFFFu)) live |= 1u << h;
-    }
-    return live;
+    return ic_block_live(G, key, s, b, ob, oe, ovt, coins.block(b, s));
   };
   // Marks the sources of a block's live edges in the bitmap and queues the
   // new ones: one live edge per lane per pass, every lane voting (live edges
@@ -338,7 +293,8 @@ __device__ __forceinline__ SetOutcome lt_walk_set(const DevGraph &G, Key key, ui
 // autotuner picks per graph).
 template <int MINB>
 __global__ void __launch_bounds__(256, MINB)
-ic_plain_kernel(DevGraph G, DevPool P, Key key, uint64_t first, uint32_t count,
+ic_plain_kernel(DevGraph G, DevPool P, Key key, const __grid_constant__ RoundKeys rk,
+                uint64_t first, uint32_t count,
                 const uint32_t *ids, unsigned int *next, uint32_t *bitmaps,
                 uint64_t bm_words, uint32_t *queues, uint32_t qcap,
                 uint64_t work_cap, FailList F, Stats st) {
@@ -354,7 +310,7 @@ ic_plain_kernel(DevGraph G, DevPool P, Key key, uint64_t first, uint32_t count,
     if (idx >= count) break;
     const uint32_t rel = ids ? ids[idx] : idx;
     const uint64_t s = first + rel;
-    const SetOutcome o = ic_plain_set(G, key, s, W, work_cap);
+    const SetOutcome o = ic_plain_set(G, key, RoundKeyCoins{rk}, s, W, work_cap);
     if (finish_set(W, o.qlen, o.overflow, s, rel, P, F, o.big)) {
       n_sets += (lane == 0);
       n_elems += (lane == 0) ? o.qlen : 0;
@@ -473,7 +429,7 @@ multi_sample_kernel(MultiLaunch L) {
     const InstanceDesc &D = L.inst[a];
     const uint32_t rel = idx - L.prefix[a];
     const uint64_t s = D.first + rel;
-    const SetOutcome o = D.model == RIP_MODEL_IC ? ic_plain_set(D.G, D.key, s, W, D.work_cap)
+    const SetOutcome o = D.model == RIP_MODEL_IC ? ic_plain_set(D.G, D.key, KeyCoins{D.key}, s, W, D.work_cap)
                                                  : lt_walk_set(D.G, D.key, s, W);
     if (store_set(W, o.qlen, o.overflow, s, D.P, D.first_bad, D.model == RIP_MODEL_IC)) {
       n_sets += 1;
@@ -499,13 +455,14 @@ void launch_multi_sample(const MultiLaunch &L, cudaStream_t stream) {
 
 void launch_ic_plain(const SampleLaunch &L, cudaStream_t stream) {
   count_launches(1);
+  const RoundKeys rk = round_keys(L.key);
   if (L.occupancy == 5)
     ic_plain_kernel<5><<<L.blocks, L.threads, 0, stream>>>(
-        L.G, L.P, L.key, L.first, L.count, L.ids, L.next, L.bitmaps, L.bm_words,
+        L.G, L.P, L.key, rk, L.first, L.count, L.ids, L.next, L.bitmaps, L.bm_words,
         L.queues, L.qcap, L.work_cap, L.F, L.st);
   else
     ic_plain_kernel<4><<<L.blocks, L.threads, 0, stream>>>(
-        L.G, L.P, L.key, L.first, L.count, L.ids, L.next, L.bitmaps, L.bm_words,
+        L.G, L.P, L.key, rk, L.first, L.count, L.ids, L.next, L.bitmaps, L.bm_words,
         L.queues, L.qcap, L.work_cap, L.F, L.st);
 }
 

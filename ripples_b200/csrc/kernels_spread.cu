@@ -5,10 +5,12 @@
 // by tools/simulator.cc); the spread is the number of vertices reached,
 // seeds included.  Here one 1024-thread CTA runs one replica at a time with
 // the level loop of the one-CTA-per-heavy-set sampler: a level's entries are
-// taken 1024 at a time, a block scan turns their 4-edge group counts into
-// offsets and all warps stride over the concatenated groups of out-edges.
-//   IC: out-edge e of a reached vertex fires in replica r iff
-//       sim_ic_coins(key, e >> 2, r)[e & 3] < threshold(e) (BFS over live
+// taken 1024 at a time, a block scan turns their out-edge unit counts into
+// offsets and all warps stride over the concatenated units (IC: 8-edge coin
+// blocks, one Philox block each; LT: 4-edge record groups).
+//   IC: out-edge e of a reached vertex fires in replica r iff its coin
+//       (coarse half from sim_ic_block(key, e >> 3, r), fine half from
+//       sim_ic_fine on a coarse tie) is below threshold(e) (BFS over live
 //       edges, diffusion_simulation.h:73-127).
 //   LT: the live-edge form of the threshold model (Kempe, Kleinberg, Tardos,
 //       KDD'03): vertex v keeps at most one in-edge -- the first j of its
@@ -112,7 +114,7 @@ spread_kernel(SpreadLaunch L) {
         }
         s_beg[tid] = beg;
         s_end[tid] = end;
-        const uint32_t ng = group_count(beg, end);
+        const uint32_t ng = LT ? group_count(beg, end) : block_count(beg, end);
         s_off[tid] = sim_block_scan(ng, s_warp, &s_total);
         if (tid == 0) s_off[SIM_THREADS] = s_total;
         __syncthreads();
@@ -125,10 +127,10 @@ spread_kernel(SpreadLaunch L) {
             else b = mid;
           }
           const uint32_t ob = s_beg[a], oe = s_end[a];
-          const uint32_t g = (ob >> 2) + (j - s_off[a]);
-          uint2 rec[4];
-          load_group(L.G.edges, g, rec);
           if (LT) {
+            const uint32_t g = (ob >> 2) + (j - s_off[a]);
+            uint2 rec[4];
+            load_group(L.G.edges, g, rec);
             const uint32_t from = s_v[a];
 #pragma unroll
             for (int t = 0; t < 4; ++t) {
@@ -145,17 +147,43 @@ spread_kernel(SpreadLaunch L) {
               }
             }
           } else {
-            const u32x4 c = sim_ic_coins(L.key, g, r);
+            // an 8-edge coin block: records two at a time (a pair past the
+            // list's end is not read: the record array ends on a 4-edge
+            // boundary), coarse coins first, the fine half on a tie
+            const uint32_t b = (ob >> 3) + (j - s_off[a]);
+            const u32x4 c = sim_ic_block(L.key, b, r);
+            const uint4 *rp = reinterpret_cast<const uint4 *>(L.G.edges + ((size_t)b << 3));
+            uint32_t live = 0, tie = 0;
 #pragma unroll
-            for (int t = 0; t < 4; ++t) {
-              const uint32_t ed = (g << 2) + t;
-              if (ed >= ob && ed < oe && lane_of(c, t) < rec[t].y) {
-                const uint32_t u = rec[t].x;
-                const uint32_t bit = 1u << (u & 31);
-                if (!(atomicOr(&bm[u >> 5], bit) & bit)) {
-                  const uint32_t pos = atomicAdd(&s_qlen, 1u);
-                  if (pos < L.qcap) q[pos] = u;
+            for (int qq = 0; qq < 4; ++qq) {
+              const uint32_t e0 = (b << 3) + 2 * qq;
+              if (e0 < oe && e0 + 1 >= ob) {
+                const uint4 rr = __ldg(rp + qq);
+                const uint32_t c0 = coarse_of(c, 2 * qq), c1 = coarse_of(c, 2 * qq + 1);
+                if (e0 >= ob) {
+                  if (c0 < (rr.y >> 16)) live |= 1u << (2 * qq);
+                  else if (c0 == (rr.y >> 16)) tie |= 1u << (2 * qq);
                 }
+                if (e0 + 1 < oe) {
+                  if (c1 < (rr.w >> 16)) live |= 2u << (2 * qq);
+                  else if (c1 == (rr.w >> 16)) tie |= 2u << (2 * qq);
+                }
+              }
+            }
+            while (tie) {
+              const uint32_t h = __ffs(tie) - 1;
+              tie &= tie - 1;
+              const uint32_t ed = (b << 3) + h;
+              if (sim_ic_fine(L.key, ed, r) < (__ldg(&L.G.edges[ed].y) & 0xFFFFu))
+                live |= 1u << h;
+            }
+            while (live) {
+              const uint32_t u = __ldg(&L.G.edges[(b << 3) + (__ffs(live) - 1)].x);
+              live &= live - 1;
+              const uint32_t bit = 1u << (u & 31);
+              if (!(atomicOr(&bm[u >> 5], bit) & bit)) {
+                const uint32_t pos = atomicAdd(&s_qlen, 1u);
+                if (pos < L.qcap) q[pos] = u;
               }
             }
           }

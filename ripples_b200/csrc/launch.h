@@ -42,13 +42,14 @@ struct GiantLaunch {
   DevGraph G;
   DevPool P;
   Key key;
+  RoundKeys rk{};                      // round_keys(key), filled by launch_giant
   const uint64_t *set_ids = nullptr;   // ncol set ids (colour c = set_ids[c])
   uint32_t ncol = 0;
   uint64_t *vis = nullptr, *pend = nullptr;  // n * cw words each, zero between batches
   uint32_t *pflag = nullptr;           // n, zero between batches
   uint32_t *front = nullptr, *front_next = nullptr, *touched = nullptr;  // n each
   uint64_t *masks = nullptr;           // n * cw: the current level's colours per entry
-  uint32_t *ng = nullptr;              // n: in-edge groups per entry
+  uint32_t *ng = nullptr;              // n: coin blocks per entry
   uint64_t *goff = nullptr;            // n + 1: exclusive scan of ng
   unsigned int *ctr = nullptr;         // [0] next-frontier tail, [1] touched count
   uint32_t *sizes = nullptr, *fill = nullptr;  // per colour
@@ -117,6 +118,7 @@ struct BigLaunch {
   DevGraph G{};
   DevPool P{};
   Key key{};
+  RoundKeys rk{};                 // round_keys(key), filled by launch_ic_bigset
   uint64_t first = 0;
   uint32_t count = 0;             // entries of ids
   const uint32_t *ids = nullptr;  // set indices relative to first
@@ -128,7 +130,7 @@ struct BigLaunch {
   FailList F{};
   Stats st{};
   int blocks = 0;
-  int threads = 1024;             // block shape: 256, 512 or 1024
+  int threads = 1024;             // block shape: 128, 256, 512 or 1024
 };
 // Resident CTAs per SM of each heavy-set block shape (the kernel's launch
 // bounds and the number of heavy-set scratch slots per SM).

@@ -24,7 +24,9 @@
 // (s_hi = bits 32..55 of the set id; set ids are limited to 2^56.)
 // Forward Monte Carlo spread simulation draws from domains of its own, keyed
 // by the replica id r instead of a set id:
-//   sim_coin(r, e)     = P(g_lo, g_hi, r_lo, SIM_IC<<24 | r_hi)[e & 3]
+//   sim_coin(r, e)     = coarse << 16 | fine as coin(s, e), from
+//                        P(b_lo, b_hi, r_lo, SIM_IC<<24 | r_hi) and
+//                        P(e_lo, e_hi, r_lo, SIM_IC_FINE<<24 | r_hi)[0]
 //   sim_lt_thr(r, v)   = P(v, 0, r_lo, SIM_LT<<24 | r_hi)[0]
 #pragma once
 #include <stdint.h>
@@ -43,7 +45,8 @@ enum : uint32_t {
   DOM_LT = 3,
   DOM_SIM_IC = 7,
   DOM_SIM_LT = 8,
-  DOM_IC_FINE = 9
+  DOM_IC_FINE = 9,
+  DOM_SIM_IC_FINE = 10
 };
 
 RIP_HD void mulhilo32(uint32_t a, uint32_t b, uint32_t &hi, uint32_t &lo) {
@@ -101,6 +104,43 @@ RIP_HD Key make_key(uint64_t seed) {
   return Key{(uint32_t)seed, (uint32_t)(seed >> 32)};
 }
 
+// Round keys of the Weyl schedule, k + r * (0x9E3779B9, 0xBB67AE85) for
+// r = 0..9, computed once per launch: a kernel that keeps them in its
+// parameter space (__grid_constant__) XORs them in from there instead of
+// adding the schedule in registers every round.
+struct RoundKeys {
+  uint32_t k0[10], k1[10];
+};
+
+RIP_HD RoundKeys round_keys(Key k) {
+  RoundKeys rk;
+  for (int r = 0; r < 10; ++r) {
+    rk.k0[r] = k.k0 + (uint32_t)r * 0x9E3779B9u;
+    rk.k1[r] = k.k1 + (uint32_t)r * 0xBB67AE85u;
+  }
+  return rk;
+}
+
+// philox() with the round keys given.
+RIP_HD u32x4 philox_rk(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
+                       const RoundKeys &rk) {
+#if defined(__CUDA_ARCH__)
+#pragma unroll
+#endif
+  for (int r = 0; r < 10; ++r) {
+    uint32_t hi0, lo0, hi1, lo1;
+    mulhilo32(0xD2511F53u, c0, hi0, lo0);
+    mulhilo32(0xCD9E8D57u, c2, hi1, lo1);
+    const uint32_t n0 = hi1 ^ c1 ^ rk.k0[r];
+    const uint32_t n2 = hi0 ^ c3 ^ rk.k1[r];
+    c0 = n0;
+    c1 = lo1;
+    c2 = n2;
+    c3 = lo0;
+  }
+  return u32x4{c0, c1, c2, c3};
+}
+
 RIP_HD uint32_t set_hi(uint64_t s, uint32_t dom) {
   return (dom << 24) | (uint32_t)((s >> 32) & 0xFFFFFFu);
 }
@@ -120,6 +160,11 @@ RIP_HD uint32_t root_of(Key k, uint64_t s, uint32_t n) {
 RIP_HD u32x4 ic_block(Key k, uint64_t b, uint64_t s) {
   return philox((uint32_t)b, (uint32_t)(b >> 32), (uint32_t)s,
                 set_hi(s, DOM_IC), k.k0, k.k1);
+}
+
+// ic_block() with the launch's round keys.
+RIP_HD u32x4 ic_block_rk(const RoundKeys &rk, uint64_t b, uint64_t s) {
+  return philox_rk((uint32_t)b, (uint32_t)(b >> 32), (uint32_t)s, set_hi(s, DOM_IC), rk);
 }
 
 // Fine (low) 16 bits of the coin of edge e of set s.
@@ -146,10 +191,16 @@ RIP_HD bool ic_live(Key k, uint64_t s, uint64_t e, uint32_t coarse, uint32_t thr
 #endif
 }
 
-// Coins for the 4 forward edges 4g .. 4g+3 in spread replica r.
-RIP_HD u32x4 sim_ic_coins(Key k, uint64_t g, uint64_t r) {
-  return philox((uint32_t)g, (uint32_t)(g >> 32), (uint32_t)r,
+// Coarse coins of the 8 forward edges 8b .. 8b+7 in spread replica r.
+RIP_HD u32x4 sim_ic_block(Key k, uint64_t b, uint64_t r) {
+  return philox((uint32_t)b, (uint32_t)(b >> 32), (uint32_t)r,
                 set_hi(r, DOM_SIM_IC), k.k0, k.k1);
+}
+
+// Fine (low) 16 bits of the coin of forward edge e in spread replica r.
+RIP_HD uint32_t sim_ic_fine(Key k, uint64_t e, uint64_t r) {
+  return philox((uint32_t)e, (uint32_t)(e >> 32), (uint32_t)r,
+                set_hi(r, DOM_SIM_IC_FINE), k.k0, k.k1).x & 0xFFFFu;
 }
 
 // Threshold of vertex v in LT spread replica r.

@@ -460,8 +460,8 @@ class Pool:
         self._chk(lib.rip_pool_heavy_batch(self.h, min_sets), "rip_pool_heavy_batch")
 
     def heavy_block(self, threads: int) -> None:
-        """Block shape (256/512/1024 threads) of the CTA-per-set kernel for
-        heavy IC sets."""
+        """Block shape (128/256/512/1024 threads) of the CTA-per-set kernel
+        for heavy IC sets."""
         self._chk(lib.rip_pool_heavy_block(self.h, threads), "rip_pool_heavy_block")
 
     def select_guess(self, percent: int) -> None:

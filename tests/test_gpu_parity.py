@@ -89,6 +89,19 @@ def test_lt_sets_bit_exact(ctx):
     assert p.stats()[4] == ost[0]
 
 
+def test_lt_long_in_lists_match_oracle(ctx):
+    # in-lists past 1024 edges: several rounds of the walk's 32-ary search
+    g = lt_graph(14, deg=16, seed=5)
+    assert np.diff(g.index).max() > 1024
+    dg = rb.DeviceGraph(ctx, g, "LT")
+    p = rb.Pool(dg)
+    p.sample(6000, seed=13)
+    off, vtx = p.export()
+    ooff, ovtx, ost = oracle_sets(g, "LT", 13, 0, 6000)
+    assert_same_sets(off, vtx, ooff, ovtx)
+    assert p.stats()[4] == ost[0]
+
+
 def test_lt_long_walks_retry(ctx):
     """A chain 0 <- 1 <- ... <- n-1 with weight 1: walks from high roots run
     past the default per-warp queue, forcing the widen-and-retry path."""
@@ -472,10 +485,11 @@ def test_uniform_thresholds_only_where_they_pay(ctx):
 
 @pytest.mark.parametrize("threads", [128, 256, 512, 1024])
 def test_cta_per_set_block_shapes_match_oracle(ctx, threads):
-    # R-MAT 2^16 with 16 draws per vertex: the largest in-lists pass 1024
-    # 4-edge groups, so every block shape sweeps some lists with the whole CTA
-    g = mixed_uniform_graph(scale=16, deg=16, seed=41)
-    assert np.diff(g.index).max() >= 4 * 1024
+    # R-MAT 2^16 with 32 draws per vertex: the largest in-list passes 1024
+    # 8-edge coin blocks, so every block shape sweeps a list with the whole
+    # CTA
+    g = mixed_uniform_graph(scale=16, deg=32, seed=41)
+    assert np.diff(g.index).max() >= 8 * 1024
     dg = rb.DeviceGraph(ctx, g, "IC")
     p = rb.Pool(dg)
     try:
