@@ -214,8 +214,9 @@ struct CoverLaunch {
   int blocks;
 };
 void launch_cover(const CoverLaunch &C, cudaStream_t stream);
-// The cover, then the last block gathers count[ids[i]] (i < nids) into out,
-// resets *done (a zeroed device word) and writes epoch to *flag (mapped).
+// The cover, then the last block gathers count[ids[i]] (i < nids) into out
+// (ids and out 16-byte aligned), resets *done (a zeroed device word) and
+// writes epoch to *flag (mapped).
 void launch_cover_gather(const CoverLaunch &C, const uint32_t *ids, uint32_t nids,
                          uint32_t *out, unsigned int *done, unsigned int *flag,
                          unsigned int epoch, cudaStream_t stream);
@@ -261,7 +262,7 @@ void launch_sel_pick(const SelDesc *d, uint32_t i, int blocks, cudaStream_t stre
 // uncovered sets (2 launches; the pick decides which, on the device).
 void launch_sel_cover(const SelDesc *d, uint32_t i, int blocks, cudaStream_t stream);
 uint32_t sel_chunk_vertices();
-// out[i] = count[ids[i]], i < m
+// out[i] = count[ids[i]], i < m (ids and out 16-byte aligned)
 void launch_gather_counts(const uint32_t *count, const uint32_t *ids, uint32_t m,
                           uint32_t *out, cudaStream_t stream);
 
