@@ -446,6 +446,14 @@ def main():
                     help="profiling case: one sampler launch of this many sets on the "
                          "workload's graph (after a 1024-set pilot launch); prints its "
                          "algorithmic bytes")
+    ap.add_argument("--imm-case", action="store_true",
+                    help="profiling case: one IMM of the workload (IC graphs autotuned), "
+                         "after two warm-up IMMs, alone between cudaProfilerStart and "
+                         "cudaProfilerStop (ncu --profile-from-start off)")
+    ap.add_argument("--spread-case", type=int, default=0,
+                    help="profiling case of the spread workload: one rip_spread_ic call "
+                         "of this many replicas after a warm-up call, alone in a "
+                         "profiler range")
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
     world, rank, local = dist_setup()
@@ -457,6 +465,10 @@ def main():
         return rc
     if args.sampler_case:
         return run_sampler_case(args, w, local)
+    if args.imm_case:
+        return run_imm_case(args, w, local)
+    if args.spread_case:
+        return run_spread_case(args, w, local)
     if w.get("kind") == "batch":
         return run_batch(args, w, world, rank, local)
     if w.get("kind") == "serve":
@@ -747,6 +759,75 @@ def run_sampler_case(args, w, local):
                       "kernel_ms": km - km0, "gb_per_s": alg / ((km - km0) / 1e3) / 1e9,
                       "stats": [int(x) for x in st]}))
     pool.close()
+    dg.close()
+    ctx.close()
+    return 0
+
+
+def case_graph(args, w, ctx):
+    """The workload's graph for a profiling case: the 2^24 graphs built on the
+    device (smaller with --case-scale, same draws per vertex), others as the
+    bench builds them."""
+    import ripples_b200 as rb
+    if w.get("scale") == 24:
+        scale = args.case_scale or w["scale"]
+        draws = w["draws"] >> (w["scale"] - scale)
+        if w["weights"] == "wc":
+            return rb.DeviceGraph.rmat_on_device(ctx, scale, draws, "IC", rb.WEIGHTS_WC, seed=0)
+        return rb.DeviceGraph.rmat_on_device(ctx, scale, draws, "IC", rb.WEIGHTS_UNIFORM,
+                                             seed=0, weight_seed=1, lo=0.0, hi=0.1)
+    return rb.DeviceGraph(ctx, build_graph(w), w["model"])
+
+
+def run_imm_case(args, w, local):
+    import torch
+    import ripples_b200 as rb
+    torch.cuda.set_device(local)
+    ctx = rb.Context(local)
+    dg = case_graph(args, w, ctx)
+    tune = dg.autotune(seed=1, pilot=32768) if w["model"] == "IC" else None
+    pool = rb.Pool(dg)
+    for s in range(2):
+        pool.clear()
+        pool.imm(w["k"], w["eps"], 1.0, seed=100 + s)
+    pool.clear()
+    ctx.sync()
+    torch.cuda.profiler.start()
+    t0 = time.perf_counter()
+    seeds, rec = pool.imm(w["k"], w["eps"], 1.0, seed=7)
+    ctx.sync()
+    ms = (time.perf_counter() - t0) * 1e3
+    torch.cuda.profiler.stop()
+    print(json.dumps({"case": w["name"], "imm_ms": ms, "theta": int(rec.theta),
+                      "tuned": tune["name"] if tune else None,
+                      "select_profile": pool.select_profile()}))
+    pool.close()
+    dg.close()
+    ctx.close()
+    return 0
+
+
+def run_spread_case(args, w, local):
+    import numpy as np
+    import torch
+    import ripples_b200 as rb
+    torch.cuda.set_device(local)
+    g = build_graph(w)
+    f = g.forward()
+    ctx = rb.Context(local)
+    dg = rb.DeviceGraph(ctx, f, "IC")
+    outdeg = np.diff(f.index).astype(np.int64)
+    seeds = np.lexsort((np.arange(g.n), -outdeg))[: w["k"]].astype(np.uint32)
+    rb.spread_ic(dg, seeds, args.spread_case, seed=1)
+    ctx.sync()
+    torch.cuda.profiler.start()
+    t0 = time.perf_counter()
+    mean = rb.spread_ic(dg, seeds, args.spread_case, seed=2)
+    ctx.sync()
+    ms = (time.perf_counter() - t0) * 1e3
+    torch.cuda.profiler.stop()
+    print(json.dumps({"case": w["name"], "replicas": args.spread_case, "ms": ms,
+                      "mean_spread": float(mean)}))
     dg.close()
     ctx.close()
     return 0
