@@ -12,9 +12,13 @@ epsilon=0.5), ic24_samplers (each IC sampler on one fixed set range of the
 
 One step = one complete IMM (martingale theta estimation + final sampling +
 final greedy selection) from an empty RRR pool, with a fresh sampler seed each
-step, the graph already resident in HBM.  value = RRR sets generated per
-second, summed over ranks, over the max-over-ranks device time of the K timed
-steps.  e2e = the same metric through the public API with the graph uploaded
+step, the graph already resident in HBM.  The K timed steps are split between
+--clients concurrent client threads (2 on the 2^24 IC workload, else 1),
+each with its own context,
+graph copy and pool, so that one query's sampling fills the GPU while
+another's reference-heap selection waits on the host.  value = RRR sets
+generated per second, summed over ranks, over the max-over-ranks device time
+of the K timed steps; one_client = the same IMMs one after another.  e2e = the same metric through the public API with the graph uploaded
 from pinned host memory and the seeds read back every step, from two client
 threads (one context each, IMMs one at a time) so that a step's upload
 overlaps the previous step's IMM; e2e.serial is one client doing both in
@@ -53,8 +57,12 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOADS = {
+    # clients: concurrent IMM clients of the timed region.  Two on the 2^24 IC
+    # graph, where one query's sampling fills the GPU while another's
+    # selection waits on the host (+19%); one on LT, where a query's walk
+    # launches hold every SM and delay the other's pick launches (-38%).
     "ic24": dict(name="imm_ic_rmat24_deg32_wc_k100_eps0.13", scale=24, draws=32 << 24,
-                 model="IC", k=100, eps=0.13, weights="wc"),
+                 model="IC", k=100, eps=0.13, weights="wc", clients=2),
     "lt20": dict(name="imm_lt_rmat20_deg16_k50_eps0.3", scale=20, draws=16 << 20, model="LT",
                  k=50, eps=0.3, weights="lt_normalized"),
     "ic14": dict(name="imm_ic_rmat14_2^18_k20_eps0.5", scale=14, draws=1 << 18, model="IC",
@@ -429,6 +437,11 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--clients", type=int, default=0,
+                    help="IMM workloads: concurrent client threads of the timed region, "
+                         "each with its own context, graph and pool (the K steps are "
+                         "split between them); 0 = the workload's default (2 for the "
+                         "2^24 IC IMM, 1 for the LT and small IC ones)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="ic24", choices=sorted(WORKLOADS))
@@ -510,9 +523,25 @@ def main():
 
     for i in range(args.warmup):
         one_step(-1 - i)
+    # Further clients: a context, graph and pool each (same host graph, tuned
+    # the same way), so that one query's sampling runs while another's
+    # selection waits on the host, as concurrent queries would.
+    n_clients = args.clients if args.clients > 0 else w.get("clients", 1)
+    extra = []
+    for j in range(1, n_clients):
+        cx = rb.Context(local)
+        dgx = rb.DeviceGraph(cx, g, w["model"])
+        if w["model"] == "IC":
+            dgx.autotune(seed=1, pilot=32768)
+        px = rb.Pool(dgx)
+        for i in range(args.warmup):
+            px.clear()
+            px.imm(w["k"], w["eps"], 1.0, seed=seed_base + 1000 * j - 1 - i)
+        extra.append((cx, dgx, px))
+    pools = [pool] + [e[2] for e in extra]
     # ---- timed region (device events on the library's stream) --------------
-    pool.clear()
-    st0 = pool.stats()
+    for px in pools:
+        px.clear()
     launches0 = rb._lib.lib.rip_kernel_launches()
     clocks = ClockSampler(local)
     barrier(world)
@@ -520,30 +549,75 @@ def main():
     clocks.start()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
-    total_sets, kern_ms, kern_n, st_tot = 0, 0.0, 0, np.zeros(8, np.uint64)
-    thetas, gen_ms, sel_ms = [], 0.0, 0.0
-    sel_prof = {}
-    for step in range(args.steps):
-        pool.clear()
-        seeds, rec = pool.imm(w["k"], w["eps"], 1.0, seed=seed_base + step)
-        total_sets += rec.total_sets
-        thetas.append(int(rec.theta))
-        nr = min(rec.num_rounds, 64)
-        gen_ms += rec.generate_ms + sum(rec.round_generate_ms[i] for i in range(nr))
-        sel_ms += rec.select_ms + sum(rec.round_select_ms[i] for i in range(nr))
-        km, kn, _ = pool.timing()
-        kern_ms += km
-        kern_n += kn
-        st_tot += pool.stats()
-        for kk, vv in pool.select_profile().items():
-            sel_prof[kk] = sel_prof.get(kk, 0.0) + vv
+    acc = [dict(sets=0, kern_ms=0.0, kern_n=0, st=np.zeros(8, np.uint64), thetas=[],
+                gen_ms=0.0, sel_ms=0.0, sel_prof={}, err=None) for _ in pools]
+
+    def client(j):
+        a, px = acc[j], pools[j]
+        try:
+            for step in range(j, args.steps, n_clients):
+                px.clear()
+                seeds, rec = px.imm(w["k"], w["eps"], 1.0, seed=seed_base + step)
+                a["sets"] += rec.total_sets
+                a["thetas"].append(int(rec.theta))
+                nr = min(rec.num_rounds, 64)
+                a["gen_ms"] += rec.generate_ms + sum(rec.round_generate_ms[i] for i in range(nr))
+                a["sel_ms"] += rec.select_ms + sum(rec.round_select_ms[i] for i in range(nr))
+                km, kn, _ = px.timing()
+                a["kern_ms"] += km
+                a["kern_n"] += kn
+                a["st"] += px.stats()
+                for kk, vv in px.select_profile().items():
+                    a["sel_prof"][kk] = a["sel_prof"].get(kk, 0.0) + vv
+        except Exception as exc:  # reported after the join
+            a["err"] = repr(exc)
+
+    workers = [threading.Thread(target=client, args=(j,)) for j in range(n_clients)]
+    for th in workers:
+        th.start()
+    for th in workers:
+        th.join()
+    torch.cuda.synchronize()  # every client's stream is done before ev1
     ev1.record(stream)
     torch.cuda.synchronize()
     barrier(world)
     clk = clocks.stop()
+    errs = [a["err"] for a in acc if a["err"]]
+    if errs:
+        raise RuntimeError("timed clients: " + "; ".join(errs))
     launches = int(rb._lib.lib.rip_kernel_launches() - launches0)
     elapsed_ms = ev0.elapsed_time(ev1)
+    total_sets = sum(a["sets"] for a in acc)
+    kern_ms = sum(a["kern_ms"] for a in acc)
+    kern_n = sum(a["kern_n"] for a in acc)
+    st_tot = sum((a["st"] for a in acc), np.zeros(8, np.uint64))
+    thetas = [t for a in acc for t in a["thetas"]]
+    gen_ms = sum(a["gen_ms"] for a in acc)
+    sel_ms = sum(a["sel_ms"] for a in acc)
+    sel_prof = {}
+    for a in acc:
+        for kk, vv in a["sel_prof"].items():
+            sel_prof[kk] = sel_prof.get(kk, 0.0) + vv
     value, t_max = aggregate(total_sets, elapsed_ms, world)
+    for cx, dgx, px in extra:
+        px.close()
+        dgx.close()
+        cx.close()
+
+    # ---- one client alone (each IMM's own latency) -------------------------
+    torch.cuda.synchronize()
+    ev4, ev5 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    one_steps = max(1, min(args.steps, 5))
+    ev4.record(stream)
+    one_sets = 0
+    for step in range(one_steps):
+        pool.clear()
+        _, rec = pool.imm(w["k"], w["eps"], 1.0, seed=seed_base + step)
+        one_sets += rec.total_sets
+    ev5.record(stream)
+    torch.cuda.synchronize()
+    one_ms = allreduce_max(ev4.elapsed_time(ev5), world)
+    one_value = allreduce_sum(one_sets, world) / (one_ms / 1e3)
 
     # ---- the same IMM runs with the reference GPU path's tie-break ---------
     # (lowest vertex id among equal counts, thrust::max_element): every pick
@@ -757,6 +831,10 @@ def main():
             "uniform_thresholds_2^18_sets": uniform_cmp,
             "branching": dg.branching if w["model"] == "IC" else None,
             "tiebreak": "reference CPU heap (CompareHeap lazy max-heap)",
+            "clients": n_clients,
+            "one_client": {"value": one_value, "unit": "sets/s", "ms_per_step": one_ms / one_steps,
+                           "steps": one_steps,
+                           "note": "the same IMMs one after another from one client"},
             "lowest_id_tiebreak": {"value": low_value, "unit": "sets/s",
                                    "ms_per_step": low_ms_per_step, "steps": low_steps,
                                    "note": "same IMM runs, reference GPU tie-break "
