@@ -13,16 +13,16 @@ epsilon=0.5), ic24_samplers (each IC sampler on one fixed set range of the
 One step = one complete IMM (martingale theta estimation + final sampling +
 final greedy selection) from an empty RRR pool, with a fresh sampler seed each
 step, the graph already resident in HBM.  The K timed steps are split between
---clients concurrent client threads (2 on the 2^24 IC workload, else 1),
-each with its own context,
+--clients concurrent client threads (3 on the 2^24 IC workload, 4 on the
+2^20 LT one, else 1), each with its own context,
 graph copy and pool, so that one query's sampling fills the GPU while
 another's reference-heap selection waits on the host.  value = RRR sets
 generated per second, summed over ranks, over the max-over-ranks device time
 of the K timed steps; one_client = the same IMMs one after another.  e2e = the same metric through the public API with the graph uploaded
-from pinned host memory and the seeds read back every step, from two client
-threads (one context each, IMMs one at a time) so that a step's upload
-overlaps the previous step's IMM; e2e.serial is one client doing both in
-turn.
+from pinned host memory and the seeds read back every step, from the
+workload's concurrent clients (at least two, one context each) so that a
+step's upload overlaps other steps' IMMs; e2e.serial is one client doing
+both in turn.
 
 Multi-GPU: the path does not shard across GPUs in this build ("replicas
 only"): each rank runs its own independent IMM query (its own seeds), and
@@ -57,14 +57,14 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOADS = {
-    # clients: concurrent IMM clients of the timed region.  Two on the 2^24 IC
-    # graph, where one query's sampling fills the GPU while another's
-    # selection waits on the host (+19%); one on LT, where a query's walk
-    # launches hold every SM and delay the other's pick launches (-38%).
+    # clients: concurrent IMM clients of the timed region (a query's
+    # reference-heap selection waits on the host while another's sampling and
+    # picks use the GPU): 3 on the 2^24 IC graph (1, 2, 3 clients: 5.5, 6.6,
+    # 7.2 M sets/s), 4 on LT (1 to 4: 2.8, 5.0, 7.0, 7.9 M sets/s).
     "ic24": dict(name="imm_ic_rmat24_deg32_wc_k100_eps0.13", scale=24, draws=32 << 24,
-                 model="IC", k=100, eps=0.13, weights="wc", clients=2),
+                 model="IC", k=100, eps=0.13, weights="wc", clients=3),
     "lt20": dict(name="imm_lt_rmat20_deg16_k50_eps0.3", scale=20, draws=16 << 20, model="LT",
-                 k=50, eps=0.3, weights="lt_normalized"),
+                 k=50, eps=0.3, weights="lt_normalized", clients=4),
     "ic14": dict(name="imm_ic_rmat14_2^18_k20_eps0.5", scale=14, draws=1 << 18, model="IC",
                  k=20, eps=0.5, weights="uniform_0_0.1"),
     # 64 IMM instances over 16 graphs (ER + R-MAT, 2^12..2^22 vertices, average
@@ -440,8 +440,8 @@ def main():
     ap.add_argument("--clients", type=int, default=0,
                     help="IMM workloads: concurrent client threads of the timed region, "
                          "each with its own context, graph and pool (the K steps are "
-                         "split between them); 0 = the workload's default (2 for the "
-                         "2^24 IC IMM, 1 for the LT and small IC ones)")
+                         "split between them); 0 = the workload's default (3 for the "
+                         "2^24 IC IMM, 4 for the 2^20 LT one, 1 otherwise)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="ic24", choices=sorted(WORKLOADS))
@@ -702,32 +702,31 @@ def main():
     e2e_ms = (time.perf_counter() - t0) * 1e3
     e2e_serial = allreduce_sum(e2e_sets, world) / (allreduce_max(e2e_ms, world) / 1e3)
 
-    # The same steps from two client threads, each with its own context, IMMs
-    # one at a time (a lock): a step's upload crosses the bus while the
-    # previous step's IMM runs on the GPU, as a serving client would overlap
-    # them.  Every step still copies its graph in and its seeds out.
-    pipe_ctx = [rb.Context(local) for _ in range(2)]
-    imm_lock = threading.Lock()
-    pipe_sets, pipe_err = [0, 0], []
+    # The same steps from the workload's concurrent clients (at least two),
+    # each with its own context: a step's upload crosses the bus while other
+    # steps' IMMs run on the GPU, as concurrent queries of a serving client
+    # would.  Every step still copies its graph in and its seeds out.
+    n_pipe = max(2, n_clients)
+    pipe_ctx = [rb.Context(local) for _ in range(n_pipe)]
+    pipe_sets, pipe_err = [0] * n_pipe, []
 
     def pipe_worker(j):
         try:
-            for step in range(j, e2e_steps, 2):
+            for step in range(j, e2e_pipe_steps, n_pipe):
                 gen_g = rb.HostGraph(g.n, pin_idx.numpy(), pin_src.numpy(), pin_w.numpy())
                 gen = rb.B200RRRGenerator(gen_g, w["model"], seed=seed_base + 7919 + step,
                                           ctx=pipe_ctx[j])
-                with imm_lock:
-                    CFG = rb.IMMConfiguration(k=w["k"], epsilon=w["eps"],
-                                              diffusionModel=w["model"])
-                    rec = rb.IMMExecutionRecord()
-                    rb.IMM(gen_g, CFG, 1.0, gen, rec)
-                    pipe_sets[j] += rec.TotalSets
+                CFG = rb.IMMConfiguration(k=w["k"], epsilon=w["eps"], diffusionModel=w["model"])
+                rec = rb.IMMExecutionRecord()
+                rb.IMM(gen_g, CFG, 1.0, gen, rec)
+                pipe_sets[j] += rec.TotalSets
                 gen.pool.close()
                 gen.graph.close()
         except Exception as exc:  # reported after the join
             pipe_err.append(repr(exc))
 
-    for j in range(2):  # each context's buffers sized once, untimed
+    e2e_pipe_steps = max(e2e_steps, 2 * n_pipe)
+    for j in range(n_pipe):  # each context's buffers sized once, untimed
         warm_g = rb.HostGraph(g.n, pin_idx.numpy(), pin_src.numpy(), pin_w.numpy())
         warm = rb.B200RRRGenerator(warm_g, w["model"], seed=seed_base + 7, ctx=pipe_ctx[j])
         rb.IMM(warm_g, rb.IMMConfiguration(k=w["k"], epsilon=w["eps"], diffusionModel=w["model"]),
@@ -737,7 +736,7 @@ def main():
     barrier(world)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    threads = [threading.Thread(target=pipe_worker, args=(j,)) for j in range(2)]
+    threads = [threading.Thread(target=pipe_worker, args=(j,)) for j in range(n_pipe)]
     for th in threads:
         th.start()
     for th in threads:
@@ -796,10 +795,11 @@ def main():
             "parallelism": f"replicas x{world}",
             "l2": "graph (%d MB) and pool exceed L2 (126 MB)" % ((g.m * 8 + g.n * 4) >> 20),
             "e2e": {"value": e2e_value, "unit": "sets/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "steps": e2e_steps,
-                    "clients": "two threads, one context each, IMMs one at a time: a step's "
-                               "upload overlaps the previous step's IMM",
-                    "ms_per_step": pipe_ms / e2e_steps,
+                    "d2h_bytes_per_step": d2h, "steps": e2e_pipe_steps,
+                    "clients": n_pipe,
+                    "note": "concurrent client threads, one context each: a step's upload "
+                            "overlaps other steps' IMMs",
+                    "ms_per_step": pipe_ms / e2e_pipe_steps,
                     "serial": {"value": e2e_serial, "note": "one client: upload, then IMM",
                                "split_ms_per_step": {kk: vv / e2e_steps
                                                      for kk, vv in e2e_split.items()},

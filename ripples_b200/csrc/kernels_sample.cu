@@ -342,8 +342,10 @@ ic_plain_kernel(DevGraph G, DevPool P, Key key, const __grid_constant__ RoundKey
 // vertex: a 32-ary search over the cumulative thresholds (one probe per lane
 // per round, log32(in-degree) rounds), finishing with one 8-byte load per lane
 // so the lane that holds the pick also holds its source id.  Walks are chains
-// of dependent loads, so the kernel is bound to 32 registers for 64 resident
-// warps per SM (and the host launches that many walks in flight).
+// of dependent loads; the kernel is bound to 32 registers (up to 64 resident
+// warps per SM) and the host launches 32 warps per SM: a launch lasts about
+// as long as its longest walk either way, and the free warp slots serve
+// other queries' kernels.
 __global__ void __launch_bounds__(256, 8)
 lt_walk_kernel(DevGraph G, DevPool P, Key key, uint64_t first, uint32_t count,
                const uint32_t *ids, unsigned int *next, uint32_t *bitmaps,

@@ -160,10 +160,12 @@ static uint32_t default_warps(rip_pool *p, uint32_t qcap) {
   rip_ctx *c = p->ctx;
   const uint64_t bm_bytes = scratch_bm_words(p) * 4;
   const uint64_t per = bm_bytes + (uint64_t)qcap * 4;
-  // LT walks: 64 resident warps per SM (latency-bound chains); IC: 32, or 40
+  // LT walks: 32 resident warps per SM -- a launch lasts about as long as its
+  // longest walk either way (a chain of dependent loads), and half the SMs'
+  // warp slots stay free for other queries' pick launches; IC: 32, or 40
   // with the register-capped kernel variant
   uint64_t want = (uint64_t)c->num_sms *
-                  (p->g->model == RIP_MODEL_LT ? 64 : p->plain_occupancy == 5 ? 40 : 32);
+                  (p->g->model == RIP_MODEL_LT ? 32 : p->plain_occupancy == 5 ? 40 : 32);
   size_t avail = c->budget > c->used ? c->budget - c->used : 0;
   uint64_t fit = (avail / 4) / per;  // scratch gets at most a quarter
   uint64_t w = std::min<uint64_t>(want, std::max<uint64_t>(fit, 8));
