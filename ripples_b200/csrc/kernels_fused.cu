@@ -10,14 +10,18 @@
 // n x colour matrix back for a host-side scan after each batch.  Here:
 //   * frontiers are sparse: a per-CTA log of (vertex) entries, one level
 //     after the other; a vertex enters a level's list once, when its pending
-//     mask first gains a colour for that level (per-vertex level flag);
+//     mask first gains a colour for that level (per-vertex level flag); the
+//     log's first kSharedLog entries are staged in shared memory (most
+//     batches never leave it), the rest in the CTA's global log;
 //   * levels are separated by __syncthreads only -- no grid sync, no host
 //     round trip; CTAs are persistent and pull batches from an atomic counter;
-//   * the coin of (set s, edge e) is Philox(seed; e>>2, s)[e&3], a pure
-//     function, so the sets equal those of the one-set-per-warp kernel and of
-//     the CPU restatement bit for bit;
+//   * the coin of (set s, edge e) is the same pure function of (seed, s, e)
+//     as every sampler's (coarse halves from an 8-edge Philox block, the fine
+//     half on a tie), so the sets equal those of the one-set-per-warp kernel
+//     and of the CPU restatement bit for bit;
 //   * in-edges are read in aligned 4-edge groups (one 32-byte load, one Philox
-//     per colour per group) with warp-level load balancing across entries;
+//     block per colour per group) with warp-level load balancing across
+//     entries;
 //   * the finished batch is compacted straight into the flat pool: one
 //     atomicAdd reserves all W sets, per-colour shared cursors place members,
 //     and the same pass clears the colour masks (atomicExch) for the next
@@ -40,6 +44,7 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
 
 constexpr int FUSED_THREADS = 512;
 constexpr int FUSED_WARPS = FUSED_THREADS / 32;
+constexpr uint32_t kSharedLog = 4096;  // frontier-log entries staged in shared memory
 
 template <int CW>
 __global__ void __launch_bounds__(FUSED_THREADS)
@@ -50,6 +55,7 @@ ic_fused_kernel(FusedLaunch L) {
   __shared__ uint32_t s_size[W];
   __shared__ uint32_t s_fill[W];
   __shared__ uint32_t s_batch, s_ncol, s_tail, s_overflow;
+  __shared__ uint32_t s_log[kSharedLog];  // log entries [0, kSharedLog)
   __shared__ unsigned long long s_base, s_work;
 
   const uint32_t tid = threadIdx.x, lane = lane_id(), wid = tid >> 5;
@@ -96,7 +102,10 @@ ic_fused_kernel(FusedLaunch L) {
       atomicAdd(&s_size[c], 1u);
       if (atomicExch(&pflag[r], 1u) != 1u) {
         const uint32_t pos = atomicAdd(&s_tail, 1u);
-        if (pos < lcap) log[pos] = r;
+        if (pos < lcap) {
+          if (pos < kSharedLog) s_log[pos] = r;
+          else log[pos] = r;
+        }
         else s_overflow = 1;
       }
     }
@@ -112,7 +121,7 @@ ic_fused_kernel(FusedLaunch L) {
 #pragma unroll
         for (int w = 0; w < CW; ++w) mask[w] = 0;
         if (ei < lvl_end) {
-          const uint32_t v = log[ei];
+          const uint32_t v = ei < kSharedLog ? s_log[ei] : log[ei];
           uint32_t any = 0;
 #pragma unroll
           for (int w = 0; w < CW; ++w) {
@@ -234,7 +243,10 @@ ic_fused_kernel(FusedLaunch L) {
             pos0 = __shfl_sync(FULL, pos0, __ffs(bal) - 1);
             if (push[t]) {
               const uint32_t pos = pos0 + __popc(bal & lanemask_lt());
-              if (pos < lcap) log[pos] = u[t];
+              if (pos < lcap) {
+                if (pos < kSharedLog) s_log[pos] = u[t];
+                else log[pos] = u[t];
+              }
               else s_overflow = 1;
             }
           }
@@ -289,7 +301,7 @@ ic_fused_kernel(FusedLaunch L) {
     const uint32_t tail = min(s_tail, lcap);
     const bool aborted = s_overflow == 3;  // frontier left unexpanded: clear pend too
     for (uint32_t i = tid; i < tail; i += FUSED_THREADS) {
-      const uint32_t v = log[i];
+      const uint32_t v = i < kSharedLog ? s_log[i] : log[i];
 #pragma unroll
       for (int w = 0; w < CW; ++w) {
         if (aborted) pend[(size_t)v * CW + w] = 0ull;
