@@ -609,11 +609,15 @@ def main():
     ev4, ev5 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     one_steps = max(1, min(args.steps, 5))
     ev4.record(stream)
-    one_sets = 0
+    one_sets, one_kern_ms, one_kern_n, one_st = 0, 0.0, 0, np.zeros(8, np.uint64)
     for step in range(one_steps):
         pool.clear()
         _, rec = pool.imm(w["k"], w["eps"], 1.0, seed=seed_base + step)
         one_sets += rec.total_sets
+        km, kn, _ = pool.timing()
+        one_kern_ms += km
+        one_kern_n += kn
+        one_st += pool.stats()
     ev5.record(stream)
     torch.cuda.synchronize()
     one_ms = allreduce_max(ev4.elapsed_time(ev5), world)
@@ -757,6 +761,9 @@ def main():
     alg_bytes = alg_bytes_of(st_tot, vthr)
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (kern_ms / 1e3) / 1e9 if kern_ms > 0 else None
+    # the same kernels with no other query's launches beside them
+    one_alg = alg_bytes_of(one_st, vthr)
+    one_achieved = one_alg / (one_kern_ms / 1e3) / 1e9 if one_kern_ms > 0 else None
     kernel = ("lt_walk_kernel" if w["model"] == "LT" else
               "ic_fused_kernel" if tune and tune["name"].startswith("fused") else
               "ic_plain_kernel + ic_bigset_kernel (every IC sampler launch)")
@@ -778,6 +785,11 @@ def main():
                          "kernel": kernel, "achieved": coins, "peak": coin_peak,
                          "peak_kind": "measured (coin-only kernel, same run)",
                          "unit": "coins/s", "frac": coins / coin_peak if coin_peak else None}
+        if one_kern_ms > 0:
+            one_coins = int(one_st[5]) / (one_kern_ms / 1e3)
+            coin_roofline["one_client"] = {
+                "achieved": one_coins, "frac": one_coins / coin_peak if coin_peak else None,
+                "note": "the one-client steps: no other query's launches beside the kernel"}
 
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -809,7 +821,12 @@ def main():
                          "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
                          "traffic": traffic,
                          "alg_bytes_per_launch": alg_bytes / max(kern_n, 1),
-                         "launches": kern_n, "kernel_ms": kern_ms},
+                         "launches": kern_n, "kernel_ms": kern_ms,
+                         "one_client": {"achieved": one_achieved,
+                                        "frac": (one_achieved / peak) if one_achieved else None,
+                                        "launches": one_kern_n, "kernel_ms": one_kern_ms,
+                                        "note": "the one-client steps: no other query's "
+                                                "launches beside the kernel"}},
             # sum over sets of the in-degrees of their members (per-set
             # semantics, fused expansions counted per colour) over the
             # sampler kernels' time
