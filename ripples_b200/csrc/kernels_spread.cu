@@ -3,9 +3,9 @@
 // The reference measures the quality of a seed set with ripples::simulate
 // (include/ripples/diffusion_simulation.h:73-178, driven replica by replica
 // by tools/simulator.cc); the spread is the number of vertices reached,
-// seeds included.  Here one 1024-thread CTA runs one replica at a time with
+// seeds included.  Here one 512-thread CTA runs one replica at a time with
 // the level loop of the one-CTA-per-heavy-set sampler: a level's entries are
-// taken 1024 at a time, a block scan turns their out-edge unit counts into
+// taken a CTA's width at a time, a block scan turns their out-edge unit counts into
 // offsets and all warps stride over the concatenated units (IC: 8-edge coin
 // blocks, one Philox block each; LT: 4-edge record groups).
 //   IC: out-edge e of a reached vertex fires in replica r iff its coin
@@ -27,7 +27,11 @@ namespace rip {
 
 namespace {
 
-constexpr int SIM_THREADS = 1024;
+// four 512-thread CTAs per SM (32 registers a thread: 64 resident warps).
+// The kernel waits on L2 latency, so replicas in flight are what move it:
+// one 1024-thread CTA per SM (32 warps) ran 19.3 K replicas/s on the 2^20
+// bench, two of 768 threads 23.1 K, three of 640 25.6 K, four of 512 26.5 K.
+constexpr int SIM_THREADS = 512;
 constexpr int SIM_WARPS = SIM_THREADS / 32;
 
 __device__ uint32_t sim_block_scan(uint32_t x, uint32_t *warp_tot, uint32_t *total) {
@@ -68,7 +72,7 @@ __device__ __forceinline__ uint32_t lt_kept_source(const DevGraph &B, Key key, u
 }
 
 template <bool LT>
-__global__ void __launch_bounds__(SIM_THREADS, 1)
+__global__ void __launch_bounds__(SIM_THREADS, kSpreadCtasPerSm)
 spread_kernel(SpreadLaunch L) {
   __shared__ uint32_t s_off[SIM_THREADS + 1];
   __shared__ uint32_t s_beg[SIM_THREADS], s_end[SIM_THREADS];

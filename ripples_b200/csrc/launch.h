@@ -157,6 +157,8 @@ struct SpreadLaunch {
   uint32_t qcap = 0;
   int blocks = 0;
 };
+// Resident spread CTAs (one replica each at a time) per SM.
+constexpr int kSpreadCtasPerSm = 4;
 void launch_spread(const SpreadLaunch &L, bool lt, cudaStream_t stream);
 void launch_ic_fused(const FusedLaunch &L, cudaStream_t stream);
 // Resident fused CTAs per SM for a colour width (occupancy API).

@@ -25,11 +25,11 @@ int spread_run(rip_graph *g, rip_graph *b, const uint32_t *seeds, uint32_t k,
   CK(c, cudaSetDevice(c->device));
 
   // per CTA slot: an n-bit visited bitmap and an n-entry queue (a replica
-  // queues every vertex at most once); at most one slot per SM, fewer when
-  // the slots would take more than a quarter of the free budget
+  // queues every vertex at most once); at most one slot per resident CTA,
+  // fewer when the slots would take more than a quarter of the free budget
   const uint64_t bm_words = ((uint64_t)g->n + 31) / 32;
   const uint64_t per_slot = 4 * bm_words + 4 * (uint64_t)g->n;
-  uint64_t slots = std::min<uint64_t>(replicas, (uint64_t)c->num_sms);
+  uint64_t slots = std::min<uint64_t>(replicas, (uint64_t)c->num_sms * kSpreadCtasPerSm);
   const uint64_t room = c->budget > c->used ? (c->budget - c->used) / 4 : 0;
   while (slots > 1 && slots * per_slot > room) slots /= 2;
 
