@@ -105,7 +105,16 @@ def workload_config(w, n, m):
     return {"workload": w["name"], "model": w["model"], "k": w["k"], "epsilon": w["eps"],
             "n": n, "m": m, "weights": w["weights"],
             "graph": "R-MAT 2^%d, %d draws, a,b,c = %s, seed 0, no self-loops or duplicates"
-                     % (w["scale"], w["draws"], ",".join(str(x) for x in RMAT_ABC))}
+                     % (w["scale"], w["draws"], ",".join(str(x) for x in RMAT_ABC)),
+            "l2": l2_note(8 * m + 4 * (n + 1))}
+
+
+def l2_note(graph_bytes):
+    """How the timed steps stand to the 126 MB L2 (no flush between steps)."""
+    mb = graph_bytes / 1e6
+    if mb > 126:
+        return "no flush: the graph alone (%.0f MB) exceeds the 126 MB L2" % mb
+    return "no flush: the graph (%.1f MB) fits in the 126 MB L2, steps run L2-warm" % mb
 
 
 def build_graph(w):
