@@ -90,6 +90,11 @@ WORKLOADS = {
     # forward Monte Carlo spread (rip_spread_ic) of the 50 vertices of largest
     # out-degree on R-MAT 2^20 (16*2^20 draws, IC p ~ U(0,0.1)), 20000
     # replicas a step; the reference's own simulator timed beside it
+    # one IMM per step with its sets split across the ranks (and --shards
+    # pools per rank), counts summed by all_reduce at every pick; lowest-id
+    # picks, so each step's answer is the single-pool one (strong scaling)
+    "ic24_sharded": dict(name="imm_sharded_ic_rmat24_deg32_wc_k100_eps0.13", kind="sharded",
+                         scale=24, draws=32 << 24, model="IC", k=100, eps=0.13, weights="wc"),
     "spread": dict(name="spread_ic_rmat20_deg16_k50", kind="spread", scale=20,
                    draws=16 << 20, model="IC", weights="uniform_0_0.1", k=50,
                    replicas=20000),
@@ -355,7 +360,9 @@ def reference_arm_other(args, w, world, rank):
         why = {"batch": "the reference runs one IMM instance per process (no batching path)",
                "serve": "the reference has no request loop (no serving path)",
                "p3": "this workload compares the library's samplers with one another; the "
-                     "reference arm of the 2^24 graph is --workload ic24"}[kind]
+                     "reference arm of the 2^24 graph is --workload ic24",
+               "sharded": "the reference's sharded IMM is its MPI build (mpi/imm.h), and "
+                          "this image has no MPI"}[kind]
         print(json.dumps({"impl": "reference", "unavailable": why}))
         return 0
     sys.path.insert(0, ROOT)
@@ -454,6 +461,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="ic24", choices=sorted(WORKLOADS))
+    ap.add_argument("--shards", type=int, default=1,
+                    help="ic24_sharded: pools (shards) per process")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--serve-scales", default="18,20,22,24",
                     help="s1: R-MAT scales of the resident graphs")
@@ -482,7 +491,7 @@ def main():
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
     world, rank, local = dist_setup()
-    if args.impl == "reference" and w.get("kind") in ("batch", "serve", "p3", "spread"):
+    if args.impl == "reference" and w.get("kind") in ("batch", "serve", "p3", "spread", "sharded"):
         rc = reference_arm_other(args, w, world, rank)
         if world > 1:
             import torch.distributed as dist
@@ -502,6 +511,8 @@ def main():
         return run_p3(args, w, world, rank, local)
     if w.get("kind") == "spread":
         return run_spread(args, w, world, rank, local)
+    if w.get("kind") == "sharded":
+        return run_sharded(args, w, world, rank, local)
     if args.impl == "reference":
         rc = reference_arm(args, w, world, rank)
         if world > 1:
@@ -1206,6 +1217,94 @@ def run_p3(args, w, world, rank, local):
             "clocks": clk}
     print(json.dumps(line))
     ctx.close()
+    return 0
+
+
+def run_sharded(args, w, world, rank, local):
+    """One IMM per step on the 2^24 weighted-cascade graph with its sets split
+    across every rank's --shards pools (ripples_b200.sharded): each rank
+    samples its id ranges, the per-pick counts are summed in process and by
+    NCCL all_reduce.  Whole-job sets/s of one IMM (strong scaling), timed on
+    the device from a synchronised start to a synchronised end, max over
+    ranks; at one GPU the single-pool IMM under the same (lowest-id)
+    tie-break is timed beside it."""
+    import torch
+    import ripples_b200 as rb
+    from ripples_b200.sharded import DeviceShard, imm_sharded
+    torch.cuda.set_device(local)
+    group = None
+    if world > 1:
+        import torch.distributed as dist
+        group = dist.group.WORLD
+    ctx = rb.Context(local)
+    scale = args.case_scale or w["scale"]
+    draws = w["draws"] >> (w["scale"] - scale)
+    dg = rb.DeviceGraph.rmat_on_device(ctx, scale, draws, "IC", rb.WEIGHTS_WC, seed=0)
+    shards = [DeviceShard(rb.Pool(dg)) for _ in range(max(1, args.shards))]
+
+    def one(step):
+        for s in shards:
+            s.pool.clear()
+        return imm_sharded(shards, w["k"], w["eps"], 1.0, seed=step, group=group)
+
+    for i in range(args.warmup):
+        one(1000 + i)
+    barrier(world)
+    clocks = ClockSampler(local)
+    clocks.start()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    sets = 0
+    recs = []
+    for i in range(args.steps):
+        _, rec = one(i)
+        sets += rec["total_sets"]
+        recs.append(rec)
+    torch.cuda.synchronize()
+    ev1.record()
+    ev1.synchronize()
+    clk = clocks.stop()
+    ms = allreduce_max(ev0.elapsed_time(ev1), world)
+    single = None
+    if world == 1:
+        p1 = rb.Pool(dg)
+        p1.imm(w["k"], w["eps"], 1.0, seed=1000, tiebreak=rb.TIE_LOWEST_ID)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s1 = 0
+        for i in range(args.steps):
+            p1.clear()
+            _, r1 = p1.imm(w["k"], w["eps"], 1.0, seed=i, tiebreak=rb.TIE_LOWEST_ID)
+            s1 += r1.total_sets
+        torch.cuda.synchronize()
+        single = {"sets_per_s": s1 / (time.perf_counter() - t0),
+                  "note": "rip_imm_pool, lowest-id tie-break, same seeds (host clock)"}
+        p1.close()
+    if rank == 0:
+        picks = sum(r["picks"] for r in recs)
+        line = {"metric": METRIC, "value": sets / (ms / 1e3), "unit": "sets/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "strong", "vs_baseline": None, "dtype": "u32",
+                "data": "synthetic R-MAT graph (seed 0), weighted cascade",
+                "config": {"workload": w["name"], "n": dg.n, "m": dg.m, "k": w["k"],
+                           "epsilon": w["eps"], "shards_per_rank": len(shards),
+                           "shards": world * len(shards), "tiebreak": "lowest_id",
+                           "l2": l2_note(8 * dg.m + 4 * (dg.n + 1))},
+                "sets_per_step": sets / args.steps,
+                "picks_per_step": picks / args.steps,
+                "select_ms_per_step": sum(sum(r["round_select_ms"]) + r["select_ms"]
+                                          for r in recs) / args.steps,
+                "allreduce_ms_per_step": sum(r["allreduce_ms"] for r in recs) / args.steps,
+                "single_pool": single, "clocks": clk}
+        print(json.dumps(line))
+    for s in shards:
+        s.pool.close()
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
     return 0
 
 

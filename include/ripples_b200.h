@@ -175,6 +175,11 @@ int rip_pool_export(rip_pool *p, uint64_t first, uint64_t count,
  * the reference's own sets to the device selection. */
 int rip_pool_import(rip_pool *p, const uint64_t *offsets,
                     const uint32_t *vertices, uint64_t count);
+/* Appends `count` empty sets: the ids that other shards of a sharded
+ * selection sample (rip_shard_*).  An empty set adds to no count and is never
+ * covered.  The reference's MPI IMM gives each rank its own sets instead
+ * (include/ripples/mpi/imm.h:181-190). */
+int rip_pool_skip(rip_pool *p, uint64_t count);
 
 /* Device counters of the sampling kernels since the pool was created/cleared:
  * stats[0] = vertex expansions (a vertex's in-edge list read once, whatever
@@ -317,6 +322,28 @@ int rip_selftest_heap_device(rip_ctx *ctx, uint64_t n, uint32_t max_count, uint6
 /* Vertex occurrence counts over sets [0, num_sets) (n values), the first
  * step of selection (CountOccurrencies, include/ripples/counting.h:65-97). */
 int rip_count(rip_pool *p, uint64_t num_sets, uint32_t *counts);
+
+/* ---- sharded selection ------------------------------------------------------ */
+/* One shard's part of a greedy lowest-id selection whose sets are split
+ * across pools (one per GPU or process).  Replaces the MPI
+ * FindMostInfluentialSet (include/ripples/mpi/find_most_influential.h:449-690:
+ * per-pick reduction of the vertex counters, the maximum picked, every rank
+ * updating its own sets).  d_sum is a device array of n uint32 (16-byte
+ * aligned) on the pool's device; each call below returns once its work on
+ * the context stream is done, so the caller may sum the shards' d_sum arrays
+ * (an all-reduce) on any stream, and must finish that sum before
+ * rip_shard_pick reads it.
+ *   rip_shard_begin: counts this pool's sets [0, num_sets) into d_sum and
+ *     builds its vertex -> sets index.
+ *   rip_shard_pick: *vertex = the largest entry of the summed d_sum, the
+ *     lowest id among equal ones; *gain = its value (0: nothing left).
+ *   rip_shard_cover: marks this pool's uncovered sets holding `vertex`
+ *     covered and writes its updated counts to d_sum; `gain` (the pick's
+ *     summed count) only sizes the launch.
+ * Any other rip_count / rip_select on the pool ends the sharded selection. */
+int rip_shard_begin(rip_pool *p, uint64_t num_sets, uint32_t *d_sum);
+int rip_shard_pick(rip_pool *p, const uint32_t *d_sum, uint32_t *vertex, uint64_t *gain);
+int rip_shard_cover(rip_pool *p, uint32_t vertex, uint64_t gain, uint32_t *d_sum);
 
 /* ---- IMM driver ----------------------------------------------------------- */
 /* Fields mirror IMMExecutionRecord (include/ripples/imm_execution_record.h:55-92)

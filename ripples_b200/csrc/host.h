@@ -309,6 +309,8 @@ struct PoolMeta {  // device-side bookkeeping block (one D2H reads it all)
   unsigned int fused_dirty;
 };
 
+constexpr uint64_t kNoShard = ~0ull;
+
 struct rip_pool {
   rip_ctx *ctx;
   rip_graph *g;
@@ -360,6 +362,11 @@ struct rip_pool {
   bool cg_done_zeroed = false;
   PinnedMem h_best;
   SelGraph sel_graph;                // the captured pick loop
+  // sharded selection: `count` holds this shard's counts over sets
+  // [0, shard_sets) with their index and covered flags (kNoShard: it does not)
+  uint64_t shard_sets = kNoShard;
+  DevMem shard_best;                 // the pick's packed key
+  PinnedMem h_shard_best;
   // selection profile: [0] count+index kernels and counts D2H, [1] heap build,
   // [2] pick loop, [3] heap pops, [4] picks, [5] candidate counts fetched,
   // [6] selections, [7] ms covering + fetching candidate counts, [8] fetches

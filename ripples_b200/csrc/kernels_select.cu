@@ -171,6 +171,43 @@ __global__ void __launch_bounds__(256) cover_kernel(CoverLaunch C) {
   }
 }
 
+// The pick of a sharded selection over the summed counts: the largest
+// count << 32 | ~v, i.e. the largest count and the lowest vertex id among
+// equal counts (thrust::max_element over the reduced counters,
+// include/ripples/mpi/find_most_influential.h:505-511).  Four counts per
+// 16-byte load; one atomicMax per block.
+__device__ __forceinline__ unsigned long long pick_key(uint32_t c, uint32_t v) {
+  return (unsigned long long)c << 32 | (uint32_t)~v;
+}
+
+__global__ void __launch_bounds__(256) argmax_kernel(const uint32_t *__restrict__ count,
+                                                     uint32_t n, unsigned long long *best) {
+  const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t n4 = n / 4;
+  const uint4 *c4 = reinterpret_cast<const uint4 *>(count);
+  unsigned long long key = 0;
+  for (uint64_t i = t; i < n4; i += stride) {
+    const uint4 q = c4[i];
+    const uint32_t v = (uint32_t)(i * 4);
+    key = max(key, pick_key(q.x, v));
+    key = max(key, pick_key(q.y, v + 1));
+    key = max(key, pick_key(q.z, v + 2));
+    key = max(key, pick_key(q.w, v + 3));
+  }
+  for (uint64_t v = n4 * 4 + t; v < n; v += stride) key = max(key, pick_key(count[v], (uint32_t)v));
+  for (int o = 16; o; o >>= 1) key = max(key, __shfl_xor_sync(FULL, key, o));
+  __shared__ unsigned long long s_key[8];
+  const uint32_t warp = threadIdx.x >> 5;
+  if (lane_id() == 0) s_key[warp] = key;
+  __syncthreads();
+  if (warp == 0) {
+    key = lane_id() < (blockDim.x >> 5) ? s_key[lane_id()] : 0ull;
+    for (int o = 4; o; o >>= 1) key = max(key, __shfl_xor_sync(FULL, key, o));
+    if (lane_id() == 0) atomicMax(best, key);
+  }
+}
+
 // A reference-heap pick in one launch: cover_kernel's work, then the last
 // block to finish (a completion ticket in *done) gathers the current counts of
 // the host's candidates for the next pick into `out` (mapped host memory),
@@ -606,6 +643,12 @@ void launch_build_inverted(const DevPool &P, uint64_t num_sets,
 void launch_cover(const CoverLaunch &C, cudaStream_t stream) {
   count_launches(1);
   cover_kernel<<<C.blocks, 256, 0, stream>>>(C);
+}
+
+void launch_argmax(const uint32_t *count, uint32_t n, unsigned long long *best, int blocks,
+                   cudaStream_t stream) {
+  count_launches(1);
+  argmax_kernel<<<blocks, 256, 0, stream>>>(count, n, best);
 }
 
 void launch_cover_gather(const CoverLaunch &C, const uint32_t *ids, uint32_t nids,

@@ -216,6 +216,10 @@ struct CoverLaunch {
   int blocks;
 };
 void launch_cover(const CoverLaunch &C, cudaStream_t stream);
+// *best = max over v < n of count[v] << 32 | ~v (the largest count, the
+// lowest id on ties) given *best == 0; count 16-byte aligned.
+void launch_argmax(const uint32_t *count, uint32_t n, unsigned long long *best, int blocks,
+                   cudaStream_t stream);
 // The cover, then the last block gathers count[ids[i]] (i < nids) into out
 // (ids and out 16-byte aligned), resets *done (a zeroed device word) and
 // writes epoch to *flag (mapped).

@@ -56,7 +56,7 @@ extern "C" int rip_pool_destroy(rip_pool *p) {
                    &p->s_cmax,  &p->s_dirty,   &p->s_best,   &p->s_desc,
 
                    &p->count,   &p->inv_off,   &p->inv_cur,  &p->inv,
-                   &p->covered,
+                   &p->covered, &p->shard_best,
                    &p->scan_sums, &p->sv_count, &p->sv_cur, &p->sv_sums};
   for (ServeSegment &g : p->sv_segs) {
     dfree(c, g.off);
@@ -79,6 +79,7 @@ extern "C" int rip_pool_clear(rip_pool *p) {
   for (double &x : p->sel_prof) x = 0.0;
   p->kernel_launches = 0;
   p->have_last_counts = false;
+  p->shard_sets = kNoShard;
   for (ServeSegment &g : p->sv_segs) {
     dfree(c, g.off);
     dfree(c, g.inv);
@@ -921,6 +922,26 @@ extern "C" int rip_pool_import(rip_pool *p, const uint64_t *offsets,
                         cudaMemcpyHostToDevice, c->stream));
   CK(c, cudaStreamSynchronize(c->stream));
   p->num_elems += P;
+  p->num_sets += count;
+  p->have_last_counts = false;
+  return RIP_OK;
+}
+
+// Appends `count` empty sets: the ids another shard samples.  An empty set
+// adds nothing to any count and is never covered, so a pool that holds its
+// own ids' sets and empty placeholders for the rest counts exactly its share.
+extern "C" int rip_pool_skip(rip_pool *p, uint64_t count) {
+  if (!p) return RIP_ERR_INVALID;
+  rip_ctx *c = p->ctx;
+  if (count == 0) return RIP_OK;
+  if (p->num_sets + count >= (1ull << 56))
+    return set_err(c, RIP_ERR_LIMIT, "rip_pool_skip: set ids are limited to 2^56");
+  CK(c, cudaSetDevice(c->device));
+  TRY(ensure_sets(p, p->num_sets + count));
+  CK(c, cudaMemsetAsync(ptr<uint64_t>(p->set_off) + p->num_sets, 0, sizeof(uint64_t) * count,
+                        c->stream));
+  CK(c, cudaMemsetAsync(ptr<uint32_t>(p->set_len) + p->num_sets, 0, sizeof(uint32_t) * count,
+                        c->stream));
   p->num_sets += count;
   p->have_last_counts = false;
   return RIP_OK;

@@ -169,6 +169,7 @@ static int count_sets(rip_pool *p, uint64_t S) {
   rip_ctx *c = p->ctx;
   const uint32_t n = p->g->n;
   TRY(settle_last_counts(p));
+  p->shard_sets = kNoShard;  // the count buffer no longer holds a shard's counts
   // padded to whole chunks of the device picks (the tail stays zero)
   const size_t chunk = sel_chunk_vertices();
   const size_t padded = ((size_t)n + chunk - 1) / chunk * chunk;
@@ -200,6 +201,44 @@ extern "C" int rip_select_counts(rip_pool *p, uint32_t *counts) {
   return RIP_OK;
 }
 
+// Counts sets [0, S) into `count`, builds the vertex -> sets index over them
+// (inv_off, inv) and clears their covered flags; *P_out = index length.
+static int prepare_cover(rip_pool *p, uint64_t S, uint64_t *P_out) {
+  rip_ctx *c = p->ctx;
+  const uint32_t n = p->g->n;
+  TRY(count_sets(p, S));
+  TRY(dalloc(c, p->inv_off, sizeof(uint64_t) * ((size_t)n + 1)));
+  TRY(dalloc(c, p->inv_cur, sizeof(uint64_t) * ((size_t)n + 1)));
+  TRY(dalloc(c, p->scan_sums, sizeof(uint64_t) * scan_block_sums_needed(n)));
+  launch_exclusive_scan(ptr<uint32_t>(p->count), ptr<uint64_t>(p->inv_off), n,
+                        ptr<uint64_t>(p->scan_sums), c->stream);
+  uint64_t P = 0;
+  CK(c, cudaMemcpyAsync(&P, ptr<uint64_t>(p->inv_off) + n, sizeof(uint64_t),
+                        cudaMemcpyDeviceToHost, c->stream));
+  CK(c, cudaMemcpyAsync(p->inv_cur.p, p->inv_off.p, sizeof(uint64_t) * ((size_t)n + 1),
+                        cudaMemcpyDeviceToDevice, c->stream));
+  CK(c, cudaStreamSynchronize(c->stream));
+  TRY(dalloc(c, p->inv, sizeof(uint32_t) * std::max<uint64_t>(P, 1)));
+  launch_build_inverted(p->view(), S, ptr<uint64_t>(p->inv_cur), ptr<uint32_t>(p->inv),
+                        c->num_sms * 8, c->stream);
+  CK(c, cudaGetLastError());
+  TRY(dalloc(c, p->covered, std::max<uint64_t>(S, 1)));
+  CK(c, cudaMemsetAsync(p->covered.p, 0, std::max<uint64_t>(S, 1), c->stream));
+  *P_out = P;
+  return RIP_OK;
+}
+
+static CoverLaunch cover_launch(rip_pool *p) {
+  CoverLaunch C;
+  C.P = p->view();
+  C.inv_off = ptr<uint64_t>(p->inv_off);
+  C.inv = ptr<uint32_t>(p->inv);
+  C.covered = ptr<uint8_t>(p->covered);
+  C.count = ptr<uint32_t>(p->count);
+  C.blocks = p->ctx->num_sms * 4;
+  return C;
+}
+
 extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
                           uint32_t *seeds, uint64_t *gains, uint32_t *num_seeds,
                           double *f) {
@@ -220,32 +259,9 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
   const auto t_sel0 = clk::now();
   // 1. histogram, 2. vertex -> sets index
   p->have_last_counts = false;  // superseded by this selection
-  TRY(count_sets(p, S));
-  TRY(dalloc(c, p->inv_off, sizeof(uint64_t) * ((size_t)n + 1)));
-  TRY(dalloc(c, p->inv_cur, sizeof(uint64_t) * ((size_t)n + 1)));
-  TRY(dalloc(c, p->scan_sums, sizeof(uint64_t) * scan_block_sums_needed(n)));
-  launch_exclusive_scan(ptr<uint32_t>(p->count), ptr<uint64_t>(p->inv_off), n,
-                        ptr<uint64_t>(p->scan_sums), c->stream);
   uint64_t P = 0;
-  CK(c, cudaMemcpyAsync(&P, ptr<uint64_t>(p->inv_off) + n, sizeof(uint64_t),
-                        cudaMemcpyDeviceToHost, c->stream));
-  CK(c, cudaMemcpyAsync(p->inv_cur.p, p->inv_off.p, sizeof(uint64_t) * ((size_t)n + 1),
-                        cudaMemcpyDeviceToDevice, c->stream));
-  CK(c, cudaStreamSynchronize(c->stream));
-  TRY(dalloc(c, p->inv, sizeof(uint32_t) * std::max<uint64_t>(P, 1)));
-  launch_build_inverted(p->view(), S, ptr<uint64_t>(p->inv_cur), ptr<uint32_t>(p->inv),
-                        c->num_sms * 8, c->stream);
-  CK(c, cudaGetLastError());
-  TRY(dalloc(c, p->covered, std::max<uint64_t>(S, 1)));
-  CK(c, cudaMemsetAsync(p->covered.p, 0, std::max<uint64_t>(S, 1), c->stream));
-
-  CoverLaunch C;
-  C.P = p->view();
-  C.inv_off = ptr<uint64_t>(p->inv_off);
-  C.inv = ptr<uint32_t>(p->inv);
-  C.covered = ptr<uint8_t>(p->covered);
-  C.count = ptr<uint32_t>(p->count);
-  C.blocks = c->num_sms * 4;
+  TRY(prepare_cover(p, S, &P));
+  CoverLaunch C = cover_launch(p);
 
   // whole-array count fetches land in the context's page-locked buffer and
   // are read there (no second host copy)
@@ -591,3 +607,78 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
   return RIP_OK;
 }
 
+// ---------------------------------------------------------------------------
+// sharded selection: one shard's part of a pick over sets split between
+// devices or processes (MPI FindMostInfluentialSet,
+// include/ripples/mpi/find_most_influential.h:449-690).  The caller sums the
+// shards' count arrays (d_sum, an all-reduce across ranks) between the calls.
+// ---------------------------------------------------------------------------
+
+static int check_sum_buffer(rip_ctx *c, const uint32_t *d_sum, const char *where) {
+  if (reinterpret_cast<uintptr_t>(d_sum) & 15)
+    return set_err(c, RIP_ERR_INVALID, "%s: d_sum must be 16-byte aligned", where);
+  return RIP_OK;
+}
+
+extern "C" int rip_shard_begin(rip_pool *p, uint64_t num_sets, uint32_t *d_sum) {
+  if (!p || !d_sum) return RIP_ERR_INVALID;
+  rip_ctx *c = p->ctx;
+  TRY(check_sum_buffer(c, d_sum, "rip_shard_begin"));
+  if (num_sets > p->num_sets)
+    return set_err(c, RIP_ERR_INVALID, "rip_shard_begin: %llu sets requested, pool has %llu",
+                   (unsigned long long)num_sets, (unsigned long long)p->num_sets);
+  if (num_sets >= (1ull << 32))
+    return set_err(c, RIP_ERR_LIMIT, "rip_shard_begin: at most 2^32-1 sets");
+  CK(c, cudaSetDevice(c->device));
+  p->have_last_counts = false;
+  uint64_t P = 0;
+  TRY(prepare_cover(p, num_sets, &P));
+  p->shard_sets = num_sets;
+  CK(c, cudaMemcpyAsync(d_sum, p->count.p, sizeof(uint32_t) * (size_t)p->g->n,
+                        cudaMemcpyDeviceToDevice, c->stream));
+  CK(c, cudaStreamSynchronize(c->stream));
+  return RIP_OK;
+}
+
+extern "C" int rip_shard_cover(rip_pool *p, uint32_t vertex, uint64_t gain, uint32_t *d_sum) {
+  if (!p || !d_sum) return RIP_ERR_INVALID;
+  rip_ctx *c = p->ctx;
+  TRY(check_sum_buffer(c, d_sum, "rip_shard_cover"));
+  if (p->shard_sets == kNoShard)
+    return set_err(c, RIP_ERR_STATE, "rip_shard_cover: no rip_shard_begin on this pool's "
+                   "current counts");
+  if (vertex >= p->g->n)
+    return set_err(c, RIP_ERR_INVALID, "rip_shard_cover: vertex %u out of range", vertex);
+  CK(c, cudaSetDevice(c->device));
+  CoverLaunch C = cover_launch(p);
+  C.vertex = vertex;
+  C.blocks = (int)std::min<uint64_t>((uint64_t)c->num_sms * 16,
+                                     std::max<uint64_t>(1, (gain + 7) / 8));
+  launch_cover(C, c->stream);
+  CK(c, cudaGetLastError());
+  CK(c, cudaMemcpyAsync(d_sum, p->count.p, sizeof(uint32_t) * (size_t)p->g->n,
+                        cudaMemcpyDeviceToDevice, c->stream));
+  CK(c, cudaStreamSynchronize(c->stream));
+  return RIP_OK;
+}
+
+extern "C" int rip_shard_pick(rip_pool *p, const uint32_t *d_sum, uint32_t *vertex,
+                              uint64_t *gain) {
+  if (!p || !d_sum || !vertex || !gain) return RIP_ERR_INVALID;
+  rip_ctx *c = p->ctx;
+  TRY(check_sum_buffer(c, d_sum, "rip_shard_pick"));
+  CK(c, cudaSetDevice(c->device));
+  TRY(dalloc(c, p->shard_best, 8));
+  TRY(p->h_shard_best.ensure(c, 8));
+  CK(c, cudaMemsetAsync(p->shard_best.p, 0, 8, c->stream));
+  launch_argmax(d_sum, p->g->n, ptr<unsigned long long>(p->shard_best), c->num_sms * 4,
+                c->stream);
+  CK(c, cudaGetLastError());
+  CK(c, cudaMemcpyAsync(p->h_shard_best.p, p->shard_best.p, 8, cudaMemcpyDeviceToHost,
+                        c->stream));
+  CK(c, cudaStreamSynchronize(c->stream));
+  const unsigned long long key = *static_cast<const unsigned long long *>(p->h_shard_best.p);
+  *vertex = ~(uint32_t)(key & 0xFFFFFFFFull);
+  *gain = key >> 32;
+  return RIP_OK;
+}

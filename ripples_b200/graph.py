@@ -223,6 +223,7 @@ class Context:
         h = ctypes.c_void_p()
         check(lib.rip_ctx_create(device, hbm_budget, ctypes.byref(h)), "rip_ctx_create")
         self.h = h
+        self.device = device
         self._children = weakref.WeakSet()
 
     def close(self) -> None:
@@ -489,6 +490,30 @@ class Pool:
 
     def sample(self, count: int, seed: int = 0, sampler: int = _lib.SAMPLER_AUTO) -> None:
         self._chk(lib.rip_sample(self.h, seed, count, sampler), "rip_sample")
+
+    def skip(self, count: int) -> None:
+        """Appends ``count`` empty sets (ids another shard samples;
+        ``rip_pool_skip``)."""
+        self._chk(lib.rip_pool_skip(self.h, count), "rip_pool_skip")
+
+    def shard_begin(self, num_sets: int, d_sum: int) -> None:
+        """This pool's counts over sets [0, num_sets) into the device array
+        at address ``d_sum`` (n uint32), and its vertex -> sets index
+        (``rip_shard_begin``)."""
+        self._chk(lib.rip_shard_begin(self.h, num_sets, d_sum), "rip_shard_begin")
+
+    def shard_pick(self, d_sum: int) -> Tuple[int, int]:
+        """(vertex, count) of the largest entry of the device array at
+        ``d_sum``, lowest id on ties (``rip_shard_pick``)."""
+        v, g = ctypes.c_uint32(), ctypes.c_uint64()
+        self._chk(lib.rip_shard_pick(self.h, d_sum, ctypes.byref(v), ctypes.byref(g)),
+                  "rip_shard_pick")
+        return v.value, g.value
+
+    def shard_cover(self, vertex: int, gain: int, d_sum: int) -> None:
+        """Covers this pool's sets holding ``vertex`` and writes its updated
+        counts to ``d_sum`` (``rip_shard_cover``)."""
+        self._chk(lib.rip_shard_cover(self.h, vertex, gain, d_sum), "rip_shard_cover")
 
     def export(self, first: int = 0, count: Optional[int] = None) -> Tuple[np.ndarray, np.ndarray]:
         if count is None:

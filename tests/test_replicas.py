@@ -67,7 +67,8 @@ def test_reference_arm_runs_on_rank_zero_only():
     assert bench.reference_arm(Args(), bench.WORKLOADS["lt20"], world=2, rank=1) == 0
 
 
-@pytest.mark.parametrize("workload", ["b1", "s1", "ic24_samplers", "ic24u_samplers"])
+@pytest.mark.parametrize("workload", ["b1", "s1", "ic24_samplers", "ic24u_samplers",
+                                      "ic24_sharded"])
 def test_reference_arm_of_other_workloads(workload, capsys):
     # batching, serving and the comparison of this library's samplers have no
     # runnable reference counterpart: one unavailable line, exit 0, no GPU
