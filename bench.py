@@ -91,7 +91,7 @@ WORKLOADS = {
     # out-degree on R-MAT 2^20 (16*2^20 draws, IC p ~ U(0,0.1)), 20000
     # replicas a step; the reference's own simulator timed beside it
     # one IMM per step with its sets split across the ranks (and --shards
-    # pools per rank), counts summed by all_reduce at every pick; lowest-id
+    # pools per rank), counts combined across them at every pick; lowest-id
     # picks, so each step's answer is the single-pool one (strong scaling)
     "ic24_sharded": dict(name="imm_sharded_ic_rmat24_deg32_wc_k100_eps0.13", kind="sharded",
                          scale=24, draws=32 << 24, model="IC", k=100, eps=0.13, weights="wc"),
@@ -463,6 +463,8 @@ def main():
     ap.add_argument("--workload", default="ic24", choices=sorted(WORKLOADS))
     ap.add_argument("--shards", type=int, default=1,
                     help="ic24_sharded: pools (shards) per process")
+    ap.add_argument("--exchange", default="auto", choices=["auto", "sparse", "dense"],
+                    help="ic24_sharded: per-pick exchange (decrement lists or whole counts)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--serve-scales", default="18,20,22,24",
                     help="s1: R-MAT scales of the resident graphs")
@@ -1223,8 +1225,10 @@ def run_p3(args, w, world, rank, local):
 def run_sharded(args, w, world, rank, local):
     """One IMM per step on the 2^24 weighted-cascade graph with its sets split
     across every rank's --shards pools (ripples_b200.sharded): each rank
-    samples its id ranges, the per-pick counts are summed in process and by
-    NCCL all_reduce.  Whole-job sets/s of one IMM (strong scaling), timed on
+    samples its id ranges; the counts are summed once per selection (in
+    process, then NCCL all_reduce) and after each pick the shards exchange
+    their decrement lists (all_gather; --exchange sparse) or sum their whole
+    counts again (--exchange dense).  Whole-job sets/s of one IMM (strong scaling), timed on
     the device from a synchronised start to a synchronised end, max over
     ranks; at one GPU the single-pool IMM under the same (lowest-id)
     tie-break is timed beside it."""
@@ -1245,7 +1249,8 @@ def run_sharded(args, w, world, rank, local):
     def one(step):
         for s in shards:
             s.pool.clear()
-        return imm_sharded(shards, w["k"], w["eps"], 1.0, seed=step, group=group)
+        return imm_sharded(shards, w["k"], w["eps"], 1.0, seed=step, group=group,
+                           exchange=args.exchange)
 
     for i in range(args.warmup):
         one(1000 + i)
@@ -1291,12 +1296,14 @@ def run_sharded(args, w, world, rank, local):
                 "config": {"workload": w["name"], "n": dg.n, "m": dg.m, "k": w["k"],
                            "epsilon": w["eps"], "shards_per_rank": len(shards),
                            "shards": world * len(shards), "tiebreak": "lowest_id",
+                           "exchange": recs[0]["exchange"] if recs else args.exchange,
                            "l2": l2_note(8 * dg.m + 4 * (dg.n + 1))},
                 "sets_per_step": sets / args.steps,
                 "picks_per_step": picks / args.steps,
                 "select_ms_per_step": sum(sum(r["round_select_ms"]) + r["select_ms"]
                                           for r in recs) / args.steps,
-                "allreduce_ms_per_step": sum(r["allreduce_ms"] for r in recs) / args.steps,
+                "collective_ms_per_step": sum(r["allreduce_ms"] for r in recs) / args.steps,
+                "exchanged_per_step": sum(r["exchanged"] for r in recs) / args.steps,
                 "single_pool": single, "clocks": clk}
         print(json.dumps(line))
     for s in shards:

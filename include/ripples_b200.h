@@ -329,21 +329,35 @@ int rip_count(rip_pool *p, uint64_t num_sets, uint32_t *counts);
  * FindMostInfluentialSet (include/ripples/mpi/find_most_influential.h:449-690:
  * per-pick reduction of the vertex counters, the maximum picked, every rank
  * updating its own sets).  d_sum is a device array of n uint32 (16-byte
- * aligned) on the pool's device; each call below returns once its work on
- * the context stream is done, so the caller may sum the shards' d_sum arrays
- * (an all-reduce) on any stream, and must finish that sum before
- * rip_shard_pick reads it.
- *   rip_shard_begin: counts this pool's sets [0, num_sets) into d_sum and
- *     builds its vertex -> sets index.
+ * aligned) on the pool's device that holds the summed counts; every call
+ * returns once its work on the context stream is done, so the caller may
+ * combine the shards' arrays on any stream (an all-reduce, an all-gather),
+ * and must finish that before the next call reads them.
+ *   rip_shard_begin: counts this pool's sets [0, num_sets) into d_sum (the
+ *     caller then sums the shards' arrays) and builds its vertex -> sets
+ *     index; *elements = those sets' element count.
  *   rip_shard_pick: *vertex = the largest entry of the summed d_sum, the
- *     lowest id among equal ones; *gain = its value (0: nothing left).
- *   rip_shard_cover: marks this pool's uncovered sets holding `vertex`
- *     covered and writes its updated counts to d_sum; `gain` (the pick's
- *     summed count) only sizes the launch.
+ *     lowest id among equal ones; *gain = its value (0: nothing left).  The
+ *     maximum of every 2048 entries is kept: a pick that follows
+ *     rip_shard_apply calls on the same array rescans only the entries they
+ *     changed (so change it between those picks only through
+ *     rip_shard_apply), any other pick rescans the whole array.
+ *   Then per pick, one of two exchanges:
+ *   rip_shard_cover (dense): covers this pool's uncovered sets holding
+ *     `vertex` and writes its updated counts to d_sum, which the caller sums
+ *     again (n values per pick, as the reference's MPI_Reduce);
+ *   rip_shard_cover_list (sparse): covers them and writes their members to
+ *     d_dec (capacity >= *elements of rip_shard_begin), *count of them; the
+ *     caller gathers every shard's list and rip_shard_apply subtracts one per
+ *     entry from the summed d_sum (the decrements only, not n values).
+ *   `gain` (the pick's summed count) only sizes the cover launch.
  * Any other rip_count / rip_select on the pool ends the sharded selection. */
-int rip_shard_begin(rip_pool *p, uint64_t num_sets, uint32_t *d_sum);
+int rip_shard_begin(rip_pool *p, uint64_t num_sets, uint32_t *d_sum, uint64_t *elements);
 int rip_shard_pick(rip_pool *p, const uint32_t *d_sum, uint32_t *vertex, uint64_t *gain);
 int rip_shard_cover(rip_pool *p, uint32_t vertex, uint64_t gain, uint32_t *d_sum);
+int rip_shard_cover_list(rip_pool *p, uint32_t vertex, uint64_t gain, uint32_t *d_dec,
+                         uint64_t capacity, uint64_t *count);
+int rip_shard_apply(rip_pool *p, uint32_t *d_sum, const uint32_t *d_dec, uint64_t count);
 
 /* ---- IMM driver ----------------------------------------------------------- */
 /* Fields mirror IMMExecutionRecord (include/ripples/imm_execution_record.h:55-92)

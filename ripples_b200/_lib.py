@@ -156,9 +156,11 @@ SIGNATURES = {
     "rip_select_profile": (I32, [P, P]),
     "rip_count": (I32, [P, U64, P]),
     "rip_pool_skip": (I32, [P, U64]),
-    "rip_shard_begin": (I32, [P, U64, P]),
+    "rip_shard_begin": (I32, [P, U64, P, ctypes.POINTER(U64)]),
     "rip_shard_pick": (I32, [P, P, ctypes.POINTER(U32), ctypes.POINTER(U64)]),
     "rip_shard_cover": (I32, [P, U32, U64, P]),
+    "rip_shard_cover_list": (I32, [P, U32, U64, P, U64, ctypes.POINTER(U64)]),
+    "rip_shard_apply": (I32, [P, P, P, U64]),
     "rip_imm": (I32, [P, P, U32, DBL, DBL, U64, I32, I32, P, ctypes.POINTER(U32),
                       ctypes.POINTER(ImmRecord)]),
     "rip_imm_pool": (I32, [P, U32, DBL, DBL, U64, I32, I32, P, ctypes.POINTER(U32),

@@ -365,8 +365,12 @@ struct rip_pool {
   // sharded selection: `count` holds this shard's counts over sets
   // [0, shard_sets) with their index and covered flags (kNoShard: it does not)
   uint64_t shard_sets = kNoShard;
-  DevMem shard_best;                 // the pick's packed key
-  PinnedMem h_shard_best;
+  uint64_t shard_elems = 0;          // elements of those sets (bound of a decrement list)
+  const void *shard_sum = nullptr;   // the summed array whose chunk maxima are cached
+  bool shard_cache_ok = false;       // shard_cmax + dirty flags describe shard_sum
+  DevMem shard_cmax, shard_dirty;    // per kPickChunk counts: max key, changed flag
+  DevMem shard_meta;                 // [0] the pick's key, [1] decrement-list cursor
+  PinnedMem h_shard_meta;
   // selection profile: [0] count+index kernels and counts D2H, [1] heap build,
   // [2] pick loop, [3] heap pops, [4] picks, [5] candidate counts fetched,
   // [6] selections, [7] ms covering + fetching candidate counts, [8] fetches

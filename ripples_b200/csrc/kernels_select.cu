@@ -174,28 +174,75 @@ __global__ void __launch_bounds__(256) cover_kernel(CoverLaunch C) {
 // The pick of a sharded selection over the summed counts: the largest
 // count << 32 | ~v, i.e. the largest count and the lowest vertex id among
 // equal counts (thrust::max_element over the reduced counters,
-// include/ripples/mpi/find_most_influential.h:505-511).  Four counts per
-// 16-byte load; one atomicMax per block.
+// include/ripples/mpi/find_most_influential.h:505-511).
 __device__ __forceinline__ unsigned long long pick_key(uint32_t c, uint32_t v) {
   return (unsigned long long)c << 32 | (uint32_t)~v;
 }
 
-__global__ void __launch_bounds__(256) argmax_kernel(const uint32_t *__restrict__ count,
-                                                     uint32_t n, unsigned long long *best) {
-  const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  const uint64_t n4 = n / 4;
-  const uint4 *c4 = reinterpret_cast<const uint4 *>(count);
-  unsigned long long key = 0;
-  for (uint64_t i = t; i < n4; i += stride) {
-    const uint4 q = c4[i];
-    const uint32_t v = (uint32_t)(i * 4);
-    key = max(key, pick_key(q.x, v));
-    key = max(key, pick_key(q.y, v + 1));
-    key = max(key, pick_key(q.z, v + 2));
-    key = max(key, pick_key(q.w, v + 3));
+// A sharded pick's cover with its decrements listed instead of applied:
+// marks this shard's uncovered sets holding the vertex covered and appends
+// their members to `out` (each entry: that vertex's summed count drops by
+// one), a warp per set as cover_kernel.  At most the shard's element count
+// is written.
+__global__ void __launch_bounds__(256) cover_list_kernel(CoverLaunch C, uint32_t *out,
+                                                         unsigned long long *cursor) {
+  const uint64_t gw = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const uint32_t lane = lane_id();
+  const uint64_t lo = C.inv_off[C.vertex], hi = C.inv_off[C.vertex + 1];
+  for (uint64_t i = lo + gw; i < hi; i += nw) {
+    const uint32_t s = C.inv[i];
+    if (C.covered[s]) continue;  // warp-uniform
+    const uint32_t len = C.P.set_len[s];
+    const uint64_t off = C.P.set_off[s];
+    unsigned long long b = 0;
+    if (lane == 0) {
+      C.covered[s] = 1;
+      b = atomicAdd(cursor, (unsigned long long)len);
+    }
+    b = __shfl_sync(FULL, b, 0);
+    for (uint32_t j = lane; j < len; j += 32) out[b + j] = C.P.vtx[off + j];
   }
-  for (uint64_t v = n4 * 4 + t; v < n; v += stride) key = max(key, pick_key(count[v], (uint32_t)v));
+}
+
+// Summed counts minus the listed decrements; marks the chunks they touch for
+// the next pick (entries >= n are skipped).
+__global__ void __launch_bounds__(256) apply_decrements_kernel(uint32_t *count, uint32_t n,
+                                                               const uint32_t *dec, uint64_t m,
+                                                               uint8_t *dirty) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < m; i += stride) {
+    const uint32_t v = dec[i];
+    if (v < n) {
+      atomicSub(count + v, 1u);
+      dirty[v / kPickChunk] = 1;
+    }
+  }
+}
+
+// The pick key maximum of every dirty chunk of kPickChunk counts, one block
+// per chunk (clean chunks return at once); clears the chunk's flag.
+__global__ void __launch_bounds__(256) chunk_max_kernel(const uint32_t *__restrict__ count,
+                                                        uint32_t n, uint8_t *dirty,
+                                                        unsigned long long *cmax) {
+  const uint32_t chunk = blockIdx.x;
+  if (!dirty[chunk]) return;
+  const uint32_t lo = chunk * kPickChunk;
+  const uint32_t hi = min(n, lo + kPickChunk);
+  unsigned long long key = 0;
+  if (hi - lo == kPickChunk) {  // whole chunk: 16-byte loads (count 16-byte aligned)
+    const uint4 *c4 = reinterpret_cast<const uint4 *>(count + lo);
+    for (uint32_t i = threadIdx.x; i < kPickChunk / 4; i += blockDim.x) {
+      const uint4 q = c4[i];
+      const uint32_t v = lo + i * 4;
+      key = max(key, pick_key(q.x, v));
+      key = max(key, pick_key(q.y, v + 1));
+      key = max(key, pick_key(q.z, v + 2));
+      key = max(key, pick_key(q.w, v + 3));
+    }
+  } else {
+    for (uint32_t v = lo + threadIdx.x; v < hi; v += blockDim.x) key = max(key, pick_key(count[v], v));
+  }
   for (int o = 16; o; o >>= 1) key = max(key, __shfl_xor_sync(FULL, key, o));
   __shared__ unsigned long long s_key[8];
   const uint32_t warp = threadIdx.x >> 5;
@@ -204,7 +251,28 @@ __global__ void __launch_bounds__(256) argmax_kernel(const uint32_t *__restrict_
   if (warp == 0) {
     key = lane_id() < (blockDim.x >> 5) ? s_key[lane_id()] : 0ull;
     for (int o = 4; o; o >>= 1) key = max(key, __shfl_xor_sync(FULL, key, o));
-    if (lane_id() == 0) atomicMax(best, key);
+    if (lane_id() == 0) {
+      cmax[chunk] = key;
+      dirty[chunk] = 0;
+    }
+  }
+}
+
+// *best = the maximum of cmax[0, nchunks) (one block).
+__global__ void __launch_bounds__(1024) cmax_max_kernel(const unsigned long long *cmax,
+                                                        uint32_t nchunks,
+                                                        unsigned long long *best) {
+  unsigned long long key = 0;
+  for (uint32_t i = threadIdx.x; i < nchunks; i += blockDim.x) key = max(key, cmax[i]);
+  for (int o = 16; o; o >>= 1) key = max(key, __shfl_xor_sync(FULL, key, o));
+  __shared__ unsigned long long s_key[32];
+  const uint32_t warp = threadIdx.x >> 5;
+  if (lane_id() == 0) s_key[warp] = key;
+  __syncthreads();
+  if (warp == 0) {
+    key = lane_id() < (blockDim.x >> 5) ? s_key[lane_id()] : 0ull;
+    for (int o = 16; o; o >>= 1) key = max(key, __shfl_xor_sync(FULL, key, o));
+    if (lane_id() == 0) *best = key;
   }
 }
 
@@ -645,10 +713,24 @@ void launch_cover(const CoverLaunch &C, cudaStream_t stream) {
   cover_kernel<<<C.blocks, 256, 0, stream>>>(C);
 }
 
-void launch_argmax(const uint32_t *count, uint32_t n, unsigned long long *best, int blocks,
-                   cudaStream_t stream) {
+void launch_cover_list(const CoverLaunch &C, uint32_t *out, unsigned long long *cursor,
+                       cudaStream_t stream) {
   count_launches(1);
-  argmax_kernel<<<blocks, 256, 0, stream>>>(count, n, best);
+  cover_list_kernel<<<C.blocks, 256, 0, stream>>>(C, out, cursor);
+}
+
+void launch_apply_decrements(uint32_t *count, uint32_t n, const uint32_t *dec, uint64_t m,
+                             uint8_t *dirty, int blocks, cudaStream_t stream) {
+  count_launches(1);
+  apply_decrements_kernel<<<blocks, 256, 0, stream>>>(count, n, dec, m, dirty);
+}
+
+void launch_chunk_pick(const uint32_t *count, uint32_t n, uint8_t *dirty,
+                       unsigned long long *cmax, unsigned long long *best, cudaStream_t stream) {
+  const uint32_t nchunks = (n + kPickChunk - 1) / kPickChunk;
+  count_launches(2);
+  chunk_max_kernel<<<nchunks, 256, 0, stream>>>(count, n, dirty, cmax);
+  cmax_max_kernel<<<1, 1024, 0, stream>>>(cmax, nchunks, best);
 }
 
 void launch_cover_gather(const CoverLaunch &C, const uint32_t *ids, uint32_t nids,

@@ -216,10 +216,19 @@ struct CoverLaunch {
   int blocks;
 };
 void launch_cover(const CoverLaunch &C, cudaStream_t stream);
-// *best = max over v < n of count[v] << 32 | ~v (the largest count, the
-// lowest id on ties) given *best == 0; count 16-byte aligned.
-void launch_argmax(const uint32_t *count, uint32_t n, unsigned long long *best, int blocks,
-                   cudaStream_t stream);
+// Sharded picks (keys count << 32 | ~v: the largest count, the lowest id on
+// ties; counts 16-byte aligned).  cover_list: the cover, with the
+// members of the newly covered sets appended to out[*cursor ...] instead of
+// decremented.  apply_decrements: count[dec[i]] -= 1 (dec[i] < n), marking
+// dirty[dec[i] / kPickChunk].  chunk_pick: recomputes the dirty chunks'
+// maxima into cmax (clearing their flags), then *best = max over cmax.
+constexpr uint32_t kPickChunk = 2048;
+void launch_cover_list(const CoverLaunch &C, uint32_t *out, unsigned long long *cursor,
+                       cudaStream_t stream);
+void launch_apply_decrements(uint32_t *count, uint32_t n, const uint32_t *dec, uint64_t m,
+                             uint8_t *dirty, int blocks, cudaStream_t stream);
+void launch_chunk_pick(const uint32_t *count, uint32_t n, uint8_t *dirty,
+                       unsigned long long *cmax, unsigned long long *best, cudaStream_t stream);
 // The cover, then the last block gathers count[ids[i]] (i < nids) into out
 // (ids and out 16-byte aligned), resets *done (a zeroed device word) and
 // writes epoch to *flag (mapped).

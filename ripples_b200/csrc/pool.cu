@@ -56,7 +56,7 @@ extern "C" int rip_pool_destroy(rip_pool *p) {
                    &p->s_cmax,  &p->s_dirty,   &p->s_best,   &p->s_desc,
 
                    &p->count,   &p->inv_off,   &p->inv_cur,  &p->inv,
-                   &p->covered, &p->shard_best,
+                   &p->covered, &p->shard_cmax, &p->shard_dirty, &p->shard_meta,
                    &p->scan_sums, &p->sv_count, &p->sv_cur, &p->sv_sums};
   for (ServeSegment &g : p->sv_segs) {
     dfree(c, g.off);

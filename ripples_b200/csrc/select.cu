@@ -611,17 +611,31 @@ extern "C" int rip_select(rip_pool *p, uint64_t S, uint32_t k, int tiebreak,
 // sharded selection: one shard's part of a pick over sets split between
 // devices or processes (MPI FindMostInfluentialSet,
 // include/ripples/mpi/find_most_influential.h:449-690).  The caller sums the
-// shards' count arrays (d_sum, an all-reduce across ranks) between the calls.
+// shards' counts into d_sum once (an all-reduce across ranks), then per pick
+// either sums the shards' updated counts again (rip_shard_cover) or applies
+// every shard's decrement list to d_sum (rip_shard_cover_list +
+// rip_shard_apply).  Picks keep the maximum of each kPickChunk counts of
+// d_sum; the next pick on the same array recomputes only the chunks that
+// rip_shard_apply calls touched since, and all of them when none ran (the
+// array may have been rewritten, or be a new one at the same address).
 // ---------------------------------------------------------------------------
 
-static int check_sum_buffer(rip_ctx *c, const uint32_t *d_sum, const char *where) {
-  if (reinterpret_cast<uintptr_t>(d_sum) & 15)
-    return set_err(c, RIP_ERR_INVALID, "%s: d_sum must be 16-byte aligned", where);
+static int check_sum_buffer(rip_ctx *c, const void *d, const char *where) {
+  if (!d || (reinterpret_cast<uintptr_t>(d) & 15))
+    return set_err(c, RIP_ERR_INVALID, "%s: device array missing or not 16-byte aligned", where);
   return RIP_OK;
 }
 
-extern "C" int rip_shard_begin(rip_pool *p, uint64_t num_sets, uint32_t *d_sum) {
-  if (!p || !d_sum) return RIP_ERR_INVALID;
+static int shard_state(rip_pool *p, const char *where) {
+  if (p->shard_sets == kNoShard)
+    return set_err(p->ctx, RIP_ERR_STATE, "%s: no rip_shard_begin on this pool's current counts",
+                   where);
+  return RIP_OK;
+}
+
+extern "C" int rip_shard_begin(rip_pool *p, uint64_t num_sets, uint32_t *d_sum,
+                               uint64_t *elements) {
+  if (!p) return RIP_ERR_INVALID;
   rip_ctx *c = p->ctx;
   TRY(check_sum_buffer(c, d_sum, "rip_shard_begin"));
   if (num_sets > p->num_sets)
@@ -633,52 +647,111 @@ extern "C" int rip_shard_begin(rip_pool *p, uint64_t num_sets, uint32_t *d_sum) 
   p->have_last_counts = false;
   uint64_t P = 0;
   TRY(prepare_cover(p, num_sets, &P));
+  const uint32_t nchunks = (p->g->n + kPickChunk - 1) / kPickChunk;
+  TRY(dalloc(c, p->shard_cmax, (size_t)nchunks * 8));
+  TRY(dalloc(c, p->shard_dirty, nchunks));
+  TRY(dalloc(c, p->shard_meta, 16));
+  TRY(p->h_shard_meta.ensure(c, 16));
   p->shard_sets = num_sets;
+  p->shard_elems = P;
+  p->shard_cache_ok = false;
   CK(c, cudaMemcpyAsync(d_sum, p->count.p, sizeof(uint32_t) * (size_t)p->g->n,
                         cudaMemcpyDeviceToDevice, c->stream));
   CK(c, cudaStreamSynchronize(c->stream));
-  return RIP_OK;
-}
-
-extern "C" int rip_shard_cover(rip_pool *p, uint32_t vertex, uint64_t gain, uint32_t *d_sum) {
-  if (!p || !d_sum) return RIP_ERR_INVALID;
-  rip_ctx *c = p->ctx;
-  TRY(check_sum_buffer(c, d_sum, "rip_shard_cover"));
-  if (p->shard_sets == kNoShard)
-    return set_err(c, RIP_ERR_STATE, "rip_shard_cover: no rip_shard_begin on this pool's "
-                   "current counts");
-  if (vertex >= p->g->n)
-    return set_err(c, RIP_ERR_INVALID, "rip_shard_cover: vertex %u out of range", vertex);
-  CK(c, cudaSetDevice(c->device));
-  CoverLaunch C = cover_launch(p);
-  C.vertex = vertex;
-  C.blocks = (int)std::min<uint64_t>((uint64_t)c->num_sms * 16,
-                                     std::max<uint64_t>(1, (gain + 7) / 8));
-  launch_cover(C, c->stream);
-  CK(c, cudaGetLastError());
-  CK(c, cudaMemcpyAsync(d_sum, p->count.p, sizeof(uint32_t) * (size_t)p->g->n,
-                        cudaMemcpyDeviceToDevice, c->stream));
-  CK(c, cudaStreamSynchronize(c->stream));
+  if (elements) *elements = P;
   return RIP_OK;
 }
 
 extern "C" int rip_shard_pick(rip_pool *p, const uint32_t *d_sum, uint32_t *vertex,
                               uint64_t *gain) {
-  if (!p || !d_sum || !vertex || !gain) return RIP_ERR_INVALID;
+  if (!p || !vertex || !gain) return RIP_ERR_INVALID;
   rip_ctx *c = p->ctx;
   TRY(check_sum_buffer(c, d_sum, "rip_shard_pick"));
+  TRY(shard_state(p, "rip_shard_pick"));
   CK(c, cudaSetDevice(c->device));
-  TRY(dalloc(c, p->shard_best, 8));
-  TRY(p->h_shard_best.ensure(c, 8));
-  CK(c, cudaMemsetAsync(p->shard_best.p, 0, 8, c->stream));
-  launch_argmax(d_sum, p->g->n, ptr<unsigned long long>(p->shard_best), c->num_sms * 4,
-                c->stream);
+  const uint32_t n = p->g->n;
+  const uint32_t nchunks = (n + kPickChunk - 1) / kPickChunk;
+  if (!p->shard_cache_ok || d_sum != p->shard_sum)
+    CK(c, cudaMemsetAsync(p->shard_dirty.p, 1, nchunks, c->stream));
+  unsigned long long *meta = ptr<unsigned long long>(p->shard_meta);
+  launch_chunk_pick(d_sum, n, ptr<uint8_t>(p->shard_dirty), ptr<unsigned long long>(p->shard_cmax),
+                    meta, c->stream);
   CK(c, cudaGetLastError());
-  CK(c, cudaMemcpyAsync(p->h_shard_best.p, p->shard_best.p, 8, cudaMemcpyDeviceToHost,
-                        c->stream));
+  CK(c, cudaMemcpyAsync(p->h_shard_meta.p, meta, 8, cudaMemcpyDeviceToHost, c->stream));
   CK(c, cudaStreamSynchronize(c->stream));
-  const unsigned long long key = *static_cast<const unsigned long long *>(p->h_shard_best.p);
+  p->shard_sum = d_sum;
+  p->shard_cache_ok = false;  // until a rip_shard_apply on this array
+  const unsigned long long key = *static_cast<const unsigned long long *>(p->h_shard_meta.p);
   *vertex = ~(uint32_t)(key & 0xFFFFFFFFull);
   *gain = key >> 32;
+  return RIP_OK;
+}
+
+static CoverLaunch shard_cover_launch(rip_pool *p, uint32_t vertex, uint64_t gain) {
+  CoverLaunch C = cover_launch(p);
+  C.vertex = vertex;
+  C.blocks = (int)std::min<uint64_t>((uint64_t)p->ctx->num_sms * 16,
+                                     std::max<uint64_t>(1, (gain + 7) / 8));
+  return C;
+}
+
+extern "C" int rip_shard_cover(rip_pool *p, uint32_t vertex, uint64_t gain, uint32_t *d_sum) {
+  if (!p) return RIP_ERR_INVALID;
+  rip_ctx *c = p->ctx;
+  TRY(check_sum_buffer(c, d_sum, "rip_shard_cover"));
+  TRY(shard_state(p, "rip_shard_cover"));
+  if (vertex >= p->g->n)
+    return set_err(c, RIP_ERR_INVALID, "rip_shard_cover: vertex %u out of range", vertex);
+  CK(c, cudaSetDevice(c->device));
+  launch_cover(shard_cover_launch(p, vertex, gain), c->stream);
+  CK(c, cudaGetLastError());
+  CK(c, cudaMemcpyAsync(d_sum, p->count.p, sizeof(uint32_t) * (size_t)p->g->n,
+                        cudaMemcpyDeviceToDevice, c->stream));
+  CK(c, cudaStreamSynchronize(c->stream));
+  p->shard_cache_ok = false;  // the caller rewrites d_sum with the new sums
+  return RIP_OK;
+}
+
+extern "C" int rip_shard_cover_list(rip_pool *p, uint32_t vertex, uint64_t gain,
+                                    uint32_t *d_dec, uint64_t capacity, uint64_t *count) {
+  if (!p || !count) return RIP_ERR_INVALID;
+  rip_ctx *c = p->ctx;
+  TRY(shard_state(p, "rip_shard_cover_list"));
+  if (vertex >= p->g->n)
+    return set_err(c, RIP_ERR_INVALID, "rip_shard_cover_list: vertex %u out of range", vertex);
+  if (capacity < p->shard_elems || (p->shard_elems && !d_dec))
+    return set_err(c, RIP_ERR_INVALID,
+                   "rip_shard_cover_list: capacity %llu below the shard's %llu elements",
+                   (unsigned long long)capacity, (unsigned long long)p->shard_elems);
+  CK(c, cudaSetDevice(c->device));
+  unsigned long long *cursor = ptr<unsigned long long>(p->shard_meta) + 1;
+  CK(c, cudaMemsetAsync(cursor, 0, 8, c->stream));
+  if (p->shard_elems) {
+    launch_cover_list(shard_cover_launch(p, vertex, gain), d_dec, cursor, c->stream);
+    CK(c, cudaGetLastError());
+  }
+  unsigned long long *h = static_cast<unsigned long long *>(p->h_shard_meta.p);
+  CK(c, cudaMemcpyAsync(h + 1, cursor, 8, cudaMemcpyDeviceToHost, c->stream));
+  CK(c, cudaStreamSynchronize(c->stream));
+  *count = h[1];
+  return RIP_OK;
+}
+
+extern "C" int rip_shard_apply(rip_pool *p, uint32_t *d_sum, const uint32_t *d_dec,
+                               uint64_t count) {
+  if (!p || (count && !d_dec)) return RIP_ERR_INVALID;
+  rip_ctx *c = p->ctx;
+  TRY(check_sum_buffer(c, d_sum, "rip_shard_apply"));
+  TRY(shard_state(p, "rip_shard_apply"));
+  CK(c, cudaSetDevice(c->device));
+  // the cached chunk maxima describe d_sum once this apply's chunks are marked
+  p->shard_cache_ok = d_sum == p->shard_sum;
+  if (count) {
+    const int blocks = (int)std::min<uint64_t>((uint64_t)c->num_sms * 8, (count + 255) / 256);
+    launch_apply_decrements(d_sum, p->g->n, d_dec, count, ptr<uint8_t>(p->shard_dirty), blocks,
+                            c->stream);
+    CK(c, cudaGetLastError());
+  }
+  CK(c, cudaStreamSynchronize(c->stream));
   return RIP_OK;
 }

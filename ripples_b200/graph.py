@@ -496,11 +496,14 @@ class Pool:
         ``rip_pool_skip``)."""
         self._chk(lib.rip_pool_skip(self.h, count), "rip_pool_skip")
 
-    def shard_begin(self, num_sets: int, d_sum: int) -> None:
+    def shard_begin(self, num_sets: int, d_sum: int) -> int:
         """This pool's counts over sets [0, num_sets) into the device array
         at address ``d_sum`` (n uint32), and its vertex -> sets index
-        (``rip_shard_begin``)."""
-        self._chk(lib.rip_shard_begin(self.h, num_sets, d_sum), "rip_shard_begin")
+        (``rip_shard_begin``); returns those sets' element count."""
+        e = ctypes.c_uint64()
+        self._chk(lib.rip_shard_begin(self.h, num_sets, d_sum, ctypes.byref(e)),
+                  "rip_shard_begin")
+        return e.value
 
     def shard_pick(self, d_sum: int) -> Tuple[int, int]:
         """(vertex, count) of the largest entry of the device array at
@@ -514,6 +517,19 @@ class Pool:
         """Covers this pool's sets holding ``vertex`` and writes its updated
         counts to ``d_sum`` (``rip_shard_cover``)."""
         self._chk(lib.rip_shard_cover(self.h, vertex, gain, d_sum), "rip_shard_cover")
+
+    def shard_cover_list(self, vertex: int, gain: int, d_dec: int, capacity: int) -> int:
+        """Covers this pool's sets holding ``vertex`` and writes their members
+        to the device array at ``d_dec``; returns how many
+        (``rip_shard_cover_list``)."""
+        c = ctypes.c_uint64()
+        self._chk(lib.rip_shard_cover_list(self.h, vertex, gain, d_dec, capacity,
+                                           ctypes.byref(c)), "rip_shard_cover_list")
+        return c.value
+
+    def shard_apply(self, d_sum: int, d_dec: int, count: int) -> None:
+        """Subtracts one from ``d_sum`` per listed vertex (``rip_shard_apply``)."""
+        self._chk(lib.rip_shard_apply(self.h, d_sum, d_dec, count), "rip_shard_apply")
 
     def export(self, first: int = 0, count: Optional[int] = None) -> Tuple[np.ndarray, np.ndarray]:
         if count is None:

@@ -51,14 +51,25 @@ class OracleShard:
         self.cnt = np.bincount(self.members, minlength=self.n).astype(np.int64)
         return torch.from_numpy(self.cnt.astype(np.int32))
 
-    def cover(self, v, gain):
-        import torch
+    def _cover(self, v):
         sets = np.unique(self.set_of[self.members == v])
         sets = sets[~self.covered[sets]]
         self.covered[sets] = True
-        for s in sets:
-            np.subtract.at(self.cnt, self.members[self.start[s]:self.start[s + 1]], 1)
+        dec = [self.members[self.start[s]:self.start[s + 1]] for s in sets]
+        return np.concatenate(dec) if dec else np.zeros(0, np.int64)
+
+    def cover(self, v, gain):
+        import torch
+        np.subtract.at(self.cnt, self._cover(v), 1)
         return torch.from_numpy(self.cnt.astype(np.int32))
+
+    def cover_list(self, v, gain):
+        import torch
+        return torch.from_numpy(self._cover(v).astype(np.int32))
+
+    def apply(self, total, dec):
+        t = total.numpy()  # shares the tensor's memory
+        np.subtract.at(t, dec.numpy(), 1)
 
     def pick(self, total):
         t = total.numpy().view(np.uint32)
@@ -85,12 +96,13 @@ def oracle_answer(model, g):
                  seed=QUERY["seed"], tiebreak=1)
 
 
-def run_sharded(model, g, local, group=None):
+def run_sharded(model, g, local, group=None, exchange="sparse"):
     from oracle import oracle as O
     from ripples_b200.sharded import imm_sharded
     thr = O.pack(model, g.index, g.weights)
     shards = [OracleShard(model, g, thr) for _ in range(local)]
-    seeds, rec = imm_sharded(shards, QUERY["k"], QUERY["epsilon"], 1.0, QUERY["seed"], group)
+    seeds, rec = imm_sharded(shards, QUERY["k"], QUERY["epsilon"], 1.0, QUERY["seed"], group,
+                             exchange)
     return seeds, rec, shards
 
 
@@ -106,9 +118,10 @@ def test_split_ranges_tile_each_growth():
 
 @pytest.mark.parametrize("model", ["IC", "LT"])
 @pytest.mark.parametrize("local", [1, 3])
-def test_one_process_shards_equal_single_pool(model, local):
+@pytest.mark.parametrize("exchange", ["sparse", "dense"])
+def test_one_process_shards_equal_single_pool(model, local, exchange):
     g = graph(model)
-    seeds, rec, shards = run_sharded(model, g, local)
+    seeds, rec, shards = run_sharded(model, g, local, exchange=exchange)
     o = oracle_answer(model, g)
     assert seeds == o["seeds"]
     assert rec["theta"] == o["theta"]
@@ -128,7 +141,7 @@ def _free_port():
         return s.getsockname()[1]
 
 
-def _rank(rank, world, port, model, local, out):
+def _rank(rank, world, port, model, local, exchange, out):
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     sys.path.insert(0, ROOT)
@@ -137,21 +150,24 @@ def _rank(rank, world, port, model, local, out):
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=120))
     try:
         g = graph(model)
-        seeds, rec, shards = run_sharded(model, g, local, group=dist.group.WORLD)
+        seeds, rec, shards = run_sharded(model, g, local, group=dist.group.WORLD,
+                                         exchange=exchange)
         owned = [int(sum(l > 0 for l in s.lens)) for s in shards]
         out.put((rank, seeds, rec["theta"], rec["theta_prime_deltas"], rec["f"],
-                 rec["total_sets"], owned))
+                 rec["total_sets"], owned, rec["exchanged"]))
     finally:
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("model,local", [("IC", 2), ("LT", 1)])
-def test_two_gloo_ranks_equal_single_pool(model, local):
+@pytest.mark.parametrize("model,local,exchange", [("IC", 2, "sparse"), ("LT", 1, "sparse"),
+                                                  ("IC", 1, "dense")])
+def test_two_gloo_ranks_equal_single_pool(model, local, exchange):
     import torch.multiprocessing as mp
     ctx = mp.get_context("spawn")
     out = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_rank, args=(r, 2, port, model, local, out)) for r in range(2)]
+    procs = [ctx.Process(target=_rank, args=(r, 2, port, model, local, exchange, out))
+             for r in range(2)]
     for p in procs:
         p.start()
     res = sorted(out.get(timeout=240) for _ in procs)
@@ -159,10 +175,12 @@ def test_two_gloo_ranks_equal_single_pool(model, local):
         p.join(timeout=60)
         assert p.exitcode == 0
     o = oracle_answer(model, graph(model))
-    for _, seeds, theta, deltas, f, total, owned in res:
+    for _, seeds, theta, deltas, f, total, owned, exchanged in res:
         assert seeds == o["seeds"]
         assert theta == o["theta"] and deltas == o["deltas"] and total == o["total_sets"]
         assert f == o["f"]
+        # sparse: decrement lists crossed between the ranks; dense: none
+        assert (exchanged > 0) == (exchange == "sparse")
     # the ranks sampled disjoint shares that add up to every set
     assert sum(sum(r[6]) for r in res) == o["total_sets"]
     assert all(min(r[6]) > 0 for r in res)
