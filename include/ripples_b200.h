@@ -539,8 +539,8 @@ int rip_server_stats(const rip_server *s, uint64_t out[10]);
  *            4 736 rip_sample runs on a B200, so large graphs sample far more
  *            slowly here.
  *   Rules  : the first call on a device looks up the array's address with
- *            cudaGetSymbolAddress and the device's SM count; make that first
- *            call before any stream capture.  The cached address belongs to
+ *            cudaGetSymbolAddress and the device's SM count and caches
+ *            both.  The cached address belongs to
  *            the device's primary context: do not call again after a
  *            cudaDeviceReset of that device.  Every call shares the array and
  *            it keeps the last call's contents (each call re-zeroes what must

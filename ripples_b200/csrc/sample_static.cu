@@ -28,8 +28,8 @@
 //     (376 warps at any n); a walk may grow to about 786 000 vertices.
 //   * The first call on a device looks up the array's device address with
 //     cudaGetSymbolAddress (with that device current) and the device's SM
-//     count, and caches both; make that first call before any stream capture.
-//     Every call then synchronises `stream` before it returns.
+//     count, and caches both.  Every call synchronises `stream` before it
+//     returns.
 //   * The cached address belongs to the device's primary context: after a
 //     cudaDeviceReset on that device the process must not call this entry
 //     point again.
