@@ -121,7 +121,7 @@ class ShardedSelection:
         self.exchange = exchange
         self._total = None
         self.allreduce_ms = 0.0  # host ms in collectives (sums and gathers)
-        self.exchanged = 0  # decrement entries this rank gathered (sparse exchange)
+        self.exchanged = 0  # decrement entries this rank received, padding included
         self.picks = 0
 
     def _sum(self, parts):
