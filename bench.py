@@ -60,12 +60,13 @@ WORKLOADS = {
     # clients: concurrent IMM clients of the timed region (a query's
     # reference-heap selection waits on the host while another's sampling and
     # picks use the GPU): 3 on the 2^24 IC graph (1, 2, 3, 4 clients: 5.5,
-    # 6.6, 7.2, 6.7 M sets/s), 8 on LT (1 to 4: 2.8, 5.0, 7.0, 7.9 M sets/s;
-    # 6: 11.3-11.8 M; 8: 13.3 M).
+    # 6.6, 7.2, 6.7 M sets/s), 12 on LT (1 to 4: 2.8, 5.0, 7.0, 7.9 M sets/s;
+    # 6: 11.3-11.8 M; 8: 13.3 M; 10: 13.2 M; 12: 13.1-14.9 M, on 16 host
+    # threads).
     "ic24": dict(name="imm_ic_rmat24_deg32_wc_k100_eps0.13", scale=24, draws=32 << 24,
                  model="IC", k=100, eps=0.13, weights="wc", clients=3),
     "lt20": dict(name="imm_lt_rmat20_deg16_k50_eps0.3", scale=20, draws=16 << 20, model="LT",
-                 k=50, eps=0.3, weights="lt_normalized", clients=8),
+                 k=50, eps=0.3, weights="lt_normalized", clients=12),
     "ic14": dict(name="imm_ic_rmat14_2^18_k20_eps0.5", scale=14, draws=1 << 18, model="IC",
                  k=20, eps=0.5, weights="uniform_0_0.1"),
     # 64 IMM instances over 16 graphs (ER + R-MAT, 2^12..2^22 vertices, average
